@@ -1,0 +1,79 @@
+// aok_common.cuh -- device helpers shared by the overlap and orbital kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "aok.h"
+
+namespace aok {
+
+constexpr int kMaxL = AOK_MAX_L;
+constexpr int kTileB = 32;          // batch elements per tile (one per lane)
+constexpr int kMaxPanels = 16;
+constexpr int kMaxShells = 64;
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// Cartesian component c of a shell of momentum l, in the reference's order
+// (kernels_2c.jl:201-217): for x = l..0, for z = 0..l-x: (x, y = l-x-z, z).
+__host__ __device__ constexpr int cart_x(int l, int c) {
+    int idx = 0;
+    for (int x = l; x >= 0; --x)
+        for (int z = 0; z <= l - x; ++z) {
+            if (idx == c) return x;
+            ++idx;
+        }
+    return 0;
+}
+__host__ __device__ constexpr int cart_z(int l, int c) {
+    int idx = 0;
+    for (int x = l; x >= 0; --x)
+        for (int z = 0; z <= l - x; ++z) {
+            if (idx == c) return z;
+            ++idx;
+        }
+    return 0;
+}
+__host__ __device__ constexpr int cart_y(int l, int c) { return l - cart_x(l, c) - cart_z(l, c); }
+
+// Accumulator elements per work item (register budget); larger shell-pair
+// blocks are split into chunks of output elements.
+__host__ __device__ constexpr int max_elems() { return 36; }
+__host__ __device__ constexpr int nchunks(int ne) { return (ne + max_elems() - 1) / max_elems(); }
+
+// Error-free sum a + b = s + e (Knuth TwoSum).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = a + b;
+    float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// Primitive-pair record of one (species pair, shell pair): everything that
+// does not depend on the geometry, computed once per call in FP64.
+//   w    = c_a c_b (pi/p)^{3/2}          mu = a b / p   (hi + lo for FP32)
+//   ra   = a/p,  rb = b/p,  oo2p = 1/(2p), flush = last pair of its ip row.
+struct PPf {
+    float w, mu_hi, mu_lo, ra, rb, oo2p, flush, pad;
+};
+struct PPd {
+    double w, mu, ra, rb, oo2p, flush, pad0, pad1;
+};
+template <typename FT> struct PPT;
+template <> struct PPT<float> { using type = PPf; };
+template <> struct PPT<double> { using type = PPd; };
+
+// Work item: a shell pair (sa, sb), or a chunk of its output elements.
+struct Item {
+    int16_t cls;    // la*4 + lb
+    int16_t chunk;
+    int16_t sa, sb;
+};
+
+struct Panels {
+    int n;                          // number of panels
+    int col0[kMaxPanels + 1];       // first output column of each panel (+ N)
+    int item0[kMaxPanels + 1];      // first item of each panel in the item list
+};
+
+}  // namespace aok

@@ -1,0 +1,116 @@
+// aok_internal.h -- host-side plan objects and kernel launchers (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "aok.h"
+#include "aok_common.cuh"
+
+struct aok_plan {
+    int64_t ns = 0, K = 0, NZ = 0, N = 0, max_batch = 0;
+    int Lmax = 0;
+    int prec = AOK_PREC_F64;
+    int device = 0;
+    int num_sms = 0;
+    std::vector<int64_t> ls, boff;
+    // shell tables on the device
+    int* d_ls = nullptr;             // ns
+    int* d_boff = nullptr;           // ns+1
+    // primitive-pair records (NZ*NZ*ns*ns*K*K) and counts (NZ*NZ*ns*ns)
+    void* d_pp = nullptr;
+    int* d_npp = nullptr;
+    // species-pair bins: permutation, tiles, tile count, work counter
+    int* d_perm = nullptr;
+    int4* d_tiles = nullptr;
+    int* d_ntiles = nullptr;
+    unsigned* d_counter = nullptr;
+    int max_tiles = 0;
+    // device error word (AOK_ERR_* of the first fault a kernel met)
+    int* d_err = nullptr;
+    // 2C forward schedule
+    aok::Item* d_items = nullptr;
+    int nitems = 0;
+    aok::Panels panels{};
+    size_t slab_stride = 0;          // elements per batch slot in the panel buffer
+    size_t smem_bytes = 0;
+    // GaussianBasis-path padded tables (ns*K)
+    void* d_gb_zeta = nullptr;
+    void* d_gb_coef = nullptr;
+    // pullback: per-block partials and scratch coef
+    void* d_partials = nullptr;
+    int max_blocks = 0;
+    void* d_coef_scratch = nullptr;  // ns*K*NZ
+    void* d_dcoef_scratch = nullptr; // ns*K*NZ
+    void* d_dalpha_scratch = nullptr;
+    // 3C schedule
+    void* d_pp3 = nullptr;
+    int* d_npp3 = nullptr;
+    aok::Item* d_items3 = nullptr;
+    int nitems3 = 0;
+    // optional event pairs around the dominant kernel (measurement aid)
+    std::vector<cudaEvent_t> ev;
+    int ev_used = 0;
+};
+
+struct aok_orbitals {
+    int64_t nRad = 0, K = 0, NZ = 0, nOrb = 0;
+    int L = 0;
+    int radial = AOK_RADIAL_GAUSSIAN;
+    int prec = AOK_PREC_F64;
+    int device = 0;
+    int num_sms = 0;
+    std::vector<int64_t> poly, iR, iY;
+    int* d_poly = nullptr;
+    int* d_iR = nullptr;
+    int* d_iY = nullptr;
+    void* d_partials = nullptr;
+    int max_blocks = 0;
+    int* d_err = nullptr;
+};
+
+namespace aok {
+
+// error helpers (api.cu)
+int set_error(int code, const std::string& msg);
+int cuda_status(cudaError_t e, const char* what);
+
+// timing aid (api.cu): record the pair's first/second event on `s`
+void timing_begin(aok_plan* p, cudaStream_t s);
+void timing_end(aok_plan* p, cudaStream_t s);
+
+// launchers (overlap2c.cu)
+int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s);
+int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s);
+int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB, int64_t B,
+                     double lengthscale, cudaStream_t s);
+int launch_gb_pad(aok_plan* p, const int64_t* nprim, const int64_t* prim_offset, const void* coef,
+                  const void* alpha, cudaStream_t s);
+int setup_overlap2c_schedule(aok_plan* p);
+
+// compile_coef.cu
+int launch_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D, cudaStream_t s);
+int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef, const void* zeta,
+                           const void* D, const void* dalpha_add, cudaStream_t s);
+
+// overlap2c_bwd.cu
+int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
+                        const void* coef, const void* posA, const void* posB, int64_t B,
+                        double lengthscale, cudaStream_t s);
+
+// overlap3c.cu
+int setup_overlap3c_schedule(aok_plan* p);
+int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC,
+                     int64_t B, cudaStream_t s);
+
+// orbitals.cu
+int launch_evaluate(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx,
+                    const void* zeta, const void* D, int64_t nX, double lengthscale, cudaStream_t s);
+int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const void* dP,
+                       const void* X, const int64_t* sidx, const void* zeta, const void* D,
+                       int64_t nX, double lengthscale, cudaStream_t s);
+
+}  // namespace aok

@@ -1,0 +1,231 @@
+// api.cu -- the C ABI declared in include/aok.h: plans, validation, error
+// reporting, and the entry points that chain the kernels on the caller's stream.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "aok_internal.h"
+
+namespace aok {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return AOK_OK;
+    return set_error(AOK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+static int dmalloc(T** p, size_t n, const char* what) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    return cuda_status(e, what);
+}
+
+static int dmalloc_bytes(void** p, size_t n, const char* what) {
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(p, n);
+    return cuda_status(e, what);
+}
+
+static void dfree(void* p) {
+    if (p) cudaFree(p);
+}
+
+void timing_begin(aok_plan* p, cudaStream_t s) {
+    if (p->ev.empty() || 2 * p->ev_used + 1 >= (int)p->ev.size()) return;
+    cudaEventRecord(p->ev[2 * p->ev_used], s);
+}
+
+void timing_end(aok_plan* p, cudaStream_t s) {
+    if (p->ev.empty() || 2 * p->ev_used + 1 >= (int)p->ev.size()) return;
+    cudaEventRecord(p->ev[2 * p->ev_used + 1], s);
+    p->ev_used++;
+}
+
+}  // namespace aok
+
+using namespace aok;
+
+#define AOK_TRY(x)                      \
+    do {                                \
+        int _st = (x);                  \
+        if (_st != AOK_OK) return _st;  \
+    } while (0)
+
+extern "C" {
+
+const char* aok_last_error(void) { return g_last_error.c_str(); }
+
+const char* aok_version(void) { return "aok_b200 0.1.0 (sm_100a)"; }
+
+int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t K, int64_t NZ, int precision,
+                    int64_t max_batch) {
+    if (!plan || !ls) return set_error(AOK_ERR_INVALID, "aok_plan_create: null pointer");
+    *plan = nullptr;
+    if (nshells <= 0 || K <= 0 || NZ <= 0 || max_batch < 0)
+        return set_error(AOK_ERR_INVALID, "aok_plan_create: nshells, K, NZ must be positive");
+    if (precision != AOK_PREC_F64 && precision != AOK_PREC_F32C)
+        return set_error(AOK_ERR_INVALID, "aok_plan_create: unknown precision");
+    if (nshells > kMaxShells) return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: more than 64 shells");
+    if (NZ * NZ > 256) return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: more than 16 species");
+    if (max_batch > (int64_t)0x7fffffff - 64)
+        return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: batch larger than 2^31");
+    for (int64_t s = 0; s < nshells; ++s)
+        if (ls[s] < 0 || ls[s] > AOK_MAX_L)
+            return set_error(AOK_ERR_UNSUPPORTED,
+                             "aok_plan_create: shell angular momentum outside 0..3 (compiled classes)");
+    aok_plan* p = new aok_plan();
+    p->ns = nshells;
+    p->K = K;
+    p->NZ = NZ;
+    p->prec = precision;
+    p->max_batch = max_batch;
+    p->ls.assign(ls, ls + nshells);
+    p->boff.assign(nshells + 1, 0);
+    for (int64_t s = 0; s < nshells; ++s) {
+        p->boff[s + 1] = p->boff[s] + ncart((int)ls[s]);
+        p->Lmax = std::max(p->Lmax, (int)ls[s]);
+    }
+    p->N = p->boff[nshells];
+    int st = AOK_OK;
+    auto fail = [&](int code) {
+        aok_plan_destroy(p);
+        return code;
+    };
+    if ((st = cuda_status(cudaGetDevice(&p->device), "cudaGetDevice")) != AOK_OK) return fail(st);
+    if ((st = cuda_status(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device),
+                          "cudaDeviceGetAttribute")) != AOK_OK)
+        return fail(st);
+    const size_t fsz = precision == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
+    const size_t ppsz = precision == AOK_PREC_F64 ? sizeof(PPd) : sizeof(PPf);
+    const size_t npairs = (size_t)(NZ * NZ * nshells * nshells);
+    p->max_tiles = (int)((max_batch + kTileB - 1) / kTileB + NZ * NZ + 1);
+    std::vector<int> ls32(nshells), boff32(nshells + 1);
+    for (int64_t s = 0; s < nshells; ++s) ls32[s] = (int)ls[s];
+    for (int64_t s = 0; s <= nshells; ++s) boff32[s] = (int)p->boff[s];
+    if ((st = dmalloc(&p->d_ls, nshells, "cudaMalloc(ls)")) ||
+        (st = dmalloc(&p->d_boff, nshells + 1, "cudaMalloc(boff)")) ||
+        (st = dmalloc_bytes(&p->d_pp, npairs * K * K * ppsz, "cudaMalloc(pp)")) ||
+        (st = dmalloc(&p->d_npp, npairs, "cudaMalloc(npp)")) ||
+        (st = dmalloc(&p->d_perm, (size_t)max_batch, "cudaMalloc(perm)")) ||
+        (st = dmalloc(&p->d_tiles, (size_t)p->max_tiles, "cudaMalloc(tiles)")) ||
+        (st = dmalloc(&p->d_ntiles, 1, "cudaMalloc(ntiles)")) ||
+        (st = dmalloc(&p->d_counter, 1, "cudaMalloc(counter)")) ||
+        (st = dmalloc(&p->d_err, 1, "cudaMalloc(err)")) ||
+        (st = dmalloc_bytes(&p->d_gb_zeta, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_zeta)")) ||
+        (st = dmalloc_bytes(&p->d_gb_coef, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_coef)")) ||
+        (st = dmalloc_bytes(&p->d_coef_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(coef)")) ||
+        (st = dmalloc_bytes(&p->d_dcoef_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(dcoef)")) ||
+        (st = dmalloc_bytes(&p->d_dalpha_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(dalpha)")))
+        return fail(st);
+    if ((st = cuda_status(cudaMemcpy(p->d_ls, ls32.data(), sizeof(int) * nshells, cudaMemcpyHostToDevice),
+                          "cudaMemcpy(ls)")) ||
+        (st = cuda_status(cudaMemcpy(p->d_boff, boff32.data(), sizeof(int) * (nshells + 1), cudaMemcpyHostToDevice),
+                          "cudaMemcpy(boff)")) ||
+        (st = cuda_status(cudaMemset(p->d_err, 0, sizeof(int)), "cudaMemset(err)")))
+        return fail(st);
+    if ((st = setup_overlap2c_schedule(p)) != AOK_OK) return fail(st);
+    *plan = p;
+    return AOK_OK;
+}
+
+int aok_plan_destroy(aok_plan* p) {
+    if (!p) return AOK_OK;
+    void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_counter,
+                    p->d_err, p->d_items, p->d_gb_zeta, p->d_gb_coef, p->d_partials, p->d_coef_scratch,
+                    p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3, p->d_npp3, p->d_items3};
+    for (void* b : bufs) dfree(b);
+    for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
+    delete p;
+    return AOK_OK;
+}
+
+int aok_plan_nbf(const aok_plan* p, int64_t* nbf_total) {
+    if (!p || !nbf_total) return set_error(AOK_ERR_INVALID, "aok_plan_nbf: null pointer");
+    *nbf_total = p->N;
+    return AOK_OK;
+}
+
+int aok_plan_check(aok_plan* p, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_plan_check: null plan");
+    cudaStream_t s = (cudaStream_t)stream;
+    AOK_TRY(cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize"));
+    int h = 0;
+    AOK_TRY(cuda_status(cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(err)"));
+    AOK_TRY(cuda_status(cudaMemset(p->d_err, 0, sizeof(int)), "cudaMemset(err)"));
+    if (h == AOK_ERR_SPECIES) return set_error(h, "species index outside 1..NZ");
+    if (h != 0) return set_error(h, "device-side validation failed");
+    return AOK_OK;
+}
+
+int aok_plan_timing_enable(aok_plan* p, int capacity) {
+    if (!p || capacity < 0) return set_error(AOK_ERR_INVALID, "aok_plan_timing_enable: bad argument");
+    for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
+    p->ev.clear();
+    p->ev_used = 0;
+    for (int i = 0; i < 2 * capacity; ++i) {
+        cudaEvent_t e;
+        AOK_TRY(cuda_status(cudaEventCreate(&e), "cudaEventCreate"));
+        p->ev.push_back(e);
+    }
+    return AOK_OK;
+}
+
+int aok_plan_timing_read(aok_plan* p, double* total_ms, int64_t* launches) {
+    if (!p || !total_ms || !launches) return set_error(AOK_ERR_INVALID, "aok_plan_timing_read: null pointer");
+    double tot = 0.0;
+    for (int i = 0; i < p->ev_used; ++i) {
+        AOK_TRY(cuda_status(cudaEventSynchronize(p->ev[2 * i + 1]), "cudaEventSynchronize"));
+        float ms = 0.f;
+        AOK_TRY(cuda_status(cudaEventElapsedTime(&ms, p->ev[2 * i], p->ev[2 * i + 1]), "cudaEventElapsedTime"));
+        tot += ms;
+    }
+    *total_ms = tot;
+    *launches = p->ev_used;
+    p->ev_used = 0;
+    return AOK_OK;
+}
+
+static int check_batch(aok_plan* p, int64_t B, const char* who) {
+    if (B < 0) return set_error(AOK_ERR_INVALID, std::string(who) + ": negative batch");
+    if (B > p->max_batch)
+        return set_error(AOK_ERR_LENGTH, std::string(who) + ": batch exceeds the plan's max_batch");
+    return AOK_OK;
+}
+
+int aok_overlap2c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
+                  const int64_t* sidxA, const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c: null plan");
+    AOK_TRY(check_batch(p, B, "aok_overlap2c"));
+    if (B == 0) return AOK_OK;
+    if (!out || !zeta || !coef || !posA || !posB || !sidxA || !sidxB)
+        return set_error(AOK_ERR_INVALID, "aok_overlap2c: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    AOK_TRY(launch_prep2c(p, zeta, coef, s));
+    AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+    return launch_overlap2c(p, out, posA, posB, B, lengthscale, s);
+}
+
+int aok_overlap2c_gb(aok_plan* p, void* out, const int64_t* nprim, const int64_t* prim_offset, const void* coef,
+                     const void* alpha, const void* posA, const void* posB, int64_t B, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c_gb: null plan");
+    if (p->NZ != 1) return set_error(AOK_ERR_INVALID, "aok_overlap2c_gb: plan must have NZ = 1");
+    AOK_TRY(check_batch(p, B, "aok_overlap2c_gb"));
+    if (B == 0) return AOK_OK;
+    if (!out || !nprim || !prim_offset || !coef || !alpha || !posA || !posB)
+        return set_error(AOK_ERR_INVALID, "aok_overlap2c_gb: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    AOK_TRY(launch_gb_pad(p, nprim, prim_offset, coef, alpha, s));
+    AOK_TRY(launch_prep2c(p, p->d_gb_zeta, p->d_gb_coef, s));
+    AOK_TRY(launch_bin(p, nullptr, nullptr, B, s));
+    return launch_overlap2c(p, out, posA, posB, B, 1.0, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// compile_coef.cu -- spherical -> Cartesian contraction normalisation and its VJP
+// on the device, so a (zeta, D) gradient step never leaves the GPU.
+//
+// Replaces _cart_normsq / _compile_coef (src/integrals/orbital/cartesian_gto_basis.jl:74-120)
+// and _compile_coef_pb (src/integrals/orbital/overlap_2c_grad.jl:251-286):
+//   normsq = c sum_ij D_i D_j / (z_i + z_j)^e,  c = pi^{3/2} (2l-1)!! / 2^l,  e = l + 3/2
+//   coef   = D / sqrt(normsq)            (zero when normsq <= 0: absent shell)
+//   dD_m   = dcoef_m / n - g_m dot / (2 n^3),  g_m = 2c sum_j D_j / (z_m+z_j)^e
+//   dz_m   = -h_m dot / (2 n^3),  h_m = -2c e D_m sum_j D_j / (z_m+z_j)^{e+1}
+// with dot = sum_i dcoef_i D_i and n = sqrt(normsq).  One thread per
+// (shell, species); K is small.  All arithmetic is FP64 (also for FP32 data:
+// these are the primitive normalisation constants).
+#include "aok_internal.h"
+
+namespace aok {
+
+__device__ __forceinline__ double cart_dfac(int n) {
+    double p = 1.0;
+    for (int k = n; k > 1; k -= 2) p *= k;
+    return p;
+}
+
+__device__ __forceinline__ double norm_c(int l) {
+    const double pi15 = 5.568327996831707845;  // pi^{3/2}
+    return (pi15 * (l == 0 ? 1.0 : cart_dfac(2 * l - 1))) / (double)(1 << l);
+}
+
+template <typename FT>
+__global__ void k_compile_coef(FT* __restrict__ coef, const FT* __restrict__ zeta, const FT* __restrict__ D,
+                               const int* __restrict__ ls, int ns, int K, int NZ) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns * NZ) return;
+    int s = q % ns, g = q / ns;
+    int l = ls[s];
+    const double e = (double)l + 1.5;
+    const size_t base = (size_t)s + (size_t)ns * K * g;
+    double acc = 0.0;
+    for (int i = 0; i < K; ++i)
+        for (int j = 0; j < K; ++j) {
+            double Di = (double)D[base + (size_t)ns * i], Dj = (double)D[base + (size_t)ns * j];
+            double zz = (double)zeta[base + (size_t)ns * i] + (double)zeta[base + (size_t)ns * j];
+            acc += (Di * Dj) / pow(zz, e);
+        }
+    double nsq = norm_c(l) * acc;
+    double n = nsq > 0.0 ? sqrt(nsq) : 0.0;
+    for (int m = 0; m < K; ++m)
+        coef[base + (size_t)ns * m] = nsq > 0.0 ? (FT)((double)D[base + (size_t)ns * m] / n) : FT(0);
+}
+
+template <typename FT>
+__global__ void k_compile_coef_pb(FT* __restrict__ dD, FT* __restrict__ dz, const FT* __restrict__ dcoef,
+                                  const FT* __restrict__ zeta, const FT* __restrict__ D,
+                                  const FT* __restrict__ dalpha_add, const int* __restrict__ ls, int ns, int K,
+                                  int NZ) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns * NZ) return;
+    int s = q % ns, g = q / ns;
+    int l = ls[s];
+    const double e = (double)l + 1.5;
+    const double c = norm_c(l);
+    const size_t base = (size_t)s + (size_t)ns * K * g;
+    auto Dv = [&](int i) { return (double)D[base + (size_t)ns * i]; };
+    auto zv = [&](int i) { return (double)zeta[base + (size_t)ns * i]; };
+    double acc = 0.0;
+    for (int i = 0; i < K; ++i)
+        for (int j = 0; j < K; ++j) acc += (Dv(i) * Dv(j)) / pow(zv(i) + zv(j), e);
+    double nsq = c * acc;
+    if (!(nsq > 0.0)) {
+        for (int m = 0; m < K; ++m) {
+            size_t o = base + (size_t)ns * m;
+            dD[o] = FT(0);
+            dz[o] = dalpha_add ? dalpha_add[o] : FT(0);
+        }
+        return;
+    }
+    double n = sqrt(nsq);
+    double dot = 0.0;
+    for (int i = 0; i < K; ++i) dot += (double)dcoef[base + (size_t)ns * i] * Dv(i);
+    double s2n3 = dot / (2.0 * ((n * n) * n));
+    for (int m = 0; m < K; ++m) {
+        double gm = 0.0, hm = 0.0;
+        for (int j = 0; j < K; ++j) {
+            double den = zv(m) + zv(j);
+            double p = pow(den, e);
+            gm += Dv(j) / p;
+            hm += Dv(j) / (p * den);
+        }
+        gm *= 2.0 * c;
+        hm *= ((-2.0 * c) * e) * Dv(m);
+        size_t o = base + (size_t)ns * m;
+        dD[o] = (FT)((double)dcoef[o] / n - gm * s2n3);
+        double dzn = -hm * s2n3;
+        dz[o] = dalpha_add ? (FT)((double)dalpha_add[o] + dzn) : (FT)dzn;
+    }
+}
+
+int launch_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D, cudaStream_t s) {
+    int n = (int)(p->ns * p->NZ), th = 64, bl = (n + th - 1) / th;
+    if (p->prec == AOK_PREC_F64)
+        k_compile_coef<double><<<bl, th, 0, s>>>((double*)coef, (const double*)zeta, (const double*)D, p->d_ls,
+                                                 (int)p->ns, (int)p->K, (int)p->NZ);
+    else
+        k_compile_coef<float><<<bl, th, 0, s>>>((float*)coef, (const float*)zeta, (const float*)D, p->d_ls,
+                                                (int)p->ns, (int)p->K, (int)p->NZ);
+    return cuda_status(cudaGetLastError(), "k_compile_coef");
+}
+
+int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef, const void* zeta, const void* D,
+                           const void* dalpha_add, cudaStream_t s) {
+    int n = (int)(p->ns * p->NZ), th = 64, bl = (n + th - 1) / th;
+    if (p->prec == AOK_PREC_F64)
+        k_compile_coef_pb<double><<<bl, th, 0, s>>>((double*)dD, (double*)dzeta, (const double*)dcoef,
+                                                    (const double*)zeta, (const double*)D,
+                                                    (const double*)dalpha_add, p->d_ls, (int)p->ns, (int)p->K,
+                                                    (int)p->NZ);
+    else
+        k_compile_coef_pb<float><<<bl, th, 0, s>>>((float*)dD, (float*)dzeta, (const float*)dcoef,
+                                                   (const float*)zeta, (const float*)D, (const float*)dalpha_add,
+                                                   p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
+    return cuda_status(cudaGetLastError(), "k_compile_coef_pb");
+}
+
+}  // namespace aok
+
+using namespace aok;
+
+extern "C" int aok_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D, void* stream) {
+    if (!p || !coef || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_compile_coef: null pointer");
+    return launch_compile_coef(p, coef, zeta, D, (cudaStream_t)stream);
+}
+
+extern "C" int aok_compile_coef_pullback(aok_plan* p, void* dD, void* dzeta, const void* dcoef, const void* zeta,
+                                         const void* D, void* stream) {
+    if (!p || !dD || !dzeta || !dcoef || !zeta || !D)
+        return set_error(AOK_ERR_INVALID, "aok_compile_coef_pullback: null pointer");
+    return launch_compile_coef_pb(p, dD, dzeta, dcoef, zeta, D, nullptr, (cudaStream_t)stream);
+}

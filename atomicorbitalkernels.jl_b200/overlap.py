@@ -1,0 +1,306 @@
+"""Batched 2- and 3-center overlaps and their (zeta, D) pullback: the reference's
+public API (names, argument meaning, errors) over the CUDA library.
+
+  batch_overlap_ / batch_overlap (GaussianBasis path)   kernels_2c.jl:247-283
+  batch_overlap_ / batch_overlap (species-aware path)   orbital/overlap_2c.jl:321-385
+  batch_overlap(orb, XA, XB, ps, st) (Lux form)         orbital/overlap_2c_grad.jl:41-57
+  batch_overlap_3c_ / batch_overlap_3c                  kernels_3c.jl:183-222
+  pullback_ps(dS, orb, XA, XB, ps, st), rrule           orbital/overlap_2c_grad.jl:296-318
+
+Julia's mutating `f!` is spelled `f_` here.  Mutating forms take a device
+output tensor in the reference's shape (a column-major view, see _dev.py) and
+return it; the allocating forms return a host (CPU) tensor like the
+reference's CPU `zeros(...)` allocation.
+"""
+import numpy as np
+import torch
+
+from . import _dev, _lib
+from .basis import (AtomicOrbitals, CartesianGTOBasis, CompiledBasis, as_pstates, compile_basis,
+                    compile_struct, species_indices)
+from .units import to_bohr
+
+NoTangent = None
+
+
+class _NoTangent:
+    def __repr__(self):
+        return "NoTangent()"
+
+
+NoTangent = _NoTangent()
+
+
+def _check_out(out, shape, who):
+    if not torch.is_tensor(out) or out.device.type != "cuda":
+        raise _lib.ArgumentError(f"{who}: `out` must be a CUDA tensor")
+    if tuple(out.shape) != tuple(shape):
+        raise _lib.ArgumentError(f"{who}: `out` has shape {tuple(out.shape)}, expected {tuple(shape)}")
+    if not _dev.is_colmajor(out):
+        raise _lib.ArgumentError(f"{who}: `out` must be column-major (use colmajor_empty)")
+
+
+def _dev_int64(a):
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(a, dtype=np.int64))).to("cuda")
+
+
+# --------------------------------------------------------------------------
+# normalisation (cartesian_gto_basis.jl:110-120) and its VJP
+# --------------------------------------------------------------------------
+
+
+def compile_coef(zeta, D, ls):
+    """_compile_coef on the device: coef = D / sqrt(normsq) per shell/species."""
+    _dev.require_cuda()
+    ns, K, NZ = zeta.shape
+    zeta = _dev.to_colmajor(zeta, zeta.dtype if torch.is_tensor(zeta) else torch.float64)
+    D = _dev.to_colmajor(D, zeta.dtype)
+    plan = _dev.plan_for(ls, K, NZ, _dev.prec_of(zeta.dtype), 1)
+    coef = _dev.colmajor_empty((ns, K, NZ), zeta.dtype)
+    _lib.check(_lib.load().aok_compile_coef(plan.h, _dev.ptr(coef), _dev.ptr(zeta), _dev.ptr(D), _dev.stream()))
+    return coef
+
+
+def compile_coef_pb(dcoef, zeta, D, ls):
+    """_compile_coef_pb (overlap_2c_grad.jl:251-286) -> (dD, dzeta_norm)."""
+    _dev.require_cuda()
+    ns, K, NZ = zeta.shape
+    dt = zeta.dtype if torch.is_tensor(zeta) else torch.float64
+    zeta, D, dcoef = _dev.to_colmajor(zeta, dt), _dev.to_colmajor(D, dt), _dev.to_colmajor(dcoef, dt)
+    plan = _dev.plan_for(ls, K, NZ, _dev.prec_of(dt), 1)
+    dD = _dev.colmajor_empty((ns, K, NZ), dt)
+    dz = _dev.colmajor_empty((ns, K, NZ), dt)
+    _lib.check(_lib.load().aok_compile_coef_pullback(plan.h, _dev.ptr(dD), _dev.ptr(dz), _dev.ptr(dcoef),
+                                                     _dev.ptr(zeta), _dev.ptr(D), _dev.stream()))
+    return dD, dz
+
+
+# --------------------------------------------------------------------------
+# 2C: GaussianBasis path
+# --------------------------------------------------------------------------
+
+
+def _gb_overlap_(out, bc, posA, posB):
+    FT = out.dtype
+    npft = np.float64 if FT == torch.float64 else np.float32
+    pa = to_bohr(posA, npft)
+    pb = to_bohr(posB, npft)
+    B = pa.shape[1]
+    if pb.shape[1] != B:
+        raise _lib.ArgumentError("posA and posB must have the same number of columns")
+    _check_out(out, (bc.nbf_total, bc.nbf_total, B), "batch_overlap!")
+    if B == 0:
+        return out
+    _dev.require_cuda()
+    K = int(np.max(np.asarray(bc.nprim.cpu() if torch.is_tensor(bc.nprim) else bc.nprim)))
+    ls = np.asarray(bc.ls.cpu() if torch.is_tensor(bc.ls) else bc.ls)
+    plan = _dev.plan_for(ls, K, 1, _dev.prec_of(FT), B)
+    dA, dB = _dev.to_colmajor(pa, FT), _dev.to_colmajor(pb, FT)
+    nprim = _dev.to_colmajor(bc.nprim, torch.int64)
+    off = _dev.to_colmajor(bc.prim_offset, torch.int64)
+    coef = _dev.to_colmajor(bc.coef, FT)
+    alpha = _dev.to_colmajor(bc.alpha, FT)
+    _lib.check(_lib.load().aok_overlap2c_gb(plan.h, _dev.ptr(out), _dev.ptr(nprim), _dev.ptr(off), _dev.ptr(coef),
+                                            _dev.ptr(alpha), _dev.ptr(dA), _dev.ptr(dB), B, _dev.stream()))
+    return out
+
+
+# --------------------------------------------------------------------------
+# 2C: species-aware path
+# --------------------------------------------------------------------------
+
+
+def _pstate_inputs(basis, XA, XB, FT):
+    XA, XB = as_pstates(XA), as_pstates(XB)
+    B = len(XA)
+    if len(XB) != B:
+        raise RuntimeError(f"XA and XB must have equal length; got {len(XA)} and {len(XB)}")
+    sA = species_indices(basis.zlist, XA.species)
+    sB = species_indices(basis.zlist, XB.species)
+    return XA, XB, sA, sB, B
+
+
+def _orb_overlap_(out, cob, XA, XB, zeta=None, coef=None):
+    FT = out.dtype
+    XA, XB, sA, sB, B = _pstate_inputs(cob, XA, XB, FT)
+    _check_out(out, (cob.nbf_total, cob.nbf_total, B), "batch_overlap!")
+    if B == 0:
+        return out
+    _dev.require_cuda()
+    plan = _dev.plan_for(cob.ls, cob.K, cob.nspecies, _dev.prec_of(FT), B)
+    zeta = _dev.to_colmajor(cob.zeta if zeta is None else zeta, FT)
+    coef = _dev.to_colmajor(cob.coef if coef is None else coef, FT)
+    dA, dB = _dev.to_colmajor(XA.pos, FT), _dev.to_colmajor(XB.pos, FT)
+    gA, gB = _dev_int64(sA), _dev_int64(sB)
+    _lib.check(_lib.load().aok_overlap2c(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(dA),
+                                         _dev.ptr(dB), _dev.ptr(gA), _dev.ptr(gB), B, float(cob.lengthscale),
+                                         _dev.stream()))
+    return out
+
+
+def _compiled_from_ps(orb, ps, FT):
+    """_compiled_from_ps (overlap_2c_grad.jl:22-30): coef recomputed from ps on the device."""
+    st = compile_struct(orb)
+    zeta = _dev.to_colmajor(ps["Rnl"]["zeta"], FT)
+    D = _dev.to_colmajor(ps["Rnl"]["D"], FT)
+    coef = compile_coef(zeta, D, st["ls"])
+    return CartesianGTOBasis(st["Lmax"], st["nshells"], st["K"], st["ls"], st["nbf"], st["basis_offset"],
+                             st["nbf_total"], zeta, coef, st["zlist"], orb.lengthscale), D
+
+
+def _ps_dtype(ps, XA):
+    z = ps["Rnl"]["zeta"]
+    if torch.is_tensor(z):
+        return z.dtype
+    return torch.float32 if np.asarray(z).dtype == np.float32 else torch.float64
+
+
+def batch_overlap_(out, basis, *args):
+    """batch_overlap!(out, basis, ...) for CompiledBasis (Length positions), CartesianGTOBasis
+    (PState batches), AtomicOrbitals (compile-on-call) and the Lux (ps, st) form."""
+    if isinstance(basis, CompiledBasis):
+        posA, posB = args
+        return _gb_overlap_(out, basis, posA, posB)
+    if isinstance(basis, CartesianGTOBasis):
+        XA, XB = args
+        return _orb_overlap_(out, basis, XA, XB)
+    if isinstance(basis, AtomicOrbitals):
+        if len(args) == 4:
+            XA, XB, ps, st = args
+            cob, _ = _compiled_from_ps(basis, ps, out.dtype)
+            return _orb_overlap_(out, cob, XA, XB)
+        XA, XB = args
+        return _orb_overlap_(out, compile_basis(basis, dtype=out.dtype), XA, XB)
+    raise TypeError(f"batch_overlap!: unsupported basis {type(basis).__name__}")
+
+
+def batch_overlap(basis, *args, FT=None, device_out=False):
+    """Allocating batch_overlap; returns a host tensor (reference: CPU `zeros`) unless device_out."""
+    if isinstance(basis, CompiledBasis):
+        posA, posB = args
+        FT = FT or torch.float64
+        B = np.shape(posA.value)[1] if hasattr(posA, "value") else np.shape(posA)[1]
+        out = _dev.colmajor_empty((basis.nbf_total, basis.nbf_total, B), FT)
+        batch_overlap_(out, basis, posA, posB)
+    elif isinstance(basis, CartesianGTOBasis):
+        XA, XB = args
+        pos = as_pstates(XA).pos
+        FT = FT or (pos.dtype if torch.is_tensor(pos) and pos.is_floating_point() else
+                    (torch.float32 if np.asarray(pos).dtype == np.float32 else torch.float64))
+        out = _dev.colmajor_empty((basis.nbf_total, basis.nbf_total, len(as_pstates(XA))), FT)
+        batch_overlap_(out, basis, XA, XB)
+    elif isinstance(basis, AtomicOrbitals):
+        if len(args) == 4:
+            XA, XB, ps, st = args
+            FT = FT or _ps_dtype(ps, XA)
+            N = compile_struct(basis)["nbf_total"]
+            out = _dev.colmajor_empty((N, N, len(as_pstates(XA))), FT)
+            batch_overlap_(out, basis, XA, XB, ps, st)
+        else:
+            XA, XB = args
+            cob = compile_basis(basis)
+            return batch_overlap(cob, XA, XB, FT=FT, device_out=device_out)
+    else:
+        raise TypeError(f"batch_overlap: unsupported basis {type(basis).__name__}")
+    return out if device_out else out.cpu()
+
+
+# --------------------------------------------------------------------------
+# 3C (GaussianBasis path)
+# --------------------------------------------------------------------------
+
+
+def batch_overlap_3c_(out, bc, posA, posB, posC):
+    FT = out.dtype
+    npft = np.float64 if FT == torch.float64 else np.float32
+    pa, pb, pc = to_bohr(posA, npft), to_bohr(posB, npft), to_bohr(posC, npft)
+    B = pa.shape[1]
+    if pb.shape[1] != B or pc.shape[1] != B:
+        raise _lib.ArgumentError("posA, posB, posC must have the same number of columns")
+    N = bc.nbf_total
+    _check_out(out, (N, N, N, B), "batch_overlap_3c!")
+    if B == 0:
+        return out
+    _dev.require_cuda()
+    K = int(np.max(np.asarray(bc.nprim.cpu() if torch.is_tensor(bc.nprim) else bc.nprim)))
+    ls = np.asarray(bc.ls.cpu() if torch.is_tensor(bc.ls) else bc.ls)
+    plan = _dev.plan_for(ls, K, 1, _dev.prec_of(FT), B)
+    dA, dB, dC = _dev.to_colmajor(pa, FT), _dev.to_colmajor(pb, FT), _dev.to_colmajor(pc, FT)
+    nprim = _dev.to_colmajor(bc.nprim, torch.int64)
+    off = _dev.to_colmajor(bc.prim_offset, torch.int64)
+    coef = _dev.to_colmajor(bc.coef, FT)
+    alpha = _dev.to_colmajor(bc.alpha, FT)
+    _lib.check(_lib.load().aok_overlap3c_gb(plan.h, _dev.ptr(out), _dev.ptr(nprim), _dev.ptr(off), _dev.ptr(coef),
+                                            _dev.ptr(alpha), _dev.ptr(dA), _dev.ptr(dB), _dev.ptr(dC), B,
+                                            _dev.stream()))
+    return out
+
+
+def batch_overlap_3c(bc, posA, posB, posC, FT=torch.float64, device_out=False):
+    B = np.shape(posA.value)[1]
+    N = bc.nbf_total
+    out = _dev.colmajor_empty((N, N, N, B), FT)
+    batch_overlap_3c_(out, bc, posA, posB, posC)
+    return out if device_out else out.cpu()
+
+
+# --------------------------------------------------------------------------
+# (zeta, D) pullback and rrule
+# --------------------------------------------------------------------------
+
+
+def overlap_pb_coef_alpha(dS, cob, XA, XB):
+    """_overlap_pb_coef_alpha (overlap_2c_grad.jl:218-242) -> (dcoef, dalpha)."""
+    FT = cob.zeta.dtype
+    XA, XB, sA, sB, B = _pstate_inputs(cob, XA, XB, FT)
+    _dev.require_cuda()
+    plan = _dev.plan_for(cob.ls, cob.K, cob.nspecies, _dev.prec_of(FT), B)
+    dS = _dev.to_colmajor(dS, FT)
+    ns, K, NZ = cob.nshells, cob.K, cob.nspecies
+    dcoef = _dev.colmajor_empty((ns, K, NZ), FT)
+    dalpha = _dev.colmajor_empty((ns, K, NZ), FT)
+    dA, dB = _dev.to_colmajor(XA.pos, FT), _dev.to_colmajor(XB.pos, FT)
+    gA, gB = _dev_int64(sA), _dev_int64(sB)
+    _lib.check(_lib.load().aok_overlap2c_pullback(plan.h, _dev.ptr(dcoef), _dev.ptr(dalpha), _dev.ptr(dS),
+                                                  _dev.ptr(_dev.to_colmajor(cob.zeta, FT)),
+                                                  _dev.ptr(_dev.to_colmajor(cob.coef, FT)), _dev.ptr(dA), _dev.ptr(dB),
+                                                  _dev.ptr(gA), _dev.ptr(gB), B, float(cob.lengthscale),
+                                                  _dev.stream()))
+    return dcoef, dalpha
+
+
+def pullback_ps(dS, orb, XA, XB, ps, st):
+    """pullback_ps(dS, orb, XA, XB, ps, st) -> {'Rnl': {'zeta', 'D'}, 'Ylm': {}} (overlap_2c_grad.jl:296-304)."""
+    FT = _ps_dtype(ps, XA)
+    XA, XB = as_pstates(XA), as_pstates(XB)
+    stc = compile_struct(orb)
+    sA = species_indices(stc["zlist"], XA.species)
+    sB = species_indices(stc["zlist"], XB.species)
+    B = len(XA)
+    if len(XB) != B:
+        raise RuntimeError(f"XA and XB must have equal length; got {len(XA)} and {len(XB)}")
+    _dev.require_cuda()
+    ns, K, NZ = stc["nshells"], stc["K"], stc["NZ"]
+    plan = _dev.plan_for(stc["ls"], K, NZ, _dev.prec_of(FT), B)
+    zeta = _dev.to_colmajor(ps["Rnl"]["zeta"], FT)
+    D = _dev.to_colmajor(ps["Rnl"]["D"], FT)
+    dS = _dev.to_colmajor(dS, FT)
+    dz = _dev.colmajor_empty((ns, K, NZ), FT)
+    dD = _dev.colmajor_empty((ns, K, NZ), FT)
+    dA, dB = _dev.to_colmajor(XA.pos, FT), _dev.to_colmajor(XB.pos, FT)
+    gA, gB = _dev_int64(sA), _dev_int64(sB)
+    _lib.check(_lib.load().aok_overlap_pullback_ps(plan.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS), _dev.ptr(zeta),
+                                                   _dev.ptr(D), _dev.ptr(dA), _dev.ptr(dB), _dev.ptr(gA),
+                                                   _dev.ptr(gB), B, float(orb.lengthscale), _dev.stream()))
+    return {"Rnl": {"zeta": dz, "D": dD}, "Ylm": {}}
+
+
+def rrule_batch_overlap(orb, XA, XB, ps, st):
+    """rrule(batch_overlap, orb, XA, XB, ps, st) (overlap_2c_grad.jl:309-318)."""
+    S = batch_overlap(orb, XA, XB, ps, st, device_out=True)
+
+    def _pb(dS):
+        dps = pullback_ps(dS, orb, XA, XB, ps, st)
+        return (NoTangent, NoTangent, NoTangent, NoTangent, dps, NoTangent)
+
+    return S, _pb

@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark: batched 2-center overlap (+ (zeta, D) gradient step) on B200.
+
+Workload (one GPU / one rank): the ragged mixed-species 2C overlap batch --
+4 species with l <= 3 synthetic bases (3-5 s, 2-3 p, 1-2 d, 0-1 f shells,
+K in 1..8 primitives per shell, seeded), B = 65,536 pairs per rank with random
+species pairs, random directions and |A-B| ~ U[0.5, 8] bohr.  A step is one
+forward pass of the FP32-compensated kernel over the whole batch (prep +
+species-pair binning + overlap kernel, all on the device).  Weak scaling: each
+rank processes its own batch, no collective on the data path.
+
+Also reported: the plain FP64 kernel on the same batch, the FP32C error
+against the FP64 oracle, the (zeta, D) gradient step of the overlap loss,
+the dominant kernel's roofline, an end-to-end number through the C ABI with
+host buffers, and the CPU oracle on the host cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl aok|reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "2c-overlap integrals/s + (ζ,D) grad step, FP32-comp vs FP64, 1 B200, rel err"
+UNIT = "integrals/s"
+B_PER_RANK = 65536
+SEED = 1002
+
+
+def _baseline_metric():
+    try:
+        with open(os.path.join(ROOT, "BASELINE.json")) as f:
+            return json.load(f).get("metric", METRIC)
+    except Exception:
+        return METRIC
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def workload(rank=0, B=B_PER_RANK):
+    import aok_b200 as aok
+    W = aok.workloads
+    basis = W.config2_basis(seed=SEED)
+    pairs = W.ragged_pairs(B, basis.NZ, SEED + 7919 * rank)
+    return basis, pairs
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except Exception:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_oracle_rate(basis, pairs, coef, target_s=12.0, nthreads=None):
+    """Integrals/s of the oracle (C, OpenMP) on a bounded sample of the workload."""
+    import oracle
+    nthreads = nthreads or os.cpu_count()
+    N = basis.nbf_total
+    b0 = 256
+    t0 = time.perf_counter()
+    oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[:b0], pairs.sidxB[:b0], pairs.posA[:, :b0],
+                         pairs.posB[:, :b0], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    bs = int(min(pairs.B, max(b0, b0 * target_s / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[:bs], pairs.sidxB[:bs], pairs.posA[:, :bs],
+                         pairs.posB[:, :bs], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return N * N * bs / dt, nthreads, bs, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    basis, pairs = workload(0)
+    coef = oracle.compile_coef(basis.zeta, basis.D, basis.ls)
+    nth = os.cpu_count()
+    N = basis.nbf_total
+    bs = 256
+    # size the per-step sample so the whole run stays within a few minutes
+    t0 = time.perf_counter()
+    oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[:bs], pairs.sidxB[:bs], pairs.posA[:, :bs],
+                         pairs.posB[:, :bs], nthreads=nth)
+    dt = time.perf_counter() - t0
+    per_step = int(min(pairs.B, max(64, bs * 10.0 / max(dt, 1e-6) / max(1, args.steps + args.warmup) * 3)))
+    sl = slice(0, per_step)
+    for _ in range(args.warmup):
+        oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[sl], pairs.sidxB[sl], pairs.posA[:, sl],
+                             pairs.posB[:, sl], nthreads=nth)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[sl], pairs.sidxB[sl], pairs.posA[:, sl],
+                             pairs.posB[:, sl], nthreads=nth)
+    dt = (time.perf_counter() - t0) / args.steps
+    val = N * N * per_step / dt
+    line = {
+        "impl": "reference", "metric": _baseline_metric(), "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "ragged 4-species l<=3 2C overlap, FP64 CPU oracle (C restatement of the "
+                               "reference's KernelAbstractions CPU path; Julia is not installed)",
+                   "batch_per_step": per_step, "nbf": N},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nth, "kind": "port",
+                         "sample": f"{per_step} pairs of the B=65536 batch per step"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="aok", choices=["aok", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+
+    import aok_b200 as aok
+    from aok_b200 import _dev, _lib
+    import oracle
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    L = _lib.load()
+    basis, pairs = workload(rank)
+    N, B, ns, K, NZ = basis.nbf_total, pairs.B, basis.nshells, basis.K, basis.NZ
+    peaks, peak_kind = _peaks()
+
+    def setup(FT):
+        plan = _dev.Plan(basis.ls, K, NZ, _dev.prec_of(FT), B)
+        zeta = _dev.to_colmajor(basis.zeta, FT)
+        D = _dev.to_colmajor(basis.D, FT)
+        coef = _dev.colmajor_empty((ns, K, NZ), FT)
+        _lib.check(L.aok_compile_coef(plan.h, _dev.ptr(coef), _dev.ptr(zeta), _dev.ptr(D), _dev.stream()))
+        pA = _dev.to_colmajor(pairs.posA, FT)
+        pB = _dev.to_colmajor(pairs.posB, FT)
+        sA = torch.as_tensor(pairs.sidxA).cuda()
+        sB = torch.as_tensor(pairs.sidxB).cuda()
+        out = _dev.colmajor_empty((N, N, B), FT)
+        return dict(plan=plan, zeta=zeta, D=D, coef=coef, pA=pA, pB=pB, sA=sA, sB=sB, out=out, FT=FT)
+
+    def step(c):
+        _lib.check(L.aok_overlap2c(c["plan"].h, _dev.ptr(c["out"]), _dev.ptr(c["zeta"]), _dev.ptr(c["coef"]),
+                                   _dev.ptr(c["pA"]), _dev.ptr(c["pB"]), ctypes.c_void_p(c["sA"].data_ptr()),
+                                   ctypes.c_void_p(c["sB"].data_ptr()), B, 1.0, _dev.stream()))
+
+    def timed(c, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            step(c)
+        barrier()
+        torch.cuda.synchronize()
+        _lib.check(L.aok_plan_timing_enable(c["plan"].h, steps))
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            st.record()
+            for _ in range(steps):
+                step(c)
+            en.record()
+            torch.cuda.synchronize()
+        barrier()
+        ms = st.elapsed_time(en) / steps
+        tot, n = ctypes.c_double(), ctypes.c_int64()
+        _lib.check(L.aok_plan_timing_read(c["plan"].h, ctypes.byref(tot), ctypes.byref(n)))
+        _lib.check(L.aok_plan_timing_enable(c["plan"].h, 0))
+        kms = tot.value / max(n.value, 1)
+        return allmax(ms), allmax(kms)
+
+    # ---- FP32C forward (headline) ----
+    c32 = setup(torch.float32)
+    sampler = ClockSampler(local)
+    ms32, kms32 = timed(c32, args.steps, args.warmup, sampler)
+    clocks = sampler.summary()
+    value = N * N * B * world / (ms32 * 1e-3)
+
+    # ---- FP64 forward ----
+    c64 = setup(torch.float64)
+    ms64, kms64 = timed(c64, max(3, args.steps // 2), args.warmup)
+    value64 = N * N * B * world / (ms64 * 1e-3)
+
+    # ---- error of FP32C and FP64 vs the FP64 oracle on a sample (inputs rounded as the GPU saw them) ----
+    nchk = 2048
+    S32 = c32["out"][:, :, :nchk].double().cpu().numpy()
+    S64 = c64["out"][:, :, :nchk].cpu().numpy()
+    z32 = basis.zeta.astype(np.float32).astype(np.float64)
+    coef32 = oracle.compile_coef(z32, basis.D.astype(np.float32).astype(np.float64), basis.ls)
+    coef32 = coef32.astype(np.float32).astype(np.float64)
+    ref32 = oracle.overlap2c_orb(basis.ls, coef32, z32, pairs.sidxA[:nchk], pairs.sidxB[:nchk],
+                                 pairs.posA[:, :nchk].astype(np.float32).astype(np.float64),
+                                 pairs.posB[:, :nchk].astype(np.float32).astype(np.float64), nthreads=os.cpu_count())
+    coef64 = oracle.compile_coef(basis.zeta, basis.D, basis.ls)
+    ref64 = oracle.overlap2c_orb(basis.ls, coef64, basis.zeta, pairs.sidxA[:nchk], pairs.sidxB[:nchk],
+                                 pairs.posA[:, :nchk], pairs.posB[:, :nchk], nthreads=os.cpu_count())
+    err32 = float(np.linalg.norm(S32 - ref32) / np.linalg.norm(ref32))
+    err64 = float(np.linalg.norm(S64 - ref64) / np.linalg.norm(ref64))
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        hA = torch.as_tensor(np.ascontiguousarray(pairs.posA.T.astype(np.float32))).pin_memory()
+        hB = torch.as_tensor(np.ascontiguousarray(pairs.posB.T.astype(np.float32))).pin_memory()
+        hsA = torch.as_tensor(pairs.sidxA).pin_memory()
+        hsB = torch.as_tensor(pairs.sidxB).pin_memory()
+        hout = torch.empty((B, N, N), dtype=torch.float32).pin_memory()
+        dA = torch.empty((B, 3), dtype=torch.float32, device="cuda")
+        dB = torch.empty((B, 3), dtype=torch.float32, device="cuda")
+        dsA = torch.empty(B, dtype=torch.int64, device="cuda")
+        dsB = torch.empty(B, dtype=torch.int64, device="cuda")
+        dout = torch.empty((B, N, N), dtype=torch.float32, device="cuda")
+
+        def e2e_step():
+            dA.copy_(hA, non_blocking=True)
+            dB.copy_(hB, non_blocking=True)
+            dsA.copy_(hsA, non_blocking=True)
+            dsB.copy_(hsB, non_blocking=True)
+            _lib.check(L.aok_overlap2c(c32["plan"].h, ctypes.c_void_p(dout.data_ptr()), _dev.ptr(c32["zeta"]),
+                                       _dev.ptr(c32["coef"]), ctypes.c_void_p(dA.data_ptr()),
+                                       ctypes.c_void_p(dB.data_ptr()), ctypes.c_void_p(dsA.data_ptr()),
+                                       ctypes.c_void_p(dsB.data_ptr()), B, 1.0, _dev.stream()))
+            hout.copy_(dout, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ke = max(3, args.steps // 4)
+        st.record()
+        for _ in range(ke):
+            e2e_step()
+        en.record()
+        torch.cuda.synchronize()
+        barrier()
+        ems = allmax(st.elapsed_time(en) / ke)
+        e2e = {"value": N * N * B * world / (ems * 1e-3), "unit": UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": int(hA.numel() * 4 + hB.numel() * 4 + hsA.numel() * 8 + hsB.numel() * 8),
+               "d2h_bytes_per_step": int(hout.numel() * 4)}
+
+    # ---- roofline of the dominant kernel (k_overlap2c, FP32C) ----
+    alg_bytes = B * (N * N * 4 + 2 * (3 * 4 + 8))
+    achieved = alg_bytes / (kms32 * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "k_overlap2c<float>",
+            "kernel_ms": kms32, "peak_kind": peak_kind,
+            "note": "algorithmic bytes = B*(N^2*4 written + 2*(12 B position + 8 B species index) read)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        rate, nth, bs, dt = cpu_oracle_rate(basis, pairs, coef64)
+        cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
+               "sample": f"first {bs} pairs of the batch, FP64 oracle with {nth} OpenMP threads ({dt:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": _baseline_metric(), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
+            "config": {"workload": "ragged 4-species l<=3 2C overlap (config 2), FP32-compensated forward",
+                       "batch_per_rank": B, "global_batch": B * world, "nbf": N, "nshells": ns, "K": K,
+                       "species": NZ, "l2": "output 321 MB per step > 126 MB L2 (no flush needed)"},
+            "fp64": {"value": value64, "ms_per_step": ms64, "kernel_ms": kms64},
+            "f32c_over_f64": value / value64,
+            "rel_err": {"f32c_vs_oracle": err32, "f64_vs_oracle": err64, "sample_pairs": nchk},
+            "roofline": roof, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+            "gpu_launches": 3 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,200 @@
+/*
+ * aok.h -- C ABI of libaok_b200.so, the sm_100a kernels behind the
+ * AtomicOrbitalKernels.jl hot path (v0.0.4 API).
+ *
+ * Every entry point takes plain device pointers and sizes, runs stream-ordered
+ * on the caller's cudaStream_t (passed as void*, NULL = legacy default
+ * stream), never synchronises the device, never aborts, throws or prints, and
+ * returns an int status (AOK_OK = 0).  On failure aok_last_error() returns a
+ * thread-local message.  The caller owns every array; a plan owns only its
+ * scratch tables (primitive-pair lists, the species-pair bins, the work-queue
+ * counter) and the device error word.
+ *
+ * Layouts are the reference's column-major (Julia) layouts:
+ *   positions (3,B)                  pos[c + 3*b]
+ *   2C output (N,N,B)                out[i + N*(j + N*b)]
+ *   3C output (N,N,N,B)              out[i + N*(j + N*(k + N*b))]
+ *   per-species tables (ns,K,NZ)     t[s + ns*(k + K*sigma)]
+ *   orbital values (nX,nOrb)         P[j + nX*i]
+ *   orbital gradients (3,nX,nOrb)    dP[c + 3*(j + nX*i)]   (SVector{3} per entry)
+ *   species indices                  int64, 1-based (as produced in Julia)
+ * The element type of every floating-point array is double for
+ * AOK_PREC_F64 and float for AOK_PREC_F32C.
+ */
+#ifndef AOK_H
+#define AOK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AOK_OK 0
+#define AOK_ERR_INVALID 1      /* null pointer, negative size, bad enum       */
+#define AOK_ERR_UNSUPPORTED 2  /* angular momentum / size beyond the kernels   */
+#define AOK_ERR_CUDA 3         /* CUDA runtime error (message has the detail)  */
+#define AOK_ERR_SPECIES 4      /* species index outside 1..NZ                  */
+#define AOK_ERR_LENGTH 5       /* inconsistent lengths                         */
+#define AOK_ERR_TIMEOUT 6      /* a bounded device-side wait gave up           */
+
+#define AOK_PREC_F64 0         /* all-FP64 kernels                             */
+#define AOK_PREC_F32C 1        /* FP32 arithmetic, compensated accumulation    */
+
+#define AOK_RADIAL_GAUSSIAN 0  /* R = sum D exp(-zeta r^2)                     */
+#define AOK_RADIAL_SLATER 1    /* R = r^poly sum D exp(-zeta r)                */
+
+#define AOK_MAX_L 3            /* highest shell angular momentum compiled      */
+
+typedef struct aok_plan aok_plan;        /* overlap plan (2C and 3C)          */
+typedef struct aok_orbitals aok_orbitals;/* orbital-evaluation plan           */
+
+/* Thread-local message for the last failing call on this thread. */
+const char* aok_last_error(void);
+/* Library version string. */
+const char* aok_version(void);
+
+/*
+ * Overlap plan for a shell structure shared by all species: ls[nshells]
+ * (host array) and K primitive slots per shell, NZ species.  Mirrors the
+ * param-free part of compile_basis, _compile_struct
+ * (src/integrals/orbital/cartesian_gto_basis.jl:88-104) and, with NZ = 1 and
+ * K = max nprim, CompiledBasis (src/integrals/compiled_basis.jl:36-99).
+ * max_batch bounds B for the 2C entry points (scratch is sized by it).
+ */
+int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t K,
+                    int64_t NZ, int precision, int64_t max_batch);
+int aok_plan_destroy(aok_plan* plan);
+/* nbf_total of the plan's shell structure (reference: basis.nbf_total). */
+int aok_plan_nbf(const aok_plan* plan, int64_t* nbf_total);
+/* Synchronises `stream`, then reports (and clears) the plan's device error
+ * word: AOK_ERR_SPECIES if a kernel met a species index outside 1..NZ. */
+int aok_plan_check(aok_plan* plan, void* stream);
+/* Measurement aid (no reference counterpart): when enabled, every call
+ * records a CUDA event pair around its dominant kernel (up to `capacity`
+ * pairs); aok_plan_timing_read synchronises those events and returns the
+ * summed kernel time and the number of timed launches, then resets. */
+int aok_plan_timing_enable(aok_plan* plan, int capacity);
+int aok_plan_timing_read(aok_plan* plan, double* total_ms, int64_t* launches);
+
+/*
+ * coef = D / sqrt(normsq) per shell and species on the device.
+ * Replaces _compile_coef / _cart_normsq
+ * (src/integrals/orbital/cartesian_gto_basis.jl:74-83, 110-120).
+ * zeta, D, coef: (ns,K,NZ).
+ */
+int aok_compile_coef(aok_plan* plan, void* coef, const void* zeta, const void* D, void* stream);
+
+/*
+ * Batched 2-center overlap, species-aware Cartesian basis.
+ * Replaces batch_S_orbital_kernel! + batch_overlap!(out, ::CartesianGTOBasis, XA, XB)
+ * (src/integrals/orbital/overlap_2c.jl:165-281, 321-347).
+ * out (N,N,B); zeta, coef (ns,K,NZ); posA, posB (3,B) in the basis's input
+ * unit (multiplied by lengthscale on the device, overlap_2c.jl:331-333);
+ * sidxA, sidxB (B) 1-based.  Zero-coefficient primitive pairs are skipped.
+ */
+int aok_overlap2c(aok_plan* plan, void* out, const void* zeta, const void* coef,
+                  const void* posA, const void* posB, const int64_t* sidxA,
+                  const int64_t* sidxB, int64_t B, double lengthscale, void* stream);
+
+/*
+ * Batched 2-center overlap, GaussianBasis path (NZ = 1 plan, K = max nprim).
+ * Replaces batch_S_kernel! + batch_overlap!(out, ::CompiledBasis, posA, posB)
+ * (src/integrals/kernels_2c.jl:110-262).  nprim (ns), prim_offset (ns+1):
+ * device int64; coef, alpha: flat per-primitive (prim_offset[ns]); posA,
+ * posB (3,B) already in Bohr (the reference's to_bohr runs on the host,
+ * src/integrals/units.jl:28-35).
+ */
+int aok_overlap2c_gb(aok_plan* plan, void* out, const int64_t* nprim,
+                     const int64_t* prim_offset, const void* coef, const void* alpha,
+                     const void* posA, const void* posB, int64_t B, void* stream);
+
+/*
+ * Batched 3-center overlap, GaussianBasis path (NZ = 1 plan).
+ * Replaces batch_V_kernel! + batch_overlap_3c! (src/integrals/kernels_3c.jl:12-200).
+ * out (N,N,N,B); posA, posB, posC (3,B) in Bohr.
+ */
+int aok_overlap3c_gb(aok_plan* plan, void* out, const int64_t* nprim,
+                     const int64_t* prim_offset, const void* coef, const void* alpha,
+                     const void* posA, const void* posB, const void* posC, int64_t B,
+                     void* stream);
+
+/*
+ * Kernel pullback of the species-aware 2C overlap: dcoef and dalpha
+ * (= d/dzeta through the kernel), both (ns,K,NZ), from the cotangent dS (N,N,B).
+ * Replaces batch_S_orbital_pb_kernel! + _overlap_pb_coef_alpha
+ * (src/integrals/orbital/overlap_2c_grad.jl:71-242).  Padded slots are not
+ * skipped (as in the reference).  Deterministic: per-block partials and a
+ * fixed-order second-stage reduction, no global atomics.
+ */
+int aok_overlap2c_pullback(aok_plan* plan, void* dcoef, void* dalpha, const void* dS,
+                           const void* zeta, const void* coef, const void* posA,
+                           const void* posB, const int64_t* sidxA, const int64_t* sidxB,
+                           int64_t B, double lengthscale, void* stream);
+
+/*
+ * Closed-form VJP of the normalisation: (dD, dzeta_norm) from dcoef.
+ * Replaces _compile_coef_pb (src/integrals/orbital/overlap_2c_grad.jl:251-286).
+ */
+int aok_compile_coef_pullback(aok_plan* plan, void* dD, void* dzeta, const void* dcoef,
+                              const void* zeta, const void* D, void* stream);
+
+/*
+ * Full parameter pullback of the differentiable overlap:
+ * dzeta = dalpha + dzeta_norm, dD, from dS.  Replaces pullback_ps(dS, orb, XA, XB, ps, st)
+ * (src/integrals/orbital/overlap_2c_grad.jl:296-304); zeta, D are ps.Rnl.
+ */
+int aok_overlap_pullback_ps(aok_plan* plan, void* dzeta, void* dD, const void* dS,
+                            const void* zeta, const void* D, const void* posA,
+                            const void* posB, const int64_t* sidxA, const int64_t* sidxB,
+                            int64_t B, double lengthscale, void* stream);
+
+/*
+ * Orbital-evaluation plan: radial spec (nRad radials, K slots, NZ species,
+ * poly[nRad] radial powers), orbital index maps iR, iY (nOrb, 1-based),
+ * harmonics up to L.  Mirrors AtomicOrbitals' state
+ * (src/orbitals/atomicorbitals.jl:31-75, 90-98) and GaussianTypeRadials /
+ * SlaterTypeRadials (src/orbitals/gtostoradials.jl:14-46).
+ */
+int aok_orbitals_create(aok_orbitals** orb, int64_t nRad, int64_t K, int64_t NZ,
+                        const int64_t* poly, int64_t nOrb, const int64_t* iR,
+                        const int64_t* iY, int64_t L, int radial_kind, int precision);
+int aok_orbitals_destroy(aok_orbitals* orb);
+
+/*
+ * P (nX,nOrb) = R_{iR} * Z_{iY} at positions X (3,nX) times lengthscale.
+ * Replaces evaluate(basis, Rs, sidx, ps, st) (src/orbitals/atomicorbitals.jl:148-162):
+ * _rnl_val_ka!, SpheriCart.compute and _aorb_val_ka! fused in one kernel.
+ */
+int aok_evaluate(aok_orbitals* orb, void* P, const void* X, const int64_t* sidx,
+                 const void* zeta, const void* D, int64_t nX, double lengthscale,
+                 void* stream);
+
+/*
+ * P and dP (3,nX,nOrb) (gradient w.r.t. the input coordinates, including the
+ * lengthscale factor).  Replaces evaluate_ed(basis, Rs, sidx, ps, st)
+ * (src/orbitals/atomicorbitals.jl:192-210): _rnl_ed_ka!,
+ * SpheriCart.compute_with_gradients, _aorb_ed_ka! and `dRnlm .*= s` fused.
+ */
+int aok_evaluate_ed(aok_orbitals* orb, void* P, void* dP, const void* X,
+                    const int64_t* sidx, const void* zeta, const void* D, int64_t nX,
+                    double lengthscale, void* stream);
+
+/*
+ * Pullback of evaluate: dX (3,nX) (may be NULL) and dzeta, dD (nRad,K,NZ)
+ * (may be NULL together) from dP (nX,nOrb).  Replaces the rrule pullback
+ * (src/orbitals/atomicorbitals.jl:249-316: _aorb_pbx_ka!, _aorb_pbrad_ka!,
+ * and the radial pullback_ps, src/orbitals/gtostoradials.jl:232-267),
+ * recomputing R, Z and their gradients instead of reading stored ones.
+ * Deterministic (per-block partials, fixed-order reduction).
+ */
+int aok_evaluate_pullback(aok_orbitals* orb, void* dX, void* dzeta, void* dD,
+                          const void* dP, const void* X, const int64_t* sidx,
+                          const void* zeta, const void* D, int64_t nX, double lengthscale,
+                          void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AOK_H */

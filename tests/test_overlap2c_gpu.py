@@ -1,0 +1,171 @@
+"""2-center overlap on the GPU vs the FP64 oracle (through the C ABI).
+
+Bars: FP64 kernel <= 1e-12 relative Frobenius error; FP32C <= 2e-6 relative
+Frobenius error, both against the oracle on identical inputs (FP32C inputs are
+the FP32-rounded positions/parameters, fed to the oracle in FP64).
+"""
+import numpy as np
+import pytest
+import torch
+
+import aok_b200 as aok
+import oracle
+from helpers import f32_round, max_abs, rel_fro
+
+W = aok.workloads
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 2e-6
+
+
+def _orb_case(basis, pairs, FT):
+    orb = aok.orbitals_from_species_basis(basis)
+    cob = aok.compile_basis(orb, dtype=FT)
+    XA = aok.PStates(pairs.posA, list(pairs.sidxA))
+    XB = aok.PStates(pairs.posB, list(pairs.sidxB))
+    S = aok.batch_overlap(cob, XA, XB, FT=FT)
+    if FT == torch.float32:
+        zeta = f32_round(basis.zeta)
+        D = f32_round(basis.D)
+        coef = oracle.compile_coef(zeta, D, basis.ls)
+        coef = f32_round(coef)
+        pA, pB = f32_round(pairs.posA), f32_round(pairs.posB)
+    else:
+        zeta, D = basis.zeta, basis.D
+        coef = oracle.compile_coef(zeta, D, basis.ls)
+        pA, pB = pairs.posA, pairs.posB
+    ref = oracle.overlap2c_orb(basis.ls, coef, zeta, pairs.sidxA, pairs.sidxB, pA, pB, nthreads=8)
+    return S, ref, cob, coef
+
+
+def test_compile_coef_matches_oracle():
+    b = W.config2_basis()
+    orb = aok.orbitals_from_species_basis(b)
+    cob = aok.compile_basis(orb, dtype=torch.float64)
+    ref = oracle.compile_coef(b.zeta, b.D, b.ls)
+    assert rel_fro(cob.coef.cpu().numpy(), ref) < 1e-14
+
+
+@pytest.mark.parametrize("B", [1, 31, 33, 1024])
+def test_config0_f64(B):
+    b = W.config0_basis()
+    pr = W.config0_pairs(B=B)
+    S, ref, _, _ = _orb_case(b, pr, torch.float64)
+    assert S.shape == (15, 15, B)
+    assert rel_fro(S, ref) < TOL64
+    assert max_abs(S, ref) < TOL64 * max(1.0, np.abs(ref).max())
+
+
+def test_config0_f32c():
+    b = W.config0_basis()
+    pr = W.config0_pairs(B=1024)
+    S, ref, _, _ = _orb_case(b, pr, torch.float32)
+    assert S.dtype == torch.float32
+    assert rel_fro(S, ref) < TOL32
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, TOL64), (torch.float32, TOL32)])
+def test_config2_ragged_species(FT, tol):
+    b = W.config2_basis()
+    pr = W.config2_pairs(B=3000)
+    S, ref, _, _ = _orb_case(b, pr, FT)
+    assert rel_fro(S, ref) < tol
+
+
+def test_self_overlap_diagonal_positive_s_shells():
+    b = W.config0_basis()
+    pr = W.config0_pairs(B=8)
+    pr.posB = pr.posA.copy()
+    S, ref, _, _ = _orb_case(b, pr, torch.float64)
+    assert rel_fro(S, ref) < TOL64
+    # normalised s shells have unit self-overlap (test_overlap_2c.jl:83-86 analogue)
+    s_idx = [0, 1, 2]
+    assert np.allclose(S.numpy()[s_idx, s_idx, :], 1.0, atol=1e-12)
+
+
+def test_absent_shells_give_zero_blocks():
+    b = W.config2_basis()
+    pr = W.config2_pairs(B=512)
+    S, ref, cob, coef = _orb_case(b, pr, torch.float64)
+    S = S.numpy()
+    boff = np.concatenate([[0], np.cumsum((b.ls + 1) * (b.ls + 2) // 2)])
+    for bi in range(64):
+        ga = pr.sidxA[bi] - 1
+        for s in range(len(b.ls)):
+            if b.nprim[s, ga] == 0:
+                assert np.all(S[boff[s]:boff[s + 1], :, bi] == 0.0)
+
+
+def test_gb_path_matches_oracle_and_orbital_path():
+    b = W.config0_basis()
+    ls, nprim, z, D = W.gb_tables(b)
+    coef_full = oracle.compile_coef(b.zeta, b.D, b.ls)
+    coef = np.concatenate([coef_full[s, :nprim[s], 0] for s in range(len(ls))])
+    shells = []
+    o = 0
+    for s in range(len(ls)):
+        shells.append(aok.CartesianShell(int(ls[s]), coef[o:o + nprim[s]], z[o:o + nprim[s]]))
+        o += nprim[s]
+    bc = aok.compile_basis(shells)
+    pr = W.config0_pairs(B=257)
+    # the GB path takes Length positions; feed Bohr values as angstrom/ang2bohr
+    pA = aok.Length(pr.posA / aok.ang2bohr, "angstrom")
+    pB = aok.Length(pr.posB / aok.ang2bohr, "angstrom")
+    S = aok.batch_overlap(bc, pA, pB)
+    ref = oracle.overlap2c_gb(ls, nprim, coef, z, aok.to_bohr(pA), aok.to_bohr(pB))
+    assert rel_fro(S, ref) < TOL64
+    S_orb, _, _, _ = _orb_case(b, pr, torch.float64)
+    assert max_abs(S, S_orb) < 1e-12
+
+
+def test_gb_path_rejects_plain_positions():
+    bc = aok.compile_basis([aok.CartesianShell(0, np.array([1.0]), np.array([1.0]))])
+    plain = np.zeros((3, 2))
+    with pytest.raises(aok.ArgumentError):
+        aok.batch_overlap(bc, plain, aok.Length(plain, "angstrom"))
+
+
+def test_unknown_species_and_length_mismatch_raise():
+    b = W.config0_basis()
+    cob = aok.compile_basis(aok.orbitals_from_species_basis(b))
+    X = aok.PStates(np.zeros((3, 2)), [1, 2])
+    with pytest.raises(aok.AOKError):
+        aok.batch_overlap(cob, X, X)
+    X1 = aok.PStates(np.zeros((3, 1)), [1])
+    X2 = aok.PStates(np.zeros((3, 2)), [1, 1])
+    with pytest.raises(RuntimeError):
+        aok.batch_overlap(cob, X1, X2)
+
+
+def test_empty_batch():
+    b = W.config0_basis()
+    cob = aok.compile_basis(aok.orbitals_from_species_basis(b))
+    X = aok.PStates(np.zeros((3, 0)), [])
+    S = aok.batch_overlap(cob, X, X)
+    assert S.shape == (15, 15, 0)
+
+
+def test_lengthscale_angstrom_equivalence():
+    b = W.config0_basis()
+    orbA = aok.orbitals_from_species_basis(b, length_unit="angstrom")
+    orbB = aok.orbitals_from_species_basis(b, length_unit="bohr")
+    pr = W.config0_pairs(B=64)
+    XA = aok.PStates(pr.posA / aok.ang2bohr, [1] * 64)
+    XB = aok.PStates(pr.posB / aok.ang2bohr, [1] * 64)
+    XAb = aok.PStates(pr.posA, [1] * 64)
+    XBb = aok.PStates(pr.posB, [1] * 64)
+    SA = aok.batch_overlap(aok.compile_basis(orbA), XA, XB)
+    SB = aok.batch_overlap(aok.compile_basis(orbB), XAb, XBb)
+    assert max_abs(SA, SB) < 1e-12
+
+
+def test_repeat_calls_deterministic():
+    b = W.config2_basis()
+    pr = W.config2_pairs(B=4096)
+    cob = aok.compile_basis(aok.orbitals_from_species_basis(b), dtype=torch.float32)
+    XA = aok.PStates(pr.posA, list(pr.sidxA))
+    XB = aok.PStates(pr.posB, list(pr.sidxB))
+    S1 = aok.batch_overlap(cob, XA, XB, FT=torch.float32)
+    S2 = aok.batch_overlap(cob, XA, XB, FT=torch.float32)
+    assert torch.equal(S1, S2)
