@@ -219,7 +219,9 @@ def compile_basis(obj, dtype=None, device="cuda"):
         if not obj.is_gaussian:
             raise RuntimeError("the overlap kernels integrate plain Gaussians; a Slater-type orbital basis "
                                "carries a nonzero radial power and is unsupported")
+        from . import _dev
         from .overlap import compile_coef
+        _dev.require_cuda()
         st = compile_struct(obj)
         tdt = dtype or (torch.float32 if obj.Rnl.zeta.dtype == np.float32 else torch.float64)
         zeta = torch.as_tensor(np.ascontiguousarray(np.asarray(obj.Rnl.zeta).transpose(2, 1, 0))).to(

@@ -51,8 +51,9 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 
 // Primitive-pair record of one (species pair, shell pair): everything that
 // does not depend on the geometry, computed once per call in FP64.
-//   w    = c_a c_b (pi/p)^{3/2}          mu = a b / p   (hi + lo for FP32)
-//   ra   = a/p,  rb = b/p,  oo2p = 1/(2p), flush = last pair of its ip row.
+//   w    = c_a c_b (pi/p)^{3/2}
+//   mu   = a b / p (FP64 record); mu log2(e) as hi + lo (FP32 record)
+//   ra   = a/p,  rb = b/p,  oo2p = 1/(2p), flush = ip (primitive row index).
 struct PPf {
     float w, mu_hi, mu_lo, ra, rb, oo2p, flush, pad;
 };

@@ -32,16 +32,24 @@ struct aok_plan {
     // device error word (AOK_ERR_* of the first fault a kernel met)
     int* d_err = nullptr;
     // 2C forward schedule
-    aok::Item* d_items = nullptr;
+    aok::Item* d_items = nullptr;    // static item list (nitems), panel-major
+    aok::Item* d_order = nullptr;    // per species pair execution order (NZ*NZ*nitems)
     int nitems = 0;
+    // multi-block binning scratch
+    int* d_blockhist = nullptr;      // nblk * NZ*NZ
+    int max_bin_blocks = 0;
     aok::Panels panels{};
     size_t slab_stride = 0;          // elements per batch slot in the panel buffer
     size_t smem_bytes = 0;
     // GaussianBasis-path padded tables (ns*K)
     void* d_gb_zeta = nullptr;
     void* d_gb_coef = nullptr;
-    // pullback: per-block partials and scratch coef
-    void* d_partials = nullptr;
+    // pullback: primitive-pair lists, per-warp FP64 partial rows, scratch coef
+    void* d_pb_full = nullptr;
+    void* d_pb_val = nullptr;
+    int2* d_pb_counts = nullptr;
+    void* d_partials = nullptr;      // per-CTA item sums
+    void* d_tilerows = nullptr;      // per-tile FP64 rows
     int max_blocks = 0;
     void* d_coef_scratch = nullptr;  // ns*K*NZ
     void* d_dcoef_scratch = nullptr; // ns*K*NZ
@@ -74,6 +82,12 @@ struct aok_orbitals {
 
 namespace aok {
 
+#define AOK_TRY_PB(x)                  \
+    do {                               \
+        int _st = (x);                 \
+        if (_st != AOK_OK) return _st; \
+    } while (0)
+
 // error helpers (api.cu)
 int set_error(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* what);
@@ -90,16 +104,22 @@ int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB,
 int launch_gb_pad(aok_plan* p, const int64_t* nprim, const int64_t* prim_offset, const void* coef,
                   const void* alpha, cudaStream_t s);
 int setup_overlap2c_schedule(aok_plan* p);
+int launch_ov2_f32(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
+int launch_ov2_f64(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
 
 // compile_coef.cu
 int launch_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D, cudaStream_t s);
 int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef, const void* zeta,
                            const void* D, const void* dalpha_add, cudaStream_t s);
 
-// overlap2c_bwd.cu
+// overlap2c_bwd*.cu
+int launch_pb_f32(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* posA, const void* posB,
+                  double lengthscale, cudaStream_t s);
+int launch_pb_f64(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* posA, const void* posB,
+                  double lengthscale, cudaStream_t s);
 int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
                         const void* coef, const void* posA, const void* posB, int64_t B,
-                        double lengthscale, cudaStream_t s);
+                        double lengthscale, int keep_absent, cudaStream_t s);
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);

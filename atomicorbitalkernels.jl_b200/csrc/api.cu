@@ -139,7 +139,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
     void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_counter,
-                    p->d_err, p->d_items, p->d_gb_zeta, p->d_gb_coef, p->d_partials, p->d_coef_scratch,
+                    p->d_err, p->d_items, p->d_order, p->d_blockhist, p->d_gb_zeta, p->d_gb_coef, p->d_pb_full, p->d_pb_val, p->d_pb_counts, p->d_partials, p->d_tilerows, p->d_coef_scratch,
                     p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3, p->d_npp3, p->d_items3};
     for (void* b : bufs) dfree(b);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
@@ -226,6 +226,44 @@ int aok_overlap2c_gb(aok_plan* p, void* out, const int64_t* nprim, const int64_t
     AOK_TRY(launch_prep2c(p, p->d_gb_zeta, p->d_gb_coef, s));
     AOK_TRY(launch_bin(p, nullptr, nullptr, B, s));
     return launch_overlap2c(p, out, posA, posB, B, 1.0, s);
+}
+
+static int overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
+                              const void* coef, const void* posA, const void* posB, const int64_t* sidxA,
+                              const int64_t* sidxB, int64_t B, double lengthscale, int keep_absent, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null plan");
+    AOK_TRY(check_batch(p, B, "aok_overlap2c_pullback"));
+    if (!dcoef || !dalpha || !zeta || !coef) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
+    if (B == 0) {
+        AOK_TRY(cuda_status(cudaMemsetAsync(dcoef, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync"));
+        return cuda_status(cudaMemsetAsync(dalpha, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync");
+    }
+    if (!dS || !posA || !posB || !sidxA || !sidxB)
+        return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
+    AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+    AOK_TRY(launch_prep2c(p, zeta, coef, s));
+    return launch_overlap2c_pb(p, dcoef, dalpha, dS, zeta, coef, posA, posB, B, lengthscale, keep_absent, s);
+}
+
+int aok_overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
+                           const void* coef, const void* posA, const void* posB, const int64_t* sidxA,
+                           const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
+    return overlap2c_pullback(p, dcoef, dalpha, dS, zeta, coef, posA, posB, sidxA, sidxB, B, lengthscale, 1,
+                              stream);
+}
+
+int aok_overlap_pullback_ps(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta, const void* D,
+                            const void* posA, const void* posB, const int64_t* sidxA, const int64_t* sidxB,
+                            int64_t B, double lengthscale, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap_pullback_ps: null plan");
+    if (!dzeta || !dD || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_overlap_pullback_ps: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    AOK_TRY(launch_compile_coef(p, p->d_coef_scratch, zeta, D, s));
+    AOK_TRY(overlap2c_pullback(p, p->d_dcoef_scratch, p->d_dalpha_scratch, dS, zeta, p->d_coef_scratch, posA, posB,
+                               sidxA, sidxB, B, lengthscale, 0, stream));
+    return launch_compile_coef_pb(p, dD, dzeta, p->d_dcoef_scratch, zeta, D, p->d_dalpha_scratch, s);
 }
 
 }  // extern "C"

@@ -7,9 +7,9 @@
 //   coef   = D / sqrt(normsq)            (zero when normsq <= 0: absent shell)
 //   dD_m   = dcoef_m / n - g_m dot / (2 n^3),  g_m = 2c sum_j D_j / (z_m+z_j)^e
 //   dz_m   = -h_m dot / (2 n^3),  h_m = -2c e D_m sum_j D_j / (z_m+z_j)^{e+1}
-// with dot = sum_i dcoef_i D_i and n = sqrt(normsq).  One thread per
-// (shell, species); K is small.  All arithmetic is FP64 (also for FP32 data:
-// these are the primitive normalisation constants).
+// with dot = sum_i dcoef_i D_i and n = sqrt(normsq).  One warp per
+// (shell, species).  All arithmetic is FP64 (also for FP32 data: these are
+// the primitive normalisation constants).
 #include "aok_internal.h"
 
 namespace aok {
@@ -25,77 +25,95 @@ __device__ __forceinline__ double norm_c(int l) {
     return (pi15 * (l == 0 ? 1.0 : cart_dfac(2 * l - 1))) / (double)(1 << l);
 }
 
+// x^(l + 3/2) = x^(l+1) * sqrt(x)
+__device__ __forceinline__ double pow_l32(double x, int l) {
+    double r = x;
+    for (int i = 0; i < l; ++i) r *= x;
+    return r * sqrt(x);
+}
+
+// sum_ij D_i D_j / (z_i + z_j)^(l+3/2) over one (shell, species): lanes split
+// the K x K terms, then a fixed-order butterfly reduction.
+template <typename FT>
+__device__ __forceinline__ double warp_normsum(const FT* __restrict__ zeta, const FT* __restrict__ D, size_t base,
+                                               int ns, int K, int l, int lane) {
+    double acc = 0.0;
+    for (int e = lane; e < K * K; e += 32) {
+        const int i = e / K, j = e % K;
+        const double Di = (double)D[base + (size_t)ns * i], Dj = (double)D[base + (size_t)ns * j];
+        const double zz = (double)zeta[base + (size_t)ns * i] + (double)zeta[base + (size_t)ns * j];
+        acc += (Di * Dj) / pow_l32(zz, l);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+// one warp per (shell, species)
 template <typename FT>
 __global__ void k_compile_coef(FT* __restrict__ coef, const FT* __restrict__ zeta, const FT* __restrict__ D,
                                const int* __restrict__ ls, int ns, int K, int NZ) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= ns * NZ) return;
-    int s = q % ns, g = q / ns;
-    int l = ls[s];
-    const double e = (double)l + 1.5;
+    const int s = q % ns, g = q / ns;
+    const int l = ls[s];
     const size_t base = (size_t)s + (size_t)ns * K * g;
-    double acc = 0.0;
-    for (int i = 0; i < K; ++i)
-        for (int j = 0; j < K; ++j) {
-            double Di = (double)D[base + (size_t)ns * i], Dj = (double)D[base + (size_t)ns * j];
-            double zz = (double)zeta[base + (size_t)ns * i] + (double)zeta[base + (size_t)ns * j];
-            acc += (Di * Dj) / pow(zz, e);
-        }
-    double nsq = norm_c(l) * acc;
-    double n = nsq > 0.0 ? sqrt(nsq) : 0.0;
-    for (int m = 0; m < K; ++m)
+    const double nsq = norm_c(l) * warp_normsum(zeta, D, base, ns, K, l, lane);
+    const double n = nsq > 0.0 ? sqrt(nsq) : 0.0;
+    for (int m = lane; m < K; m += 32)
         coef[base + (size_t)ns * m] = nsq > 0.0 ? (FT)((double)D[base + (size_t)ns * m] / n) : FT(0);
 }
 
+// one warp per (shell, species); lane m handles primitive slot m (K <= 32
+// per pass)
 template <typename FT>
 __global__ void k_compile_coef_pb(FT* __restrict__ dD, FT* __restrict__ dz, const FT* __restrict__ dcoef,
                                   const FT* __restrict__ zeta, const FT* __restrict__ D,
                                   const FT* __restrict__ dalpha_add, const int* __restrict__ ls, int ns, int K,
                                   int NZ) {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= ns * NZ) return;
-    int s = q % ns, g = q / ns;
-    int l = ls[s];
+    const int s = q % ns, g = q / ns;
+    const int l = ls[s];
     const double e = (double)l + 1.5;
     const double c = norm_c(l);
     const size_t base = (size_t)s + (size_t)ns * K * g;
     auto Dv = [&](int i) { return (double)D[base + (size_t)ns * i]; };
     auto zv = [&](int i) { return (double)zeta[base + (size_t)ns * i]; };
-    double acc = 0.0;
-    for (int i = 0; i < K; ++i)
-        for (int j = 0; j < K; ++j) acc += (Dv(i) * Dv(j)) / pow(zv(i) + zv(j), e);
-    double nsq = c * acc;
+    const double nsq = c * warp_normsum(zeta, D, base, ns, K, l, lane);
+    double dot = 0.0;
+    for (int i = lane; i < K; i += 32) dot += (double)dcoef[base + (size_t)ns * i] * Dv(i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
     if (!(nsq > 0.0)) {
-        for (int m = 0; m < K; ++m) {
+        for (int m = lane; m < K; m += 32) {
             size_t o = base + (size_t)ns * m;
             dD[o] = FT(0);
             dz[o] = dalpha_add ? dalpha_add[o] : FT(0);
         }
         return;
     }
-    double n = sqrt(nsq);
-    double dot = 0.0;
-    for (int i = 0; i < K; ++i) dot += (double)dcoef[base + (size_t)ns * i] * Dv(i);
-    double s2n3 = dot / (2.0 * ((n * n) * n));
-    for (int m = 0; m < K; ++m) {
+    const double n = sqrt(nsq);
+    const double s2n3 = dot / (2.0 * ((n * n) * n));
+    for (int m = lane; m < K; m += 32) {
         double gm = 0.0, hm = 0.0;
         for (int j = 0; j < K; ++j) {
-            double den = zv(m) + zv(j);
-            double p = pow(den, e);
+            const double den = zv(m) + zv(j);
+            const double p = pow_l32(den, l);
             gm += Dv(j) / p;
             hm += Dv(j) / (p * den);
         }
         gm *= 2.0 * c;
         hm *= ((-2.0 * c) * e) * Dv(m);
-        size_t o = base + (size_t)ns * m;
+        const size_t o = base + (size_t)ns * m;
         dD[o] = (FT)((double)dcoef[o] / n - gm * s2n3);
-        double dzn = -hm * s2n3;
+        const double dzn = -hm * s2n3;
         dz[o] = dalpha_add ? (FT)((double)dalpha_add[o] + dzn) : (FT)dzn;
     }
 }
 
 int launch_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D, cudaStream_t s) {
-    int n = (int)(p->ns * p->NZ), th = 64, bl = (n + th - 1) / th;
+    int n = (int)(p->ns * p->NZ), th = 128, bl = (n * 32 + th - 1) / th;
     if (p->prec == AOK_PREC_F64)
         k_compile_coef<double><<<bl, th, 0, s>>>((double*)coef, (const double*)zeta, (const double*)D, p->d_ls,
                                                  (int)p->ns, (int)p->K, (int)p->NZ);
@@ -107,7 +125,7 @@ int launch_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D
 
 int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef, const void* zeta, const void* D,
                            const void* dalpha_add, cudaStream_t s) {
-    int n = (int)(p->ns * p->NZ), th = 64, bl = (n + th - 1) / th;
+    int n = (int)(p->ns * p->NZ), th = 128, bl = (n * 32 + th - 1) / th;
     if (p->prec == AOK_PREC_F64)
         k_compile_coef_pb<double><<<bl, th, 0, s>>>((double*)dD, (double*)dzeta, (const double*)dcoef,
                                                     (const double*)zeta, (const double*)D,

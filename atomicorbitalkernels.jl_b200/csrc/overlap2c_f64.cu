@@ -1,0 +1,11 @@
+// overlap2c_f64.cu -- double instantiation of the 2-center overlap kernel.
+#include "overlap2c_kernel.cuh"
+
+namespace aok {
+
+int launch_ov2_f64(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale,
+                   cudaStream_t s) {
+    return launch_ov2<double, kThreadsF64>(p, out, posA, posB, lengthscale, s);
+}
+
+}  // namespace aok

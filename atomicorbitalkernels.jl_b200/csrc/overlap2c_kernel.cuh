@@ -1,0 +1,363 @@
+// overlap2c_kernel.cuh -- the persistent 2-center overlap kernel, templated
+// on the element type; instantiated once per precision (overlap2c_f32.cu,
+// overlap2c_f64.cu) so the two builds compile in parallel.  See overlap2c.cu
+// for the design notes.
+#pragma once
+
+#include <cstring>
+
+#include "aok_internal.h"
+
+namespace aok {
+
+constexpr int kThreadsF32 = 256;   // 2 CTAs per SM (registers <= 128)
+constexpr int kThreadsF64 = 256;   // 1 CTA per SM
+template <typename FT> constexpr int min_blocks();
+template <> constexpr int min_blocks<float>() { return 2; }
+template <> constexpr int min_blocks<double>() { return 1; }
+
+// --------------------------------------------------------------------------
+// Geometry per lane.
+// --------------------------------------------------------------------------
+template <typename FT> struct Geo;
+template <> struct Geo<float> {
+    float AB[3];
+    float R2, R2lo;
+};
+template <> struct Geo<double> {
+    double AB[3];
+    double R2;
+};
+
+__device__ __forceinline__ void load_geo(Geo<float>& g, const float* A, const float* B, float s, bool use_s) {
+    double R2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float a = A[c], b = B[c];
+        if (use_s) {
+            a = a * s;
+            b = b * s;
+        }
+        double d = (double)a - (double)b;  // exact
+        g.AB[c] = (float)d;
+        R2 += d * d;
+    }
+    g.R2 = (float)R2;
+    g.R2lo = (float)(R2 - (double)g.R2);
+}
+__device__ __forceinline__ void load_geo(Geo<double>& g, const double* A, const double* B, double s, bool use_s) {
+    double R2 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double a = A[c], b = B[c];
+        if (use_s) {
+            a = a * s;
+            b = b * s;
+        }
+        double d = a - b;
+        g.AB[c] = d;
+        R2 += d * d;
+    }
+    g.R2 = R2;
+}
+
+// --------------------------------------------------------------------------
+// 1-D overlap table E[i][j] = E_0^{ij} (McMurchie-Davidson t = 0 coefficient,
+// built with the Obara-Saika form of the recursion, HJO eq. 9.5.6-9.5.7 with
+// E_1^{ij} = (i E_0^{i-1,j} + j E_0^{i,j-1}) / 2p), seeded with E[0][0] = e00:
+//   E[i+1][j] = PA E[i][j] + (i E[i-1][j] + j E[i][j-1]) / 2p
+//   E[i][j+1] = PB E[i][j] + (i E[i-1][j] + j E[i][j-1]) / 2p
+// PA = -(b/p) AB and PB = (a/p) AB are formed directly (no P - A cancellation).
+// --------------------------------------------------------------------------
+template <int LA, int LB, typename FT>
+__device__ __forceinline__ void build_E(FT (&E)[LA + 1][LB + 1], FT PA, FT PB, const FT (&O)[4], FT e00) {
+    // O[k] = k / 2p (shared by the three axes)
+    E[0][0] = e00;
+#pragma unroll
+    for (int i = 1; i <= LA; ++i) {
+        if (i >= 2)
+            E[i][0] = PA * E[i - 1][0] + O[i - 1] * E[i - 2][0];
+        else
+            E[i][0] = PA * E[i - 1][0];
+    }
+#pragma unroll
+    for (int j = 1; j <= LB; ++j) {
+        if (j >= 2)
+            E[0][j] = PB * E[0][j - 1] + O[j - 1] * E[0][j - 2];
+        else
+            E[0][j] = PB * E[0][j - 1];
+#pragma unroll
+        for (int i = 1; i <= LA; ++i) {
+            FT c = O[j] * E[i - 1][j - 1];
+            if (i >= 2) c = c + O[i - 1] * E[i - 2][j];
+            E[i][j] = PA * E[i - 1][j] + c;
+        }
+    }
+}
+
+template <int LA, int LB>
+struct ClassInfo {
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NE = NA * NB, N1 = 2 * LA + 1;
+    static constexpr int NCH = nchunks(NE);
+};
+
+// --------------------------------------------------------------------------
+// One work item for one lane (batch element): FP32C.
+// dst points at the block's (0,0) element inside this lane's slab; element
+// (i, j) of the block lives at dst[j*N + i].
+// --------------------------------------------------------------------------
+template <int LA, int LB, int C>
+__device__ __noinline__ void run_item(const PPf* __restrict__ pp, int n, const Geo<float> g, float* dst, int N) {
+    using CI = ClassInfo<LA, LB>;
+    constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
+    // hi/part in registers; the TwoSum rounding errors (lo) accumulate in this
+    // lane's slab slots, which the item owns until it writes its result.
+    float hi[M], part[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        hi[m] = 0.f;
+        part[m] = 0.f;
+        dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] = 0.f;
+    }
+    float prev_ip = 0.f;
+    // software pipeline: the next record is in flight while this one computes
+    float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
+    if (n > 0) {
+        n0 = __ldg(reinterpret_cast<const float4*>(pp));
+        n1 = __ldg(reinterpret_cast<const float4*>(pp) + 1);
+    }
+    for (int q = 0; q < n; ++q) {
+        const float4 r0 = n0, r1 = n1;
+        if (q + 1 < n) {
+            n0 = __ldg(reinterpret_cast<const float4*>(pp + q + 1));
+            n1 = __ldg(reinterpret_cast<const float4*>(pp + q + 1) + 1);
+        }
+        // mu2 = mu * log2(e) as hi + lo (FP64 on the host of the record)
+        const float w = r0.x, mu_hi = r0.y, mu_lo = r0.z, ra = r0.w, rb = r1.x, oo2p = r1.y, ip = r1.z;
+        if (ip != prev_ip) {
+            // fold the previous ip row's partial sums into (hi, lo)
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                float s, e;
+                two_sum(hi[m], part[m], s, e);
+                hi[m] = s;
+                part[m] = 0.f;
+                dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] += e;
+            }
+            prev_ip = ip;
+        }
+        // exp(-mu R^2) = 2^-(mu2 R^2) with the argument in double-float:
+        // 2^-(xh + xl) = 2^-xh (1 - ln2 xl) to first order in |xl| < 2^-20 xh
+        const float xh = mu_hi * g.R2;
+        const float xl = fmaf(mu_hi, g.R2, -xh) + fmaf(mu_lo, g.R2, mu_hi * g.R2lo);
+        const float e00 = (exp2f(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
+        const float O[4] = {0.f, oo2p, 2.f * oo2p, 3.f * oo2p};
+        float Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
+        build_E<LA, LB, float>(Ex, -rb * g.AB[0], ra * g.AB[0], O, e00);
+        build_E<LA, LB, float>(Ey, -rb * g.AB[1], ra * g.AB[1], O, 1.f);
+        build_E<LA, LB, float>(Ez, -rb * g.AB[2], ra * g.AB[2], O, 1.f);
+#pragma unroll
+        for (int c2 = 0; c2 < CI::NB; ++c2)
+#pragma unroll
+            for (int c1 = 0; c1 < CI::NA; ++c1) {
+                const int lin = c1 + CI::N1 * c2;
+                if (lin >= L0 && lin < L1) {
+                    const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)] * Ez[cart_z(LA, c1)][cart_z(LB, c2)];
+                    part[lin - L0] = fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)], yz, part[lin - L0]);
+                }
+            }
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float s, e;
+        two_sum(hi[m], part[m], s, e);
+        float* d = dst + ((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA;
+        *d = s + (*d + e);
+    }
+}
+
+// FP64 variant: plain double accumulation.
+template <int LA, int LB, int C>
+__device__ __noinline__ void run_item(const PPd* __restrict__ pp, int n, const Geo<double> g, double* dst, int N) {
+    using CI = ClassInfo<LA, LB>;
+    constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
+    double acc[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    double2 n0 = make_double2(0.0, 0.0), n1 = n0;
+    double n2 = 0.0;
+    if (n > 0) {
+        n0 = __ldg(reinterpret_cast<const double2*>(pp));
+        n1 = __ldg(reinterpret_cast<const double2*>(pp) + 1);
+        n2 = __ldg(reinterpret_cast<const double*>(pp) + 4);
+    }
+    for (int q = 0; q < n; ++q) {
+        const double2 r0 = n0, r1 = n1;
+        const double r2w = n2;
+        if (q + 1 < n) {
+            n0 = __ldg(reinterpret_cast<const double2*>(pp + q + 1));
+            n1 = __ldg(reinterpret_cast<const double2*>(pp + q + 1) + 1);
+            n2 = __ldg(reinterpret_cast<const double*>(pp + q + 1) + 4);
+        }
+        const double w = r0.x, mu = r0.y, ra = r1.x, rb = r1.y, oo2p = r2w;
+        const double e00 = exp(-mu * g.R2) * w;
+        const double O[4] = {0.0, oo2p, 2.0 * oo2p, 3.0 * oo2p};
+        double Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
+        build_E<LA, LB, double>(Ex, -rb * g.AB[0], ra * g.AB[0], O, e00);
+        build_E<LA, LB, double>(Ey, -rb * g.AB[1], ra * g.AB[1], O, 1.0);
+        build_E<LA, LB, double>(Ez, -rb * g.AB[2], ra * g.AB[2], O, 1.0);
+#pragma unroll
+        for (int c2 = 0; c2 < CI::NB; ++c2)
+#pragma unroll
+            for (int c1 = 0; c1 < CI::NA; ++c1) {
+                const int lin = c1 + CI::N1 * c2;
+                if (lin >= L0 && lin < L1) {
+                    const double yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)] * Ez[cart_z(LA, c1)][cart_z(LB, c2)];
+                    acc[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)], yz, acc[lin - L0]);
+                }
+            }
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] = acc[m];
+}
+
+template <typename PP, typename FT, int LA, int LB>
+__device__ __forceinline__ void run_chunks(int chunk, const PP* pp, int n, const Geo<FT>& g, FT* dst, int N) {
+    constexpr int NCH = ClassInfo<LA, LB>::NCH;
+    if constexpr (NCH == 1) {
+        run_item<LA, LB, 0>(pp, n, g, dst, N);
+    } else if constexpr (NCH == 2) {
+        if (chunk == 0) run_item<LA, LB, 0>(pp, n, g, dst, N);
+        else run_item<LA, LB, 1>(pp, n, g, dst, N);
+    } else {
+        static_assert(NCH == 3, "chunk count");
+        if (chunk == 0) run_item<LA, LB, 0>(pp, n, g, dst, N);
+        else if (chunk == 1) run_item<LA, LB, 1>(pp, n, g, dst, N);
+        else run_item<LA, LB, 2>(pp, n, g, dst, N);
+    }
+}
+
+template <typename PP, typename FT>
+__device__ __forceinline__ void dispatch(int cls, int chunk, const PP* pp, int n, const Geo<FT>& g, FT* dst, int N) {
+    switch (cls) {
+#define AOK_CASE(LA, LB) \
+    case (LA) * 4 + (LB): run_chunks<PP, FT, LA, LB>(chunk, pp, n, g, dst, N); break;
+        AOK_CASE(0, 0) AOK_CASE(0, 1) AOK_CASE(0, 2) AOK_CASE(0, 3)
+        AOK_CASE(1, 0) AOK_CASE(1, 1) AOK_CASE(1, 2) AOK_CASE(1, 3)
+        AOK_CASE(2, 0) AOK_CASE(2, 1) AOK_CASE(2, 2) AOK_CASE(2, 3)
+        AOK_CASE(3, 0) AOK_CASE(3, 1) AOK_CASE(3, 2) AOK_CASE(3, 3)
+#undef AOK_CASE
+        default: break;
+    }
+}
+
+template <typename FT>
+struct Ov2Params {
+    FT* out;
+    const FT* posA;
+    const FT* posB;
+    FT scale;
+    int use_scale;
+    const typename PPT<FT>::type* pp;
+    const int* npp;
+    const int* perm;
+    const int4* tiles;
+    const int* ntiles;
+    unsigned* counter;
+    const Item* items;   // per species pair: items in execution order (nitems each)
+    int nitems;
+    Panels panels;
+    int ns, K, N, slab_stride;
+    int boff[kMaxShells + 1];
+};
+
+template <typename FT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_constant__ Ov2Params<FT> P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FT* slab = reinterpret_cast<FT*>(smem_raw);
+    __shared__ int s_tile;
+    __shared__ int s_next[kMaxPanels];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = THREADS / 32;
+    const int ntiles = *P.ntiles;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_tile = (int)atomicAdd(P.counter, 1u);
+            for (int i = 0; i < P.panels.n; ++i) s_next[i] = 0;
+        }
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= ntiles) break;
+        const int4 td = P.tiles[tile];
+        const int pair = td.x, start = td.y, cnt = td.z;
+        Geo<FT> g;
+        if (lane < cnt) {
+            const int b = P.perm[start + lane];
+            load_geo(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
+        } else {
+            const FT z[3] = {FT(0), FT(0), FT(0)};
+            load_geo(g, z, z, P.scale, false);
+        }
+        FT* sl = slab + (size_t)lane * P.slab_stride;
+        for (int pn = 0; pn < P.panels.n; ++pn) {
+            const int col0 = P.panels.col0[pn];
+            const int i0 = P.panels.item0[pn], i1 = P.panels.item0[pn + 1];
+            for (;;) {
+                int it = 0;
+                if (lane == 0) it = atomicAdd(&s_next[pn], 1);
+                it = __shfl_sync(0xffffffffu, it, 0) + i0;
+                if (it >= i1) break;
+                const Item wi = P.items[(size_t)pair * P.nitems + it];
+                const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
+                const int n = __ldg(P.npp + q);
+                FT* dst = sl + (size_t)(P.boff[wi.sb] - col0) * P.N + P.boff[wi.sa];
+                dispatch(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K, n, g, dst, P.N);
+            }
+            __syncthreads();
+            const int len = (P.panels.col0[pn + 1] - col0) * P.N;
+            for (int bl = warp; bl < cnt; bl += NW) {
+                const int bg = P.perm[start + bl];
+                FT* o = P.out + (size_t)bg * P.N * P.N + (size_t)col0 * P.N;
+                const FT* s = slab + (size_t)bl * P.slab_stride;
+                for (int e = lane; e < len; e += 32) o[e] = s[e];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <typename FT, int THREADS>
+inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale,
+                      cudaStream_t s) {
+    Ov2Params<FT> P;
+    memset(&P, 0, sizeof(P));
+    P.out = (FT*)out;
+    P.posA = (const FT*)posA;
+    P.posB = (const FT*)posB;
+    P.scale = (FT)lengthscale;
+    P.use_scale = (FT)lengthscale != FT(1);
+    P.pp = (const typename PPT<FT>::type*)p->d_pp;
+    P.npp = p->d_npp;
+    P.perm = p->d_perm;
+    P.tiles = p->d_tiles;
+    P.ntiles = p->d_ntiles;
+    P.counter = p->d_counter;
+    P.items = p->d_order;
+    P.nitems = p->nitems;
+    P.panels = p->panels;
+    P.ns = (int)p->ns;
+    P.K = (int)p->K;
+    P.N = (int)p->N;
+    P.slab_stride = (int)p->slab_stride;
+    for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
+    auto kern = k_overlap2c<FT, THREADS, min_blocks<FT>()>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_bytes);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap2c)");
+    timing_begin(p, s);
+    kern<<<p->num_sms * min_blocks<FT>(), THREADS, p->smem_bytes, s>>>(P);
+    timing_end(p, s);
+    return cuda_status(cudaGetLastError(), "k_overlap2c");
+}
+
+
+}  // namespace aok

@@ -7,14 +7,6 @@ int aok_overlap3c_gb(aok_plan*, void*, const int64_t*, const int64_t*, const voi
                      const void*, const void*, int64_t, void*) {
     return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: not implemented yet");
 }
-int aok_overlap2c_pullback(aok_plan*, void*, void*, const void*, const void*, const void*, const void*, const void*,
-                           const int64_t*, const int64_t*, int64_t, double, void*) {
-    return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap2c_pullback: not implemented yet");
-}
-int aok_overlap_pullback_ps(aok_plan*, void*, void*, const void*, const void*, const void*, const void*,
-                            const void*, const int64_t*, const int64_t*, int64_t, double, void*) {
-    return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap_pullback_ps: not implemented yet");
-}
 int aok_orbitals_create(aok_orbitals**, int64_t, int64_t, int64_t, const int64_t*, int64_t, const int64_t*,
                         const int64_t*, int64_t, int, int) {
     return set_error(AOK_ERR_UNSUPPORTED, "aok_orbitals_create: not implemented yet");

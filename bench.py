@@ -79,6 +79,10 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.05)
+            self.rows.clear()
         except Exception:
             self.proc = None
         return self
@@ -114,21 +118,22 @@ class ClockSampler:
 
 
 def cpu_oracle_rate(basis, pairs, coef, target_s=12.0, nthreads=None):
-    """Integrals/s of the oracle (C, OpenMP) on a bounded sample of the workload."""
+    """Integrals/s of the oracle (C, OpenMP) on a bounded sample of the workload:
+    whole passes over the batch until about `target_s` seconds of CPU work."""
     import oracle
     nthreads = nthreads or os.cpu_count()
     N = basis.nbf_total
-    b0 = 256
     t0 = time.perf_counter()
-    oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[:b0], pairs.sidxB[:b0], pairs.posA[:, :b0],
-                         pairs.posB[:, :b0], nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    bs = int(min(pairs.B, max(b0, b0 * target_s / max(dt, 1e-6))))
-    t0 = time.perf_counter()
-    oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA[:bs], pairs.sidxB[:bs], pairs.posA[:, :bs],
-                         pairs.posB[:, :bs], nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    return N * N * bs / dt, nthreads, bs, dt
+    passes, done = 0, 0
+    while True:
+        oracle.overlap2c_orb(basis.ls, coef, basis.zeta, pairs.sidxA, pairs.sidxB, pairs.posA, pairs.posB,
+                             nthreads=nthreads)
+        passes += 1
+        done += pairs.B
+        dt = time.perf_counter() - t0
+        if dt >= target_s or passes >= 200:
+            break
+    return N * N * done / dt, nthreads, done, dt
 
 
 def run_reference(args):
@@ -175,11 +180,15 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="aok", choices=["aok", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient step")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the FP32C forward steps (for ncu launch lists / captures); prints no JSON")
+    ap.add_argument("--batch", type=int, default=B_PER_RANK, help="pairs per rank")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -212,7 +221,7 @@ def main():
         return float(t.item())
 
     L = _lib.load()
-    basis, pairs = workload(rank)
+    basis, pairs = workload(rank, args.batch)
     N, B, ns, K, NZ = basis.nbf_total, pairs.B, basis.nshells, basis.K, basis.NZ
     peaks, peak_kind = _peaks()
 
@@ -258,6 +267,11 @@ def main():
 
     # ---- FP32C forward (headline) ----
     c32 = setup(torch.float32)
+    if args.profile:
+        for _ in range(args.warmup + args.steps):
+            step(c32)
+        torch.cuda.synchronize()
+        return 0
     sampler = ClockSampler(local)
     ms32, kms32 = timed(c32, args.steps, args.warmup, sampler)
     clocks = sampler.summary()
@@ -266,7 +280,66 @@ def main():
     # ---- FP64 forward ----
     c64 = setup(torch.float64)
     ms64, kms64 = timed(c64, max(3, args.steps // 2), args.warmup)
+    del c64["plan"]
     value64 = N * N * B * world / (ms64 * 1e-3)
+
+    # ---- (zeta, D) gradient step (config 3): L = sum (S - S_tgt)^2, B = 16384 pairs ----
+    grad = None
+    if not args.no_grad:
+        Bg = min(16384, B)
+        zt, Dt = aok.workloads.config3_target(basis)
+        cg = {k: v for k, v in c32.items()}
+        gpl = _dev.Plan(basis.ls, K, NZ, _dev.prec_of(torch.float32), Bg)
+        zt_d = _dev.to_colmajor(zt, torch.float32)
+        Dt_d = _dev.to_colmajor(Dt, torch.float32)
+        ct_d = _dev.colmajor_empty((ns, K, NZ), torch.float32)
+        _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(ct_d), _dev.ptr(zt_d), _dev.ptr(Dt_d), _dev.stream()))
+        Sg = _dev.colmajor_empty((N, N, Bg), torch.float32)
+        Tg = _dev.colmajor_empty((N, N, Bg), torch.float32)
+        dz = _dev.colmajor_empty((ns, K, NZ), torch.float32)
+        dD = _dev.colmajor_empty((ns, K, NZ), torch.float32)
+        pA, pB = c32["pA"][:, :Bg], c32["pB"][:, :Bg]
+        sA = ctypes.c_void_p(c32["sA"].data_ptr())
+        sB = ctypes.c_void_p(c32["sB"].data_ptr())
+
+        def fwd(out, coef):
+            _lib.check(L.aok_overlap2c(gpl.h, _dev.ptr(out), _dev.ptr(c32["zeta"]), _dev.ptr(coef), _dev.ptr(pA),
+                                       _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
+
+        _lib.check(L.aok_overlap2c(gpl.h, _dev.ptr(Tg), _dev.ptr(zt_d), _dev.ptr(ct_d), _dev.ptr(pA), _dev.ptr(pB),
+                                   sA, sB, Bg, 1.0, _dev.stream()))
+
+        def gstep():
+            _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(c32["coef"]), _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]),
+                                          _dev.stream()))
+            fwd(Sg, c32["coef"])
+            dS = (Sg - Tg).mul_(2.0)
+            _lib.check(L.aok_overlap_pullback_ps(gpl.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS),
+                                                 _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
+                                                 _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
+
+        def fstep():
+            fwd(Sg, c32["coef"])
+
+        def tloop(fn, n):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st.record()
+            for _ in range(n):
+                fn()
+            en.record()
+            torch.cuda.synchronize()
+            return allmax(st.elapsed_time(en) / n)
+
+        ng = max(3, args.steps // 10)
+        f_ms = tloop(fstep, ng)
+        g_ms = tloop(gstep, ng)
+        del gpl
+        grad = {"workload": "config 3: L = sum (S - S_tgt)^2 over B=16384 pairs, FP32C forward + pullback_ps",
+                "batch": Bg, "forward_ms": f_ms, "step_ms": g_ms, "step_over_forward": g_ms / f_ms,
+                "launches_per_step": 3 + 5 + 7}
 
     # ---- error of FP32C and FP64 vs the FP64 oracle on a sample (inputs rounded as the GPU saw them) ----
     nchk = 2048
@@ -314,7 +387,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ke = max(3, args.steps // 4)
+        ke = max(3, min(200, args.steps // 10))
         st.record()
         for _ in range(ke):
             e2e_step()
@@ -338,7 +411,8 @@ def main():
     if rank == 0 and not args.no_cpu:
         rate, nth, bs, dt = cpu_oracle_rate(basis, pairs, coef64)
         cpu = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
-               "sample": f"first {bs} pairs of the batch, FP64 oracle with {nth} OpenMP threads ({dt:.1f} s)"}
+               "sample": f"{bs} pairs (whole passes over the batch), FP64 oracle, {nth} OpenMP threads, "
+                         f"{dt:.1f} s"}
 
     if rank == 0:
         line = {
@@ -351,6 +425,7 @@ def main():
             "fp64": {"value": value64, "ms_per_step": ms64, "kernel_ms": kms64},
             "f32c_over_f64": value / value64,
             "rel_err": {"f32c_vs_oracle": err32, "f64_vs_oracle": err64, "sample_pairs": nchk},
+            "grad_step": grad,
             "roofline": roof, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
             "gpu_launches": 3 * args.steps,
         }

@@ -1,0 +1,114 @@
+"""CPU tests of the boundary and host logic: the C-ABI library loads and
+exports every symbol include/aok.h declares (no compute calls), and the
+host-side mirror of the reference API behaves like the reference (units,
+species lookup, errors, index maps, workloads)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+import aok_b200 as aok
+from aok_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "aok.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(aok_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_header_symbol():
+    if not os.path.exists(_lib.SO_PATH):
+        _lib.build()
+    L = ctypes.CDLL(_lib.SO_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 18
+    for s in syms:
+        assert hasattr(L, s), f"libaok_b200.so does not export {s}"
+    assert sorted(_lib.EXPORTS) == syms
+    v = ctypes.CDLL(_lib.SO_PATH)
+    v.aok_version.restype = ctypes.c_char_p
+    assert b"sm_100a" in v.aok_version()
+
+
+def test_plan_create_rejects_bad_arguments_without_gpu():
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    ls = _lib.int64_array([0, 1, 4])
+    assert L.aok_plan_create(ctypes.byref(h), 3, ls, 2, 1, 0, 16) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"angular momentum" in L.aok_last_error()
+    assert L.aok_plan_create(ctypes.byref(h), 0, ls, 2, 1, 0, 16) == _lib.AOK_ERR_INVALID
+    assert L.aok_plan_create(ctypes.byref(h), 1, ls, 2, 1, 7, 16) == _lib.AOK_ERR_INVALID
+    assert L.aok_overlap2c(None, None, None, None, None, None, None, None, 4, 1.0, None) == _lib.AOK_ERR_INVALID
+
+
+def test_to_bohr_requires_units_and_converts():
+    pos = np.array([[0.1, 1.0], [0.0, -2.0], [3.0, 0.5]])
+    with pytest.raises(aok.ArgumentError):
+        aok.to_bohr(pos)
+    b1 = aok.to_bohr(aok.Length(pos, "angstrom"))
+    b2 = aok.to_bohr(aok.Length(pos / 10, "nm"))
+    assert np.allclose(b1, pos * aok.ang2bohr)
+    assert np.max(np.abs(b1 - b2)) < 1e-12
+    assert aok.to_bohr(aok.Length(pos, "angstrom"), np.float32).dtype == np.float32
+
+
+def test_length_factor():
+    from aok_b200.units import length_factor
+    assert length_factor("bohr") == 1.0
+    assert length_factor("angstrom") == aok.ang2bohr
+    assert abs(length_factor("nm") - 10 * aok.ang2bohr) < 1e-12
+    with pytest.raises(RuntimeError):
+        length_factor("furlong")
+
+
+def test_species_lookup_and_errors():
+    from aok_b200.basis import species_indices
+    assert list(species_indices((6, 1, 8), [8, 6, 1, 1])) == [3, 1, 2, 2]
+    with pytest.raises(aok.AOKError):
+        species_indices((6, 1, 8), [99])
+
+
+def test_orbital_index_maps():
+    orb = aok.gaussian_orbitals(4, 3, length_unit="bohr")
+    assert len(orb) == sum((2 * s["l"] + 1) for s in orb.Rnl.spec)
+    for k, s in enumerate(orb.spec):
+        l, m = s["l"], s["m"]
+        assert orb.ylmidx[k] == l * l + l + m + 1
+        assert orb.Rnl.spec[orb.radidx[k] - 1]["l"] == l
+    st = aok.initialstates(orb)
+    assert np.all(st["Rnl"]["poly"] == 0)
+    sto = aok.slater_orbitals(3, 2, length_unit="angstrom", K=4)
+    assert abs(sto.lengthscale - aok.ang2bohr) < 1e-15
+    assert list(aok.initialstates(sto)["Rnl"]["poly"]) == [nn["n1"] - 1 for nn in sto.Rnl.nnspec]
+
+
+def test_slater_compile_rejected():
+    with pytest.raises(RuntimeError):
+        aok.compile_basis(aok.slater_orbitals(3, 2, length_unit="bohr"))
+
+
+def test_workloads_reproducible():
+    W = aok.workloads
+    a, b = W.config2_basis(), W.config2_basis()
+    assert np.array_equal(a.zeta, b.zeta) and np.array_equal(a.D, b.D)
+    assert a.NZ == 4 and a.ls.max() <= 3 and 15 <= a.nbf_total <= 36
+    c0 = W.config0_basis()
+    assert c0.nbf_total == 15 and list(c0.ls) == [0, 0, 0, 1, 1, 2]
+    pr = W.config2_pairs(B=1000)
+    d = np.linalg.norm(pr.posB - pr.posA, axis=0)
+    assert d.min() >= 0.5 - 1e-12 and d.max() <= 8.0 + 1e-12
+    assert set(np.unique(pr.sidxA)) <= {1, 2, 3, 4}
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU failure path")
+def test_product_path_fails_loudly_without_gpu():
+    b = aok.workloads.config0_basis()
+    orb = aok.orbitals_from_species_basis(b)
+    with pytest.raises(aok.AOKError):
+        aok.compile_basis(orb)

@@ -1,0 +1,207 @@
+"""Pins the CPU oracle (test infrastructure) against known answers from the
+reference's own tests and against independent computations:
+
+* golden vectors (tests/golden, Gauss-Hermite quadrature / explicit harmonic
+  polynomials, see make_golden.py),
+* s/s closed form (test/integrals/test_reference.jl:10-20),
+* p-shell transpose symmetry (test_reference.jl:24-41),
+* analytic single-atom orbital overlap (test/orbitals/test_gaussianbasis.jl:226-246),
+* central finite differences for every pullback,
+* absent species -> zero gradient (test/integrals/test_overlap_2c_diff.jl:241-247).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import aok_b200 as aok
+import oracle
+
+W = aok.workloads
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "overlap_golden.npz"))
+
+
+def test_golden_2c():
+    S = oracle.overlap2c_gb(G["ls"], G["nprim"], G["coef"], G["alpha"], G["posA"], G["posB"])
+    assert np.max(np.abs(S - G["S"])) < 1e-13 * max(1.0, np.abs(G["S"]).max())
+
+
+def test_golden_3c():
+    V = oracle.overlap3c_gb(G["ls3"], G["nprim3"], G["coef3"], G["alpha3"], G["posA3"], G["posB3"], G["posC3"])
+    assert np.max(np.abs(V - G["V"])) < 1e-13 * max(1.0, np.abs(G["V"]).max())
+
+
+def test_golden_solid_harmonics():
+    Z, _ = oracle.solid_harmonics(G["pts"], 3)
+    assert np.max(np.abs(Z - G["Z"])) < 1e-13
+
+
+def test_ss_closed_form():
+    a, b = 1.3, 0.7
+    S = oracle.overlap2c_gb([0, 0], [1, 1], [1.0, 1.0], [a, b], np.zeros((3, 1)), np.zeros((3, 1)))
+    assert abs(S[0, 1, 0] - (math.pi / (a + b)) ** 1.5) < 1e-12
+
+
+def test_p_shell_transpose_symmetry():
+    A = np.zeros((3, 1))
+    B = np.array([[0.4], [0.7], [-0.2]]) * aok.ang2bohr
+    ls, nprim, coef, ex = [1, 1], [2, 2], [0.7, 0.3, 0.7, 0.3], [1.2, 0.4, 1.2, 0.4]
+    SAB = oracle.overlap2c_gb(ls, nprim, coef, ex, A, B)[:3, 3:, 0]
+    SBA = oracle.overlap2c_gb(ls, nprim, coef, ex, B, A)[:3, 3:, 0]
+    assert np.max(np.abs(SAB - SBA.T)) < 1e-12
+
+
+def test_orbital_path_equals_gb_path():
+    b = W.config0_basis()
+    coef = oracle.compile_coef(b.zeta, b.D, b.ls)
+    pr = W.config0_pairs(B=6)
+    S1 = oracle.overlap2c_orb(b.ls, coef, b.zeta, pr.sidxA, pr.sidxB, pr.posA, pr.posB)
+    ls, nprim, z, _ = W.gb_tables(b)
+    c = np.concatenate([coef[s, :nprim[s], 0] for s in range(len(ls))])
+    S2 = oracle.overlap2c_gb(ls, nprim, c, z, pr.posA, pr.posB)
+    assert np.max(np.abs(S1 - S2)) < 1e-14
+
+
+def test_harmonics_gradient_and_orthonormality():
+    rng = np.random.default_rng(0)
+    X = rng.normal(size=(3, 5))
+    Z, dZ = oracle.solid_harmonics(X, 3)
+    h = 1e-6
+    for c in range(3):
+        Xp, Xm = X.copy(), X.copy()
+        Xp[c] += h
+        Xm[c] -= h
+        fd = (oracle.solid_harmonics(Xp, 3)[0] - oracle.solid_harmonics(Xm, 3)[0]) / (2 * h)
+        assert np.max(np.abs(fd - dZ[c])) < 1e-7
+    # orthonormal on the unit sphere: Gauss-Legendre in cos(theta) x uniform phi
+    ct, wt = np.polynomial.legendre.leggauss(16)
+    ph = np.arange(32) * 2 * math.pi / 32
+    pts = np.array([[math.sqrt(1 - c * c) * math.cos(p), math.sqrt(1 - c * c) * math.sin(p), c]
+                    for c in ct for p in ph]).T
+    w = np.array([wc * 2 * math.pi / 32 for wc in wt for _ in ph])
+    Zs, _ = oracle.solid_harmonics(pts, 3)
+    gram = (Zs * w[:, None]).T @ Zs
+    assert np.max(np.abs(gram - np.eye(16))) < 1e-12
+    # l = 1 ordering (y, z, x)
+    Z1, _ = oracle.solid_harmonics(np.array([[0.3], [0.5], [0.7]]), 1)
+    c1 = math.sqrt(3 / (4 * math.pi))
+    assert np.allclose(Z1[0, 1:], c1 * np.array([0.5, 0.7, 0.3]), atol=1e-15)
+
+
+def test_analytic_single_atom_overlap():
+    """Numerical quadrature of <phi_i|phi_j> from the oracle's evaluate equals the
+    analytic single-atom overlap of test_gaussianbasis.jl:226-246."""
+    b = W.config0_basis()
+    sp = W.orbital_spec(b.ls)
+    # radial Gauss-Legendre on [0, 12] x angular product rule
+    rr, wr = np.polynomial.legendre.leggauss(160)
+    rr = 6.0 * (rr + 1.0)
+    wr = 6.0 * wr
+    ct, wt = np.polynomial.legendre.leggauss(12)
+    ph = np.arange(24) * 2 * math.pi / 24
+    dirs = np.array([[math.sqrt(1 - c * c) * math.cos(p), math.sqrt(1 - c * c) * math.sin(p), c]
+                     for c in ct for p in ph]).T
+    wa = np.array([wc * 2 * math.pi / 24 for wc in wt for _ in ph])
+    X = (dirs[:, None, :] * rr[None, :, None]).reshape(3, -1)
+    w = (wr[:, None] * rr[:, None] ** 2 * wa[None, :]).reshape(-1)
+    P = oracle.evaluate_ed(X, np.ones(X.shape[1], np.int64), b.zeta, b.D, np.zeros(6, np.int64), sp.iR, sp.iY,
+                           sp.L, with_grad=False)
+    Snum = (P * w[:, None]).T @ P
+    nb = len(sp.iR)
+    San = np.zeros((nb, nb))
+    for i in range(nb):
+        for j in range(nb):
+            (ni, li, mi), (nj, lj, mj) = sp.spec[i], sp.spec[j]
+            if li != lj or mi != mj:
+                continue
+            ki, kj = sp.iR[i] - 1, sp.iR[j] - 1
+            g = 0.5 * float(np.prod(np.arange(2 * li + 1, 0, -2))) / 2.0 ** (li + 1) * math.sqrt(math.pi)
+            acc = 0.0
+            for a in range(b.K):
+                for c in range(b.K):
+                    acc += b.D[ki, a, 0] * b.D[kj, c, 0] * (b.zeta[ki, a, 0] + b.zeta[kj, c, 0]) ** (-(li + 1.5))
+            San[i, j] = g * acc
+    assert np.max(np.abs(Snum - San)) < 1e-8
+    # unit self-overlap (the generator normalises D)
+    assert np.allclose(np.diag(San), 1.0, atol=1e-12)
+
+
+def _small_basis():
+    b = W.config2_basis()
+    return b
+
+
+def test_overlap_pullback_fd():
+    b = _small_basis()
+    pr = W.ragged_pairs(4, b.NZ, 3)
+    rng = np.random.default_rng(1)
+    dS = rng.standard_normal((b.nbf_total, b.nbf_total, 4))
+    coef = oracle.compile_coef(b.zeta, b.D, b.ls)
+    dc, da = oracle.overlap2c_orb_pb(dS, b.ls, coef, b.zeta, pr.sidxA, pr.sidxB, pr.posA, pr.posB)
+    V = rng.standard_normal(coef.shape)
+    h = 1e-6
+    f = lambda c, z: float(np.sum(dS * oracle.overlap2c_orb(b.ls, c, z, pr.sidxA, pr.sidxB, pr.posA, pr.posB)))
+    # coef: the overlap is bilinear; FD on real (non-zero) slots, as the forward skips zero coefs
+    Vr = V * (coef != 0)
+    fdc = (f(coef + h * Vr, b.zeta) - f(coef - h * Vr, b.zeta)) / (2 * h)
+    assert abs(np.sum(dc * Vr) - fdc) < 1e-7 * max(1, abs(fdc))
+    fda = (f(coef, b.zeta + h * Vr) - f(coef, b.zeta - h * Vr)) / (2 * h)
+    assert abs(np.sum(da * Vr) - fda) < 1e-6 * max(1, abs(fda))
+
+
+def test_compile_coef_pb_fd():
+    b = _small_basis()
+    rng = np.random.default_rng(2)
+    dcoef = rng.standard_normal(b.zeta.shape)
+    dD, dz = oracle.compile_coef_pb(dcoef, b.zeta, b.D, b.ls)
+    Wd = rng.standard_normal(b.D.shape) * (b.D != 0)
+    V = rng.standard_normal(b.zeta.shape) * (b.D != 0)
+    h = 1e-6
+    f = lambda z, D: float(np.sum(dcoef * oracle.compile_coef(z, D, b.ls)))
+    fdD = (f(b.zeta, b.D + h * Wd) - f(b.zeta, b.D - h * Wd)) / (2 * h)
+    fdz = (f(b.zeta + h * V, b.D) - f(b.zeta - h * V, b.D)) / (2 * h)
+    assert abs(np.sum(dD * Wd) - fdD) < 1e-7 * max(1, abs(fdD))
+    assert abs(np.sum(dz * V) - fdz) < 1e-7 * max(1, abs(fdz))
+
+
+def test_absent_species_zero_gradient():
+    b = _small_basis()
+    pr = W.ragged_pairs(8, 2, 5)
+    dS = np.random.default_rng(3).standard_normal((b.nbf_total, b.nbf_total, 8))
+    dz, dD = oracle.overlap_pullback_ps(dS, b.ls, b.zeta, b.D, pr.sidxA, pr.sidxB, pr.posA, pr.posB)
+    assert np.all(dz[:, :, 2:] == 0) and np.all(dD[:, :, 2:] == 0)
+
+
+@pytest.mark.parametrize("slater", [False, True])
+def test_evaluate_gradients_fd(slater):
+    b = W.config1_basis()
+    sp = W.orbital_spec(b.ls)
+    rng = np.random.default_rng(4)
+    X = rng.normal(size=(3, 9)) * 1.5
+    sidx = rng.integers(1, 4, size=9)
+    poly = np.array([0, 1, 2, 0, 1, 0]) if slater else np.zeros(6, np.int64)
+    P, dP = oracle.evaluate_ed(X, sidx, b.zeta, b.D, poly, sp.iR, sp.iY, sp.L, slater=slater, lengthscale=1.3)
+    h = 1e-6
+    for c in range(3):
+        Xp, Xm = X.copy(), X.copy()
+        Xp[c] += h
+        Xm[c] -= h
+        fd = (oracle.evaluate_ed(Xp, sidx, b.zeta, b.D, poly, sp.iR, sp.iY, sp.L, slater, 1.3, False) -
+              oracle.evaluate_ed(Xm, sidx, b.zeta, b.D, poly, sp.iR, sp.iY, sp.L, slater, 1.3, False)) / (2 * h)
+        assert np.max(np.abs(fd - dP[c])) < 1e-6
+    dPv = rng.standard_normal(P.shape)
+    dz, dD = oracle.evaluate_pb(dPv, X, sidx, b.zeta, b.D, poly, sp.iR, sp.iY, sp.L, slater, 1.3)
+    V = rng.standard_normal(b.zeta.shape)
+    f = lambda z, D: float(np.sum(dPv * oracle.evaluate_ed(X, sidx, z, D, poly, sp.iR, sp.iY, sp.L, slater, 1.3,
+                                                           False)))
+    fdz = (f(b.zeta + h * V, b.D) - f(b.zeta - h * V, b.D)) / (2 * h)
+    fdD = (f(b.zeta, b.D + h * V) - f(b.zeta, b.D - h * V)) / (2 * h)
+    assert abs(np.sum(dz * V) - fdz) < 1e-6 * max(1, abs(fdz))
+    assert abs(np.sum(dD * V) - fdD) < 1e-6 * max(1, abs(fdD))
+    dX = oracle.evaluate_pbx(dPv, dP)
+    U = rng.standard_normal(X.shape)
+    g = lambda Y: float(np.sum(dPv * oracle.evaluate_ed(Y, sidx, b.zeta, b.D, poly, sp.iR, sp.iY, sp.L, slater, 1.3,
+                                                        False)))
+    fdx = (g(X + h * U) - g(X - h * U)) / (2 * h)
+    assert abs(np.sum(dX * U) - fdx) < 1e-6 * max(1, abs(fdx))
