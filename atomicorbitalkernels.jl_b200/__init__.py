@@ -15,3 +15,5 @@ from .overlap import (NoTangent, batch_overlap, batch_overlap_, batch_overlap_3c
                       compile_coef, compile_coef_pb, overlap_pb_coef_alpha, rrule_batch_overlap)
 from .overlap import pullback_ps as overlap_pullback_ps  # noqa: F401
 from ._dev import colmajor_empty, colmajor_zeros  # noqa: F401
+from .orbitals import evaluate, evaluate_ed, rrule_evaluate  # noqa: F401,E402
+from .orbitals import pullback_ps as evaluate_pullback_ps  # noqa: F401,E402

@@ -1,0 +1,606 @@
+// orbitals.cu -- fused atomic-orbital evaluation phi_i = R_{iR[i]}(r) Z_{iY[i]}(r)
+// with spatial gradients, and its pullback, sm_100a.
+//
+// Replaces, in one kernel per call:
+//   _rnl_val_ka! / _rnl_ed_ka!        src/orbitals/gtostoradials.jl:117-153
+//   SpheriCart compute[_with_gradients] (called at atomicorbitals.jl:155,200)
+//   _aorb_val_ka! / _aorb_ed_ka!      src/orbitals/atomicorbitals.jl:110-125
+//   `r = norm.(Rs)`, `s .* Rs`, `dRnlm .*= s`   atomicorbitals.jl:138-141,153,198,208
+// and for the pullback
+//   _aorb_pbx_ka!                     atomicorbitals.jl:283-299
+//   _aorb_pbrad_ka! + radial pullback atomicorbitals.jl:249-267, gtostoradials.jl:232-267
+//
+// One thread per point: the radials (per-species zeta, D staged in shared
+// memory), the real solid harmonics Z_lm and their gradients (compile-time
+// L, recursion in registers), then the products written straight to the
+// reference layouts P[j + nX*i] and dP[c + 3*(j + nX*i)] (coalesced per
+// orbital).  The per-thread R, dR, Z, dZ live in shared memory so the
+// orbital index maps iR/iY can be arbitrary.
+//
+// Real solid harmonics (L2-normalised on the unit sphere, index l^2+l+m):
+//   Z_l0 = F_l0 Q_l^0,  Z_l,+m = sqrt2 F_lm Q_l^m C_m,  Z_l,-m = sqrt2 F_lm Q_l^m S_m,
+//   F_lm = sqrt((2l+1)/(4 pi) (l-m)!/(l+m)!),  C_m + i S_m = (x + i y)^m,
+//   Q_m^m = (2m-1)!!,  Q_{m+1}^m = (2m+1) z Q_m^m,
+//   Q_l^m = ((2l-1) z Q_{l-1}^m - (l+m-1) r^2 Q_{l-2}^m) / (l - m),
+// no Condon-Shortley phase (Z_1,-1 : Z_1,0 : Z_1,1 = y : z : x).
+//
+// The parameter pullback is deterministic: each warp reduces its 32 points'
+// contributions per species with a fixed butterfly, warps are summed in order
+// into a per-block FP64 row, and the rows are summed in block order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "aok_internal.h"
+
+namespace aok {
+
+constexpr int kEvalThreads = 128;
+constexpr int kEvalMaxL = 4;
+constexpr int kMaxY = (kEvalMaxL + 1) * (kEvalMaxL + 1);
+
+struct EvalParams {
+    void* P;          // (nX, nOrb)
+    void* dP;         // (3, nX, nOrb) or null
+    const void* X;    // (3, nX)
+    const int64_t* sidx;
+    const void* zeta; // (nRad, K, NZ)
+    const void* D;
+    const int* poly;  // (nRad)
+    const int* iR;    // (nOrb) 0-based
+    const int* iY;    // (nOrb) 0-based
+    int* err;
+    long long nX;
+    int nRad, K, NZ, nOrb, slater;
+    double scale;
+    double F[kMaxY];  // F_lm by index l^2+l+m (m >= 0 entries used)
+    // pullback only
+    const void* dPin; // (nX, nOrb)
+    void* dX;         // (3, nX) or null
+    double* rows;     // [block][2 * nRad*K*NZ] or null
+};
+
+// value + gradient
+template <typename FT> struct D4 {
+    FT v, x, y, z;
+};
+template <typename FT>
+__device__ __forceinline__ D4<FT> dmul(const D4<FT>& a, const D4<FT>& b) {
+    return {a.v * b.v, a.x * b.v + a.v * b.x, a.y * b.v + a.v * b.y, a.z * b.v + a.v * b.z};
+}
+template <typename FT>
+__device__ __forceinline__ D4<FT> dlin(FT ca, const D4<FT>& a, FT cb, const D4<FT>& b) {
+    return {ca * a.v + cb * b.v, ca * a.x + cb * b.x, ca * a.y + cb * b.y, ca * a.z + cb * b.z};
+}
+
+// Z_lm and gradients for l <= L at (x, y, z), written to Z[idx], G[3*idx + c].
+template <typename FT, int L>
+__device__ __forceinline__ void solid_harmonics(FT x, FT y, FT z, const double* F, FT* Zs, FT* Gs, int stride) {
+    const D4<FT> X{x, FT(1), FT(0), FT(0)}, Y{y, FT(0), FT(1), FT(0)}, Zd{z, FT(0), FT(0), FT(1)};
+    const D4<FT> r2{x * x + y * y + z * z, FT(2) * x, FT(2) * y, FT(2) * z};
+    D4<FT> C[L + 1], S[L + 1];
+    C[0] = {FT(1), FT(0), FT(0), FT(0)};
+    S[0] = {FT(0), FT(0), FT(0), FT(0)};
+#pragma unroll
+    for (int m = 0; m < L; ++m) {
+        C[m + 1] = dlin(FT(1), dmul(X, C[m]), FT(-1), dmul(Y, S[m]));
+        S[m + 1] = dlin(FT(1), dmul(X, S[m]), FT(1), dmul(Y, C[m]));
+    }
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+        D4<FT> q2{FT(0), FT(0), FT(0), FT(0)}, q1{FT(0), FT(0), FT(0), FT(0)};
+        FT dfac = FT(1);
+        for (int k = 2 * m - 1; k > 1; k -= 2) dfac *= FT(k);
+        D4<FT> q{dfac, FT(0), FT(0), FT(0)};  // Q_m^m
+#pragma unroll
+        for (int l = m; l <= L; ++l) {
+            if (l == m + 1) {
+                q = dmul(D4<FT>{FT(2 * m + 1) * z, FT(0), FT(0), FT(2 * m + 1)}, q1);
+            } else if (l >= m + 2) {
+                const D4<FT> a = dmul(D4<FT>{FT(2 * l - 1) * z, FT(0), FT(0), FT(2 * l - 1)}, q1);
+                const D4<FT> b = dmul(D4<FT>{FT(l + m - 1) * r2.v, FT(l + m - 1) * r2.x, FT(l + m - 1) * r2.y,
+                                             FT(l + m - 1) * r2.z},
+                                      q2);
+                const FT inv = FT(1) / FT(l - m);
+                q = dlin(inv, a, -inv, b);
+            }
+            const int i0 = l * l + l;
+            if (m == 0) {
+                const FT f = (FT)F[i0];
+                Zs[i0 * stride] = f * q.v;
+                Gs[(3 * i0 + 0) * stride] = f * q.x;
+                Gs[(3 * i0 + 1) * stride] = f * q.y;
+                Gs[(3 * i0 + 2) * stride] = f * q.z;
+            } else {
+                const FT f = (FT)(1.4142135623730951 * F[i0 + m]);
+                const D4<FT> pc = dmul(q, C[m]), ps = dmul(q, S[m]);
+                Zs[(i0 + m) * stride] = f * pc.v;
+                Gs[(3 * (i0 + m) + 0) * stride] = f * pc.x;
+                Gs[(3 * (i0 + m) + 1) * stride] = f * pc.y;
+                Gs[(3 * (i0 + m) + 2) * stride] = f * pc.z;
+                Zs[(i0 - m) * stride] = f * ps.v;
+                Gs[(3 * (i0 - m) + 0) * stride] = f * ps.x;
+                Gs[(3 * (i0 - m) + 1) * stride] = f * ps.y;
+                Gs[(3 * (i0 - m) + 2) * stride] = f * ps.z;
+            }
+            q2 = q1;
+            q1 = q;
+        }
+    }
+}
+
+// Radial k at r for species sg: R = r^p sum_m D e^{-zeta f(r)}, dR/dr.
+// FP32 sums use TwoSum compensation over the K terms.
+template <typename FT>
+__device__ __forceinline__ void radial(const FT* sz, const FT* sD, int k, int sg, int nRad, int K, int p, int slater,
+                                       FT r, FT& R, FT& dR) {
+    const FT f = slater ? r : r * r;
+    const FT df = slater ? FT(1) : FT(2) * r;
+    FT s = FT(0), se = FT(0), ds = FT(0);
+    for (int m = 0; m < K; ++m) {
+        const int o = k + nRad * (m + K * sg);
+        const FT z = sz[o];
+        const FT a = sD[o] * exp(-z * f);
+        if constexpr (sizeof(FT) == 4) {
+            const float t = s + a, bb = t - s;
+            se += (s - (t - bb)) + (a - bb);
+            s = t;
+        } else {
+            s += a;
+        }
+        ds += (-z * df) * a;
+    }
+    s += se;
+    FT rp = FT(1);
+    for (int i = 0; i < p; ++i) rp *= r;
+    FT drp = FT(0);
+    if (p > 0) {
+        drp = FT(p);
+        for (int i = 0; i < p - 1; ++i) drp *= r;
+    }
+    R = rp * s;
+    dR = drp * s + rp * ds;
+}
+
+// shared layout: zeta, D tables, then per-thread R, dR (nRad), Z (nY), G (3 nY)
+template <typename FT>
+struct EvalSmem {
+    FT* sz;
+    FT* sD;
+    FT* R;
+    FT* dR;
+    FT* Z;
+    FT* G;
+};
+template <typename FT>
+__device__ __forceinline__ EvalSmem<FT> eval_smem(unsigned char* raw, int ntab, int nRad, int nY) {
+    EvalSmem<FT> s;
+    FT* p = reinterpret_cast<FT*>(raw);
+    s.sz = p;
+    s.sD = p + ntab;
+    p += 2 * ntab;
+    s.R = p;
+    p += nRad * kEvalThreads;
+    s.dR = p;
+    p += nRad * kEvalThreads;
+    s.Z = p;
+    p += nY * kEvalThreads;
+    s.G = p;
+    return s;
+}
+
+template <typename FT, int L, bool GRAD>
+__global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant__ EvalParams P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int nY = (L + 1) * (L + 1);
+    const int ntab = P.nRad * P.K * P.NZ;
+    EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, nY);
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
+        S.sz[i] = ((const FT*)P.zeta)[i];
+        S.sD[i] = ((const FT*)P.D)[i];
+    }
+    __syncthreads();
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= P.nX) return;
+    const int t = threadIdx.x;
+    const FT* X = (const FT*)P.X;
+    FT x = X[3 * j], y = X[3 * j + 1], z = X[3 * j + 2];
+    const FT sc = (FT)P.scale;
+    if (sc != FT(1)) {
+        x = sc * x;
+        y = sc * y;
+        z = sc * z;
+    }
+    const FT r = sqrt(x * x + y * y + z * z);
+    int sg = (int)P.sidx[j] - 1;
+    if (sg < 0 || sg >= P.NZ) {
+        atomicCAS(P.err, 0, AOK_ERR_SPECIES);
+        sg = 0;
+    }
+    for (int k = 0; k < P.nRad; ++k) {
+        FT R, dR;
+        radial<FT>(S.sz, S.sD, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+        S.R[k * kEvalThreads + t] = R;
+        S.dR[k * kEvalThreads + t] = dR;
+    }
+    solid_harmonics<FT, L>(x, y, z, P.F, S.Z + t, S.G + t, kEvalThreads);
+    FT* Pout = (FT*)P.P;
+    FT* dPout = (FT*)P.dP;
+    const FT ux = x / r, uy = y / r, uz = z / r;  // X[j] / r[j] (NaN at r = 0, as the reference)
+    for (int i = 0; i < P.nOrb; ++i) {
+        const int k = P.iR[i], yi = P.iY[i];
+        const FT rn = S.R[k * kEvalThreads + t], yl = S.Z[yi * kEvalThreads + t];
+        Pout[j + P.nX * i] = rn * yl;
+        if (GRAD) {
+            const FT dr = S.dR[k * kEvalThreads + t];
+            FT* o = dPout + 3 * (j + P.nX * i);
+            FT gx = (dr * ux) * yl + rn * S.G[(3 * yi + 0) * kEvalThreads + t];
+            FT gy = (dr * uy) * yl + rn * S.G[(3 * yi + 1) * kEvalThreads + t];
+            FT gz = (dr * uz) * yl + rn * S.G[(3 * yi + 2) * kEvalThreads + t];
+            if (sc != FT(1)) {
+                gx *= sc;
+                gy *= sc;
+                gz *= sc;
+            }
+            o[0] = gx;
+            o[1] = gy;
+            o[2] = gz;
+        }
+    }
+}
+
+// Pullback: dX (optional) and per-block rows of (dD, dzeta) partials.
+template <typename FT, int L>
+__global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_constant__ EvalParams P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int nY = (L + 1) * (L + 1);
+    constexpr int NW = kEvalThreads / 32;
+    const int ntab = P.nRad * P.K * P.NZ;
+    EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, nY);
+    // per-warp FP64 accumulators [warp][2][ntab] after the per-thread scratch
+    double* wacc = reinterpret_cast<double*>(
+        smem_raw + (((size_t)2 * ntab + (size_t)(2 * P.nRad + 4 * nY) * kEvalThreads) * sizeof(FT) + 7) / 8 * 8);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
+        S.sz[i] = ((const FT*)P.zeta)[i];
+        S.sD[i] = ((const FT*)P.D)[i];
+    }
+    for (int i = threadIdx.x; i < NW * 2 * ntab; i += blockDim.x) wacc[i] = 0.0;
+    __syncthreads();
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = j < P.nX;
+    const int t = threadIdx.x;
+    FT x = FT(0), y = FT(0), z = FT(1);
+    int sg = -1;
+    if (valid) {
+        const FT* X = (const FT*)P.X;
+        x = X[3 * j];
+        y = X[3 * j + 1];
+        z = X[3 * j + 2];
+        const FT sc = (FT)P.scale;
+        if (sc != FT(1)) {
+            x = sc * x;
+            y = sc * y;
+            z = sc * z;
+        }
+        sg = (int)P.sidx[j] - 1;
+        if (sg < 0 || sg >= P.NZ) {
+            atomicCAS(P.err, 0, AOK_ERR_SPECIES);
+            sg = -1;
+        }
+    }
+    const FT r = sqrt(x * x + y * y + z * z);
+    const int sgc = sg < 0 ? 0 : sg;
+    for (int k = 0; k < P.nRad; ++k) {
+        FT R, dR;
+        radial<FT>(S.sz, S.sD, k, sgc, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+        S.R[k * kEvalThreads + t] = R;
+        S.dR[k * kEvalThreads + t] = dR;
+    }
+    solid_harmonics<FT, L>(x, y, z, P.F, S.Z + t, S.G + t, kEvalThreads);
+    const FT* dPin = (const FT*)P.dPin;
+    // dX = sum_i dP[j,i] grad phi_i ; dRad[k] = sum_{i: iR = k} dP[j,i] Z_iY  (reuses the dR slots' neighbour)
+    FT ax = FT(0), ay = FT(0), az = FT(0);
+    const FT ux = x / r, uy = y / r, uz = z / r;
+    // accumulate dRad into S.R after dX is done: first pass dX
+    if (valid && P.dX) {
+        for (int i = 0; i < P.nOrb; ++i) {
+            const int k = P.iR[i], yi = P.iY[i];
+            const FT g = dPin[j + P.nX * i];
+            const FT rn = S.R[k * kEvalThreads + t], yl = S.Z[yi * kEvalThreads + t];
+            const FT dr = S.dR[k * kEvalThreads + t];
+            ax += g * ((dr * ux) * yl + rn * S.G[(3 * yi + 0) * kEvalThreads + t]);
+            ay += g * ((dr * uy) * yl + rn * S.G[(3 * yi + 1) * kEvalThreads + t]);
+            az += g * ((dr * uz) * yl + rn * S.G[(3 * yi + 2) * kEvalThreads + t]);
+        }
+        const FT sc = (FT)P.scale;
+        FT* dX = (FT*)P.dX;
+        dX[3 * j] = sc != FT(1) ? ax * sc : ax;
+        dX[3 * j + 1] = sc != FT(1) ? ay * sc : ay;
+        dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
+    }
+    if (!P.rows) return;
+    // dRad[k] into S.dR (radial derivative no longer needed)
+    for (int k = 0; k < P.nRad; ++k) S.dR[k * kEvalThreads + t] = FT(0);
+    if (valid)
+        for (int i = 0; i < P.nOrb; ++i) {
+            const int k = P.iR[i], yi = P.iY[i];
+            S.dR[k * kEvalThreads + t] += dPin[j + P.nX * i] * S.Z[yi * kEvalThreads + t];
+        }
+    // per (k, m): contributions of this point to its species' slot, reduced over the warp per species
+    const FT f = P.slater ? r : r * r;
+    for (int k = 0; k < P.nRad; ++k) {
+        const int p = P.poly[k];
+        FT rp = FT(1);
+        for (int i = 0; i < p; ++i) rp *= r;
+        const FT gg = S.dR[k * kEvalThreads + t] * rp;
+        for (int m = 0; m < P.K; ++m) {
+            FT cD = FT(0), cZ = FT(0);
+            if (sg >= 0) {
+                const int o = k + P.nRad * (m + P.K * sg);
+                const FT a = exp(-S.sz[o] * f);
+                cD = gg * a;
+                cZ = ((gg * S.sD[o]) * a) * (-f);
+            }
+            for (int s = 0; s < P.NZ; ++s) {
+                double vD = (sg == s) ? (double)cD : 0.0, vZ = (sg == s) ? (double)cZ : 0.0;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    vD += __shfl_xor_sync(0xffffffffu, vD, off);
+                    vZ += __shfl_xor_sync(0xffffffffu, vZ, off);
+                }
+                if (lane == 0) {
+                    const int o = k + P.nRad * (m + P.K * s);
+                    wacc[(size_t)warp * 2 * ntab + o] += vD;
+                    wacc[(size_t)warp * 2 * ntab + ntab + o] += vZ;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    double* row = P.rows + (size_t)blockIdx.x * 2 * ntab;
+    for (int i = threadIdx.x; i < 2 * ntab; i += blockDim.x) {
+        double sum = 0.0;
+        for (int w = 0; w < NW; ++w) sum += wacc[(size_t)w * 2 * ntab + i];
+        row[i] = sum;
+    }
+}
+
+template <typename FT>
+__global__ void k_eval_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const double* __restrict__ rows, int nrows,
+                              int ntab) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * ntab) return;
+    double s = 0.0;
+    for (int r = 0; r < nrows; ++r) s += rows[(size_t)r * 2 * ntab + t];
+    if (t < ntab) dD[t] = (FT)s;
+    else dzeta[t - ntab] = (FT)s;
+}
+
+static size_t eval_smem_bytes(const aok_orbitals* o, bool pb) {
+    const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
+    const int nY = (o->L + 1) * (o->L + 1);
+    const size_t ntab = (size_t)(o->nRad * o->K * o->NZ);
+    size_t b = (2 * ntab + (size_t)(2 * o->nRad + 4 * nY) * kEvalThreads) * fsz;
+    if (pb) b = (b + 7) / 8 * 8 + (size_t)(kEvalThreads / 32) * 2 * ntab * 8;
+    return b;
+}
+
+template <typename FT, int L>
+static int launch_eval_L(aok_orbitals* o, EvalParams& P, bool grad, bool pb, cudaStream_t s) {
+    const size_t smem = eval_smem_bytes(o, pb);
+    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "evaluate: basis too large for shared memory");
+    const int grid = (int)((P.nX + kEvalThreads - 1) / kEvalThreads);
+    cudaError_t e;
+    if (pb) {
+        auto k = k_evaluate_pb<FT, L>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pb)");
+        k<<<grid, kEvalThreads, smem, s>>>(P);
+        return cuda_status(cudaGetLastError(), "k_evaluate_pb");
+    }
+    if (grad) {
+        auto k = k_evaluate<FT, L, true>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate)");
+        k<<<grid, kEvalThreads, smem, s>>>(P);
+    } else {
+        auto k = k_evaluate<FT, L, false>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate)");
+        k<<<grid, kEvalThreads, smem, s>>>(P);
+    }
+    return cuda_status(cudaGetLastError(), "k_evaluate");
+}
+
+template <typename FT>
+static int launch_eval_T(aok_orbitals* o, EvalParams& P, bool grad, bool pb, cudaStream_t s) {
+    switch (o->L) {
+        case 0: return launch_eval_L<FT, 0>(o, P, grad, pb, s);
+        case 1: return launch_eval_L<FT, 1>(o, P, grad, pb, s);
+        case 2: return launch_eval_L<FT, 2>(o, P, grad, pb, s);
+        case 3: return launch_eval_L<FT, 3>(o, P, grad, pb, s);
+        case 4: return launch_eval_L<FT, 4>(o, P, grad, pb, s);
+        default: return set_error(AOK_ERR_UNSUPPORTED, "evaluate: harmonics above l = 4");
+    }
+}
+
+static void fill_params(aok_orbitals* o, EvalParams& P, const void* X, const int64_t* sidx, const void* zeta,
+                        const void* D, int64_t nX, double lengthscale) {
+    memset(&P, 0, sizeof(P));
+    P.X = X;
+    P.sidx = sidx;
+    P.zeta = zeta;
+    P.D = D;
+    P.poly = o->d_poly;
+    P.iR = o->d_iR;
+    P.iY = o->d_iY;
+    P.err = o->d_err;
+    P.nX = nX;
+    P.nRad = (int)o->nRad;
+    P.K = (int)o->K;
+    P.NZ = (int)o->NZ;
+    P.nOrb = (int)o->nOrb;
+    P.slater = o->radial == AOK_RADIAL_SLATER;
+    P.scale = lengthscale;
+    for (int l = 0; l <= o->L; ++l)
+        for (int m = 0; m <= l; ++m) {
+            double fac = 1.0;
+            for (int q = l - m + 1; q <= l + m; ++q) fac /= (double)q;
+            P.F[l * l + l + m] = std::sqrt((2.0 * l + 1.0) / (4.0 * 3.14159265358979323846) * fac);
+        }
+}
+
+int launch_evaluate(aok_orbitals* o, void* Pv, void* dP, const void* X, const int64_t* sidx, const void* zeta,
+                    const void* D, int64_t nX, double lengthscale, cudaStream_t s) {
+    EvalParams P;
+    fill_params(o, P, X, sidx, zeta, D, nX, lengthscale);
+    P.P = Pv;
+    P.dP = dP;
+    if (o->prec == AOK_PREC_F64) return launch_eval_T<double>(o, P, dP != nullptr, false, s);
+    return launch_eval_T<float>(o, P, dP != nullptr, false, s);
+}
+
+int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const void* dPin, const void* X,
+                       const int64_t* sidx, const void* zeta, const void* D, int64_t nX, double lengthscale,
+                       cudaStream_t s) {
+    EvalParams P;
+    fill_params(o, P, X, sidx, zeta, D, nX, lengthscale);
+    P.dPin = dPin;
+    P.dX = dX;
+    const int grid = (int)((nX + kEvalThreads - 1) / kEvalThreads);
+    const int ntab = (int)(o->nRad * o->K * o->NZ);
+    if (dzeta && dD) {
+        if (grid > o->max_blocks) {
+            if (o->d_partials) cudaFree(o->d_partials);
+            o->d_partials = nullptr;
+            cudaError_t e = cudaMalloc(&o->d_partials, sizeof(double) * 2 * ntab * (size_t)grid);
+            if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(evaluate partials)");
+            o->max_blocks = grid;
+        }
+        P.rows = (double*)o->d_partials;
+    }
+    int st = o->prec == AOK_PREC_F64 ? launch_eval_T<double>(o, P, true, true, s)
+                                     : launch_eval_T<float>(o, P, true, true, s);
+    if (st != AOK_OK || !P.rows) return st;
+    if (o->prec == AOK_PREC_F64)
+        k_eval_reduce<double><<<(2 * ntab + 127) / 128, 128, 0, s>>>((double*)dD, (double*)dzeta, P.rows, grid, ntab);
+    else
+        k_eval_reduce<float><<<(2 * ntab + 127) / 128, 128, 0, s>>>((float*)dD, (float*)dzeta, P.rows, grid, ntab);
+    return cuda_status(cudaGetLastError(), "k_eval_reduce");
+}
+
+}  // namespace aok
+
+using namespace aok;
+
+extern "C" {
+
+int aok_orbitals_create(aok_orbitals** out, int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly, int64_t nOrb,
+                        const int64_t* iR, const int64_t* iY, int64_t L, int radial_kind, int precision) {
+    if (!out || !poly || !iR || !iY) return set_error(AOK_ERR_INVALID, "aok_orbitals_create: null pointer");
+    *out = nullptr;
+    if (nRad <= 0 || K <= 0 || NZ <= 0 || nOrb <= 0 || L < 0)
+        return set_error(AOK_ERR_INVALID, "aok_orbitals_create: sizes must be positive");
+    if (L > kEvalMaxL) return set_error(AOK_ERR_UNSUPPORTED, "aok_orbitals_create: harmonics above l = 4");
+    if (radial_kind != AOK_RADIAL_GAUSSIAN && radial_kind != AOK_RADIAL_SLATER)
+        return set_error(AOK_ERR_INVALID, "aok_orbitals_create: unknown radial kind");
+    if (precision != AOK_PREC_F64 && precision != AOK_PREC_F32C)
+        return set_error(AOK_ERR_INVALID, "aok_orbitals_create: unknown precision");
+    const int64_t nY = (L + 1) * (L + 1);
+    std::vector<int> p32(nRad), r32(nOrb), y32(nOrb);
+    for (int64_t k = 0; k < nRad; ++k) {
+        if (poly[k] < 0 || poly[k] > 64) return set_error(AOK_ERR_INVALID, "aok_orbitals_create: bad radial power");
+        p32[k] = (int)poly[k];
+    }
+    for (int64_t i = 0; i < nOrb; ++i) {
+        if (iR[i] < 1 || iR[i] > nRad || iY[i] < 1 || iY[i] > nY)
+            return set_error(AOK_ERR_INVALID, "aok_orbitals_create: orbital index map out of range");
+        r32[i] = (int)(iR[i] - 1);
+        y32[i] = (int)(iY[i] - 1);
+    }
+    aok_orbitals* o = new aok_orbitals();
+    o->nRad = nRad;
+    o->K = K;
+    o->NZ = NZ;
+    o->nOrb = nOrb;
+    o->L = (int)L;
+    o->radial = radial_kind;
+    o->prec = precision;
+    o->poly.assign(poly, poly + nRad);
+    o->iR.assign(iR, iR + nOrb);
+    o->iY.assign(iY, iY + nOrb);
+    auto fail = [&](int code) {
+        aok_orbitals_destroy(o);
+        return code;
+    };
+    int st;
+    if ((st = cuda_status(cudaGetDevice(&o->device), "cudaGetDevice"))) return fail(st);
+    if ((st = cuda_status(cudaDeviceGetAttribute(&o->num_sms, cudaDevAttrMultiProcessorCount, o->device),
+                          "cudaDeviceGetAttribute")))
+        return fail(st);
+    if ((st = cuda_status(cudaMalloc(&o->d_poly, sizeof(int) * nRad), "cudaMalloc(poly)")) ||
+        (st = cuda_status(cudaMalloc(&o->d_iR, sizeof(int) * nOrb), "cudaMalloc(iR)")) ||
+        (st = cuda_status(cudaMalloc(&o->d_iY, sizeof(int) * nOrb), "cudaMalloc(iY)")) ||
+        (st = cuda_status(cudaMalloc(&o->d_err, sizeof(int)), "cudaMalloc(err)")))
+        return fail(st);
+    if ((st = cuda_status(cudaMemcpy(o->d_poly, p32.data(), sizeof(int) * nRad, cudaMemcpyHostToDevice), "memcpy")) ||
+        (st = cuda_status(cudaMemcpy(o->d_iR, r32.data(), sizeof(int) * nOrb, cudaMemcpyHostToDevice), "memcpy")) ||
+        (st = cuda_status(cudaMemcpy(o->d_iY, y32.data(), sizeof(int) * nOrb, cudaMemcpyHostToDevice), "memcpy")) ||
+        (st = cuda_status(cudaMemset(o->d_err, 0, sizeof(int)), "memset")))
+        return fail(st);
+    if (eval_smem_bytes(o, true) > 227 * 1024)
+        return fail(set_error(AOK_ERR_UNSUPPORTED, "aok_orbitals_create: basis too large for shared memory"));
+    *out = o;
+    return AOK_OK;
+}
+
+int aok_orbitals_destroy(aok_orbitals* o) {
+    if (!o) return AOK_OK;
+    void* bufs[] = {o->d_poly, o->d_iR, o->d_iY, o->d_partials, o->d_err};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    delete o;
+    return AOK_OK;
+}
+
+int aok_evaluate(aok_orbitals* o, void* P, const void* X, const int64_t* sidx, const void* zeta, const void* D,
+                 int64_t nX, double lengthscale, void* stream) {
+    if (!o) return set_error(AOK_ERR_INVALID, "aok_evaluate: null plan");
+    if (nX < 0) return set_error(AOK_ERR_INVALID, "aok_evaluate: negative nX");
+    if (nX == 0) return AOK_OK;
+    if (!P || !X || !sidx || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_evaluate: null pointer");
+    return launch_evaluate(o, P, nullptr, X, sidx, zeta, D, nX, lengthscale, (cudaStream_t)stream);
+}
+
+int aok_evaluate_ed(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx, const void* zeta,
+                    const void* D, int64_t nX, double lengthscale, void* stream) {
+    if (!o) return set_error(AOK_ERR_INVALID, "aok_evaluate_ed: null plan");
+    if (nX < 0) return set_error(AOK_ERR_INVALID, "aok_evaluate_ed: negative nX");
+    if (nX == 0) return AOK_OK;
+    if (!P || !dP || !X || !sidx || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_evaluate_ed: null pointer");
+    return launch_evaluate(o, P, dP, X, sidx, zeta, D, nX, lengthscale, (cudaStream_t)stream);
+}
+
+int aok_evaluate_pullback(aok_orbitals* o, void* dX, void* dzeta, void* dD, const void* dP, const void* X,
+                          const int64_t* sidx, const void* zeta, const void* D, int64_t nX, double lengthscale,
+                          void* stream) {
+    if (!o) return set_error(AOK_ERR_INVALID, "aok_evaluate_pullback: null plan");
+    if ((dzeta == nullptr) != (dD == nullptr))
+        return set_error(AOK_ERR_INVALID, "aok_evaluate_pullback: dzeta and dD must both be given or both null");
+    if (nX < 0) return set_error(AOK_ERR_INVALID, "aok_evaluate_pullback: negative nX");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
+    if (nX == 0) {
+        if (dzeta) {
+            int st = cuda_status(cudaMemsetAsync(dzeta, 0, fsz * o->nRad * o->K * o->NZ, s), "memset");
+            if (st) return st;
+            return cuda_status(cudaMemsetAsync(dD, 0, fsz * o->nRad * o->K * o->NZ, s), "memset");
+        }
+        return AOK_OK;
+    }
+    if (!dP || !X || !sidx || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_evaluate_pullback: null pointer");
+    return launch_evaluate_pb(o, dX, dzeta, dD, dP, X, sidx, zeta, D, nX, lengthscale, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,123 @@
+"""Fused orbital evaluation (values, spatial gradients, pullbacks) on the GPU
+vs the FP64 oracle, through the C ABI."""
+import numpy as np
+import pytest
+import torch
+
+import aok_b200 as aok
+import oracle
+from helpers import f32_round, rel_fro
+
+W = aok.workloads
+pytestmark = pytest.mark.gpu
+
+
+def _basis(slater=False, unit="bohr"):
+    b = W.config1_basis()
+    orb = aok.orbitals_from_species_basis(b, length_unit=unit)
+    if slater:
+        nn = [dict(n1=i % 3 + 1, n2=1, l=s["l"]) for i, s in enumerate(orb.Rnl.spec)]
+        rad = aok.SlaterTypeRadials(b.zeta, b.D, orb.Rnl.spec, nn, b.zlist)
+        orb = aok.AtomicOrbitals(rad, orb.L, unit)
+    return b, orb
+
+
+def _ref(orb, X, sidx, FT=np.float64):
+    sp = W.orbital_spec([s["l"] for s in orb.Rnl.spec])
+    poly = orb.Rnl.powers()
+    z, D = orb.Rnl.zeta, orb.Rnl.D
+    if FT == np.float32:
+        z, D, X = f32_round(z), f32_round(D), f32_round(X)
+    P, dP = oracle.evaluate_ed(X, sidx, z, D, poly, orb.radidx, orb.ylmidx, orb.L,
+                               slater=not orb.is_gaussian, lengthscale=orb.lengthscale, nthreads=8)
+    return P, dP
+
+
+@pytest.mark.parametrize("slater", [False, True])
+def test_evaluate_ed_f64(slater):
+    b, orb = _basis(slater)
+    X, sidx = W.config1_points(nX=5000)
+    Xs = aok.PStates(X, list(sidx))
+    P, dP = aok.evaluate_ed(orb, Xs)
+    Pr, dPr = _ref(orb, X, sidx)
+    assert P.shape == (5000, len(orb)) and dP.shape == (5000, len(orb), 3)
+    assert rel_fro(P.cpu().numpy(), Pr) < 1e-12
+    assert rel_fro(dP.cpu().numpy(), np.transpose(dPr, (1, 2, 0))) < 1e-12
+    P2 = aok.evaluate(orb, Xs)
+    assert torch.equal(P2, P)
+
+
+def test_evaluate_ed_f32c():
+    b, orb = _basis()
+    X, sidx = W.config1_points(nX=1 << 16)
+    ps = {"Rnl": {"zeta": b.zeta.astype(np.float32), "D": b.D.astype(np.float32)}, "Ylm": {}}
+    st = aok.initialstates(orb)
+    P, dP = aok.evaluate_ed(orb, aok.PStates(X.astype(np.float32), sidx), ps, st)
+    assert P.dtype == torch.float32
+    Pr, dPr = _ref(orb, X, sidx, np.float32)
+    assert rel_fro(P.cpu().numpy(), Pr) < 2e-6
+    assert rel_fro(dP.cpu().numpy(), np.transpose(dPr, (1, 2, 0))) < 2e-6
+
+
+def test_positions_default_to_species_1_and_lengthscale():
+    b, orbA = _basis(unit="angstrom")
+    _, orbB = _basis(unit="bohr")
+    X = np.random.default_rng(0).normal(size=(3, 77))
+    PA, dA = aok.evaluate_ed(orbA, X)
+    PB, dB = aok.evaluate_ed(orbB, X * aok.ang2bohr)
+    assert np.max(np.abs(PA.cpu().numpy() - PB.cpu().numpy())) < 1e-12
+    assert np.max(np.abs(dA.cpu().numpy() - aok.ang2bohr * dB.cpu().numpy())) < 1e-12
+    P1 = aok.evaluate(orbB, aok.PStates(X, [1] * 77))
+    assert torch.equal(aok.evaluate(orbB, X), P1)
+
+
+def test_unknown_species_raises():
+    b, orb = _basis()
+    with pytest.raises(aok.AOKError):
+        aok.evaluate(orb, aok.PStates(np.zeros((3, 1)), [99]))
+
+
+@pytest.mark.parametrize("slater", [False, True])
+def test_pullbacks_f64(slater):
+    b, orb = _basis(slater)
+    X, sidx = W.config1_points(nX=3000)
+    Xs = aok.PStates(X, list(sidx))
+    ps, st = aok.initialparameters(orb), aok.initialstates(orb)
+    dPv = np.random.default_rng(2).standard_normal((3000, len(orb)))
+    g = aok.evaluate_pullback_ps(dPv, orb, Xs, ps, st)
+    rz, rD = oracle.evaluate_pb(dPv, X, sidx, b.zeta, b.D, orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L,
+                                slater=slater, lengthscale=orb.lengthscale)
+    assert rel_fro(g["Rnl"]["zeta"].cpu().numpy(), rz) < 1e-12
+    assert rel_fro(g["Rnl"]["D"].cpu().numpy(), rD) < 1e-12
+    P, pb = aok.rrule_evaluate(orb, Xs, ps, st)
+    out = pb(dPv)
+    _, dPr = _ref(orb, X, sidx)
+    rX = oracle.evaluate_pbx(dPv, dPr)
+    assert rel_fro(out[2].cpu().numpy(), rX) < 1e-12
+    assert torch.equal(out[3]["Rnl"]["zeta"], g["Rnl"]["zeta"])
+
+
+def test_pullback_f32c_and_deterministic():
+    b, orb = _basis()
+    X, sidx = W.config1_points(nX=1 << 18)
+    ps = {"Rnl": {"zeta": b.zeta.astype(np.float32), "D": b.D.astype(np.float32)}, "Ylm": {}}
+    st = aok.initialstates(orb)
+    dPv = np.random.default_rng(3).standard_normal((1 << 18, len(orb))).astype(np.float32)
+    Xs = aok.PStates(X.astype(np.float32), sidx)
+    g1 = aok.evaluate_pullback_ps(dPv, orb, Xs, ps, st)
+    g2 = aok.evaluate_pullback_ps(dPv, orb, Xs, ps, st)
+    assert torch.equal(g1["Rnl"]["zeta"], g2["Rnl"]["zeta"]) and torch.equal(g1["Rnl"]["D"], g2["Rnl"]["D"])
+    rz, rD = oracle.evaluate_pb(f32_round(dPv), f32_round(X), sidx, f32_round(b.zeta), f32_round(b.D),
+                                orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L)
+    assert rel_fro(g1["Rnl"]["zeta"].cpu().numpy(), rz) < 2e-5
+    assert rel_fro(g1["Rnl"]["D"].cpu().numpy(), rD) < 2e-5
+
+
+def test_absent_species_zero_param_gradient():
+    b, orb = _basis()
+    X, _ = W.config1_points(nX=500)
+    sidx = np.random.default_rng(4).integers(1, 3, size=500)
+    g = aok.evaluate_pullback_ps(np.ones((500, len(orb))), orb, aok.PStates(X, list(sidx)),
+                                 aok.initialparameters(orb), aok.initialstates(orb))
+    assert np.all(g["Rnl"]["zeta"].cpu().numpy()[:, :, 2] == 0)
+    assert np.all(g["Rnl"]["D"].cpu().numpy()[:, :, 2] == 0)
