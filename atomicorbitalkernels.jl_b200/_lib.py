@@ -31,7 +31,7 @@ EXPORTS = [
     "aok_plan_check", "aok_plan_timing_enable", "aok_plan_timing_read", "aok_compile_coef", "aok_overlap2c", "aok_overlap2c_gb", "aok_overlap3c_gb",
     "aok_overlap2c_pullback", "aok_compile_coef_pullback", "aok_overlap_pullback_ps",
     "aok_orbitals_create", "aok_orbitals_destroy", "aok_evaluate", "aok_evaluate_ed",
-    "aok_evaluate_pullback",
+    "aok_evaluate_pullback", "aok_evaluate_pullback_noalloc",
 ]
 
 
@@ -89,6 +89,8 @@ def load():
     L.aok_evaluate.argtypes = [vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_evaluate_ed.argtypes = [vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_evaluate_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
+    L.aok_evaluate_pullback_noalloc.argtypes = [i64, i64, i64, pi64, i64, pi64, pi64, i64, cint, cint, vp, vp, vp,
+                                                vp, vp, vp, vp, vp, i64, dbl, vp]
     for name in EXPORTS:
         if name not in ("aok_last_error", "aok_version"):
             getattr(L, name).restype = cint

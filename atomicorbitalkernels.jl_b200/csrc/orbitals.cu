@@ -604,3 +604,171 @@ int aok_evaluate_pullback(aok_orbitals* o, void* dX, void* dzeta, void* dD, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free evaluate pullback.
+//
+// Some callers cannot allocate device memory when they need this pullback:
+// a host framework that owns the whole device through its own pooling
+// allocator (and forbids allocations behind its back), or a long-running
+// service that reserves its memory at start-up and must not grow later.
+// aok_evaluate_pullback allocates twice (the aok_orbitals plan and, on
+// first use, its per-block partial rows); this variant needs neither: the
+// index maps, the device error word and the per-block FP64 partial rows live
+// in one file-scope device array of kNoAllocScratchBytes (8 MiB) that every
+// GPU which loads the library holds until the process exits.
+//
+// The array's host-side name is not a device address, so the first call on
+// each device looks up the real address with cudaGetSymbolAddress (with that
+// device current) and caches it; make that first call before any stream
+// capture.  Every call shares the one array and overwrites it (the error word
+// is cleared by each call, every partial row is rewritten), so calls that can
+// overlap on the GPU -- on different streams, or on the same device from
+// different threads without ordering -- race on it and must be serialised by
+// the caller.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace aok {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
+constexpr int kNoAllocMaxRad = 64;
+constexpr int kNoAllocMaxOrb = 256;
+constexpr size_t kNoAllocMapsOffset = 256;        // after the error word
+constexpr size_t kNoAllocRowsOffset = 4096;       // after the index maps
+static_assert(kNoAllocMapsOffset + sizeof(int) * (kNoAllocMaxRad + 2 * kNoAllocMaxOrb) <= kNoAllocRowsOffset,
+              "index maps overflow their region");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[256];
+
+struct NoAllocMaps {
+    int nRad, nOrb;
+    int poly[kNoAllocMaxRad];
+    int iR[kNoAllocMaxOrb];
+    int iY[kNoAllocMaxOrb];
+};
+
+// copies the index maps (kernel parameters) into the scratch and clears the error word
+__global__ void k_noalloc_setup(const __grid_constant__ NoAllocMaps m, unsigned char* scratch) {
+    int* err = reinterpret_cast<int*>(scratch);
+    int* maps = reinterpret_cast<int*>(scratch + kNoAllocMapsOffset);
+    if (threadIdx.x == 0) *err = 0;
+    for (int i = threadIdx.x; i < m.nRad; i += blockDim.x) maps[i] = m.poly[i];
+    for (int i = threadIdx.x; i < m.nOrb; i += blockDim.x) {
+        maps[kNoAllocMaxRad + i] = m.iR[i];
+        maps[kNoAllocMaxRad + kNoAllocMaxOrb + i] = m.iY[i];
+    }
+}
+
+static int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    int st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != AOK_OK) return st;
+    if (dev < 0 || dev >= 256) return set_error(AOK_ERR_UNSUPPORTED, "aok_evaluate_pullback_noalloc: device id");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        st = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(noalloc scratch)");
+        if (st != AOK_OK) return st;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = (unsigned char*)g_noalloc_ptr[dev];
+    return AOK_OK;
+}
+
+}  // namespace aok
+
+extern "C" int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly, int64_t nOrb,
+                                             const int64_t* iR, const int64_t* iY, int64_t L, int radial_kind,
+                                             int precision, void* dX, void* dzeta, void* dD, const void* dP,
+                                             const void* X, const int64_t* sidx, const void* zeta, const void* D,
+                                             int64_t nX, double lengthscale, void* stream) {
+    using namespace aok;
+    const char* who = "aok_evaluate_pullback_noalloc";
+    if (!poly || !iR || !iY) return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    if (nRad <= 0 || K <= 0 || NZ <= 0 || nOrb <= 0 || L < 0 || nX < 0)
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": sizes must be positive");
+    if (L > kEvalMaxL) return set_error(AOK_ERR_UNSUPPORTED, std::string(who) + ": harmonics above l = 4");
+    if (radial_kind != AOK_RADIAL_GAUSSIAN && radial_kind != AOK_RADIAL_SLATER)
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": unknown radial kind");
+    if (precision != AOK_PREC_F64 && precision != AOK_PREC_F32C)
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": unknown precision");
+    if ((dzeta == nullptr) != (dD == nullptr))
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": dzeta and dD must both be given or both null");
+    if (nRad > kNoAllocMaxRad || nOrb > kNoAllocMaxOrb)
+        return set_error(AOK_ERR_UNSUPPORTED, std::string(who) + ": more than 64 radials or 256 orbitals");
+    const int64_t nY = (L + 1) * (L + 1);
+    NoAllocMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    maps.nRad = (int)nRad;
+    maps.nOrb = (int)nOrb;
+    for (int64_t k = 0; k < nRad; ++k) {
+        if (poly[k] < 0 || poly[k] > 64) return set_error(AOK_ERR_INVALID, std::string(who) + ": bad radial power");
+        maps.poly[k] = (int)poly[k];
+    }
+    for (int64_t i = 0; i < nOrb; ++i) {
+        if (iR[i] < 1 || iR[i] > nRad || iY[i] < 1 || iY[i] > nY)
+            return set_error(AOK_ERR_INVALID, std::string(who) + ": orbital index map out of range");
+        maps.iR[i] = (int)(iR[i] - 1);
+        maps.iY[i] = (int)(iY[i] - 1);
+    }
+    const int64_t ntab = nRad * K * NZ;
+    const int64_t grid = (nX + kEvalThreads - 1) / kEvalThreads;
+    const size_t need = kNoAllocRowsOffset + sizeof(double) * 2 * (size_t)ntab * (size_t)grid;
+    if (need > kNoAllocScratchBytes)
+        return set_error(AOK_ERR_UNSUPPORTED,
+                         std::string(who) + ": nX = " + std::to_string(nX) + " needs " + std::to_string(need) +
+                             " bytes of scratch; the static scratch holds " +
+                             std::to_string(kNoAllocScratchBytes) + " (use aok_evaluate_pullback)");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t fsz = precision == AOK_PREC_F64 ? 8 : 4;
+    if (nX == 0) {
+        if (dzeta) {
+            int st = cuda_status(cudaMemsetAsync(dzeta, 0, fsz * ntab, s), "memset");
+            if (st) return st;
+            return cuda_status(cudaMemsetAsync(dD, 0, fsz * ntab, s), "memset");
+        }
+        return AOK_OK;
+    }
+    if (!dP || !X || !sidx || !zeta || !D) return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    unsigned char* scratch = nullptr;
+    int st = noalloc_scratch(&scratch);
+    if (st != AOK_OK) return st;
+    // a plan-shaped descriptor on the stack whose tables point into the scratch
+    aok_orbitals o;
+    o.nRad = nRad;
+    o.K = K;
+    o.NZ = NZ;
+    o.nOrb = nOrb;
+    o.L = (int)L;
+    o.radial = radial_kind;
+    o.prec = precision;
+    int* mp = reinterpret_cast<int*>(scratch + kNoAllocMapsOffset);
+    o.d_poly = mp;
+    o.d_iR = mp + kNoAllocMaxRad;
+    o.d_iY = mp + kNoAllocMaxRad + kNoAllocMaxOrb;
+    o.d_err = reinterpret_cast<int*>(scratch);
+    if (eval_smem_bytes(&o, true) > 227 * 1024)
+        return set_error(AOK_ERR_UNSUPPORTED, std::string(who) + ": basis too large for shared memory");
+    k_noalloc_setup<<<1, 256, 0, s>>>(maps, scratch);
+    st = cuda_status(cudaGetLastError(), "k_noalloc_setup");
+    if (st != AOK_OK) return st;
+    EvalParams P;
+    fill_params(&o, P, X, sidx, zeta, D, nX, lengthscale);
+    P.dPin = dP;
+    P.dX = dX;
+    P.rows = dzeta ? reinterpret_cast<double*>(scratch + kNoAllocRowsOffset) : nullptr;
+    st = precision == AOK_PREC_F64 ? launch_eval_T<double>(&o, P, true, true, s)
+                                   : launch_eval_T<float>(&o, P, true, true, s);
+    if (st != AOK_OK || !P.rows) return st;
+    if (precision == AOK_PREC_F64)
+        k_eval_reduce<double><<<(int)((2 * ntab + 127) / 128), 128, 0, s>>>((double*)dD, (double*)dzeta, P.rows,
+                                                                          (int)grid, (int)ntab);
+    else
+        k_eval_reduce<float><<<(int)((2 * ntab + 127) / 128), 128, 0, s>>>((float*)dD, (float*)dzeta, P.rows,
+                                                                         (int)grid, (int)ntab);
+    return cuda_status(cudaGetLastError(), "k_eval_reduce");
+}

@@ -193,6 +193,32 @@ int aok_evaluate_pullback(aok_orbitals* orb, void* dX, void* dzeta, void* dD,
                           const void* zeta, const void* D, int64_t nX, double lengthscale,
                           void* stream);
 
+/*
+ * Allocation-free variant of aok_evaluate_pullback.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they need the pullback -- a host framework that owns the whole device
+ * through its own pooling allocator, or a service that reserves its memory at
+ * start-up and must not grow afterwards.  It takes the orbital description by
+ * value (host arrays poly[nRad], iR[nOrb], iY[nOrb], 1-based maps as in
+ * aok_orbitals_create) instead of a plan, and allocates nothing: its scratch
+ * (index maps, error word, per-block FP64 partial rows) is one static device
+ * array of AOK_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps
+ * until the process exits.  Limits: nRad <= 64, nOrb <= 256, and
+ * 4096 + 16 * nRad*K*NZ * ceil(nX / 128) bytes must fit the scratch; larger
+ * requests return AOK_ERR_UNSUPPORTED with the sizes in the message.  The
+ * first call on a device looks up the array's device address (make it before
+ * any stream capture).  All calls share the array and overwrite it, so calls
+ * that may overlap on the GPU race and must be serialised by the caller.
+ * Arguments and results otherwise as aok_evaluate_pullback.
+ */
+#define AOK_NOALLOC_SCRATCH_BYTES (8u << 20)
+int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly,
+                                  int64_t nOrb, const int64_t* iR, const int64_t* iY, int64_t L,
+                                  int radial_kind, int precision, void* dX, void* dzeta,
+                                  void* dD, const void* dP, const void* X, const int64_t* sidx,
+                                  const void* zeta, const void* D, int64_t nX,
+                                  double lengthscale, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
