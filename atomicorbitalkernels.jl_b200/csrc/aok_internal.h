@@ -54,11 +54,14 @@ struct aok_plan {
     void* d_coef_scratch = nullptr;  // ns*K*NZ
     void* d_dcoef_scratch = nullptr; // ns*K*NZ
     void* d_dalpha_scratch = nullptr;
-    // 3C schedule
+    // 3C schedule (overlap3c.cu)
     void* d_pp3 = nullptr;
     int* d_npp3 = nullptr;
-    aok::Item* d_items3 = nullptr;
+    void* d_items3 = nullptr;
     int nitems3 = 0;
+    alignas(8) unsigned char panels3_raw[160] = {};
+    size_t slab_stride3 = 0;
+    size_t smem3 = 0;
     // optional event pairs around the dominant kernel (measurement aid)
     std::vector<cudaEvent_t> ev;
     int ev_used = 0;
@@ -125,6 +128,8 @@ int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, 
 int setup_overlap3c_schedule(aok_plan* p);
 int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC,
                      int64_t B, cudaStream_t s);
+int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s);
+int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s);
 
 // orbitals.cu
 int launch_evaluate(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx,

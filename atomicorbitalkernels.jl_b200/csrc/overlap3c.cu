@@ -1,0 +1,191 @@
+// overlap3c.cu -- 3-center overlap host side: primitive-triple records, the
+// page-panel schedule, and the aok_overlap3c_gb entry point.  The kernel is in
+// overlap3c_kernel.cuh (one instantiation per precision: overlap3c_f32.cu,
+// overlap3c_f64.cu).
+#include <algorithm>
+#include <vector>
+
+#include "overlap3c_kernel.cuh"
+
+namespace aok {
+
+__device__ __forceinline__ void fill_pt(PTf& r, double ca, double cb, double cc, double a, double b, double c, int grp) {
+    const double q = a + b + c, x = 3.14159265358979323846 / q, l2e = 1.4426950408889634074;
+    const double kab = a * b / q * l2e, kac = a * c / q * l2e, kbc = b * c / q * l2e;
+    r.w = (float)(ca * cb * cc * (x * sqrt(x)));
+    r.kab_hi = (float)kab;
+    r.kab_lo = (float)(kab - (double)r.kab_hi);
+    r.kac_hi = (float)kac;
+    r.kac_lo = (float)(kac - (double)r.kac_hi);
+    r.kbc_hi = (float)kbc;
+    r.kbc_lo = (float)(kbc - (double)r.kbc_hi);
+    r.ra = (float)(a / q);
+    r.rb = (float)(b / q);
+    r.rc = (float)(c / q);
+    r.oo2q = (float)(0.5 / q);
+    r.grp = (float)grp;
+}
+__device__ __forceinline__ void fill_pt(PTd& r, double ca, double cb, double cc, double a, double b, double c, int) {
+    const double q = a + b + c, x = 3.14159265358979323846 / q;
+    r.w = ca * cb * cc * (x * sqrt(x));
+    r.kab = a * b / q;
+    r.kac = a * c / q;
+    r.kbc = b * c / q;
+    r.ra = a / q;
+    r.rb = b / q;
+    r.rc = c / q;
+    r.oo2q = 0.5 / q;
+}
+
+// One warp per shell triple; lanes sweep the K^3 grid in (ip, jp, kp) order
+// and compact the non-zero-coefficient triples (ballot), preserving order.
+template <typename FT>
+__global__ void k_prep3c(typename PTT<FT>::type* __restrict__ pp, int* __restrict__ npp, const FT* __restrict__ zeta,
+                         const FT* __restrict__ coef, int ns, int K) {
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (q >= ns * ns * ns) return;
+    const int sc = q % ns, sb = (q / ns) % ns, sa = q / (ns * ns);
+    auto* out = pp + (size_t)q * K * K * K;
+    int n = 0;
+    const int K3 = K * K * K;
+    for (int e0 = 0; e0 < K3; e0 += 32) {
+        const int e = e0 + lane;
+        const int ip = e / (K * K), jp = (e / K) % K, kp = e % K;
+        double ca = 0, cb = 0, cc = 0, a = 1, b = 1, c = 1;
+        if (e < K3) {
+            ca = (double)coef[sa + ns * ip];
+            cb = (double)coef[sb + ns * jp];
+            cc = (double)coef[sc + ns * kp];
+            a = (double)zeta[sa + ns * ip];
+            b = (double)zeta[sb + ns * jp];
+            c = (double)zeta[sc + ns * kp];
+        }
+        const bool valid = e < K3 && ca != 0.0 && cb != 0.0 && cc != 0.0;
+        const unsigned m = __ballot_sync(0xffffffffu, valid);
+        if (valid) fill_pt(out[n + __popc(m & ((1u << lane) - 1u))], ca, cb, cc, a, b, c, ip * K + jp);
+        n += __popc(m);
+    }
+    if (lane == 0) npp[q] = n;
+}
+
+int setup_overlap3c_schedule(aok_plan* p) {
+    if (p->d_items3) return AOK_OK;
+    if (p->NZ != 1) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: plan must have NZ = 1");
+    if (p->Lmax > kMaxL3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: shells above l = 2");
+    const int ns = (int)p->ns, N = (int)p->N;
+    const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
+    const size_t N2 = (size_t)N * N;
+    const size_t budget = 200 * 1024;
+    auto stride_for = [&](int pages) {
+        size_t s = N2 * pages;
+        if (s % 2 == 0) s += 1;
+        return s;
+    };
+    int maxpages = 0;
+    while (maxpages < N && stride_for(maxpages + 1) * kTileB * fsz <= budget) ++maxpages;
+    if (maxpages == 0) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: one output page exceeds the slab");
+    // panels: whole shells where they fit, otherwise page ranges of one shell
+    std::vector<int> pg{0};
+    int cur = 0;
+    for (int s = 0; s < ns; ++s) {
+        const int np = ncart((int)p->ls[s]);
+        if (cur > 0 && cur + np > maxpages) {
+            pg.push_back(pg.back() + cur);
+            cur = 0;
+        }
+        int left = np;
+        while (left > maxpages) {
+            pg.push_back(pg.back() + cur + maxpages);
+            left -= maxpages;
+            cur = 0;
+        }
+        cur += left;
+    }
+    pg.push_back(pg.back() + cur);
+    const int npan = (int)pg.size() - 1;
+    if (npan > kMaxPanels) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: basis too large for the panels");
+    Panels3 pan{};
+    pan.n = npan;
+    std::vector<Item3> items;
+    for (int pn = 0; pn < npan; ++pn) {
+        pan.page0[pn] = pg[pn];
+        pan.item0[pn] = (int)items.size();
+        std::vector<std::pair<int, Item3>> v;
+        for (int sc = 0; sc < ns; ++sc) {
+            const int k0 = (int)p->boff[sc], k1 = (int)p->boff[sc + 1];
+            if (k1 <= pg[pn] || k0 >= pg[pn + 1]) continue;
+            for (int sa = 0; sa < ns; ++sa)
+                for (int sb = 0; sb < ns; ++sb) {
+                    const int la = (int)p->ls[sa], lb = (int)p->ls[sb], lc = (int)p->ls[sc];
+                    const int ppc = pages_per_chunk3(la, lb), nch = nchunks3(la, lb, lc);
+                    for (int c = 0; c < nch; ++c) {
+                        const int c0 = k0 + c * ppc, c1 = std::min(k0 + (c + 1) * ppc, k1);
+                        if (c1 <= pg[pn] || c0 >= pg[pn + 1]) continue;
+                        const int cost = (la + 1) * (lb + 1) * (lc + 1) * 12 + 2 * ncart(la) * ncart(lb) * (c1 - c0);
+                        v.push_back({cost, Item3{(int16_t)(la * 9 + lb * 3 + lc), (int16_t)c, (int16_t)sa,
+                                                 (int16_t)sb, (int16_t)sc, 0}});
+                    }
+                }
+        }
+        std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        for (auto& x : v) items.push_back(x.second);
+    }
+    pan.page0[npan] = pg[npan];
+    pan.item0[npan] = (int)items.size();
+    static_assert(sizeof(Panels3) <= sizeof(p->panels3_raw), "panels3 storage");
+    memcpy(p->panels3_raw, &pan, sizeof(Panels3));
+    size_t maxw = 0;
+    for (int i = 0; i < npan; ++i) maxw = std::max(maxw, (size_t)(pg[i + 1] - pg[i]));
+    p->slab_stride3 = stride_for((int)maxw);
+    p->smem3 = p->slab_stride3 * kTileB * fsz;
+    p->nitems3 = (int)items.size();
+    const size_t nrec = (size_t)ns * ns * ns * p->K * p->K * p->K;
+    const size_t rec = p->prec == AOK_PREC_F64 ? sizeof(PTd) : sizeof(PTf);
+    cudaError_t e;
+    if ((e = cudaMalloc(&p->d_items3, sizeof(Item3) * items.size())) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(items3)");
+    if ((e = cudaMemcpy(p->d_items3, items.data(), sizeof(Item3) * items.size(), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return cuda_status(e, "cudaMemcpy(items3)");
+    if ((e = cudaMalloc(&p->d_pp3, nrec * rec)) != cudaSuccess) return cuda_status(e, "cudaMalloc(pp3)");
+    if ((e = cudaMalloc(&p->d_npp3, sizeof(int) * (size_t)ns * ns * ns)) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(npp3)");
+    return AOK_OK;
+}
+
+int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
+                     cudaStream_t s) {
+    (void)B;
+    const int n = (int)(p->ns * p->ns * p->ns), th = 128, bl = (n * 32 + th - 1) / th;
+    if (p->prec == AOK_PREC_F64)
+        k_prep3c<double><<<bl, th, 0, s>>>((PTd*)p->d_pp3, p->d_npp3, (const double*)p->d_gb_zeta,
+                                           (const double*)p->d_gb_coef, (int)p->ns, (int)p->K);
+    else
+        k_prep3c<float><<<bl, th, 0, s>>>((PTf*)p->d_pp3, p->d_npp3, (const float*)p->d_gb_zeta,
+                                          (const float*)p->d_gb_coef, (int)p->ns, (int)p->K);
+    int st = cuda_status(cudaGetLastError(), "k_prep3c");
+    if (st != AOK_OK) return st;
+    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, s);
+    return launch_ov3_f32(p, out, posA, posB, posC, s);
+}
+
+}  // namespace aok
+
+using namespace aok;
+
+extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, const int64_t* prim_offset,
+                                const void* coef, const void* alpha, const void* posA, const void* posB,
+                                const void* posC, int64_t B, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: null plan");
+    if (B < 0) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: negative batch");
+    if (B > p->max_batch) return set_error(AOK_ERR_LENGTH, "aok_overlap3c_gb: batch exceeds the plan's max_batch");
+    int st = setup_overlap3c_schedule(p);
+    if (st != AOK_OK) return st;
+    if (B == 0) return AOK_OK;
+    if (!out || !nprim || !prim_offset || !coef || !alpha || !posA || !posB || !posC)
+        return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    if ((st = launch_gb_pad(p, nprim, prim_offset, coef, alpha, s)) != AOK_OK) return st;
+    if ((st = launch_bin(p, nullptr, nullptr, B, s)) != AOK_OK) return st;
+    return launch_overlap3c(p, out, posA, posB, posC, B, s);
+}

@@ -1,0 +1,10 @@
+// overlap3c_f32.cu -- float instantiation of the 3-center overlap kernel.
+#include "overlap3c_kernel.cuh"
+
+namespace aok {
+
+int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s) {
+    return launch_ov3<float>(p, out, posA, posB, posC, s);
+}
+
+}  // namespace aok

@@ -1,0 +1,415 @@
+// overlap3c_kernel.cuh -- batched 3-center overlap kernel, templated on the
+// element type (instantiated in overlap3c_f32.cu / overlap3c_f64.cu).
+//
+// Replaces batch_V_kernel! (src/integrals/kernels_3c.jl:12-162):
+//   V_{mu nu lambda}(b) = int phi_mu(r - A_b) phi_nu(r - B_b) phi_lambda(r - C_b) dr.
+// Per primitive triple the three Gaussians combine at Q = (aA + bB + cC)/q
+// with prefactor c_a c_b c_c (pi/q)^{3/2} exp(-(ab|AB|^2 + ac|AC|^2 + bc|BC|^2)/q)
+// (the reference's mu|AB|^2 + nu|PC|^2), and the 1-D factors are the t = 0
+// three-index coefficients, built with the Obara-Saika form
+//   E[i+1][j][k] = QA E + (i E[i-1][j][k] + j E[i][j-1][k] + k E[i][j][k-1]) / 2q
+// and its j / k analogues (QB, QC); QA = -(b AB + c AC)/q, QB = (a AB - c BC)/q,
+// QC = (a AC + b BC)/q are formed directly.  The reference's aliased layout
+// lin = c1 + (2la+1) c2 + (2la+1)(2lb+1) c3 (kernels_3c.jl:146-160) is
+// reproduced at compile time.
+//
+// Same execution model as the 2C kernel: tiles of 32 batch elements (lane =
+// element), a persistent CTA per SM, shell-triple classes (la, lb, lc <= 2)
+// compile-time specialised, work items drained from a per-tile shared-memory
+// counter, results staged per output-page panel in shared memory and written
+// out coalesced (a batch element's (N,N,N) slab is contiguous).  Items are
+// whole shell-triple blocks or chunks of whole output pages; a chunk whose
+// pages straddle a panel boundary is computed in each panel it touches and
+// stores only the pages inside the current panel.
+#pragma once
+
+#include <cstring>
+
+#include "aok_internal.h"
+
+namespace aok {
+
+constexpr int kMaxL3 = 2;
+constexpr int kThreads3 = 256;
+
+__host__ __device__ constexpr int pages_per_chunk3(int la, int lb) {
+    return (ncart(la) * ncart(lb)) >= 36 ? 1 : 36 / (ncart(la) * ncart(lb));
+}
+__host__ __device__ constexpr int nchunks3(int la, int lb, int lc) {
+    return (ncart(lc) + pages_per_chunk3(la, lb) - 1) / pages_per_chunk3(la, lb);
+}
+
+// Geometry-free primitive-triple record (FP64-computed).  FP32: exponent
+// coefficients k_xy = (x y / q) log2(e) as hi + lo; `grp` = ip*K + jp (the
+// partial sums are folded with TwoSum whenever it changes).
+struct PTf {
+    float w, kab_hi, kab_lo, kac_hi, kac_lo, kbc_hi, kbc_lo, ra, rb, rc, oo2q, grp, pad[4];
+};
+struct PTd {
+    double w, kab, kac, kbc, ra, rb, rc, oo2q;
+};
+template <typename FT> struct PTT;
+template <> struct PTT<float> { using type = PTf; };
+template <> struct PTT<double> { using type = PTd; };
+
+struct Item3 {
+    int16_t cls;    // la*9 + lb*3 + lc
+    int16_t chunk;
+    int16_t sa, sb, sc, pad;
+};
+
+struct Panels3 {
+    int n;
+    int page0[kMaxPanels + 1];   // global output page (k index) range of each panel
+    int item0[kMaxPanels + 1];
+};
+
+template <typename FT> struct Geo3;
+template <> struct Geo3<float> {
+    float AB[3], AC[3], BC[3];
+    float R2[3], R2lo[3];  // |AB|^2, |AC|^2, |BC|^2 as hi + lo
+};
+template <> struct Geo3<double> {
+    double AB[3], AC[3], BC[3];
+    double R2[3];
+};
+
+__device__ __forceinline__ void load_geo3(Geo3<float>& g, const float* A, const float* B, const float* C) {
+    double r[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double ab = (double)A[c] - (double)B[c], ac = (double)A[c] - (double)C[c],
+                     bc = (double)B[c] - (double)C[c];  // exact differences of FP32 values
+        g.AB[c] = (float)ab;
+        g.AC[c] = (float)ac;
+        g.BC[c] = (float)bc;
+        r[0] += ab * ab;
+        r[1] += ac * ac;
+        r[2] += bc * bc;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        g.R2[i] = (float)r[i];
+        g.R2lo[i] = (float)(r[i] - (double)g.R2[i]);
+    }
+}
+__device__ __forceinline__ void load_geo3(Geo3<double>& g, const double* A, const double* B, const double* C) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g.R2[i] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        g.AB[c] = A[c] - B[c];
+        g.AC[c] = A[c] - C[c];
+        g.BC[c] = B[c] - C[c];
+        g.R2[0] += g.AB[c] * g.AB[c];
+        g.R2[1] += g.AC[c] * g.AC[c];
+        g.R2[2] += g.BC[c] * g.BC[c];
+    }
+}
+
+// E[i][j][k] for i <= LA, j <= LB, k <= LC, seeded with E[0][0][0] = e000.
+template <int LA, int LB, int LC, typename FT>
+__device__ __forceinline__ void build_E3(FT (&E)[LA + 1][LB + 1][LC + 1], FT QA, FT QB, FT QC, FT o2q, FT e000) {
+    E[0][0][0] = e000;
+#pragma unroll
+    for (int k = 0; k <= LC; ++k)
+#pragma unroll
+        for (int j = 0; j <= LB; ++j)
+#pragma unroll
+            for (int i = 0; i <= LA; ++i) {
+                if (i == 0 && j == 0 && k == 0) continue;
+                // raise the first non-zero index from its predecessor
+                FT v;
+                if (k > 0 && i == 0 && j == 0) {
+                    v = QC * E[0][0][k - 1];
+                    if (k >= 2) v += (FT(k - 1) * o2q) * E[0][0][k - 2];
+                } else if (i == 0) {
+                    v = QB * E[0][j - 1][k];
+                    FT c = FT(0);
+                    if (j >= 2) c += FT(j - 1) * E[0][j - 2][k];
+                    if (k >= 1) c += FT(k) * E[0][j - 1][k - 1];
+                    v += o2q * c;
+                } else {
+                    v = QA * E[i - 1][j][k];
+                    FT c = FT(0);
+                    if (i >= 2) c += FT(i - 1) * E[i - 2][j][k];
+                    if (j >= 1) c += FT(j) * E[i - 1][j - 1][k];
+                    if (k >= 1) c += FT(k) * E[i - 1][j][k - 1];
+                    v += o2q * c;
+                }
+                E[i][j][k] = v;
+            }
+}
+
+template <int LA, int LB, int LC>
+struct Class3 {
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC);
+    static constexpr int PS = NA * NB;            // elements per output page of the block
+    static constexpr int NE = PS * NC;
+    static constexpr int N1 = 2 * LA + 1, N2 = 2 * LB + 1;
+    static constexpr int PPC = pages_per_chunk3(LA, LB);
+};
+
+// lin (0-based, within the block) -> offset in the lane's panel slab;
+// block element (i, j, k) = (lin % NA, (lin / NA) % NB, lin / PS).
+// Only pages inside [kp0, kp1) (block-local) are stored.
+template <int LA, int LB, int LC, int C>
+__device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const Geo3<float> g, float* dst, int N,
+                                       int kp0, int kp1) {
+    using CI = Class3<LA, LB, LC>;
+    constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
+    constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
+    float hi[M], part[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        hi[m] = 0.f;
+        part[m] = 0.f;
+    }
+    float lo[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) lo[m] = 0.f;
+    float prev = -1.f;
+    for (int q = 0; q < n; ++q) {
+        const float4 r0 = __ldg(reinterpret_cast<const float4*>(pp + q));
+        const float4 r1 = __ldg(reinterpret_cast<const float4*>(pp + q) + 1);
+        const float4 r2 = __ldg(reinterpret_cast<const float4*>(pp + q) + 2);
+        const float w = r0.x;
+        if (r2.w != prev) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                float s, e;
+                two_sum(hi[m], part[m], s, e);
+                hi[m] = s;
+                part[m] = 0.f;
+                lo[m] += e;
+            }
+            prev = r2.w;
+        }
+        // exponent x = (k_ab |AB|^2 + k_ac |AC|^2 + k_bc |BC|^2) log2(e), double-float
+        const float xa = r0.y * g.R2[0], xb = r0.w * g.R2[1], xc = r1.y * g.R2[2];
+        float s1, e1, xh, e2;
+        two_sum(xa, xb, s1, e1);
+        two_sum(s1, xc, xh, e2);
+        const float xl = (fmaf(r0.y, g.R2[0], -xa) + fmaf(r0.w, g.R2[1], -xb) + fmaf(r1.y, g.R2[2], -xc)) +
+                         ((r0.z * g.R2[0] + r0.y * g.R2lo[0]) + (r1.x * g.R2[1] + r0.w * g.R2lo[1]) +
+                          (r1.z * g.R2[2] + r1.y * g.R2lo[2])) +
+                         (e1 + e2);
+        const float e000 = (exp2f(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
+        const float ra = r1.w, rb = r2.x, rc = r2.y, o2q = r2.z;
+        float Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
+        build_E3<LA, LB, LC, float>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
+                                    ra * g.AC[0] + rb * g.BC[0], o2q, e000);
+        build_E3<LA, LB, LC, float>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
+                                    ra * g.AC[1] + rb * g.BC[1], o2q, 1.f);
+        build_E3<LA, LB, LC, float>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
+                                    ra * g.AC[2] + rb * g.BC[2], o2q, 1.f);
+#pragma unroll
+        for (int c3 = 0; c3 < CI::NC; ++c3)
+#pragma unroll
+            for (int c2 = 0; c2 < CI::NB; ++c2)
+#pragma unroll
+                for (int c1 = 0; c1 < CI::NA; ++c1) {
+                    const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
+                    if (lin >= L0 && lin < L0 + M) {
+                        const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
+                                         Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
+                        part[lin - L0] =
+                            fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
+                    }
+                }
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int lin = L0 + m, pg = lin / CI::PS;
+        if (pg >= kp0 && pg < kp1) {
+            float s, e;
+            two_sum(hi[m], part[m], s, e);
+            const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
+            dst[(size_t)(pg - kp0) * N * N + (size_t)j * N + i] = s + (lo[m] + e);
+        }
+    }
+}
+
+template <int LA, int LB, int LC, int C>
+__device__ __noinline__ void run_item3(const PTd* __restrict__ pp, int n, const Geo3<double> g, double* dst, int N,
+                                       int kp0, int kp1) {
+    using CI = Class3<LA, LB, LC>;
+    constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
+    constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
+    double acc[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    for (int q = 0; q < n; ++q) {
+        const double2 r0 = __ldg(reinterpret_cast<const double2*>(pp + q));
+        const double2 r1 = __ldg(reinterpret_cast<const double2*>(pp + q) + 1);
+        const double2 r2 = __ldg(reinterpret_cast<const double2*>(pp + q) + 2);
+        const double2 r3 = __ldg(reinterpret_cast<const double2*>(pp + q) + 3);
+        const double w = r0.x, kab = r0.y, kac = r1.x, kbc = r1.y, ra = r2.x, rb = r2.y, rc = r3.x, o2q = r3.y;
+        const double e000 = exp(-(kab * g.R2[0] + kac * g.R2[1] + kbc * g.R2[2])) * w;
+        double Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
+        build_E3<LA, LB, LC, double>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
+                                     ra * g.AC[0] + rb * g.BC[0], o2q, e000);
+        build_E3<LA, LB, LC, double>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
+                                     ra * g.AC[1] + rb * g.BC[1], o2q, 1.0);
+        build_E3<LA, LB, LC, double>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
+                                     ra * g.AC[2] + rb * g.BC[2], o2q, 1.0);
+#pragma unroll
+        for (int c3 = 0; c3 < CI::NC; ++c3)
+#pragma unroll
+            for (int c2 = 0; c2 < CI::NB; ++c2)
+#pragma unroll
+                for (int c1 = 0; c1 < CI::NA; ++c1) {
+                    const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
+                    if (lin >= L0 && lin < L0 + M) {
+                        const double yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
+                                          Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
+                        acc[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, acc[lin - L0]);
+                    }
+                }
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const int lin = L0 + m, pg = lin / CI::PS;
+        if (pg >= kp0 && pg < kp1) {
+            const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
+            dst[(size_t)(pg - kp0) * N * N + (size_t)j * N + i] = acc[m];
+        }
+    }
+}
+
+template <typename PT, typename FT, int LA, int LB, int LC>
+__device__ __forceinline__ void run_chunks3(int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N, int kp0,
+                                            int kp1) {
+    constexpr int NCH = nchunks3(LA, LB, LC);
+    switch (chunk) {
+        case 0: run_item3<LA, LB, LC, 0>(pp, n, g, dst, N, kp0, kp1); break;
+        case 1: if constexpr (NCH > 1) run_item3<LA, LB, LC, 1>(pp, n, g, dst, N, kp0, kp1); break;
+        case 2: if constexpr (NCH > 2) run_item3<LA, LB, LC, 2>(pp, n, g, dst, N, kp0, kp1); break;
+        case 3: if constexpr (NCH > 3) run_item3<LA, LB, LC, 3>(pp, n, g, dst, N, kp0, kp1); break;
+        case 4: if constexpr (NCH > 4) run_item3<LA, LB, LC, 4>(pp, n, g, dst, N, kp0, kp1); break;
+        case 5: if constexpr (NCH > 5) run_item3<LA, LB, LC, 5>(pp, n, g, dst, N, kp0, kp1); break;
+        default: break;
+    }
+}
+
+template <typename PT, typename FT>
+__device__ __forceinline__ void dispatch3(int cls, int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N,
+                                          int kp0, int kp1) {
+    switch (cls) {
+#define AOK_C3(LA, LB, LC) \
+    case (LA) * 9 + (LB) * 3 + (LC): run_chunks3<PT, FT, LA, LB, LC>(chunk, pp, n, g, dst, N, kp0, kp1); break;
+        AOK_C3(0, 0, 0) AOK_C3(0, 0, 1) AOK_C3(0, 0, 2) AOK_C3(0, 1, 0) AOK_C3(0, 1, 1) AOK_C3(0, 1, 2)
+        AOK_C3(0, 2, 0) AOK_C3(0, 2, 1) AOK_C3(0, 2, 2) AOK_C3(1, 0, 0) AOK_C3(1, 0, 1) AOK_C3(1, 0, 2)
+        AOK_C3(1, 1, 0) AOK_C3(1, 1, 1) AOK_C3(1, 1, 2) AOK_C3(1, 2, 0) AOK_C3(1, 2, 1) AOK_C3(1, 2, 2)
+        AOK_C3(2, 0, 0) AOK_C3(2, 0, 1) AOK_C3(2, 0, 2) AOK_C3(2, 1, 0) AOK_C3(2, 1, 1) AOK_C3(2, 1, 2)
+        AOK_C3(2, 2, 0) AOK_C3(2, 2, 1) AOK_C3(2, 2, 2)
+#undef AOK_C3
+        default: break;
+    }
+}
+
+template <typename FT>
+struct Ov3Params {
+    FT* out;
+    const FT* posA;
+    const FT* posB;
+    const FT* posC;
+    const typename PTT<FT>::type* pp;
+    const int* npp;
+    const int* perm;
+    const int4* tiles;
+    const int* ntiles;
+    unsigned* counter;
+    const Item3* items;
+    Panels3 panels;
+    int ns, K, N, slab_stride;
+    int boff[kMaxShells + 1];
+};
+
+template <typename FT>
+__global__ void __launch_bounds__(kThreads3, 1) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FT* slab = reinterpret_cast<FT*>(smem_raw);
+    __shared__ int s_tile;
+    __shared__ int s_next[kMaxPanels];
+    constexpr int NW = kThreads3 / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ntiles = *P.ntiles;
+    const size_t N2 = (size_t)P.N * P.N;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_tile = (int)atomicAdd(P.counter, 1u);
+            for (int i = 0; i < P.panels.n; ++i) s_next[i] = 0;
+        }
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= ntiles) break;
+        const int4 td = P.tiles[tile];
+        const int start = td.y, cnt = td.z;
+        Geo3<FT> g;
+        {
+            const int b = lane < cnt ? P.perm[start + lane] : P.perm[start];
+            load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b);
+        }
+        FT* sl = slab + (size_t)lane * P.slab_stride;
+        for (int pn = 0; pn < P.panels.n; ++pn) {
+            const int pg0 = P.panels.page0[pn], pg1 = P.panels.page0[pn + 1];
+            const int i0 = P.panels.item0[pn], i1 = P.panels.item0[pn + 1];
+            for (;;) {
+                int it = 0;
+                if (lane == 0) it = atomicAdd(&s_next[pn], 1);
+                it = __shfl_sync(0xffffffffu, it, 0) + i0;
+                if (it >= i1) break;
+                const Item3 wi = P.items[it];
+                const int q = (wi.sa * P.ns + wi.sb) * P.ns + wi.sc;
+                const int n = __ldg(P.npp + q);
+                const int koff = P.boff[wi.sc];
+                // block-local page window of this panel, and the block's (0,0,first page) in the slab
+                const int kp0 = max(pg0 - koff, 0), kp1 = min(pg1 - koff, P.boff[wi.sc + 1] - koff);
+                FT* dst = sl + (size_t)(koff + kp0 - pg0) * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
+                dispatch3(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K * P.K, n, g, dst, P.N, kp0, kp1);
+            }
+            __syncthreads();
+            const size_t len = (size_t)(pg1 - pg0) * N2;
+            for (int bl = warp; bl < cnt; bl += NW) {
+                const int bg = P.perm[start + bl];
+                FT* o = P.out + (size_t)bg * N2 * P.N + (size_t)pg0 * N2;
+                const FT* s = slab + (size_t)bl * P.slab_stride;
+                for (size_t e = lane; e < len; e += 32) o[e] = s[e];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <typename FT>
+inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s) {
+    Ov3Params<FT> P;
+    memset(&P, 0, sizeof(P));
+    P.out = (FT*)out;
+    P.posA = (const FT*)posA;
+    P.posB = (const FT*)posB;
+    P.posC = (const FT*)posC;
+    P.pp = (const typename PTT<FT>::type*)p->d_pp3;
+    P.npp = p->d_npp3;
+    P.perm = p->d_perm;
+    P.tiles = p->d_tiles;
+    P.ntiles = p->d_ntiles;
+    P.counter = p->d_counter;
+    P.items = (const Item3*)p->d_items3;
+    memcpy(&P.panels, p->panels3_raw, sizeof(Panels3));
+    P.ns = (int)p->ns;
+    P.K = (int)p->K;
+    P.N = (int)p->N;
+    P.slab_stride = (int)p->slab_stride3;
+    for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
+    auto kern = k_overlap3c<FT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem3);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap3c)");
+    timing_begin(p, s);
+    kern<<<p->num_sms, kThreads3, p->smem3, s>>>(P);
+    timing_end(p, s);
+    return cuda_status(cudaGetLastError(), "k_overlap3c");
+}
+
+}  // namespace aok

@@ -237,7 +237,7 @@ def batch_overlap_3c_(out, bc, posA, posB, posC):
 
 
 def batch_overlap_3c(bc, posA, posB, posC, FT=torch.float64, device_out=False):
-    B = np.shape(posA.value)[1]
+    B = np.shape(posA.value if hasattr(posA, "value") else posA)[1]
     N = bc.nbf_total
     out = _dev.colmajor_empty((N, N, N, B), FT)
     batch_overlap_3c_(out, bc, posA, posB, posC)

@@ -1,0 +1,76 @@
+"""3-center overlap on the GPU vs the FP64 oracle and the quadrature golden
+vectors (through the C ABI)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import aok_b200 as aok
+import oracle
+from helpers import f32_round, rel_fro
+
+W = aok.workloads
+pytestmark = pytest.mark.gpu
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "overlap_golden.npz"))
+
+
+def _bc(b):
+    ls, nprim, z, D = W.gb_tables(b)
+    coef_full = oracle.compile_coef(b.zeta, b.D, b.ls)
+    coef = np.concatenate([coef_full[s, :nprim[s], 0] for s in range(len(ls))])
+    shells, o = [], 0
+    for s in range(len(ls)):
+        shells.append(aok.CartesianShell(int(ls[s]), coef[o:o + nprim[s]], z[o:o + nprim[s]]))
+        o += nprim[s]
+    return aok.compile_basis(shells), ls, nprim, coef, z
+
+
+def _L(p):
+    return aok.Length(p / aok.ang2bohr, "angstrom")
+
+
+@pytest.mark.parametrize("B", [1, 33, 600])
+def test_config4_f64(B):
+    b = W.config0_basis()
+    bc, ls, nprim, coef, z = _bc(b)
+    tr = W.config4_triples(B=B)
+    pA, pB, pC = _L(tr.posA), _L(tr.posB), _L(tr.posC)
+    V = aok.batch_overlap_3c(bc, pA, pB, pC)
+    ref = oracle.overlap3c_gb(ls, nprim, coef, z, aok.to_bohr(pA), aok.to_bohr(pB), aok.to_bohr(pC), nthreads=8)
+    assert V.shape == (15, 15, 15, B)
+    assert rel_fro(V, ref) < 1e-12
+
+
+def test_config4_f32c():
+    b = W.config0_basis()
+    bc, ls, nprim, coef, z = _bc(b)
+    tr = W.config4_triples(B=1024)
+    pA, pB, pC = _L(tr.posA), _L(tr.posB), _L(tr.posC)
+    V = aok.batch_overlap_3c(bc, pA, pB, pC, FT=torch.float32)
+    ref = oracle.overlap3c_gb(ls, nprim, f32_round(coef), f32_round(z), f32_round(aok.to_bohr(pA, np.float32)),
+                              f32_round(aok.to_bohr(pB, np.float32)), f32_round(aok.to_bohr(pC, np.float32)),
+                              nthreads=8)
+    assert V.dtype == torch.float32
+    assert rel_fro(V, ref) < 2e-6
+
+
+def test_golden_vectors_3c():
+    shells, o = [], 0
+    for s in range(len(G["ls3"])):
+        n = int(G["nprim3"][s])
+        shells.append(aok.CartesianShell(int(G["ls3"][s]), G["coef3"][o:o + n], G["alpha3"][o:o + n]))
+        o += n
+    bc = aok.compile_basis(shells)
+    V = aok.batch_overlap_3c(bc, _L(G["posA3"]), _L(G["posB3"]), _L(G["posC3"]))
+    assert np.max(np.abs(V.numpy() - G["V"])) < 1e-12
+
+
+def test_3c_rejects_f_shells_and_plain_positions():
+    bc = aok.compile_basis([aok.CartesianShell(3, np.array([1.0]), np.array([1.0]))])
+    p = aok.Length(np.zeros((3, 1)), "angstrom")
+    with pytest.raises(aok.AOKError):
+        aok.batch_overlap_3c(bc, p, p, p)
+    bc2 = aok.compile_basis([aok.CartesianShell(0, np.array([1.0]), np.array([1.0]))])
+    with pytest.raises(aok.ArgumentError):
+        aok.batch_overlap_3c(bc2, np.zeros((3, 1)), p, p)
