@@ -17,24 +17,14 @@ __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
 // Cartesian component c of a shell of momentum l, in the reference's order
 // (kernels_2c.jl:201-217): for x = l..0, for z = 0..l-x: (x, y = l-x-z, z).
-__host__ __device__ constexpr int cart_x(int l, int c) {
-    int idx = 0;
-    for (int x = l; x >= 0; --x)
-        for (int z = 0; z <= l - x; ++z) {
-            if (idx == c) return x;
-            ++idx;
-        }
-    return 0;
+// Closed form (no loops, so unrolled call sites fold instantly): with
+// n = l - x, the first component of that x is n(n+1)/2, so
+// n = #{t >= 1 : t(t+1)/2 <= c} and z = c - n(n+1)/2.
+__host__ __device__ constexpr int cart_n(int c) {
+    return (c >= 1) + (c >= 3) + (c >= 6) + (c >= 10) + (c >= 15) + (c >= 21);
 }
-__host__ __device__ constexpr int cart_z(int l, int c) {
-    int idx = 0;
-    for (int x = l; x >= 0; --x)
-        for (int z = 0; z <= l - x; ++z) {
-            if (idx == c) return z;
-            ++idx;
-        }
-    return 0;
-}
+__host__ __device__ constexpr int cart_x(int l, int c) { return l - cart_n(c); }
+__host__ __device__ constexpr int cart_z(int l, int c) { return c - cart_n(c) * (cart_n(c) + 1) / 2; }
 __host__ __device__ constexpr int cart_y(int l, int c) { return l - cart_x(l, c) - cart_z(l, c); }
 
 // Accumulator elements per work item (register budget); larger shell-pair
