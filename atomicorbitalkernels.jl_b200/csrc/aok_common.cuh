@@ -43,7 +43,7 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 // does not depend on the geometry, computed once per call in FP64.
 //   w    = c_a c_b (pi/p)^{3/2}
 //   mu   = a b / p (FP64 record); mu log2(e) as hi + lo (FP32 record)
-//   ra   = a/p,  rb = b/p,  oo2p = 1/(2p), flush = ip (primitive row index).
+//   ra   = a/p,  rb = b/p,  oo2p = 1/(2p), flush = row length (non-zero ket coefficients).
 struct PPf {
     float w, mu_hi, mu_lo, ra, rb, oo2p, flush, pad;
 };

@@ -102,8 +102,9 @@ __device__ __forceinline__ void fill_pp(PPd& r, double ca, double cb, double aa,
 // One warp per (species pair, shell pair); lanes sweep the K x K primitive
 // grid in ip-major order and compact the non-zero-coefficient pairs with a
 // ballot, preserving the reference's (ip, jp) summation order.  The record's
-// `flush` field carries ip (the kernel folds its FP32 partial sums whenever
-// ip changes).
+// `flush` field carries the row length (the number of non-zero ket
+// coefficients): the records form rows of equal length, one per ip, and the
+// kernel folds its FP32 partial sums after each row.
 template <typename FT>
 __global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restrict__ npp,
                          const FT* __restrict__ zeta, const FT* __restrict__ coef, int ns, int K, int NZ) {
@@ -117,6 +118,9 @@ __global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restric
     int gb = t % NZ, ga = t / NZ;
     auto* out = pp + (size_t)q * K * K;
     int n = 0;
+    // every row (ip with a non-zero coefficient) holds the same jp set
+    int nb = 0;
+    for (int jp = 0; jp < K; ++jp) nb += coef[sb + ns * (jp + K * gb)] != FT(0);
     for (int e0 = 0; e0 < K * K; e0 += 32) {
         const int e = e0 + lane;
         const int ip = e / K, jp = e % K;
@@ -132,7 +136,7 @@ __global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restric
         if (valid) {
             auto& r = out[n + __popc(m & ((1u << lane) - 1u))];
             fill_pp(r, ca, cb, aa, ab);
-            r.flush = (decltype(r.flush))ip;
+            r.flush = (decltype(r.flush))nb;
         }
         n += __popc(m);
     }
@@ -319,7 +323,8 @@ static double class_cost(int la, int lb, int elems) {
 int setup_overlap2c_schedule(aok_plan* p) {
     const int ns = (int)p->ns, N = (int)p->N;
     const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    const size_t budget = 100 * 1024;  // two CTAs per SM
+    // FP32: two CTAs per SM; FP64: one (leaves room for the per-warp record buffers)
+    const size_t budget = (p->prec == AOK_PREC_F64 ? 148 : 96) * 1024;
     // panels: consecutive ket shells whose column range fits the slab budget
     std::vector<int> pcols{0};
     std::vector<int> pshell{0};

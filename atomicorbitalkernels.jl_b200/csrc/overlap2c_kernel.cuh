@@ -102,12 +102,33 @@ struct ClassInfo {
 };
 
 // --------------------------------------------------------------------------
+// Shared-memory record access (the warp stages an item's records first).
+// --------------------------------------------------------------------------
+__device__ __forceinline__ float4 lds128(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ double2 lds128d(uint32_t a) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// --------------------------------------------------------------------------
 // One work item for one lane (batch element): FP32C.
+// rec: shared-memory address of the item's n records, ip-major in rows of
+// equal length (the number of non-zero ket coefficients, record field 6).
 // dst points at the block's (0,0) element inside this lane's slab; element
 // (i, j) of the block lives at dst[j*N + i].
 // --------------------------------------------------------------------------
 template <int LA, int LB, int C>
-__device__ __noinline__ void run_item(const PPf* __restrict__ pp, int n, const Geo<float> g, float* dst, int N) {
+__device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, float* dst, int N) {
     using CI = ClassInfo<LA, LB>;
     constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
     // hi/part in registers; the TwoSum rounding errors (lo) accumulate in this
@@ -119,87 +140,62 @@ __device__ __noinline__ void run_item(const PPf* __restrict__ pp, int n, const G
         part[m] = 0.f;
         dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] = 0.f;
     }
-    float prev_ip = 0.f;
-    // software pipeline: the next record is in flight while this one computes
-    float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
-    if (n > 0) {
-        n0 = __ldg(reinterpret_cast<const float4*>(pp));
-        n1 = __ldg(reinterpret_cast<const float4*>(pp) + 1);
-    }
-    for (int q = 0; q < n; ++q) {
-        const float4 r0 = n0, r1 = n1;
-        if (q + 1 < n) {
-            n0 = __ldg(reinterpret_cast<const float4*>(pp + q + 1));
-            n1 = __ldg(reinterpret_cast<const float4*>(pp + q + 1) + 1);
-        }
-        // mu2 = mu * log2(e) as hi + lo (FP64 on the host of the record)
-        const float w = r0.x, mu_hi = r0.y, mu_lo = r0.z, ra = r0.w, rb = r1.x, oo2p = r1.y, ip = r1.z;
-        if (ip != prev_ip) {
-            // fold the previous ip row's partial sums into (hi, lo)
+    const int rowlen = n > 0 ? (int)lds128(rec + 16).z : 1;
+    for (int q0 = 0; q0 < n; q0 += rowlen) {
+        for (int q = q0; q < q0 + rowlen; ++q) {
+            const float4 r0 = lds128(rec + 32u * q), r1 = lds128(rec + 32u * q + 16u);
+            // w, mu2 = mu log2(e) as hi + lo, a/p, b/p, 1/2p
+            const float w = r0.x, mu_hi = r0.y, mu_lo = r0.z, ra = r0.w, rb = r1.x, oo2p = r1.y;
+            // exp(-mu R^2) = 2^-(mu2 R^2), argument in double-float:
+            // 2^-(xh + xl) = 2^-xh (1 - ln2 xl) to first order in |xl| < 2^-20 xh
+            const float xh = mu_hi * g.R2;
+            const float xl = fmaf(mu_hi, g.R2, -xh) + fmaf(mu_lo, g.R2, mu_hi * g.R2lo);
+            const float e00 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
+            const float O[4] = {0.f, oo2p, 2.f * oo2p, 3.f * oo2p};
+            float Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
+            build_E<LA, LB, float>(Ex, -rb * g.AB[0], ra * g.AB[0], O, e00);
+            build_E<LA, LB, float>(Ey, -rb * g.AB[1], ra * g.AB[1], O, 1.f);
+            build_E<LA, LB, float>(Ez, -rb * g.AB[2], ra * g.AB[2], O, 1.f);
 #pragma unroll
-            for (int m = 0; m < M; ++m) {
-                float s, e;
-                two_sum(hi[m], part[m], s, e);
-                hi[m] = s;
-                part[m] = 0.f;
-                dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] += e;
-            }
-            prev_ip = ip;
-        }
-        // exp(-mu R^2) = 2^-(mu2 R^2) with the argument in double-float:
-        // 2^-(xh + xl) = 2^-xh (1 - ln2 xl) to first order in |xl| < 2^-20 xh
-        const float xh = mu_hi * g.R2;
-        const float xl = fmaf(mu_hi, g.R2, -xh) + fmaf(mu_lo, g.R2, mu_hi * g.R2lo);
-        const float e00 = (exp2f(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
-        const float O[4] = {0.f, oo2p, 2.f * oo2p, 3.f * oo2p};
-        float Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
-        build_E<LA, LB, float>(Ex, -rb * g.AB[0], ra * g.AB[0], O, e00);
-        build_E<LA, LB, float>(Ey, -rb * g.AB[1], ra * g.AB[1], O, 1.f);
-        build_E<LA, LB, float>(Ez, -rb * g.AB[2], ra * g.AB[2], O, 1.f);
+            for (int c2 = 0; c2 < CI::NB; ++c2)
 #pragma unroll
-        for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-            for (int c1 = 0; c1 < CI::NA; ++c1) {
-                const int lin = c1 + CI::N1 * c2;
-                if (lin >= L0 && lin < L1) {
-                    const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)] * Ez[cart_z(LA, c1)][cart_z(LB, c2)];
-                    part[lin - L0] = fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)], yz, part[lin - L0]);
+                for (int c1 = 0; c1 < CI::NA; ++c1) {
+                    const int lin = c1 + CI::N1 * c2;
+                    if (lin >= L0 && lin < L1) {
+                        const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)] * Ez[cart_z(LA, c1)][cart_z(LB, c2)];
+                        part[lin - L0] = fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)], yz, part[lin - L0]);
+                    }
                 }
-            }
+        }
+        // fold the ip row's partial sums into (hi, lo)
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            float s, e;
+            two_sum(hi[m], part[m], s, e);
+            hi[m] = s;
+            part[m] = 0.f;
+            dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] += e;
+        }
     }
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-        float s, e;
-        two_sum(hi[m], part[m], s, e);
         float* d = dst + ((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA;
-        *d = s + (*d + e);
+        *d = hi[m] + *d;
     }
 }
 
-// FP64 variant: plain double accumulation.
+// FP64 variant: plain double accumulation, records from shared memory.
 template <int LA, int LB, int C>
-__device__ __noinline__ void run_item(const PPd* __restrict__ pp, int n, const Geo<double> g, double* dst, int N) {
+__device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<double> g, double* dst, int N) {
     using CI = ClassInfo<LA, LB>;
     constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
     double acc[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) acc[m] = 0.0;
-    double2 n0 = make_double2(0.0, 0.0), n1 = n0;
-    double n2 = 0.0;
-    if (n > 0) {
-        n0 = __ldg(reinterpret_cast<const double2*>(pp));
-        n1 = __ldg(reinterpret_cast<const double2*>(pp) + 1);
-        n2 = __ldg(reinterpret_cast<const double*>(pp) + 4);
-    }
     for (int q = 0; q < n; ++q) {
-        const double2 r0 = n0, r1 = n1;
-        const double r2w = n2;
-        if (q + 1 < n) {
-            n0 = __ldg(reinterpret_cast<const double2*>(pp + q + 1));
-            n1 = __ldg(reinterpret_cast<const double2*>(pp + q + 1) + 1);
-            n2 = __ldg(reinterpret_cast<const double*>(pp + q + 1) + 4);
-        }
-        const double w = r0.x, mu = r0.y, ra = r1.x, rb = r1.y, oo2p = r2w;
+        const double2 r0 = lds128d(rec + 64u * q), r1 = lds128d(rec + 64u * q + 16u),
+                      r2 = lds128d(rec + 64u * q + 32u);
+        const double w = r0.x, mu = r0.y, ra = r1.x, rb = r1.y, oo2p = r2.x;
         const double e00 = exp(-mu * g.R2) * w;
         const double O[4] = {0.0, oo2p, 2.0 * oo2p, 3.0 * oo2p};
         double Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
@@ -221,8 +217,8 @@ __device__ __noinline__ void run_item(const PPd* __restrict__ pp, int n, const G
     for (int m = 0; m < M; ++m) dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] = acc[m];
 }
 
-template <typename PP, typename FT, int LA, int LB>
-__device__ __forceinline__ void run_chunks(int chunk, const PP* pp, int n, const Geo<FT>& g, FT* dst, int N) {
+template <typename FT, int LA, int LB>
+__device__ __forceinline__ void run_chunks(int chunk, uint32_t pp, int n, const Geo<FT>& g, FT* dst, int N) {
     constexpr int NCH = ClassInfo<LA, LB>::NCH;
     if constexpr (NCH == 1) {
         run_item<LA, LB, 0>(pp, n, g, dst, N);
@@ -237,11 +233,11 @@ __device__ __forceinline__ void run_chunks(int chunk, const PP* pp, int n, const
     }
 }
 
-template <typename PP, typename FT>
-__device__ __forceinline__ void dispatch(int cls, int chunk, const PP* pp, int n, const Geo<FT>& g, FT* dst, int N) {
+template <typename FT>
+__device__ __forceinline__ void dispatch(int cls, int chunk, uint32_t pp, int n, const Geo<FT>& g, FT* dst, int N) {
     switch (cls) {
 #define AOK_CASE(LA, LB) \
-    case (LA) * 4 + (LB): run_chunks<PP, FT, LA, LB>(chunk, pp, n, g, dst, N); break;
+    case (LA) * 4 + (LB): run_chunks<FT, LA, LB>(chunk, pp, n, g, dst, N); break;
         AOK_CASE(0, 0) AOK_CASE(0, 1) AOK_CASE(0, 2) AOK_CASE(0, 3)
         AOK_CASE(1, 0) AOK_CASE(1, 1) AOK_CASE(1, 2) AOK_CASE(1, 3)
         AOK_CASE(2, 0) AOK_CASE(2, 1) AOK_CASE(2, 2) AOK_CASE(2, 3)
@@ -268,6 +264,7 @@ struct Ov2Params {
     int nitems;
     Panels panels;
     int ns, K, N, slab_stride;
+    unsigned rec_offset;  // byte offset of the per-warp record buffers in dynamic smem
     int boff[kMaxShells + 1];
 };
 
@@ -279,6 +276,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
     __shared__ int s_next[kMaxPanels];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = THREADS / 32;
+    constexpr int REC16 = sizeof(typename PPT<FT>::type) / 16;  // 16-byte words per record
+    // per-warp staging buffer for the current item's records (K*K records)
+    float4* recbuf = reinterpret_cast<float4*>(smem_raw + P.rec_offset) + (size_t)warp * P.K * P.K * REC16;
+    const uint32_t rec_saddr = (uint32_t)__cvta_generic_to_shared(recbuf);
     const int ntiles = *P.ntiles;
     for (;;) {
         if (threadIdx.x == 0) {
@@ -310,8 +311,14 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                 const Item wi = P.items[(size_t)pair * P.nitems + it];
                 const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
                 const int n = __ldg(P.npp + q);
+                {
+                    const float4* src = reinterpret_cast<const float4*>(P.pp + (size_t)q * P.K * P.K);
+                    for (int i = lane; i < n * REC16; i += 32) recbuf[i] = __ldg(src + i);
+                    __syncwarp();
+                }
                 FT* dst = sl + (size_t)(P.boff[wi.sb] - col0) * P.N + P.boff[wi.sa];
-                dispatch(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K, n, g, dst, P.N);
+                dispatch(wi.cls, wi.chunk, rec_saddr, n, g, dst, P.N);
+                __syncwarp();
             }
             __syncthreads();
             const int len = (P.panels.col0[pn + 1] - col0) * P.N;
@@ -350,11 +357,14 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     P.N = (int)p->N;
     P.slab_stride = (int)p->slab_stride;
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
+    const size_t slab = (p->smem_bytes + 15) / 16 * 16;
+    P.rec_offset = (unsigned)slab;
+    const size_t smem = slab + (size_t)(THREADS / 32) * p->K * p->K * sizeof(typename PPT<FT>::type);
     auto kern = k_overlap2c<FT, THREADS, min_blocks<FT>()>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem_bytes);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap2c)");
     timing_begin(p, s);
-    kern<<<p->num_sms * min_blocks<FT>(), THREADS, p->smem_bytes, s>>>(P);
+    kern<<<p->num_sms * min_blocks<FT>(), THREADS, smem, s>>>(P);
     timing_end(p, s);
     return cuda_status(cudaGetLastError(), "k_overlap2c");
 }

@@ -189,6 +189,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="only the FP32C forward steps (for ncu launch lists / captures); prints no JSON")
     ap.add_argument("--batch", type=int, default=B_PER_RANK, help="pairs per rank")
+    ap.add_argument("--workload", default="overlap2c", choices=["overlap2c", "evaluate", "overlap3c", "pullback"],
+                    help="with --profile: which kernel family to run (ncu captures)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -264,6 +267,13 @@ def main():
         _lib.check(L.aok_plan_timing_enable(c["plan"].h, 0))
         kms = tot.value / max(n.value, 1)
         return allmax(ms), allmax(kms)
+
+    if args.profile and args.workload != "overlap2c":
+        fn = side_workload(args.workload, L, _dev, _lib, aok, torch)
+        for _ in range(args.warmup + args.steps):
+            fn()
+        torch.cuda.synchronize()
+        return 0
 
     # ---- FP32C forward (headline) ----
     c32 = setup(torch.float32)
@@ -407,6 +417,10 @@ def main():
             "kernel_ms": kms32, "peak_kind": peak_kind,
             "note": "algorithmic bytes = B*(N^2*4 written + 2*(12 B position + 8 B species index) read)"}
 
+    extra = None
+    if not args.no_extra:
+        extra = side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         rate, nth, bs, dt = cpu_oracle_rate(basis, pairs, coef64)
@@ -425,7 +439,7 @@ def main():
             "fp64": {"value": value64, "ms_per_step": ms64, "kernel_ms": kms64},
             "f32c_over_f64": value / value64,
             "rel_err": {"f32c_vs_oracle": err32, "f64_vs_oracle": err64, "sample_pairs": nchk},
-            "grad_step": grad,
+            "grad_step": grad, "other_configs": extra,
             "roofline": roof, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
             "gpu_launches": 3 * args.steps,
         }
@@ -434,6 +448,146 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _evaluate_setup(aok, _dev, _lib, torch, L, nX, FT, with_pb=False):
+    W = aok.workloads
+    b = W.config1_basis()
+    orb = aok.orbitals_from_species_basis(b)
+    X, sidx = W.config1_points(nX=nX)
+    pl = _dev.OrbPlan(b.zeta.shape[0], b.K, b.NZ, orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L, orb.Rnl.kind,
+                      _dev.prec_of(FT))
+    d = dict(plan=pl, X=_dev.to_colmajor(X, FT), sidx=torch.as_tensor(sidx).cuda(), z=_dev.to_colmajor(b.zeta, FT),
+             D=_dev.to_colmajor(b.D, FT), P=_dev.colmajor_empty((nX, len(orb)), FT),
+             dP=_dev.colmajor_empty((3, nX, len(orb)), FT), nX=nX, nOrb=len(orb), b=b, orb=orb, Xh=X, sh=sidx)
+    if with_pb:
+        rng = np.random.default_rng(1003)
+        d["dPin"] = _dev.to_colmajor(rng.standard_normal((nX, len(orb))), FT)
+        d["dX"] = _dev.colmajor_empty((3, nX), FT)
+        d["dz"] = _dev.colmajor_empty(b.zeta.shape, FT)
+        d["dD"] = _dev.colmajor_empty(b.zeta.shape, FT)
+    return d
+
+
+def _overlap3c_setup(aok, _dev, _lib, torch, L, B, FT):
+    import oracle
+    W = aok.workloads
+    b = W.config0_basis()
+    ls, nprim, z, D = W.gb_tables(b)
+    coef_full = oracle.compile_coef(b.zeta, b.D, b.ls)
+    coef = np.concatenate([coef_full[s, :nprim[s], 0] for s in range(len(ls))])
+    tr = W.config4_triples(B=B)
+    N = int(((ls + 1) * (ls + 2) // 2).sum())
+    pl = _dev.Plan(ls, int(nprim.max()), 1, _dev.prec_of(FT), B)
+    off = np.concatenate([[0], np.cumsum(nprim)])
+    d = dict(plan=pl, N=N, B=B, nprim=torch.as_tensor(nprim).cuda(), off=torch.as_tensor(off).cuda(),
+             coef=torch.as_tensor(coef).to("cuda", FT), alpha=torch.as_tensor(z).to("cuda", FT),
+             pA=_dev.to_colmajor(tr.posA, FT), pB=_dev.to_colmajor(tr.posB, FT), pC=_dev.to_colmajor(tr.posC, FT),
+             out=_dev.colmajor_empty((N, N, N, B), FT), ls=ls, nprim_h=nprim, coef_h=coef, z_h=z, tr=tr)
+    return d
+
+
+def side_workload(name, L, _dev, _lib, aok, torch):
+    """One launch chain of a side workload, for ncu captures (--profile --workload ...)."""
+    if name in ("evaluate", "pullback"):
+        d = _evaluate_setup(aok, _dev, _lib, torch, L, 1 << 20 if name == "evaluate" else 1 << 18, torch.float32,
+                            with_pb=(name == "pullback"))
+        if name == "evaluate":
+            return lambda: _lib.check(L.aok_evaluate_ed(d["plan"].h, _dev.ptr(d["P"]), _dev.ptr(d["dP"]),
+                                                        _dev.ptr(d["X"]), ctypes.c_void_p(d["sidx"].data_ptr()),
+                                                        _dev.ptr(d["z"]), _dev.ptr(d["D"]), d["nX"], 1.0,
+                                                        _dev.stream()))
+        return lambda: _lib.check(L.aok_evaluate_pullback(d["plan"].h, _dev.ptr(d["dX"]), _dev.ptr(d["dz"]),
+                                                          _dev.ptr(d["dD"]), _dev.ptr(d["dPin"]), _dev.ptr(d["X"]),
+                                                          ctypes.c_void_p(d["sidx"].data_ptr()), _dev.ptr(d["z"]),
+                                                          _dev.ptr(d["D"]), d["nX"], 1.0, _dev.stream()))
+    d = _overlap3c_setup(aok, _dev, _lib, torch, L, 4096, torch.float32)
+    return lambda: _lib.check(L.aok_overlap3c_gb(d["plan"].h, _dev.ptr(d["out"]), ctypes.c_void_p(d["nprim"].data_ptr()),
+                                                 ctypes.c_void_p(d["off"].data_ptr()),
+                                                 ctypes.c_void_p(d["coef"].data_ptr()),
+                                                 ctypes.c_void_p(d["alpha"].data_ptr()), _dev.ptr(d["pA"]),
+                                                 _dev.ptr(d["pB"]), _dev.ptr(d["pC"]), d["B"], _dev.stream()))
+
+
+def _time(fn, steps, warmup, torch, allmax):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record()
+    for _ in range(steps):
+        fn()
+    en.record()
+    torch.cuda.synchronize()
+    return allmax(st.elapsed_time(en) / steps)
+
+
+def side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks):
+    """Config 1 (evaluate_ed, nX=2^20), the evaluate pullback at nX=2^18 (config 3)
+    and config 4 (3C, B=4096): times, throughput and error vs the oracle."""
+    out = {}
+    n = max(5, min(200, args.steps // 10))
+    # config 1
+    res = {}
+    for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
+        d = _evaluate_setup(aok, _dev, _lib, torch, L, 1 << 20, FT)
+        fn = lambda: _lib.check(L.aok_evaluate_ed(d["plan"].h, _dev.ptr(d["P"]), _dev.ptr(d["dP"]), _dev.ptr(d["X"]),
+                                                  ctypes.c_void_p(d["sidx"].data_ptr()), _dev.ptr(d["z"]),
+                                                  _dev.ptr(d["D"]), d["nX"], 1.0, _dev.stream()))
+        ms = _time(fn, n, args.warmup, torch, allmax)
+        fsz = 4 if FT == torch.float32 else 8
+        alg = d["nX"] * (3 * fsz + 8 + 4 * d["nOrb"] * fsz)
+        m = 4096
+        zz, DD, XX = d["b"].zeta, d["b"].D, d["Xh"][:, :m]
+        if FT == torch.float32:
+            zz, DD, XX = [a.astype(np.float32).astype(np.float64) for a in (zz, DD, XX)]
+        Pr, dPr = oracle.evaluate_ed(XX, d["sh"][:m], zz, DD, d["orb"].Rnl.powers(), d["orb"].radidx,
+                                     d["orb"].ylmidx, d["orb"].L, nthreads=os.cpu_count())
+        Pg = d["P"][:m].double().cpu().numpy()
+        dPg = d["dP"][:, :m].double().cpu().numpy()
+        err = float(np.sqrt(np.sum((Pg - Pr) ** 2) + np.sum((dPg - dPr) ** 2)) / np.sqrt(np.sum(Pr ** 2) + np.sum(dPr ** 2)))
+        res[tag] = {"ms": ms, "points_per_s": d["nX"] / (ms * 1e-3), "hbm_gbs": alg / (ms * 1e-3) / 1e9,
+                    "hbm_frac": alg / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"], "rel_err_vs_oracle": err}
+        del d
+    out["config1_evaluate_ed_nX_2^20"] = res
+    # config 3, evaluate pullback at nX = 2^18
+    d = _evaluate_setup(aok, _dev, _lib, torch, L, 1 << 18, torch.float32, with_pb=True)
+    fwd = lambda: _lib.check(L.aok_evaluate_ed(d["plan"].h, _dev.ptr(d["P"]), _dev.ptr(d["dP"]), _dev.ptr(d["X"]),
+                                               ctypes.c_void_p(d["sidx"].data_ptr()), _dev.ptr(d["z"]),
+                                               _dev.ptr(d["D"]), d["nX"], 1.0, _dev.stream()))
+    pb = lambda: _lib.check(L.aok_evaluate_pullback(d["plan"].h, _dev.ptr(d["dX"]), _dev.ptr(d["dz"]),
+                                                    _dev.ptr(d["dD"]), _dev.ptr(d["dPin"]), _dev.ptr(d["X"]),
+                                                    ctypes.c_void_p(d["sidx"].data_ptr()), _dev.ptr(d["z"]),
+                                                    _dev.ptr(d["D"]), d["nX"], 1.0, _dev.stream()))
+    fms = _time(fwd, n, args.warmup, torch, allmax)
+    pms = _time(pb, n, args.warmup, torch, allmax)
+    out["config3_evaluate_pullback_nX_2^18_f32c"] = {"evaluate_ed_ms": fms, "pullback_ms": pms,
+                                                      "pullback_over_forward": pms / fms}
+    del d
+    # config 4
+    res = {}
+    for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
+        d = _overlap3c_setup(aok, _dev, _lib, torch, L, 4096, FT)
+        fn = lambda: _lib.check(L.aok_overlap3c_gb(d["plan"].h, _dev.ptr(d["out"]), ctypes.c_void_p(d["nprim"].data_ptr()),
+                                                   ctypes.c_void_p(d["off"].data_ptr()),
+                                                   ctypes.c_void_p(d["coef"].data_ptr()),
+                                                   ctypes.c_void_p(d["alpha"].data_ptr()), _dev.ptr(d["pA"]),
+                                                   _dev.ptr(d["pB"]), _dev.ptr(d["pC"]), d["B"], _dev.stream()))
+        ms = _time(fn, n, args.warmup, torch, allmax)
+        m = 256
+        tr = d["tr"]
+        cs, zs = d["coef_h"], d["z_h"]
+        pa, pb_, pc = tr.posA[:, :m], tr.posB[:, :m], tr.posC[:, :m]
+        if FT == torch.float32:
+            cs, zs, pa, pb_, pc = [a.astype(np.float32).astype(np.float64) for a in (cs, zs, pa, pb_, pc)]
+        ref = oracle.overlap3c_gb(d["ls"], d["nprim_h"], cs, zs, pa, pb_, pc, nthreads=os.cpu_count())
+        got = d["out"][:, :, :, :m].double().cpu().numpy()
+        err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        res[tag] = {"ms": ms, "integrals_per_s": d["N"] ** 3 * d["B"] / (ms * 1e-3), "rel_err_vs_oracle": err}
+        del d
+    res["f32c_over_f64"] = res["f32c"]["integrals_per_s"] / res["f64"]["integrals_per_s"]
+    out["config4_overlap3c_B_4096"] = res
+    return out
 
 
 class _Null:
