@@ -37,6 +37,7 @@ struct aok_plan {
     int nitems = 0;
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
+    unsigned* d_ticket = nullptr;    // last-block ticket of k_bin_count (reset by that block)
     int max_bin_blocks = 0;
     aok::Panels panels{};
     size_t slab_stride = 0;          // elements per batch slot in the panel buffer
@@ -62,6 +63,10 @@ struct aok_plan {
     alignas(8) unsigned char panels3_raw[160] = {};
     size_t slab_stride3 = 0;
     size_t smem3 = 0;
+    // side stream for the record preparation (forked/joined with events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool basis_set = false;          // records fixed by aok_plan_set_basis
     // optional event pairs around the dominant kernel (measurement aid)
     std::vector<cudaEvent_t> ev;
     int ev_used = 0;

@@ -132,6 +132,10 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
         (st = cuda_status(cudaMemset(p->d_err, 0, sizeof(int)), "cudaMemset(err)")))
         return fail(st);
     if ((st = setup_overlap2c_schedule(p)) != AOK_OK) return fail(st);
+    if ((st = cuda_status(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+        (st = cuda_status(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming), "cudaEventCreate")) ||
+        (st = cuda_status(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming), "cudaEventCreate")))
+        return fail(st);
     *plan = p;
     return AOK_OK;
 }
@@ -139,10 +143,13 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
     void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_counter,
-                    p->d_err, p->d_items, p->d_order, p->d_blockhist, p->d_gb_zeta, p->d_gb_coef, p->d_pb_full, p->d_pb_val, p->d_pb_counts, p->d_partials, p->d_tilerows, p->d_coef_scratch,
+                    p->d_err, p->d_items, p->d_order, p->d_blockhist, p->d_ticket, p->d_gb_zeta, p->d_gb_coef, p->d_pb_full, p->d_pb_val, p->d_pb_counts, p->d_partials, p->d_tilerows, p->d_coef_scratch,
                     p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3, p->d_npp3, p->d_items3};
     for (void* b : bufs) dfree(b);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_join) cudaEventDestroy(p->ev_join);
+    if (p->side) cudaStreamDestroy(p->side);
     delete p;
     return AOK_OK;
 }
@@ -205,12 +212,30 @@ int aok_overlap2c(aok_plan* p, void* out, const void* zeta, const void* coef, co
     if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c: null plan");
     AOK_TRY(check_batch(p, B, "aok_overlap2c"));
     if (B == 0) return AOK_OK;
-    if (!out || !zeta || !coef || !posA || !posB || !sidxA || !sidxB)
+    if (!out || !posA || !posB || !sidxA || !sidxB || (!zeta) != (!coef))
         return set_error(AOK_ERR_INVALID, "aok_overlap2c: null pointer");
     cudaStream_t s = (cudaStream_t)stream;
-    AOK_TRY(launch_prep2c(p, zeta, coef, s));
-    AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+    if (zeta && coef) {
+        // record preparation on the side stream, concurrent with the binning
+        p->basis_set = false;
+        AOK_TRY(cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord"));
+        AOK_TRY(cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent"));
+        AOK_TRY(launch_prep2c(p, zeta, coef, p->side));
+        AOK_TRY(cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord"));
+        AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+        AOK_TRY(cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent"));
+    } else {
+        if (!p->basis_set) return set_error(AOK_ERR_INVALID, "aok_overlap2c: no zeta/coef and no aok_plan_set_basis");
+        AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+    }
     return launch_overlap2c(p, out, posA, posB, B, lengthscale, s);
+}
+
+int aok_plan_set_basis(aok_plan* p, const void* zeta, const void* coef, void* stream) {
+    if (!p || !zeta || !coef) return set_error(AOK_ERR_INVALID, "aok_plan_set_basis: null pointer");
+    AOK_TRY(launch_prep2c(p, zeta, coef, (cudaStream_t)stream));
+    p->basis_set = true;
+    return AOK_OK;
 }
 
 int aok_overlap2c_gb(aok_plan* p, void* out, const int64_t* nprim, const int64_t* prim_offset, const void* coef,
@@ -222,6 +247,7 @@ int aok_overlap2c_gb(aok_plan* p, void* out, const int64_t* nprim, const int64_t
     if (!out || !nprim || !prim_offset || !coef || !alpha || !posA || !posB)
         return set_error(AOK_ERR_INVALID, "aok_overlap2c_gb: null pointer");
     cudaStream_t s = (cudaStream_t)stream;
+    p->basis_set = false;
     AOK_TRY(launch_gb_pad(p, nprim, prim_offset, coef, alpha, s));
     AOK_TRY(launch_prep2c(p, p->d_gb_zeta, p->d_gb_coef, s));
     AOK_TRY(launch_bin(p, nullptr, nullptr, B, s));
@@ -242,6 +268,7 @@ static int overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void
     }
     if (!dS || !posA || !posB || !sidxA || !sidxB)
         return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
+    p->basis_set = false;
     AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
     AOK_TRY(launch_prep2c(p, zeta, coef, s));
     return launch_overlap2c_pb(p, dcoef, dalpha, dS, zeta, coef, posA, posB, B, lengthscale, keep_absent, s);

@@ -74,16 +74,16 @@ __global__ void k_gb_pad(FT* __restrict__ zeta, FT* __restrict__ coef, const int
 // Primitive-pair records.
 // --------------------------------------------------------------------------
 __device__ __forceinline__ void fill_pp(PPf& r, double ca, double cb, double aa, double ab) {
-    double p = aa + ab;
-    double x = kPi / p;
+    const double p = aa + ab, ip = 1.0 / p;
+    const double x = kPi * ip;
     const double log2e = 1.4426950408889634074;
-    double mu2 = (aa * ab / p) * log2e;  // exponent in base 2
+    const double mu2 = ((aa * ab) * ip) * log2e;  // exponent in base 2
     r.w = (float)(ca * cb * (x * sqrt(x)));
     r.mu_hi = (float)mu2;
     r.mu_lo = (float)(mu2 - (double)r.mu_hi);
-    r.ra = (float)(aa / p);
-    r.rb = (float)(ab / p);
-    r.oo2p = (float)(0.5 / p);
+    r.ra = (float)(aa * ip);
+    r.rb = (float)(ab * ip);
+    r.oo2p = (float)(0.5 * ip);
     r.flush = 0.f;
     r.pad = 0.f;
 }
@@ -193,17 +193,18 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
 }
 
 // --------------------------------------------------------------------------
-// Species-pair bins: multi-block counting sort.
+// Species-pair bins: multi-block counting sort in two launches, no waiting.
 //   k_bin_count    per block: histogram of its chunk of the batch
-//   k_bin_scan     one block: per-key totals, key bases, per-block offsets,
-//                  the tile table (tiles of <= 32 elements of one key), the
-//                  tile count, and the work-queue counter reset
-//   k_bin_scatter  per block: scatter its chunk into the key ranges
-// The scatter is stable inside each block, so the permutation is reproducible
-// (the forward does not need it, the pullback's fixed-order sums do).
+//   k_bin_scatter  per block: reads every block's histogram (at most 128
+//                  blocks x NZ^2 keys), derives its own offsets, scatters its
+//                  chunk stably (so the permutation is reproducible), and
+//                  writes every nblk-th entry of the tile table (tiles of
+//                  <= 32 elements of one key); block 0 also sets the tile
+//                  count and resets the work-queue counter.
+// k_bin_identity replaces both for single-species batches.
 // --------------------------------------------------------------------------
 constexpr int kBinThreads = 256;
-constexpr int kBinChunk = 2048;
+constexpr int kBinMaxBlocks = 128;
 constexpr int kMaxPairs = 256;
 
 __device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sidxB, int b, int B, int NZ, int* err) {
@@ -218,37 +219,49 @@ __device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sid
 
 __global__ void __launch_bounds__(kBinThreads) k_bin_count(const int64_t* __restrict__ sidxA,
                                                             const int64_t* __restrict__ sidxB, int B, int NZ,
-                                                            int* __restrict__ blockhist, int* __restrict__ err) {
+                                                            int chunk, int* __restrict__ blockhist,
+                                                            int* __restrict__ err) {
     __shared__ int hist[kMaxPairs];
-    const int np = NZ * NZ, lane = threadIdx.x & 31;
+    const int np = NZ * NZ;
     for (int k = threadIdx.x; k < np; k += blockDim.x) hist[k] = 0;
     __syncthreads();
-    const int c0 = blockIdx.x * kBinChunk;
-    for (int b0 = c0 + (threadIdx.x & ~31); b0 < min(B, c0 + kBinChunk); b0 += blockDim.x) {
-        const int key = pair_key(sidxA, sidxB, b0 + lane, min(B, c0 + kBinChunk), NZ, err);
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[key], __popc(peers));
+    const int c0 = blockIdx.x * chunk, c1 = min(B, c0 + chunk);
+    for (int b = c0 + threadIdx.x; b < c1; b += blockDim.x) {
+        const int key = pair_key(sidxA, sidxB, b, c1, NZ, err);
+        if (key >= 0) atomicAdd(&hist[key], 1);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < np; k += blockDim.x) blockhist[(size_t)blockIdx.x * np + k] = hist[k];
 }
 
-__global__ void __launch_bounds__(kMaxPairs) k_bin_scan(int* __restrict__ blockhist, int nblk, int NZ,
-                                                        int4* __restrict__ tiles, int* __restrict__ ntiles,
-                                                        unsigned* __restrict__ counter) {
-    __shared__ int tot[kMaxPairs], base[kMaxPairs], tbase[kMaxPairs];
-    const int np = NZ * NZ, k = threadIdx.x;
-    if (k < np) {
-        int t = 0;
-        for (int blk = 0; blk < nblk; ++blk) {
-            int v = blockhist[(size_t)blk * np + k];
-            blockhist[(size_t)blk * np + k] = t;  // exclusive offset inside key k
-            t += v;
-        }
-        tot[k] = t;
+constexpr int kBinWarps = kBinThreads / 32;
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __restrict__ sidxA,
+                                                              const int64_t* __restrict__ sidxB, int B, int NZ,
+                                                              int chunk, const int* __restrict__ blockhist,
+                                                              int* __restrict__ perm, int4* __restrict__ tiles,
+                                                              int* __restrict__ ntiles,
+                                                              unsigned* __restrict__ counter, int* __restrict__ err) {
+    __shared__ int wcount[kBinWarps][kMaxPairs];
+    __shared__ int before[kMaxPairs], tot[kMaxPairs], base[kMaxPairs], tbase[kMaxPairs + 1];
+    const int np = NZ * NZ, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nblk = gridDim.x, me = blockIdx.x;
+    // per key: elements in earlier blocks, and the total (integer sums, so the
+    // order of the shared atomics does not matter)
+    for (int k = threadIdx.x; k < np; k += blockDim.x) {
+        before[k] = 0;
+        tot[k] = 0;
     }
     __syncthreads();
-    if (k == 0) {
+    for (int i = threadIdx.x; i < nblk * np; i += blockDim.x) {
+        const int k = i % np, blk = i / np;
+        const int v = blockhist[i];
+        if (v) {
+            atomicAdd(&tot[k], v);
+            if (blk < me) atomicAdd(&before[k], v);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
         int acc = 0, tacc = 0;
         for (int q = 0; q < np; ++q) {
             base[q] = acc;
@@ -256,32 +269,24 @@ __global__ void __launch_bounds__(kMaxPairs) k_bin_scan(int* __restrict__ blockh
             acc += tot[q];
             tacc += (tot[q] + kTileB - 1) / kTileB;
         }
-        *ntiles = tacc;
-        *counter = 0u;
+        tbase[np] = tacc;
+        if (me == 0) {
+            *ntiles = tacc;
+            *counter = 0u;
+        }
     }
+    // tiles: this block writes tiles me, me + nblk, ...
     __syncthreads();
-    if (k < np) {
-        for (int blk = 0; blk < nblk; ++blk) blockhist[(size_t)blk * np + k] += base[k];
-        const int n = tot[k];
-        for (int t = 0; t * kTileB < n; ++t)
-            tiles[tbase[k] + t] = make_int4(k, base[k] + t * kTileB, min(kTileB, n - t * kTileB), 0);
+    for (int t = me + (int)threadIdx.x * nblk; t < tbase[np]; t += blockDim.x * nblk) {
+        int k = 0;
+        while (tbase[k + 1] <= t) ++k;
+        const int off = (t - tbase[k]) * kTileB;
+        tiles[t] = make_int4(k, base[k] + off, min(kTileB, tot[k] - off), 0);
     }
-}
-
-// Stable within the block: warp w owns the contiguous sub-range
-// [c0 + w*kBinChunk/NWB, ...) and walks it in order; per-warp key counts and a
-// scan over warps give every element a position that does not depend on
-// scheduling, so perm (and the tiles built from it) is reproducible.
-constexpr int kBinWarps = kBinThreads / 32;
-__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __restrict__ sidxA,
-                                                              const int64_t* __restrict__ sidxB, int B, int NZ,
-                                                              const int* __restrict__ blockoff,
-                                                              int* __restrict__ perm, int* __restrict__ err) {
-    __shared__ int wcount[kBinWarps][kMaxPairs];
-    const int np = NZ * NZ, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int sub = kBinChunk / kBinWarps;
-    const int c0 = blockIdx.x * kBinChunk + warp * sub;
-    const int c1 = min(B, c0 + sub);
+    // stable scatter of this block's chunk: warp w owns a contiguous sub-range
+    const int sub = (chunk + kBinWarps - 1) / kBinWarps;
+    const int c0 = me * chunk + warp * sub;
+    const int c1 = min(min(B, (me + 1) * chunk), c0 + sub);
     for (int k = lane; k < np; k += 32) wcount[warp][k] = 0;
     __syncwarp();
     for (int b0 = c0; b0 < c1; b0 += 32) {
@@ -291,9 +296,8 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
         __syncwarp();
     }
     __syncthreads();
-    // exclusive scan over warps per key, seeded with the block's offset
     for (int k = threadIdx.x; k < np; k += blockDim.x) {
-        int acc = blockoff[(size_t)blockIdx.x * np + k];
+        int acc = base[k] + before[k];
         for (int w = 0; w < kBinWarps; ++w) {
             const int v = wcount[w][k];
             wcount[w][k] = acc;
@@ -309,6 +313,17 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
         __syncwarp();
         if (key >= 0 && lane == __ffs(peers) - 1) wcount[warp][key] += __popc(peers);
         __syncwarp();
+    }
+}
+
+__global__ void k_bin_identity(int B, int* __restrict__ perm, int4* __restrict__ tiles, int* __restrict__ ntiles,
+                               unsigned* __restrict__ counter) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < B) perm[b] = b;
+    if (b * kTileB < B) tiles[b] = make_int4(0, b * kTileB, min(kTileB, B - b * kTileB), 0);
+    if (b == 0) {
+        *ntiles = (B + kTileB - 1) / kTileB;
+        *counter = 0u;
     }
 }
 
@@ -380,9 +395,13 @@ int setup_overlap2c_schedule(aok_plan* p) {
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(items)");
     e = cudaMalloc(&p->d_order, sizeof(Item) * items.size() * p->NZ * p->NZ);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(order)");
-    p->max_bin_blocks = (int)std::max<int64_t>(1, (p->max_batch + kBinChunk - 1) / kBinChunk);
+    p->max_bin_blocks = kBinMaxBlocks;
     e = cudaMalloc(&p->d_blockhist, sizeof(int) * p->max_bin_blocks * p->NZ * p->NZ);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(blockhist)");
+    e = cudaMalloc(&p->d_ticket, sizeof(unsigned));
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(ticket)");
+    e = cudaMemset(p->d_ticket, 0, sizeof(unsigned));
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemset(ticket)");
     e = cudaMemcpy(p->d_items, items.data(), sizeof(Item) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(items)");
     return AOK_OK;
@@ -419,13 +438,18 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
 }
 
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s) {
-    const int nblk = (int)((B + kBinChunk - 1) / kBinChunk);
+    const int chunk = (int)std::max<int64_t>(512, (B + kBinMaxBlocks - 1) / kBinMaxBlocks);
+    const int nblk = (int)((B + chunk - 1) / chunk);
     const int NZ = (int)p->NZ;
-    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, p->d_blockhist, p->d_err);
+    if (NZ == 1 || (!sidxA && !sidxB)) {
+        k_bin_identity<<<(int)((B + 255) / 256), 256, 0, s>>>((int)B, p->d_perm, p->d_tiles, p->d_ntiles,
+                                                             p->d_counter);
+        return cuda_status(cudaGetLastError(), "k_bin_identity");
+    }
+    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, p->d_blockhist, p->d_err);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_bin_count"));
-    k_bin_scan<<<1, kMaxPairs, 0, s>>>(p->d_blockhist, nblk, NZ, p->d_tiles, p->d_ntiles, p->d_counter);
-    AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_bin_scan"));
-    k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, p->d_blockhist, p->d_perm, p->d_err);
+    k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, p->d_blockhist, p->d_perm,
+                                               p->d_tiles, p->d_ntiles, p->d_counter, p->d_err);
     return cuda_status(cudaGetLastError(), "k_bin_scatter");
 }
 

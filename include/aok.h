@@ -86,12 +86,23 @@ int aok_plan_timing_read(aok_plan* plan, double* total_ms, int64_t* launches);
 int aok_compile_coef(aok_plan* plan, void* coef, const void* zeta, const void* D, void* stream);
 
 /*
+ * Fixes the plan's basis parameters: the geometry-free primitive-pair records
+ * (and their execution order) are computed once from zeta, coef (ns,K,NZ) and
+ * kept in the plan.  This is the device half of compile_basis
+ * (src/integrals/orbital/cartesian_gto_basis.jl:138-146): later aok_overlap2c
+ * calls given zeta = coef = NULL use these records, as batch_overlap! uses a
+ * compiled CartesianGTOBasis.  Calling it again replaces the parameters.
+ */
+int aok_plan_set_basis(aok_plan* plan, const void* zeta, const void* coef, void* stream);
+
+/*
  * Batched 2-center overlap, species-aware Cartesian basis.
  * Replaces batch_S_orbital_kernel! + batch_overlap!(out, ::CartesianGTOBasis, XA, XB)
  * (src/integrals/orbital/overlap_2c.jl:165-281, 321-347).
  * out (N,N,B); zeta, coef (ns,K,NZ); posA, posB (3,B) in the basis's input
  * unit (multiplied by lengthscale on the device, overlap_2c.jl:331-333);
  * sidxA, sidxB (B) 1-based.  Zero-coefficient primitive pairs are skipped.
+ * zeta = coef = NULL uses the parameters fixed by aok_plan_set_basis.
  */
 int aok_overlap2c(aok_plan* plan, void* out, const void* zeta, const void* coef,
                   const void* posA, const void* posB, const int64_t* sidxA,
