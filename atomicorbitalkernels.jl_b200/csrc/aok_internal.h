@@ -37,7 +37,9 @@ struct aok_plan {
     int nitems = 0;
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
-    unsigned* d_ticket = nullptr;    // last-block ticket of k_bin_count (reset by that block)
+    int* d_order_id = nullptr;       // static item id of each position of d_order (NZ*NZ*nitems)
+    int* d_pb_csr = nullptr;         // per (side, shell): static item ids, ascending (2*nitems)
+    std::vector<int> pb_csr_off;     // 2*(ns+1) offsets into d_pb_csr
     int max_bin_blocks = 0;
     aok::Panels panels{};
     size_t slab_stride = 0;          // elements per batch slot in the panel buffer
@@ -121,9 +123,11 @@ int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef
                            const void* D, const void* dalpha_add, cudaStream_t s);
 
 // overlap2c_bwd*.cu
-int launch_pb_f32(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* posA, const void* posB,
+int launch_pb_f32(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
+                  const void* posA, const void* posB,
                   double lengthscale, cudaStream_t s);
-int launch_pb_f64(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* posA, const void* posB,
+int launch_pb_f64(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
+                  const void* posA, const void* posB,
                   double lengthscale, cudaStream_t s);
 int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
                         const void* coef, const void* posA, const void* posB, int64_t B,

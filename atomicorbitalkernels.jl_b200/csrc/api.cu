@@ -143,8 +143,10 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
     void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_counter,
-                    p->d_err, p->d_items, p->d_order, p->d_blockhist, p->d_ticket, p->d_gb_zeta, p->d_gb_coef, p->d_pb_full, p->d_pb_val, p->d_pb_counts, p->d_partials, p->d_tilerows, p->d_coef_scratch,
-                    p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3, p->d_npp3, p->d_items3};
+                    p->d_err, p->d_items, p->d_order, p->d_order_id, p->d_pb_csr, p->d_blockhist,
+                    p->d_gb_zeta, p->d_gb_coef, p->d_pb_full, p->d_pb_val, p->d_pb_counts, p->d_partials,
+                    p->d_tilerows, p->d_coef_scratch, p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3,
+                    p->d_npp3, p->d_items3};
     for (void* b : bufs) dfree(b);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);

@@ -38,6 +38,7 @@
 #include <cstring>
 
 #include "aok_internal.h"
+#include "md2c.cuh"
 
 namespace aok {
 
@@ -152,32 +153,33 @@ __global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restric
 // --------------------------------------------------------------------------
 constexpr int kOrderMax = 2048;
 
-__device__ __forceinline__ int class_cost(int cls, int elems) {
-    int la = cls >> 2, lb = cls & 3;
-    return 24 + 12 * (la + 1) * (lb + 1) + 2 * elems;
-}
 
-__global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const Item* __restrict__ items,
-                                                 const int* __restrict__ npp, Panels panels, int nitems, int ns) {
+__global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, int* __restrict__ order_id,
+                                                 const Item* __restrict__ items, const int* __restrict__ npp,
+                                                 Panels panels, int nitems, int ns) {
     __shared__ unsigned long long key[kOrderMax];
     const int pair = blockIdx.x;
     Item* out = order + (size_t)pair * nitems;
+    int* out_id = order_id + (size_t)pair * nitems;
     if (nitems > kOrderMax) {  // very large bases: keep the static order
-        for (int i = threadIdx.x; i < nitems; i += blockDim.x) out[i] = items[i];
+        for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
+            out[i] = items[i];
+            out_id[i] = i;
+        }
         return;
     }
     for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
         const Item it = items[i];
         int pn = 0;
         while (pn + 1 < panels.n && i >= panels.item0[pn + 1]) ++pn;
+        // heavy classes first (terms of the geometry transform), grouped by class
+        // so that the warps of a CTA mostly run the same code; then by primitive pairs
         const int la = it.cls >> 2, lb = it.cls & 3;
-        const int ne = ncart(la) * ncart(lb), nch = nchunks(ne);
-        const int elems = (it.chunk + 1) * ne / nch - it.chunk * ne / nch;
         const int n = npp[((size_t)pair * ns + it.sa) * ns + it.sb];
         const unsigned long long k = ((unsigned long long)pn << 48) |
-                                     ((unsigned long long)(0xFFFF - class_cost(it.cls, elems)) << 32) |
+                                     ((unsigned long long)(0xFFFF - md_terms(la, lb)) << 32) |
                                      ((unsigned long long)(0xFFFF - min(n, 0xFFFF)) << 16) |
-                                     (unsigned long long)(it.cls * 4 + it.chunk);
+                                     (unsigned long long)it.cls;
         key[i] = (k << 0);
     }
     __syncthreads();
@@ -189,6 +191,7 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
             r += (kj < ki) || (kj == ki && j < i);
         }
         out[r] = items[i];
+        out_id[r] = i;
     }
 }
 
@@ -330,10 +333,6 @@ __global__ void k_bin_identity(int B, int* __restrict__ perm, int4* __restrict__
 // --------------------------------------------------------------------------
 // Host side: schedule and launchers.
 // --------------------------------------------------------------------------
-static double class_cost(int la, int lb, int elems) {
-    // per primitive pair: setup + three 1-D tables + contraction of `elems`
-    return 24.0 + 12.0 * (la + 1) * (lb + 1) + 2.0 * elems;
-}
 
 int setup_overlap2c_schedule(aok_plan* p) {
     const int ns = (int)p->ns, N = (int)p->N;
@@ -378,12 +377,8 @@ int setup_overlap2c_schedule(aok_plan* p) {
         for (int sb = pshell[pn]; sb < pshell[pn + 1]; ++sb)
             for (int sa = 0; sa < ns; ++sa) {
                 int la = (int)p->ls[sa], lb = (int)p->ls[sb];
-                int ne = ncart(la) * ncart(lb), nch = nchunks(ne);
-                for (int c = 0; c < nch; ++c) {
-                    int e = (c + 1) * ne / nch - c * ne / nch;
-                    Item it{(int16_t)(la * 4 + lb), (int16_t)c, (int16_t)sa, (int16_t)sb};
-                    v.push_back({class_cost(la, lb, e), it});
-                }
+                Item it{(int16_t)(la * 4 + lb), (int16_t)0, (int16_t)sa, (int16_t)sb};
+                v.push_back({(double)md_terms(la, lb), it});
             }
         std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
         for (auto& x : v) items.push_back(x.second);
@@ -398,12 +393,25 @@ int setup_overlap2c_schedule(aok_plan* p) {
     p->max_bin_blocks = kBinMaxBlocks;
     e = cudaMalloc(&p->d_blockhist, sizeof(int) * p->max_bin_blocks * p->NZ * p->NZ);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(blockhist)");
-    e = cudaMalloc(&p->d_ticket, sizeof(unsigned));
-    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(ticket)");
-    e = cudaMemset(p->d_ticket, 0, sizeof(unsigned));
-    if (e != cudaSuccess) return cuda_status(e, "cudaMemset(ticket)");
+    e = cudaMalloc(&p->d_order_id, sizeof(int) * items.size() * p->NZ * p->NZ);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(order_id)");
     e = cudaMemcpy(p->d_items, items.data(), sizeof(Item) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(items)");
+    // per shell and side, the static item ids whose bra (side 0) or ket (side 1)
+    // shell it is, ascending: the pullback sums its per-item partials along these
+    std::vector<int> csr;
+    p->pb_csr_off.assign(2 * (ns + 1), 0);
+    for (int side = 0; side < 2; ++side)
+        for (int s = 0; s < ns; ++s) {
+            p->pb_csr_off[side * (ns + 1) + s] = (int)csr.size();
+            for (int i = 0; i < (int)items.size(); ++i)
+                if ((side == 0 ? items[i].sa : items[i].sb) == s) csr.push_back(i);
+            p->pb_csr_off[side * (ns + 1) + s + 1] = (int)csr.size();
+        }
+    e = cudaMalloc(&p->d_pb_csr, sizeof(int) * csr.size());
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(pb_csr)");
+    e = cudaMemcpy(p->d_pb_csr, csr.data(), sizeof(int) * csr.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(pb_csr)");
     return AOK_OK;
 }
 
@@ -432,8 +440,8 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
         k_prep2c<float><<<bl, th, 0, s>>>((PPf*)p->d_pp, p->d_npp, (const float*)zeta, (const float*)coef,
                                           (int)p->ns, (int)p->K, (int)p->NZ);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_prep2c"));
-    k_order2c<<<(int)(p->NZ * p->NZ), 256, 0, s>>>(p->d_order, p->d_items, p->d_npp, p->panels, p->nitems,
-                                                  (int)p->ns);
+    k_order2c<<<(int)(p->NZ * p->NZ), 256, 0, s>>>(p->d_order, p->d_order_id, p->d_items, p->d_npp, p->panels,
+                                                  p->nitems, (int)p->ns);
     return cuda_status(cudaGetLastError(), "k_order2c");
 }
 

@@ -44,8 +44,8 @@ int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, 
     (void)B;
     AOK_TRY_PB(ensure_pb_buffers(p));
     AOK_TRY_PB(launch_prep_pb(p, zeta, coef, keep_absent, s));
-    if (p->prec == AOK_PREC_F64) return launch_pb_f64(p, dcoef, dalpha, dS, posA, posB, lengthscale, s);
-    return launch_pb_f32(p, dcoef, dalpha, dS, posA, posB, lengthscale, s);
+    if (p->prec == AOK_PREC_F64) return launch_pb_f64(p, dcoef, dalpha, dS, zeta, coef, posA, posB, lengthscale, s);
+    return launch_pb_f32(p, dcoef, dalpha, dS, zeta, coef, posA, posB, lengthscale, s);
 }
 
 }  // namespace aok

@@ -9,15 +9,16 @@
 // through the same aliased lin -> (i, j) map as the forward:
 //   Bsum = sum_c g_c E_prod,   dcoef[sa,ip] += cb pref0 Bsum,  dcoef[sb,jp] += ca pref0 Bsum
 //   dalpha[sa,ip] += ca cb d/dalpha_a (pref0 E_prod) . g,  and symmetrically for jp.
-// The reference evaluates d/dalpha through raised-momentum tables to l+2; here
-// the same derivative is taken in forward mode on the t = 0 recursion:
-//   d(pref0 F T)/d a = pref0 F [(-3/(2p) - R^2 (b/p)^2) T + dT/da],
-// with F = exp(-mu R^2), T = E^x E^y E^z, dPA/da = dPB/da = (b/p) AB / p,
-// dPA/db = dPB/db = -(a/p) AB / p, d(k/2p)/da = d(k/2p)/db = -(k/2p)/p.
-// The contraction with g is factored per axis: H^x[i][j] = sum over
-// components with x powers (i, j) of g E^y E^z (and H^y, H^z), so that
-// Bsum = sum E^x H^x and the derivative = sum_axes sum dE H.
+// The reference evaluates d/dalpha through raised-momentum tables to l+2.
+// Here the cotangent block is first contracted with the geometry into
+// cotangent moments G (md2c.cuh, the transpose of the forward transform), so
+// that per primitive pair Bsum = sum G mono(ra, rb, q) and the exponent
+// derivatives follow from the chain rule on (ra, rb, q) and
+//   d log(pref0 exp(-mu R^2))/da = -3/(2p) - R^2 (b/p)^2   (and a <-> b).
 //
+// Padded slots whose exponent equals that of an earlier zero slot of the same
+// shell are listed once; k_pb_reduce copies the first one's (bitwise equal)
+// value to the others.
 // Padded slots are not skipped (as in the reference): a pair with exactly one
 // zero coefficient still feeds the zero slot's dcoef (value-only work).  In
 // the full parameter pullback, pairs whose zero slot belongs to an absent
@@ -116,7 +117,15 @@ __global__ void k_prep_pb(typename PBT<FT>::type* __restrict__ full, typename PB
         }
         const bool in = e < K * K;
         const bool isf = in && ca != 0.0 && cb != 0.0;
-        const bool isv = in && ((ca == 0.0 && cb != 0.0 && presA) || (cb == 0.0 && ca != 0.0 && presB));
+        bool isv = in && ((ca == 0.0 && cb != 0.0 && presA) || (cb == 0.0 && ca != 0.0 && presB));
+        if (isv) {
+            // a zero slot whose exponent equals that of an earlier zero slot of the
+            // same shell receives bitwise the same dcoef: k_pb_reduce copies it
+            const int z = ca == 0.0 ? ip : jp, sz = ca == 0.0 ? sa : sb, gz = ca == 0.0 ? ga : gb;
+            const FT zz = zeta[sz + ns * (z + K * gz)];
+            for (int k = 0; k < z; ++k)
+                if (coef[sz + ns * (k + K * gz)] == FT(0) && zeta[sz + ns * (k + K * gz)] == zz) isv = false;
+        }
         const unsigned mf = __ballot_sync(0xffffffffu, isf), mv = __ballot_sync(0xffffffffu, isv);
         const unsigned lt = (1u << lane) - 1u;
         if (isf) fill_pb(of[nf + __popc(mf & lt)], ca, cb, aa, ab, ip, jp, 0);
@@ -128,89 +137,44 @@ __global__ void k_prep_pb(typename PBT<FT>::type* __restrict__ full, typename PB
 }
 
 // ---------------------------------------------------------------------------
-// Per-axis tables.
+// Per primitive pair, from the cotangent moments G (md2c.cuh):
+//   T0 = sum G mono,  Ta = (1/2q) d/da sum G mono,  Tb = (1/2q) d/db sum G mono
+// with mono = rb^al ra^be q^ga and, by the chain rule on (ra, rb, q),
+//   d mono/da = 2q [-(al + ga) mono + be rb^{al+1} ra^{be-1} q^ga]
+//   d mono/db = 2q [al rb^{al-1} ra^{be+1} q^ga - (be + ga) mono].
 // ---------------------------------------------------------------------------
-// H^x[i][j] (and H^y, H^z) from the cotangent values g of the item's chunk.
-template <int LA, int LB, int L0, int L1, typename FT>
-__device__ __forceinline__ void build_H(FT (&Hx)[LA + 1][LB + 1], FT (&Hy)[LA + 1][LB + 1], FT (&Hz)[LA + 1][LB + 1],
-                                        const FT (&Ex)[LA + 1][LB + 1], const FT (&Ey)[LA + 1][LB + 1],
-                                        const FT (&Ez)[LA + 1][LB + 1], const FT* g, bool need_yz) {
-    using CI = ClassInfo<LA, LB>;
+template <int LA, int LB, typename FT, bool DERIV>
+__device__ __forceinline__ void md_dual(const FT (&G)[(LA + 1) * (LB + 1)], FT ra, FT rb, FT q, FT& T0, FT& Ta,
+                                        FT& Tb) {
+    constexpr int W = LA + LB;
+    FT rbp[LA + 2], rap[LB + 2], qp[W / 2 + 1];
+    rbp[0] = FT(1);
 #pragma unroll
-    for (int i = 0; i <= LA; ++i)
+    for (int k = 1; k <= LA + 1; ++k) rbp[k] = rbp[k - 1] * rb;
+    rap[0] = FT(1);
 #pragma unroll
-        for (int j = 0; j <= LB; ++j) Hx[i][j] = Hy[i][j] = Hz[i][j] = FT(0);
+    for (int k = 1; k <= LB + 1; ++k) rap[k] = rap[k - 1] * ra;
+    qp[0] = FT(1);
 #pragma unroll
-    for (int c2 = 0; c2 < CI::NB; ++c2)
+    for (int k = 1; k <= W / 2; ++k) qp[k] = qp[k - 1] * q;
+    T0 = Ta = Tb = FT(0);
 #pragma unroll
-        for (int c1 = 0; c1 < CI::NA; ++c1) {
-            const int lin = c1 + CI::N1 * c2;
-            if (lin >= L0 && lin < L1) {
-                const int x1 = cart_x(LA, c1), x2 = cart_x(LB, c2), y1 = cart_y(LA, c1), y2 = cart_y(LB, c2),
-                          z1 = cart_z(LA, c1), z2 = cart_z(LB, c2);
-                const FT gv = g[lin - L0];
-                Hx[x1][x2] += gv * (Ey[y1][y2] * Ez[z1][z2]);
-                if (need_yz) {
-                    const FT gx = gv * Ex[x1][x2];
-                    Hy[y1][y2] += gx * Ez[z1][z2];
-                    Hz[z1][z2] += gx * Ey[y1][y2];
+    for (int al = 0; al <= LA; ++al)
+#pragma unroll
+        for (int be = 0; be <= LB; ++be)
+            if (MdTab<LA, LB>::used(al, be)) {
+                const int ga = (W - al - be) / 2;
+                const FT Gm = G[al * (LB + 1) + be];
+                const FT mono = (rbp[al] * rap[be]) * qp[ga];
+                T0 = fma(Gm, mono, T0);
+                if (DERIV) {
+                    FT da = FT(-(al + ga)) * mono, db = FT(-(be + ga)) * mono;
+                    if (be > 0) da = fma(FT(be), (rbp[al + 1] * rap[be - 1]) * qp[ga], da);
+                    if (al > 0) db = fma(FT(al), (rbp[al - 1] * rap[be + 1]) * qp[ga], db);
+                    Ta = fma(Gm, da, Ta);
+                    Tb = fma(Gm, db, Tb);
                 }
             }
-        }
-}
-
-// sum_ij dE/da[i][j] H[i][j] and sum_ij dE/db[i][j] H[i][j] for one axis, by
-// forward-mode differentiation of the build_E recursion.
-template <int LA, int LB, typename FT>
-__device__ __forceinline__ void dual_sums(const FT (&E)[LA + 1][LB + 1], const FT (&H)[LA + 1][LB + 1], FT PA, FT PB,
-                                          const FT (&O)[4], FT invp, FT ua, FT ub, FT& Sa, FT& Sb) {
-    FT Da[LA + 1][LB + 1], Db[LA + 1][LB + 1];
-    Da[0][0] = FT(0);
-    Db[0][0] = FT(0);
-#pragma unroll
-    for (int i = 1; i <= LA; ++i) {
-        FT c = FT(0), da = ua * E[i - 1][0] + PA * Da[i - 1][0], db = ub * E[i - 1][0] + PA * Db[i - 1][0];
-        if (i >= 2) {
-            c = O[i - 1] * E[i - 2][0];
-            da += O[i - 1] * Da[i - 2][0];
-            db += O[i - 1] * Db[i - 2][0];
-        }
-        Da[i][0] = da - c * invp;
-        Db[i][0] = db - c * invp;
-    }
-#pragma unroll
-    for (int j = 1; j <= LB; ++j) {
-        {
-            FT c = FT(0), da = ua * E[0][j - 1] + PB * Da[0][j - 1], db = ub * E[0][j - 1] + PB * Db[0][j - 1];
-            if (j >= 2) {
-                c = O[j - 1] * E[0][j - 2];
-                da += O[j - 1] * Da[0][j - 2];
-                db += O[j - 1] * Db[0][j - 2];
-            }
-            Da[0][j] = da - c * invp;
-            Db[0][j] = db - c * invp;
-        }
-#pragma unroll
-        for (int i = 1; i <= LA; ++i) {
-            FT c = O[j] * E[i - 1][j - 1];
-            FT da = ua * E[i - 1][j] + PA * Da[i - 1][j] + O[j] * Da[i - 1][j - 1];
-            FT db = ub * E[i - 1][j] + PA * Db[i - 1][j] + O[j] * Db[i - 1][j - 1];
-            if (i >= 2) {
-                c += O[i - 1] * E[i - 2][j];
-                da += O[i - 1] * Da[i - 2][j];
-                db += O[i - 1] * Db[i - 2][j];
-            }
-            Da[i][j] = da - c * invp;
-            Db[i][j] = db - c * invp;
-        }
-    }
-#pragma unroll
-    for (int i = 0; i <= LA; ++i)
-#pragma unroll
-        for (int j = 0; j <= LB; ++j) {
-            Sa += Da[i][j] * H[i][j];
-            Sb += Db[i][j] * H[i][j];
-        }
 }
 
 template <typename FT> struct PBLoad;
@@ -254,102 +218,49 @@ __device__ __forceinline__ FT& acc_at(FT* acc, int row, int lane) {
     return acc[row * 33 + lane];
 }
 
-// One work item (shell-pair chunk) for one lane: FT = float or double.
-template <typename FT, int LA, int LB, int C>
+// One work item (shell pair) for one lane: FT = float or double.
+template <typename FT, int LA, int LB>
 __device__ __noinline__ void pb_item(const typename PBT<FT>::type* __restrict__ pf, int nf,
                                      const typename PBT<FT>::type* __restrict__ pv, int nv, const Geo<FT> g,
                                      const FT* gslab, int N, FT* acc, int K, int lane) {
-    using CI = ClassInfo<LA, LB>;
-    constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
-    FT gv[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) gv[m] = gslab[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA];
+    FT G[(LA + 1) * (LB + 1)];
+    md_cotangent<LA, LB, FT>(G, g.AB, gslab, N);
     // full pairs: value + both exponent derivatives
     for (int q = 0; q < nf; ++q) {
         PBLoad<FT> r;
         r.load(pf + q);
-        const FT P = r.pref(g);
-        const FT O[4] = {FT(0), r.oo2p, FT(2) * r.oo2p, FT(3) * r.oo2p};
-        const FT invp = FT(2) * r.oo2p;
-        FT PA[3], PB[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            PA[a] = -r.rb * g.AB[a];
-            PB[a] = r.ra * g.AB[a];
-        }
-        FT Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
-        build_E<LA, LB, FT>(Ex, PA[0], PB[0], O, FT(1));
-        build_E<LA, LB, FT>(Ey, PA[1], PB[1], O, FT(1));
-        build_E<LA, LB, FT>(Ez, PA[2], PB[2], O, FT(1));
-        FT Hx[LA + 1][LB + 1], Hy[LA + 1][LB + 1], Hz[LA + 1][LB + 1];
-        build_H<LA, LB, L0, L1, FT>(Hx, Hy, Hz, Ex, Ey, Ez, gv, true);
-        FT Bs = FT(0);
-#pragma unroll
-        for (int i = 0; i <= LA; ++i)
-#pragma unroll
-            for (int j = 0; j <= LB; ++j) Bs += Ex[i][j] * Hx[i][j];
-        FT Ba = FT(0), Bb = FT(0);
-        if (LA + LB > 0) {
-            dual_sums<LA, LB, FT>(Ex, Hx, PA[0], PB[0], O, invp, r.rb * g.AB[0] * invp, -r.ra * g.AB[0] * invp, Ba, Bb);
-            dual_sums<LA, LB, FT>(Ey, Hy, PA[1], PB[1], O, invp, r.rb * g.AB[1] * invp, -r.ra * g.AB[1] * invp, Ba, Bb);
-            dual_sums<LA, LB, FT>(Ez, Hz, PA[2], PB[2], O, invp, r.rb * g.AB[2] * invp, -r.ra * g.AB[2] * invp, Ba, Bb);
-        }
-        const FT kpre = FT(-3) * r.oo2p;  // -3/(2p)
+        const FT P = r.pref(g);  // pref0 exp(-mu R^2)
+        FT T0, Ta, Tb;
+        md_dual<LA, LB, FT, true>(G, r.ra, r.rb, r.oo2p, T0, Ta, Tb);
+        const FT two_q = FT(2) * r.oo2p, kpre = FT(-3) * r.oo2p;  // -3/(2p)
         const FT ka = kpre - g.R2 * (r.rb * r.rb), kb = kpre - g.R2 * (r.ra * r.ra);
-        const FT PBs = P * Bs, cab = r.ca * r.cb * P;
-        acc_at(acc, 0 * K + r.ip, lane) += r.cb * PBs;
-        acc_at(acc, 1 * K + r.ip, lane) += cab * (ka * Bs + Ba);
-        acc_at(acc, 2 * K + r.jp, lane) += r.ca * PBs;
-        acc_at(acc, 3 * K + r.jp, lane) += cab * (kb * Bs + Bb);
+        const FT V = P * T0, cab = r.ca * r.cb * P;
+        acc_at(acc, 0 * K + r.ip, lane) += r.cb * V;
+        acc_at(acc, 1 * K + r.ip, lane) += cab * fma(two_q, Ta, ka * T0);
+        acc_at(acc, 2 * K + r.jp, lane) += r.ca * V;
+        acc_at(acc, 3 * K + r.jp, lane) += cab * fma(two_q, Tb, kb * T0);
     }
     // one-zero pairs: the zero slot's dcoef only
     for (int q = 0; q < nv; ++q) {
         PBLoad<FT> r;
         r.load(pv + q);
         const FT P = r.pref(g);
-        const FT O[4] = {FT(0), r.oo2p, FT(2) * r.oo2p, FT(3) * r.oo2p};
-        FT Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
-        build_E<LA, LB, FT>(Ex, -r.rb * g.AB[0], r.ra * g.AB[0], O, FT(1));
-        build_E<LA, LB, FT>(Ey, -r.rb * g.AB[1], r.ra * g.AB[1], O, FT(1));
-        build_E<LA, LB, FT>(Ez, -r.rb * g.AB[2], r.ra * g.AB[2], O, FT(1));
-        FT Hx[LA + 1][LB + 1], Hy[LA + 1][LB + 1], Hz[LA + 1][LB + 1];
-        build_H<LA, LB, L0, L1, FT>(Hx, Hy, Hz, Ex, Ey, Ez, gv, false);
-        FT Bs = FT(0);
-#pragma unroll
-        for (int i = 0; i <= LA; ++i)
-#pragma unroll
-            for (int j = 0; j <= LB; ++j) Bs += Ex[i][j] * Hx[i][j];
+        FT T0, Ta, Tb;
+        md_dual<LA, LB, FT, false>(G, r.ra, r.rb, r.oo2p, T0, Ta, Tb);
         if (r.side == 0)
-            acc_at(acc, 0 * K + r.ip, lane) += r.cb * (P * Bs);
+            acc_at(acc, 0 * K + r.ip, lane) += r.cb * (P * T0);
         else
-            acc_at(acc, 2 * K + r.jp, lane) += r.ca * (P * Bs);
-    }
-}
-
-template <typename FT, int LA, int LB>
-__device__ __forceinline__ void pb_chunks(int chunk, const typename PBT<FT>::type* pf, int nf,
-                                          const typename PBT<FT>::type* pv, int nv, const Geo<FT>& g, const FT* gs,
-                                          int N, FT* acc, int K, int lane) {
-    constexpr int NCH = ClassInfo<LA, LB>::NCH;
-    if constexpr (NCH == 1) {
-        pb_item<FT, LA, LB, 0>(pf, nf, pv, nv, g, gs, N, acc, K, lane);
-    } else if constexpr (NCH == 2) {
-        if (chunk == 0) pb_item<FT, LA, LB, 0>(pf, nf, pv, nv, g, gs, N, acc, K, lane);
-        else pb_item<FT, LA, LB, 1>(pf, nf, pv, nv, g, gs, N, acc, K, lane);
-    } else {
-        if (chunk == 0) pb_item<FT, LA, LB, 0>(pf, nf, pv, nv, g, gs, N, acc, K, lane);
-        else if (chunk == 1) pb_item<FT, LA, LB, 1>(pf, nf, pv, nv, g, gs, N, acc, K, lane);
-        else pb_item<FT, LA, LB, 2>(pf, nf, pv, nv, g, gs, N, acc, K, lane);
+            acc_at(acc, 2 * K + r.jp, lane) += r.ca * (P * T0);
     }
 }
 
 template <typename FT>
-__device__ __forceinline__ void pb_dispatch(int cls, int chunk, const typename PBT<FT>::type* pf, int nf,
+__device__ __forceinline__ void pb_dispatch(int cls, const typename PBT<FT>::type* pf, int nf,
                                             const typename PBT<FT>::type* pv, int nv, const Geo<FT>& g,
                                             const FT* gs, int N, FT* acc, int K, int lane) {
     switch (cls) {
 #define AOK_PB_CASE(LA, LB) \
-    case (LA) * 4 + (LB): pb_chunks<FT, LA, LB>(chunk, pf, nf, pv, nv, g, gs, N, acc, K, lane); break;
+    case (LA) * 4 + (LB): pb_item<FT, LA, LB>(pf, nf, pv, nv, g, gs, N, acc, K, lane); break;
         AOK_PB_CASE(0, 0) AOK_PB_CASE(0, 1) AOK_PB_CASE(0, 2) AOK_PB_CASE(0, 3)
         AOK_PB_CASE(1, 0) AOK_PB_CASE(1, 1) AOK_PB_CASE(1, 2) AOK_PB_CASE(1, 3)
         AOK_PB_CASE(2, 0) AOK_PB_CASE(2, 1) AOK_PB_CASE(2, 2) AOK_PB_CASE(2, 3)
@@ -376,10 +287,13 @@ struct PbParams {
     const Item* items;
     int nitems;
     Panels panels;
-    double* itemacc;   // [gridDim.x][nitems][4K]
-    double* tilerows;  // [tile][4 * ns * K]: (side, kind, shell, k)
+    const int* order_id;  // static item id of each position of `items`
+    const int* csr;       // per (side, shell): static item ids, ascending
+    double* itemacc;      // [gridDim.x][nitems][4K], indexed by static item id
+    double* tilerows;     // [tile][4 * ns * K]: (side, kind, shell, k)
     int ns, K, NZ, N, slab_stride;
     int boff[kMaxShells + 1];
+    int csr_off[2 * (kMaxShells + 1)];
 };
 
 template <typename FT, int THREADS>
@@ -437,17 +351,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_overlap2c_pb(const __grid_consta
                 it = __shfl_sync(0xffffffffu, it, 0) + i0;
                 if (it >= i1) break;
                 const Item wi = order[it];
+                const int sid = P.order_id[(size_t)pair * P.nitems + it];
                 const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
                 const int2 n = P.counts[q];
                 const FT* gs = sl + (size_t)(P.boff[wi.sb] - col0) * P.N + P.boff[wi.sa];
-                pb_dispatch<FT>(wi.cls, wi.chunk, P.pf + (size_t)q * P.K * P.K, n.x, P.pv + (size_t)q * P.K * P.K,
-                                n.y, g, gs, P.N, acc, P.K, lane);
+                pb_dispatch<FT>(wi.cls, P.pf + (size_t)q * P.K * P.K, n.x, P.pv + (size_t)q * P.K * P.K, n.y, g, gs,
+                                P.N, acc, P.K, lane);
                 __syncwarp();
                 // the item's slot sums over the 32 lanes, in lane order
                 for (int r = lane; r < K4; r += 32) {
                     double sum = 0.0;
                     for (int l = 0; l < 32; ++l) sum += (double)acc[r * 33 + l];
-                    iacc[(size_t)it * K4 + r] = sum;
+                    iacc[(size_t)sid * K4 + r] = sum;
                 }
                 __syncwarp();
                 for (int i = lane; i < K4 * 33; i += 32) acc[i] = FT(0);
@@ -455,48 +370,81 @@ __global__ void __launch_bounds__(THREADS, 1) k_overlap2c_pb(const __grid_consta
             }
             __syncthreads();
         }
-        // the tile's row: items summed in their fixed order
+        // the tile's row: the items of each (side, shell) summed in static id order
         double* trow = P.tilerows + (size_t)tile * 4 * P.ns * P.K;
         for (int t = threadIdx.x; t < 4 * P.ns * P.K; t += blockDim.x) {
             const int k = t % P.K, s = (t / P.K) % P.ns, sk = t / (P.K * P.ns);  // sk = side*2 + kind
-            const int side = sk >> 1, kind = sk & 1;
+            const int side = sk >> 1;
+            const int c0 = P.csr_off[side * (P.ns + 1) + s], c1 = P.csr_off[side * (P.ns + 1) + s + 1];
             double sum = 0.0;
-            for (int i = 0; i < P.nitems; ++i) {
-                const Item wi = order[i];
-                if ((side == 0 ? wi.sa : wi.sb) == s) sum += iacc[(size_t)i * K4 + (side * 2 + kind) * P.K + k];
-            }
+            for (int c = c0; c < c1; ++c) sum += iacc[(size_t)P.csr[c] * K4 + sk * P.K + k];
             trow[t] = sum;
         }
     }
 }
 
 // Fixed-order sum of the tile rows: out[kind][(s, k, sigma)].
+// Grid (column groups of 32, NZ): lane = column (kind, s, k) of species sigma,
+// warp w sums tiles w, w + NW, ... in order (both sides), and warp 0 adds the
+// NW partials in warp order, so the result does not depend on scheduling.
+constexpr int kPbReduceThreads = 512;
+
 template <typename FT>
-__global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, const double* __restrict__ tilerows,
-                            const int4* __restrict__ tiles, const int* __restrict__ ntiles, int ns, int K, int NZ) {
-    const int S = ns * K * NZ;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * S) return;
-    const int kind = t / S, slot = t % S;
-    const int s = slot % ns, k = (slot / ns) % K, sigma = slot / (ns * K);
-    const int nt = *ntiles, R = 4 * ns * K;
-    double sum = 0.0;
-    for (int tile = 0; tile < nt; ++tile) {
-        const int pair = tiles[tile].x;
-        const double* row = tilerows + (size_t)tile * R;
-        if (pair / NZ == sigma) sum += row[((0 * 2 + kind) * ns + s) * K + k];
-        if (pair % NZ == sigma) sum += row[((1 * 2 + kind) * ns + s) * K + k];
+__global__ void __launch_bounds__(kPbReduceThreads) k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha,
+                                                                const double* __restrict__ tilerows,
+                                                                const int4* __restrict__ tiles,
+                                                                const int* __restrict__ ntiles,
+                                                                const FT* __restrict__ zeta,
+                                                                const FT* __restrict__ coef, int ns, int K, int NZ) {
+    constexpr int NW = kPbReduceThreads / 32;
+    __shared__ double part[NW][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sigma = blockIdx.y, SK = ns * K;
+    const int col = blockIdx.x * 32 + lane;  // kind * SK + s * K + k
+    const bool valid = col < 2 * SK;
+    const int kind = valid ? col / SK : 0, s = valid ? (col % SK) / K : 0;
+    int k = valid ? col % K : 0;
+    const int slot = s + ns * (k + K * sigma);
+    if (valid && kind == 0 && coef[slot] == FT(0)) {
+        // zero slots with equal exponents share the first one's value (k_prep_pb
+        // lists the first only)
+        const FT z = zeta[slot];
+        for (int k2 = 0; k2 < k; ++k2) {
+            const int o = s + ns * (k2 + K * sigma);
+            if (coef[o] == FT(0) && zeta[o] == z) {
+                k = k2;
+                break;
+            }
+        }
     }
-    if (kind == 0) dcoef[slot] = (FT)sum;
-    else dalpha[slot] = (FT)sum;
+    const int nt = *ntiles, R = 4 * SK;
+    const int c0 = (0 * 2 + kind) * SK + s * K + k, c1 = (1 * 2 + kind) * SK + s * K + k;
+    double sum = 0.0;
+    if (valid) {
+        for (int tile = warp; tile < nt; tile += NW) {
+            const int pair = tiles[tile].x;
+            const double* row = tilerows + (size_t)tile * R;
+            if (pair / NZ == sigma) sum += row[c0];
+            if (pair % NZ == sigma) sum += row[c1];
+        }
+    }
+    part[warp][lane] = sum;
+    __syncthreads();
+    if (warp == 0 && valid) {
+        double tot = 0.0;
+        for (int w = 0; w < NW; ++w) tot += part[w][lane];
+        const int out = s + ns * (((col % SK) % K) + K * sigma);
+        if (kind == 0) dcoef[out] = (FT)tot;
+        else dalpha[out] = (FT)tot;
+    }
 }
 
 constexpr int kPbThreadsF32 = 512;
 constexpr int kPbThreadsF64 = 256;
 
 template <typename FT, int THREADS>
-inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* posA, const void* posB,
-                     double lengthscale, cudaStream_t s) {
+inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
+                     const void* posA, const void* posB, double lengthscale, cudaStream_t s) {
     constexpr int NW = THREADS / 32;
     PbParams<FT> P;
     memset(&P, 0, sizeof(P));
@@ -515,6 +463,9 @@ inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, con
     P.items = p->d_order;
     P.nitems = p->nitems;
     P.panels = p->panels;
+    P.order_id = p->d_order_id;
+    P.csr = p->d_pb_csr;
+    for (size_t i = 0; i < p->pb_csr_off.size(); ++i) P.csr_off[i] = p->pb_csr_off[i];
     P.itemacc = (double*)p->d_partials;
     P.tilerows = (double*)p->d_tilerows;
     P.ns = (int)p->ns;
@@ -533,10 +484,10 @@ inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, con
     kern<<<grid, THREADS, smem, s>>>(P);
     timing_end(p, s);
     AOK_TRY_PB(cuda_status(cudaGetLastError(), "k_overlap2c_pb"));
-    const int S = (int)(p->ns * p->K * p->NZ);
-    k_pb_reduce<FT><<<(2 * S + 127) / 128, 128, 0, s>>>((FT*)dcoef, (FT*)dalpha, (const double*)p->d_tilerows,
-                                                       p->d_tiles, p->d_ntiles, (int)p->ns, (int)p->K,
-                                                       (int)p->NZ);
+    const dim3 rgrid((unsigned)((2 * p->ns * p->K + 31) / 32), (unsigned)p->NZ);
+    k_pb_reduce<FT><<<rgrid, kPbReduceThreads, 0, s>>>((FT*)dcoef, (FT*)dalpha, (const double*)p->d_tilerows,
+                                                       p->d_tiles, p->d_ntiles, (const FT*)zeta,
+                                                       (const FT*)coef, (int)p->ns, (int)p->K, (int)p->NZ);
     return cuda_status(cudaGetLastError(), "k_pb_reduce");
 }
 

@@ -3,9 +3,10 @@
 
 namespace aok {
 
-int launch_pb_f64(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* posA, const void* posB,
+int launch_pb_f64(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
+                  const void* posA, const void* posB,
                   double lengthscale, cudaStream_t s) {
-    return launch_pb<double, kPbThreadsF64>(p, dcoef, dalpha, dS, posA, posB, lengthscale, s);
+    return launch_pb<double, kPbThreadsF64>(p, dcoef, dalpha, dS, zeta, coef, posA, posB, lengthscale, s);
 }
 
 }  // namespace aok

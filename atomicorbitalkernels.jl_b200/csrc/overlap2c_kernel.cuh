@@ -7,6 +7,7 @@
 #include <cstring>
 
 #include "aok_internal.h"
+#include "md2c.cuh"
 
 namespace aok {
 
@@ -62,46 +63,6 @@ __device__ __forceinline__ void load_geo(Geo<double>& g, const double* A, const 
 }
 
 // --------------------------------------------------------------------------
-// 1-D overlap table E[i][j] = E_0^{ij} (McMurchie-Davidson t = 0 coefficient,
-// built with the Obara-Saika form of the recursion, HJO eq. 9.5.6-9.5.7 with
-// E_1^{ij} = (i E_0^{i-1,j} + j E_0^{i,j-1}) / 2p), seeded with E[0][0] = e00:
-//   E[i+1][j] = PA E[i][j] + (i E[i-1][j] + j E[i][j-1]) / 2p
-//   E[i][j+1] = PB E[i][j] + (i E[i-1][j] + j E[i][j-1]) / 2p
-// PA = -(b/p) AB and PB = (a/p) AB are formed directly (no P - A cancellation).
-// --------------------------------------------------------------------------
-template <int LA, int LB, typename FT>
-__device__ __forceinline__ void build_E(FT (&E)[LA + 1][LB + 1], FT PA, FT PB, const FT (&O)[4], FT e00) {
-    // O[k] = k / 2p (shared by the three axes)
-    E[0][0] = e00;
-#pragma unroll
-    for (int i = 1; i <= LA; ++i) {
-        if (i >= 2)
-            E[i][0] = PA * E[i - 1][0] + O[i - 1] * E[i - 2][0];
-        else
-            E[i][0] = PA * E[i - 1][0];
-    }
-#pragma unroll
-    for (int j = 1; j <= LB; ++j) {
-        if (j >= 2)
-            E[0][j] = PB * E[0][j - 1] + O[j - 1] * E[0][j - 2];
-        else
-            E[0][j] = PB * E[0][j - 1];
-#pragma unroll
-        for (int i = 1; i <= LA; ++i) {
-            FT c = O[j] * E[i - 1][j - 1];
-            if (i >= 2) c = c + O[i - 1] * E[i - 2][j];
-            E[i][j] = PA * E[i - 1][j] + c;
-        }
-    }
-}
-
-template <int LA, int LB>
-struct ClassInfo {
-    static constexpr int NA = ncart(LA), NB = ncart(LB), NE = NA * NB, N1 = 2 * LA + 1;
-    static constexpr int NCH = nchunks(NE);
-};
-
-// --------------------------------------------------------------------------
 // Shared-memory record access (the warp stages an item's records first).
 // --------------------------------------------------------------------------
 __device__ __forceinline__ float4 lds128(uint32_t a) {
@@ -121,25 +82,46 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 
 // --------------------------------------------------------------------------
-// One work item for one lane (batch element): FP32C.
+// Moments of one primitive pair: part[al*(LB+1)+be] += e00 rb^al ra^be q^ga for
+// the used slots (al + be + 2 ga = LA + LB).
+// --------------------------------------------------------------------------
+template <int LA, int LB, typename FT>
+__device__ __forceinline__ void md_accumulate(FT (&part)[(LA + 1) * (LB + 1)], FT e00, FT ra, FT rb, FT q) {
+    constexpr int W = LA + LB;
+    FT rbp[LA + 1], rap[LB + 1], qp[W / 2 + 1];
+    rbp[0] = e00;
+#pragma unroll
+    for (int k = 1; k <= LA; ++k) rbp[k] = rbp[k - 1] * rb;
+    rap[0] = FT(1);
+#pragma unroll
+    for (int k = 1; k <= LB; ++k) rap[k] = rap[k - 1] * ra;
+    qp[0] = FT(1);
+#pragma unroll
+    for (int k = 1; k <= W / 2; ++k) qp[k] = qp[k - 1] * q;
+#pragma unroll
+    for (int al = 0; al <= LA; ++al)
+#pragma unroll
+        for (int be = 0; be <= LB; ++be)
+            if (MdTab<LA, LB>::used(al, be)) {
+                const int m = al * (LB + 1) + be;
+                part[m] = fma(rbp[al] * rap[be], qp[(W - al - be) / 2], part[m]);
+            }
+}
+
+// --------------------------------------------------------------------------
+// One work item (shell pair) for one lane (batch element): FP32C.
 // rec: shared-memory address of the item's n records, ip-major in rows of
 // equal length (the number of non-zero ket coefficients, record field 6).
 // dst points at the block's (0,0) element inside this lane's slab; element
-// (i, j) of the block lives at dst[j*N + i].
+// (i, j) of the block lives at dst[j*N + i].  The moments are summed per ip
+// row in FP32 and folded into (hi, lo) with TwoSum at the end of each row.
 // --------------------------------------------------------------------------
-template <int LA, int LB, int C>
+template <int LA, int LB>
 __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, float* dst, int N) {
-    using CI = ClassInfo<LA, LB>;
-    constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
-    // hi/part in registers; the TwoSum rounding errors (lo) accumulate in this
-    // lane's slab slots, which the item owns until it writes its result.
-    float hi[M], part[M];
+    constexpr int NM = (LA + 1) * (LB + 1);
+    float hi[NM], lo[NM], part[NM];
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-        hi[m] = 0.f;
-        part[m] = 0.f;
-        dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] = 0.f;
-    }
+    for (int m = 0; m < NM; ++m) hi[m] = lo[m] = part[m] = 0.f;
     const int rowlen = n > 0 ? (int)lds128(rec + 16).z : 1;
     for (int q0 = 0; q0 < n; q0 += rowlen) {
         for (int q = q0; q < q0 + rowlen; ++q) {
@@ -151,93 +133,43 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, f
             const float xh = mu_hi * g.R2;
             const float xl = fmaf(mu_hi, g.R2, -xh) + fmaf(mu_lo, g.R2, mu_hi * g.R2lo);
             const float e00 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
-            const float O[4] = {0.f, oo2p, 2.f * oo2p, 3.f * oo2p};
-            float Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
-            build_E<LA, LB, float>(Ex, -rb * g.AB[0], ra * g.AB[0], O, e00);
-            build_E<LA, LB, float>(Ey, -rb * g.AB[1], ra * g.AB[1], O, 1.f);
-            build_E<LA, LB, float>(Ez, -rb * g.AB[2], ra * g.AB[2], O, 1.f);
-#pragma unroll
-            for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-                for (int c1 = 0; c1 < CI::NA; ++c1) {
-                    const int lin = c1 + CI::N1 * c2;
-                    if (lin >= L0 && lin < L1) {
-                        const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)] * Ez[cart_z(LA, c1)][cart_z(LB, c2)];
-                        part[lin - L0] = fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)], yz, part[lin - L0]);
-                    }
-                }
+            md_accumulate<LA, LB, float>(part, e00, ra, rb, oo2p);
         }
-        // fold the ip row's partial sums into (hi, lo)
 #pragma unroll
-        for (int m = 0; m < M; ++m) {
+        for (int m = 0; m < NM; ++m) {
             float s, e;
             two_sum(hi[m], part[m], s, e);
             hi[m] = s;
+            lo[m] += e;
             part[m] = 0.f;
-            dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] += e;
         }
     }
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-        float* d = dst + ((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA;
-        *d = hi[m] + *d;
-    }
+    for (int m = 0; m < NM; ++m) hi[m] += lo[m];
+    md_transform<LA, LB, float>(hi, g.AB, dst, N);
 }
 
 // FP64 variant: plain double accumulation, records from shared memory.
-template <int LA, int LB, int C>
+template <int LA, int LB>
 __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<double> g, double* dst, int N) {
-    using CI = ClassInfo<LA, LB>;
-    constexpr int L0 = C * CI::NE / CI::NCH, L1 = (C + 1) * CI::NE / CI::NCH, M = L1 - L0;
-    double acc[M];
+    constexpr int NM = (LA + 1) * (LB + 1);
+    double mom[NM];
 #pragma unroll
-    for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    for (int m = 0; m < NM; ++m) mom[m] = 0.0;
     for (int q = 0; q < n; ++q) {
         const double2 r0 = lds128d(rec + 64u * q), r1 = lds128d(rec + 64u * q + 16u),
                       r2 = lds128d(rec + 64u * q + 32u);
         const double w = r0.x, mu = r0.y, ra = r1.x, rb = r1.y, oo2p = r2.x;
-        const double e00 = exp(-mu * g.R2) * w;
-        const double O[4] = {0.0, oo2p, 2.0 * oo2p, 3.0 * oo2p};
-        double Ex[LA + 1][LB + 1], Ey[LA + 1][LB + 1], Ez[LA + 1][LB + 1];
-        build_E<LA, LB, double>(Ex, -rb * g.AB[0], ra * g.AB[0], O, e00);
-        build_E<LA, LB, double>(Ey, -rb * g.AB[1], ra * g.AB[1], O, 1.0);
-        build_E<LA, LB, double>(Ez, -rb * g.AB[2], ra * g.AB[2], O, 1.0);
-#pragma unroll
-        for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-            for (int c1 = 0; c1 < CI::NA; ++c1) {
-                const int lin = c1 + CI::N1 * c2;
-                if (lin >= L0 && lin < L1) {
-                    const double yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)] * Ez[cart_z(LA, c1)][cart_z(LB, c2)];
-                    acc[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)], yz, acc[lin - L0]);
-                }
-            }
+        md_accumulate<LA, LB, double>(mom, exp(-mu * g.R2) * w, ra, rb, oo2p);
     }
-#pragma unroll
-    for (int m = 0; m < M; ++m) dst[((L0 + m) / CI::NA) * N + (L0 + m) % CI::NA] = acc[m];
-}
-
-template <typename FT, int LA, int LB>
-__device__ __forceinline__ void run_chunks(int chunk, uint32_t pp, int n, const Geo<FT>& g, FT* dst, int N) {
-    constexpr int NCH = ClassInfo<LA, LB>::NCH;
-    if constexpr (NCH == 1) {
-        run_item<LA, LB, 0>(pp, n, g, dst, N);
-    } else if constexpr (NCH == 2) {
-        if (chunk == 0) run_item<LA, LB, 0>(pp, n, g, dst, N);
-        else run_item<LA, LB, 1>(pp, n, g, dst, N);
-    } else {
-        static_assert(NCH == 3, "chunk count");
-        if (chunk == 0) run_item<LA, LB, 0>(pp, n, g, dst, N);
-        else if (chunk == 1) run_item<LA, LB, 1>(pp, n, g, dst, N);
-        else run_item<LA, LB, 2>(pp, n, g, dst, N);
-    }
+    md_transform<LA, LB, double>(mom, g.AB, dst, N);
 }
 
 template <typename FT>
-__device__ __forceinline__ void dispatch(int cls, int chunk, uint32_t pp, int n, const Geo<FT>& g, FT* dst, int N) {
+__device__ __forceinline__ void dispatch(int cls, uint32_t pp, int n, const Geo<FT>& g, FT* dst, int N) {
     switch (cls) {
 #define AOK_CASE(LA, LB) \
-    case (LA) * 4 + (LB): run_chunks<FT, LA, LB>(chunk, pp, n, g, dst, N); break;
+    case (LA) * 4 + (LB): run_item<LA, LB>(pp, n, g, dst, N); break;
         AOK_CASE(0, 0) AOK_CASE(0, 1) AOK_CASE(0, 2) AOK_CASE(0, 3)
         AOK_CASE(1, 0) AOK_CASE(1, 1) AOK_CASE(1, 2) AOK_CASE(1, 3)
         AOK_CASE(2, 0) AOK_CASE(2, 1) AOK_CASE(2, 2) AOK_CASE(2, 3)
@@ -317,7 +249,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                     __syncwarp();
                 }
                 FT* dst = sl + (size_t)(P.boff[wi.sb] - col0) * P.N + P.boff[wi.sa];
-                dispatch(wi.cls, wi.chunk, rec_saddr, n, g, dst, P.N);
+                dispatch(wi.cls, rec_saddr, n, g, dst, P.N);
                 __syncwarp();
             }
             __syncthreads();

@@ -180,7 +180,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="aok", choices=["aok", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
@@ -189,7 +189,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="only the FP32C forward steps (for ncu launch lists / captures); prints no JSON")
     ap.add_argument("--batch", type=int, default=B_PER_RANK, help="pairs per rank")
-    ap.add_argument("--workload", default="overlap2c", choices=["overlap2c", "evaluate", "overlap3c", "pullback"],
+    ap.add_argument("--workload", default="overlap2c",
+                    choices=["overlap2c", "evaluate", "overlap3c", "pullback", "grad"],
                     help="with --profile: which kernel family to run (ncu captures)")
     ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
     args = ap.parse_args()
@@ -272,7 +273,7 @@ def main():
         kms = tot.value / max(n.value, 1)
         return allmax(ms), allmax(kms)
 
-    if args.profile and args.workload != "overlap2c":
+    if args.profile and args.workload not in ("overlap2c", "grad"):
         fn = side_workload(args.workload, L, _dev, _lib, aok, torch)
         for _ in range(args.warmup + args.steps):
             fn()
@@ -281,6 +282,12 @@ def main():
 
     # ---- FP32C forward (headline) ----
     c32 = setup(torch.float32)
+    if args.profile and args.workload == "grad":
+        gd = _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch)
+        for _ in range(args.warmup + args.steps):
+            gd["gstep"]()
+        torch.cuda.synchronize()
+        return 0
     if args.profile:
         for _ in range(args.warmup + args.steps):
             step(c32)
@@ -302,40 +309,8 @@ def main():
     # ---- (zeta, D) gradient step (config 3): L = sum (S - S_tgt)^2, B = 16384 pairs ----
     grad = None
     if not args.no_grad:
-        Bg = min(16384, B)
-        zt, Dt = aok.workloads.config3_target(basis)
-        cg = {k: v for k, v in c32.items()}
-        gpl = _dev.Plan(basis.ls, K, NZ, _dev.prec_of(torch.float32), Bg)
-        zt_d = _dev.to_colmajor(zt, torch.float32)
-        Dt_d = _dev.to_colmajor(Dt, torch.float32)
-        ct_d = _dev.colmajor_empty((ns, K, NZ), torch.float32)
-        _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(ct_d), _dev.ptr(zt_d), _dev.ptr(Dt_d), _dev.stream()))
-        Sg = _dev.colmajor_empty((N, N, Bg), torch.float32)
-        Tg = _dev.colmajor_empty((N, N, Bg), torch.float32)
-        dz = _dev.colmajor_empty((ns, K, NZ), torch.float32)
-        dD = _dev.colmajor_empty((ns, K, NZ), torch.float32)
-        pA, pB = c32["pA"][:, :Bg], c32["pB"][:, :Bg]
-        sA = ctypes.c_void_p(c32["sA"].data_ptr())
-        sB = ctypes.c_void_p(c32["sB"].data_ptr())
-
-        def fwd(out, coef):
-            _lib.check(L.aok_overlap2c(gpl.h, _dev.ptr(out), _dev.ptr(c32["zeta"]), _dev.ptr(coef), _dev.ptr(pA),
-                                       _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
-
-        _lib.check(L.aok_overlap2c(gpl.h, _dev.ptr(Tg), _dev.ptr(zt_d), _dev.ptr(ct_d), _dev.ptr(pA), _dev.ptr(pB),
-                                   sA, sB, Bg, 1.0, _dev.stream()))
-
-        def gstep():
-            _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(c32["coef"]), _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]),
-                                          _dev.stream()))
-            fwd(Sg, c32["coef"])
-            dS = (Sg - Tg).mul_(2.0)
-            _lib.check(L.aok_overlap_pullback_ps(gpl.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS),
-                                                 _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
-                                                 _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
-
-        def fstep():
-            fwd(Sg, c32["coef"])
+        gd = _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch)
+        gstep, fstep = gd["gstep"], gd["fstep"]
 
         def tloop(fn, n):
             for _ in range(args.warmup):
@@ -352,7 +327,8 @@ def main():
         ng = max(3, args.steps // 10)
         f_ms = tloop(fstep, ng)
         g_ms = tloop(gstep, ng)
-        del gpl
+        Bg = gd["Bg"]
+        del gd
         grad = {"workload": "config 3: L = sum (S - S_tgt)^2 over B=16384 pairs, FP32C forward + pullback_ps",
                 "batch": Bg, "forward_ms": f_ms, "step_ms": g_ms, "step_over_forward": g_ms / f_ms,
                 "launches_per_step": 3 + 5 + 7}
@@ -418,8 +394,14 @@ def main():
     # ---- roofline of the dominant kernel (k_overlap2c, FP32C) ----
     alg_bytes = B * (N * N * 4 + 2 * (3 * 4 + 8))
     achieved = alg_bytes / (kms32 * 1e-3) / 1e9
+    # DRAM bytes of one ncu capture of this kernel at B = 32768 (read 2.12 MB + write
+    # 102.3 MB), scaled to this launch's batch; the output still dirty in L2 when the
+    # kernel ends is not counted by dram__bytes_write.
+    traffic = (2.121728e6 + 102.310656e6) * B / 32768
     roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "k_overlap2c<float>",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "algorithmic_bytes": alg_bytes,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, B=32768 capture scaled by B/32768",
+            "kernel": "k_overlap2c<float>",
             "kernel_ms": kms32, "peak_kind": peak_kind,
             "note": "algorithmic bytes = B*(N^2*4 written + 2*(12 B position + 8 B species index) read)"}
 
@@ -459,6 +441,52 @@ def main():
     return 0
 
 
+def _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch):
+    """Config 3: L = sum (S - S_tgt)^2 over the first 16384 pairs of the batch, FP32C.
+    gstep = compile_coef + forward + dL/dS + pullback_ps (dzeta, dD); fstep = forward."""
+    N, ns, K, NZ = basis.nbf_total, basis.nshells, basis.K, basis.NZ
+    Bg = min(16384, B)
+    zt, Dt = aok.workloads.config3_target(basis)
+    gpl = _dev.Plan(basis.ls, K, NZ, _dev.prec_of(torch.float32), Bg)
+    zt_d = _dev.to_colmajor(zt, torch.float32)
+    Dt_d = _dev.to_colmajor(Dt, torch.float32)
+    ct_d = _dev.colmajor_empty((ns, K, NZ), torch.float32)
+    _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(ct_d), _dev.ptr(zt_d), _dev.ptr(Dt_d), _dev.stream()))
+    Sg = _dev.colmajor_empty((N, N, Bg), torch.float32)
+    Tg = _dev.colmajor_empty((N, N, Bg), torch.float32)
+    dS = _dev.colmajor_empty((N, N, Bg), torch.float32)
+    dz = _dev.colmajor_empty((ns, K, NZ), torch.float32)
+    dD = _dev.colmajor_empty((ns, K, NZ), torch.float32)
+    pA, pB = c32["pA"][:, :Bg], c32["pB"][:, :Bg]
+    sA = ctypes.c_void_p(c32["sA"].data_ptr())
+    sB = ctypes.c_void_p(c32["sB"].data_ptr())
+
+    def fwd(out, coef):
+        _lib.check(L.aok_overlap2c(gpl.h, _dev.ptr(out), _dev.ptr(c32["zeta"]), _dev.ptr(coef), _dev.ptr(pA),
+                                   _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
+
+    _lib.check(L.aok_overlap2c(gpl.h, _dev.ptr(Tg), _dev.ptr(zt_d), _dev.ptr(ct_d), _dev.ptr(pA), _dev.ptr(pB),
+                               sA, sB, Bg, 1.0, _dev.stream()))
+
+    def gstep():
+        _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(c32["coef"]), _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]),
+                                      _dev.stream()))
+        fwd(Sg, c32["coef"])
+        # dL/dS = 2 (S - S_tgt); the pullback is linear in dS, so the factor 2 is applied
+        # to the (ns, K, NZ) gradients instead of the (N, N, B) cotangent
+        torch.sub(Sg, Tg, out=dS)
+        _lib.check(L.aok_overlap_pullback_ps(gpl.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS),
+                                             _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
+                                             _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
+        dz.mul_(2.0)
+        dD.mul_(2.0)
+
+    def fstep():
+        fwd(Sg, c32["coef"])
+
+    return dict(plan=gpl, gstep=gstep, fstep=fstep, Bg=Bg, dz=dz, dD=dD)
+
+
 def _evaluate_setup(aok, _dev, _lib, torch, L, nX, FT, with_pb=False):
     W = aok.workloads
     b = W.config1_basis()
@@ -479,11 +507,11 @@ def _evaluate_setup(aok, _dev, _lib, torch, L, nX, FT, with_pb=False):
 
 
 def _overlap3c_setup(aok, _dev, _lib, torch, L, B, FT):
-    import oracle
     W = aok.workloads
     b = W.config0_basis()
     ls, nprim, z, D = W.gb_tables(b)
-    coef_full = oracle.compile_coef(b.zeta, b.D, b.ls)
+    # contracted, normalised coefficients from the library's own compile step (FP64)
+    coef_full = aok.compile_coef(torch.as_tensor(b.zeta), torch.as_tensor(b.D), b.ls).cpu().numpy()
     coef = np.concatenate([coef_full[s, :nprim[s], 0] for s in range(len(ls))])
     tr = W.config4_triples(B=B)
     N = int(((ls + 1) * (ls + 2) // 2).sum())
