@@ -39,25 +39,29 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     e = (a - (s - bb)) + (b - bb);
 }
 
-// Primitive-pair record of one (species pair, shell pair): everything that
-// does not depend on the geometry, computed once per call in FP64.
-//   w    = c_a c_b (pi/p)^{3/2}
-//   mu   = a b / p (FP64 record); mu log2(e) as hi + lo (FP32 record)
-//   ra   = a/p,  rb = b/p,  oo2p = 1/(2p), flush = row length (non-zero ket coefficients).
-struct PPf {
-    float w, mu_hi, mu_lo, ra, rb, oo2p, flush, pad;
-};
-struct PPd {
-    double w, mu, ra, rb, oo2p, flush, pad0, pad1;
-};
-template <typename FT> struct PPT;
-template <> struct PPT<float> { using type = PPf; };
-template <> struct PPT<double> { using type = PPd; };
+// Primitive-pair record of one (species pair, shell pair) of class (la, lb):
+// everything that does not depend on the geometry, computed once per call in
+// FP64.  With p = a + b, w = c_a c_b (pi/p)^{3/2} and the moment slots
+// (al, be) used by the class (al <= la, be <= lb, (la - al) + (lb - be) even,
+// ga = (la + lb - al - be) / 2), in slot order:
+//   FP32:  mu log2(e) as hi, lo;  row length;  w rb^al ra^be q^ga per slot
+//   FP64:  mu;                    row length;  w rb^al ra^be q^ga per slot
+// (ra = a/p, rb = b/p, q = 1/2p), padded to whole 16-byte words.  The row
+// length is the number of non-zero ket coefficients: records form rows of
+// equal length, one per bra primitive.
+__host__ __device__ constexpr int md_nv(int la, int lb) {
+    return ((la + 1) * (lb + 1) + (((la + lb) & 1) == 0 ? 1 : 0)) / 2;
+}
+__host__ __device__ constexpr int rec_words16_f32(int la, int lb) { return (3 + md_nv(la, lb) + 3) / 4; }
+__host__ __device__ constexpr int rec_words16_f64(int la, int lb) { return (2 + md_nv(la, lb) + 1) / 2; }
+constexpr int kRecMaxBytesF32 = 16 * rec_words16_f32(kMaxL, kMaxL);
+constexpr int kRecMaxBytesF64 = 16 * rec_words16_f64(kMaxL, kMaxL);
+static_assert(md_nv(3, 3) == 8 && md_nv(2, 3) == 6 && md_nv(1, 1) == 2 && md_nv(0, 1) == 1, "moment slots");
 
-// Work item: a shell pair (sa, sb), or a chunk of its output elements.
+// Work item: a shell pair (sa, sb).
 struct Item {
     int16_t cls;    // la*4 + lb
-    int16_t chunk;
+    int16_t chunk;  // 0 (reserved)
     int16_t sa, sb;
 };
 

@@ -104,7 +104,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
                           "cudaDeviceGetAttribute")) != AOK_OK)
         return fail(st);
     const size_t fsz = precision == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    const size_t ppsz = precision == AOK_PREC_F64 ? sizeof(PPd) : sizeof(PPf);
+    const size_t ppsz = precision == AOK_PREC_F64 ? kRecMaxBytesF64 : kRecMaxBytesF32;
     const size_t npairs = (size_t)(NZ * NZ * nshells * nshells);
     p->max_tiles = (int)((max_batch + kTileB - 1) / kTileB + NZ * NZ + 1);
     std::vector<int> ls32(nshells), boff32(nshells + 1);

@@ -74,41 +74,58 @@ __global__ void k_gb_pad(FT* __restrict__ zeta, FT* __restrict__ coef, const int
 // --------------------------------------------------------------------------
 // Primitive-pair records.
 // --------------------------------------------------------------------------
-__device__ __forceinline__ void fill_pp(PPf& r, double ca, double cb, double aa, double ab) {
+// w rb^al ra^be q^ga for the class's moment slots, in slot order.
+__device__ __forceinline__ int fill_monos(double* wm, int la, int lb, double w, double ra, double rb, double q) {
+    int j = 0;
+    for (int al = 0; al <= la; ++al)
+        for (int be = 0; be <= lb; ++be) {
+            if (((la - al) + (lb - be)) & 1) continue;
+            double v = w;
+            for (int k = 0; k < al; ++k) v *= rb;
+            for (int k = 0; k < be; ++k) v *= ra;
+            for (int k = 0; k < (la + lb - al - be) / 2; ++k) v *= q;
+            wm[j++] = v;
+        }
+    return j;
+}
+
+__device__ __forceinline__ void fill_pp(float* r, int la, int lb, double ca, double cb, double aa, double ab,
+                                        int rowlen) {
     const double p = aa + ab, ip = 1.0 / p;
     const double x = kPi * ip;
     const double log2e = 1.4426950408889634074;
     const double mu2 = ((aa * ab) * ip) * log2e;  // exponent in base 2
-    r.w = (float)(ca * cb * (x * sqrt(x)));
-    r.mu_hi = (float)mu2;
-    r.mu_lo = (float)(mu2 - (double)r.mu_hi);
-    r.ra = (float)(aa * ip);
-    r.rb = (float)(ab * ip);
-    r.oo2p = (float)(0.5 * ip);
-    r.flush = 0.f;
-    r.pad = 0.f;
+    double wm[8];
+    const int nv = fill_monos(wm, la, lb, ca * cb * (x * sqrt(x)), aa * ip, ab * ip, 0.5 * ip);
+    r[0] = (float)mu2;
+    r[1] = (float)(mu2 - (double)r[0]);
+    r[2] = (float)rowlen;
+    for (int j = 0; j < nv; ++j) r[3 + j] = (float)wm[j];
+    for (int j = 3 + nv; j < 4 * rec_words16_f32(la, lb); ++j) r[j] = 0.f;
 }
-__device__ __forceinline__ void fill_pp(PPd& r, double ca, double cb, double aa, double ab) {
-    double p = aa + ab;
-    double x = kPi / p;
-    r.w = ca * cb * (x * sqrt(x));
-    r.mu = aa * ab / p;
-    r.ra = aa / p;
-    r.rb = ab / p;
-    r.oo2p = 0.5 / p;
-    r.flush = 0.0;
-    r.pad0 = r.pad1 = 0.0;
+__device__ __forceinline__ void fill_pp(double* r, int la, int lb, double ca, double cb, double aa, double ab,
+                                        int rowlen) {
+    const double p = aa + ab;
+    const double x = kPi / p;
+    double wm[8];
+    const int nv = fill_monos(wm, la, lb, ca * cb * (x * sqrt(x)), aa / p, ab / p, 0.5 / p);
+    r[0] = aa * ab / p;
+    r[1] = (double)rowlen;
+    for (int j = 0; j < nv; ++j) r[2 + j] = wm[j];
+    for (int j = 2 + nv; j < 2 * rec_words16_f64(la, lb); ++j) r[j] = 0.0;
 }
+template <typename FT> __host__ __device__ constexpr int rec_words16(int la, int lb);
+template <> __host__ __device__ constexpr int rec_words16<float>(int la, int lb) { return rec_words16_f32(la, lb); }
+template <> __host__ __device__ constexpr int rec_words16<double>(int la, int lb) { return rec_words16_f64(la, lb); }
 
 // One warp per (species pair, shell pair); lanes sweep the K x K primitive
 // grid in ip-major order and compact the non-zero-coefficient pairs with a
-// ballot, preserving the reference's (ip, jp) summation order.  The record's
-// `flush` field carries the row length (the number of non-zero ket
-// coefficients): the records form rows of equal length, one per ip, and the
-// kernel folds its FP32 partial sums after each row.
+// ballot, preserving the reference's (ip, jp) summation order.  Records of a
+// shell pair are contiguous at the class's record size, starting at the
+// shell pair's region of K*K maximum-size records.
 template <typename FT>
-__global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restrict__ npp,
-                         const FT* __restrict__ zeta, const FT* __restrict__ coef, int ns, int K, int NZ) {
+__global__ void k_prep2c(FT* __restrict__ pp, int* __restrict__ npp, const FT* __restrict__ zeta,
+                         const FT* __restrict__ coef, const int* __restrict__ ls, int ns, int K, int NZ) {
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (q >= NZ * NZ * ns * ns) return;
@@ -117,7 +134,10 @@ __global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restric
     int sa = t % ns;
     t /= ns;
     int gb = t % NZ, ga = t / NZ;
-    auto* out = pp + (size_t)q * K * K;
+    const int la = ls[sa], lb = ls[sb];
+    constexpr int kMaxWords = sizeof(FT) == 4 ? kRecMaxBytesF32 / 4 : kRecMaxBytesF64 / 8;
+    const int words = rec_words16<FT>(la, lb) * (16 / (int)sizeof(FT));
+    FT* out = pp + (size_t)q * K * K * kMaxWords;
     int n = 0;
     // every row (ip with a non-zero coefficient) holds the same jp set
     int nb = 0;
@@ -134,11 +154,7 @@ __global__ void k_prep2c(typename PPT<FT>::type* __restrict__ pp, int* __restric
         }
         const bool valid = (e < K * K) && ca != 0.0 && cb != 0.0;
         const unsigned m = __ballot_sync(0xffffffffu, valid);
-        if (valid) {
-            auto& r = out[n + __popc(m & ((1u << lane) - 1u))];
-            fill_pp(r, ca, cb, aa, ab);
-            r.flush = (decltype(r.flush))nb;
-        }
+        if (valid) fill_pp(out + (size_t)(n + __popc(m & ((1u << lane) - 1u))) * words, la, lb, ca, cb, aa, ab, nb);
         n += __popc(m);
     }
     if (lane == 0) npp[q] = n;
@@ -337,8 +353,18 @@ __global__ void k_bin_identity(int B, int* __restrict__ perm, int4* __restrict__
 int setup_overlap2c_schedule(aok_plan* p) {
     const int ns = (int)p->ns, N = (int)p->N;
     const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    // FP32: two CTAs per SM; FP64: one (leaves room for the per-warp record buffers)
-    const size_t budget = (p->prec == AOK_PREC_F64 ? 148 : 96) * 1024;
+    // FP32: two CTAs per SM; FP64: one.  The slab shares the CTA's shared memory
+    // with the per-warp record buffers (K*K maximum-size records per warp); a
+    // basis whose widest shell column would not fit falls back to one CTA per SM.
+    const size_t recbuf = (size_t)8 * p->K * p->K * (p->prec == AOK_PREC_F64 ? kRecMaxBytesF64 : kRecMaxBytesF32);
+    size_t budget = p->prec == AOK_PREC_F64 ? (size_t)148 * 1024
+                                            : (size_t)112 * 1024 - std::min(recbuf, (size_t)112 * 1024);
+    {
+        size_t widest = 0;
+        for (int s = 0; s < ns; ++s) widest = std::max(widest, (size_t)ncart((int)p->ls[s]));
+        const size_t need = ((size_t)N * widest + 1) * kTileB * fsz;
+        if (budget < need) budget = (size_t)224 * 1024 - std::min(recbuf, (size_t)224 * 1024);
+    }
     // panels: consecutive ket shells whose column range fits the slab budget
     std::vector<int> pcols{0};
     std::vector<int> pshell{0};
@@ -434,11 +460,11 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
     int n = (int)(p->NZ * p->NZ * p->ns * p->ns);
     int th = 128, bl = (n * 32 + th - 1) / th;
     if (p->prec == AOK_PREC_F64)
-        k_prep2c<double><<<bl, th, 0, s>>>((PPd*)p->d_pp, p->d_npp, (const double*)zeta, (const double*)coef,
-                                           (int)p->ns, (int)p->K, (int)p->NZ);
+        k_prep2c<double><<<bl, th, 0, s>>>((double*)p->d_pp, p->d_npp, (const double*)zeta, (const double*)coef,
+                                           p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
     else
-        k_prep2c<float><<<bl, th, 0, s>>>((PPf*)p->d_pp, p->d_npp, (const float*)zeta, (const float*)coef,
-                                          (int)p->ns, (int)p->K, (int)p->NZ);
+        k_prep2c<float><<<bl, th, 0, s>>>((float*)p->d_pp, p->d_npp, (const float*)zeta, (const float*)coef,
+                                          p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_prep2c"));
     k_order2c<<<(int)(p->NZ * p->NZ), 256, 0, s>>>(p->d_order, p->d_order_id, p->d_items, p->d_npp, p->panels,
                                                   p->nitems, (int)p->ns);

@@ -223,6 +223,7 @@ template <typename FT, int LA, int LB>
 __device__ __noinline__ void pb_item(const typename PBT<FT>::type* __restrict__ pf, int nf,
                                      const typename PBT<FT>::type* __restrict__ pv, int nv, const Geo<FT> g,
                                      const FT* gslab, int N, FT* acc, int K, int lane) {
+    if (nf == 0 && nv == 0) return;  // absent shell: nothing to add
     FT G[(LA + 1) * (LB + 1)];
     md_cotangent<LA, LB, FT>(G, g.AB, gslab, N);
     // full pairs: value + both exponent derivatives

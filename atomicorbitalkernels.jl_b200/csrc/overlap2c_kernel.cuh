@@ -81,59 +81,59 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
-// --------------------------------------------------------------------------
-// Moments of one primitive pair: part[al*(LB+1)+be] += e00 rb^al ra^be q^ga for
-// the used slots (al + be + 2 ga = LA + LB).
-// --------------------------------------------------------------------------
+// Zero block (a shell pair with no primitive pair: an absent shell).
 template <int LA, int LB, typename FT>
-__device__ __forceinline__ void md_accumulate(FT (&part)[(LA + 1) * (LB + 1)], FT e00, FT ra, FT rb, FT q) {
-    constexpr int W = LA + LB;
-    FT rbp[LA + 1], rap[LB + 1], qp[W / 2 + 1];
-    rbp[0] = e00;
+__device__ __forceinline__ void md_zero(FT* dst, int N) {
 #pragma unroll
-    for (int k = 1; k <= LA; ++k) rbp[k] = rbp[k - 1] * rb;
-    rap[0] = FT(1);
+    for (int j = 0; j < ncart(LB); ++j)
 #pragma unroll
-    for (int k = 1; k <= LB; ++k) rap[k] = rap[k - 1] * ra;
-    qp[0] = FT(1);
-#pragma unroll
-    for (int k = 1; k <= W / 2; ++k) qp[k] = qp[k - 1] * q;
-#pragma unroll
-    for (int al = 0; al <= LA; ++al)
-#pragma unroll
-        for (int be = 0; be <= LB; ++be)
-            if (MdTab<LA, LB>::used(al, be)) {
-                const int m = al * (LB + 1) + be;
-                part[m] = fma(rbp[al] * rap[be], qp[(W - al - be) / 2], part[m]);
-            }
+        for (int i = 0; i < ncart(LA); ++i) dst[j * N + i] = FT(0);
 }
 
 // --------------------------------------------------------------------------
 // One work item (shell pair) for one lane (batch element): FP32C.
-// rec: shared-memory address of the item's n records, ip-major in rows of
-// equal length (the number of non-zero ket coefficients, record field 6).
-// dst points at the block's (0,0) element inside this lane's slab; element
-// (i, j) of the block lives at dst[j*N + i].  The moments are summed per ip
-// row in FP32 and folded into (hi, lo) with TwoSum at the end of each row.
+// rec: shared-memory address of the item's n records (class-sized, see
+// aok_common.cuh), ip-major in rows of equal length.  dst points at the
+// block's (0,0) element inside this lane's slab; element (i, j) of the block
+// lives at dst[j*N + i].  Moment m += exp(-mu R^2) * (w mono_m); the partial
+// sums of a row are folded into (hi, lo) with TwoSum at the end of the row.
 // --------------------------------------------------------------------------
 template <int LA, int LB>
 __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, float* dst, int N) {
-    constexpr int NM = (LA + 1) * (LB + 1);
+    constexpr int NM = (LA + 1) * (LB + 1), R16 = rec_words16_f32(LA, LB);
+    if (n == 0) {
+        md_zero<LA, LB, float>(dst, N);
+        return;
+    }
     float hi[NM], lo[NM], part[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) hi[m] = lo[m] = part[m] = 0.f;
-    const int rowlen = n > 0 ? (int)lds128(rec + 16).z : 1;
+    const int rowlen = (int)lds128(rec).z;
     for (int q0 = 0; q0 < n; q0 += rowlen) {
         for (int q = q0; q < q0 + rowlen; ++q) {
-            const float4 r0 = lds128(rec + 32u * q), r1 = lds128(rec + 32u * q + 16u);
-            // w, mu2 = mu log2(e) as hi + lo, a/p, b/p, 1/2p
-            const float w = r0.x, mu_hi = r0.y, mu_lo = r0.z, ra = r0.w, rb = r1.x, oo2p = r1.y;
-            // exp(-mu R^2) = 2^-(mu2 R^2), argument in double-float:
+            float r[4 * R16];
+#pragma unroll
+            for (int w = 0; w < R16; ++w) {
+                const float4 v = lds128(rec + 16u * (R16 * q + w));
+                r[4 * w] = v.x;
+                r[4 * w + 1] = v.y;
+                r[4 * w + 2] = v.z;
+                r[4 * w + 3] = v.w;
+            }
+            // exp(-mu R^2) = 2^-(mu2 R^2), argument in double-float (mu2 = r0 + r1):
             // 2^-(xh + xl) = 2^-xh (1 - ln2 xl) to first order in |xl| < 2^-20 xh
-            const float xh = mu_hi * g.R2;
-            const float xl = fmaf(mu_hi, g.R2, -xh) + fmaf(mu_lo, g.R2, mu_hi * g.R2lo);
-            const float e00 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
-            md_accumulate<LA, LB, float>(part, e00, ra, rb, oo2p);
+            const float xh = r[0] * g.R2;
+            const float xl = fmaf(r[0], g.R2, -xh) + fmaf(r[1], g.R2, r[0] * g.R2lo);
+            const float e = ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f);
+            int j = 0;
+#pragma unroll
+            for (int al = 0; al <= LA; ++al)
+#pragma unroll
+                for (int be = 0; be <= LB; ++be)
+                    if (MdTab<LA, LB>::used(al, be)) {
+                        part[al * (LB + 1) + be] = fmaf(e, r[3 + j], part[al * (LB + 1) + be]);
+                        ++j;
+                    }
         }
 #pragma unroll
         for (int m = 0; m < NM; ++m) {
@@ -152,15 +152,32 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, f
 // FP64 variant: plain double accumulation, records from shared memory.
 template <int LA, int LB>
 __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<double> g, double* dst, int N) {
-    constexpr int NM = (LA + 1) * (LB + 1);
+    constexpr int NM = (LA + 1) * (LB + 1), R16 = rec_words16_f64(LA, LB);
+    if (n == 0) {
+        md_zero<LA, LB, double>(dst, N);
+        return;
+    }
     double mom[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) mom[m] = 0.0;
     for (int q = 0; q < n; ++q) {
-        const double2 r0 = lds128d(rec + 64u * q), r1 = lds128d(rec + 64u * q + 16u),
-                      r2 = lds128d(rec + 64u * q + 32u);
-        const double w = r0.x, mu = r0.y, ra = r1.x, rb = r1.y, oo2p = r2.x;
-        md_accumulate<LA, LB, double>(mom, exp(-mu * g.R2) * w, ra, rb, oo2p);
+        double r[2 * R16];
+#pragma unroll
+        for (int w = 0; w < R16; ++w) {
+            const double2 v = lds128d(rec + 16u * (R16 * q + w));
+            r[2 * w] = v.x;
+            r[2 * w + 1] = v.y;
+        }
+        const double e = exp(-r[0] * g.R2);
+        int j = 0;
+#pragma unroll
+        for (int al = 0; al <= LA; ++al)
+#pragma unroll
+            for (int be = 0; be <= LB; ++be)
+                if (MdTab<LA, LB>::used(al, be)) {
+                    mom[al * (LB + 1) + be] = fma(e, r[2 + j], mom[al * (LB + 1) + be]);
+                    ++j;
+                }
     }
     md_transform<LA, LB, double>(mom, g.AB, dst, N);
 }
@@ -186,7 +203,7 @@ struct Ov2Params {
     const FT* posB;
     FT scale;
     int use_scale;
-    const typename PPT<FT>::type* pp;
+    const FT* pp;         // records: per (species pair, shell pair) a region of K*K maximum-size records
     const int* npp;
     const int* perm;
     const int4* tiles;
@@ -208,9 +225,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
     __shared__ int s_next[kMaxPanels];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = THREADS / 32;
-    constexpr int REC16 = sizeof(typename PPT<FT>::type) / 16;  // 16-byte words per record
+    constexpr int MAXREC16 = (sizeof(FT) == 4 ? kRecMaxBytesF32 : kRecMaxBytesF64) / 16;
     // per-warp staging buffer for the current item's records (K*K records)
-    float4* recbuf = reinterpret_cast<float4*>(smem_raw + P.rec_offset) + (size_t)warp * P.K * P.K * REC16;
+    float4* recbuf = reinterpret_cast<float4*>(smem_raw + P.rec_offset) + (size_t)warp * P.K * P.K * MAXREC16;
     const uint32_t rec_saddr = (uint32_t)__cvta_generic_to_shared(recbuf);
     const int ntiles = *P.ntiles;
     for (;;) {
@@ -244,8 +261,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                 const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
                 const int n = __ldg(P.npp + q);
                 {
-                    const float4* src = reinterpret_cast<const float4*>(P.pp + (size_t)q * P.K * P.K);
-                    for (int i = lane; i < n * REC16; i += 32) recbuf[i] = __ldg(src + i);
+                    const int rec16 = sizeof(FT) == 4 ? rec_words16_f32(wi.cls >> 2, wi.cls & 3)
+                                                      : rec_words16_f64(wi.cls >> 2, wi.cls & 3);
+                    const float4* src = reinterpret_cast<const float4*>(P.pp) + (size_t)q * P.K * P.K * MAXREC16;
+                    for (int i = lane; i < n * rec16; i += 32) recbuf[i] = __ldg(src + i);
                     __syncwarp();
                 }
                 FT* dst = sl + (size_t)(P.boff[wi.sb] - col0) * P.N + P.boff[wi.sa];
@@ -275,7 +294,7 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     P.posB = (const FT*)posB;
     P.scale = (FT)lengthscale;
     P.use_scale = (FT)lengthscale != FT(1);
-    P.pp = (const typename PPT<FT>::type*)p->d_pp;
+    P.pp = (const FT*)p->d_pp;
     P.npp = p->d_npp;
     P.perm = p->d_perm;
     P.tiles = p->d_tiles;
@@ -291,7 +310,8 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
     const size_t slab = (p->smem_bytes + 15) / 16 * 16;
     P.rec_offset = (unsigned)slab;
-    const size_t smem = slab + (size_t)(THREADS / 32) * p->K * p->K * sizeof(typename PPT<FT>::type);
+    const size_t smem = slab + (size_t)(THREADS / 32) * p->K * p->K * (sizeof(FT) == 4 ? kRecMaxBytesF32
+                                                                                         : kRecMaxBytesF64);
     auto kern = k_overlap2c<FT, THREADS, min_blocks<FT>()>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap2c)");
