@@ -37,9 +37,6 @@ struct aok_plan {
     int nitems = 0;
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
-    int* d_order_id = nullptr;       // static item id of each position of d_order (NZ*NZ*nitems)
-    int* d_pb_csr = nullptr;         // per (side, shell): static item ids, ascending (2*nitems)
-    std::vector<int> pb_csr_off;     // 2*(ns+1) offsets into d_pb_csr
     int max_bin_blocks = 0;
     aok::Panels panels{};
     size_t slab_stride = 0;          // elements per batch slot in the panel buffer
@@ -48,9 +45,11 @@ struct aok_plan {
     void* d_gb_zeta = nullptr;
     void* d_gb_coef = nullptr;
     // pullback: primitive-pair lists, per-warp FP64 partial rows, scratch coef
-    void* d_pb_full = nullptr;
-    void* d_pb_val = nullptr;
-    int2* d_pb_counts = nullptr;
+    void* d_pb_rec = nullptr;        // pullback records: per (species pair, shell pair) K*K
+    int4* d_pb_counts = nullptr;     // (na, nb, nza, nzb) per (species pair, shell pair)
+    void* d_pb_zeros = nullptr;      // N*N zeros (cotangent of lanes past a tile's end)
+    aok::Item* d_pb_order = nullptr; // per species pair: pullback items grouped by warp
+    int* d_pb_woff = nullptr;        // per species pair: warp offsets into d_pb_order
     void* d_partials = nullptr;      // per-CTA item sums
     void* d_tilerows = nullptr;      // per-tile FP64 rows
     int max_blocks = 0;

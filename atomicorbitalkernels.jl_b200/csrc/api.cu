@@ -143,8 +143,8 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
     void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_counter,
-                    p->d_err, p->d_items, p->d_order, p->d_order_id, p->d_pb_csr, p->d_blockhist,
-                    p->d_gb_zeta, p->d_gb_coef, p->d_pb_full, p->d_pb_val, p->d_pb_counts, p->d_partials,
+                    p->d_err, p->d_items, p->d_order, p->d_blockhist,
+                    p->d_gb_zeta, p->d_gb_coef, p->d_pb_rec, p->d_pb_counts, p->d_pb_zeros, p->d_pb_order, p->d_pb_woff, p->d_partials,
                     p->d_tilerows, p->d_coef_scratch, p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3,
                     p->d_npp3, p->d_items3};
     for (void* b : bufs) dfree(b);
@@ -270,9 +270,7 @@ static int overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void
     }
     if (!dS || !posA || !posB || !sidxA || !sidxB)
         return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
-    p->basis_set = false;
     AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
-    AOK_TRY(launch_prep2c(p, zeta, coef, s));
     return launch_overlap2c_pb(p, dcoef, dalpha, dS, zeta, coef, posA, posB, B, lengthscale, keep_absent, s);
 }
 

@@ -113,9 +113,14 @@ struct MdTab {
 
 // Number of terms of class (la, lb) (scheduling cost model).
 __host__ __device__ constexpr int md_terms(int la, int lb) {
-    constexpr int t[4][4] = {{1, 3, 9, 19}, {3, 12, 36, 84}, {9, 36, 111, 261}, {19, 84, 261, 632}};
-    return t[la][lb];
+    // symmetric in (la, lb); written as a branch chain so device code needs no table
+    return la > lb ? md_terms(lb, la)
+           : la == 0 ? (lb == 0 ? 1 : lb == 1 ? 3 : lb == 2 ? 9 : 19)
+           : la == 1 ? (lb == 1 ? 12 : lb == 2 ? 36 : 84)
+           : la == 2 ? (lb == 2 ? 111 : 261)
+                     : 632;
 }
+static_assert(md_terms(3, 1) == 84 && md_terms(2, 2) == 111 && md_terms(0, 3) == 19, "term counts");
 // table size = terms + one placeholder per block element no component maps to
 static_assert(MdTab<3, 3>::T == 632 + 27, "f-f term count");
 static_assert(MdTab<2, 2>::T == 111 + 5, "d-d term count");

@@ -170,18 +170,13 @@ __global__ void k_prep2c(FT* __restrict__ pp, int* __restrict__ npp, const FT* _
 constexpr int kOrderMax = 2048;
 
 
-__global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, int* __restrict__ order_id,
-                                                 const Item* __restrict__ items, const int* __restrict__ npp,
-                                                 Panels panels, int nitems, int ns) {
+__global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const Item* __restrict__ items,
+                                                 const int* __restrict__ npp, Panels panels, int nitems, int ns) {
     __shared__ unsigned long long key[kOrderMax];
     const int pair = blockIdx.x;
     Item* out = order + (size_t)pair * nitems;
-    int* out_id = order_id + (size_t)pair * nitems;
     if (nitems > kOrderMax) {  // very large bases: keep the static order
-        for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
-            out[i] = items[i];
-            out_id[i] = i;
-        }
+        for (int i = threadIdx.x; i < nitems; i += blockDim.x) out[i] = items[i];
         return;
     }
     for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
@@ -207,7 +202,6 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, int* 
             r += (kj < ki) || (kj == ki && j < i);
         }
         out[r] = items[i];
-        out_id[r] = i;
     }
 }
 
@@ -357,7 +351,7 @@ int setup_overlap2c_schedule(aok_plan* p) {
     // with the per-warp record buffers (K*K maximum-size records per warp); a
     // basis whose widest shell column would not fit falls back to one CTA per SM.
     const size_t recbuf = (size_t)8 * p->K * p->K * (p->prec == AOK_PREC_F64 ? kRecMaxBytesF64 : kRecMaxBytesF32);
-    size_t budget = p->prec == AOK_PREC_F64 ? (size_t)148 * 1024
+    size_t budget = p->prec == AOK_PREC_F64 ? (size_t)120 * 1024
                                             : (size_t)112 * 1024 - std::min(recbuf, (size_t)112 * 1024);
     {
         size_t widest = 0;
@@ -419,25 +413,8 @@ int setup_overlap2c_schedule(aok_plan* p) {
     p->max_bin_blocks = kBinMaxBlocks;
     e = cudaMalloc(&p->d_blockhist, sizeof(int) * p->max_bin_blocks * p->NZ * p->NZ);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(blockhist)");
-    e = cudaMalloc(&p->d_order_id, sizeof(int) * items.size() * p->NZ * p->NZ);
-    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(order_id)");
     e = cudaMemcpy(p->d_items, items.data(), sizeof(Item) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(items)");
-    // per shell and side, the static item ids whose bra (side 0) or ket (side 1)
-    // shell it is, ascending: the pullback sums its per-item partials along these
-    std::vector<int> csr;
-    p->pb_csr_off.assign(2 * (ns + 1), 0);
-    for (int side = 0; side < 2; ++side)
-        for (int s = 0; s < ns; ++s) {
-            p->pb_csr_off[side * (ns + 1) + s] = (int)csr.size();
-            for (int i = 0; i < (int)items.size(); ++i)
-                if ((side == 0 ? items[i].sa : items[i].sb) == s) csr.push_back(i);
-            p->pb_csr_off[side * (ns + 1) + s + 1] = (int)csr.size();
-        }
-    e = cudaMalloc(&p->d_pb_csr, sizeof(int) * csr.size());
-    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(pb_csr)");
-    e = cudaMemcpy(p->d_pb_csr, csr.data(), sizeof(int) * csr.size(), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(pb_csr)");
     return AOK_OK;
 }
 
@@ -466,8 +443,8 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
         k_prep2c<float><<<bl, th, 0, s>>>((float*)p->d_pp, p->d_npp, (const float*)zeta, (const float*)coef,
                                           p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_prep2c"));
-    k_order2c<<<(int)(p->NZ * p->NZ), 256, 0, s>>>(p->d_order, p->d_order_id, p->d_items, p->d_npp, p->panels,
-                                                  p->nitems, (int)p->ns);
+    k_order2c<<<(int)(p->NZ * p->NZ), 256, 0, s>>>(p->d_order, p->d_items, p->d_npp, p->panels, p->nitems,
+                                                  (int)p->ns);
     return cuda_status(cudaGetLastError(), "k_order2c");
 }
 
