@@ -12,6 +12,7 @@ constexpr int kMaxL = AOK_MAX_L;
 constexpr int kTileB = 32;          // batch elements per tile (one per lane)
 constexpr int kMaxPanels = 16;
 constexpr int kMaxShells = 64;
+constexpr int kMaxPairs = 256;     // species pairs (NZ <= 16)
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 

@@ -27,6 +27,7 @@ struct aok_plan {
     int* d_perm = nullptr;
     int4* d_tiles = nullptr;
     int* d_ntiles = nullptr;
+    int* d_tbase = nullptr;          // first tile of each species pair (NZ*NZ + 1)
     unsigned* d_counter = nullptr;
     int max_tiles = 0;
     // device error word (AOK_ERR_* of the first fault a kernel met)
@@ -47,11 +48,10 @@ struct aok_plan {
     // pullback: primitive-pair lists, per-warp FP64 partial rows, scratch coef
     void* d_pb_rec = nullptr;        // pullback records: per (species pair, shell pair) K*K
     int4* d_pb_counts = nullptr;     // (na, nb, nza, nzb) per (species pair, shell pair)
-    void* d_pb_zeros = nullptr;      // N*N zeros (cotangent of lanes past a tile's end)
-    aok::Item* d_pb_order = nullptr; // per species pair: pullback items grouped by warp
-    int* d_pb_woff = nullptr;        // per species pair: warp offsets into d_pb_order
+    aok::Item* d_pb_items = nullptr; // pullback items (one per shell pair), heaviest classes first
+    int* d_pb_itemidx = nullptr;     // (sa, sb) -> position in d_pb_items
+    void* d_pb_rows = nullptr;       // per (species pair, item): unit sums (FP64, 4*K)
     void* d_partials = nullptr;      // per-CTA item sums
-    void* d_tilerows = nullptr;      // per-tile FP64 rows
     int max_blocks = 0;
     void* d_coef_scratch = nullptr;  // ns*K*NZ
     void* d_dcoef_scratch = nullptr; // ns*K*NZ

@@ -117,6 +117,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
         (st = dmalloc(&p->d_perm, (size_t)max_batch, "cudaMalloc(perm)")) ||
         (st = dmalloc(&p->d_tiles, (size_t)p->max_tiles, "cudaMalloc(tiles)")) ||
         (st = dmalloc(&p->d_ntiles, 1, "cudaMalloc(ntiles)")) ||
+        (st = dmalloc(&p->d_tbase, (size_t)(NZ * NZ + 1), "cudaMalloc(tbase)")) ||
         (st = dmalloc(&p->d_counter, 1, "cudaMalloc(counter)")) ||
         (st = dmalloc(&p->d_err, 1, "cudaMalloc(err)")) ||
         (st = dmalloc_bytes(&p->d_gb_zeta, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_zeta)")) ||
@@ -142,10 +143,10 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
-    void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_counter,
+    void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter,
                     p->d_err, p->d_items, p->d_order, p->d_blockhist,
-                    p->d_gb_zeta, p->d_gb_coef, p->d_pb_rec, p->d_pb_counts, p->d_pb_zeros, p->d_pb_order, p->d_pb_woff, p->d_partials,
-                    p->d_tilerows, p->d_coef_scratch, p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3,
+                    p->d_gb_zeta, p->d_gb_coef, p->d_pb_rec, p->d_pb_counts, p->d_pb_items, p->d_pb_itemidx, p->d_pb_rows, p->d_partials,
+                    p->d_coef_scratch, p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3,
                     p->d_npp3, p->d_items3};
     for (void* b : bufs) dfree(b);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);

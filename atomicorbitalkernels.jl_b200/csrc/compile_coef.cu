@@ -64,8 +64,9 @@ __global__ void k_compile_coef(FT* __restrict__ coef, const FT* __restrict__ zet
         coef[base + (size_t)ns * m] = nsq > 0.0 ? (FT)((double)D[base + (size_t)ns * m] / n) : FT(0);
 }
 
-// one warp per (shell, species); lane m handles primitive slot m (K <= 32
-// per pass)
+// one warp per (shell, species): the K*K terms D_j / (z_m + z_j)^e (and the
+// same over (z_m + z_j)) are spread over the lanes, then lane m adds row m in
+// order j = 0..K-1
 template <typename FT>
 __global__ void k_compile_coef_pb(FT* __restrict__ dD, FT* __restrict__ dz, const FT* __restrict__ dcoef,
                                   const FT* __restrict__ zeta, const FT* __restrict__ D,
@@ -95,13 +96,22 @@ __global__ void k_compile_coef_pb(FT* __restrict__ dD, FT* __restrict__ dz, cons
     }
     const double n = sqrt(nsq);
     const double s2n3 = dot / (2.0 * ((n * n) * n));
+    extern __shared__ double terms[];  // per warp: [2][K*K]
+    double* tg = terms + (size_t)(threadIdx.x >> 5) * 2 * K * K;
+    double* th = tg + K * K;
+    for (int e2 = lane; e2 < K * K; e2 += 32) {
+        const int m = e2 / K, j = e2 % K;
+        const double den = zv(m) + zv(j);
+        const double p = pow_l32(den, l);
+        tg[e2] = Dv(j) / p;
+        th[e2] = Dv(j) / (p * den);
+    }
+    __syncwarp();
     for (int m = lane; m < K; m += 32) {
         double gm = 0.0, hm = 0.0;
         for (int j = 0; j < K; ++j) {
-            const double den = zv(m) + zv(j);
-            const double p = pow_l32(den, l);
-            gm += Dv(j) / p;
-            hm += Dv(j) / (p * den);
+            gm += tg[m * K + j];
+            hm += th[m * K + j];
         }
         gm *= 2.0 * c;
         hm *= ((-2.0 * c) * e) * Dv(m);
@@ -126,13 +136,15 @@ int launch_compile_coef(aok_plan* p, void* coef, const void* zeta, const void* D
 int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef, const void* zeta, const void* D,
                            const void* dalpha_add, cudaStream_t s) {
     int n = (int)(p->ns * p->NZ), th = 128, bl = (n * 32 + th - 1) / th;
+    const size_t sm = sizeof(double) * (th / 32) * 2 * p->K * p->K;
+    if (sm > 48 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "compile_coef pullback: K too large");
     if (p->prec == AOK_PREC_F64)
-        k_compile_coef_pb<double><<<bl, th, 0, s>>>((double*)dD, (double*)dzeta, (const double*)dcoef,
+        k_compile_coef_pb<double><<<bl, th, sm, s>>>((double*)dD, (double*)dzeta, (const double*)dcoef,
                                                     (const double*)zeta, (const double*)D,
                                                     (const double*)dalpha_add, p->d_ls, (int)p->ns, (int)p->K,
                                                     (int)p->NZ);
     else
-        k_compile_coef_pb<float><<<bl, th, 0, s>>>((float*)dD, (float*)dzeta, (const float*)dcoef,
+        k_compile_coef_pb<float><<<bl, th, sm, s>>>((float*)dD, (float*)dzeta, (const float*)dcoef,
                                                    (const float*)zeta, (const float*)D, (const float*)dalpha_add,
                                                    p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
     return cuda_status(cudaGetLastError(), "k_compile_coef_pb");

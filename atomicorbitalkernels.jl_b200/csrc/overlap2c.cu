@@ -218,7 +218,6 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
 // --------------------------------------------------------------------------
 constexpr int kBinThreads = 256;
 constexpr int kBinMaxBlocks = 128;
-constexpr int kMaxPairs = 256;
 
 __device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sidxB, int b, int B, int NZ, int* err) {
     if (b >= B) return -1;
@@ -252,7 +251,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
                                                               const int64_t* __restrict__ sidxB, int B, int NZ,
                                                               int chunk, const int* __restrict__ blockhist,
                                                               int* __restrict__ perm, int4* __restrict__ tiles,
-                                                              int* __restrict__ ntiles,
+                                                              int* __restrict__ ntiles, int* __restrict__ tbase_out,
                                                               unsigned* __restrict__ counter, int* __restrict__ err) {
     __shared__ int wcount[kBinWarps][kMaxPairs];
     __shared__ int before[kMaxPairs], tot[kMaxPairs], base[kMaxPairs], tbase[kMaxPairs + 1];
@@ -288,8 +287,10 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
             *counter = 0u;
         }
     }
-    // tiles: this block writes tiles me, me + nblk, ...
     __syncthreads();
+    if (me == 0)
+        for (int q = threadIdx.x; q <= np; q += blockDim.x) tbase_out[q] = tbase[q];
+    // tiles: this block writes tiles me, me + nblk, ...
     for (int t = me + (int)threadIdx.x * nblk; t < tbase[np]; t += blockDim.x * nblk) {
         int k = 0;
         while (tbase[k + 1] <= t) ++k;
@@ -329,13 +330,15 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
     }
 }
 
-__global__ void k_bin_identity(int B, int* __restrict__ perm, int4* __restrict__ tiles, int* __restrict__ ntiles,
-                               unsigned* __restrict__ counter) {
+__global__ void k_bin_identity(int B, int np, int* __restrict__ perm, int4* __restrict__ tiles,
+                               int* __restrict__ ntiles, int* __restrict__ tbase, unsigned* __restrict__ counter) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = (B + kTileB - 1) / kTileB;
     if (b < B) perm[b] = b;
     if (b * kTileB < B) tiles[b] = make_int4(0, b * kTileB, min(kTileB, B - b * kTileB), 0);
+    if (b <= np) tbase[b] = b == 0 ? 0 : nt;  // every element is in species pair 0
     if (b == 0) {
-        *ntiles = (B + kTileB - 1) / kTileB;
+        *ntiles = nt;
         *counter = 0u;
     }
 }
@@ -453,14 +456,15 @@ int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t 
     const int nblk = (int)((B + chunk - 1) / chunk);
     const int NZ = (int)p->NZ;
     if (NZ == 1 || (!sidxA && !sidxB)) {
-        k_bin_identity<<<(int)((B + 255) / 256), 256, 0, s>>>((int)B, p->d_perm, p->d_tiles, p->d_ntiles,
-                                                             p->d_counter);
+        const int np = NZ * NZ;
+        k_bin_identity<<<(int)((std::max<int64_t>(B, np + 1) + 255) / 256), 256, 0, s>>>(
+            (int)B, np, p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter);
         return cuda_status(cudaGetLastError(), "k_bin_identity");
     }
     k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, p->d_blockhist, p->d_err);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_bin_count"));
     k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, p->d_blockhist, p->d_perm,
-                                               p->d_tiles, p->d_ntiles, p->d_counter, p->d_err);
+                                               p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_err);
     return cuda_status(cudaGetLastError(), "k_bin_scatter");
 }
 

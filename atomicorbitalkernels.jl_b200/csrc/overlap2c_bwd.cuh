@@ -25,20 +25,26 @@
 // pullback discards that shell (overlap_2c_grad.jl:262); the kernel-level
 // pullback keeps them, so its dcoef matches the reference slot for slot.
 //
-// Records of a (species pair, shell pair), all row-structured:
-//   full   na rows (bra primitives with c_a != 0) x nb columns (c_b != 0)
-//   valA   nza rows (listed zero bra slots) x nb columns: feeds dcoef of the row
-//   valB   nzb rows (listed zero ket slots) x na columns: feeds dcoef of the row
-// Within a row the bra-side sums stay in registers; the ket-side sums of the
-// full list go to a small per-lane shared-memory column buffer.  Row and column
-// sums are added over the warp's 32 lanes by a fixed butterfly.
+// Records of a (species pair, shell pair), in one region of K*K records:
+//   full   na x nb pairs (c_a != 0, c_b != 0): value and both exponent derivatives
+//   valA   nza x nb pairs (listed zero bra slots): dcoef of the bra slot
+//   valB   nzb x na pairs (listed zero ket slots): dcoef of the ket slot
 //
-// Deterministic, no global atomics: items are assigned to warps statically
-// (item i of a panel to warp i mod NW), each warp adds its sums into its own
-// FP64 row of (side, kind, shell, k) slots in item order, the tile's row is the
-// sum of the warp rows in warp order, and k_pb_reduce sums the tile rows in
-// tile order.  With the stable species-pair binning every partial is
-// reproducible.
+// Record-parallel evaluation.  A work unit is (species pair, shell pair, chunk
+// of 4 tiles = 128 batch elements, group of <= 32 records).  For each 32 batch
+// elements the warp first puts lane = element and computes the cotangent
+// moments G_m(b) (md2c.cuh) into shared memory; then lane = record and the
+// warp loops over the elements accumulating
+//   S0_m = sum_b exp(-mu R_b^2) G_m(b),   S1_m = sum_b exp(-mu R_b^2) R_b^2 G_m(b),
+// (records fewer than 32 are replicated over the lanes, each copy taking every
+// r-th element; the copies are added by a fixed butterfly).  Everything that
+// depends on the primitive pair only (monomials, their exponent derivatives,
+// coefficients, pref0) is applied once per record and unit:
+//   V = pref0 sum_m mono_m S0_m,
+//   dV/da = pref0 [2q sum_m dmono_m/da' S0_m - 3q sum mono S0 - rb^2 sum mono S1].
+// Each unit writes its (dcoef, dalpha) for the bra and ket slots to its own
+// FP64 partial row; k_pb_reduce sums the partial rows in a fixed order, so
+// the result does not depend on which warp ran which unit.
 #pragma once
 
 #include "overlap2c_kernel.cuh"
@@ -156,9 +162,6 @@ __global__ void __launch_bounds__(32 * kPrepPbWarps)
     if (lane == 0) counts[q] = make_int4(na, nb, nza, nzb);
 }
 
-// Warps per pullback CTA and the largest item list k_pb_assign sorts.
-constexpr int kPbWarps = 8;
-constexpr int kAssignMax = 2048;
 
 // ---------------------------------------------------------------------------
 // Per primitive pair, from the cotangent moments G (md2c.cuh):
@@ -201,149 +204,50 @@ __device__ __forceinline__ void md_dual(const FT (&G)[(LA + 1) * (LB + 1)], FT r
             }
 }
 
-// Record fields from shared memory.
+constexpr int kPbWarps = 8;        // warps per pullback CTA
+constexpr int kPbChunkTiles = 4;   // tiles (of 32 batch elements) per work unit
+
+template <typename FT>
+__device__ __forceinline__ FT warp_sum_from(FT v, int first) {
+    // butterfly over the lane bits >= log2(first): adds the copies of a record
+    for (int o = first; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Record fields, loaded by the lane that owns the record.
 template <typename FT> struct PBLoad;
 template <> struct PBLoad<float> {
     float mu_hi, mu_lo, pref0, ca, cb, ra, rb, oo2p;
     int idx;
-    __device__ __forceinline__ void load(uint32_t a) {
-        const float4 x = lds128(a), y = lds128(a + 16u), z = lds128(a + 32u);
+    __device__ __forceinline__ void load(const PBf* r) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(r)), y = __ldg(reinterpret_cast<const float4*>(r) + 1),
+                     z = __ldg(reinterpret_cast<const float4*>(r) + 2);
         mu_hi = x.x; mu_lo = x.y; pref0 = x.z; ca = x.w;
         cb = y.x; ra = y.y; rb = y.z; oo2p = y.w;
         idx = (int)z.x;
     }
-    // pref0 * exp(-mu R^2), argument in double-float (as the forward)
-    __device__ __forceinline__ float pref(const Geo<float>& g) const {
-        const float xh = mu_hi * g.R2;
-        const float xl = fmaf(mu_hi, g.R2, -xh) + fmaf(mu_lo, g.R2, mu_hi * g.R2lo);
-        return (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * pref0;
+    __device__ __forceinline__ void zero() { mu_hi = mu_lo = pref0 = ca = cb = ra = rb = oo2p = 0.f; idx = 0; }
+    // exp(-mu R^2) with the argument in double-float (as the forward)
+    __device__ __forceinline__ float ex(float R2, float R2lo) const {
+        const float xh = mu_hi * R2;
+        const float xl = fmaf(mu_hi, R2, -xh) + fmaf(mu_lo, R2, mu_hi * R2lo);
+        return ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f);
     }
 };
 template <> struct PBLoad<double> {
     double mu, pref0, ca, cb, ra, rb, oo2p;
     int idx;
-    __device__ __forceinline__ void load(uint32_t a) {
-        const double2 x = lds128d(a), y = lds128d(a + 16u), z = lds128d(a + 32u), w = lds128d(a + 48u);
-        mu = x.x; pref0 = x.y; ca = y.x; cb = y.y; ra = z.x; rb = z.y; oo2p = w.x;
-        idx = (int)w.y;
+    __device__ __forceinline__ void load(const PBd* r) {
+        mu = r->mu; pref0 = r->pref0; ca = r->ca; cb = r->cb; ra = r->ra; rb = r->rb; oo2p = r->oo2p;
+        idx = (int)r->idx;
     }
-    __device__ __forceinline__ double pref(const Geo<double>& g) const { return exp(-mu * g.R2) * pref0; }
+    __device__ __forceinline__ void zero() { mu = pref0 = ca = cb = ra = rb = oo2p = 0.0; idx = 0; }
+    __device__ __forceinline__ double ex(double R2, double) const { return exp(-mu * R2); }
 };
-
-template <typename FT>
-__device__ __forceinline__ FT warp_sum(FT v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// One work item (shell pair) for one lane.  rec: shared-memory address of the
-// item's records; n = (na, nb, nza, nzb); colbuf: this warp's ket-side column
-// sums [2][K][33]; wrow: this warp's FP64 row, slot ((side*2 + kind)*ns + s)*K + k.
-template <typename FT, int LA, int LB>
-__device__ __noinline__ void pb_item(uint32_t rec, int4 n, const Geo<FT> g, const FT* gslab, int N, FT* colbuf,
-                                     double* wrow, int ns, int K, int sa, int sb, int lane) {
-    constexpr int RB = sizeof(typename PBT<FT>::type);
-    const int na = n.x, nb = n.y, nza = n.z, nzb = n.w;
-    if (na * nb + nza * nb + nzb * na == 0) return;  // absent shell: nothing to add
-    FT G[(LA + 1) * (LB + 1)];
-    md_cotangent<LA, LB, FT>(G, g.AB, gslab, N);
-    const int SK = ns * K;
-    // full list: value + both exponent derivatives
-    for (int r = 0; r < na; ++r) {
-        FT a0 = FT(0), a1 = FT(0);
-        int ip = 0;
-        for (int c = 0; c < nb; ++c) {
-            PBLoad<FT> R;
-            R.load(rec + (uint32_t)(RB * (r * nb + c)));
-            const FT P = R.pref(g);  // pref0 exp(-mu R^2)
-            FT T0, Ta, Tb;
-            md_dual<LA, LB, FT, true>(G, R.ra, R.rb, R.oo2p, T0, Ta, Tb);
-            const FT two_q = FT(2) * R.oo2p, kpre = FT(-3) * R.oo2p;  // -3/(2p)
-            const FT ka = kpre - g.R2 * (R.rb * R.rb), kb = kpre - g.R2 * (R.ra * R.ra);
-            const FT V = P * T0, cab = R.ca * R.cb * P;
-            a0 += R.cb * V;
-            a1 += cab * fma(two_q, Ta, ka * T0);
-            colbuf[(0 * K + c) * 33 + lane] += R.ca * V;
-            colbuf[(1 * K + c) * 33 + lane] += cab * fma(two_q, Tb, kb * T0);
-            ip = R.idx & 255;
-        }
-        a0 = warp_sum(a0);
-        a1 = warp_sum(a1);
-        if (lane == 0) {
-            wrow[(0 * 2 + 0) * SK + sa * K + ip] += (double)a0;
-            wrow[(0 * 2 + 1) * SK + sa * K + ip] += (double)a1;
-        }
-    }
-    if (na > 0) {
-        __syncwarp();
-        for (int c = 0; c < nb; ++c) {
-            const FT s0 = warp_sum(colbuf[(0 * K + c) * 33 + lane]), s1 = warp_sum(colbuf[(1 * K + c) * 33 + lane]);
-            colbuf[(0 * K + c) * 33 + lane] = FT(0);
-            colbuf[(1 * K + c) * 33 + lane] = FT(0);
-            PBLoad<FT> R;
-            R.load(rec + (uint32_t)(RB * c));
-            if (lane == 0) {
-                const int jp = R.idx >> 8;
-                wrow[(1 * 2 + 0) * SK + sb * K + jp] += (double)s0;
-                wrow[(1 * 2 + 1) * SK + sb * K + jp] += (double)s1;
-            }
-        }
-        __syncwarp();
-    }
-    // listed zero bra slots: dcoef of the row's slot only
-    uint32_t base = rec + (uint32_t)(RB * na * nb);
-    for (int r = 0; r < nza; ++r) {
-        FT a0 = FT(0);
-        int ip = 0;
-        for (int c = 0; c < nb; ++c) {
-            PBLoad<FT> R;
-            R.load(base + (uint32_t)(RB * (r * nb + c)));
-            FT T0, Ta, Tb;
-            md_dual<LA, LB, FT, false>(G, R.ra, R.rb, R.oo2p, T0, Ta, Tb);
-            a0 += R.cb * (R.pref(g) * T0);
-            ip = R.idx & 255;
-        }
-        a0 = warp_sum(a0);
-        if (lane == 0 && nb > 0) wrow[(0 * 2 + 0) * SK + sa * K + ip] += (double)a0;
-    }
-    // listed zero ket slots
-    base += (uint32_t)(RB * nza * nb);
-    for (int r = 0; r < nzb; ++r) {
-        FT b0 = FT(0);
-        int jp = 0;
-        for (int c = 0; c < na; ++c) {
-            PBLoad<FT> R;
-            R.load(base + (uint32_t)(RB * (r * na + c)));
-            FT T0, Ta, Tb;
-            md_dual<LA, LB, FT, false>(G, R.ra, R.rb, R.oo2p, T0, Ta, Tb);
-            b0 += R.ca * (R.pref(g) * T0);
-            jp = R.idx >> 8;
-        }
-        b0 = warp_sum(b0);
-        if (lane == 0 && na > 0) wrow[(1 * 2 + 0) * SK + sb * K + jp] += (double)b0;
-    }
-}
-
-template <typename FT>
-__device__ __forceinline__ void pb_dispatch(int cls, uint32_t rec, int4 n, const Geo<FT>& g, const FT* gs, int N,
-                                            FT* colbuf, double* wrow, int ns, int K, int sa, int sb, int lane) {
-    switch (cls) {
-#define AOK_PB_CASE(LA, LB) \
-    case (LA) * 4 + (LB): pb_item<FT, LA, LB>(rec, n, g, gs, N, colbuf, wrow, ns, K, sa, sb, lane); break;
-        AOK_PB_CASE(0, 0) AOK_PB_CASE(0, 1) AOK_PB_CASE(0, 2) AOK_PB_CASE(0, 3)
-        AOK_PB_CASE(1, 0) AOK_PB_CASE(1, 1) AOK_PB_CASE(1, 2) AOK_PB_CASE(1, 3)
-        AOK_PB_CASE(2, 0) AOK_PB_CASE(2, 1) AOK_PB_CASE(2, 2) AOK_PB_CASE(2, 3)
-        AOK_PB_CASE(3, 0) AOK_PB_CASE(3, 1) AOK_PB_CASE(3, 2) AOK_PB_CASE(3, 3)
-#undef AOK_PB_CASE
-        default: break;
-    }
-}
 
 template <typename FT>
 struct PbParams {
     const FT* dS;
-    const FT* zeros;   // N*N zeros: the cotangent seen by lanes past a tile's end
     const FT* posA;
     const FT* posB;
     FT scale;
@@ -352,171 +256,286 @@ struct PbParams {
     const int4* counts;
     const int* perm;
     const int4* tiles;
-    const int* ntiles;
-    unsigned* counter;
-    const Item* items;    // per pair: items grouped by warp (k_pb_assign)
-    const int* woff;      // per pair: kPbWarps + 1 offsets
-    int nitems;
-    double* grows;     // per (CTA, warp) rows in global memory when they do not fit in shared memory
-    double* tilerows;  // [tile][4 * ns * K]: (side, kind, shell, k)
+    const int* tbase;      // first tile of each species pair (np + 1)
+    unsigned* counter;     // unit queue
+    const Item* items;     // static pullback item list, heaviest classes first
+    int nitems, np, gmax;  // gmax: record groups per item (ceil(K*K / 32))
+    double* partial;       // [unit][4][K]: bra dcoef, bra dalpha, ket dcoef, ket dalpha
     int ns, K, NZ, N;
-    unsigned col_offset, row_offset;  // byte offsets in dynamic shared memory (records at 0)
     int boff[kMaxShells + 1];
 };
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+// Per-warp shared memory: the 32 elements' cotangent moments and R^2, and the
+// records' results for the slot sums.
+template <typename FT>
+struct PbWarpSmem {
+    FT G[32][9];    // used moment slots (<= 8) per element, odd stride
+    FT R2[32], R2lo[32];
+    FT val[32][4];
+    int slotA[32], slotB[32];
+};
+
+template <typename FT>
+struct Sums4 {
+    FT a0, a1, b0, b1;  // bra dcoef, bra dalpha, ket dcoef, ket dalpha of slot k = lane
+};
+
+// One unit: records [32 g, 32 g + ng) of item (sa, sb) over elements
+// perm[e0, e1).  Lanes k < K return the unit's sums for slot k.
+template <typename FT, int LA, int LB>
+__device__ __noinline__ Sums4<FT> pb_unit(const PbParams<FT>& P, PbWarpSmem<FT>& W, int q, int4 n, int sa, int sb,
+                                          int g, int e0, int e1, int lane) {
+    constexpr int NM = (LA + 1) * (LB + 1), NV = md_nv(LA, LB);
+    const int na = n.x, nb = n.y, nza = n.z, nzb = n.w;
+    const int nrec = na * nb + nza * nb + nzb * na;
+    const int ng = min(32, nrec - 32 * g);
+    int npad = 1;
+    while (npad < ng) npad <<= 1;
+    const int reps = 32 / npad;
+    const int r = 32 * g + (lane & (npad - 1)), rep = lane / npad;
+    const bool own = (lane & (npad - 1)) < ng;
+    PBLoad<FT> R;
+    if (own) R.load(P.rec + (size_t)q * P.K * P.K + r);
+    else R.zero();
+    FT S0[NM], S1[NM];
+#pragma unroll
+    for (int m = 0; m < NM; ++m) S0[m] = S1[m] = FT(0);
+    for (int c0 = e0; c0 < e1; c0 += 32) {
+        // phase A: lane = element; cotangent moments of its block
+        {
+            const int e = c0 + lane;
+            FT G[NM];
+            FT R2 = FT(0), R2lo = FT(0);
+            if (e < e1) {
+                const int b = P.perm[e];
+                Geo<FT> geo;
+                load_geo(geo, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
+                const FT* gs = P.dS + (size_t)b * P.N * P.N + (size_t)P.boff[sb] * P.N + P.boff[sa];
+                md_cotangent<LA, LB, FT>(G, geo.AB, gs, P.N);
+                R2 = geo.R2;
+                if constexpr (sizeof(FT) == 4) R2lo = geo.R2lo;
+            } else {
+#pragma unroll
+                for (int m = 0; m < NM; ++m) G[m] = FT(0);
+            }
+            int j = 0;
+#pragma unroll
+            for (int al = 0; al <= LA; ++al)
+#pragma unroll
+                for (int be = 0; be <= LB; ++be)
+                    if (MdTab<LA, LB>::used(al, be)) W.G[lane][j++] = G[al * (LB + 1) + be];
+            W.R2[lane] = R2;
+            W.R2lo[lane] = R2lo;
+        }
+        __syncwarp();
+        // phase B: lane = record (copy `rep` of it takes elements rep, rep + reps, ...)
+        const int ne = min(32, e1 - c0);
+        for (int t = rep; t < ne; t += reps) {
+            const FT x = R.ex(W.R2[t], W.R2lo[t]);
+            const FT xr = x * W.R2[t];
+            int j = 0;
+#pragma unroll
+            for (int al = 0; al <= LA; ++al)
+#pragma unroll
+                for (int be = 0; be <= LB; ++be)
+                    if (MdTab<LA, LB>::used(al, be)) {
+                        const FT Gm = W.G[t][j++];
+                        S0[al * (LB + 1) + be] = fma(x, Gm, S0[al * (LB + 1) + be]);
+                        S1[al * (LB + 1) + be] = fma(xr, Gm, S1[al * (LB + 1) + be]);
+                    }
+        }
+        __syncwarp();
+    }
+    (void)NV;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        S0[m] = warp_sum_from(S0[m], npad);
+        S1[m] = warp_sum_from(S1[m], npad);
+    }
+    // per record: geometry-free factors, once
+    FT vA0 = FT(0), vA1 = FT(0), vB0 = FT(0), vB1 = FT(0);
+    int slotA = -1, slotB = -1;
+    if (own && rep == 0) {
+        FT T0, Ta, Tb, U, u1, u2;
+        md_dual<LA, LB, FT, true>(S0, R.ra, R.rb, R.oo2p, T0, Ta, Tb);
+        md_dual<LA, LB, FT, false>(S1, R.ra, R.rb, R.oo2p, U, u1, u2);
+        const FT V = R.pref0 * T0;
+        const int ip = R.idx & 255, jp = R.idx >> 8;
+        if (r < na * nb) {
+            const FT two_q = FT(2) * R.oo2p, m3q = FT(-3) * R.oo2p, cab = R.ca * R.cb * R.pref0;
+            vA0 = R.cb * V;
+            vA1 = cab * (two_q * Ta + m3q * T0 - (R.rb * R.rb) * U);
+            vB0 = R.ca * V;
+            vB1 = cab * (two_q * Tb + m3q * T0 - (R.ra * R.ra) * U);
+            slotA = ip;
+            slotB = jp;
+        } else if (r < na * nb + nza * nb) {
+            vA0 = R.cb * V;
+            slotA = ip;
+        } else {
+            vB0 = R.ca * V;
+            slotB = jp;
+        }
+    }
+    W.val[lane][0] = vA0;
+    W.val[lane][1] = vA1;
+    W.val[lane][2] = vB0;
+    W.val[lane][3] = vB1;
+    W.slotA[lane] = slotA;
+    W.slotB[lane] = slotB;
+    __syncwarp();
+    Sums4<FT> res{FT(0), FT(0), FT(0), FT(0)};
+    if (lane < P.K) {
+        for (int l = 0; l < npad; ++l) {
+            if (W.slotA[l] == lane) {
+                res.a0 += W.val[l][0];
+                res.a1 += W.val[l][1];
+            }
+            if (W.slotB[l] == lane) {
+                res.b0 += W.val[l][2];
+                res.b1 += W.val[l][3];
+            }
+        }
+    }
+    __syncwarp();
+    return res;
 }
 
-// Persistent kernel over tiles (32 batch elements of one species pair).  Each
-// lane reads its cotangent blocks directly from global memory (contiguous runs
-// of a block column), so there is no shared panel and no barrier inside a
-// tile.  Each warp runs its own list of the pair's items (k_pb_assign); the
-// next item's records are copied into shared memory (cp.async,
-// double-buffered) while the current one runs.
+template <typename FT>
+__device__ __forceinline__ Sums4<FT> pb_dispatch(int cls, const PbParams<FT>& P, PbWarpSmem<FT>& W, int q, int4 n,
+                                                 int sa, int sb, int g, int e0, int e1, int lane) {
+    switch (cls) {
+#define AOK_PB_CASE(LA, LB) \
+    case (LA) * 4 + (LB): return pb_unit<FT, LA, LB>(P, W, q, n, sa, sb, g, e0, e1, lane);
+        AOK_PB_CASE(0, 0) AOK_PB_CASE(0, 1) AOK_PB_CASE(0, 2) AOK_PB_CASE(0, 3)
+        AOK_PB_CASE(1, 0) AOK_PB_CASE(1, 1) AOK_PB_CASE(1, 2) AOK_PB_CASE(1, 3)
+        AOK_PB_CASE(2, 0) AOK_PB_CASE(2, 1) AOK_PB_CASE(2, 2) AOK_PB_CASE(2, 3)
+        AOK_PB_CASE(3, 0) AOK_PB_CASE(3, 1) AOK_PB_CASE(3, 2) AOK_PB_CASE(3, 3)
+#undef AOK_PB_CASE
+        default: return Sums4<FT>{FT(0), FT(0), FT(0), FT(0)};
+    }
+}
+
+// Unit numbering.  Species pair k has nch_k = ceil(tiles_k / kPbChunkTiles)
+// chunks; chpre = prefix of nch over the pairs (NCH = total).
+//   storage id:  ((chpre[k] + j) * nitems + i) * gmax + g
+//   queue order: item i outermost (heaviest classes first), then (k, j), then g.
+__device__ __forceinline__ int pb_nch(const int* tbase, int k) {
+    return (tbase[k + 1] - tbase[k] + kPbChunkTiles - 1) / kPbChunkTiles;
+}
+
 template <typename FT, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c_pb(const __grid_constant__ PbParams<FT> P) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NW = THREADS / 32;
-    constexpr int REC = sizeof(typename PBT<FT>::type), REC16 = REC / 16;
+    __shared__ int chpre[kMaxPairs + 1];
+    __shared__ PbWarpSmem<FT> wsm[NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int R = 4 * P.ns * P.K, KK = P.K * P.K;
-    // two record buffers per warp
-    const uint32_t rec0 = (uint32_t)__cvta_generic_to_shared(smem_raw) + (uint32_t)(2 * warp * KK * REC);
-    FT* colbuf = reinterpret_cast<FT*>(smem_raw + P.col_offset) + (size_t)warp * 2 * P.K * 33;
-    double* rows = P.grows ? P.grows + (size_t)blockIdx.x * NW * R : reinterpret_cast<double*>(smem_raw + P.row_offset);
-    double* wrow = rows + (size_t)warp * R;
-    __shared__ int s_tile;
-    for (int i = lane; i < 2 * P.K * 33; i += 32) colbuf[i] = FT(0);
-    const int ntiles = *P.ntiles;
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < P.np; ++k) {
+            chpre[k] = acc;
+            acc += pb_nch(P.tbase, k);
+        }
+        chpre[P.np] = acc;
+    }
+    __syncthreads();
+    const int NCH = chpre[P.np];
+    const long long total = (long long)NCH * P.nitems * P.gmax;
     for (;;) {
-        if (threadIdx.x == 0) s_tile = (int)atomicAdd(P.counter, 1u);
-        __syncthreads();
-        const int tile = s_tile;
-        if (tile >= ntiles) break;
-        for (int i = lane; i < R; i += 32) wrow[i] = 0.0;
-        __syncwarp();
-        const int4 td = P.tiles[tile];
-        const int pair = td.x, start = td.y, cnt = td.z;
-        Geo<FT> g;
-        const FT* gbase = P.zeros;
-        if (lane < cnt) {
-            const int b = P.perm[start + lane];
-            load_geo(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
-            gbase = P.dS + (size_t)b * P.N * P.N;
-        } else {
-            const FT z[3] = {FT(0), FT(0), FT(0)};
-            load_geo(g, z, z, P.scale, false);
-        }
-        const Item* order = P.items + (size_t)pair * P.nitems;
-        const int w0 = P.woff[pair * (kPbWarps + 1) + warp], w1 = P.woff[pair * (kPbWarps + 1) + warp + 1];
-        auto issue = [&](int it, uint32_t dst) {
-            const Item wi = order[it];
-            const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
-            const int4 n = P.counts[q];
-            const int nrec = n.x * n.y + n.z * n.y + n.w * n.x;
-            const float4* src = reinterpret_cast<const float4*>(P.rec + (size_t)q * KK);
-            for (int i = lane; i < nrec * REC16; i += 32) cp_async16(dst + 16u * i, src + i);
-        };
+        long long u = 0;
+        if (lane == 0) u = (long long)atomicAdd(P.counter, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= total) break;
+        const int g = (int)(u % P.gmax);
+        const long long kj_i = u / P.gmax;
+        const int i = (int)(kj_i / NCH), kj = (int)(kj_i % NCH);
         int k = 0;
-        if (w0 < w1) issue(w0, rec0);
-        cp_async_commit();
-        for (int it = w0; it < w1; ++it, ++k) {
-            const uint32_t cur = rec0 + (uint32_t)((k & 1) * KK * REC);
-            if (it + 1 < w1) issue(it + 1, rec0 + (uint32_t)(((k + 1) & 1) * KK * REC));
-            cp_async_commit();
-            cp_async_wait<1>();
-            __syncwarp();
-            const Item wi = order[it];
-            const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
-            const FT* gs = gbase + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-            pb_dispatch<FT>(wi.cls, cur, P.counts[q], g, gs, P.N, colbuf, wrow, P.ns, P.K, wi.sa, wi.sb, lane);
-            __syncwarp();
-        }
-        cp_async_wait<0>();
-        __syncthreads();
-        // the tile's row: the warp rows summed in warp order
-        double* trow = P.tilerows + (size_t)tile * R;
-        for (int t = threadIdx.x; t < R; t += blockDim.x) {
-            double sum = 0.0;
-            for (int w = 0; w < NW; ++w) sum += rows[(size_t)w * R + t];
-            trow[t] = sum;
+        while (chpre[k + 1] <= kj) ++k;
+        const int j = kj - chpre[k];
+        const Item wi = P.items[i];
+        const int q = (k * P.ns + wi.sa) * P.ns + wi.sb;
+        const int4 n = P.counts[q];
+        const int nrec = n.x * n.y + n.z * n.y + n.w * n.x;
+        if (32 * g >= nrec) continue;  // empty unit: k_pb_reduce skips it
+        const int t0 = P.tbase[k] + j * kPbChunkTiles, t1 = min(t0 + kPbChunkTiles, P.tbase[k + 1]);
+        const int e0 = P.tiles[t0].y, e1 = P.tiles[t1 - 1].y + P.tiles[t1 - 1].z;
+        const Sums4<FT> res = pb_dispatch<FT>(wi.cls, P, wsm[warp], q, n, wi.sa, wi.sb, g, e0, e1, lane);
+        if (lane < P.K) {
+            double* out = P.partial + ((((size_t)(chpre[k] + j) * P.nitems + i) * P.gmax + g) * 4) * P.K;
+            out[0 * P.K + lane] = (double)res.a0;
+            out[1 * P.K + lane] = (double)res.a1;
+            out[2 * P.K + lane] = (double)res.b0;
+            out[3 * P.K + lane] = (double)res.b1;
         }
     }
 }
 
-// Fixed-order sum of the tile rows: out[kind][(s, k, sigma)].
-// Grid (column groups of 32, NZ): lane = column (kind, s, k) of species sigma,
-// warp w sums tiles w, w + NW, ... in order (both sides), and warp 0 adds the
-// NW partials in warp order, so the result does not depend on scheduling.
-constexpr int kPbReduceThreads = 512;
+// Fixed-order sums of the unit partials, in two stages.
+// k_pb_sum_units: one warp per (species pair k, item i); lane = (value v, slot
+// kk); sums the item's units over chunks j, then record groups g (empty units
+// skipped) into rows[k][i][4][K] (zeros for an item without records).
+static __global__ void k_pb_sum_units(double* __restrict__ rows, const double* __restrict__ partial,
+                                      const int4* __restrict__ counts, const int* __restrict__ tbase,
+                                      const Item* __restrict__ items, int ns, int K, int np, int nitems, int gmax) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wid >= np * nitems) return;
+    const int k = wid / nitems, i = wid % nitems;
+    int chbase = 0;
+    for (int k2 = 0; k2 < k; ++k2) chbase += pb_nch(tbase, k2);
+    const int nch = pb_nch(tbase, k);
+    const Item wi = items[i];
+    const int4 n = counts[((size_t)k * ns + wi.sa) * ns + wi.sb];
+    const int nrec = n.x * n.y + n.z * n.y + n.w * n.x;
+    const int ng = (nrec + 31) / 32;
+    double* out = rows + ((size_t)k * nitems + i) * 4 * K;
+    for (int c = lane; c < 4 * K; c += 32) {
+        double sum = 0.0;
+        for (int j = 0; j < nch; ++j)
+            for (int g = 0; g < ng; ++g)
+                sum += partial[((((size_t)(chbase + j) * nitems + i) * gmax + g) * 4) * K + c];
+        out[c] = sum;
+    }
+}
 
+// k_pb_reduce: one warp per output slot (kind, s, kk, sigma); lanes take the
+// (side, species pair, other shell) rows in a fixed strided order and a fixed
+// butterfly adds the lanes.  Zero slots with equal exponents take the first
+// one's value (k_prep_pb lists the first only).
 template <typename FT>
-__global__ void __launch_bounds__(kPbReduceThreads) k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha,
-                                                                const double* __restrict__ tilerows,
-                                                                const int4* __restrict__ tiles,
-                                                                const int* __restrict__ ntiles,
-                                                                const FT* __restrict__ zeta,
-                                                                const FT* __restrict__ coef, int ns, int K, int NZ) {
-    constexpr int NW = kPbReduceThreads / 32;
-    __shared__ double part[NW][33];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int sigma = blockIdx.y, SK = ns * K;
-    const int col = blockIdx.x * 32 + lane;  // kind * SK + s * K + k
-    const bool valid = col < 2 * SK;
-    const int kind = valid ? col / SK : 0, s = valid ? (col % SK) / K : 0;
-    int k = valid ? col % K : 0;
-    const int slot = s + ns * (k + K * sigma);
-    if (valid && kind == 0 && coef[slot] == FT(0)) {
-        // zero slots with equal exponents share the first one's value (k_prep_pb
-        // lists the first only)
+__global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, const double* __restrict__ rows,
+                            const int* __restrict__ itemidx, const FT* __restrict__ zeta, const FT* __restrict__ coef,
+                            int ns, int K, int NZ, int nitems) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int S = ns * K * NZ;
+    if (wid >= 2 * S) return;
+    const int kind = wid / S, slot = wid % S;
+    const int s = slot % ns, sigma = slot / (ns * K);
+    int kk = (slot / ns) % K;
+    if (kind == 0 && coef[slot] == FT(0)) {
         const FT z = zeta[slot];
-        for (int k2 = 0; k2 < k; ++k2) {
+        for (int k2 = 0; k2 < kk; ++k2) {
             const int o = s + ns * (k2 + K * sigma);
             if (coef[o] == FT(0) && zeta[o] == z) {
-                k = k2;
+                kk = k2;
                 break;
             }
         }
     }
-    const int nt = *ntiles, R = 4 * SK;
-    const int c0 = (0 * 2 + kind) * SK + s * K + k, c1 = (1 * 2 + kind) * SK + s * K + k;
     double sum = 0.0;
-    if (valid) {
-        // four tiles' loads in flight at a time; the additions stay in tile order
-        int tile = warp;
-        for (; tile + 3 * NW < nt; tile += 4 * NW) {
-            double v[8];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int pair = tiles[tile + u * NW].x;
-                const double* row = tilerows + (size_t)(tile + u * NW) * R;
-                v[2 * u] = pair / NZ == sigma ? row[c0] : 0.0;
-                v[2 * u + 1] = pair % NZ == sigma ? row[c1] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) sum += v[u];
-        }
-        for (; tile < nt; tile += NW) {
-            const int pair = tiles[tile].x;
-            const double* row = tilerows + (size_t)tile * R;
-            if (pair / NZ == sigma) sum += row[c0];
-            if (pair % NZ == sigma) sum += row[c1];
-        }
+    for (int w = lane; w < 2 * NZ * ns; w += 32) {
+        const int side = w / (NZ * ns), other = (w / ns) % NZ, o = w % ns;
+        const int k = side == 0 ? sigma * NZ + other : other * NZ + sigma;
+        const int i = side == 0 ? itemidx[s * ns + o] : itemidx[o * ns + s];
+        sum += rows[((size_t)k * nitems + i) * 4 * K + (side * 2 + kind) * K + kk];
     }
-    part[warp][lane] = sum;
-    __syncthreads();
-    if (warp == 0 && valid) {
-        double tot = 0.0;
-        for (int w = 0; w < NW; ++w) tot += part[w][lane];
-        const int out = s + ns * (((col % SK) % K) + K * sigma);
-        if (kind == 0) dcoef[out] = (FT)tot;
-        else dalpha[out] = (FT)tot;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) {
+        const int out = s + ns * (((slot / ns) % K) + K * sigma);
+        if (kind == 0) dcoef[out] = (FT)sum;
+        else dalpha[out] = (FT)sum;
     }
 }
 
@@ -527,12 +546,10 @@ template <typename FT> constexpr int pb_min_blocks() { return sizeof(FT) == 4 ? 
 template <typename FT, int THREADS>
 inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
                      const void* posA, const void* posB, double lengthscale, cudaStream_t s) {
-    constexpr int NW = THREADS / 32;
     constexpr int MINB = pb_min_blocks<FT>();
     PbParams<FT> P;
     memset(&P, 0, sizeof(P));
     P.dS = (const FT*)dS;
-    P.zeros = (const FT*)p->d_pb_zeros;
     P.posA = (const FT*)posA;
     P.posB = (const FT*)posB;
     P.scale = (FT)lengthscale;
@@ -541,43 +558,32 @@ inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, con
     P.counts = p->d_pb_counts;
     P.perm = p->d_perm;
     P.tiles = p->d_tiles;
-    P.ntiles = p->d_ntiles;
+    P.tbase = p->d_tbase;
     P.counter = p->d_counter;
-    P.items = p->d_pb_order;
-    P.woff = p->d_pb_woff;
+    P.items = p->d_pb_items;
     P.nitems = p->nitems;
-    P.tilerows = (double*)p->d_tilerows;
+    P.np = (int)(p->NZ * p->NZ);
+    P.gmax = (int)((p->K * p->K + 31) / 32);
+    P.partial = (double*)p->d_partials;
     P.ns = (int)p->ns;
     P.K = (int)p->K;
     P.NZ = (int)p->NZ;
     P.N = (int)p->N;
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
-    // dynamic shared memory: record buffers (2 per warp) | column buffers | warp rows
-    auto up16 = [](size_t x) { return (x + 15) / 16 * 16; };
-    const size_t recs = up16((size_t)NW * 2 * p->K * p->K * sizeof(typename PBT<FT>::type));
-    const size_t cols = up16((size_t)NW * 2 * p->K * 33 * sizeof(FT));
-    const size_t rows = (size_t)NW * 4 * p->ns * p->K * sizeof(double);
-    const size_t cap = (size_t)(MINB == 2 ? 112 : 224) * 1024;
-    P.col_offset = (unsigned)recs;
-    P.row_offset = (unsigned)(recs + cols);
-    size_t smem = recs + cols + rows;
-    if (smem > cap) {  // warp rows in global memory instead
-        smem = recs + cols;
-        if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "pullback: shared-memory budget exceeded");
-        P.grows = (double*)p->d_partials;
-    }
     auto kern = k_overlap2c_pb<FT, THREADS, MINB>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap2c_pb)");
-    const int grid = p->num_sms * MINB;
     timing_begin(p, s);
-    kern<<<grid, THREADS, smem, s>>>(P);
+    kern<<<p->num_sms * MINB, THREADS, 0, s>>>(P);
     timing_end(p, s);
     AOK_TRY_PB(cuda_status(cudaGetLastError(), "k_overlap2c_pb"));
-    const dim3 rgrid((unsigned)((2 * p->ns * p->K + 31) / 32), (unsigned)p->NZ);
-    k_pb_reduce<FT><<<rgrid, kPbReduceThreads, 0, s>>>((FT*)dcoef, (FT*)dalpha, (const double*)p->d_tilerows,
-                                                       p->d_tiles, p->d_ntiles, (const FT*)zeta,
-                                                       (const FT*)coef, (int)p->ns, (int)p->K, (int)p->NZ);
+    const int nw1 = P.np * p->nitems;
+    k_pb_sum_units<<<(nw1 * 32 + 255) / 256, 256, 0, s>>>((double*)p->d_pb_rows, (const double*)p->d_partials,
+                                                         p->d_pb_counts, p->d_tbase, p->d_pb_items, (int)p->ns,
+                                                         (int)p->K, P.np, p->nitems, P.gmax);
+    AOK_TRY_PB(cuda_status(cudaGetLastError(), "k_pb_sum_units"));
+    const int S = (int)(p->ns * p->K * p->NZ);
+    k_pb_reduce<FT><<<(2 * S * 32 + 255) / 256, 256, 0, s>>>((FT*)dcoef, (FT*)dalpha, (const double*)p->d_pb_rows,
+                                                            p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
+                                                            (int)p->ns, (int)p->K, (int)p->NZ, p->nitems);
     return cuda_status(cudaGetLastError(), "k_pb_reduce");
 }
 
