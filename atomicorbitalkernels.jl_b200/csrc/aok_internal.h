@@ -54,8 +54,6 @@ struct aok_plan {
     void* d_partials = nullptr;      // per-CTA item sums
     int max_blocks = 0;
     void* d_coef_scratch = nullptr;  // ns*K*NZ
-    void* d_dcoef_scratch = nullptr; // ns*K*NZ
-    void* d_dalpha_scratch = nullptr;
     // 3C schedule (overlap3c.cu)
     void* d_pp3 = nullptr;
     int* d_npp3 = nullptr;
@@ -122,15 +120,13 @@ int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef
                            const void* D, const void* dalpha_add, cudaStream_t s);
 
 // overlap2c_bwd*.cu
-int launch_pb_f32(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
-                  const void* posA, const void* posB,
-                  double lengthscale, cudaStream_t s);
-int launch_pb_f64(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
-                  const void* posA, const void* posB,
-                  double lengthscale, cudaStream_t s);
-int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
-                        const void* coef, const void* posA, const void* posB, int64_t B,
-                        double lengthscale, int keep_absent, cudaStream_t s);
+int launch_pb_f32(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
+                  const void* D, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
+int launch_pb_f64(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
+                  const void* D, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
+int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
+                        const void* D, const int64_t* sidxA, const int64_t* sidxB, const void* posA,
+                        const void* posB, int64_t B, double lengthscale, int keep_absent, cudaStream_t s);
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);

@@ -122,9 +122,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
         (st = dmalloc(&p->d_err, 1, "cudaMalloc(err)")) ||
         (st = dmalloc_bytes(&p->d_gb_zeta, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_zeta)")) ||
         (st = dmalloc_bytes(&p->d_gb_coef, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_coef)")) ||
-        (st = dmalloc_bytes(&p->d_coef_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(coef)")) ||
-        (st = dmalloc_bytes(&p->d_dcoef_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(dcoef)")) ||
-        (st = dmalloc_bytes(&p->d_dalpha_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(dalpha)")))
+        (st = dmalloc_bytes(&p->d_coef_scratch, (size_t)(nshells * K * NZ) * fsz, "cudaMalloc(coef)")))
         return fail(st);
     if ((st = cuda_status(cudaMemcpy(p->d_ls, ls32.data(), sizeof(int) * nshells, cudaMemcpyHostToDevice),
                           "cudaMemcpy(ls)")) ||
@@ -143,11 +141,11 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
-    void* bufs[] = {p->d_ls, p->d_boff, p->d_pp, p->d_npp, p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter,
-                    p->d_err, p->d_items, p->d_order, p->d_blockhist,
-                    p->d_gb_zeta, p->d_gb_coef, p->d_pb_rec, p->d_pb_counts, p->d_pb_items, p->d_pb_itemidx, p->d_pb_rows, p->d_partials,
-                    p->d_coef_scratch, p->d_dcoef_scratch, p->d_dalpha_scratch, p->d_pp3,
-                    p->d_npp3, p->d_items3};
+    void* bufs[] = {p->d_ls,        p->d_boff,      p->d_pp,        p->d_npp,        p->d_perm,
+                    p->d_tiles,     p->d_ntiles,    p->d_tbase,     p->d_counter,    p->d_err,
+                    p->d_items,     p->d_order,     p->d_blockhist, p->d_gb_zeta,    p->d_gb_coef,
+                    p->d_pb_rec,    p->d_pb_counts, p->d_pb_items,  p->d_pb_itemidx, p->d_pb_rows,
+                    p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3};
     for (void* b : bufs) dfree(b);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);
@@ -257,29 +255,30 @@ int aok_overlap2c_gb(aok_plan* p, void* out, const int64_t* nprim, const int64_t
     return launch_overlap2c(p, out, posA, posB, B, 1.0, s);
 }
 
-static int overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
-                              const void* coef, const void* posA, const void* posB, const int64_t* sidxA,
-                              const int64_t* sidxB, int64_t B, double lengthscale, int keep_absent, void* stream) {
-    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null plan");
-    AOK_TRY(check_batch(p, B, "aok_overlap2c_pullback"));
-    if (!dcoef || !dalpha || !zeta || !coef) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
+static int overlap2c_pullback(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta,
+                              const void* coef, const void* D, const void* posA, const void* posB,
+                              const int64_t* sidxA, const int64_t* sidxB, int64_t B, double lengthscale,
+                              int keep_absent, void* stream, const char* who) {
+    AOK_TRY(check_batch(p, B, who));
     cudaStream_t s = (cudaStream_t)stream;
     const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    if (B == 0) {
-        AOK_TRY(cuda_status(cudaMemsetAsync(dcoef, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync"));
-        return cuda_status(cudaMemsetAsync(dalpha, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync");
+    if (B == 0) {  // no pairs: zero gradients
+        AOK_TRY(cuda_status(cudaMemsetAsync(out0, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync"));
+        return cuda_status(cudaMemsetAsync(out1, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync");
     }
     if (!dS || !posA || !posB || !sidxA || !sidxB)
-        return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
-    AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
-    return launch_overlap2c_pb(p, dcoef, dalpha, dS, zeta, coef, posA, posB, B, lengthscale, keep_absent, s);
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    return launch_overlap2c_pb(p, out0, out1, dS, zeta, coef, D, sidxA, sidxB, posA, posB, B, lengthscale,
+                               keep_absent, s);
 }
 
 int aok_overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta,
                            const void* coef, const void* posA, const void* posB, const int64_t* sidxA,
                            const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
-    return overlap2c_pullback(p, dcoef, dalpha, dS, zeta, coef, posA, posB, sidxA, sidxB, B, lengthscale, 1,
-                              stream);
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null plan");
+    if (!dcoef || !dalpha || !zeta || !coef) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
+    return overlap2c_pullback(p, dcoef, dalpha, dS, zeta, coef, nullptr, posA, posB, sidxA, sidxB, B, lengthscale, 1,
+                              stream, "aok_overlap2c_pullback");
 }
 
 int aok_overlap_pullback_ps(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta, const void* D,
@@ -287,11 +286,8 @@ int aok_overlap_pullback_ps(aok_plan* p, void* dzeta, void* dD, const void* dS, 
                             int64_t B, double lengthscale, void* stream) {
     if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap_pullback_ps: null plan");
     if (!dzeta || !dD || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_overlap_pullback_ps: null pointer");
-    cudaStream_t s = (cudaStream_t)stream;
-    AOK_TRY(launch_compile_coef(p, p->d_coef_scratch, zeta, D, s));
-    AOK_TRY(overlap2c_pullback(p, p->d_dcoef_scratch, p->d_dalpha_scratch, dS, zeta, p->d_coef_scratch, posA, posB,
-                               sidxA, sidxB, B, lengthscale, 0, stream));
-    return launch_compile_coef_pb(p, dD, dzeta, p->d_dcoef_scratch, zeta, D, p->d_dalpha_scratch, s);
+    return overlap2c_pullback(p, dD, dzeta, dS, zeta, nullptr, D, posA, posB, sidxA, sidxB, B, lengthscale, 0, stream,
+                              "aok_overlap_pullback_ps");
 }
 
 }  // extern "C"

@@ -12,13 +12,13 @@ int launch_prep_pb(aok_plan* p, const void* zeta, const void* coef, int keep_abs
     const int bl = (n + kPrepPbWarps - 1) / kPrepPbWarps;
     const size_t sm = (size_t)kPrepPbWarps * 4 * p->K;
     if (p->prec == AOK_PREC_F64)
-        k_prep_pb<double><<<bl, 32 * kPrepPbWarps, sm, s>>>((PBd*)p->d_pb_rec, p->d_pb_counts, (const double*)zeta,
-                                                            (const double*)coef, (int)p->ns, (int)p->K, (int)p->NZ,
-                                                            keep_absent);
+        k_prep_pb<double><<<bl, 32 * kPrepPbWarps, sm, s>>>(
+            (PBd*)p->d_pb_rec, p->d_pb_counts, (const double*)zeta, (const double*)coef, (int)p->ns, (int)p->K,
+            (int)p->NZ, keep_absent);
     else
-        k_prep_pb<float><<<bl, 32 * kPrepPbWarps, sm, s>>>((PBf*)p->d_pb_rec, p->d_pb_counts, (const float*)zeta,
-                                                           (const float*)coef, (int)p->ns, (int)p->K, (int)p->NZ,
-                                                           keep_absent);
+        k_prep_pb<float><<<bl, 32 * kPrepPbWarps, sm, s>>>(
+            (PBf*)p->d_pb_rec, p->d_pb_counts, (const float*)zeta, (const float*)coef, (int)p->ns, (int)p->K,
+            (int)p->NZ, keep_absent);
     return cuda_status(cudaGetLastError(), "k_prep_pb");
 }
 
@@ -67,14 +67,27 @@ int ensure_pb_buffers(aok_plan* p) {
     return AOK_OK;
 }
 
-int launch_overlap2c_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
-                        const void* posA, const void* posB, int64_t B, double lengthscale, int keep_absent,
-                        cudaStream_t s) {
-    (void)B;
+// The pullback after argument checks: the record lists (for the parameter
+// pullback after compiling the coefficients from D) are built on the plan's
+// side stream while the batch is binned on the caller's stream; then the
+// record-parallel kernel and its reductions.  D == nullptr: kernel-level
+// pullback (out0, out1) = (dcoef, dalpha) from `coef`; otherwise
+// (out0, out1) = (dD, dzeta) and `coef` is ignored.
+int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
+                        const void* D, const int64_t* sidxA, const int64_t* sidxB, const void* posA,
+                        const void* posB, int64_t B, double lengthscale, int keep_absent, cudaStream_t s) {
     AOK_TRY_PB(ensure_pb_buffers(p));
-    AOK_TRY_PB(launch_prep_pb(p, zeta, coef, keep_absent, s));
-    if (p->prec == AOK_PREC_F64) return launch_pb_f64(p, dcoef, dalpha, dS, zeta, coef, posA, posB, lengthscale, s);
-    return launch_pb_f32(p, dcoef, dalpha, dS, zeta, coef, posA, posB, lengthscale, s);
+    if (D) coef = p->d_coef_scratch;
+    AOK_TRY_PB(cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord"));
+    AOK_TRY_PB(cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent"));
+    if (D) AOK_TRY_PB(launch_compile_coef(p, p->d_coef_scratch, zeta, D, p->side));
+    AOK_TRY_PB(launch_prep_pb(p, zeta, coef, keep_absent, p->side));
+    AOK_TRY_PB(cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord"));
+    AOK_TRY_PB(launch_bin(p, sidxA, sidxB, B, s));
+    AOK_TRY_PB(cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent"));
+    if (p->prec == AOK_PREC_F64)
+        return launch_pb_f64(p, out0, out1, dS, zeta, coef, D, posA, posB, lengthscale, s);
+    return launch_pb_f32(p, out0, out1, dS, zeta, coef, D, posA, posB, lengthscale, s);
 }
 
 }  // namespace aok

@@ -47,6 +47,7 @@
 // the result does not depend on which warp ran which unit.
 #pragma once
 
+#include "compile_coef.cuh"
 #include "overlap2c_kernel.cuh"
 
 namespace aok {
@@ -471,9 +472,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c_pb(const __grid_con
 }
 
 // Fixed-order sums of the unit partials, in two stages.
-// k_pb_sum_units: one warp per (species pair k, item i); lane = (value v, slot
-// kk); sums the item's units over chunks j, then record groups g (empty units
-// skipped) into rows[k][i][4][K] (zeros for an item without records).
+// k_pb_sum_units: one warp per (species pair k, item i); lane = (value, slot);
+// sums the item's units over chunks, then record groups (empty units
+// skipped), eight loads in flight, into rows[k][i][4][K] (zeros for an item
+// without records or a species pair without batch elements).
 static __global__ void k_pb_sum_units(double* __restrict__ rows, const double* __restrict__ partial,
                                       const int4* __restrict__ counts, const int* __restrict__ tbase,
                                       const Item* __restrict__ items, int ns, int K, int np, int nitems, int gmax) {
@@ -481,38 +483,43 @@ static __global__ void k_pb_sum_units(double* __restrict__ rows, const double* _
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (wid >= np * nitems) return;
     const int k = wid / nitems, i = wid % nitems;
-    int chbase = 0;
-    for (int k2 = 0; k2 < k; ++k2) chbase += pb_nch(tbase, k2);
+    int chbase = 0;  // chunks of the earlier species pairs (integer sum: order-free)
+    for (int k2 = lane; k2 < k; k2 += 32) chbase += pb_nch(tbase, k2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) chbase += __shfl_xor_sync(0xffffffffu, chbase, o);
     const int nch = pb_nch(tbase, k);
     const Item wi = items[i];
     const int4 n = counts[((size_t)k * ns + wi.sa) * ns + wi.sb];
-    const int nrec = n.x * n.y + n.z * n.y + n.w * n.x;
-    const int ng = (nrec + 31) / 32;
+    const int ng = (n.x * n.y + n.z * n.y + n.w * n.x + 31) / 32;
+    const int nu = nch * ng;
     double* out = rows + ((size_t)k * nitems + i) * 4 * K;
     for (int c = lane; c < 4 * K; c += 32) {
         double sum = 0.0;
-        for (int j = 0; j < nch; ++j)
-            for (int g = 0; g < ng; ++g)
-                sum += partial[((((size_t)(chbase + j) * nitems + i) * gmax + g) * 4) * K + c];
+        for (int u0 = 0; u0 < nu; u0 += 8) {
+            double v[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int u = u0 + t, j = u / ng, g = u % ng;
+                v[t] = u < nu ? partial[((((size_t)(chbase + j) * nitems + i) * gmax + g) * 4) * K + c] : 0.0;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; ++t) sum += v[t];
+        }
         out[c] = sum;
     }
 }
 
-// k_pb_reduce: one warp per output slot (kind, s, kk, sigma); lanes take the
-// (side, species pair, other shell) rows in a fixed strided order and a fixed
-// butterfly adds the lanes.  Zero slots with equal exponents take the first
-// one's value (k_prep_pb lists the first only).
+// Sum of one output slot (kind, shell s, primitive kk, species sigma) over the
+// (side, species pair, other shell) rows, by one warp: lanes take the rows in
+// a fixed strided order and a fixed butterfly adds the lanes, so the result
+// is reproducible.  Zero slots with equal exponents take the first one's
+// value (k_prep_pb lists the first only).
 template <typename FT>
-__global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, const double* __restrict__ rows,
-                            const int* __restrict__ itemidx, const FT* __restrict__ zeta, const FT* __restrict__ coef,
-                            int ns, int K, int NZ, int nitems) {
-    const int lane = threadIdx.x & 31;
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int S = ns * K * NZ;
-    if (wid >= 2 * S) return;
-    const int kind = wid / S, slot = wid % S;
-    const int s = slot % ns, sigma = slot / (ns * K);
-    int kk = (slot / ns) % K;
+__device__ __forceinline__ double pb_slot_sum(const double* __restrict__ rows, const int* __restrict__ itemidx,
+                                              const FT* __restrict__ zeta, const FT* __restrict__ coef, int ns,
+                                              int K, int NZ, int nitems, int kind, int s, int kk, int sigma,
+                                              int lane) {
+    const int slot = s + ns * (kk + K * sigma);
     if (kind == 0 && coef[slot] == FT(0)) {
         const FT z = zeta[slot];
         for (int k2 = 0; k2 < kk; ++k2) {
@@ -532,10 +539,48 @@ __global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, con
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    return sum;
+}
+
+// Kernel-level pullback: one warp per output slot, (dcoef, dalpha).
+template <typename FT>
+__global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, const double* __restrict__ rows,
+                            const int* __restrict__ itemidx, const FT* __restrict__ zeta, const FT* __restrict__ coef,
+                            int ns, int K, int NZ, int nitems) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int S = ns * K * NZ;
+    if (wid >= 2 * S) return;
+    const int kind = wid / S, slot = wid % S;
+    const int s = slot % ns, kk = (slot / ns) % K, sigma = slot / (ns * K);
+    const double sum = pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, kind, s, kk, sigma, lane);
     if (lane == 0) {
-        const int out = s + ns * (((slot / ns) % K) + K * sigma);
-        if (kind == 0) dcoef[out] = (FT)sum;
-        else dalpha[out] = (FT)sum;
+        if (kind == 0) dcoef[slot] = (FT)sum;
+        else dalpha[slot] = (FT)sum;
+    }
+}
+
+// Parameter pullback: one CTA per (shell, species).  Its warps sum the 2K
+// slots of the shell (as k_pb_reduce, kept in FP64), then warp 0 applies the
+// VJP of the contraction normalisation (compile_coef.cuh) -> (dD, dzeta).
+template <typename FT>
+__global__ void k_pb_reduce_ps(FT* __restrict__ dD, FT* __restrict__ dz, const double* __restrict__ rows,
+                               const int* __restrict__ itemidx, const FT* __restrict__ zeta,
+                               const FT* __restrict__ coef, const FT* __restrict__ D, const int* __restrict__ ls,
+                               int ns, int K, int NZ, int nitems) {
+    extern __shared__ double red[];  // dcoef[K], dalpha[K], VJP terms [2][K*K]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int s = blockIdx.x % ns, sigma = blockIdx.x / ns;
+    for (int w = warp; w < 2 * K; w += nw) {
+        const double v = pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, w / K, s, w % K, sigma, lane);
+        if (lane == 0) red[w] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const size_t base = (size_t)s + (size_t)ns * K * sigma;
+        coef_vjp_warp<FT>(
+            dD, dz, [&](int i) { return red[i]; }, [&](int i) { return red[K + i]; }, zeta, D, red + 2 * K, base,
+            ns, K, ls[s], lane);
     }
 }
 
@@ -543,9 +588,12 @@ constexpr int kPbThreadsF32 = 32 * kPbWarps;  // two CTAs per SM
 constexpr int kPbThreadsF64 = 32 * kPbWarps;  // one CTA per SM
 template <typename FT> constexpr int pb_min_blocks() { return sizeof(FT) == 4 ? 2 : 1; }
 
+// Launches the pullback kernel and its reductions.  D == nullptr: kernel-level
+// pullback, out0/out1 = (dcoef, dalpha).  Otherwise the parameter pullback,
+// out0/out1 = (dD, dzeta).
 template <typename FT, int THREADS>
-inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, const void* zeta, const void* coef,
-                     const void* posA, const void* posB, double lengthscale, cudaStream_t s) {
+inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
+                     const void* D, const void* posA, const void* posB, double lengthscale, cudaStream_t s) {
     constexpr int MINB = pb_min_blocks<FT>();
     PbParams<FT> P;
     memset(&P, 0, sizeof(P));
@@ -580,8 +628,16 @@ inline int launch_pb(aok_plan* p, void* dcoef, void* dalpha, const void* dS, con
                                                          p->d_pb_counts, p->d_tbase, p->d_pb_items, (int)p->ns,
                                                          (int)p->K, P.np, p->nitems, P.gmax);
     AOK_TRY_PB(cuda_status(cudaGetLastError(), "k_pb_sum_units"));
+    if (D) {
+        const size_t sm = sizeof(double) * (2 * p->K + 2 * p->K * p->K);
+        if (sm > 48 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "pullback: K too large");
+        k_pb_reduce_ps<FT><<<(int)(p->ns * p->NZ), 256, sm, s>>>(
+            (FT*)out0, (FT*)out1, (const double*)p->d_pb_rows, p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
+            (const FT*)D, p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems);
+        return cuda_status(cudaGetLastError(), "k_pb_reduce_ps");
+    }
     const int S = (int)(p->ns * p->K * p->NZ);
-    k_pb_reduce<FT><<<(2 * S * 32 + 255) / 256, 256, 0, s>>>((FT*)dcoef, (FT*)dalpha, (const double*)p->d_pb_rows,
+    k_pb_reduce<FT><<<(2 * S * 32 + 255) / 256, 256, 0, s>>>((FT*)out0, (FT*)out1, (const double*)p->d_pb_rows,
                                                             p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
                                                             (int)p->ns, (int)p->K, (int)p->NZ, p->nitems);
     return cuda_status(cudaGetLastError(), "k_pb_reduce");

@@ -478,8 +478,7 @@ def _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch):
         _lib.check(L.aok_overlap_pullback_ps(gpl.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS),
                                              _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
                                              _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
-        dz.mul_(2.0)
-        dD.mul_(2.0)
+        torch._foreach_mul_([dz, dD], 2.0)
 
     def fstep():
         fwd(Sg, c32["coef"])
