@@ -4,7 +4,7 @@ Public names mirror the reference's API (Julia's `f!` is spelled `f_`):
 compile_basis, adapt_basis, batch_overlap(_), batch_overlap_3c(_), pullback_ps,
 evaluate, evaluate_ed, rrule forms, gaussian_orbitals, slater_orbitals.
 """
-from . import _lib, workloads  # noqa: F401
+from . import _lib, parallel, workloads  # noqa: F401
 from ._lib import AOKError, ArgumentError, build  # noqa: F401
 from .basis import (AtomicOrbitals, CartesianGTOBasis, CartesianShell, CompiledBasis,  # noqa: F401
                     GaussianTypeRadials, PState, PStates, SlaterTypeRadials, adapt_basis, compile_basis,

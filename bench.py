@@ -442,6 +442,7 @@ def main():
 
 
 def _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch):
+    import torch.distributed as dist
     """Config 3: L = sum (S - S_tgt)^2 over the first 16384 pairs of the batch, FP32C.
     gstep = compile_coef + forward + dL/dS + pullback_ps (dzeta, dD); fstep = forward."""
     N, ns, K, NZ = basis.nbf_total, basis.nshells, basis.K, basis.NZ
@@ -479,6 +480,8 @@ def _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch):
                                              _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
                                              _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
         torch._foreach_mul_([dz, dD], 2.0)
+        if dist.is_initialized() and dist.get_world_size() > 1:
+            aok.parallel.allreduce_sum([dz, dD])  # data-parallel step: sum the ranks' gradients
 
     def fstep():
         fwd(Sg, c32["coef"])
