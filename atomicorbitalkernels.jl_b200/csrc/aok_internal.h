@@ -85,6 +85,15 @@ struct aok_orbitals {
     void* d_partials = nullptr;
     int max_blocks = 0;
     int* d_err = nullptr;
+    // slot-parallel pullback: points binned by species, unit partial rows
+    int64_t epb_cap = 0, epb_ucap = 0;
+    int* d_epb_perm = nullptr;
+    int4* d_epb_tiles = nullptr;
+    int* d_epb_ntiles = nullptr;
+    int* d_epb_tbase = nullptr;
+    unsigned* d_epb_counter = nullptr;
+    int* d_epb_blockhist = nullptr;
+    void* d_epb_partial = nullptr;
 };
 
 namespace aok {
@@ -105,6 +114,21 @@ void timing_end(aok_plan* p, cudaStream_t s);
 
 // launchers (overlap2c.cu)
 int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s);
+// Counting sort of a batch by species key (stable), tiles of 32 elements of
+// one key, and the first tile of each key.  Buffers: perm (B), tiles
+// (B/32 + NZ^2 + 1), tbase (NZ^2 + 1), blockhist (kBinMaxBlocksHost * NZ^2).
+struct BinBufs {
+    int* perm;
+    int4* tiles;
+    int* ntiles;
+    int* tbase;
+    unsigned* counter;
+    int* blockhist;
+    int* err;
+};
+constexpr int kBinMaxBlocksHost = 512;
+int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
+                    cudaStream_t s);
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s);
 int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB, int64_t B,
                      double lengthscale, cudaStream_t s);

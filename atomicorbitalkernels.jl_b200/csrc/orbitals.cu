@@ -27,6 +27,7 @@
 // The parameter pullback is deterministic: each warp reduces its 32 points'
 // contributions per species with a fixed butterfly, warps are summed in order
 // into a per-block FP64 row, and the rows are summed in block order.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -366,6 +367,196 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Slot-parallel parameter pullback (used by aok_evaluate_pullback).
+//
+// The points are counting-sorted by species (the 2C batch binning, keys
+// sigma*NZ) into tiles of 32.  A work unit is (species sigma, 4 tiles = 128
+// points).  For each 32 points the warp first puts lane = point: radials,
+// harmonics, dX (written at the point's original index), and the radial
+// cotangents gg_k = r^p_k sum_{i: iR[i] = k} dP[j,i] Z_{iY[i]} and f(r) into
+// shared memory.  Then lane = slot (k, m) of species sigma and the warp
+// loops over the 32 points:
+//   dD[k,m,sigma]    += gg_k exp(-zeta f),
+//   dzeta[k,m,sigma] += -D gg_k exp(-zeta f) f        (gtostoradials.jl:232-253),
+// with no cross-lane reduction.  Each unit writes its own FP64 partial row;
+// k_epb_reduce adds a species' units in order, so the result is reproducible.
+// ---------------------------------------------------------------------------
+constexpr int kEpbChunkTiles = 4;  // tiles of 32 points per unit
+constexpr int kEpbMaxGroups = 4;   // slots per species <= 128
+
+struct EpbParams {
+    EvalParams E;
+    const int* perm;
+    const int4* tiles;
+    const int* tbase;   // first tile of key sigma*NZ (species sigma)
+    unsigned* counter;  // unit queue
+    double* partial;    // [2][nRad*K][ucap]: dD, dzeta per slot, units contiguous
+    int ucap;           // unit capacity (row length of partial)
+};
+
+__device__ __forceinline__ int epb_nch(const int* tbase, int sigma, int NZ) {
+    return (tbase[sigma * NZ + 1] - tbase[sigma * NZ] + kEpbChunkTiles - 1) / kEpbChunkTiles;
+}
+
+// per-warp shared memory of the slot-parallel pullback (floats of FT):
+// R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][32], f [32]
+__host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) { return (size_t)(3 * nRad + 4 * nY + 1) * 32; }
+
+template <typename FT, int L>
+__global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ EpbParams Q) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int nY = (L + 1) * (L + 1);
+    const EvalParams& P = Q.E;
+    const int ntab = P.nRad * P.K * P.NZ, nslot = P.nRad * P.K;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int chpre[kMaxPairs + 1];
+    FT* sz = reinterpret_cast<FT*>(smem_raw);
+    FT* sD = sz + ntab;
+    FT* wbase = sD + ntab + (size_t)warp * epb_warp_words(P.nRad, nY);
+    FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY, *gg = G + 96 * nY,
+       *fv = gg + 32 * P.nRad;
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
+        sz[i] = ((const FT*)P.zeta)[i];
+        sD[i] = ((const FT*)P.D)[i];
+    }
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int g = 0; g < P.NZ; ++g) {
+            chpre[g] = acc;
+            acc += epb_nch(Q.tbase, g, P.NZ);
+        }
+        chpre[P.NZ] = acc;
+    }
+    __syncthreads();
+    const int nunits = chpre[P.NZ];
+    const FT* dPin = (const FT*)P.dPin;
+    const FT* Xin = (const FT*)P.X;
+    const FT sc = (FT)P.scale;
+    for (;;) {
+        int u = 0;
+        if (lane == 0) u = (int)atomicAdd(Q.counter, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= nunits) break;
+        int sigma = 0;
+        while (chpre[sigma + 1] <= u) ++sigma;
+        const int jch = u - chpre[sigma];
+        const int tb = Q.tbase[sigma * P.NZ];
+        const int t0 = tb + jch * kEpbChunkTiles, t1 = min(t0 + kEpbChunkTiles, Q.tbase[sigma * P.NZ + 1]);
+        const int e0 = Q.tiles[t0].y, e1 = Q.tiles[t1 - 1].y + Q.tiles[t1 - 1].z;
+        FT accD[kEpbMaxGroups], accZ[kEpbMaxGroups];
+#pragma unroll
+        for (int g = 0; g < kEpbMaxGroups; ++g) accD[g] = accZ[g] = FT(0);
+        for (int c0 = e0; c0 < e1; c0 += 32) {
+            // phase A: lane = point
+            {
+                const int e = c0 + lane;
+                const bool valid = e < e1;
+                const long long j = valid ? (long long)Q.perm[e] : 0;
+                FT x = FT(0), y = FT(0), z = FT(1);
+                if (valid) {
+                    x = Xin[3 * j];
+                    y = Xin[3 * j + 1];
+                    z = Xin[3 * j + 2];
+                    if (sc != FT(1)) {
+                        x = sc * x;
+                        y = sc * y;
+                        z = sc * z;
+                    }
+                }
+                const FT r = sqrt(x * x + y * y + z * z);
+                for (int k = 0; k < P.nRad; ++k) {
+                    FT Rk, dRk;
+                    radial<FT>(sz, sD, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
+                    R[k * 32 + lane] = Rk;
+                    dR[k * 32 + lane] = dRk;
+                    gg[k * 32 + lane] = FT(0);
+                }
+                solid_harmonics<FT, L>(x, y, z, P.F, Z + lane, G + lane, 32);
+                const FT ux = x / r, uy = y / r, uz = z / r;
+                FT ax = FT(0), ay = FT(0), az = FT(0);
+                if (valid) {
+                    for (int i = 0; i < P.nOrb; ++i) {
+                        const int k = P.iR[i], yi = P.iY[i];
+                        const FT g = dPin[j + P.nX * i];
+                        const FT rn = R[k * 32 + lane], yl = Z[yi * 32 + lane], dr = dR[k * 32 + lane];
+                        ax += g * ((dr * ux) * yl + rn * G[(3 * yi + 0) * 32 + lane]);
+                        ay += g * ((dr * uy) * yl + rn * G[(3 * yi + 1) * 32 + lane]);
+                        az += g * ((dr * uz) * yl + rn * G[(3 * yi + 2) * 32 + lane]);
+                        gg[k * 32 + lane] += g * yl;
+                    }
+                    if (P.dX) {
+                        FT* dX = (FT*)P.dX;
+                        dX[3 * j] = sc != FT(1) ? ax * sc : ax;
+                        dX[3 * j + 1] = sc != FT(1) ? ay * sc : ay;
+                        dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
+                    }
+                }
+                for (int k = 0; k < P.nRad; ++k) {
+                    FT rp = FT(1);
+                    for (int i = 0; i < P.poly[k]; ++i) rp *= r;
+                    gg[k * 32 + lane] *= rp;  // zero for lanes past the chunk's end
+                }
+                fv[lane] = P.slater ? r : r * r;
+            }
+            __syncwarp();
+            // phase B: lane = slot (k, m) of species sigma
+            const int np = min(32, e1 - c0);
+#pragma unroll
+            for (int g = 0; g < kEpbMaxGroups; ++g) {
+                const int s = g * 32 + lane;
+                if (g * 32 < nslot && s < nslot) {
+                    const int k = s % P.nRad;
+                    const FT zk = sz[s + nslot * sigma];
+                    FT aD = accD[g], aZ = accZ[g];
+                    for (int t = 0; t < np; ++t) {
+                        const FT f = fv[t], w = gg[k * 32 + t];
+                        const FT ex = exp(-zk * f) * w;
+                        aD += ex;
+                        aZ = fma(ex, f, aZ);
+                    }
+                    accD[g] = aD;
+                    accZ[g] = aZ;
+                }
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int g = 0; g < kEpbMaxGroups; ++g) {
+            const int s = g * 32 + lane;
+            if (s < nslot) {
+                Q.partial[(size_t)s * Q.ucap + u] = (double)accD[g];
+                Q.partial[(size_t)(nslot + s) * Q.ucap + u] = -(double)sD[s + nslot * sigma] * (double)accZ[g];
+            }
+        }
+    }
+}
+
+// dD, dzeta of slot (k, m, sigma): one warp per output value; lanes take
+// species sigma's unit rows in a fixed strided order and a fixed butterfly
+// adds the lanes, so the result is reproducible.
+template <typename FT>
+__global__ void k_epb_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const double* __restrict__ partial,
+                             const int* __restrict__ tbase, int nslot, int NZ, int ucap) {
+    const int lane = threadIdx.x & 31;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= 2 * nslot * NZ) return;
+    const int kind = t / (nslot * NZ), o = t % (nslot * NZ);
+    const int sigma = o / nslot, s = o % nslot;
+    int u0 = 0;
+    for (int g = 0; g < sigma; ++g) u0 += epb_nch(tbase, g, NZ);
+    const int nu = epb_nch(tbase, sigma, NZ);
+    double sum = 0.0;
+    const double* row = partial + (size_t)(kind * nslot + s) * ucap + u0;
+    for (int v = lane; v < nu; v += 32) sum += row[v];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (lane == 0) {
+        if (kind == 0) dD[o] = (FT)sum;
+        else dzeta[o] = (FT)sum;
+    }
+}
+
 template <typename FT>
 __global__ void k_eval_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const double* __restrict__ rows, int nrows,
                               int ntab) {
@@ -461,6 +652,66 @@ int launch_evaluate(aok_orbitals* o, void* Pv, void* dP, const void* X, const in
     return launch_eval_T<float>(o, P, dP != nullptr, false, s);
 }
 
+// buffers of the slot-parallel pullback, grown to nX points
+static int ensure_epb_buffers(aok_orbitals* o, int64_t nX) {
+    if (nX <= o->epb_cap) return AOK_OK;
+    void* bufs[] = {o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
+                    o->d_epb_blockhist, o->d_epb_partial};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    o->d_epb_perm = nullptr;
+    o->d_epb_tiles = nullptr;
+    o->d_epb_ntiles = o->d_epb_tbase = o->d_epb_blockhist = nullptr;
+    o->d_epb_counter = nullptr;
+    o->d_epb_partial = nullptr;
+    o->epb_cap = 0;
+    const int64_t np = o->NZ * o->NZ;
+    const int64_t tiles = (nX + 31) / 32 + np + 1;
+    const int64_t units = tiles / kEpbChunkTiles + o->NZ + 1;
+    cudaError_t e;
+    if ((e = cudaMalloc(&o->d_epb_perm, sizeof(int) * nX)) != cudaSuccess ||
+        (e = cudaMalloc(&o->d_epb_tiles, sizeof(int4) * tiles)) != cudaSuccess ||
+        (e = cudaMalloc(&o->d_epb_ntiles, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&o->d_epb_tbase, sizeof(int) * (np + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&o->d_epb_counter, sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMalloc(&o->d_epb_blockhist, sizeof(int) * kBinMaxBlocksHost * np)) != cudaSuccess ||
+        (e = cudaMalloc(&o->d_epb_partial, sizeof(double) * units * 2 * o->nRad * o->K)) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(evaluate pullback buffers)");
+    o->epb_cap = nX;
+    o->epb_ucap = units;
+    return AOK_OK;
+}
+
+template <typename FT, int L>
+static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
+    constexpr int nY = (L + 1) * (L + 1);
+    const size_t fsz = sizeof(FT);
+    const size_t tab = 2 * (size_t)(o->nRad * o->K * o->NZ) * fsz;
+    const size_t per_warp = epb_warp_words((int)o->nRad, nY) * fsz;
+    int nw = 8;
+    while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;
+    const size_t smem = tab + nw * per_warp;
+    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "evaluate pullback: basis too large");
+    auto k = k_evaluate_pbs<FT, L>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs)");
+    const int per_sm = std::max(1, std::min(2, (int)((228 * 1024) / (smem + 1024))));
+    k<<<o->num_sms * per_sm, 32 * nw, smem, s>>>(Q);
+    return cuda_status(cudaGetLastError(), "k_evaluate_pbs");
+}
+
+template <typename FT>
+static int launch_epb_T(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
+    switch (o->L) {
+        case 0: return launch_epb_L<FT, 0>(o, Q, s);
+        case 1: return launch_epb_L<FT, 1>(o, Q, s);
+        case 2: return launch_epb_L<FT, 2>(o, Q, s);
+        case 3: return launch_epb_L<FT, 3>(o, Q, s);
+        case 4: return launch_epb_L<FT, 4>(o, Q, s);
+        default: return set_error(AOK_ERR_UNSUPPORTED, "evaluate: harmonics above l = 4");
+    }
+}
+
 int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const void* dPin, const void* X,
                        const int64_t* sidx, const void* zeta, const void* D, int64_t nX, double lengthscale,
                        cudaStream_t s) {
@@ -468,6 +719,31 @@ int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const v
     fill_params(o, P, X, sidx, zeta, D, nX, lengthscale);
     P.dPin = dPin;
     P.dX = dX;
+    const int nslot = (int)(o->nRad * o->K);
+    if (dzeta && dD && nslot <= 32 * kEpbMaxGroups && o->NZ * o->NZ <= kMaxPairs) {
+        // slot-parallel: points binned by species, lanes = (radial, primitive) slots
+        AOK_TRY_PB(ensure_epb_buffers(o, nX));
+        const BinBufs bb{o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
+                         o->d_epb_blockhist, o->d_err};
+        AOK_TRY_PB(launch_bin_into(bb, sidx, nullptr, nX, (int)o->NZ, s));
+        EpbParams Q;
+        Q.E = P;
+        Q.perm = o->d_epb_perm;
+        Q.tiles = o->d_epb_tiles;
+        Q.tbase = o->d_epb_tbase;
+        Q.counter = o->d_epb_counter;
+        Q.partial = (double*)o->d_epb_partial;
+        Q.ucap = (int)o->epb_ucap;
+        AOK_TRY_PB(o->prec == AOK_PREC_F64 ? launch_epb_T<double>(o, Q, s) : launch_epb_T<float>(o, Q, s));
+        const int nout = 2 * nslot * (int)o->NZ, rb = (nout * 32 + 255) / 256;
+        if (o->prec == AOK_PREC_F64)
+            k_epb_reduce<double><<<rb, 256, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, o->d_epb_tbase, nslot,
+                                                   (int)o->NZ, Q.ucap);
+        else
+            k_epb_reduce<float><<<rb, 256, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, o->d_epb_tbase, nslot,
+                                                  (int)o->NZ, Q.ucap);
+        return cuda_status(cudaGetLastError(), "k_epb_reduce");
+    }
     const int grid = (int)((nX + kEvalThreads - 1) / kEvalThreads);
     const int ntab = (int)(o->nRad * o->K * o->NZ);
     if (dzeta && dD) {
@@ -557,7 +833,9 @@ int aok_orbitals_create(aok_orbitals** out, int64_t nRad, int64_t K, int64_t NZ,
 
 int aok_orbitals_destroy(aok_orbitals* o) {
     if (!o) return AOK_OK;
-    void* bufs[] = {o->d_poly, o->d_iR, o->d_iY, o->d_partials, o->d_err};
+    void* bufs[] = {o->d_poly,        o->d_iR,          o->d_iY,          o->d_partials,      o->d_err,
+                    o->d_epb_perm,    o->d_epb_tiles,   o->d_epb_ntiles,  o->d_epb_tbase,     o->d_epb_counter,
+                    o->d_epb_blockhist, o->d_epb_partial};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete o;

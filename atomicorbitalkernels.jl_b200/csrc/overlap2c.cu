@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
 // --------------------------------------------------------------------------
 // Species-pair bins: multi-block counting sort in two launches, no waiting.
 //   k_bin_count    per block: histogram of its chunk of the batch
-//   k_bin_scatter  per block: reads every block's histogram (at most 128
+//   k_bin_scatter  per block: reads every block's histogram (at most 512
 //                  blocks x NZ^2 keys), derives its own offsets, scatters its
 //                  chunk stably (so the permutation is reproducible), and
 //                  writes every nblk-th entry of the tile table (tiles of
@@ -217,13 +217,13 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
 // k_bin_identity replaces both for single-species batches.
 // --------------------------------------------------------------------------
 constexpr int kBinThreads = 256;
-constexpr int kBinMaxBlocks = 128;
+constexpr int kBinMaxBlocks = kBinMaxBlocksHost;
 
 __device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sidxB, int b, int B, int NZ, int* err) {
     if (b >= B) return -1;
     int64_t a = sidxA ? sidxA[b] : 1, c = sidxB ? sidxB[b] : 1;
     if (a < 1 || a > NZ || c < 1 || c > NZ) {
-        atomicCAS(err, 0, AOK_ERR_SPECIES);
+        if (err) atomicCAS(err, 0, AOK_ERR_SPECIES);
         return -1;
     }
     return (int)((a - 1) * NZ + (c - 1));
@@ -264,12 +264,28 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
         tot[k] = 0;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nblk * np; i += blockDim.x) {
-        const int k = i % np, blk = i / np;
-        const int v = blockhist[i];
-        if (v) {
-            atomicAdd(&tot[k], v);
-            if (blk < me) atomicAdd(&before[k], v);
+    if (np <= (int)blockDim.x) {
+        // thread t sums key t % np over blocks t / np, t / np + stride, ... in
+        // registers, then one shared atomic per thread and key
+        const int k = threadIdx.x % np, r0 = threadIdx.x / np, stride = blockDim.x / np;
+        if (r0 < stride) {
+            int tt = 0, b4 = 0;
+            for (int blk = r0; blk < nblk; blk += stride) {
+                const int v = blockhist[(size_t)blk * np + k];
+                tt += v;
+                if (blk < me) b4 += v;
+            }
+            if (tt) atomicAdd(&tot[k], tt);
+            if (b4) atomicAdd(&before[k], b4);
+        }
+    } else {
+        for (int i = threadIdx.x; i < nblk * np; i += blockDim.x) {
+            const int k = i % np, blk = i / np;
+            const int v = blockhist[i];
+            if (v) {
+                atomicAdd(&tot[k], v);
+                if (blk < me) atomicAdd(&before[k], v);
+            }
         }
     }
     __syncthreads();
@@ -451,21 +467,29 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
     return cuda_status(cudaGetLastError(), "k_order2c");
 }
 
-int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s) {
-    const int chunk = (int)std::max<int64_t>(512, (B + kBinMaxBlocks - 1) / kBinMaxBlocks);
+int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
+                    cudaStream_t s) {
+    // blocks of >= 512 elements; at most 512 blocks, and few enough that each
+    // block's read of all block histograms stays <= 16K entries
+    const int maxb = std::min(kBinMaxBlocks, std::max(128, 16384 / (NZ * NZ)));
+    const int chunk = (int)std::max<int64_t>(512, (B + maxb - 1) / maxb);
     const int nblk = (int)((B + chunk - 1) / chunk);
-    const int NZ = (int)p->NZ;
     if (NZ == 1 || (!sidxA && !sidxB)) {
         const int np = NZ * NZ;
         k_bin_identity<<<(int)((std::max<int64_t>(B, np + 1) + 255) / 256), 256, 0, s>>>(
-            (int)B, np, p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter);
+            (int)B, np, bb.perm, bb.tiles, bb.ntiles, bb.tbase, bb.counter);
         return cuda_status(cudaGetLastError(), "k_bin_identity");
     }
-    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, p->d_blockhist, p->d_err);
+    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.err);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_bin_count"));
-    k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, p->d_blockhist, p->d_perm,
-                                               p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_err);
+    k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.perm, bb.tiles,
+                                               bb.ntiles, bb.tbase, bb.counter, bb.err);
     return cuda_status(cudaGetLastError(), "k_bin_scatter");
+}
+
+int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s) {
+    const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
+    return launch_bin_into(bb, sidxA, sidxB, B, (int)p->NZ, s);
 }
 
 int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB, int64_t B, double lengthscale,
