@@ -277,7 +277,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                 const int bg = P.perm[start + bl];
                 FT* o = P.out + (size_t)bg * P.N * P.N + (size_t)col0 * P.N;
                 const FT* s = slab + (size_t)bl * P.slab_stride;
-                for (int e = lane; e < len; e += 32) o[e] = s[e];
+                int e = lane;
+                for (; e + 96 < len; e += 128) {  // four loads in flight, streaming stores
+                    const FT v0 = s[e], v1 = s[e + 32], v2 = s[e + 64], v3 = s[e + 96];
+                    __stcs(o + e, v0);
+                    __stcs(o + e + 32, v1);
+                    __stcs(o + e + 64, v2);
+                    __stcs(o + e + 96, v3);
+                }
+                for (; e < len; e += 32) __stcs(o + e, s[e]);
             }
             __syncthreads();
         }
