@@ -62,7 +62,7 @@ static_assert(md_nv(3, 3) == 8 && md_nv(2, 3) == 6 && md_nv(1, 1) == 2 && md_nv(
 // Work item: a shell pair (sa, sb).
 struct Item {
     int16_t cls;    // la*4 + lb
-    int16_t chunk;  // 0 (reserved)
+    int16_t chunk;  // 2C forward execution order: the item's primitive-pair count
     int16_t sa, sb;
 };
 

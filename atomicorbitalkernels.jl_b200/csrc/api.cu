@@ -75,6 +75,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
         return set_error(AOK_ERR_INVALID, "aok_plan_create: unknown precision");
     if (nshells > kMaxShells) return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: more than 64 shells");
     if (NZ * NZ > 256) return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: more than 16 species");
+    if (K > 128) return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: more than 128 primitives per shell");
     if (max_batch > (int64_t)0x7fffffff - 64)
         return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_create: batch larger than 2^31");
     for (int64_t s = 0; s < nshells; ++s)

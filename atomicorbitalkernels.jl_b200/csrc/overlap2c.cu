@@ -161,7 +161,8 @@ __global__ void k_prep2c(FT* __restrict__ pp, int* __restrict__ npp, const FT* _
 }
 
 // --------------------------------------------------------------------------
-// Execution order of the work items of one species pair: within each panel,
+// Execution order of the work items of one species pair (each item carries its
+// number of primitive pairs in `chunk`): within each panel,
 // heavier classes first (warps that run concurrently share the class's code
 // in the instruction cache), and inside a class the items with more primitive
 // pairs first (longest-processing-time order for the warps' dynamic queue).
@@ -176,7 +177,11 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
     const int pair = blockIdx.x;
     Item* out = order + (size_t)pair * nitems;
     if (nitems > kOrderMax) {  // very large bases: keep the static order
-        for (int i = threadIdx.x; i < nitems; i += blockDim.x) out[i] = items[i];
+        for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
+            Item o = items[i];
+            o.chunk = (int16_t)min(npp[((size_t)pair * ns + o.sa) * ns + o.sb], 32767);
+            out[i] = o;
+        }
         return;
     }
     for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
@@ -201,7 +206,9 @@ __global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const
             const unsigned long long kj = key[j];
             r += (kj < ki) || (kj == ki && j < i);
         }
-        out[r] = items[i];
+        Item o = items[i];
+        o.chunk = (int16_t)min(npp[((size_t)pair * ns + o.sa) * ns + o.sb], 32767);
+        out[r] = o;
     }
 }
 

@@ -204,7 +204,6 @@ struct Ov2Params {
     FT scale;
     int use_scale;
     const FT* pp;         // records: per (species pair, shell pair) a region of K*K maximum-size records
-    const int* npp;
     const int* perm;
     const int4* tiles;
     const int* ntiles;
@@ -252,14 +251,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
         for (int pn = 0; pn < P.panels.n; ++pn) {
             const int col0 = P.panels.col0[pn];
             const int i0 = P.panels.item0[pn], i1 = P.panels.item0[pn + 1];
+            const Item* order = P.items + (size_t)pair * P.nitems;
             for (;;) {
                 int it = 0;
                 if (lane == 0) it = atomicAdd(&s_next[pn], 1);
                 it = __shfl_sync(0xffffffffu, it, 0) + i0;
                 if (it >= i1) break;
-                const Item wi = P.items[(size_t)pair * P.nitems + it];
+                const Item wi = order[it];
                 const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
-                const int n = __ldg(P.npp + q);
+                const int n = wi.chunk;  // primitive pairs of the item
                 {
                     const int rec16 = sizeof(FT) == 4 ? rec_words16_f32(wi.cls >> 2, wi.cls & 3)
                                                       : rec_words16_f64(wi.cls >> 2, wi.cls & 3);
@@ -303,7 +303,6 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     P.scale = (FT)lengthscale;
     P.use_scale = (FT)lengthscale != FT(1);
     P.pp = (const FT*)p->d_pp;
-    P.npp = p->d_npp;
     P.perm = p->d_perm;
     P.tiles = p->d_tiles;
     P.ntiles = p->d_ntiles;

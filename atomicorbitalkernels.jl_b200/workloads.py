@@ -127,6 +127,22 @@ def config2_basis(seed=1002, nspecies=4):
     return _assemble(per, Kmax)
 
 
+def outputbound_basis(seed=1005, nspecies=4):
+    """The config-2 shell structure (3-5 s, 2-3 p, 1-2 d, 0-1 f per species) with one
+    primitive per shell: few primitive pairs per integral, so the 2C kernel is bound
+    by writing its output (the "output-bound classes" of the roofline criterion)."""
+    rng = _rng(seed)
+    per = []
+    ranges = {0: (3, 5), 1: (2, 3), 2: (1, 2), 3: (0, 1)}
+    for _ in range(nspecies):
+        sp = {}
+        for l, (lo, hi) in ranges.items():
+            n = int(rng.integers(lo, hi + 1))
+            sp[l] = [_draw_shell(rng, l, 1) for _ in range(n)]
+        per.append(sp)
+    return _assemble(per, 1)
+
+
 @dataclass
 class PairBatch:
     posA: np.ndarray        # (3,B) Bohr

@@ -566,6 +566,37 @@ def side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks):
     and config 4 (3C, B=4096): times, throughput and error vs the oracle."""
     out = {}
     n = max(5, min(200, args.steps // 10))
+    # output-bound 2C: the config-2 shell structure with one primitive per shell
+    ob = aok.workloads.outputbound_basis()
+    obp = aok.workloads.ragged_pairs(B_PER_RANK, ob.NZ, SEED + 1)
+    Nob = ob.nbf_total
+    res = {}
+    for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
+        pl = _dev.Plan(ob.ls, ob.K, ob.NZ, _dev.prec_of(FT), obp.B)
+        zt, Dt = _dev.to_colmajor(ob.zeta, FT), _dev.to_colmajor(ob.D, FT)
+        cf = _dev.colmajor_empty((ob.nshells, ob.K, ob.NZ), FT)
+        _lib.check(L.aok_compile_coef(pl.h, _dev.ptr(cf), _dev.ptr(zt), _dev.ptr(Dt), _dev.stream()))
+        _lib.check(L.aok_plan_set_basis(pl.h, _dev.ptr(zt), _dev.ptr(cf), _dev.stream()))
+        pa, pb = _dev.to_colmajor(obp.posA, FT), _dev.to_colmajor(obp.posB, FT)
+        sa, sb = torch.as_tensor(obp.sidxA).cuda(), torch.as_tensor(obp.sidxB).cuda()
+        o = _dev.colmajor_empty((Nob, Nob, obp.B), FT)
+        fn = lambda: _lib.check(L.aok_overlap2c(pl.h, _dev.ptr(o), None, None, _dev.ptr(pa), _dev.ptr(pb),
+                                                ctypes.c_void_p(sa.data_ptr()), ctypes.c_void_p(sb.data_ptr()),
+                                                obp.B, 1.0, _dev.stream()))
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        _lib.check(L.aok_plan_timing_enable(pl.h, n))
+        ms = _time(fn, n, 0, torch, allmax)
+        tot, cnt = ctypes.c_double(), ctypes.c_int64()
+        _lib.check(L.aok_plan_timing_read(pl.h, ctypes.byref(tot), ctypes.byref(cnt)))
+        kms = tot.value / max(cnt.value, 1)
+        fsz = 4 if FT == torch.float32 else 8
+        alg = obp.B * (Nob * Nob * fsz + 2 * (3 * fsz + 8))
+        res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obp.B / (ms * 1e-3),
+                    "kernel_hbm_gbs": alg / (kms * 1e-3) / 1e9, "kernel_hbm_frac": alg / (kms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+        del pl
+    out["outputbound_2c_K1_B65536"] = dict(res, nbf=Nob, note="config-2 shell structure, one primitive per shell")
     # config 1
     res = {}
     for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
