@@ -33,6 +33,13 @@ __host__ __device__ constexpr int cart_y(int l, int c) { return l - cart_x(l, c)
 __host__ __device__ constexpr int max_elems() { return 36; }
 __host__ __device__ constexpr int nchunks(int ne) { return (ne + max_elems() - 1) / max_elems(); }
 
+// 2^x with the hardware approximation (MUFU ex2, flushes subnormal results).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Error-free sum a + b = s + e (Knuth TwoSum).
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = a + b;

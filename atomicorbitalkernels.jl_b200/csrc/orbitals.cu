@@ -132,16 +132,27 @@ __device__ __forceinline__ void solid_harmonics(FT x, FT y, FT z, const double* 
 
 // Radial k at r for species sg: R = r^p sum_m D e^{-zeta f(r)}, dR/dr.
 // FP32 sums use TwoSum compensation over the K terms.
+// exp(-zeta f): FP32 as 2^{-(zeta log2 e) f} with zl = zeta log2(e) computed in
+// FP64 and rounded once (relative error ~1e-7 (1 + zeta f)); FP64 plain exp.
+__device__ __forceinline__ float exp_neg(float z, float zl, float f) {
+    (void)z;
+    return ex2_approx(-zl * f);
+}
+__device__ __forceinline__ double exp_neg(double z, double zl, double f) {
+    (void)zl;
+    return exp(-z * f);
+}
+
 template <typename FT>
-__device__ __forceinline__ void radial(const FT* sz, const FT* sD, int k, int sg, int nRad, int K, int p, int slater,
-                                       FT r, FT& R, FT& dR) {
+__device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl, int k, int sg, int nRad, int K,
+                                       int p, int slater, FT r, FT& R, FT& dR) {
     const FT f = slater ? r : r * r;
     const FT df = slater ? FT(1) : FT(2) * r;
     FT s = FT(0), se = FT(0), ds = FT(0);
     for (int m = 0; m < K; ++m) {
         const int o = k + nRad * (m + K * sg);
         const FT z = sz[o];
-        const FT a = sD[o] * exp(-z * f);
+        const FT a = sD[o] * exp_neg(z, sl[o], f);
         if constexpr (sizeof(FT) == 4) {
             const float t = s + a, bb = t - s;
             se += (s - (t - bb)) + (a - bb);
@@ -168,6 +179,7 @@ template <typename FT>
 struct EvalSmem {
     FT* sz;
     FT* sD;
+    FT* sl;  // zeta log2(e)
     FT* R;
     FT* dR;
     FT* Z;
@@ -179,7 +191,8 @@ __device__ __forceinline__ EvalSmem<FT> eval_smem(unsigned char* raw, int ntab, 
     FT* p = reinterpret_cast<FT*>(raw);
     s.sz = p;
     s.sD = p + ntab;
-    p += 2 * ntab;
+    s.sl = p + 2 * ntab;
+    p += 3 * ntab;
     s.R = p;
     p += nRad * kEvalThreads;
     s.dR = p;
@@ -199,6 +212,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         S.sz[i] = ((const FT*)P.zeta)[i];
         S.sD[i] = ((const FT*)P.D)[i];
+        S.sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
     }
     __syncthreads();
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
     }
     for (int k = 0; k < P.nRad; ++k) {
         FT R, dR;
-        radial<FT>(S.sz, S.sD, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+        radial<FT>(S.sz, S.sD, S.sl, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
         S.R[k * kEvalThreads + t] = R;
         S.dR[k * kEvalThreads + t] = dR;
     }
@@ -260,11 +274,12 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
     EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, nY);
     // per-warp FP64 accumulators [warp][2][ntab] after the per-thread scratch
     double* wacc = reinterpret_cast<double*>(
-        smem_raw + (((size_t)2 * ntab + (size_t)(2 * P.nRad + 4 * nY) * kEvalThreads) * sizeof(FT) + 7) / 8 * 8);
+        smem_raw + (((size_t)3 * ntab + (size_t)(2 * P.nRad + 4 * nY) * kEvalThreads) * sizeof(FT) + 7) / 8 * 8);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         S.sz[i] = ((const FT*)P.zeta)[i];
         S.sD[i] = ((const FT*)P.D)[i];
+        S.sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
     }
     for (int i = threadIdx.x; i < NW * 2 * ntab; i += blockDim.x) wacc[i] = 0.0;
     __syncthreads();
@@ -294,7 +309,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
     const int sgc = sg < 0 ? 0 : sg;
     for (int k = 0; k < P.nRad; ++k) {
         FT R, dR;
-        radial<FT>(S.sz, S.sD, k, sgc, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+        radial<FT>(S.sz, S.sD, S.sl, k, sgc, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
         S.R[k * kEvalThreads + t] = R;
         S.dR[k * kEvalThreads + t] = dR;
     }
@@ -339,7 +354,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
             FT cD = FT(0), cZ = FT(0);
             if (sg >= 0) {
                 const int o = k + P.nRad * (m + P.K * sg);
-                const FT a = exp(-S.sz[o] * f);
+                const FT a = exp_neg(S.sz[o], S.sl[o], f);
                 cD = gg * a;
                 cZ = ((gg * S.sD[o]) * a) * (-f);
             }
@@ -413,12 +428,14 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
     __shared__ int chpre[kMaxPairs + 1];
     FT* sz = reinterpret_cast<FT*>(smem_raw);
     FT* sD = sz + ntab;
-    FT* wbase = sD + ntab + (size_t)warp * epb_warp_words(P.nRad, nY);
+    FT* sl = sD + ntab;  // zeta log2(e)
+    FT* wbase = sl + ntab + (size_t)warp * epb_warp_words(P.nRad, nY);
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY, *gg = G + 96 * nY,
        *fv = gg + 32 * P.nRad;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         sz[i] = ((const FT*)P.zeta)[i];
         sD[i] = ((const FT*)P.D)[i];
+        sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
     }
     if (threadIdx.x == 0) {
         int acc = 0;
@@ -467,7 +484,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                 const FT r = sqrt(x * x + y * y + z * z);
                 for (int k = 0; k < P.nRad; ++k) {
                     FT Rk, dRk;
-                    radial<FT>(sz, sD, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
+                    radial<FT>(sz, sD, sl, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
                     R[k * 32 + lane] = Rk;
                     dR[k * 32 + lane] = dRk;
                     gg[k * 32 + lane] = FT(0);
@@ -507,11 +524,11 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                 const int s = g * 32 + lane;
                 if (g * 32 < nslot && s < nslot) {
                     const int k = s % P.nRad;
-                    const FT zk = sz[s + nslot * sigma];
+                    const FT zk = sz[s + nslot * sigma], zl = sl[s + nslot * sigma];
                     FT aD = accD[g], aZ = accZ[g];
                     for (int t = 0; t < np; ++t) {
                         const FT f = fv[t], w = gg[k * 32 + t];
-                        const FT ex = exp(-zk * f) * w;
+                        const FT ex = exp_neg(zk, zl, f) * w;
                         aD += ex;
                         aZ = fma(ex, f, aZ);
                     }
@@ -572,7 +589,7 @@ static size_t eval_smem_bytes(const aok_orbitals* o, bool pb) {
     const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
     const int nY = (o->L + 1) * (o->L + 1);
     const size_t ntab = (size_t)(o->nRad * o->K * o->NZ);
-    size_t b = (2 * ntab + (size_t)(2 * o->nRad + 4 * nY) * kEvalThreads) * fsz;
+    size_t b = (3 * ntab + (size_t)(2 * o->nRad + 4 * nY) * kEvalThreads) * fsz;
     if (pb) b = (b + 7) / 8 * 8 + (size_t)(kEvalThreads / 32) * 2 * ntab * 8;
     return b;
 }
@@ -686,7 +703,7 @@ template <typename FT, int L>
 static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
     constexpr int nY = (L + 1) * (L + 1);
     const size_t fsz = sizeof(FT);
-    const size_t tab = 2 * (size_t)(o->nRad * o->K * o->NZ) * fsz;
+    const size_t tab = 3 * (size_t)(o->nRad * o->K * o->NZ) * fsz;
     const size_t per_warp = epb_warp_words((int)o->nRad, nY) * fsz;
     int nw = 8;
     while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;

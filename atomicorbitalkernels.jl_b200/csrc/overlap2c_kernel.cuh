@@ -75,11 +75,6 @@ __device__ __forceinline__ double2 lds128d(uint32_t a) {
     asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
     return v;
 }
-__device__ __forceinline__ float ex2_approx(float x) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
 
 // Zero block (a shell pair with no primitive pair: an absent shell).
 template <int LA, int LB, typename FT>
