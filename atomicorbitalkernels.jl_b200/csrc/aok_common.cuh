@@ -73,6 +73,25 @@ struct Item {
     int16_t sa, sb;
 };
 
+// 2C forward stage images.  Per species pair, the records of the items in
+// execution order are cut into chunks that fit the kernel's shared-memory
+// stage; a chunk is [one ExecItem per item, padded to 16 bytes][the items'
+// records].  A segment is a run of items of one panel inside one chunk.
+struct __align__(8) ExecItem {
+    int16_t cls;  // la*4 + lb
+    int16_t n;    // primitive pairs (records)
+    int16_t rec;  // 16-byte offset of the item's first record in the stage
+    int16_t dst;  // element offset of the block's (0,0) entry in a lane's slab
+};
+struct __align__(8) Seg {
+    int it0, it1;  // items [it0, it1) of the pair's execution order
+    int ibase;     // first item of the chunk: its ExecItem opens the stage
+    int off;       // 16-byte offset of the chunk in the packed array
+    int n16;       // chunk size, 16-byte words
+    int pn;        // panel, + kSegPanelEnd when the segment closes the panel
+};
+constexpr int kSegPanelEnd = 256;
+
 struct Panels {
     int n;                          // number of panels
     int col0[kMaxPanels + 1];       // first output column of each panel (+ N)

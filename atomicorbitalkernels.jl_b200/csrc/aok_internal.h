@@ -20,9 +20,6 @@ struct aok_plan {
     // shell tables on the device
     int* d_ls = nullptr;             // ns
     int* d_boff = nullptr;           // ns+1
-    // primitive-pair records (NZ*NZ*ns*ns*K*K) and counts (NZ*NZ*ns*ns)
-    void* d_pp = nullptr;
-    int* d_npp = nullptr;
     // species-pair bins: permutation, tiles, tile count, work counter
     int* d_perm = nullptr;
     int4* d_tiles = nullptr;
@@ -34,8 +31,13 @@ struct aok_plan {
     int* d_err = nullptr;
     // 2C forward schedule
     aok::Item* d_items = nullptr;    // static item list (nitems), panel-major
-    aok::Item* d_order = nullptr;    // per species pair execution order (NZ*NZ*nitems)
     int nitems = 0;
+    // stage images of the forward kernel (k_pack2c): packed chunks and segments
+    void* d_pk = nullptr;            // NZ*NZ regions of pair16 16-byte words
+    aok::Seg* d_segs = nullptr;      // NZ*NZ regions of seg_stride segments
+    int* d_nseg = nullptr;           // segments per species pair
+    int pair16 = 0, seg_stride = 0;
+    size_t stage_bytes = 0;          // shared-memory stage of the forward kernel
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
     int max_bin_blocks = 0;

@@ -105,16 +105,12 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
                           "cudaDeviceGetAttribute")) != AOK_OK)
         return fail(st);
     const size_t fsz = precision == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    const size_t ppsz = precision == AOK_PREC_F64 ? kRecMaxBytesF64 : kRecMaxBytesF32;
-    const size_t npairs = (size_t)(NZ * NZ * nshells * nshells);
     p->max_tiles = (int)((max_batch + kTileB - 1) / kTileB + NZ * NZ + 1);
     std::vector<int> ls32(nshells), boff32(nshells + 1);
     for (int64_t s = 0; s < nshells; ++s) ls32[s] = (int)ls[s];
     for (int64_t s = 0; s <= nshells; ++s) boff32[s] = (int)p->boff[s];
     if ((st = dmalloc(&p->d_ls, nshells, "cudaMalloc(ls)")) ||
         (st = dmalloc(&p->d_boff, nshells + 1, "cudaMalloc(boff)")) ||
-        (st = dmalloc_bytes(&p->d_pp, npairs * K * K * ppsz, "cudaMalloc(pp)")) ||
-        (st = dmalloc(&p->d_npp, npairs, "cudaMalloc(npp)")) ||
         (st = dmalloc(&p->d_perm, (size_t)max_batch, "cudaMalloc(perm)")) ||
         (st = dmalloc(&p->d_tiles, (size_t)p->max_tiles, "cudaMalloc(tiles)")) ||
         (st = dmalloc(&p->d_ntiles, 1, "cudaMalloc(ntiles)")) ||
@@ -142,11 +138,12 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
 
 int aok_plan_destroy(aok_plan* p) {
     if (!p) return AOK_OK;
-    void* bufs[] = {p->d_ls,        p->d_boff,      p->d_pp,        p->d_npp,        p->d_perm,
+    void* bufs[] = {p->d_ls,        p->d_boff,      p->d_perm,
                     p->d_tiles,     p->d_ntiles,    p->d_tbase,     p->d_counter,    p->d_err,
-                    p->d_items,     p->d_order,     p->d_blockhist, p->d_gb_zeta,    p->d_gb_coef,
+                    p->d_items,     p->d_blockhist, p->d_gb_zeta,    p->d_gb_coef,
                     p->d_pb_rec,    p->d_pb_counts, p->d_pb_items,  p->d_pb_itemidx, p->d_pb_rows,
-                    p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3};
+                    p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3,
+                    p->d_pk,        p->d_segs,      p->d_nseg};
     for (void* b : bufs) dfree(b);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);

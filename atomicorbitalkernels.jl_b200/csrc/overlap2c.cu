@@ -4,35 +4,35 @@
 // and batch_S_kernel! (src/integrals/kernels_2c.jl:110-224).
 //
 // Pipeline per call (all stream-ordered, no host synchronisation):
-//   k_prep2c    one warp per (species pair, shell pair): the geometry-free
-//               primitive-pair records (w, mu, a/p, b/p, 1/2p) in FP64,
+//   k_pack2c    per species pair: the execution order of the shell pairs and
+//               their geometry-free primitive-pair records (FP64-computed),
 //               compacted to the non-zero-coefficient pairs in the
-//               reference's (ip, jp) order.
-//   k_order2c   per species pair, the execution order of the work items.
+//               reference's (ip, jp) order and packed with item headers in
+//               execution order into chunks that fit the forward kernel's
+//               shared-memory stage.
 //   k_bin_*     counting sort of the batch by species pair; tiles of 32
 //               batch elements of one species pair; resets the work counter.
 //   k_overlap2c persistent kernel (two CTAs per SM for FP32, one for FP64)
-//               draining the tile queue.
+//               draining the tile queue (overlap2c_kernel.cuh).
 //               Lane = batch element, so a warp runs one shell pair for 32
-//               geometries with identical control flow.  Shell-pair classes
-//               (la, lb) are compile-time specialised: the 1-D overlap
-//               tables E^x_ij (Obara-Saika form of the MD t=0 coefficients)
-//               and the block accumulators live in registers.  Blocks are
-//               written into a shared-memory slab holding complete output
-//               columns of 32 batch elements, which is then streamed out
-//               with fully coalesced stores (each batch element's (N,N) slab
+//               geometries with identical control flow.  Per shell pair the
+//               primitive-pair loop accumulates the <= 8 moments
+//               exp(-mu R^2) w rb^al ra^be q^ga (one FMA each), and the
+//               compile-time geometry terms of the class (md2c.cuh) turn them
+//               into the block once.  Records come from the shared-memory
+//               stage; blocks go into a shared-memory slab holding complete
+//               output columns of 32 batch elements, which is then streamed
+//               out with coalesced stores (each batch element's (N,N) matrix
 //               is contiguous in the reference layout).
 //
 // The reference's l >= 2 stride aliasing (block element lin = c1 + (2la+1)*c2,
 // read back as blk[i + nbf_a*j], kernels_2c.jl:209-223) is reproduced at
-// compile time: component pair (c1, c2) accumulates into element
-// lin = c1 + (2la+1) c2 of the (nbf_a, nbf_b) block.
+// compile time in the term tables.
 //
-// FP32C precision: FP32 arithmetic; the Gaussian prefactor exp(-mu R^2) uses
-// a double-float argument (mu and R^2 each carried as hi + lo), and the
-// primitive-pair sum is accumulated per ip row in FP32 and folded into the
-// running block sum with TwoSum whenever ip changes; the rounding errors are
-// collected in the shared-memory slab and added at the end.
+// FP32C precision: FP32 arithmetic on FP64-computed records; the Gaussian
+// prefactor exp(-mu R^2) uses a double-float argument (mu log2 e and R^2 each
+// carried as hi + lo), and the moments are summed per bra row in FP32 and
+// folded into the running sums with TwoSum at each row's end.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -118,97 +118,211 @@ template <typename FT> __host__ __device__ constexpr int rec_words16(int la, int
 template <> __host__ __device__ constexpr int rec_words16<float>(int la, int lb) { return rec_words16_f32(la, lb); }
 template <> __host__ __device__ constexpr int rec_words16<double>(int la, int lb) { return rec_words16_f64(la, lb); }
 
-// One warp per (species pair, shell pair); lanes sweep the K x K primitive
-// grid in ip-major order and compact the non-zero-coefficient pairs with a
-// ballot, preserving the reference's (ip, jp) summation order.  Records of a
-// shell pair are contiguous at the class's record size, starting at the
-// shell pair's region of K*K maximum-size records.
-template <typename FT>
-__global__ void k_prep2c(FT* __restrict__ pp, int* __restrict__ npp, const FT* __restrict__ zeta,
-                         const FT* __restrict__ coef, const int* __restrict__ ls, int ns, int K, int NZ) {
-    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (q >= NZ * NZ * ns * ns) return;
-    int sb = q % ns;
-    int t = q / ns;
-    int sa = t % ns;
-    t /= ns;
-    int gb = t % NZ, ga = t / NZ;
-    const int la = ls[sa], lb = ls[sb];
-    constexpr int kMaxWords = sizeof(FT) == 4 ? kRecMaxBytesF32 / 4 : kRecMaxBytesF64 / 8;
-    const int words = rec_words16<FT>(la, lb) * (16 / (int)sizeof(FT));
-    FT* out = pp + (size_t)q * K * K * kMaxWords;
-    int n = 0;
-    // every row (ip with a non-zero coefficient) holds the same jp set
-    int nb = 0;
-    for (int jp = 0; jp < K; ++jp) nb += coef[sb + ns * (jp + K * gb)] != FT(0);
-    for (int e0 = 0; e0 < K * K; e0 += 32) {
-        const int e = e0 + lane;
-        const int ip = e / K, jp = e % K;
-        double ca = 0.0, cb = 0.0, aa = 0.0, ab = 0.0;
-        if (e < K * K) {
-            ca = (double)coef[sa + ns * (ip + K * ga)];
-            cb = (double)coef[sb + ns * (jp + K * gb)];
-            aa = (double)zeta[sa + ns * (ip + K * ga)];
-            ab = (double)zeta[sb + ns * (jp + K * gb)];
-        }
-        const bool valid = (e < K * K) && ca != 0.0 && cb != 0.0;
-        const unsigned m = __ballot_sync(0xffffffffu, valid);
-        if (valid) fill_pp(out + (size_t)(n + __popc(m & ((1u << lane) - 1u))) * words, la, lb, ca, cb, aa, ab, nb);
-        n += __popc(m);
-    }
-    if (lane == 0) npp[q] = n;
-}
-
 // --------------------------------------------------------------------------
-// Execution order of the work items of one species pair (each item carries its
-// number of primitive pairs in `chunk`): within each panel,
-// heavier classes first (warps that run concurrently share the class's code
-// in the instruction cache), and inside a class the items with more primitive
-// pairs first (longest-processing-time order for the warps' dynamic queue).
-// One CTA per species pair, rank sort in shared memory.
+// Execution order, records and stage images of one species pair.
+//
+// Primitive pairs: those with non-zero coefficients on both sides, na * nb
+// per shell pair, in the reference's (ip, jp) order (ip-major); each record
+// carries nb as its row length.
+//
+// Order: within each panel, heavier classes first (warps that run
+// concurrently share the class's code in the instruction cache), and inside a
+// class the items with more primitive pairs first (longest-processing-time
+// order for the warps' dynamic queue); rank sort in shared memory, or the
+// static order for bases of more than kOrderMax items.
+//
+// Stage images: the items, in that order, are cut greedily into chunks of at
+// most stage16 16-byte words, each laid out as [ExecItem per item, padded to
+// 16 bytes][the items' records]; the segments are the runs of items of one
+// panel inside one chunk.  The cut is a binary search per chunk over the
+// prefix sums of the record sizes.  The host sizes the stage to hold the
+// largest item, so every chunk holds at least one.
+//
+// Grid (species pairs, parts): every CTA of a pair sorts and cuts (cheap,
+// identical results); part 0 writes the segments; the parts share the record
+// computation, one warp per item, lanes over the K x K primitive grid with a
+// ballot compaction.  Dynamic shared memory: pack2c_smem(nitems) bytes.
 // --------------------------------------------------------------------------
 constexpr int kOrderMax = 2048;
 
+size_t pack2c_smem(int nitems) { return (size_t)28 * nitems + 16; }
+int pack2c_parts(int nitems) { return std::min(32, std::max(1, (nitems + 7) / 8)); }
 
-__global__ void __launch_bounds__(256) k_order2c(Item* __restrict__ order, const Item* __restrict__ items,
-                                                 const int* __restrict__ npp, Panels panels, int nitems, int ns) {
-    __shared__ unsigned long long key[kOrderMax];
-    const int pair = blockIdx.x;
-    Item* out = order + (size_t)pair * nitems;
-    if (nitems > kOrderMax) {  // very large bases: keep the static order
-        for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
-            Item o = items[i];
-            o.chunk = (int16_t)min(npp[((size_t)pair * ns + o.sa) * ns + o.sb], 32767);
-            out[i] = o;
-        }
-        return;
+template <typename FT>
+__global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __restrict__ segs,
+                                                int* __restrict__ nseg, const Item* __restrict__ items,
+                                                const FT* __restrict__ zeta, const FT* __restrict__ coef,
+                                                Panels panels, const int* __restrict__ boff, int nitems, int ns,
+                                                int K, int NZ, int N, int stage16, int pair16, int seg_stride) {
+    extern __shared__ unsigned long long psm64[];
+    unsigned long long* key = psm64;                               // nitems
+    Item* sorted = reinterpret_cast<Item*>(psm64 + nitems);        // nitems; chunk = primitive pairs
+    int* P = reinterpret_cast<int*>(psm64 + 2 * (size_t)nitems);   // nitems + 1: exclusive prefix, record words
+    int* cst = P + nitems + 1;                                     // first item of chunk j (+ nitems)
+    int* chd = cst + nitems + 1;                                   // header words before chunk j
+    __shared__ int s_item0[kMaxPanels + 1], s_col0[kMaxPanels + 1], s_boff[kMaxShells + 1];
+    __shared__ int s_nnz[2][kMaxShells];
+    __shared__ int s_wsum[8], s_nch;
+    const int pair = blockIdx.x, ga = pair / NZ, gb = pair % NZ;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = 8;
+    const int npan = panels.n;
+    if (tid <= npan) {
+        s_item0[tid] = panels.item0[tid];
+        s_col0[tid] = panels.col0[tid];
     }
-    for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
-        const Item it = items[i];
-        int pn = 0;
-        while (pn + 1 < panels.n && i >= panels.item0[pn + 1]) ++pn;
-        // heavy classes first (terms of the geometry transform), grouped by class
-        // so that the warps of a CTA mostly run the same code; then by primitive pairs
-        const int la = it.cls >> 2, lb = it.cls & 3;
-        const int n = npp[((size_t)pair * ns + it.sa) * ns + it.sb];
-        const unsigned long long k = ((unsigned long long)pn << 48) |
-                                     ((unsigned long long)(0xFFFF - md_terms(la, lb)) << 32) |
-                                     ((unsigned long long)(0xFFFF - min(n, 0xFFFF)) << 16) |
-                                     (unsigned long long)it.cls;
-        key[i] = (k << 0);
+    if (tid <= ns) s_boff[tid] = boff[tid];
+    for (int i = tid; i < 2 * ns; i += blockDim.x) {
+        const int sh = i % ns, g = i < ns ? ga : gb;
+        int c = 0;
+        for (int k = 0; k < K; ++k) c += coef[sh + ns * (k + K * g)] != FT(0);
+        s_nnz[i / ns][sh] = c;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nitems; i += blockDim.x) {
-        const unsigned long long ki = key[i];
-        int r = 0;
-        for (int j = 0; j < nitems; ++j) {
-            const unsigned long long kj = key[j];
-            r += (kj < ki) || (kj == ki && j < i);
+    auto panel_of = [&](int i) {
+        int pn = 0;
+        while (pn + 1 < npan && i >= s_item0[pn + 1]) ++pn;
+        return pn;
+    };
+    for (int i = tid; i < nitems; i += blockDim.x) {
+        Item it = items[i];
+        const int n = s_nnz[0][it.sa] * s_nnz[1][it.sb];
+        it.chunk = (int16_t)n;
+        sorted[i] = it;
+        const int la = it.cls >> 2, lb = it.cls & 3;
+        key[i] = ((unsigned long long)panel_of(i) << 48) |
+                 ((unsigned long long)(0xFFFF - md_terms(la, lb)) << 32) |
+                 ((unsigned long long)(0xFFFF - n) << 16) | (unsigned long long)it.cls;
+    }
+    __syncthreads();
+    if (nitems <= kOrderMax) {
+        Item mine[kOrderMax / 256];
+        int rank[kOrderMax / 256];
+#pragma unroll
+        for (int t = 0; t < kOrderMax / 256; ++t) {
+            const int i = tid + 256 * t;
+            rank[t] = -1;
+            if (i < nitems) {
+                const unsigned long long ki = key[i];
+                int r = 0;
+                for (int j = 0; j < nitems; ++j) {
+                    const unsigned long long kj = key[j];
+                    r += (kj < ki) || (kj == ki && j < i);
+                }
+                rank[t] = r;
+                mine[t] = sorted[i];
+            }
         }
-        Item o = items[i];
-        o.chunk = (int16_t)min(npp[((size_t)pair * ns + o.sa) * ns + o.sb], 32767);
-        out[r] = o;
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < kOrderMax / 256; ++t)
+            if (rank[t] >= 0) sorted[rank[t]] = mine[t];
+        __syncthreads();
+    }
+    // record words per item and their exclusive prefix (block scan)
+    {
+        const int per = (nitems + 255) / 256;
+        const int i0 = min(nitems, tid * per), i1 = min(nitems, i0 + per);
+        int sum = 0;
+        for (int i = i0; i < i1; ++i) {
+            const int w = (int)sorted[i].chunk * rec_words16<FT>(sorted[i].cls >> 2, sorted[i].cls & 3);
+            P[i] = w;
+            sum += w;
+        }
+        int incl = sum;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        if (lane == 31) s_wsum[warp] = incl;
+        __syncthreads();
+        int run = incl - sum;
+        for (int w = 0; w < warp; ++w) run += s_wsum[w];
+        for (int i = i0; i < i1; ++i) {
+            const int w = P[i];
+            P[i] = run;
+            run += w;
+        }
+        if (tid == 255) P[nitems] = run;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int nch = 0, c0 = 0, h = 0;
+        while (c0 < nitems) {
+            cst[nch] = c0;
+            chd[nch] = h;
+            int lo = c0 + 1, hi = nitems;  // the largest c1 whose chunk [c0, c1) fits
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if ((mid - c0 + 1) / 2 + P[mid] - P[c0] <= stage16) lo = mid;
+                else hi = mid - 1;
+            }
+            h += (lo - c0 + 1) / 2;
+            c0 = lo;
+            ++nch;
+        }
+        cst[nch] = nitems;
+        chd[nch] = h;
+        s_nch = nch;
+        if (blockIdx.y == 0) {
+            Seg* sg = segs + (size_t)pair * seg_stride;
+            int nout = 0;
+            for (int j = 0; j < nch; ++j) {
+                const int a0 = cst[j], a1 = cst[j + 1];
+                const int off = pair * pair16 + P[a0] + chd[j];
+                const int n16 = (a1 - a0 + 1) / 2 + P[a1] - P[a0];
+                for (int a = a0; a < a1;) {  // split the chunk at panel starts
+                    const int pn = panel_of(a);
+                    const int b = min(a1, s_item0[pn + 1]);
+                    sg[nout++] = Seg{a, b, a0, off, n16, pn + (b == s_item0[pn + 1] ? kSegPanelEnd : 0)};
+                    a = b;
+                }
+            }
+            nseg[pair] = nout;
+        }
+    }
+    __syncthreads();
+    const int nch = s_nch;
+    for (int i = blockIdx.y * NW + warp; i < nitems; i += gridDim.y * NW) {
+        const Item it = sorted[i];
+        int lo = 0, hi = nch - 1;  // chunk j with cst[j] <= i < cst[j + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cst[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const int a0 = cst[lo], a1 = cst[lo + 1];
+        float4* cbase = pk + (size_t)pair * pair16 + P[a0] + chd[lo];
+        const int r0 = (a1 - a0 + 1) / 2 + P[i] - P[a0];
+        const int la = it.cls >> 2, lb = it.cls & 3;
+        if (lane == 0) {
+            const int pn = panel_of(i);
+            ExecItem e;
+            e.cls = it.cls;
+            e.n = it.chunk;
+            e.rec = (int16_t)r0;
+            e.dst = (int16_t)((s_boff[it.sb] - s_col0[pn]) * N + s_boff[it.sa]);
+            reinterpret_cast<ExecItem*>(cbase)[i - a0] = e;
+        }
+        FT* out = reinterpret_cast<FT*>(cbase + r0);
+        const int words = rec_words16<FT>(la, lb) * (16 / (int)sizeof(FT));
+        const int nb = s_nnz[1][it.sb];
+        int n = 0;
+        for (int e0 = 0; e0 < K * K; e0 += 32) {
+            const int e = e0 + lane;
+            const int ip = e / K, jp = e % K;
+            double ca = 0.0, cb = 0.0, aa = 0.0, ab = 0.0;
+            if (e < K * K) {
+                ca = (double)coef[it.sa + ns * (ip + K * ga)];
+                cb = (double)coef[it.sb + ns * (jp + K * gb)];
+                aa = (double)zeta[it.sa + ns * (ip + K * ga)];
+                ab = (double)zeta[it.sb + ns * (jp + K * gb)];
+            }
+            const bool valid = (e < K * K) && ca != 0.0 && cb != 0.0;
+            const unsigned m = __ballot_sync(0xffffffffu, valid);
+            if (valid) fill_pp(out + (size_t)(n + __popc(m & ((1u << lane) - 1u))) * words, la, lb, ca, cb, aa, ab, nb);
+            n += __popc(m);
+        }
     }
 }
 
@@ -370,20 +484,36 @@ __global__ void k_bin_identity(int B, int np, int* __restrict__ perm, int4* __re
 // Host side: schedule and launchers.
 // --------------------------------------------------------------------------
 
+static size_t npairs_of(const aok_plan* p) { return (size_t)(p->NZ * p->NZ); }
+
 int setup_overlap2c_schedule(aok_plan* p) {
     const int ns = (int)p->ns, N = (int)p->N;
-    const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
+    const bool f64 = p->prec == AOK_PREC_F64;
+    const size_t fsz = f64 ? sizeof(double) : sizeof(float);
+    // Stage images (k_pack2c): a species pair's records fill at most pair16
+    // 16-byte words (every primitive pair present, plus item headers and
+    // padding); the stage holds one chunk and at least the largest item.
+    const size_t K2 = (size_t)p->K * p->K;
+    size_t pair16 = 2 * (size_t)ns * ns;
+    for (int a = 0; a < ns; ++a)
+        for (int b = 0; b < ns; ++b) {
+            const int la = (int)p->ls[a], lb = (int)p->ls[b];
+            pair16 += K2 * (size_t)(f64 ? rec_words16_f64(la, lb) : rec_words16_f32(la, lb));
+        }
+    const size_t one_item = 16 + K2 * (f64 ? kRecMaxBytesF64 : kRecMaxBytesF32);
+    const size_t stage = std::max(one_item, std::min((size_t)(f64 ? 48 : 24) * 1024, pair16 * 16));
+    if (stage > (size_t)200 * 1024)
+        return set_error(AOK_ERR_UNSUPPORTED, "too many primitives per shell for the 2C stage");
     // FP32: two CTAs per SM; FP64: one.  The slab shares the CTA's shared memory
-    // with the per-warp record buffers (K*K maximum-size records per warp); a
-    // basis whose widest shell column would not fit falls back to one CTA per SM.
-    const size_t recbuf = (size_t)8 * p->K * p->K * (p->prec == AOK_PREC_F64 ? kRecMaxBytesF64 : kRecMaxBytesF32);
-    size_t budget = p->prec == AOK_PREC_F64 ? (size_t)120 * 1024
-                                            : (size_t)112 * 1024 - std::min(recbuf, (size_t)112 * 1024);
+    // with the stage; a basis whose widest shell column would not fit falls back
+    // to one CTA per SM.
+    size_t budget = f64 ? std::min((size_t)120 * 1024, (size_t)224 * 1024 - stage)
+                        : (size_t)112 * 1024 - std::min(stage, (size_t)112 * 1024);
     {
         size_t widest = 0;
         for (int s = 0; s < ns; ++s) widest = std::max(widest, (size_t)ncart((int)p->ls[s]));
         const size_t need = ((size_t)N * widest + 1) * kTileB * fsz;
-        if (budget < need) budget = (size_t)224 * 1024 - std::min(recbuf, (size_t)224 * 1024);
+        if (budget < need) budget = (size_t)224 * 1024 - stage;
     }
     // panels: consecutive ket shells whose column range fits the slab budget
     std::vector<int> pcols{0};
@@ -411,7 +541,8 @@ int setup_overlap2c_schedule(aok_plan* p) {
     for (int i = 0; i < npan; ++i) maxw = std::max(maxw, (size_t)(pcols[i + 1] - pcols[i]));
     p->slab_stride = stride_for((int)maxw);
     p->smem_bytes = p->slab_stride * kTileB * fsz;
-    if (p->smem_bytes > 227 * 1024)
+    p->stage_bytes = stage;
+    if ((p->smem_bytes + 15) / 16 * 16 + stage > 227 * 1024)
         return set_error(AOK_ERR_UNSUPPORTED, "a single shell column exceeds the shared-memory slab");
     // items per panel, heaviest first
     std::vector<Item> items;
@@ -432,10 +563,27 @@ int setup_overlap2c_schedule(aok_plan* p) {
     p->panels.col0[npan] = pcols[npan];
     p->panels.item0[npan] = (int)items.size();
     p->nitems = (int)items.size();
-    cudaError_t e = cudaMalloc(&p->d_items, sizeof(Item) * items.size());
+    if (pair16 * npairs_of(p) >= ((size_t)1 << 31))
+        return set_error(AOK_ERR_UNSUPPORTED, "basis too large for the 2C stage images");
+    p->pair16 = (int)pair16;
+    p->seg_stride = p->nitems + npan;
+    const size_t npairs = (size_t)(p->NZ * p->NZ);
+    cudaError_t e = cudaMalloc(&p->d_pk, 16 * pair16 * npairs);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(pk)");
+    e = cudaMalloc(&p->d_segs, sizeof(Seg) * p->seg_stride * npairs);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(segs)");
+    e = cudaMalloc(&p->d_nseg, sizeof(int) * npairs);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(nseg)");
+    e = cudaMalloc(&p->d_items, sizeof(Item) * items.size());
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(items)");
-    e = cudaMalloc(&p->d_order, sizeof(Item) * items.size() * p->NZ * p->NZ);
-    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(order)");
+    if (pack2c_smem((int)items.size()) > 48 * 1024) {
+        const int smem = (int)pack2c_smem((int)items.size());
+        if ((e = cudaFuncSetAttribute(k_pack2c<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+                cudaSuccess ||
+            (e = cudaFuncSetAttribute(k_pack2c<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+                cudaSuccess)
+            return cuda_status(e, "cudaFuncSetAttribute(k_pack2c)");
+    }
     p->max_bin_blocks = kBinMaxBlocks;
     e = cudaMalloc(&p->d_blockhist, sizeof(int) * p->max_bin_blocks * p->NZ * p->NZ);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(blockhist)");
@@ -460,18 +608,20 @@ int launch_gb_pad(aok_plan* p, const int64_t* nprim, const int64_t* prim_offset,
 }
 
 int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s) {
-    int n = (int)(p->NZ * p->NZ * p->ns * p->ns);
-    int th = 128, bl = (n * 32 + th - 1) / th;
+    const dim3 grid((unsigned)(p->NZ * p->NZ), (unsigned)pack2c_parts(p->nitems));
+    const size_t smem = pack2c_smem(p->nitems);
+    const int stage16 = (int)(p->stage_bytes / 16);
     if (p->prec == AOK_PREC_F64)
-        k_prep2c<double><<<bl, th, 0, s>>>((double*)p->d_pp, p->d_npp, (const double*)zeta, (const double*)coef,
-                                           p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
+        k_pack2c<double><<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items,
+                                                 (const double*)zeta, (const double*)coef, p->panels, p->d_boff,
+                                                 p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16,
+                                                 p->pair16, p->seg_stride);
     else
-        k_prep2c<float><<<bl, th, 0, s>>>((float*)p->d_pp, p->d_npp, (const float*)zeta, (const float*)coef,
-                                          p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ);
-    AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_prep2c"));
-    k_order2c<<<(int)(p->NZ * p->NZ), 256, 0, s>>>(p->d_order, p->d_items, p->d_npp, p->panels, p->nitems,
-                                                  (int)p->ns);
-    return cuda_status(cudaGetLastError(), "k_order2c");
+        k_pack2c<float><<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items,
+                                                (const float*)zeta, (const float*)coef, p->panels, p->d_boff,
+                                                p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16,
+                                                p->pair16, p->seg_stride);
+    return cuda_status(cudaGetLastError(), "k_pack2c");
 }
 
 int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,

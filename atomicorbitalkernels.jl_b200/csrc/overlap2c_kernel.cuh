@@ -198,42 +198,72 @@ struct Ov2Params {
     const FT* posB;
     FT scale;
     int use_scale;
-    const FT* pp;         // records: per (species pair, shell pair) a region of K*K maximum-size records
+    const float4* pk;     // stage images: per species pair, chunks of [ExecItem...][records]
+    const Seg* segs;      // per species pair: seg_stride segments
+    const int* nseg;      // segments per species pair
+    int seg_stride;
     const int* perm;
     const int4* tiles;
     const int* ntiles;
     unsigned* counter;
-    const Item* items;   // per species pair: items in execution order (nitems each)
-    int nitems;
     Panels panels;
-    int ns, K, N, slab_stride;
-    unsigned rec_offset;  // byte offset of the per-warp record buffers in dynamic smem
-    int boff[kMaxShells + 1];
+    int N, slab_stride;
+    unsigned stage_offset;  // byte offset of the stage in dynamic shared memory
 };
 
+// Copy n16 16-byte words of a packed chunk into the stage, all threads, four
+// loads in flight per thread.
+template <int THREADS>
+__device__ __forceinline__ void stage_chunk(float4* dst, const float4* __restrict__ src, int n16) {
+    int i = threadIdx.x;
+    for (; i + 3 * THREADS < n16; i += 4 * THREADS) {
+        const float4 v0 = __ldg(src + i), v1 = __ldg(src + i + THREADS), v2 = __ldg(src + i + 2 * THREADS),
+                     v3 = __ldg(src + i + 3 * THREADS);
+        dst[i] = v0;
+        dst[i + THREADS] = v1;
+        dst[i + 2 * THREADS] = v2;
+        dst[i + 3 * THREADS] = v3;
+    }
+    for (; i < n16; i += THREADS) dst[i] = __ldg(src + i);
+}
+
+// Persistent CTAs take tiles (<= 32 batch elements of one species pair, one per
+// lane) from a global queue.  Per tile the CTA walks the pair's segments: the
+// warps take the segment's items from a shared counter and run them on the
+// staged chunk, writing their blocks into the lane's slab of the current panel;
+// at a panel's end the CTA streams the slab out.  A chunk is copied into the
+// stage only when it is not there already (consecutive tiles of one species
+// pair whose records fit one chunk stage them once).
 template <typename FT, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_constant__ Ov2Params<FT> P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FT* slab = reinterpret_cast<FT*>(smem_raw);
-    __shared__ int s_tile;
-    __shared__ int s_next[kMaxPanels];
+    float4* stage = reinterpret_cast<float4*>(smem_raw + P.stage_offset);
+    const ExecItem* sitems = reinterpret_cast<const ExecItem*>(stage);
+    const uint32_t stage_saddr = (uint32_t)__cvta_generic_to_shared(stage);
+    __shared__ int s_tile, s_cnt;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = THREADS / 32;
-    constexpr int MAXREC16 = (sizeof(FT) == 4 ? kRecMaxBytesF32 : kRecMaxBytesF64) / 16;
-    // per-warp staging buffer for the current item's records (K*K records)
-    float4* recbuf = reinterpret_cast<float4*>(smem_raw + P.rec_offset) + (size_t)warp * P.K * P.K * MAXREC16;
-    const uint32_t rec_saddr = (uint32_t)__cvta_generic_to_shared(recbuf);
     const int ntiles = *P.ntiles;
+    int staged = -1;  // packed offset of the chunk in the stage (the same in every thread)
     for (;;) {
         if (threadIdx.x == 0) {
             s_tile = (int)atomicAdd(P.counter, 1u);
-            for (int i = 0; i < P.panels.n; ++i) s_next[i] = 0;
+            s_cnt = 0;
         }
         __syncthreads();
         const int tile = s_tile;
         if (tile >= ntiles) break;
         const int4 td = P.tiles[tile];
         const int pair = td.x, start = td.y, cnt = td.z;
+        const Seg* segs = P.segs + (size_t)pair * P.seg_stride;
+        const int nseg = P.nseg[pair];
+        Seg S = segs[0];
+        if (S.off != staged) {
+            stage_chunk<THREADS>(stage, P.pk + S.off, S.n16);
+            staged = S.off;
+            __syncthreads();
+        }
         Geo<FT> g;
         if (lane < cnt) {
             const int b = P.perm[start + lane];
@@ -243,46 +273,43 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
             load_geo(g, z, z, P.scale, false);
         }
         FT* sl = slab + (size_t)lane * P.slab_stride;
-        for (int pn = 0; pn < P.panels.n; ++pn) {
-            const int col0 = P.panels.col0[pn];
-            const int i0 = P.panels.item0[pn], i1 = P.panels.item0[pn + 1];
-            const Item* order = P.items + (size_t)pair * P.nitems;
+        for (int k = 0; k < nseg; ++k) {
             for (;;) {
                 int it = 0;
-                if (lane == 0) it = atomicAdd(&s_next[pn], 1);
-                it = __shfl_sync(0xffffffffu, it, 0) + i0;
-                if (it >= i1) break;
-                const Item wi = order[it];
-                const int q = (pair * P.ns + wi.sa) * P.ns + wi.sb;
-                const int n = wi.chunk;  // primitive pairs of the item
-                {
-                    const int rec16 = sizeof(FT) == 4 ? rec_words16_f32(wi.cls >> 2, wi.cls & 3)
-                                                      : rec_words16_f64(wi.cls >> 2, wi.cls & 3);
-                    const float4* src = reinterpret_cast<const float4*>(P.pp) + (size_t)q * P.K * P.K * MAXREC16;
-                    for (int i = lane; i < n * rec16; i += 32) recbuf[i] = __ldg(src + i);
-                    __syncwarp();
-                }
-                FT* dst = sl + (size_t)(P.boff[wi.sb] - col0) * P.N + P.boff[wi.sa];
-                dispatch(wi.cls, rec_saddr, n, g, dst, P.N);
-                __syncwarp();
+                if (lane == 0) it = atomicAdd(&s_cnt, 1);
+                it = __shfl_sync(0xffffffffu, it, 0) + S.it0;
+                if (it >= S.it1) break;
+                const ExecItem e = sitems[it - S.ibase];
+                dispatch(e.cls, stage_saddr + 16u * (uint32_t)e.rec, e.n, g, sl + e.dst, P.N);
             }
+            const Seg Sn = k + 1 < nseg ? segs[k + 1] : S;
             __syncthreads();
-            const int len = (P.panels.col0[pn + 1] - col0) * P.N;
-            for (int bl = warp; bl < cnt; bl += NW) {
-                const int bg = P.perm[start + bl];
-                FT* o = P.out + (size_t)bg * P.N * P.N + (size_t)col0 * P.N;
-                const FT* s = slab + (size_t)bl * P.slab_stride;
-                int e = lane;
-                for (; e + 96 < len; e += 128) {  // four loads in flight, streaming stores
-                    const FT v0 = s[e], v1 = s[e + 32], v2 = s[e + 64], v3 = s[e + 96];
-                    __stcs(o + e, v0);
-                    __stcs(o + e + 32, v1);
-                    __stcs(o + e + 64, v2);
-                    __stcs(o + e + 96, v3);
+            if (S.pn >= kSegPanelEnd) {  // the panel is complete: stream the slab out
+                const int pn = S.pn - kSegPanelEnd;
+                const int col0 = P.panels.col0[pn];
+                const int len = (P.panels.col0[pn + 1] - col0) * P.N;
+                for (int bl = warp; bl < cnt; bl += NW) {
+                    const int bg = P.perm[start + bl];
+                    FT* o = P.out + (size_t)bg * P.N * P.N + (size_t)col0 * P.N;
+                    const FT* s = slab + (size_t)bl * P.slab_stride;
+                    int e = lane;
+                    for (; e + 96 < len; e += 128) {  // four loads in flight, streaming stores
+                        const FT v0 = s[e], v1 = s[e + 32], v2 = s[e + 64], v3 = s[e + 96];
+                        __stcs(o + e, v0);
+                        __stcs(o + e + 32, v1);
+                        __stcs(o + e + 64, v2);
+                        __stcs(o + e + 96, v3);
+                    }
+                    for (; e < len; e += 32) __stcs(o + e, s[e]);
                 }
-                for (; e < len; e += 32) __stcs(o + e, s[e]);
             }
+            if (Sn.off != staged) {
+                stage_chunk<THREADS>(stage, P.pk + Sn.off, Sn.n16);
+                staged = Sn.off;
+            }
+            if (threadIdx.x == 0) s_cnt = 0;
             __syncthreads();
+            S = Sn;
         }
     }
 }
@@ -297,23 +324,20 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     P.posB = (const FT*)posB;
     P.scale = (FT)lengthscale;
     P.use_scale = (FT)lengthscale != FT(1);
-    P.pp = (const FT*)p->d_pp;
+    P.pk = (const float4*)p->d_pk;
+    P.segs = p->d_segs;
+    P.nseg = p->d_nseg;
+    P.seg_stride = p->seg_stride;
     P.perm = p->d_perm;
     P.tiles = p->d_tiles;
     P.ntiles = p->d_ntiles;
     P.counter = p->d_counter;
-    P.items = p->d_order;
-    P.nitems = p->nitems;
     P.panels = p->panels;
-    P.ns = (int)p->ns;
-    P.K = (int)p->K;
     P.N = (int)p->N;
     P.slab_stride = (int)p->slab_stride;
-    for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
     const size_t slab = (p->smem_bytes + 15) / 16 * 16;
-    P.rec_offset = (unsigned)slab;
-    const size_t smem = slab + (size_t)(THREADS / 32) * p->K * p->K * (sizeof(FT) == 4 ? kRecMaxBytesF32
-                                                                                         : kRecMaxBytesF64);
+    P.stage_offset = (unsigned)slab;
+    const size_t smem = slab + p->stage_bytes;
     auto kern = k_overlap2c<FT, THREADS, min_blocks<FT>()>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap2c)");
