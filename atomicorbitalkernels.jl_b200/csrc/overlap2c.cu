@@ -146,7 +146,7 @@ template <> __host__ __device__ constexpr int rec_words16<double>(int la, int lb
 constexpr int kOrderMax = 2048;
 
 size_t pack2c_smem(int nitems) { return (size_t)28 * nitems + 16; }
-int pack2c_parts(int nitems) { return std::min(32, std::max(1, (nitems + 7) / 8)); }
+int pack2c_parts(int nitems) { return std::min(16, std::max(1, (nitems + 15) / 16)); }
 
 template <typename FT>
 __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __restrict__ segs,

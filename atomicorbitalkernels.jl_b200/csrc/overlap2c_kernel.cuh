@@ -130,13 +130,21 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, f
                         ++j;
                     }
         }
+        if (q0 == 0) {  // the first row opens the sums exactly
 #pragma unroll
-        for (int m = 0; m < NM; ++m) {
-            float s, e;
-            two_sum(hi[m], part[m], s, e);
-            hi[m] = s;
-            lo[m] += e;
-            part[m] = 0.f;
+            for (int m = 0; m < NM; ++m) {
+                hi[m] = part[m];
+                part[m] = 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                float s, e;
+                two_sum(hi[m], part[m], s, e);
+                hi[m] = s;
+                lo[m] += e;
+                part[m] = 0.f;
+            }
         }
     }
 #pragma unroll
@@ -227,13 +235,27 @@ __device__ __forceinline__ void stage_chunk(float4* dst, const float4* __restric
     for (; i < n16; i += THREADS) dst[i] = __ldg(src + i);
 }
 
+// Geometry of the tile's 32 lanes (zero geometry for lanes past the tile's end).
+template <typename FT>
+__device__ __forceinline__ void tile_geo(Geo<FT>& g, const Ov2Params<FT>& P, int start, int cnt, int lane) {
+    if (lane < cnt) {
+        const int b = P.perm[start + lane];
+        load_geo(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
+    } else {
+        const FT z[3] = {FT(0), FT(0), FT(0)};
+        load_geo(g, z, z, P.scale, false);
+    }
+}
+
 // Persistent CTAs take tiles (<= 32 batch elements of one species pair, one per
 // lane) from a global queue.  Per tile the CTA walks the pair's segments: the
 // warps take the segment's items from a shared counter and run them on the
 // staged chunk, writing their blocks into the lane's slab of the current panel;
 // at a panel's end the CTA streams the slab out.  A chunk is copied into the
 // stage only when it is not there already (consecutive tiles of one species
-// pair whose records fit one chunk stage them once).
+// pair whose records fit one chunk stage them once).  The next tile is
+// claimed when the last segment starts, and its geometry and first chunk are
+// fetched while the last panel streams out, so a tile starts without a wait.
 template <typename FT, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_constant__ Ov2Params<FT> P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -242,38 +264,43 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
     const ExecItem* sitems = reinterpret_cast<const ExecItem*>(stage);
     const uint32_t stage_saddr = (uint32_t)__cvta_generic_to_shared(stage);
     __shared__ int s_tile, s_cnt;
+    __shared__ int4 s_td;
+    __shared__ Geo<FT> s_geo[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = THREADS / 32;
     const int ntiles = *P.ntiles;
     int staged = -1;  // packed offset of the chunk in the stage (the same in every thread)
-    for (;;) {
-        if (threadIdx.x == 0) {
-            s_tile = (int)atomicAdd(P.counter, 1u);
-            s_cnt = 0;
-        }
-        __syncthreads();
-        const int tile = s_tile;
-        if (tile >= ntiles) break;
+    // prologue: the first tile, its geometry and its first chunk
+    if (threadIdx.x == 0) {
+        s_tile = (int)atomicAdd(P.counter, 1u);
+        s_cnt = 0;
+    }
+    __syncthreads();
+    int tile = s_tile;
+    if (tile < ntiles) {
         const int4 td = P.tiles[tile];
+        if (warp == NW - 1) {
+            Geo<FT> g;
+            tile_geo(g, P, td.y, td.z, lane);
+            s_geo[lane] = g;
+            if (lane == 0) s_td = td;
+        }
+        const Seg S0 = P.segs[(size_t)td.x * P.seg_stride];
+        stage_chunk<THREADS>(stage, P.pk + S0.off, S0.n16);
+        staged = S0.off;
+    }
+    __syncthreads();
+    while (tile < ntiles) {
+        const int4 td = s_td;
         const int pair = td.x, start = td.y, cnt = td.z;
+        const Geo<FT> g = s_geo[lane];
         const Seg* segs = P.segs + (size_t)pair * P.seg_stride;
         const int nseg = P.nseg[pair];
-        Seg S = segs[0];
-        if (S.off != staged) {
-            stage_chunk<THREADS>(stage, P.pk + S.off, S.n16);
-            staged = S.off;
-            __syncthreads();
-        }
-        Geo<FT> g;
-        if (lane < cnt) {
-            const int b = P.perm[start + lane];
-            load_geo(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
-        } else {
-            const FT z[3] = {FT(0), FT(0), FT(0)};
-            load_geo(g, z, z, P.scale, false);
-        }
         FT* sl = slab + (size_t)lane * P.slab_stride;
+        int next = ntiles;
+        Seg S = segs[0];
         for (int k = 0; k < nseg; ++k) {
+            if (k == nseg - 1 && threadIdx.x == 0) s_tile = (int)atomicAdd(P.counter, 1u);
             for (;;) {
                 int it = 0;
                 if (lane == 0) it = atomicAdd(&s_cnt, 1);
@@ -284,6 +311,19 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
             }
             const Seg Sn = k + 1 < nseg ? segs[k + 1] : S;
             __syncthreads();
+            int4 tdn = make_int4(0, 0, 0, 0);
+            if (k == nseg - 1) {
+                next = s_tile;
+                if (next < ntiles) {
+                    tdn = P.tiles[next];
+                    if (warp == NW - 1) {  // the next tile's geometry, ahead of this warp's share of the stores
+                        Geo<FT> gn;
+                        tile_geo(gn, P, tdn.y, tdn.z, lane);
+                        s_geo[lane] = gn;
+                        if (lane == 0) s_td = tdn;
+                    }
+                }
+            }
             if (S.pn >= kSegPanelEnd) {  // the panel is complete: stream the slab out
                 const int pn = S.pn - kSegPanelEnd;
                 const int col0 = P.panels.col0[pn];
@@ -303,14 +343,23 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                     for (; e < len; e += 32) __stcs(o + e, s[e]);
                 }
             }
-            if (Sn.off != staged) {
-                stage_chunk<THREADS>(stage, P.pk + Sn.off, Sn.n16);
-                staged = Sn.off;
+            if (k + 1 < nseg) {
+                if (Sn.off != staged) {
+                    stage_chunk<THREADS>(stage, P.pk + Sn.off, Sn.n16);
+                    staged = Sn.off;
+                }
+            } else if (next < ntiles) {
+                const Seg S0 = P.segs[(size_t)tdn.x * P.seg_stride];
+                if (S0.off != staged) {
+                    stage_chunk<THREADS>(stage, P.pk + S0.off, S0.n16);
+                    staged = S0.off;
+                }
             }
             if (threadIdx.x == 0) s_cnt = 0;
             __syncthreads();
             S = Sn;
         }
+        tile = next;
     }
 }
 

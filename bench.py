@@ -190,7 +190,7 @@ def main():
                     help="only the FP32C forward steps (for ncu launch lists / captures); prints no JSON")
     ap.add_argument("--batch", type=int, default=B_PER_RANK, help="pairs per rank")
     ap.add_argument("--workload", default="overlap2c",
-                    choices=["overlap2c", "evaluate", "overlap3c", "pullback", "grad"],
+                    choices=["overlap2c", "evaluate", "overlap3c", "pullback", "grad", "outputbound"],
                     help="with --profile: which kernel family to run (ncu captures)")
     ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
     args = ap.parse_args()
@@ -274,7 +274,7 @@ def main():
         return allmax(ms), allmax(kms)
 
     if args.profile and args.workload not in ("overlap2c", "grad"):
-        fn = side_workload(args.workload, L, _dev, _lib, aok, torch)
+        fn = side_workload(args.workload, L, _dev, _lib, aok, torch, args.batch)
         for _ in range(args.warmup + args.steps):
             fn()
         torch.cuda.synchronize()
@@ -526,8 +526,31 @@ def _overlap3c_setup(aok, _dev, _lib, torch, L, B, FT):
     return d
 
 
-def side_workload(name, L, _dev, _lib, aok, torch):
+def _outputbound_setup(aok, _dev, _lib, torch, L, B, FT):
+    """The output-bound 2C case: config-2 shell structure, one primitive per shell."""
+    ob = aok.workloads.outputbound_basis()
+    obp = aok.workloads.ragged_pairs(B, ob.NZ, SEED + 1)
+    Nob = ob.nbf_total
+    pl = _dev.Plan(ob.ls, ob.K, ob.NZ, _dev.prec_of(FT), obp.B)
+    zt, Dt = _dev.to_colmajor(ob.zeta, FT), _dev.to_colmajor(ob.D, FT)
+    cf = _dev.colmajor_empty((ob.nshells, ob.K, ob.NZ), FT)
+    _lib.check(L.aok_compile_coef(pl.h, _dev.ptr(cf), _dev.ptr(zt), _dev.ptr(Dt), _dev.stream()))
+    _lib.check(L.aok_plan_set_basis(pl.h, _dev.ptr(zt), _dev.ptr(cf), _dev.stream()))
+    pa, pb = _dev.to_colmajor(obp.posA, FT), _dev.to_colmajor(obp.posB, FT)
+    sa, sb = torch.as_tensor(obp.sidxA).cuda(), torch.as_tensor(obp.sidxB).cuda()
+    o = _dev.colmajor_empty((Nob, Nob, obp.B), FT)
+    fn = lambda: _lib.check(L.aok_overlap2c(pl.h, _dev.ptr(o), None, None, _dev.ptr(pa), _dev.ptr(pb),
+                                            ctypes.c_void_p(sa.data_ptr()), ctypes.c_void_p(sb.data_ptr()),
+                                            obp.B, 1.0, _dev.stream()))
+    return dict(plan=pl, fn=fn, N=Nob, B=obp.B, keep=(zt, cf, pa, pb, sa, sb, o))
+
+
+def side_workload(name, L, _dev, _lib, aok, torch, B=None):
     """One launch chain of a side workload, for ncu captures (--profile --workload ...)."""
+    if name == "outputbound":
+        d = _outputbound_setup(aok, _dev, _lib, torch, L, B or B_PER_RANK, torch.float32)
+        side_workload.keep = d
+        return d["fn"]
     if name in ("evaluate", "pullback"):
         d = _evaluate_setup(aok, _dev, _lib, torch, L, 1 << 20 if name == "evaluate" else 1 << 18, torch.float32,
                             with_pb=(name == "pullback"))
@@ -567,22 +590,10 @@ def side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks):
     out = {}
     n = max(5, min(200, args.steps // 10))
     # output-bound 2C: the config-2 shell structure with one primitive per shell
-    ob = aok.workloads.outputbound_basis()
-    obp = aok.workloads.ragged_pairs(B_PER_RANK, ob.NZ, SEED + 1)
-    Nob = ob.nbf_total
     res = {}
     for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
-        pl = _dev.Plan(ob.ls, ob.K, ob.NZ, _dev.prec_of(FT), obp.B)
-        zt, Dt = _dev.to_colmajor(ob.zeta, FT), _dev.to_colmajor(ob.D, FT)
-        cf = _dev.colmajor_empty((ob.nshells, ob.K, ob.NZ), FT)
-        _lib.check(L.aok_compile_coef(pl.h, _dev.ptr(cf), _dev.ptr(zt), _dev.ptr(Dt), _dev.stream()))
-        _lib.check(L.aok_plan_set_basis(pl.h, _dev.ptr(zt), _dev.ptr(cf), _dev.stream()))
-        pa, pb = _dev.to_colmajor(obp.posA, FT), _dev.to_colmajor(obp.posB, FT)
-        sa, sb = torch.as_tensor(obp.sidxA).cuda(), torch.as_tensor(obp.sidxB).cuda()
-        o = _dev.colmajor_empty((Nob, Nob, obp.B), FT)
-        fn = lambda: _lib.check(L.aok_overlap2c(pl.h, _dev.ptr(o), None, None, _dev.ptr(pa), _dev.ptr(pb),
-                                                ctypes.c_void_p(sa.data_ptr()), ctypes.c_void_p(sb.data_ptr()),
-                                                obp.B, 1.0, _dev.stream()))
+        d = _outputbound_setup(aok, _dev, _lib, torch, L, B_PER_RANK, FT)
+        pl, fn, Nob, obB = d["plan"], d["fn"], d["N"], d["B"]
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
@@ -592,10 +603,10 @@ def side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks):
         _lib.check(L.aok_plan_timing_read(pl.h, ctypes.byref(tot), ctypes.byref(cnt)))
         kms = tot.value / max(cnt.value, 1)
         fsz = 4 if FT == torch.float32 else 8
-        alg = obp.B * (Nob * Nob * fsz + 2 * (3 * fsz + 8))
-        res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obp.B / (ms * 1e-3),
+        alg = obB * (Nob * Nob * fsz + 2 * (3 * fsz + 8))
+        res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obB / (ms * 1e-3),
                     "kernel_hbm_gbs": alg / (kms * 1e-3) / 1e9, "kernel_hbm_frac": alg / (kms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
-        del pl
+        del pl, d
     out["outputbound_2c_K1_B65536"] = dict(res, nbf=Nob, note="config-2 shell structure, one primitive per shell")
     # config 1
     res = {}
