@@ -235,11 +235,13 @@ __device__ __forceinline__ void stage_chunk(float4* dst, const float4* __restric
     for (; i < n16; i += THREADS) dst[i] = __ldg(src + i);
 }
 
-// Geometry of the tile's 32 lanes (zero geometry for lanes past the tile's end).
+// Geometry of the tile's 32 lanes (zero geometry for lanes past the tile's end)
+// and each lane's batch element (b).
 template <typename FT>
-__device__ __forceinline__ void tile_geo(Geo<FT>& g, const Ov2Params<FT>& P, int start, int cnt, int lane) {
+__device__ __forceinline__ void tile_geo(Geo<FT>& g, int& b, const Ov2Params<FT>& P, int start, int cnt, int lane) {
+    b = 0;
     if (lane < cnt) {
-        const int b = P.perm[start + lane];
+        b = P.perm[start + lane];
         load_geo(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
     } else {
         const FT z[3] = {FT(0), FT(0), FT(0)};
@@ -266,6 +268,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
     __shared__ int s_tile, s_cnt;
     __shared__ int4 s_td;
     __shared__ Geo<FT> s_geo[32];
+    __shared__ int s_b[2][32];  // batch element of each lane, double-buffered across tiles
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = THREADS / 32;
     const int ntiles = *P.ntiles;
@@ -281,8 +284,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
         const int4 td = P.tiles[tile];
         if (warp == NW - 1) {
             Geo<FT> g;
-            tile_geo(g, P, td.y, td.z, lane);
+            int b;
+            tile_geo(g, b, P, td.y, td.z, lane);
             s_geo[lane] = g;
+            s_b[0][lane] = b;
             if (lane == 0) s_td = td;
         }
         const Seg S0 = P.segs[(size_t)td.x * P.seg_stride];
@@ -290,9 +295,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
         staged = S0.off;
     }
     __syncthreads();
+    int buf = 0;  // s_b buffer of the current tile
     while (tile < ntiles) {
         const int4 td = s_td;
-        const int pair = td.x, start = td.y, cnt = td.z;
+        const int pair = td.x, cnt = td.z;
         const Geo<FT> g = s_geo[lane];
         const Seg* segs = P.segs + (size_t)pair * P.seg_stride;
         const int nseg = P.nseg[pair];
@@ -318,8 +324,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                     tdn = P.tiles[next];
                     if (warp == NW - 1) {  // the next tile's geometry, ahead of this warp's share of the stores
                         Geo<FT> gn;
-                        tile_geo(gn, P, tdn.y, tdn.z, lane);
+                        int bn;
+                        tile_geo(gn, bn, P, tdn.y, tdn.z, lane);
                         s_geo[lane] = gn;
+                        s_b[buf ^ 1][lane] = bn;
                         if (lane == 0) s_td = tdn;
                     }
                 }
@@ -329,7 +337,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
                 const int col0 = P.panels.col0[pn];
                 const int len = (P.panels.col0[pn + 1] - col0) * P.N;
                 for (int bl = warp; bl < cnt; bl += NW) {
-                    const int bg = P.perm[start + bl];
+                    const int bg = s_b[buf][bl];
                     FT* o = P.out + (size_t)bg * P.N * P.N + (size_t)col0 * P.N;
                     const FT* s = slab + (size_t)bl * P.slab_stride;
                     int e = lane;
@@ -360,6 +368,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
             S = Sn;
         }
         tile = next;
+        buf ^= 1;
     }
 }
 
