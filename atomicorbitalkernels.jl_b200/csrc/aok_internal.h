@@ -38,6 +38,7 @@ struct aok_plan {
     int* d_nseg = nullptr;           // segments per species pair
     int pair16 = 0, seg_stride = 0;
     size_t stage_bytes = 0;          // shared-memory stage of the forward kernel
+    int fwd_ctas = 2;                // forward kernel CTAs per SM
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
     int max_bin_blocks = 0;

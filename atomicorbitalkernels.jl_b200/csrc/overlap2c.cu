@@ -504,11 +504,15 @@ int setup_overlap2c_schedule(aok_plan* p) {
     const size_t stage = std::max(one_item, std::min((size_t)(f64 ? 48 : 24) * 1024, pair16 * 16));
     if (stage > (size_t)200 * 1024)
         return set_error(AOK_ERR_UNSUPPORTED, "too many primitives per shell for the 2C stage");
-    // FP32: two CTAs per SM; FP64: one.  The slab shares the CTA's shared memory
+    // FP32: two CTAs per SM, three for bases of <= 2 primitives per shell;
+    // FP64: one, two for such bases.  The slab shares the CTA's shared memory
     // with the stage; a basis whose widest shell column would not fit falls back
     // to one CTA per SM.
-    size_t budget = f64 ? std::min((size_t)120 * 1024, (size_t)224 * 1024 - stage)
-                        : (size_t)112 * 1024 - std::min(stage, (size_t)112 * 1024);
+    const bool few = p->K <= 2;
+    p->fwd_ctas = f64 ? (few ? 2 : 1) : (few ? 3 : 2);
+    const size_t cap = p->fwd_ctas == 3 ? (size_t)72 * 1024 : p->fwd_ctas == 2 ? (size_t)112 * 1024 : (size_t)224 * 1024;
+    size_t budget = p->fwd_ctas == 1 ? std::min((size_t)120 * 1024, (size_t)224 * 1024 - stage)
+                                     : cap - std::min(stage, cap);
     {
         size_t widest = 0;
         for (int s = 0; s < ns; ++s) widest = std::max(widest, (size_t)ncart((int)p->ls[s]));

@@ -11,11 +11,12 @@
 
 namespace aok {
 
-constexpr int kThreadsF32 = 256;   // 2 CTAs per SM (registers <= 128)
-constexpr int kThreadsF64 = 256;   // 1 CTA per SM
-template <typename FT> constexpr int min_blocks();
-template <> constexpr int min_blocks<float>() { return 2; }
-template <> constexpr int min_blocks<double>() { return 1; }
+// 256 threads per CTA; CTAs per SM (the plan's fwd_ctas): FP32 2 (registers
+// <= 128), or 3 for bases of <= 2 primitives per shell (<= 80 registers: the
+// few f-f items spill a little, the many cheap items gain latency hiding);
+// FP64 1, or 2 for such bases.
+constexpr int kThreadsF32 = 256;
+constexpr int kThreadsF64 = 256;
 
 // --------------------------------------------------------------------------
 // Geometry per lane.
@@ -372,7 +373,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
     }
 }
 
-template <typename FT, int THREADS>
+template <typename FT, int THREADS, int MINB>
 inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale,
                       cudaStream_t s) {
     Ov2Params<FT> P;
@@ -396,11 +397,11 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     const size_t slab = (p->smem_bytes + 15) / 16 * 16;
     P.stage_offset = (unsigned)slab;
     const size_t smem = slab + p->stage_bytes;
-    auto kern = k_overlap2c<FT, THREADS, min_blocks<FT>()>;
+    auto kern = k_overlap2c<FT, THREADS, MINB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap2c)");
     timing_begin(p, s);
-    kern<<<p->num_sms * min_blocks<FT>(), THREADS, smem, s>>>(P);
+    kern<<<p->num_sms * MINB, THREADS, smem, s>>>(P);
     timing_end(p, s);
     return cuda_status(cudaGetLastError(), "k_overlap2c");
 }
