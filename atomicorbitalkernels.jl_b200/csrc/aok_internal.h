@@ -65,6 +65,18 @@ struct aok_plan {
     alignas(8) unsigned char panels3_raw[160] = {};
     size_t slab_stride3 = 0;
     size_t smem3 = 0;
+    // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated
+    // launch chain, the arguments it was captured with, a private capture stream
+    bool graph_on = false;
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t cap = nullptr;
+    struct GraphKey {
+        void* out;
+        const void *posA, *posB;
+        const int64_t *sidxA, *sidxB;
+        int64_t B;
+        double lengthscale;
+    } gkey{};
     // side stream for the record preparation (forked/joined with events)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;

@@ -145,6 +145,8 @@ int aok_plan_destroy(aok_plan* p) {
                     p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3,
                     p->d_pk,        p->d_segs,      p->d_nseg};
     for (void* b : bufs) dfree(b);
+    if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    if (p->cap) cudaStreamDestroy(p->cap);
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);
     if (p->ev_join) cudaEventDestroy(p->ev_join);
@@ -206,6 +208,47 @@ static int check_batch(aok_plan* p, int64_t B, const char* who) {
     return AOK_OK;
 }
 
+// The fixed-basis forward from the plan's CUDA graph: captured on the plan's
+// capture stream (thread-local mode), instantiated once, updated in place when
+// the arguments change (re-instantiated if the update is refused), launched on
+// the caller's stream.
+static int overlap2c_graph(aok_plan* p, void* out, const void* posA, const void* posB, const int64_t* sidxA,
+                           const int64_t* sidxB, int64_t B, double lengthscale, cudaStream_t s) {
+    const aok_plan::GraphKey k{out, posA, posB, sidxA, sidxB, B, lengthscale};
+    const aok_plan::GraphKey& o = p->gkey;
+    const bool same = p->gexec && o.out == k.out && o.posA == k.posA && o.posB == k.posB && o.sidxA == k.sidxA &&
+                      o.sidxB == k.sidxB && o.B == k.B && o.lengthscale == k.lengthscale;
+    if (!same) {
+        if (!p->cap) AOK_TRY(cuda_status(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking), "cudaStreamCreate"));
+        AOK_TRY(cuda_status(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
+        int st = launch_bin(p, sidxA, sidxB, B, p->cap);
+        if (st == AOK_OK) st = launch_overlap2c(p, out, posA, posB, B, lengthscale, p->cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(p->cap, &g);
+        if (st != AOK_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return st != AOK_OK ? st : cuda_status(e, "cudaStreamEndCapture");
+        }
+        if (p->gexec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(p->gexec, g, &info) != cudaSuccess) {
+                (void)cudaGetLastError();
+                cudaGraphExecDestroy(p->gexec);
+                p->gexec = nullptr;
+            }
+        }
+        cudaError_t ei = cudaSuccess;
+        if (!p->gexec) ei = cudaGraphInstantiate(&p->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            p->gexec = nullptr;
+            return cuda_status(ei, "cudaGraphInstantiate");
+        }
+        p->gkey = k;
+    }
+    return cuda_status(cudaGraphLaunch(p->gexec, s), "cudaGraphLaunch");
+}
+
 int aok_overlap2c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
                   const int64_t* sidxA, const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
     if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c: null plan");
@@ -225,9 +268,16 @@ int aok_overlap2c(aok_plan* p, void* out, const void* zeta, const void* coef, co
         AOK_TRY(cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent"));
     } else {
         if (!p->basis_set) return set_error(AOK_ERR_INVALID, "aok_overlap2c: no zeta/coef and no aok_plan_set_basis");
+        if (p->graph_on && p->ev.empty()) return overlap2c_graph(p, out, posA, posB, sidxA, sidxB, B, lengthscale, s);
         AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
     }
     return launch_overlap2c(p, out, posA, posB, B, lengthscale, s);
+}
+
+int aok_plan_set_graph(aok_plan* p, int enable) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_plan_set_graph: null plan");
+    p->graph_on = enable != 0;
+    return AOK_OK;
 }
 
 int aok_plan_set_basis(aok_plan* p, const void* zeta, const void* coef, void* stream) {

@@ -94,6 +94,16 @@ int aok_compile_coef(aok_plan* plan, void* coef, const void* zeta, const void* D
  * compiled CartesianGTOBasis.  Calling it again replaces the parameters.
  */
 int aok_plan_set_basis(aok_plan* plan, const void* zeta, const void* coef, void* stream);
+/*
+ * Graph mode for a fixed basis (no reference counterpart; the launch form of
+ * batch_overlap! on a compiled basis).  enable != 0: aok_overlap2c calls with
+ * zeta = coef = NULL replay their launch chain (species-pair binning + the
+ * overlap kernel) from one instantiated CUDA graph per plan, captured on the
+ * first call and re-captured (graph update) when out, the positions, the
+ * species indices, B or lengthscale change.  While timing is enabled
+ * (aok_plan_timing_enable) calls launch directly.  Default: disabled.
+ */
+int aok_plan_set_graph(aok_plan* plan, int enable);
 
 /*
  * Batched 2-center overlap, species-aware Cartesian basis.
