@@ -149,7 +149,8 @@ int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB,
                      double lengthscale, cudaStream_t s);
 int launch_gb_pad(aok_plan* p, const int64_t* nprim, const int64_t* prim_offset, const void* coef,
                   const void* alpha, cudaStream_t s);
-int setup_overlap2c_schedule(aok_plan* p);
+// ctas = 0, stage_req = 0: the defaults (see overlap2c.cu).
+int setup_overlap2c_schedule(aok_plan* p, int ctas = 0, size_t stage_req = 0);
 int launch_ov2_f32(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
 int launch_ov2_f64(aok_plan* p, void* out, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
 

@@ -5,6 +5,10 @@
 #include <cstring>
 #include <string>
 
+#include <map>
+#include <mutex>
+#include <string>
+
 #include "aok_internal.h"
 
 namespace aok {
@@ -272,6 +276,114 @@ int aok_overlap2c(aok_plan* p, void* out, const void* zeta, const void* coef, co
         AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
     }
     return launch_overlap2c(p, out, posA, posB, B, lengthscale, s);
+}
+
+// Shapes chosen by aok_plan_autotune, per (precision, shells, K, NZ, non-zero
+// coefficient pattern, B).
+namespace {
+struct TuneChoice {
+    int ctas;
+    size_t stage;
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> g_tune_cache;
+}  // namespace
+
+int aok_plan_autotune(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
+                      const void* posB, const int64_t* sidxA, const int64_t* sidxB, int64_t B, double lengthscale,
+                      void* stream, int64_t* choice) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_plan_autotune: null plan");
+    AOK_TRY(check_batch(p, B, "aok_plan_autotune"));
+    if (!out || !zeta || !coef || !posA || !posB || !sidxA || !sidxB || B == 0)
+        return set_error(AOK_ERR_INVALID, "aok_plan_autotune: null pointer or empty batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool f64 = p->prec == AOK_PREC_F64;
+    // key: precision, shells, K, NZ, non-zero coefficient pattern, B
+    const size_t nc = (size_t)(p->ns * p->K * p->NZ);
+    std::vector<unsigned char> c(nc * (f64 ? 8 : 4));
+    AOK_TRY(cuda_status(cudaMemcpyAsync(c.data(), coef, c.size(), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync"));
+    AOK_TRY(cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize"));
+    std::string key = std::to_string(p->prec) + "|" + std::to_string(p->K) + "|" + std::to_string(p->NZ) + "|" +
+                      std::to_string(B) + "|";
+    for (int64_t l : p->ls) key += (char)('0' + l);
+    key += "|";
+    for (size_t i = 0; i < nc; ++i) {
+        const double v = f64 ? ((const double*)c.data())[i] : (double)((const float*)c.data())[i];
+        key += v != 0.0 ? '1' : '0';
+    }
+    auto apply = [&](int ctas, size_t stage) -> int {
+        AOK_TRY(setup_overlap2c_schedule(p, ctas, stage));
+        AOK_TRY(launch_prep2c(p, zeta, coef, s));
+        p->basis_set = true;
+        return AOK_OK;
+    };
+    auto forward = [&]() -> int {
+        AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+        return launch_overlap2c(p, out, posA, posB, B, lengthscale, s);
+    };
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            AOK_TRY(apply(it->second.ctas, it->second.stage));
+            AOK_TRY(forward());
+            if (choice) {
+                choice[0] = p->fwd_ctas;
+                choice[1] = (int64_t)p->stage_bytes;
+                choice[2] = 1;
+            }
+            return cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+        }
+    }
+    std::vector<int> ctas = f64 ? std::vector<int>{1, 2} : std::vector<int>{2, 3};
+    std::vector<size_t> stages = f64 ? std::vector<size_t>{48 * 1024, 80 * 1024}
+                                     : std::vector<size_t>{24 * 1024, 40 * 1024};
+    std::vector<cudaEvent_t> ev0(p->ev);
+    p->ev.clear();  // direct launches, no measurement events of the plan
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int st = cuda_status(cudaEventCreate(&e0), "cudaEventCreate");
+    if (st == AOK_OK) st = cuda_status(cudaEventCreate(&e1), "cudaEventCreate");
+    float best = -1.f;
+    TuneChoice bestc{0, 0};
+    for (int ct : ctas)
+        for (size_t sb : stages) {
+            if (st != AOK_OK) break;
+            if (apply(ct, sb) != AOK_OK) continue;  // shape does not fit this basis
+            if (forward() != AOK_OK) continue;
+            constexpr int kReps = 5;
+            st = cuda_status(cudaEventRecord(e0, s), "cudaEventRecord");
+            for (int r = 0; r < kReps && st == AOK_OK; ++r) st = forward();
+            if (st == AOK_OK) st = cuda_status(cudaEventRecord(e1, s), "cudaEventRecord");
+            if (st == AOK_OK) st = cuda_status(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            if (st == AOK_OK) st = cuda_status(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (st == AOK_OK && (best < 0.f || ms < best)) {
+                best = ms;
+                bestc = TuneChoice{p->fwd_ctas, p->stage_bytes};
+            }
+        }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    p->ev = ev0;
+    if (st != AOK_OK || best < 0.f) {  // leave the plan with its default shape
+        const int st2 = setup_overlap2c_schedule(p);
+        p->basis_set = false;
+        if (st != AOK_OK) return st;
+        if (st2 != AOK_OK) return st2;
+        return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_autotune: no launch shape fits this basis");
+    }
+    AOK_TRY(apply(bestc.ctas, bestc.stage));
+    AOK_TRY(forward());
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = bestc;
+    }
+    if (choice) {
+        choice[0] = p->fwd_ctas;
+        choice[1] = (int64_t)p->stage_bytes;
+        choice[2] = 0;
+    }
+    return cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize");
 }
 
 int aok_plan_set_graph(aok_plan* p, int enable) {

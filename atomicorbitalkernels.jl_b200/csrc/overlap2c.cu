@@ -486,10 +486,25 @@ __global__ void k_bin_identity(int B, int np, int* __restrict__ perm, int4* __re
 
 static size_t npairs_of(const aok_plan* p) { return (size_t)(p->NZ * p->NZ); }
 
-int setup_overlap2c_schedule(aok_plan* p) {
+static void free_schedule(aok_plan* p) {
+    void** bufs[] = {(void**)&p->d_pk, (void**)&p->d_segs, (void**)&p->d_nseg, (void**)&p->d_items,
+                     (void**)&p->d_blockhist};
+    for (void** b : bufs)
+        if (*b) {
+            cudaFree(*b);
+            *b = nullptr;
+        }
+    if (p->gexec) {  // kernel parameters of the captured chain change with the schedule
+        cudaGraphExecDestroy(p->gexec);
+        p->gexec = nullptr;
+    }
+}
+
+int setup_overlap2c_schedule(aok_plan* p, int ctas, size_t stage_req) {
     const int ns = (int)p->ns, N = (int)p->N;
     const bool f64 = p->prec == AOK_PREC_F64;
     const size_t fsz = f64 ? sizeof(double) : sizeof(float);
+    free_schedule(p);
     // Stage images (k_pack2c): a species pair's records fill at most pair16
     // 16-byte words (every primitive pair present, plus item headers and
     // padding); the stage holds one chunk and at least the largest item.
@@ -501,7 +516,8 @@ int setup_overlap2c_schedule(aok_plan* p) {
             pair16 += K2 * (size_t)(f64 ? rec_words16_f64(la, lb) : rec_words16_f32(la, lb));
         }
     const size_t one_item = 16 + K2 * (f64 ? kRecMaxBytesF64 : kRecMaxBytesF32);
-    const size_t stage = std::max(one_item, std::min((size_t)(f64 ? 48 : 24) * 1024, pair16 * 16));
+    const size_t stage_pref = stage_req ? stage_req : (size_t)(f64 ? 48 : 24) * 1024;
+    const size_t stage = (std::max(one_item, std::min(stage_pref, pair16 * 16)) + 15) / 16 * 16;
     if (stage > (size_t)200 * 1024)
         return set_error(AOK_ERR_UNSUPPORTED, "too many primitives per shell for the 2C stage");
     // FP32: two CTAs per SM, three for bases of <= 2 primitives per shell;
@@ -509,7 +525,9 @@ int setup_overlap2c_schedule(aok_plan* p) {
     // with the stage; a basis whose widest shell column would not fit falls back
     // to one CTA per SM.
     const bool few = p->K <= 2;
-    p->fwd_ctas = f64 ? (few ? 2 : 1) : (few ? 3 : 2);
+    p->fwd_ctas = ctas ? ctas : f64 ? (few ? 2 : 1) : (few ? 3 : 2);
+    if (f64 ? (p->fwd_ctas < 1 || p->fwd_ctas > 2) : (p->fwd_ctas < 2 || p->fwd_ctas > 3))
+        return set_error(AOK_ERR_INVALID, "2C forward: unsupported CTAs per SM");
     const size_t cap = p->fwd_ctas == 3 ? (size_t)72 * 1024 : p->fwd_ctas == 2 ? (size_t)112 * 1024 : (size_t)224 * 1024;
     size_t budget = p->fwd_ctas == 1 ? std::min((size_t)120 * 1024, (size_t)224 * 1024 - stage)
                                      : cap - std::min(stage, cap);

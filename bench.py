@@ -240,10 +240,15 @@ def main():
         sA = torch.as_tensor(pairs.sidxA).cuda()
         sB = torch.as_tensor(pairs.sidxB).cuda()
         out = _dev.colmajor_empty((N, N, B), FT)
-        # compile_basis equivalent: the geometry-free records are fixed once
-        _lib.check(L.aok_plan_set_basis(plan.h, _dev.ptr(zeta), _dev.ptr(coef), _dev.stream()))
+        # compile_basis equivalent: the geometry-free records are fixed once, under the
+        # launch shape the autotuner picks for this (basis, B)
+        ch = (ctypes.c_int64 * 3)()
+        _lib.check(L.aok_plan_autotune(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(pA),
+                                       _dev.ptr(pB), ctypes.c_void_p(sA.data_ptr()), ctypes.c_void_p(sB.data_ptr()),
+                                       B, 1.0, _dev.stream(), ch))
         _lib.check(L.aok_plan_set_graph(plan.h, 1))  # one captured launch chain per compiled basis
-        return dict(plan=plan, zeta=zeta, D=D, coef=coef, pA=pA, pB=pB, sA=sA, sB=sB, out=out, FT=FT)
+        return dict(plan=plan, zeta=zeta, D=D, coef=coef, pA=pA, pB=pB, sA=sA, sB=sB, out=out, FT=FT,
+                    shape={"ctas_per_sm": int(ch[0]), "stage_bytes": int(ch[1])})
 
     def step(c, with_params=False):
         z = _dev.ptr(c["zeta"]) if with_params else None
@@ -429,10 +434,12 @@ def main():
             "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
             "config": {"workload": "ragged 4-species l<=3 2C overlap (config 2), FP32-compensated forward; "
                                    "step = species binning + overlap kernel on a compiled basis "
-                                   "(aok_plan_set_basis once, like compile_basis)",
+                                   "(records fixed once, like compile_basis, under the autotuned launch "
+                                   "shape; replayed from the plan's CUDA graph)",
                        "batch_per_rank": B, "global_batch": B * world, "nbf": N, "nshells": ns, "K": K,
-                       "species": NZ, "l2": "output 321 MB per step > 126 MB L2 (no flush needed)"},
-            "fp64": {"value": value64, "ms_per_step": ms64, "kernel_ms": kms64},
+                       "species": NZ, "l2": "output 321 MB per step > 126 MB L2 (no flush needed)",
+                       "launch_shape": c32["shape"]},
+            "fp64": {"value": value64, "ms_per_step": ms64, "kernel_ms": kms64, "launch_shape": c64["shape"]},
             "ms_per_step_params_per_call": ms32p,
             "f32c_over_f64": value / value64,
             "rel_err": {"f32c_vs_oracle": err32, "f64_vs_oracle": err64, "sample_pairs": nchk},
@@ -541,14 +548,18 @@ def _outputbound_setup(aok, _dev, _lib, torch, L, B, FT):
     zt, Dt = _dev.to_colmajor(ob.zeta, FT), _dev.to_colmajor(ob.D, FT)
     cf = _dev.colmajor_empty((ob.nshells, ob.K, ob.NZ), FT)
     _lib.check(L.aok_compile_coef(pl.h, _dev.ptr(cf), _dev.ptr(zt), _dev.ptr(Dt), _dev.stream()))
-    _lib.check(L.aok_plan_set_basis(pl.h, _dev.ptr(zt), _dev.ptr(cf), _dev.stream()))
     pa, pb = _dev.to_colmajor(obp.posA, FT), _dev.to_colmajor(obp.posB, FT)
     sa, sb = torch.as_tensor(obp.sidxA).cuda(), torch.as_tensor(obp.sidxB).cuda()
     o = _dev.colmajor_empty((Nob, Nob, obp.B), FT)
+    ch = (ctypes.c_int64 * 3)()
+    _lib.check(L.aok_plan_autotune(pl.h, _dev.ptr(o), _dev.ptr(zt), _dev.ptr(cf), _dev.ptr(pa), _dev.ptr(pb),
+                                   ctypes.c_void_p(sa.data_ptr()), ctypes.c_void_p(sb.data_ptr()), obp.B, 1.0,
+                                   _dev.stream(), ch))
     fn = lambda: _lib.check(L.aok_overlap2c(pl.h, _dev.ptr(o), None, None, _dev.ptr(pa), _dev.ptr(pb),
                                             ctypes.c_void_p(sa.data_ptr()), ctypes.c_void_p(sb.data_ptr()),
                                             obp.B, 1.0, _dev.stream()))
-    return dict(plan=pl, fn=fn, N=Nob, B=obp.B, keep=(zt, cf, pa, pb, sa, sb, o))
+    return dict(plan=pl, fn=fn, N=Nob, B=obp.B, keep=(zt, cf, pa, pb, sa, sb, o),
+                shape={"ctas_per_sm": int(ch[0]), "stage_bytes": int(ch[1])})
 
 
 def side_workload(name, L, _dev, _lib, aok, torch, B=None):
@@ -610,7 +621,7 @@ def side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks):
         kms = tot.value / max(cnt.value, 1)
         fsz = 4 if FT == torch.float32 else 8
         alg = obB * (Nob * Nob * fsz + 2 * (3 * fsz + 8))
-        res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obB / (ms * 1e-3),
+        res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obB / (ms * 1e-3), "shape": d["shape"],
                     "kernel_hbm_gbs": alg / (kms * 1e-3) / 1e9, "kernel_hbm_frac": alg / (kms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
         del pl, d
     out["outputbound_2c_K1_B65536"] = dict(res, nbf=Nob, note="config-2 shell structure, one primitive per shell")

@@ -104,6 +104,21 @@ int aok_plan_set_basis(aok_plan* plan, const void* zeta, const void* coef, void*
  * (aok_plan_timing_enable) calls launch directly.  Default: disabled.
  */
 int aok_plan_set_graph(aok_plan* plan, int enable);
+/*
+ * Autotuner of the 2C forward's launch shape (no reference counterpart).  Times
+ * aok_overlap2c on these inputs under each candidate shape (CTAs per SM; size
+ * of the shared-memory record stage, which trades against the output slab),
+ * keeps the fastest in the plan, and caches it process-wide under (precision,
+ * shell structure, K, NZ, pattern of non-zero coefficients, B): a later call
+ * with the same key applies the cached shape without timing.  Leaves the basis
+ * fixed as aok_plan_set_basis(zeta, coef) does and out holding the forward.
+ * Synchronises `stream`.  choice (may be NULL) receives {CTAs per SM, stage
+ * bytes, 1 if taken from the cache else 0}.
+ */
+int aok_plan_autotune(aok_plan* plan, void* out, const void* zeta, const void* coef,
+                      const void* posA, const void* posB, const int64_t* sidxA,
+                      const int64_t* sidxB, int64_t B, double lengthscale, void* stream,
+                      int64_t* choice);
 
 /*
  * Batched 2-center overlap, species-aware Cartesian basis.

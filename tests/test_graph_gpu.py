@@ -82,3 +82,42 @@ def test_graph_replay_matches_direct(FT):
     _lib.check(L.aok_plan_timing_read(plan.h, ctypes.byref(tot), ctypes.byref(n)))
     assert n.value == 1 and torch.equal(o1, o2)
     _lib.check(L.aok_plan_check(plan.h, _dev.stream()))
+
+
+@pytest.mark.parametrize("FT", [torch.float32, torch.float64])
+def test_autotune_keeps_results_and_caches(FT):
+    """aok_plan_autotune: every candidate shape computes the same blocks (the schedule
+    only reorders work), the chosen shape is reported, and a second plan with the same
+    key takes it from the process-wide cache."""
+    L = _lib.load()
+    b = W.config2_basis()
+    pr = W.ragged_pairs(2500, b.NZ, 91)
+    N, B = b.nbf_total, pr.B
+    zeta = _dev.to_colmajor(b.zeta, FT)
+    D = _dev.to_colmajor(b.D, FT)
+    c = dict(pA=_dev.to_colmajor(pr.posA, FT), pB=_dev.to_colmajor(pr.posB, FT),
+             sA=torch.as_tensor(pr.sidxA).cuda(), sB=torch.as_tensor(pr.sidxB).cuda())
+    outs, choices = [], []
+    for _ in range(2):
+        plan = _dev.Plan(b.ls, b.K, b.NZ, _dev.prec_of(FT), B)
+        coef = _dev.colmajor_empty(b.zeta.shape, FT)
+        _lib.check(L.aok_compile_coef(plan.h, _dev.ptr(coef), _dev.ptr(zeta), _dev.ptr(D), _dev.stream()))
+        ref = _dev.colmajor_empty((N, N, B), FT)
+        _lib.check(L.aok_overlap2c(plan.h, _dev.ptr(ref), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(c["pA"]),
+                                   _dev.ptr(c["pB"]), ctypes.c_void_p(c["sA"].data_ptr()),
+                                   ctypes.c_void_p(c["sB"].data_ptr()), B, 1.0, _dev.stream()))
+        out = _dev.colmajor_empty((N, N, B), FT)
+        ch = (ctypes.c_int64 * 3)()
+        _lib.check(L.aok_plan_autotune(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(c["pA"]),
+                                       _dev.ptr(c["pB"]), ctypes.c_void_p(c["sA"].data_ptr()),
+                                       ctypes.c_void_p(c["sB"].data_ptr()), B, 1.0, _dev.stream(), ch))
+        assert torch.equal(out, ref)
+        out2 = _dev.colmajor_empty((N, N, B), FT)
+        _forward(L, plan, out2, c, B)  # the basis stays fixed in the tuned plan
+        torch.cuda.synchronize()
+        assert torch.equal(out2, ref)
+        outs.append(ref)
+        choices.append(tuple(ch))
+    ctas, stage, cached = choices[0]
+    assert ctas in ((1, 2) if FT == torch.float64 else (2, 3)) and stage > 0
+    assert choices[1][:2] == choices[0][:2] and choices[1][2] == 1
