@@ -59,6 +59,8 @@ int ensure_pb_buffers(aok_plan* p) {
     // unit partials: chunks (each species pair rounds up) x items x record groups x 4 x K
     const size_t nch = (size_t)(p->max_tiles + kPbChunkTiles - 1) / kPbChunkTiles + (size_t)(p->NZ * p->NZ);
     const size_t gmax = (size_t)((p->K * p->K + 31) / 32);
+    if (nch * items.size() * gmax >= ((size_t)1 << 31))
+        return set_error(AOK_ERR_UNSUPPORTED, "pullback: too many work units (batch x shell pairs)");
     if ((e = cudaMalloc(&p->d_partials, sizeof(double) * nch * items.size() * gmax * 4 * p->K)) != cudaSuccess)
         return cuda_status(e, "cudaMalloc(pb_partials)");
     if ((e = cudaMalloc(&p->d_pb_rows, sizeof(double) * (size_t)(p->NZ * p->NZ) * items.size() * 4 * p->K)) !=

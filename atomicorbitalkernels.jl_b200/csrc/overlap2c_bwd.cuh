@@ -268,9 +268,12 @@ struct PbParams {
 
 // Per-warp shared memory: the 32 elements' cotangent moments and R^2, and the
 // records' results for the slot sums.
+// FP32 rows of G are 16-byte aligned (read as float4 broadcasts); FP64 rows
+// keep an odd stride.
+template <typename FT> constexpr int pb_gstride() { return sizeof(FT) == 4 ? 12 : 9; }
 template <typename FT>
-struct PbWarpSmem {
-    FT G[32][9];    // used moment slots (<= 8) per element, odd stride
+struct __align__(16) PbWarpSmem {
+    FT G[32][pb_gstride<FT>()];  // used moment slots (<= 8) per element
     FT R2[32], R2lo[32];
     FT val[32][4];
     int slotA[32], slotB[32];
@@ -301,6 +304,9 @@ __device__ __noinline__ Sums4<FT> pb_unit(const PbParams<FT>& P, PbWarpSmem<FT>&
     FT S0[NM], S1[NM];
 #pragma unroll
     for (int m = 0; m < NM; ++m) S0[m] = S1[m] = FT(0);
+    float2 S01[NV];  // FP32: (S0, S1) of the used slots as pairs, one paired FMA per slot
+#pragma unroll
+    for (int j = 0; j < NV; ++j) S01[j] = make_float2(0.f, 0.f);
     for (int c0 = e0; c0 < e1; c0 += 32) {
         // phase A: lane = element; cotangent moments of its block
         {
@@ -331,21 +337,51 @@ __device__ __noinline__ Sums4<FT> pb_unit(const PbParams<FT>& P, PbWarpSmem<FT>&
         __syncwarp();
         // phase B: lane = record (copy `rep` of it takes elements rep, rep + reps, ...)
         const int ne = min(32, e1 - c0);
-        for (int t = rep; t < ne; t += reps) {
-            const FT x = R.ex(W.R2[t], W.R2lo[t]);
-            const FT xr = x * W.R2[t];
-            int j = 0;
+        if constexpr (sizeof(FT) == 4) {
+            for (int t = rep; t < ne; t += reps) {
+                const float x = R.ex(W.R2[t], W.R2lo[t]);
+                const float2 xx = make_float2(x, x * W.R2[t]);
+                float gv[4 * ((NV + 3) / 4)];
 #pragma unroll
-            for (int al = 0; al <= LA; ++al)
+                for (int w = 0; w < (NV + 3) / 4; ++w) {
+                    const float4 v = *reinterpret_cast<const float4*>(&W.G[t][4 * w]);
+                    gv[4 * w] = v.x;
+                    gv[4 * w + 1] = v.y;
+                    gv[4 * w + 2] = v.z;
+                    gv[4 * w + 3] = v.w;
+                }
 #pragma unroll
-                for (int be = 0; be <= LB; ++be)
-                    if (MdTab<LA, LB>::used(al, be)) {
-                        const FT Gm = W.G[t][j++];
-                        S0[al * (LB + 1) + be] = fma(x, Gm, S0[al * (LB + 1) + be]);
-                        S1[al * (LB + 1) + be] = fma(xr, Gm, S1[al * (LB + 1) + be]);
-                    }
+                for (int j = 0; j < NV; ++j) S01[j] = __ffma2_rn(xx, make_float2(gv[j], gv[j]), S01[j]);
+            }
+        } else {
+            for (int t = rep; t < ne; t += reps) {
+                const FT x = R.ex(W.R2[t], W.R2lo[t]);
+                const FT xr = x * W.R2[t];
+                int j = 0;
+#pragma unroll
+                for (int al = 0; al <= LA; ++al)
+#pragma unroll
+                    for (int be = 0; be <= LB; ++be)
+                        if (MdTab<LA, LB>::used(al, be)) {
+                            const FT Gm = W.G[t][j++];
+                            S0[al * (LB + 1) + be] = fma(x, Gm, S0[al * (LB + 1) + be]);
+                            S1[al * (LB + 1) + be] = fma(xr, Gm, S1[al * (LB + 1) + be]);
+                        }
+            }
         }
         __syncwarp();
+    }
+    if constexpr (sizeof(FT) == 4) {
+        int j = 0;
+#pragma unroll
+        for (int al = 0; al <= LA; ++al)
+#pragma unroll
+            for (int be = 0; be <= LB; ++be)
+                if (MdTab<LA, LB>::used(al, be)) {
+                    S0[al * (LB + 1) + be] = S01[j].x;
+                    S1[al * (LB + 1) + be] = S01[j].y;
+                    ++j;
+                }
     }
     (void)NV;
 #pragma unroll
@@ -441,15 +477,17 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c_pb(const __grid_con
     }
     __syncthreads();
     const int NCH = chpre[P.np];
-    const long long total = (long long)NCH * P.nitems * P.gmax;
+    // 32-bit unit numbers: the partial rows of all units fit in device memory,
+    // so there are far fewer than 2^32 of them
+    const unsigned total = (unsigned)NCH * (unsigned)P.nitems * (unsigned)P.gmax;
     for (;;) {
-        long long u = 0;
-        if (lane == 0) u = (long long)atomicAdd(P.counter, 1u);
+        unsigned u = 0;
+        if (lane == 0) u = atomicAdd(P.counter, 1u);
         u = __shfl_sync(0xffffffffu, u, 0);
         if (u >= total) break;
-        const int g = (int)(u % P.gmax);
-        const long long kj_i = u / P.gmax;
-        const int i = (int)(kj_i / NCH), kj = (int)(kj_i % NCH);
+        const int g = (int)(u % (unsigned)P.gmax);
+        const unsigned kj_i = u / (unsigned)P.gmax;
+        const int i = (int)(kj_i / (unsigned)NCH), kj = (int)(kj_i % (unsigned)NCH);
         int k = 0;
         while (chpre[k + 1] <= kj) ++k;
         const int j = kj - chpre[k];
