@@ -62,7 +62,7 @@ struct aok_plan {
     int* d_npp3 = nullptr;
     void* d_items3 = nullptr;
     int nitems3 = 0;
-    alignas(8) unsigned char panels3_raw[160] = {};
+    alignas(8) unsigned char panels3_raw[528] = {};
     size_t slab_stride3 = 0;
     size_t smem3 = 0;
     // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated

@@ -71,11 +71,11 @@ __global__ void k_prep3c(typename PTT<FT>::type* __restrict__ pp, int* __restric
 int setup_overlap3c_schedule(aok_plan* p) {
     if (p->d_items3) return AOK_OK;
     if (p->NZ != 1) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: plan must have NZ = 1");
-    if (p->Lmax > kMaxL3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: shells above l = 2");
+    if (p->Lmax > kMaxL3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: shells above l = 3");
     const int ns = (int)p->ns, N = (int)p->N;
     const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
     const size_t N2 = (size_t)N * N;
-    const size_t budget = 200 * 1024;
+    const size_t budget = 220 * 1024;
     auto stride_for = [&](int pages) {
         size_t s = N2 * pages;
         if (s % 2 == 0) s += 1;
@@ -103,7 +103,7 @@ int setup_overlap3c_schedule(aok_plan* p) {
     }
     pg.push_back(pg.back() + cur);
     const int npan = (int)pg.size() - 1;
-    if (npan > kMaxPanels) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: basis too large for the panels");
+    if (npan > kMaxPanels3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: basis too large for the panels");
     Panels3 pan{};
     pan.n = npan;
     std::vector<Item3> items;
@@ -122,8 +122,10 @@ int setup_overlap3c_schedule(aok_plan* p) {
                         const int c0 = k0 + c * ppc, c1 = std::min(k0 + (c + 1) * ppc, k1);
                         if (c1 <= pg[pn] || c0 >= pg[pn + 1]) continue;
                         const int cost = (la + 1) * (lb + 1) * (lc + 1) * 12 + 2 * ncart(la) * ncart(lb) * (c1 - c0);
-                        v.push_back({cost, Item3{(int16_t)(la * 9 + lb * 3 + lc), (int16_t)c, (int16_t)sa,
-                                                 (int16_t)sb, (int16_t)sc, 0}});
+                        const bool f = std::max(la, std::max(lb, lc)) > kMaxL3Spec;
+                        const int cls = f ? kClsF3 + la * 16 + lb * 4 + lc : la * 9 + lb * 3 + lc;
+                        v.push_back({f ? 4 * cost : cost, Item3{(int16_t)cls, (int16_t)c, (int16_t)sa, (int16_t)sb,
+                                                                (int16_t)sc, 0}});
                     }
                 }
         }

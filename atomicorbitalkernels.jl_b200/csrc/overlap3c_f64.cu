@@ -4,7 +4,8 @@
 namespace aok {
 
 int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s) {
-    return launch_ov3<double>(p, out, posA, posB, posC, s);
+    if (p->Lmax > kMaxL3Spec) return launch_ov3<double, true>(p, out, posA, posB, posC, s);
+    return launch_ov3<double, false>(p, out, posA, posB, posC, s);
 }
 
 }  // namespace aok

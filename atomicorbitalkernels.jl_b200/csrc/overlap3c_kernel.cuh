@@ -15,7 +15,7 @@
 //
 // Same execution model as the 2C kernel: tiles of 32 batch elements (lane =
 // element), a persistent CTA per SM, shell-triple classes (la, lb, lc <= 2)
-// compile-time specialised, work items drained from a per-tile shared-memory
+// compile-time specialised (classes with an f shell: run_item3_f, below), work items drained from a per-tile shared-memory
 // counter, results staged per output-page panel in shared memory and written
 // out coalesced (a batch element's (N,N,N) slab is contiguous).  Items are
 // whole shell-triple blocks or chunks of whole output pages; a chunk whose
@@ -29,8 +29,11 @@
 
 namespace aok {
 
-constexpr int kMaxL3 = 2;
+constexpr int kMaxL3 = 3;        // shells up to f
+constexpr int kMaxL3Spec = 2;    // compile-time specialised classes up to d
+constexpr int kClsF3 = 100;      // Item3 class code of a triple with an f shell: kClsF3 + la*16 + lb*4 + lc
 constexpr int kThreads3 = 256;
+constexpr int kMaxPanels3 = 64;  // output-page panels (one page per panel for wide FP64 bases)
 
 __host__ __device__ constexpr int pages_per_chunk3(int la, int lb) {
     return (ncart(la) * ncart(lb)) >= 36 ? 1 : 36 / (ncart(la) * ncart(lb));
@@ -60,8 +63,8 @@ struct Item3 {
 
 struct Panels3 {
     int n;
-    int page0[kMaxPanels + 1];   // global output page (k index) range of each panel
-    int item0[kMaxPanels + 1];
+    int page0[kMaxPanels3 + 1];  // global output page (k index) range of each panel
+    int item0[kMaxPanels3 + 1];
 };
 
 template <typename FT> struct Geo3;
@@ -277,6 +280,108 @@ __device__ __noinline__ void run_item3(const PTd* __restrict__ pp, int n, const 
     }
 }
 
+// Classes with an f shell (la, lb or lc = 3), one routine with run-time loops:
+// the E tables of the three axes (4 x 4 x 4 each) and the chunk's <= 100 block
+// elements live in local memory, and the recursion runs in FP64 for both
+// precisions (an FP32 record's exponent coefficient is rebuilt from its hi + lo
+// words).  The class and chunk follow the specialised path's conventions
+// (aliased lin, pages [P0, P1) of the block).  Only the kernel instantiated
+// for bases with f shells calls it, so its local memory is not reserved by
+// the others.
+__device__ __forceinline__ void e3_axis(double (&E)[4][4][4], int la, int lb, int lc, double QA, double QB, double QC,
+                                        double o2q, double e000) {
+    for (int k = 0; k <= lc; ++k)
+        for (int j = 0; j <= lb; ++j)
+            for (int i = 0; i <= la; ++i) {
+                double v;
+                if (i == 0 && j == 0 && k == 0) {
+                    v = e000;
+                } else if (i == 0 && j == 0) {
+                    v = QC * E[0][0][k - 1];
+                    if (k >= 2) v += ((k - 1) * o2q) * E[0][0][k - 2];
+                } else if (i == 0) {
+                    v = QB * E[0][j - 1][k];
+                    double c = 0.0;
+                    if (j >= 2) c += (j - 1) * E[0][j - 2][k];
+                    if (k >= 1) c += k * E[0][j - 1][k - 1];
+                    v += o2q * c;
+                } else {
+                    v = QA * E[i - 1][j][k];
+                    double c = 0.0;
+                    if (i >= 2) c += (i - 1) * E[i - 2][j][k];
+                    if (j >= 1) c += j * E[i - 1][j - 1][k];
+                    if (k >= 1) c += k * E[i - 1][j][k - 1];
+                    v += o2q * c;
+                }
+                E[i][j][k] = v;
+            }
+}
+
+__device__ __forceinline__ double pt_exponent(const PTf* r, const double (&R2)[3]) {
+    const double kab = (double)r->kab_hi + (double)r->kab_lo, kac = (double)r->kac_hi + (double)r->kac_lo,
+                 kbc = (double)r->kbc_hi + (double)r->kbc_lo;
+    return (kab * R2[0] + kac * R2[1] + kbc * R2[2]) * 0.69314718055994530942;  // records carry k log2(e)
+}
+__device__ __forceinline__ double pt_exponent(const PTd* r, const double (&R2)[3]) {
+    return r->kab * R2[0] + r->kac * R2[1] + r->kbc * R2[2];
+}
+
+template <typename PT, typename FT>
+__device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const Geo3<FT> g, FT* dst, int N, int kp0,
+                                         int kp1, int cls, int chunk) {
+    const int c = cls - kClsF3, la = c >> 4, lb = (c >> 2) & 3, lc = c & 3;
+    const int NA = ncart(la), NB = ncart(lb), NC = ncart(lc), PS = NA * NB, N1 = 2 * la + 1, N2 = 2 * lb + 1;
+    const int ppc = pages_per_chunk3(la, lb);
+    const int P0 = chunk * ppc, P1 = min((chunk + 1) * ppc, NC);
+    const int L0 = P0 * PS, M = (P1 - P0) * PS;  // <= 100
+    // the component pages c3 whose aliased lin can land in [L0, L0 + M)
+    const int span = (NA - 1) + N1 * (NB - 1);
+    int c3lo = 0, c3hi = NC;
+    while (c3lo < NC && N1 * N2 * c3lo + span < L0) ++c3lo;
+    while (c3hi > c3lo && N1 * N2 * (c3hi - 1) >= L0 + M) --c3hi;
+    double acc[100];
+    for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    double AB[3], AC[3], BC[3], R2[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        AB[a] = (double)g.AB[a];
+        AC[a] = (double)g.AC[a];
+        BC[a] = (double)g.BC[a];
+        R2[a] = (double)g.R2[a];
+        if constexpr (sizeof(FT) == 4) R2[a] += (double)g.R2lo[a];
+    }
+    double E[3][4][4][4];
+    for (int q = 0; q < n; ++q) {
+        const PT* r = pp + q;
+        const double w = (double)r->w, ra = (double)r->ra, rb = (double)r->rb, rc = (double)r->rc,
+                     o2q = (double)r->oo2q;
+        const double e000 = exp(-pt_exponent(r, R2)) * w;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            e3_axis(E[a], la, lb, lc, -(rb * AB[a] + rc * AC[a]), ra * AB[a] - rc * BC[a], ra * AC[a] + rb * BC[a],
+                    o2q, a == 0 ? e000 : 1.0);
+        for (int c3 = c3lo; c3 < c3hi; ++c3) {
+            const int x3 = cart_x(lc, c3), y3 = cart_y(lc, c3), z3 = cart_z(lc, c3);
+            for (int c2 = 0; c2 < NB; ++c2) {
+                const int x2 = cart_x(lb, c2), y2 = cart_y(lb, c2), z2 = cart_z(lb, c2);
+                for (int c1 = 0; c1 < NA; ++c1) {
+                    const int lin = c1 + N1 * c2 + N1 * N2 * c3 - L0;
+                    if (lin < 0 || lin >= M) continue;
+                    acc[lin] += E[0][cart_x(la, c1)][x2][x3] * (E[1][cart_y(la, c1)][y2][y3] *
+                                                                  E[2][cart_z(la, c1)][z2][z3]);
+                }
+            }
+        }
+    }
+    for (int m = 0; m < M; ++m) {
+        const int lin = L0 + m, pg = lin / PS;
+        if (pg >= kp0 && pg < kp1) {
+            const int i = lin % NA, j = (lin / NA) % NB;
+            dst[(size_t)(pg - kp0) * N * N + (size_t)j * N + i] = (FT)acc[m];
+        }
+    }
+}
+
 template <typename PT, typename FT, int LA, int LB, int LC>
 __device__ __forceinline__ void run_chunks3(int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N, int kp0,
                                             int kp1) {
@@ -292,9 +397,15 @@ __device__ __forceinline__ void run_chunks3(int chunk, const PT* pp, int n, cons
     }
 }
 
-template <typename PT, typename FT>
+template <typename PT, typename FT, bool F3>
 __device__ __forceinline__ void dispatch3(int cls, int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N,
                                           int kp0, int kp1) {
+    if constexpr (F3) {
+        if (cls >= kClsF3) {
+            run_item3_f<PT, FT>(pp, n, g, dst, N, kp0, kp1, cls, chunk);
+            return;
+        }
+    }
     switch (cls) {
 #define AOK_C3(LA, LB, LC) \
     case (LA) * 9 + (LB) * 3 + (LC): run_chunks3<PT, FT, LA, LB, LC>(chunk, pp, n, g, dst, N, kp0, kp1); break;
@@ -326,12 +437,13 @@ struct Ov3Params {
     int boff[kMaxShells + 1];
 };
 
-template <typename FT>
+// F3: the instantiation for bases with f shells (it alone holds run_item3_f).
+template <typename FT, bool F3>
 __global__ void __launch_bounds__(kThreads3, 1) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FT* slab = reinterpret_cast<FT*>(smem_raw);
     __shared__ int s_tile;
-    __shared__ int s_next[kMaxPanels];
+    __shared__ int s_next[kMaxPanels3];
     constexpr int NW = kThreads3 / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ntiles = *P.ntiles;
@@ -367,7 +479,8 @@ __global__ void __launch_bounds__(kThreads3, 1) k_overlap3c(const __grid_constan
                 // block-local page window of this panel, and the block's (0,0,first page) in the slab
                 const int kp0 = max(pg0 - koff, 0), kp1 = min(pg1 - koff, P.boff[wi.sc + 1] - koff);
                 FT* dst = sl + (size_t)(koff + kp0 - pg0) * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-                dispatch3(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K * P.K, n, g, dst, P.N, kp0, kp1);
+                dispatch3<typename PTT<FT>::type, FT, F3>(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K * P.K, n,
+                                                          g, dst, P.N, kp0, kp1);
             }
             __syncthreads();
             const size_t len = (size_t)(pg1 - pg0) * N2;
@@ -382,7 +495,7 @@ __global__ void __launch_bounds__(kThreads3, 1) k_overlap3c(const __grid_constan
     }
 }
 
-template <typename FT>
+template <typename FT, bool F3>
 inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s) {
     Ov3Params<FT> P;
     memset(&P, 0, sizeof(P));
@@ -403,7 +516,7 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.N = (int)p->N;
     P.slab_stride = (int)p->slab_stride3;
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
-    auto kern = k_overlap3c<FT>;
+    auto kern = k_overlap3c<FT, F3>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem3);
     if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap3c)");
     timing_begin(p, s);

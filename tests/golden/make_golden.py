@@ -152,6 +152,21 @@ def main():
              posC3=np.stack([g[2] for g in g3], 1), V=out3,
              pts=pts, Z=Z)
     print("wrote overlap_golden.npz", out2.shape, out3.shape, Z.shape)
+    make_f3(pack)
+
+
+def make_f3(pack):
+    """3C with an f shell (every class with l = 3 against s, p and f): overlap3c_f_golden.npz."""
+    rng = np.random.default_rng(20241203)
+    sh3 = [(0, [0.8], [1.3]), (3, [0.6, 0.5], [1.1, 0.45]), (1, [1.0], [0.7])]
+    g3 = [(np.zeros(3), np.array([1.1, 0.2, 0]), np.array([0, 0.9, -0.3])),
+          (rng.normal(size=3) * 0.4, rng.normal(size=3) * 0.4 + [1.2, 0, 0], rng.normal(size=3) * 0.4 + [0, 1, 0])]
+    out3 = np.stack([full3(sh3, A, B, C) for A, B, C in g3], axis=-1)
+    ls3, nprim3, coef3, alpha3 = pack(sh3)
+    np.savez(os.path.join(HERE, "overlap3c_f_golden.npz"), ls3=ls3, nprim3=nprim3, coef3=coef3, alpha3=alpha3,
+             posA3=np.stack([g[0] for g in g3], 1), posB3=np.stack([g[1] for g in g3], 1),
+             posC3=np.stack([g[2] for g in g3], 1), V=out3)
+    print("wrote overlap3c_f_golden.npz", out3.shape)
 
 
 if __name__ == "__main__":

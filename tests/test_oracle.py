@@ -32,6 +32,12 @@ def test_golden_3c():
     assert np.max(np.abs(V - G["V"])) < 1e-13 * max(1.0, np.abs(G["V"]).max())
 
 
+def test_golden_3c_f_shell():
+    F = np.load(os.path.join(os.path.dirname(__file__), "golden", "overlap3c_f_golden.npz"))
+    V = oracle.overlap3c_gb(F["ls3"], F["nprim3"], F["coef3"], F["alpha3"], F["posA3"], F["posB3"], F["posC3"])
+    assert np.max(np.abs(V - F["V"])) < 1e-13 * max(1.0, np.abs(F["V"]).max())
+
+
 def test_golden_solid_harmonics():
     Z, _ = oracle.solid_harmonics(G["pts"], 3)
     assert np.max(np.abs(Z - G["Z"])) < 1e-13

@@ -66,10 +66,62 @@ def test_golden_vectors_3c():
     assert np.max(np.abs(V.numpy() - G["V"])) < 1e-12
 
 
-def test_3c_rejects_f_shells_and_plain_positions():
-    bc = aok.compile_basis([aok.CartesianShell(3, np.array([1.0]), np.array([1.0]))])
+def test_golden_vectors_3c_f_shell():
+    F = np.load(os.path.join(os.path.dirname(__file__), "golden", "overlap3c_f_golden.npz"))
+    shells, o = [], 0
+    for s in range(len(F["ls3"])):
+        n = int(F["nprim3"][s])
+        shells.append(aok.CartesianShell(int(F["ls3"][s]), F["coef3"][o:o + n], F["alpha3"][o:o + n]))
+        o += n
+    bc = aok.compile_basis(shells)
+    V = aok.batch_overlap_3c(bc, _L(F["posA3"]), _L(F["posB3"]), _L(F["posC3"]))
+    assert np.max(np.abs(V.numpy() - F["V"])) < 1e-12 * max(1.0, np.abs(F["V"]).max())
+
+
+def _f_basis(seed=1010):
+    """s(2) p(1) d(2) f(2): every 3C class with an f shell occurs (N = 20; an FP64 output
+    page of 30 x 30 x 32 elements would exceed the shared-memory slab)."""
+    rng = np.random.default_rng(seed)
+    shells, ls, nprim, coef, alpha = [], [], [], [], []
+    for l, K in ((0, 2), (1, 1), (2, 2), (3, 2)):
+        a = np.sort(rng.uniform(0.3, 4.0, K))[::-1].copy()
+        c = rng.uniform(0.4, 1.2, K)
+        shells.append(aok.CartesianShell(l, c, a))
+        ls.append(l)
+        nprim.append(K)
+        coef.append(c)
+        alpha.append(a)
+    return (aok.compile_basis(shells), np.array(ls), np.array(nprim), np.concatenate(coef),
+            np.concatenate(alpha))
+
+
+@pytest.mark.parametrize("B", [1, 70])
+def test_f_shells_f64(B):
+    bc, ls, nprim, coef, z = _f_basis()
+    tr = W.config4_triples(B=B, seed=1011)
+    pA, pB, pC = _L(tr.posA), _L(tr.posB), _L(tr.posC)
+    V = aok.batch_overlap_3c(bc, pA, pB, pC)
+    ref = oracle.overlap3c_gb(ls, nprim, coef, z, aok.to_bohr(pA), aok.to_bohr(pB), aok.to_bohr(pC), nthreads=8)
+    assert V.shape == (20, 20, 20, B)
+    assert rel_fro(V, ref) < 1e-12
+
+
+def test_f_shells_f32c():
+    bc, ls, nprim, coef, z = _f_basis()
+    tr = W.config4_triples(B=96, seed=1012)
+    pA, pB, pC = _L(tr.posA), _L(tr.posB), _L(tr.posC)
+    V = aok.batch_overlap_3c(bc, pA, pB, pC, FT=torch.float32)
+    ref = oracle.overlap3c_gb(ls, nprim, f32_round(coef), f32_round(z), f32_round(aok.to_bohr(pA, np.float32)),
+                              f32_round(aok.to_bohr(pB, np.float32)), f32_round(aok.to_bohr(pC, np.float32)),
+                              nthreads=8)
+    assert V.dtype == torch.float32
+    assert rel_fro(V, ref) < 2e-6
+
+
+def test_3c_rejects_g_shells_and_plain_positions():
+    bc = aok.compile_basis([aok.CartesianShell(4, np.array([1.0]), np.array([1.0]))])
     p = aok.Length(np.zeros((3, 1)), "angstrom")
-    with pytest.raises(aok.AOKError):
+    with pytest.raises((aok.AOKError, aok.ArgumentError, ValueError)):
         aok.batch_overlap_3c(bc, p, p, p)
     bc2 = aok.compile_basis([aok.CartesianShell(0, np.array([1.0]), np.array([1.0]))])
     with pytest.raises(aok.ArgumentError):
