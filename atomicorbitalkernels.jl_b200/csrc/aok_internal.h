@@ -77,6 +77,18 @@ struct aok_plan {
         int64_t B;
         double lengthscale;
     } gkey{};
+    // rrule state (aok_overlap2c_rrule -> aok_overlap_pullback_ps_rrule): the
+    // arguments of the forward, the generation of the plan's bins and pullback
+    // records it left, and the event after its pullback-record preparation
+    struct RruleKey {
+        const void *zeta, *D, *posA, *posB;
+        const int64_t *sidxA, *sidxB;
+        int64_t B;
+        double lengthscale;
+    } rkey{};
+    uint64_t gen = 0;        // bumped by every call that rebins or rebuilds pullback records
+    uint64_t rgen = 0;       // the generation an rrule forward left (0: none)
+    cudaEvent_t ev_pb = nullptr;
     // side stream for the record preparation (forked/joined with events)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -145,6 +157,10 @@ constexpr int kBinMaxBlocksHost = 512;
 int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
                     cudaStream_t s);
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s);
+int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* D,
+                       const void* posA, const void* posB, double lengthscale, cudaStream_t s);
+int ensure_pb_buffers(aok_plan* p);
+int launch_prep_pb(aok_plan* p, const void* zeta, const void* coef, int keep_absent, cudaStream_t s);
 int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB, int64_t B,
                      double lengthscale, cudaStream_t s);
 int launch_gb_pad(aok_plan* p, const int64_t* nprim, const int64_t* prim_offset, const void* coef,

@@ -154,6 +154,7 @@ int aok_plan_destroy(aok_plan* p) {
     for (cudaEvent_t e : p->ev) cudaEventDestroy(e);
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);
     if (p->ev_join) cudaEventDestroy(p->ev_join);
+    if (p->ev_pb) cudaEventDestroy(p->ev_pb);
     if (p->side) cudaStreamDestroy(p->side);
     delete p;
     return AOK_OK;
@@ -250,6 +251,7 @@ static int overlap2c_graph(aok_plan* p, void* out, const void* posA, const void*
         }
         p->gkey = k;
     }
+    ++p->gen;  // the replayed chain rebins
     return cuda_status(cudaGraphLaunch(p->gexec, s), "cudaGraphLaunch");
 }
 
@@ -439,6 +441,60 @@ int aok_overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void* d
     if (!dcoef || !dalpha || !zeta || !coef) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
     return overlap2c_pullback(p, dcoef, dalpha, dS, zeta, coef, nullptr, posA, posB, sidxA, sidxB, B, lengthscale, 1,
                               stream, "aok_overlap2c_pullback");
+}
+
+int aok_overlap2c_rrule(aok_plan* p, void* out, const void* zeta, const void* D, const void* posA, const void* posB,
+                        const int64_t* sidxA, const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
+    if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap2c_rrule: null plan");
+    AOK_TRY(check_batch(p, B, "aok_overlap2c_rrule"));
+    p->rgen = 0;
+    if (B == 0) return AOK_OK;
+    if (!out || !zeta || !D || !posA || !posB || !sidxA || !sidxB)
+        return set_error(AOK_ERR_INVALID, "aok_overlap2c_rrule: null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    AOK_TRY(ensure_pb_buffers(p));
+    if (!p->ev_pb)
+        AOK_TRY(cuda_status(cudaEventCreateWithFlags(&p->ev_pb, cudaEventDisableTiming), "cudaEventCreate"));
+    p->basis_set = false;
+    void* coef = p->d_coef_scratch;
+    // side stream: coef, the forward records, then (while the overlap kernel runs) the pullback records
+    AOK_TRY(cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord"));
+    AOK_TRY(cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent"));
+    AOK_TRY(launch_compile_coef(p, coef, zeta, D, p->side));
+    AOK_TRY(launch_prep2c(p, zeta, coef, p->side));
+    AOK_TRY(cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord"));
+    AOK_TRY(launch_prep_pb(p, zeta, coef, 0, p->side));
+    AOK_TRY(cuda_status(cudaEventRecord(p->ev_pb, p->side), "cudaEventRecord"));
+    AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));
+    AOK_TRY(cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent"));
+    AOK_TRY(launch_overlap2c(p, out, posA, posB, B, lengthscale, s));
+    p->rkey = aok_plan::RruleKey{zeta, D, posA, posB, sidxA, sidxB, B, lengthscale};
+    p->rgen = p->gen;
+    return AOK_OK;
+}
+
+int aok_overlap_pullback_ps_rrule(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta,
+                                  const void* D, const void* posA, const void* posB, const int64_t* sidxA,
+                                  const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
+    static const char* who = "aok_overlap_pullback_ps_rrule";
+    if (!p) return set_error(AOK_ERR_INVALID, std::string(who) + ": null plan");
+    if (!dzeta || !dD || !zeta || !D) return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    AOK_TRY(check_batch(p, B, who));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (B == 0) {
+        const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
+        AOK_TRY(cuda_status(cudaMemsetAsync(dD, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync"));
+        return cuda_status(cudaMemsetAsync(dzeta, 0, fsz * p->ns * p->K * p->NZ, s), "cudaMemsetAsync");
+    }
+    if (!dS || !posA || !posB || !sidxA || !sidxB) return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    const aok_plan::RruleKey& k = p->rkey;
+    const bool match = p->rgen != 0 && p->rgen == p->gen && k.zeta == zeta && k.D == D && k.posA == posA &&
+                       k.posB == posB && k.sidxA == sidxA && k.sidxB == sidxB && k.B == B &&
+                       k.lengthscale == lengthscale;
+    if (!match)
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": no matching aok_overlap2c_rrule on this plan "
+                                                             "(other arguments, or another 2C call in between)");
+    return launch_pb_prepared(p, dD, dzeta, dS, zeta, D, posA, posB, lengthscale, s);
 }
 
 int aok_overlap_pullback_ps(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta, const void* D,

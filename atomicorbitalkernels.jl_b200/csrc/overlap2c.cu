@@ -667,6 +667,7 @@ int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidx
 }
 
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s) {
+    ++p->gen;  // the plan's bins change
     const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
     return launch_bin_into(bb, sidxA, sidxB, B, (int)p->NZ, s);
 }

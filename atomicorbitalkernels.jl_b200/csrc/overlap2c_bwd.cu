@@ -8,6 +8,7 @@
 namespace aok {
 
 int launch_prep_pb(aok_plan* p, const void* zeta, const void* coef, int keep_absent, cudaStream_t s) {
+    ++p->gen;  // the pullback records change
     const int n = (int)(p->NZ * p->NZ * p->ns * p->ns);
     const int bl = (n + kPrepPbWarps - 1) / kPrepPbWarps;
     const size_t sm = (size_t)kPrepPbWarps * 4 * p->K;
@@ -90,6 +91,18 @@ int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, con
     if (p->prec == AOK_PREC_F64)
         return launch_pb_f64(p, out0, out1, dS, zeta, coef, D, posA, posB, lengthscale, s);
     return launch_pb_f32(p, out0, out1, dS, zeta, coef, D, posA, posB, lengthscale, s);
+}
+
+// The pullback of an rrule forward (aok_overlap2c_rrule): its bins and its
+// pullback records (prepared on the side stream, ev_pb) are reused; the work
+// counter, consumed by the forward kernel, is reset.
+int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* D,
+                       const void* posA, const void* posB, double lengthscale, cudaStream_t s) {
+    AOK_TRY_PB(cuda_status(cudaStreamWaitEvent(s, p->ev_pb, 0), "cudaStreamWaitEvent"));
+    AOK_TRY_PB(cuda_status(cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned), s), "cudaMemsetAsync"));
+    if (p->prec == AOK_PREC_F64)
+        return launch_pb_f64(p, out0, out1, dS, zeta, p->d_coef_scratch, D, posA, posB, lengthscale, s);
+    return launch_pb_f32(p, out0, out1, dS, zeta, p->d_coef_scratch, D, posA, posB, lengthscale, s);
 }
 
 }  // namespace aok

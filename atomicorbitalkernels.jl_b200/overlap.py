@@ -296,11 +296,48 @@ def pullback_ps(dS, orb, XA, XB, ps, st):
 
 
 def rrule_batch_overlap(orb, XA, XB, ps, st):
-    """rrule(batch_overlap, orb, XA, XB, ps, st) (overlap_2c_grad.jl:309-318)."""
-    S = batch_overlap(orb, XA, XB, ps, st, device_out=True)
+    """rrule(batch_overlap, orb, XA, XB, ps, st) (overlap_2c_grad.jl:309-318).
+
+    The forward (aok_overlap2c_rrule) also prepares the pullback's records and
+    keeps the species bins, so that the pullback (aok_overlap_pullback_ps_rrule)
+    runs only the pullback kernel and its reductions.  If another 2C call used
+    the plan in between, the pullback takes the full pullback_ps path."""
+    FT = _ps_dtype(ps, XA)
+    XAp, XBp = as_pstates(XA), as_pstates(XB)
+    stc = compile_struct(orb)
+    sA = species_indices(stc["zlist"], XAp.species)
+    sB = species_indices(stc["zlist"], XBp.species)
+    B = len(XAp)
+    if len(XBp) != B:
+        raise RuntimeError(f"XA and XB must have equal length; got {len(XAp)} and {len(XBp)}")
+    ns, K, NZ, N = stc["nshells"], stc["K"], stc["NZ"], stc["nbf_total"]
+    S = _dev.colmajor_empty((N, N, B), FT)
+    if B == 0:
+        return S, lambda dS: (NoTangent, NoTangent, NoTangent, NoTangent, pullback_ps(dS, orb, XA, XB, ps, st),
+                              NoTangent)
+    _dev.require_cuda()
+    L = _lib.load()
+    plan = _dev.plan_for(stc["ls"], K, NZ, _dev.prec_of(FT), B)
+    zeta = _dev.to_colmajor(ps["Rnl"]["zeta"], FT)
+    D = _dev.to_colmajor(ps["Rnl"]["D"], FT)
+    dA, dB = _dev.to_colmajor(XAp.pos, FT), _dev.to_colmajor(XBp.pos, FT)
+    gA, gB = _dev_int64(sA), _dev_int64(sB)
+    ls = float(orb.lengthscale)
+    _lib.check(L.aok_overlap2c_rrule(plan.h, _dev.ptr(S), _dev.ptr(zeta), _dev.ptr(D), _dev.ptr(dA), _dev.ptr(dB),
+                                     _dev.ptr(gA), _dev.ptr(gB), B, ls, _dev.stream()))
 
     def _pb(dS):
-        dps = pullback_ps(dS, orb, XA, XB, ps, st)
+        dSd = _dev.to_colmajor(dS, FT)
+        dz = _dev.colmajor_empty((ns, K, NZ), FT)
+        dD = _dev.colmajor_empty((ns, K, NZ), FT)
+        status = L.aok_overlap_pullback_ps_rrule(plan.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dSd), _dev.ptr(zeta),
+                                                 _dev.ptr(D), _dev.ptr(dA), _dev.ptr(dB), _dev.ptr(gA), _dev.ptr(gB),
+                                                 B, ls, _dev.stream())
+        if status == _lib.AOK_ERR_INVALID:  # the plan served another call since the forward
+            dps = pullback_ps(dS, orb, XA, XB, ps, st)
+        else:
+            _lib.check(status)
+            dps = {"Rnl": {"zeta": dz, "D": dD}, "Ylm": {}}
         return (NoTangent, NoTangent, NoTangent, NoTangent, dps, NoTangent)
 
     return S, _pb

@@ -340,9 +340,10 @@ def main():
         g_ms = tloop(gstep, ng)
         Bg = gd["Bg"]
         del gd
-        grad = {"workload": "config 3: L = sum (S - S_tgt)^2 over B=16384 pairs, FP32C forward + pullback_ps",
+        grad = {"workload": "config 3: L = sum (S - S_tgt)^2 over B=16384 pairs, FP32C rrule forward (coef from D, "
+                            "pullback records prepared beside the overlap kernel) + dL/dS + rrule pullback",
                 "batch": Bg, "forward_ms": f_ms, "step_ms": g_ms, "step_over_forward": g_ms / f_ms,
-                "launches_per_step": 3 + 5 + 7}
+                "launches_per_step": 6 + 3, "torch_launches_per_step": 2}
 
     # ---- error of FP32C and FP64 vs the FP64 oracle on a sample (inputs rounded as the GPU saw them) ----
     nchk = 2048
@@ -457,7 +458,8 @@ def main():
 def _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch):
     import torch.distributed as dist
     """Config 3: L = sum (S - S_tgt)^2 over the first 16384 pairs of the batch, FP32C.
-    gstep = compile_coef + forward + dL/dS + pullback_ps (dzeta, dD); fstep = forward."""
+    gstep = rrule forward (coef compiled from D, the pullback's records prepared beside the
+    overlap kernel, bins kept) + dL/dS + the rrule's pullback (dzeta, dD); fstep = forward."""
     N, ns, K, NZ = basis.nbf_total, basis.nshells, basis.K, basis.NZ
     Bg = min(16384, B)
     zt, Dt = aok.workloads.config3_target(basis)
@@ -483,15 +485,14 @@ def _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch):
                                sA, sB, Bg, 1.0, _dev.stream()))
 
     def gstep():
-        _lib.check(L.aok_compile_coef(gpl.h, _dev.ptr(c32["coef"]), _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]),
-                                      _dev.stream()))
-        fwd(Sg, c32["coef"])
+        _lib.check(L.aok_overlap2c_rrule(gpl.h, _dev.ptr(Sg), _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]),
+                                         _dev.ptr(pA), _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
         # dL/dS = 2 (S - S_tgt); the pullback is linear in dS, so the factor 2 is applied
         # to the (ns, K, NZ) gradients instead of the (N, N, B) cotangent
         torch.sub(Sg, Tg, out=dS)
-        _lib.check(L.aok_overlap_pullback_ps(gpl.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS),
-                                             _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
-                                             _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
+        _lib.check(L.aok_overlap_pullback_ps_rrule(gpl.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dS),
+                                                   _dev.ptr(c32["zeta"]), _dev.ptr(c32["D"]), _dev.ptr(pA),
+                                                   _dev.ptr(pB), sA, sB, Bg, 1.0, _dev.stream()))
         torch._foreach_mul_([dz, dD], 2.0)
         if dist.is_initialized() and dist.get_world_size() > 1:
             aok.parallel.allreduce_sum([dz, dD])  # data-parallel step: sum the ranks' gradients

@@ -188,6 +188,27 @@ int aok_overlap_pullback_ps(aok_plan* plan, void* dzeta, void* dD, const void* d
                             int64_t B, double lengthscale, void* stream);
 
 /*
+ * The two halves of rrule(batch_overlap, orb, XA, XB, ps, st)
+ * (src/integrals/orbital/overlap_2c_grad.jl:309-318) with the pullback's
+ * preparation moved into the forward.  aok_overlap2c_rrule computes coef from
+ * (zeta, D) as compile_basis does, writes S = batch_overlap(orb, XA, XB, ps, st)
+ * into out, and, on the plan's side stream while the overlap kernel runs,
+ * prepares the pullback's primitive-pair records; it keeps the species binning.
+ * aok_overlap_pullback_ps_rrule then returns (dzeta, dD) as aok_overlap_pullback_ps
+ * would, without compiling, preparing or binning again.  It must follow the
+ * forward on the same plan with the same zeta, D, posA, posB, sidxA, sidxB, B and
+ * lengthscale, and with no other 2C call on the plan in between; otherwise it
+ * returns AOK_ERR_INVALID.  The caller keeps the inputs unchanged in between.
+ */
+int aok_overlap2c_rrule(aok_plan* plan, void* out, const void* zeta, const void* D,
+                        const void* posA, const void* posB, const int64_t* sidxA,
+                        const int64_t* sidxB, int64_t B, double lengthscale, void* stream);
+int aok_overlap_pullback_ps_rrule(aok_plan* plan, void* dzeta, void* dD, const void* dS,
+                                  const void* zeta, const void* D, const void* posA,
+                                  const void* posB, const int64_t* sidxA, const int64_t* sidxB,
+                                  int64_t B, double lengthscale, void* stream);
+
+/*
  * Orbital-evaluation plan: radial spec (nRad radials, K slots, NZ species,
  * poly[nRad] radial powers), orbital index maps iR, iY (nOrb, 1-based),
  * harmonics up to L.  Mirrors AtomicOrbitals' state

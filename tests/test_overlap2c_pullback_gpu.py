@@ -110,6 +110,40 @@ def test_rrule_roundtrip():
     assert torch.equal(out[4]["Rnl"]["D"], g["Rnl"]["D"])
 
 
+@pytest.mark.parametrize("FT", [torch.float64, torch.float32])
+def test_rrule_prepared_pullback(FT):
+    """The rrule's pullback right after its forward runs the prepared path (records and
+    bins of the forward); its gradient equals pullback_ps bit for bit, also when called
+    twice.  Another 2C call on the plan in between makes the C entry point refuse with
+    AOK_ERR_INVALID, and the Python pullback then takes the pullback_ps path."""
+    import ctypes
+    from aok_b200 import _dev, _lib
+    b, pr, dS = _inputs(1500, seed=23)
+    np_ft = np.float64 if FT == torch.float64 else np.float32
+    orb, cob, XA, XB = _cob_and_states(b, pr, FT)
+    ps = {"Rnl": {"zeta": b.zeta.astype(np_ft), "D": b.D.astype(np_ft)}, "Ylm": {}}
+    st = aok.initialstates(orb)
+    dS = dS.astype(np_ft)
+    S, pb = aok.rrule_batch_overlap(orb, XA, XB, ps, st)
+    g1 = pb(dS)[4]
+    g1b = pb(dS)[4]
+    S2 = aok.batch_overlap(orb, XA, XB, ps, st)  # uses the same plan: the prepared state is gone
+    assert torch.equal(S.cpu(), S2)
+    g2 = aok.overlap_pullback_ps(dS, orb, XA, XB, ps, st)
+    for g in (g1, g1b):
+        assert torch.equal(g["Rnl"]["zeta"], g2["Rnl"]["zeta"]) and torch.equal(g["Rnl"]["D"], g2["Rnl"]["D"])
+    g3 = pb(dS)[4]  # fallback path
+    assert torch.equal(g3["Rnl"]["zeta"], g2["Rnl"]["zeta"]) and torch.equal(g3["Rnl"]["D"], g2["Rnl"]["D"])
+    # the C entry point refuses a pullback whose forward is not the plan's last 2C call
+    L = _lib.load()
+    plan = _dev.plan_for(tuple(int(x) for x in b.ls), b.K, b.NZ, _dev.prec_of(FT), pr.B)
+    z = _dev.colmajor_empty(b.zeta.shape, FT)
+    status = L.aok_overlap_pullback_ps_rrule(plan.h, _dev.ptr(z), _dev.ptr(z), _dev.ptr(z), _dev.ptr(z), _dev.ptr(z),
+                                             _dev.ptr(z), _dev.ptr(z), ctypes.c_void_p(8), ctypes.c_void_p(8), pr.B,
+                                             1.0, _dev.stream())
+    assert status == _lib.AOK_ERR_INVALID
+
+
 def test_pullback_deterministic():
     b, pr, dS = _inputs(2048, seed=19)
     orb, cob, XA, XB = _cob_and_states(b, pr, torch.float32)
