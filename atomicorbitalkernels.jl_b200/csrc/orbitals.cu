@@ -149,7 +149,12 @@ __device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl,
     const FT f = slater ? r : r * r;
     const FT df = slater ? FT(1) : FT(2) * r;
     FT s = FT(0), se = FT(0), ds = FT(0);
-    for (int m = 0; m < K; ++m) {
+    // FP64: trailing primitives with D = 0 (padding of shorter contractions) add exact
+    // zeros, so their exp is skipped (in FP32 the scan costs more than the cheap exps)
+    int mk = K;
+    if constexpr (sizeof(FT) == 8)
+        while (mk > 0 && sD[k + nRad * (mk - 1 + K * sg)] == FT(0)) --mk;
+    for (int m = 0; m < mk; ++m) {
         const int o = k + nRad * (m + K * sg);
         const FT z = sz[o];
         const FT a = sD[o] * exp_neg(z, sl[o], f);
