@@ -143,17 +143,25 @@ __device__ __forceinline__ double exp_neg(double z, double zl, double f) {
     return exp(-z * f);
 }
 
+// Words (of FT) of the per-(radial, species) primitive counts that follow the tables.
+__host__ __device__ constexpr int count_words(int nRad, int NZ, int fsz) { return (nRad * NZ * 4 + fsz - 1) / fsz; }
+
+// Primitives of radial k, species sg, up to the last non-zero D: the trailing ones
+// (padding of shorter contractions) add exact zeros to R and dR, so they are skipped.
 template <typename FT>
-__device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl, int k, int sg, int nRad, int K,
-                                       int p, int slater, FT r, FT& R, FT& dR) {
+__device__ __forceinline__ int radial_count(const FT* D, int k, int sg, int nRad, int K) {
+    int mk = K;
+    while (mk > 0 && D[k + nRad * (mk - 1 + K * sg)] == FT(0)) --mk;
+    return mk;
+}
+
+template <typename FT>
+__device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl, const int* sn, int k, int sg,
+                                       int nRad, int K, int p, int slater, FT r, FT& R, FT& dR) {
     const FT f = slater ? r : r * r;
     const FT df = slater ? FT(1) : FT(2) * r;
     FT s = FT(0), se = FT(0), ds = FT(0);
-    // FP64: trailing primitives with D = 0 (padding of shorter contractions) add exact
-    // zeros, so their exp is skipped (in FP32 the scan costs more than the cheap exps)
-    int mk = K;
-    if constexpr (sizeof(FT) == 8)
-        while (mk > 0 && sD[k + nRad * (mk - 1 + K * sg)] == FT(0)) --mk;
+    const int mk = sn[k + nRad * sg];
     for (int m = 0; m < mk; ++m) {
         const int o = k + nRad * (m + K * sg);
         const FT z = sz[o];
@@ -185,19 +193,21 @@ struct EvalSmem {
     FT* sz;
     FT* sD;
     FT* sl;  // zeta log2(e)
+    int* sn; // primitive counts per (radial, species), radial_count
     FT* R;
     FT* dR;
     FT* Z;
     FT* G;
 };
 template <typename FT>
-__device__ __forceinline__ EvalSmem<FT> eval_smem(unsigned char* raw, int ntab, int nRad, int nY) {
+__device__ __forceinline__ EvalSmem<FT> eval_smem(unsigned char* raw, int ntab, int nRad, int NZ, int nY) {
     EvalSmem<FT> s;
     FT* p = reinterpret_cast<FT*>(raw);
     s.sz = p;
     s.sD = p + ntab;
     s.sl = p + 2 * ntab;
-    p += 3 * ntab;
+    s.sn = reinterpret_cast<int*>(p + 3 * ntab);
+    p += 3 * ntab + count_words(nRad, NZ, (int)sizeof(FT));
     s.R = p;
     p += nRad * kEvalThreads;
     s.dR = p;
@@ -213,12 +223,14 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int nY = (L + 1) * (L + 1);
     const int ntab = P.nRad * P.K * P.NZ;
-    EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, nY);
+    EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, P.NZ, nY);
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         S.sz[i] = ((const FT*)P.zeta)[i];
         S.sD[i] = ((const FT*)P.D)[i];
         S.sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
     }
+    for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
+        S.sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
     __syncthreads();
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= P.nX) return;
@@ -239,7 +251,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
     }
     for (int k = 0; k < P.nRad; ++k) {
         FT R, dR;
-        radial<FT>(S.sz, S.sD, S.sl, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+        radial<FT>(S.sz, S.sD, S.sl, S.sn, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
         S.R[k * kEvalThreads + t] = R;
         S.dR[k * kEvalThreads + t] = dR;
     }
@@ -276,16 +288,19 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
     constexpr int nY = (L + 1) * (L + 1);
     constexpr int NW = kEvalThreads / 32;
     const int ntab = P.nRad * P.K * P.NZ;
-    EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, nY);
+    EvalSmem<FT> S = eval_smem<FT>(smem_raw, ntab, P.nRad, P.NZ, nY);
     // per-warp FP64 accumulators [warp][2][ntab] after the per-thread scratch
     double* wacc = reinterpret_cast<double*>(
-        smem_raw + (((size_t)3 * ntab + (size_t)(2 * P.nRad + 4 * nY) * kEvalThreads) * sizeof(FT) + 7) / 8 * 8);
+        smem_raw + (((size_t)3 * ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) +
+                     (size_t)(2 * P.nRad + 4 * nY) * kEvalThreads) * sizeof(FT) + 7) / 8 * 8);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         S.sz[i] = ((const FT*)P.zeta)[i];
         S.sD[i] = ((const FT*)P.D)[i];
         S.sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
     }
+    for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
+        S.sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
     for (int i = threadIdx.x; i < NW * 2 * ntab; i += blockDim.x) wacc[i] = 0.0;
     __syncthreads();
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -314,7 +329,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
     const int sgc = sg < 0 ? 0 : sg;
     for (int k = 0; k < P.nRad; ++k) {
         FT R, dR;
-        radial<FT>(S.sz, S.sD, S.sl, k, sgc, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+        radial<FT>(S.sz, S.sD, S.sl, S.sn, k, sgc, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
         S.R[k * kEvalThreads + t] = R;
         S.dR[k * kEvalThreads + t] = dR;
     }
@@ -434,7 +449,8 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
     FT* sz = reinterpret_cast<FT*>(smem_raw);
     FT* sD = sz + ntab;
     FT* sl = sD + ntab;  // zeta log2(e)
-    FT* wbase = sl + ntab + (size_t)warp * epb_warp_words(P.nRad, nY);
+    int* sn = reinterpret_cast<int*>(sl + ntab);
+    FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) + (size_t)warp * epb_warp_words(P.nRad, nY);
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY, *gg = G + 96 * nY,
        *fv = gg + 32 * P.nRad;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
@@ -442,6 +458,8 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
         sD[i] = ((const FT*)P.D)[i];
         sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
     }
+    for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
+        sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
     if (threadIdx.x == 0) {
         int acc = 0;
         for (int g = 0; g < P.NZ; ++g) {
@@ -489,7 +507,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                 const FT r = sqrt(x * x + y * y + z * z);
                 for (int k = 0; k < P.nRad; ++k) {
                     FT Rk, dRk;
-                    radial<FT>(sz, sD, sl, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
+                    radial<FT>(sz, sD, sl, sn, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
                     R[k * 32 + lane] = Rk;
                     dR[k * 32 + lane] = dRk;
                     gg[k * 32 + lane] = FT(0);
@@ -594,7 +612,8 @@ static size_t eval_smem_bytes(const aok_orbitals* o, bool pb) {
     const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
     const int nY = (o->L + 1) * (o->L + 1);
     const size_t ntab = (size_t)(o->nRad * o->K * o->NZ);
-    size_t b = (3 * ntab + (size_t)(2 * o->nRad + 4 * nY) * kEvalThreads) * fsz;
+    size_t b = (3 * ntab + (size_t)count_words((int)o->nRad, (int)o->NZ, (int)fsz) +
+                (size_t)(2 * o->nRad + 4 * nY) * kEvalThreads) * fsz;
     if (pb) b = (b + 7) / 8 * 8 + (size_t)(kEvalThreads / 32) * 2 * ntab * 8;
     return b;
 }
@@ -708,7 +727,7 @@ template <typename FT, int L>
 static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
     constexpr int nY = (L + 1) * (L + 1);
     const size_t fsz = sizeof(FT);
-    const size_t tab = 3 * (size_t)(o->nRad * o->K * o->NZ) * fsz;
+    const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
     const size_t per_warp = epb_warp_words((int)o->nRad, nY) * fsz;
     int nw = 8;
     while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;
