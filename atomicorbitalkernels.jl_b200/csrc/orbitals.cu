@@ -232,51 +232,53 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
     for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
         S.sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
     __syncthreads();
-    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= P.nX) return;
-    const int t = threadIdx.x;
-    const FT* X = (const FT*)P.X;
-    FT x = X[3 * j], y = X[3 * j + 1], z = X[3 * j + 2];
-    const FT sc = (FT)P.scale;
-    if (sc != FT(1)) {
-        x = sc * x;
-        y = sc * y;
-        z = sc * z;
-    }
-    const FT r = sqrt(x * x + y * y + z * z);
-    int sg = (int)P.sidx[j] - 1;
-    if (sg < 0 || sg >= P.NZ) {
-        atomicCAS(P.err, 0, AOK_ERR_SPECIES);
-        sg = 0;
-    }
-    for (int k = 0; k < P.nRad; ++k) {
-        FT R, dR;
-        radial<FT>(S.sz, S.sD, S.sl, S.sn, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
-        S.R[k * kEvalThreads + t] = R;
-        S.dR[k * kEvalThreads + t] = dR;
-    }
-    solid_harmonics<FT, L>(x, y, z, P.F, S.Z + t, S.G + t, kEvalThreads);
-    FT* Pout = (FT*)P.P;
-    FT* dPout = (FT*)P.dP;
-    const FT ux = x / r, uy = y / r, uz = z / r;  // X[j] / r[j] (NaN at r = 0, as the reference)
-    for (int i = 0; i < P.nOrb; ++i) {
-        const int k = P.iR[i], yi = P.iY[i];
-        const FT rn = S.R[k * kEvalThreads + t], yl = S.Z[yi * kEvalThreads + t];
-        Pout[j + P.nX * i] = rn * yl;
-        if (GRAD) {
-            const FT dr = S.dR[k * kEvalThreads + t];
-            FT* o = dPout + 3 * (j + P.nX * i);
-            FT gx = (dr * ux) * yl + rn * S.G[(3 * yi + 0) * kEvalThreads + t];
-            FT gy = (dr * uy) * yl + rn * S.G[(3 * yi + 1) * kEvalThreads + t];
-            FT gz = (dr * uz) * yl + rn * S.G[(3 * yi + 2) * kEvalThreads + t];
-            if (sc != FT(1)) {
-                gx *= sc;
-                gy *= sc;
-                gz *= sc;
+    // the blocks stay resident and stride over the points, so each stages the tables once
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < P.nX;
+         j += (long long)gridDim.x * blockDim.x) {
+        const int t = threadIdx.x;
+        const FT* X = (const FT*)P.X;
+        FT x = X[3 * j], y = X[3 * j + 1], z = X[3 * j + 2];
+        const FT sc = (FT)P.scale;
+        if (sc != FT(1)) {
+            x = sc * x;
+            y = sc * y;
+            z = sc * z;
+        }
+        const FT r = sqrt(x * x + y * y + z * z);
+        int sg = (int)P.sidx[j] - 1;
+        if (sg < 0 || sg >= P.NZ) {
+            atomicCAS(P.err, 0, AOK_ERR_SPECIES);
+            sg = 0;
+        }
+        for (int k = 0; k < P.nRad; ++k) {
+            FT R, dR;
+            radial<FT>(S.sz, S.sD, S.sl, S.sn, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+            S.R[k * kEvalThreads + t] = R;
+            S.dR[k * kEvalThreads + t] = dR;
+        }
+        solid_harmonics<FT, L>(x, y, z, P.F, S.Z + t, S.G + t, kEvalThreads);
+        FT* Pout = (FT*)P.P;
+        FT* dPout = (FT*)P.dP;
+        const FT ux = x / r, uy = y / r, uz = z / r;  // X[j] / r[j] (NaN at r = 0, as the reference)
+        for (int i = 0; i < P.nOrb; ++i) {
+            const int k = P.iR[i], yi = P.iY[i];
+            const FT rn = S.R[k * kEvalThreads + t], yl = S.Z[yi * kEvalThreads + t];
+            Pout[j + P.nX * i] = rn * yl;
+            if (GRAD) {
+                const FT dr = S.dR[k * kEvalThreads + t];
+                FT* o = dPout + 3 * (j + P.nX * i);
+                FT gx = (dr * ux) * yl + rn * S.G[(3 * yi + 0) * kEvalThreads + t];
+                FT gy = (dr * uy) * yl + rn * S.G[(3 * yi + 1) * kEvalThreads + t];
+                FT gz = (dr * uz) * yl + rn * S.G[(3 * yi + 2) * kEvalThreads + t];
+                if (sc != FT(1)) {
+                    gx *= sc;
+                    gy *= sc;
+                    gz *= sc;
+                }
+                o[0] = gx;
+                o[1] = gy;
+                o[2] = gz;
             }
-            o[0] = gx;
-            o[1] = gy;
-            o[2] = gz;
         }
     }
 }
@@ -622,8 +624,17 @@ template <typename FT, int L>
 static int launch_eval_L(aok_orbitals* o, EvalParams& P, bool grad, bool pb, cudaStream_t s) {
     const size_t smem = eval_smem_bytes(o, pb);
     if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "evaluate: basis too large for shared memory");
-    const int grid = (int)((P.nX + kEvalThreads - 1) / kEvalThreads);
+    int grid = (int)((P.nX + kEvalThreads - 1) / kEvalThreads);
     cudaError_t e;
+    if (!pb) {  // resident blocks striding over the points (k_evaluate)
+        int occ = 0;
+        auto kq = grad ? k_evaluate<FT, L, true> : k_evaluate<FT, L, false>;
+        if ((e = cudaFuncSetAttribute(kq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate)");
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kq, kEvalThreads, smem)) != cudaSuccess)
+            return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        grid = std::max(1, std::min(grid, o->num_sms * std::max(occ, 1)));
+    }
     if (pb) {
         auto k = k_evaluate_pb<FT, L>;
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
