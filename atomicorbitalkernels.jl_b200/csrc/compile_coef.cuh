@@ -48,15 +48,38 @@ __device__ __forceinline__ double warp_normsum(const FT* __restrict__ zeta, cons
 // tg: 2*K*K doubles of this warp's shared memory.  The K*K terms
 // D_j / (z_m + z_j)^e (and the same over (z_m + z_j)) are spread over the
 // lanes; lane m adds row m in order j = 0..K-1.
+// The parameter-only half of the VJP below: normsq = c * sum_ij ..., and the K*K
+// terms D_j / (z_m + z_j)^e (tg) and the same over (z_m + z_j) (th), in this
+// warp's shared memory.  Returns normsq.
+template <typename FT>
+__device__ __forceinline__ double coef_vjp_prepare(const FT* __restrict__ zeta, const FT* __restrict__ D, double* tg,
+                                                   size_t base, int ns, int K, int l, int lane) {
+    auto Dv = [&](int i) { return (double)D[base + (size_t)ns * i]; };
+    auto zv = [&](int i) { return (double)zeta[base + (size_t)ns * i]; };
+    const double nsq = norm_c(l) * warp_normsum(zeta, D, base, ns, K, l, lane);
+    double* th = tg + K * K;
+    for (int e2 = lane; e2 < K * K; e2 += 32) {
+        const int m = e2 / K, j = e2 % K;
+        const double den = zv(m) + zv(j);
+        const double p = pow_l32(den, l);
+        tg[e2] = Dv(j) / p;
+        th[e2] = Dv(j) / (p * den);
+    }
+    __syncwarp();
+    return nsq;
+}
+
+// The cotangent half: dD_m = dcoef_m / n - g_m dot / (2 n^3),  dz_m = dalpha_m - h_m dot / (2 n^3).
+// dcoef(i), dalpha(i): callables giving the incoming cotangents (double); tg and nsq
+// from coef_vjp_prepare (same warp, or after a barrier).  Lane m adds row m in order
+// j = 0..K-1.
 template <typename FT, typename DC, typename DA>
-__device__ __forceinline__ void coef_vjp_warp(FT* __restrict__ dD, FT* __restrict__ dz, DC dcoef, DA dalpha,
-                                              const FT* __restrict__ zeta, const FT* __restrict__ D, double* tg,
-                                              size_t base, int ns, int K, int l, int lane) {
+__device__ __forceinline__ void coef_vjp_finish(FT* __restrict__ dD, FT* __restrict__ dz, DC dcoef, DA dalpha,
+                                                const FT* __restrict__ D, const double* tg, double nsq, size_t base,
+                                                int ns, int K, int l, int lane) {
     const double e = (double)l + 1.5;
     const double c = norm_c(l);
     auto Dv = [&](int i) { return (double)D[base + (size_t)ns * i]; };
-    auto zv = [&](int i) { return (double)zeta[base + (size_t)ns * i]; };
-    const double nsq = c * warp_normsum(zeta, D, base, ns, K, l, lane);
     double dot = 0.0;
     for (int i = lane; i < K; i += 32) dot += dcoef(i) * Dv(i);
 #pragma unroll
@@ -71,15 +94,7 @@ __device__ __forceinline__ void coef_vjp_warp(FT* __restrict__ dD, FT* __restric
     }
     const double n = sqrt(nsq);
     const double s2n3 = dot / (2.0 * ((n * n) * n));
-    double* th = tg + K * K;
-    for (int e2 = lane; e2 < K * K; e2 += 32) {
-        const int m = e2 / K, j = e2 % K;
-        const double den = zv(m) + zv(j);
-        const double p = pow_l32(den, l);
-        tg[e2] = Dv(j) / p;
-        th[e2] = Dv(j) / (p * den);
-    }
-    __syncwarp();
+    const double* th = tg + K * K;
     for (int m = lane; m < K; m += 32) {
         double gm = 0.0, hm = 0.0;
         for (int j = 0; j < K; ++j) {
@@ -92,6 +107,17 @@ __device__ __forceinline__ void coef_vjp_warp(FT* __restrict__ dD, FT* __restric
         dD[o] = (FT)(dcoef(m) / n - gm * s2n3);
         dz[o] = (FT)(dalpha(m) - hm * s2n3);
     }
+}
+
+// VJP of coef = D / sqrt(normsq) for one (shell, species), run by one warp
+// (coef_vjp_prepare, then coef_vjp_finish); tg: 2*K*K doubles of this warp's
+// shared memory.
+template <typename FT, typename DC, typename DA>
+__device__ __forceinline__ void coef_vjp_warp(FT* __restrict__ dD, FT* __restrict__ dz, DC dcoef, DA dalpha,
+                                              const FT* __restrict__ zeta, const FT* __restrict__ D, double* tg,
+                                              size_t base, int ns, int K, int l, int lane) {
+    const double nsq = coef_vjp_prepare<FT>(zeta, D, tg, base, ns, K, l, lane);
+    coef_vjp_finish<FT>(dD, dz, dcoef, dalpha, D, tg, nsq, base, ns, K, l, lane);
 }
 
 }  // namespace aok

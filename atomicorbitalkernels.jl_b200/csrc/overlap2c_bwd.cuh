@@ -607,19 +607,23 @@ __global__ void k_pb_reduce_ps(FT* __restrict__ dD, FT* __restrict__ dz, const d
                                const FT* __restrict__ coef, const FT* __restrict__ D, const int* __restrict__ ls,
                                int ns, int K, int NZ, int nitems) {
     extern __shared__ double red[];  // dcoef[K], dalpha[K], VJP terms [2][K*K]
+    __shared__ double s_nsq;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int s = blockIdx.x % ns, sigma = blockIdx.x / ns;
-    for (int w = warp; w < 2 * K; w += nw) {
+    const size_t base = (size_t)s + (size_t)ns * K * sigma;
+    if (warp == 0) {  // the parameter-only half of the VJP, beside the slot sums
+        const double nsq = coef_vjp_prepare<FT>(zeta, D, red + 2 * K, base, ns, K, ls[s], lane);
+        if (lane == 0) s_nsq = nsq;
+    }
+    for (int w = warp - 1; w >= 0 && w < 2 * K; w += nw - 1) {
         const double v = pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, w / K, s, w % K, sigma, lane);
         if (lane == 0) red[w] = v;
     }
     __syncthreads();
-    if (warp == 0) {
-        const size_t base = (size_t)s + (size_t)ns * K * sigma;
-        coef_vjp_warp<FT>(
-            dD, dz, [&](int i) { return red[i]; }, [&](int i) { return red[K + i]; }, zeta, D, red + 2 * K, base,
+    if (warp == 0)
+        coef_vjp_finish<FT>(
+            dD, dz, [&](int i) { return red[i]; }, [&](int i) { return red[K + i]; }, D, red + 2 * K, s_nsq, base,
             ns, K, ls[s], lane);
-    }
 }
 
 constexpr int kPbThreadsF32 = 32 * kPbWarps;  // two CTAs per SM
