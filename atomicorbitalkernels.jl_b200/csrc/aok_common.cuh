@@ -52,7 +52,9 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 // FP64.  With p = a + b, w = c_a c_b (pi/p)^{3/2} and the moment slots
 // (al, be) used by the class (al <= la, be <= lb, (la - al) + (lb - be) even,
 // ga = (la + lb - al - be) / 2), in slot order:
-//   FP32:  mu log2(e) as hi, lo;  row length;  w rb^al ra^be q^ga per slot
+//   FP32:  w rb^al ra^be q^ga per slot;  mu log2(e) as hi, lo;  row length
+//          (the slot values first, so that pairs of them are aligned register
+//          pairs for the paired FMA)
 //   FP64:  mu;                    row length;  w rb^al ra^be q^ga per slot
 // (ra = a/p, rb = b/p, q = 1/2p), padded to whole 16-byte words.  The row
 // length is the number of non-zero ket coefficients: records form rows of

@@ -97,10 +97,10 @@ __device__ __forceinline__ void fill_pp(float* r, int la, int lb, double ca, dou
     const double mu2 = ((aa * ab) * ip) * log2e;  // exponent in base 2
     double wm[8];
     const int nv = fill_monos(wm, la, lb, ca * cb * (x * sqrt(x)), aa * ip, ab * ip, 0.5 * ip);
-    r[0] = (float)mu2;
-    r[1] = (float)(mu2 - (double)r[0]);
-    r[2] = (float)rowlen;
-    for (int j = 0; j < nv; ++j) r[3 + j] = (float)wm[j];
+    for (int j = 0; j < nv; ++j) r[j] = (float)wm[j];
+    r[nv] = (float)mu2;
+    r[nv + 1] = (float)(mu2 - (double)r[nv]);
+    r[nv + 2] = (float)rowlen;
     for (int j = 3 + nv; j < 4 * rec_words16_f32(la, lb); ++j) r[j] = 0.f;
 }
 __device__ __forceinline__ void fill_pp(double* r, int la, int lb, double ca, double cb, double aa, double ab,

@@ -94,17 +94,28 @@ __device__ __forceinline__ void md_zero(FT* dst, int N) {
 // lives at dst[j*N + i].  Moment m += exp(-mu R^2) * (w mono_m); the partial
 // sums of a row are folded into (hi, lo) with TwoSum at the end of the row.
 // --------------------------------------------------------------------------
+__device__ __forceinline__ float lds32(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+
 template <int LA, int LB>
 __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, float* dst, int N) {
-    constexpr int NM = (LA + 1) * (LB + 1), R16 = rec_words16_f32(LA, LB);
+    constexpr int NM = (LA + 1) * (LB + 1), NV = md_nv(LA, LB), NP = (NV + 1) / 2, R16 = rec_words16_f32(LA, LB);
     if (n == 0) {
         md_zero<LA, LB, float>(dst, N);
         return;
     }
-    float hi[NM], lo[NM], part[NM];
+    // moment sums in slot order: hi + lo per slot, and the current row's partial
+    // sums as pairs (slots 2i, 2i+1; for odd NV the last pair's second half is unused)
+    float hi[NV], lo[NV];
+    float2 part[NP];
 #pragma unroll
-    for (int m = 0; m < NM; ++m) hi[m] = lo[m] = part[m] = 0.f;
-    const int rowlen = (int)lds128(rec).z;
+    for (int j = 0; j < NV; ++j) hi[j] = lo[j] = 0.f;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) part[i] = make_float2(0.f, 0.f);
+    const int rowlen = (int)lds32(rec + 4u * (NV + 2));
     for (int q0 = 0; q0 < n; q0 += rowlen) {
         for (int q = q0; q < q0 + rowlen; ++q) {
             float r[4 * R16];
@@ -116,41 +127,44 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, f
                 r[4 * w + 2] = v.z;
                 r[4 * w + 3] = v.w;
             }
-            // exp(-mu R^2) = 2^-(mu2 R^2), argument in double-float (mu2 = r0 + r1):
+            // exp(-mu R^2) = 2^-(mu2 R^2), argument in double-float (mu2 = hi + lo):
             // 2^-(xh + xl) = 2^-xh (1 - ln2 xl) to first order in |xl| < 2^-20 xh
-            const float xh = r[0] * g.R2;
-            const float xl = fmaf(r[0], g.R2, -xh) + fmaf(r[1], g.R2, r[0] * g.R2lo);
+            const float m0 = r[NV], m1 = r[NV + 1];
+            const float xh = m0 * g.R2;
+            const float xl = fmaf(m0, g.R2, -xh) + fmaf(m1, g.R2, m0 * g.R2lo);
             const float e = ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f);
-            int j = 0;
+            const float2 ee = make_float2(e, e);
 #pragma unroll
-            for (int al = 0; al <= LA; ++al)
-#pragma unroll
-                for (int be = 0; be <= LB; ++be)
-                    if (MdTab<LA, LB>::used(al, be)) {
-                        part[al * (LB + 1) + be] = fmaf(e, r[3 + j], part[al * (LB + 1) + be]);
-                        ++j;
-                    }
+            for (int i = 0; i < NP; ++i) part[i] = __ffma2_rn(ee, make_float2(r[2 * i], r[2 * i + 1]), part[i]);
         }
         if (q0 == 0) {  // the first row opens the sums exactly
 #pragma unroll
-            for (int m = 0; m < NM; ++m) {
-                hi[m] = part[m];
-                part[m] = 0.f;
-            }
+            for (int j = 0; j < NV; ++j) hi[j] = (j & 1) ? part[j / 2].y : part[j / 2].x;
         } else {
 #pragma unroll
-            for (int m = 0; m < NM; ++m) {
+            for (int j = 0; j < NV; ++j) {
                 float s, e;
-                two_sum(hi[m], part[m], s, e);
-                hi[m] = s;
-                lo[m] += e;
-                part[m] = 0.f;
+                two_sum(hi[j], (j & 1) ? part[j / 2].y : part[j / 2].x, s, e);
+                hi[j] = s;
+                lo[j] += e;
             }
         }
-    }
 #pragma unroll
-    for (int m = 0; m < NM; ++m) hi[m] += lo[m];
-    md_transform<LA, LB, float>(hi, g.AB, dst, N);
+        for (int i = 0; i < NP; ++i) part[i] = make_float2(0.f, 0.f);
+    }
+    float M[NM];
+    int j = 0;
+#pragma unroll
+    for (int al = 0; al <= LA; ++al)
+#pragma unroll
+        for (int be = 0; be <= LB; ++be) {
+            M[al * (LB + 1) + be] = 0.f;
+            if (MdTab<LA, LB>::used(al, be)) {
+                M[al * (LB + 1) + be] = hi[j] + lo[j];
+                ++j;
+            }
+        }
+    md_transform<LA, LB, float>(M, g.AB, dst, N);
 }
 
 // FP64 variant: plain double accumulation, records from shared memory.
