@@ -307,14 +307,17 @@ __device__ __noinline__ Sums4<FT> pb_unit(const PbParams<FT>& P, PbWarpSmem<FT>&
     float2 S01[NV];  // FP32: (S0, S1) of the used slots as pairs, one paired FMA per slot
 #pragma unroll
     for (int j = 0; j < NV; ++j) S01[j] = make_float2(0.f, 0.f);
+    // each lane's batch element of the next 32, loaded one round ahead
+    int bnext = e0 + lane < e1 ? P.perm[e0 + lane] : 0;
     for (int c0 = e0; c0 < e1; c0 += 32) {
         // phase A: lane = element; cotangent moments of its block
         {
             const int e = c0 + lane;
+            const int b = bnext;
+            if (c0 + 32 + lane < e1) bnext = P.perm[c0 + 32 + lane];
             FT G[NM];
             FT R2 = FT(0), R2lo = FT(0);
             if (e < e1) {
-                const int b = P.perm[e];
                 Geo<FT> geo;
                 load_geo(geo, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
                 const FT* gs = P.dS + (size_t)b * P.N * P.N + (size_t)P.boff[sb] * P.N + P.boff[sa];
