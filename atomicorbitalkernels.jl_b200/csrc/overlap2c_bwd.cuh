@@ -31,7 +31,7 @@
 //   valB   nzb x na pairs (listed zero ket slots): dcoef of the ket slot
 //
 // Record-parallel evaluation.  A work unit is (species pair, shell pair, chunk
-// of 4 tiles = 128 batch elements, group of <= 32 records).  For each 32 batch
+// of 8 tiles = 256 batch elements, group of <= 32 records).  For each 32 batch
 // elements the warp first puts lane = element and computes the cotangent
 // moments G_m(b) (md2c.cuh) into shared memory; then lane = record and the
 // warp loops over the elements accumulating
@@ -206,7 +206,7 @@ __device__ __forceinline__ void md_dual(const FT (&G)[(LA + 1) * (LB + 1)], FT r
 }
 
 constexpr int kPbWarps = 8;        // warps per pullback CTA
-constexpr int kPbChunkTiles = 4;   // tiles (of 32 batch elements) per work unit
+constexpr int kPbChunkTiles = 8;   // tiles (of 32 batch elements) per work unit
 
 template <typename FT>
 __device__ __forceinline__ FT warp_sum_from(FT v, int first) {
