@@ -361,6 +361,35 @@ def main():
     err32 = float(np.linalg.norm(S32 - ref32) / np.linalg.norm(ref32))
     err64 = float(np.linalg.norm(S64 - ref64) / np.linalg.norm(ref64))
 
+    def _elem_errs(X, R):
+        """max |X - R| and max |X - R| / |R| over elements with |R| > 1e-12 max |R|."""
+        d = np.abs(X - R)
+        big = np.abs(R) > 1e-12 * np.abs(R).max()
+        return {"max_abs": float(d.max()), "max_rel": float((d[big] / np.abs(R[big])).max())}
+
+    err_detail = {"f32c": _elem_errs(S32, ref32), "f64": _elem_errs(S64, ref64)}
+    # useful integrals: blocks whose two shells are both present in the pair's species
+    present = basis.nprim > 0  # (ns, NZ)
+    nbf_sh = (basis.ls + 1) * (basis.ls + 2) // 2
+    useful = 0
+    sa0, sb0 = np.asarray(pairs.sidxA) - 1, np.asarray(pairs.sidxB) - 1
+    for ga in range(NZ):
+        for gb in range(NZ):
+            cnt = int(np.count_nonzero((sa0 == ga) & (sb0 == gb)))
+            if cnt:
+                na = int((nbf_sh * present[:, ga]).sum())
+                nb = int((nbf_sh * present[:, gb]).sum())
+                useful += cnt * na * nb
+    useful_frac = useful / float(N * N * B)
+
+    # ---- FMA-pipe peaks of this GPU (denominators for the compute-bound kernels' pipe use) ----
+    pipe_peaks = {"method": "aok_measure_fma_peak: independent FMA chains, 8 blocks x 256 threads per SM"}
+    for name, prec, paired in (("fp32_tflops", _lib.AOK_PREC_F32C, 0), ("fp32_paired_tflops", _lib.AOK_PREC_F32C, 1),
+                               ("fp64_tflops", _lib.AOK_PREC_F64, 0)):
+        v = ctypes.c_double()
+        _lib.check(L.aok_measure_fma_peak(prec, paired, ctypes.byref(v), _dev.stream()))
+        pipe_peaks[name] = allmax(v.value)
+
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -443,7 +472,11 @@ def main():
             "fp64": {"value": value64, "ms_per_step": ms64, "kernel_ms": kms64, "launch_shape": c64["shape"]},
             "ms_per_step_params_per_call": ms32p,
             "f32c_over_f64": value / value64,
-            "rel_err": {"f32c_vs_oracle": err32, "f64_vs_oracle": err64, "sample_pairs": nchk},
+            "rel_err": {"f32c_vs_oracle": err32, "f64_vs_oracle": err64, "sample_pairs": nchk,
+                        "elementwise": err_detail},
+            "pipe_peaks": pipe_peaks,
+            "useful_integrals_per_s": value * useful_frac,
+            "useful_integral_fraction": useful_frac,
             "grad_step": grad, "other_configs": extra,
             "roofline": roof, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
             "gpu_launches": 3 * args.steps,

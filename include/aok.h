@@ -76,6 +76,12 @@ int aok_plan_check(aok_plan* plan, void* stream);
  * summed kernel time and the number of timed launches, then resets. */
 int aok_plan_timing_enable(aok_plan* plan, int capacity);
 int aok_plan_timing_read(aok_plan* plan, double* total_ms, int64_t* launches);
+/* Measurement aid (no reference counterpart): the FMA-pipe throughput of the
+ * current GPU in TFLOP/s, FP32 (precision AOK_PREC_F32C; paired != 0 uses the
+ * paired FP32 FMA) or FP64, from a kernel of independent FMA chains on every SM
+ * timed with CUDA events on `stream` (synchronises it).  The denominator for
+ * the pipe use of compute-bound kernels. */
+int aok_measure_fma_peak(int precision, int paired, double* tflops, void* stream);
 
 /*
  * coef = D / sqrt(normsq) per shell and species on the device.
