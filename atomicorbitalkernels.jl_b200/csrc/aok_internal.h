@@ -61,6 +61,7 @@ struct aok_plan {
     void* d_pp3 = nullptr;
     int* d_npp3 = nullptr;
     void* d_items3 = nullptr;
+    void* d_order3 = nullptr;        // per call: each panel's items, heaviest first (k_order3c)
     int nitems3 = 0;
     alignas(8) unsigned char panels3_raw[528] = {};
     size_t slab_stride3 = 0;

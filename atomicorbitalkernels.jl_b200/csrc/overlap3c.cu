@@ -3,6 +3,7 @@
 // overlap3c_kernel.cuh (one instantiation per precision: overlap3c_f32.cu,
 // overlap3c_f64.cu).
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "overlap3c_kernel.cuh"
@@ -66,6 +67,44 @@ __global__ void k_prep3c(typename PTT<FT>::type* __restrict__ pp, int* __restric
         n += __popc(m);
     }
     if (lane == 0) npp[q] = n;
+}
+
+// Per call, one CTA per panel: the panel's items sorted by estimated cost,
+// heaviest first, so that the warps' dynamic queue ends with cheap items (the
+// panel's barrier then waits less for its slowest warp).  Cost = primitive
+// triples x (E tables + the chunk's products) + a fixed part per item; the f-shell
+// classes (run-time loops, FP64 tables) count four times.  Rank sort in shared
+// memory; panels of more than kOrder3Max items keep the static order.
+constexpr int kOrder3Max = 2048;
+
+__global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, const Item3* __restrict__ items,
+                                                 const int* __restrict__ npp, Panels3 panels, int ns) {
+    __shared__ unsigned long long key[kOrder3Max];
+    const int pn = blockIdx.x;
+    const int i0 = panels.item0[pn], n = panels.item0[pn + 1] - i0;
+    if (n > kOrder3Max) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) order[i0 + i] = items[i0 + i];
+        return;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const Item3 it = items[i0 + i];
+        const bool f = it.cls >= kClsF3;
+        const int c = f ? it.cls - kClsF3 : it.cls;
+        const int la = f ? c >> 4 : c / 9, lb = f ? (c >> 2) & 3 : (c / 3) % 3, lc = f ? c & 3 : c % 3;
+        const int ppc = pages_per_chunk3(la, lb);
+        const int pages = min(ppc, ncart(lc) - it.chunk * ppc);
+        const long long per = 12LL * (la + 1) * (lb + 1) * (lc + 1) + 2LL * ncart(la) * ncart(lb) * pages;
+        long long cost = (long long)npp[(it.sa * ns + it.sb) * ns + it.sc] * per * (f ? 4 : 1) + 64;
+        cost = min(cost, (long long)0x7FFFFFFF);
+        key[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | (unsigned)i;  // ascending key = descending cost
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned long long ki = key[i];
+        int r = 0;
+        for (int j = 0; j < n; ++j) r += key[j] < ki;
+        order[i0 + r] = items[i0 + i];
+    }
 }
 
 int setup_overlap3c_schedule(aok_plan* p) {
@@ -146,6 +185,8 @@ int setup_overlap3c_schedule(aok_plan* p) {
     cudaError_t e;
     if ((e = cudaMalloc(&p->d_items3, sizeof(Item3) * items.size())) != cudaSuccess)
         return cuda_status(e, "cudaMalloc(items3)");
+    if ((e = cudaMalloc(&p->d_order3, sizeof(Item3) * items.size())) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(order3)");
     if ((e = cudaMemcpy(p->d_items3, items.data(), sizeof(Item3) * items.size(), cudaMemcpyHostToDevice)) !=
         cudaSuccess)
         return cuda_status(e, "cudaMemcpy(items3)");
@@ -167,6 +208,10 @@ int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB,
                                           (const float*)p->d_gb_coef, (int)p->ns, (int)p->K);
     int st = cuda_status(cudaGetLastError(), "k_prep3c");
     if (st != AOK_OK) return st;
+    Panels3 pan;
+    memcpy(&pan, p->panels3_raw, sizeof(Panels3));
+    k_order3c<<<pan.n, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, pan, (int)p->ns);
+    if ((st = cuda_status(cudaGetLastError(), "k_order3c")) != AOK_OK) return st;
     if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, s);
     return launch_ov3_f32(p, out, posA, posB, posC, s);
 }

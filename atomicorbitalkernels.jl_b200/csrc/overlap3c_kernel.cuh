@@ -56,7 +56,7 @@ template <> struct PTT<float> { using type = PTf; };
 template <> struct PTT<double> { using type = PTd; };
 
 struct Item3 {
-    int16_t cls;    // la*9 + lb*3 + lc
+    int16_t cls;    // la*9 + lb*3 + lc, or kClsF3 + la*16 + lb*4 + lc with an f shell
     int16_t chunk;
     int16_t sa, sb, sc, pad;
 };
@@ -509,7 +509,7 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.tiles = p->d_tiles;
     P.ntiles = p->d_ntiles;
     P.counter = p->d_counter;
-    P.items = (const Item3*)p->d_items3;
+    P.items = (const Item3*)p->d_order3;
     memcpy(&P.panels, p->panels3_raw, sizeof(Panels3));
     P.ns = (int)p->ns;
     P.K = (int)p->K;
