@@ -193,6 +193,7 @@ def main():
                     choices=["overlap2c", "evaluate", "overlap3c", "pullback", "grad", "outputbound"],
                     help="with --profile: which kernel family to run (ncu captures)")
     ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
+    ap.add_argument("--fp64", action="store_true", help="with --profile: run the FP64 kernels (overlap2c, overlap3c)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -285,7 +286,7 @@ def main():
         return allmax(ms), allmax(kms)
 
     if args.profile and args.workload not in ("overlap2c", "grad"):
-        fn = side_workload(args.workload, L, _dev, _lib, aok, torch, args.batch)
+        fn = side_workload(args.workload, L, _dev, _lib, aok, torch, args.batch, torch.float64 if args.fp64 else None)
         for _ in range(args.warmup + args.steps):
             fn()
         torch.cuda.synchronize()
@@ -300,8 +301,9 @@ def main():
         torch.cuda.synchronize()
         return 0
     if args.profile:
+        cp = setup(torch.float64) if args.fp64 else c32
         for _ in range(args.warmup + args.steps):
-            step(c32)
+            step(cp)
         torch.cuda.synchronize()
         return 0
     sampler = ClockSampler(local)
@@ -596,7 +598,7 @@ def _outputbound_setup(aok, _dev, _lib, torch, L, B, FT):
                 shape={"ctas_per_sm": int(ch[0]), "stage_bytes": int(ch[1])})
 
 
-def side_workload(name, L, _dev, _lib, aok, torch, B=None):
+def side_workload(name, L, _dev, _lib, aok, torch, B=None, FT=None):
     """One launch chain of a side workload, for ncu captures (--profile --workload ...)."""
     if name == "outputbound":
         d = _outputbound_setup(aok, _dev, _lib, torch, L, B or B_PER_RANK, torch.float32)
@@ -614,7 +616,7 @@ def side_workload(name, L, _dev, _lib, aok, torch, B=None):
                                                           _dev.ptr(d["dD"]), _dev.ptr(d["dPin"]), _dev.ptr(d["X"]),
                                                           ctypes.c_void_p(d["sidx"].data_ptr()), _dev.ptr(d["z"]),
                                                           _dev.ptr(d["D"]), d["nX"], 1.0, _dev.stream()))
-    d = _overlap3c_setup(aok, _dev, _lib, torch, L, 4096, torch.float32)
+    d = _overlap3c_setup(aok, _dev, _lib, torch, L, 4096, FT or torch.float32)
     return lambda: _lib.check(L.aok_overlap3c_gb(d["plan"].h, _dev.ptr(d["out"]), ctypes.c_void_p(d["nprim"].data_ptr()),
                                                  ctypes.c_void_p(d["off"].data_ptr()),
                                                  ctypes.c_void_p(d["coef"].data_ptr()),
