@@ -74,8 +74,10 @@ __global__ void k_gb_pad(FT* __restrict__ zeta, FT* __restrict__ coef, const int
 // --------------------------------------------------------------------------
 // Primitive-pair records.
 // --------------------------------------------------------------------------
-// w rb^al ra^be q^ga for the class's moment slots, in slot order.
-__device__ __forceinline__ int fill_monos(double* wm, int la, int lb, double w, double ra, double rb, double q) {
+// w rb^al ra^be q^ga for the class's moment slots, in slot order, written as
+// out[j] (converted to FT) as they are formed; returns the slot count.
+template <typename FT>
+__device__ __forceinline__ int fill_monos(FT* out, int la, int lb, double w, double ra, double rb, double q) {
     int j = 0;
     for (int al = 0; al <= la; ++al)
         for (int be = 0; be <= lb; ++be) {
@@ -84,7 +86,7 @@ __device__ __forceinline__ int fill_monos(double* wm, int la, int lb, double w, 
             for (int k = 0; k < al; ++k) v *= rb;
             for (int k = 0; k < be; ++k) v *= ra;
             for (int k = 0; k < (la + lb - al - be) / 2; ++k) v *= q;
-            wm[j++] = v;
+            out[j++] = (FT)v;
         }
     return j;
 }
@@ -95,9 +97,7 @@ __device__ __forceinline__ void fill_pp(float* r, int la, int lb, double ca, dou
     const double x = kPi * ip;
     const double log2e = 1.4426950408889634074;
     const double mu2 = ((aa * ab) * ip) * log2e;  // exponent in base 2
-    double wm[8];
-    const int nv = fill_monos(wm, la, lb, ca * cb * (x * sqrt(x)), aa * ip, ab * ip, 0.5 * ip);
-    for (int j = 0; j < nv; ++j) r[j] = (float)wm[j];
+    const int nv = fill_monos(r, la, lb, ca * cb * (x * sqrt(x)), aa * ip, ab * ip, 0.5 * ip);
     r[nv] = (float)mu2;
     r[nv + 1] = (float)(mu2 - (double)r[nv]);
     r[nv + 2] = (float)rowlen;
@@ -107,11 +107,9 @@ __device__ __forceinline__ void fill_pp(double* r, int la, int lb, double ca, do
                                         int rowlen) {
     const double p = aa + ab;
     const double x = kPi / p;
-    double wm[8];
-    const int nv = fill_monos(wm, la, lb, ca * cb * (x * sqrt(x)), aa / p, ab / p, 0.5 / p);
+    const int nv = fill_monos(r + 2, la, lb, ca * cb * (x * sqrt(x)), aa / p, ab / p, 0.5 / p);
     r[0] = aa * ab / p;
     r[1] = (double)rowlen;
-    for (int j = 0; j < nv; ++j) r[2 + j] = wm[j];
     for (int j = 2 + nv; j < 2 * rec_words16_f64(la, lb); ++j) r[j] = 0.0;
 }
 template <typename FT> __host__ __device__ constexpr int rec_words16(int la, int lb);
