@@ -135,6 +135,17 @@ int aok_plan_autotune(aok_plan* plan, void* out, const void* zeta, const void* c
  * sidxA, sidxB (B) 1-based.  Zero-coefficient primitive pairs are skipped.
  * zeta = coef = NULL uses the parameters fixed by aok_plan_set_basis.
  */
+/*
+ * Species labels -> 1-based species indices on the device.  Replaces the host
+ * lookup _cgto_species_index / _cgto_sidx (src/integrals/orbital/overlap_2c.jl:148-158):
+ * sidx[i] = first k + 1 with zlist[k] == label[i].  label, sidx: device int64 (n);
+ * zlist: host int64 (the plan's NZ labels in basis order).  A label not in the
+ * list gets 0 and sets the plan's error word (AOK_ERR_SPECIES from
+ * aok_plan_check), as the 2C entry points do for an index outside 1..NZ.
+ */
+int aok_species_index(aok_plan* plan, int64_t* sidx, const int64_t* label, int64_t n,
+                      const int64_t* zlist, void* stream);
+
 int aok_overlap2c(aok_plan* plan, void* out, const void* zeta, const void* coef,
                   const void* posA, const void* posB, const int64_t* sidxA,
                   const int64_t* sidxB, int64_t B, double lengthscale, void* stream);

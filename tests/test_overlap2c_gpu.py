@@ -169,3 +169,30 @@ def test_repeat_calls_deterministic():
     S1 = aok.batch_overlap(cob, XA, XB, FT=torch.float32)
     S2 = aok.batch_overlap(cob, XA, XB, FT=torch.float32)
     assert torch.equal(S1, S2)
+
+
+def test_species_index_on_device():
+    """aok_species_index: labels -> 1-based species indices on the device (the reference's
+    _cgto_species_index lookup); an unknown label yields 0 and the species error."""
+    import ctypes
+    from aok_b200 import _dev, _lib
+    L = _lib.load()
+    zlist = np.array([8, 1, 6, 29], dtype=np.int64)
+    plan = _dev.Plan((0, 1), 1, len(zlist), _dev.prec_of(torch.float64), 16)
+    rng = np.random.default_rng(31)
+    labels = zlist[rng.integers(0, len(zlist), 5000)]
+    lab = torch.as_tensor(labels).cuda()
+    out = torch.full((len(labels),), -7, dtype=torch.int64, device="cuda")
+    zl = (ctypes.c_int64 * len(zlist))(*zlist.tolist())
+    _lib.check(L.aok_species_index(plan.h, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(lab.data_ptr()),
+                                   len(labels), zl, _dev.stream()))
+    _lib.check(L.aok_plan_check(plan.h, _dev.stream()))
+    expect = np.array([int(np.flatnonzero(zlist == z)[0]) + 1 for z in labels])
+    assert np.array_equal(out.cpu().numpy(), expect)
+    bad = torch.as_tensor(np.array([8, 2, 1], dtype=np.int64)).cuda()
+    out2 = torch.empty(3, dtype=torch.int64, device="cuda")
+    _lib.check(L.aok_species_index(plan.h, ctypes.c_void_p(out2.data_ptr()), ctypes.c_void_p(bad.data_ptr()), 3, zl,
+                                   _dev.stream()))
+    with pytest.raises(aok.AOKError):
+        _lib.check(L.aok_plan_check(plan.h, _dev.stream()))
+    assert out2.cpu().tolist() == [1, 0, 2]
