@@ -100,8 +100,41 @@ __device__ __forceinline__ float lds32(uint32_t a) {
     return v;
 }
 
+// One primitive pair (n == 1): the moments are the record's slot values times
+// its exponential; no loop and no compensation are needed.
 template <int LA, int LB>
-__device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, float* dst, int N) {
+__device__ __forceinline__ void run_item1_body(uint32_t rec, const Geo<float> g, float* dst, int N) {
+    constexpr int NM = (LA + 1) * (LB + 1), NV = md_nv(LA, LB), R16 = rec_words16_f32(LA, LB);
+    float r[4 * R16];
+#pragma unroll
+    for (int w = 0; w < R16; ++w) {
+        const float4 v = lds128(rec + 16u * w);
+        r[4 * w] = v.x;
+        r[4 * w + 1] = v.y;
+        r[4 * w + 2] = v.z;
+        r[4 * w + 3] = v.w;
+    }
+    const float m0 = r[NV], m1 = r[NV + 1];
+    const float xh = m0 * g.R2;
+    const float xl = fmaf(m0, g.R2, -xh) + fmaf(m1, g.R2, m0 * g.R2lo);
+    const float e = ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f);
+    float M[NM];
+    int j = 0;
+#pragma unroll
+    for (int al = 0; al <= LA; ++al)
+#pragma unroll
+        for (int be = 0; be <= LB; ++be) {
+            M[al * (LB + 1) + be] = 0.f;
+            if (MdTab<LA, LB>::used(al, be)) {
+                M[al * (LB + 1) + be] = e * r[j];
+                ++j;
+            }
+        }
+    md_transform<LA, LB, float>(M, g.AB, dst, N);
+}
+
+template <int LA, int LB>
+__device__ __forceinline__ void run_item_body(uint32_t rec, int n, const Geo<float> g, float* dst, int N) {
     constexpr int NM = (LA + 1) * (LB + 1), NV = md_nv(LA, LB), NP = (NV + 1) / 2, R16 = rec_words16_f32(LA, LB);
     if (n == 0) {
         md_zero<LA, LB, float>(dst, N);
@@ -169,7 +202,7 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<float> g, f
 
 // FP64 variant: plain double accumulation, records from shared memory.
 template <int LA, int LB>
-__device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<double> g, double* dst, int N) {
+__device__ __forceinline__ void run_item_body(uint32_t rec, int n, const Geo<double> g, double* dst, int N) {
     constexpr int NM = (LA + 1) * (LB + 1), R16 = rec_words16_f64(LA, LB);
     if (n == 0) {
         md_zero<LA, LB, double>(dst, N);
@@ -200,11 +233,40 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<double> g, 
     md_transform<LA, LB, double>(mom, g.AB, dst, N);
 }
 
+template <int LA, int LB, typename FT>
+__device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<FT> g, FT* dst, int N) {
+    run_item_body<LA, LB>(rec, n, g, dst, N);
+}
+
+// Classes with l <= 1 on both sides run inline, and in FP32C an item of one
+// primitive pair takes the loop-free routine: for these few-output blocks a call
+// and the loop cost more than the arithmetic.  The other classes run as calls
+// (one copy of each class's code, so the kernel keeps its register budget and
+// the instruction cache holds the loop).
+template <int LA, int LB>
+__device__ __forceinline__ void run_class(uint32_t rec, int n, const Geo<float>& g, float* dst, int N) {
+    if constexpr (LA <= 1 && LB <= 1) {
+        if (n == 1)
+            run_item1_body<LA, LB>(rec, g, dst, N);
+        else
+            run_item_body<LA, LB>(rec, n, g, dst, N);
+    } else {
+        run_item<LA, LB, float>(rec, n, g, dst, N);
+    }
+}
+template <int LA, int LB>
+__device__ __forceinline__ void run_class(uint32_t rec, int n, const Geo<double>& g, double* dst, int N) {
+    if constexpr (LA <= 1 && LB <= 1)
+        run_item_body<LA, LB>(rec, n, g, dst, N);
+    else
+        run_item<LA, LB, double>(rec, n, g, dst, N);
+}
+
 template <typename FT>
 __device__ __forceinline__ void dispatch(int cls, uint32_t pp, int n, const Geo<FT>& g, FT* dst, int N) {
     switch (cls) {
 #define AOK_CASE(LA, LB) \
-    case (LA) * 4 + (LB): run_item<LA, LB>(pp, n, g, dst, N); break;
+    case (LA) * 4 + (LB): run_class<LA, LB>(pp, n, g, dst, N); break;
         AOK_CASE(0, 0) AOK_CASE(0, 1) AOK_CASE(0, 2) AOK_CASE(0, 3)
         AOK_CASE(1, 0) AOK_CASE(1, 1) AOK_CASE(1, 2) AOK_CASE(1, 3)
         AOK_CASE(2, 0) AOK_CASE(2, 1) AOK_CASE(2, 2) AOK_CASE(2, 3)

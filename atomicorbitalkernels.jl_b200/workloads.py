@@ -143,6 +143,21 @@ def outputbound_basis(seed=1005, nspecies=4):
     return _assemble(per, 1)
 
 
+def outputbound_sp_basis(seed=1006, nspecies=4):
+    """The low-l output-bound classes alone: 3-5 s and 2-3 p shells per species, one
+    primitive per shell (classes s-s, s-p, p-s, p-p; nbf_total 14)."""
+    rng = _rng(seed)
+    per = []
+    ranges = {0: (3, 5), 1: (2, 3)}
+    for _ in range(nspecies):
+        sp = {}
+        for l, (lo, hi) in ranges.items():
+            n = int(rng.integers(lo, hi + 1))
+            sp[l] = [_draw_shell(rng, l, 1) for _ in range(n)]
+        per.append(sp)
+    return _assemble(per, 1)
+
+
 @dataclass
 class PairBatch:
     posA: np.ndarray        # (3,B) Bohr

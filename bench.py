@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 METRIC = "2c-overlap integrals/s + (ζ,D) grad step, FP32-comp vs FP64, 1 B200, rel err"
 UNIT = "integrals/s"
 B_PER_RANK = 65536
+B_SP = 262144  # the s/p output-bound batch: 14^2 x 4 B x B = 205 MB of FP32 output (> L2)
 SEED = 1002
 
 
@@ -190,7 +191,7 @@ def main():
                     help="only the FP32C forward steps (for ncu launch lists / captures); prints no JSON")
     ap.add_argument("--batch", type=int, default=B_PER_RANK, help="pairs per rank")
     ap.add_argument("--workload", default="overlap2c",
-                    choices=["overlap2c", "evaluate", "overlap3c", "pullback", "grad", "outputbound"],
+                    choices=["overlap2c", "evaluate", "overlap3c", "pullback", "grad", "outputbound", "outputbound_sp"],
                     help="with --profile: which kernel family to run (ncu captures)")
     ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
     ap.add_argument("--fp64", action="store_true", help="with --profile: run the FP64 kernels (overlap2c, overlap3c)")
@@ -575,9 +576,10 @@ def _overlap3c_setup(aok, _dev, _lib, torch, L, B, FT):
     return d
 
 
-def _outputbound_setup(aok, _dev, _lib, torch, L, B, FT):
-    """The output-bound 2C case: config-2 shell structure, one primitive per shell."""
-    ob = aok.workloads.outputbound_basis()
+def _outputbound_setup(aok, _dev, _lib, torch, L, B, FT, basis=None):
+    """The output-bound 2C case: config-2 shell structure, one primitive per shell (or
+    the given basis, e.g. its s and p shells alone)."""
+    ob = basis if basis is not None else aok.workloads.outputbound_basis()
     obp = aok.workloads.ragged_pairs(B, ob.NZ, SEED + 1)
     Nob = ob.nbf_total
     pl = _dev.Plan(ob.ls, ob.K, ob.NZ, _dev.prec_of(FT), obp.B)
@@ -601,7 +603,12 @@ def _outputbound_setup(aok, _dev, _lib, torch, L, B, FT):
 def side_workload(name, L, _dev, _lib, aok, torch, B=None, FT=None):
     """One launch chain of a side workload, for ncu captures (--profile --workload ...)."""
     if name == "outputbound":
-        d = _outputbound_setup(aok, _dev, _lib, torch, L, B or B_PER_RANK, torch.float32)
+        d = _outputbound_setup(aok, _dev, _lib, torch, L, B or B_PER_RANK, FT or torch.float32)
+        side_workload.keep = d
+        return d["fn"]
+    if name == "outputbound_sp":
+        d = _outputbound_setup(aok, _dev, _lib, torch, L, B or B_SP, FT or torch.float32,
+                               aok.workloads.outputbound_sp_basis())
         side_workload.keep = d
         return d["fn"]
     if name in ("evaluate", "pullback"):
@@ -643,24 +650,31 @@ def side_measurements(args, L, _dev, _lib, aok, torch, oracle, allmax, peaks):
     out = {}
     n = max(5, min(200, args.steps // 10))
     # output-bound 2C: the config-2 shell structure with one primitive per shell
-    res = {}
-    for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
-        d = _outputbound_setup(aok, _dev, _lib, torch, L, B_PER_RANK, FT)
-        pl, fn, Nob, obB = d["plan"], d["fn"], d["N"], d["B"]
-        for _ in range(args.warmup):
-            fn()
-        torch.cuda.synchronize()
-        _lib.check(L.aok_plan_timing_enable(pl.h, n))
-        ms = _time(fn, n, 0, torch, allmax)
-        tot, cnt = ctypes.c_double(), ctypes.c_int64()
-        _lib.check(L.aok_plan_timing_read(pl.h, ctypes.byref(tot), ctypes.byref(cnt)))
-        kms = tot.value / max(cnt.value, 1)
-        fsz = 4 if FT == torch.float32 else 8
-        alg = obB * (Nob * Nob * fsz + 2 * (3 * fsz + 8))
-        res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obB / (ms * 1e-3), "shape": d["shape"],
-                    "kernel_hbm_gbs": alg / (kms * 1e-3) / 1e9, "kernel_hbm_frac": alg / (kms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
-        del pl, d
-    out["outputbound_2c_K1_B65536"] = dict(res, nbf=Nob, note="config-2 shell structure, one primitive per shell")
+    # and its low-l classes alone (s and p shells, one primitive each), at a batch whose
+    # output is larger than L2
+    for key, basis, Bo, note in (
+            ("outputbound_2c_K1_B65536", None, B_PER_RANK, "config-2 shell structure, one primitive per shell"),
+            ("outputbound_2c_sp_K1_B262144", aok.workloads.outputbound_sp_basis(), B_SP,
+             "low-l classes alone: 3-5 s and 2-3 p shells per species, one primitive per shell")):
+        res = {}
+        for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
+            d = _outputbound_setup(aok, _dev, _lib, torch, L, Bo, FT, basis)
+            pl, fn, Nob, obB = d["plan"], d["fn"], d["N"], d["B"]
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            _lib.check(L.aok_plan_timing_enable(pl.h, n))
+            ms = _time(fn, n, 0, torch, allmax)
+            tot, cnt = ctypes.c_double(), ctypes.c_int64()
+            _lib.check(L.aok_plan_timing_read(pl.h, ctypes.byref(tot), ctypes.byref(cnt)))
+            kms = tot.value / max(cnt.value, 1)
+            fsz = 4 if FT == torch.float32 else 8
+            alg = obB * (Nob * Nob * fsz + 2 * (3 * fsz + 8))
+            res[tag] = {"ms": ms, "kernel_ms": kms, "integrals_per_s": Nob * Nob * obB / (ms * 1e-3),
+                        "shape": d["shape"], "kernel_hbm_gbs": alg / (kms * 1e-3) / 1e9,
+                        "kernel_hbm_frac": alg / (kms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+            del pl, d
+        out[key] = dict(res, nbf=Nob, batch=Bo, note=note)
     # config 1
     res = {}
     for FT, tag in ((torch.float32, "f32c"), (torch.float64, "f64")):
