@@ -200,6 +200,33 @@ __device__ __forceinline__ void run_item_body(uint32_t rec, int n, const Geo<flo
     md_transform<LA, LB, float>(M, g.AB, dst, N);
 }
 
+// FP64, one primitive pair: no loop.
+template <int LA, int LB>
+__device__ __forceinline__ void run_item1_body(uint32_t rec, const Geo<double> g, double* dst, int N) {
+    constexpr int NM = (LA + 1) * (LB + 1), R16 = rec_words16_f64(LA, LB);
+    double r[2 * R16];
+#pragma unroll
+    for (int w = 0; w < R16; ++w) {
+        const double2 v = lds128d(rec + 16u * w);
+        r[2 * w] = v.x;
+        r[2 * w + 1] = v.y;
+    }
+    const double e = exp(-r[0] * g.R2);
+    double mom[NM];
+    int j = 0;
+#pragma unroll
+    for (int al = 0; al <= LA; ++al)
+#pragma unroll
+        for (int be = 0; be <= LB; ++be) {
+            mom[al * (LB + 1) + be] = 0.0;
+            if (MdTab<LA, LB>::used(al, be)) {
+                mom[al * (LB + 1) + be] = e * r[2 + j];
+                ++j;
+            }
+        }
+    md_transform<LA, LB, double>(mom, g.AB, dst, N);
+}
+
 // FP64 variant: plain double accumulation, records from shared memory.
 template <int LA, int LB>
 __device__ __forceinline__ void run_item_body(uint32_t rec, int n, const Geo<double> g, double* dst, int N) {
@@ -238,7 +265,7 @@ __device__ __noinline__ void run_item(uint32_t rec, int n, const Geo<FT> g, FT* 
     run_item_body<LA, LB>(rec, n, g, dst, N);
 }
 
-// Classes with l <= 1 on both sides run inline, and in FP32C an item of one
+// Classes with l <= 1 on both sides run inline, and an item of one
 // primitive pair takes the loop-free routine: for these few-output blocks a call
 // and the loop cost more than the arithmetic.  The other classes run as calls
 // (one copy of each class's code, so the kernel keeps its register budget and
@@ -256,10 +283,14 @@ __device__ __forceinline__ void run_class(uint32_t rec, int n, const Geo<float>&
 }
 template <int LA, int LB>
 __device__ __forceinline__ void run_class(uint32_t rec, int n, const Geo<double>& g, double* dst, int N) {
-    if constexpr (LA <= 1 && LB <= 1)
-        run_item_body<LA, LB>(rec, n, g, dst, N);
-    else
+    if constexpr (LA <= 1 && LB <= 1) {
+        if (n == 1)
+            run_item1_body<LA, LB>(rec, g, dst, N);
+        else
+            run_item_body<LA, LB>(rec, n, g, dst, N);
+    } else {
         run_item<LA, LB, double>(rec, n, g, dst, N);
+    }
 }
 
 template <typename FT>
