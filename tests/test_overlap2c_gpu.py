@@ -73,6 +73,17 @@ def test_config2_ragged_species(FT, tol):
     assert rel_fro(S, ref) < tol
 
 
+@pytest.mark.parametrize("FT,tol", [(torch.float64, TOL64), (torch.float32, TOL32)])
+@pytest.mark.parametrize("which", ["outputbound", "outputbound_sp"])
+def test_one_primitive_bases(which, FT, tol):
+    """Bases of one primitive per shell: every item takes the loop-free path (inline
+    for l <= 1 classes); the s/p basis has only l <= 1 classes."""
+    b = W.outputbound_basis() if which == "outputbound" else W.outputbound_sp_basis()
+    pr = W.ragged_pairs(2500, b.NZ, 29)
+    S, ref, _, _ = _orb_case(b, pr, FT)
+    assert rel_fro(S, ref) < tol
+
+
 def test_self_overlap_diagonal_positive_s_shells():
     b = W.config0_basis()
     pr = W.config0_pairs(B=8)
