@@ -38,14 +38,6 @@ B_SP = 262144  # the s/p output-bound batch: 14^2 x 4 B x B = 205 MB of FP32 out
 SEED = 1002
 
 
-def _baseline_metric():
-    try:
-        with open(os.path.join(ROOT, "BASELINE.json")) as f:
-            return json.load(f).get("metric", METRIC)
-    except Exception:
-        return METRIC
-
-
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -164,7 +156,7 @@ def run_reference(args):
     dt = (time.perf_counter() - t0) / args.steps
     val = N * N * per_step / dt
     line = {
-        "impl": "reference", "metric": _baseline_metric(), "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "ragged 4-species l<=3 2C overlap, FP64 CPU oracle (C restatement of the "
@@ -462,7 +454,7 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": _baseline_metric(), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32c", "data": "synthetic",
             "config": {"workload": "ragged 4-species l<=3 2C overlap (config 2), FP32-compensated forward; "
