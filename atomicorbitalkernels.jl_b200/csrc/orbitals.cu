@@ -894,6 +894,19 @@ int aok_orbitals_destroy(aok_orbitals* o) {
     return AOK_OK;
 }
 
+int aok_orbitals_check(aok_orbitals* o, void* stream) {
+    if (!o) return set_error(AOK_ERR_INVALID, "aok_orbitals_check: null plan");
+    int st = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "cudaStreamSynchronize");
+    if (st != AOK_OK) return st;
+    int h = 0;
+    if ((st = cuda_status(cudaMemcpy(&h, o->d_err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(err)")))
+        return st;
+    if ((st = cuda_status(cudaMemset(o->d_err, 0, sizeof(int)), "cudaMemset(err)"))) return st;
+    if (h == AOK_ERR_SPECIES) return set_error(h, "species index outside 1..NZ");
+    if (h != 0) return set_error(h, "device-side validation failed");
+    return AOK_OK;
+}
+
 int aok_evaluate(aok_orbitals* o, void* P, const void* X, const int64_t* sidx, const void* zeta, const void* D,
                  int64_t nX, double lengthscale, void* stream) {
     if (!o) return set_error(AOK_ERR_INVALID, "aok_evaluate: null plan");

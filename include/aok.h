@@ -236,6 +236,17 @@ int aok_orbitals_create(aok_orbitals** orb, int64_t nRad, int64_t K, int64_t NZ,
                         const int64_t* poly, int64_t nOrb, const int64_t* iR,
                         const int64_t* iY, int64_t L, int radial_kind, int precision);
 int aok_orbitals_destroy(aok_orbitals* orb);
+/* Synchronises `stream`, then reports (and clears) the orbitals' device error
+ * word: AOK_ERR_SPECIES if aok_evaluate or aok_evaluate_ed met a species index
+ * outside 1..NZ, or aok_evaluate_pullback did with NZ > 1.  No memory outside
+ * the arguments is touched for such a point, but its outputs are not
+ * meaningful: the forward evaluates it as species 1; the pullback leaves it
+ * out of the (zeta, D) gradient (with NZ = 1 it counts as species 1, as every
+ * point does) and may leave its dX unwritten.  The device half of the
+ * reference's unknown-species error (_cgto_species_index,
+ * src/integrals/orbital/overlap_2c.jl:148-158) for callers that pass device
+ * species indices unchecked. */
+int aok_orbitals_check(aok_orbitals* orb, void* stream);
 
 /*
  * P (nX,nOrb) = R_{iR} * Z_{iY} at positions X (3,nX) times lengthscale.

@@ -121,3 +121,53 @@ def test_absent_species_zero_param_gradient():
                                  aok.initialparameters(orb), aok.initialstates(orb))
     assert np.all(g["Rnl"]["zeta"].cpu().numpy()[:, :, 2] == 0)
     assert np.all(g["Rnl"]["D"].cpu().numpy()[:, :, 2] == 0)
+
+
+def test_orbitals_check_reports_bad_device_species():
+    """Species indices handed to the C ABI unchecked: an index outside 1..NZ is
+    reported once by aok_orbitals_check (then cleared); the (zeta, D) gradient
+    leaves those points out, the other points' values are unaffected."""
+    import ctypes
+
+    from aok_b200 import _dev, _lib
+    FT = torch.float64
+    b, orb = _basis()
+    nX = 3000
+    X, sidx = W.config1_points(nX=nX, seed=7)
+    plan = _dev.OrbPlan(b.zeta.shape[0], b.K, b.NZ, orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L,
+                        orb.Rnl.kind, _dev.prec_of(FT))
+    L = _lib.load()
+    z, D = _dev.to_colmajor(b.zeta, FT), _dev.to_colmajor(b.D, FT)
+    dPin = np.random.default_rng(8).standard_normal((nX, len(orb)))
+
+    def run(Xh, sh):
+        n = Xh.shape[1]
+        Xd, sd = _dev.to_colmajor(Xh, FT), torch.as_tensor(np.ascontiguousarray(sh)).cuda()
+        P = _dev.colmajor_empty((n, len(orb)), FT)
+        dP = _dev.colmajor_empty((3, n, len(orb)), FT)
+        dz = _dev.colmajor_empty(b.zeta.shape, FT)
+        dD = _dev.colmajor_empty(b.zeta.shape, FT)
+        dPd = _dev.to_colmajor(dPin[:n] if n == nX else np.delete(dPin, bad_at, axis=0), FT)
+        sp = ctypes.c_void_p(sd.data_ptr())
+        _lib.check(L.aok_evaluate_ed(plan.h, _dev.ptr(P), _dev.ptr(dP), _dev.ptr(Xd), sp, _dev.ptr(z), _dev.ptr(D),
+                                     n, 1.0, _dev.stream()))
+        _lib.check(L.aok_evaluate_pullback(plan.h, None, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dPd), _dev.ptr(Xd),
+                                           sp, _dev.ptr(z), _dev.ptr(D), n, 1.0, _dev.stream()))
+        return P.cpu().numpy(), dz.cpu().numpy(), dD.cpu().numpy(), L.aok_orbitals_check(plan.h, _dev.stream())
+
+    bad_at = [3, 10, 2999]
+    P0, _, _, st = run(X, sidx)
+    assert st == 0
+    bad = sidx.copy()
+    bad[bad_at] = [0, b.NZ + 1, -5]
+    P1, dz1, dD1, st = run(X, bad)
+    assert st == _lib.AOK_ERR_SPECIES
+    assert b"species" in L.aok_last_error()
+    assert L.aok_orbitals_check(plan.h, _dev.stream()) == 0  # the error word was cleared
+    keep = np.ones(nX, bool)
+    keep[bad_at] = False
+    assert np.array_equal(P1[keep], P0[keep])
+    # the gradient with the bad points equals the gradient without them
+    _, dz2, dD2, st = run(np.asfortranarray(X[:, keep]), sidx[keep])
+    assert st == 0
+    assert rel_fro(dz1, dz2) < 1e-12 and rel_fro(dD1, dD2) < 1e-12
