@@ -1,0 +1,87 @@
+"""The reference's known-answer tests, run through the GPU kernels instead of the
+oracle: the closed-form s/s overlap (test/integrals/test_reference.jl:10-20, here
+also at separated centres by the Gaussian product theorem), the p-shell transpose
+symmetry (test_reference.jl:24-41), and the analytic single-atom overlap of the
+evaluated orbitals (test/orbitals/test_gaussianbasis.jl:50-66), integrated by
+quadrature over the GPU evaluate."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import aok_b200 as aok
+from helpers import to_np
+
+W = aok.workloads
+pytestmark = pytest.mark.gpu
+
+
+def _gb_basis(shells):
+    return aok.compile_basis([aok.CartesianShell(l, np.asarray(c, float), np.asarray(e, float)) for l, c, e in shells])
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-13), (torch.float32, 1e-6)])
+def test_ss_closed_form(FT, tol):
+    """<s_a|s_b> of unit-coefficient primitives = (pi/p)^{3/2} exp(-a b/p |A-B|^2), p = a + b."""
+    a, b = 1.3, 0.7
+    bc = _gb_basis([(0, [1.0], [a]), (0, [1.0], [b])])
+    d = np.array([0.0, 0.3, 0.9, 1.7, 2.6])
+    A = np.zeros((3, len(d)))
+    B = np.stack([d * 0.6, d * 0.0, d * 0.8])  # |A - B| = d
+    S = to_np(aok.batch_overlap(bc, aok.Length(A, "bohr"), aok.Length(B, "bohr"), FT=FT))
+    p = a + b
+    expect = (math.pi / p) ** 1.5 * np.exp(-a * b / p * d ** 2)
+    assert np.max(np.abs(S[0, 1, :] - expect) / expect) < tol
+    assert np.max(np.abs(S[1, 0, :] - expect) / expect) < tol
+    # rows are functions on A, columns on B: S[0, 0] = <s_a(A)|s_a(B)>
+    expect_aa = (math.pi / (2 * a)) ** 1.5 * np.exp(-a / 2 * d ** 2)
+    assert np.max(np.abs(S[0, 0, :] - expect_aa) / expect_aa) < tol
+
+
+def test_p_shell_transpose_symmetry():
+    """S(A, B) restricted to (p on A, p on B) is the transpose of S(B, A)'s."""
+    bc = _gb_basis([(1, [0.7, 0.3], [1.2, 0.4]), (1, [0.7, 0.3], [1.2, 0.4])])
+    rng = np.random.default_rng(41)
+    A = rng.standard_normal((3, 64))
+    B = A + rng.standard_normal((3, 64))
+    SAB = to_np(aok.batch_overlap(bc, aok.Length(A, "bohr"), aok.Length(B, "bohr")))
+    SBA = to_np(aok.batch_overlap(bc, aok.Length(B, "bohr"), aok.Length(A, "bohr")))
+    blkAB = SAB[:3, 3:, :]
+    blkBA = SBA[:3, 3:, :]
+    assert np.max(np.abs(blkAB - blkBA.transpose(1, 0, 2))) < 1e-14
+    assert np.max(np.abs(blkAB)) > 1e-3  # the blocks are not trivially zero
+
+
+def test_analytic_single_atom_overlap_of_evaluated_orbitals():
+    """Quadrature of <phi_i|phi_j> over the GPU evaluate (FP64) equals the analytic
+    single-atom overlap: delta_{l l'} delta_{m m'} Gamma(l + 3/2)/2 sum_ac D_a D_c (z_a + z_c)^{-(l + 3/2)}."""
+    b = W.config0_basis()
+    orb = aok.orbitals_from_species_basis(b)
+    # radial Gauss-Legendre on [0, 12] Bohr x a product rule on the sphere
+    rr, wr = np.polynomial.legendre.leggauss(160)
+    rr, wr = 6.0 * (rr + 1.0), 6.0 * wr
+    ct, wt = np.polynomial.legendre.leggauss(12)
+    ph = np.arange(24) * 2 * math.pi / 24
+    dirs = np.array([[math.sqrt(1 - c * c) * math.cos(q), math.sqrt(1 - c * c) * math.sin(q), c]
+                     for c in ct for q in ph]).T
+    wa = np.array([wc * 2 * math.pi / 24 for wc in wt for _ in ph])
+    X = np.asfortranarray((dirs[:, None, :] * rr[None, :, None]).reshape(3, -1))
+    w = (wr[:, None] * rr[:, None] ** 2 * wa[None, :]).reshape(-1)
+    P = to_np(aok.evaluate(orb, X))
+    Snum = (P * w[:, None]).T @ P
+    nb = len(orb.radidx)
+    San = np.zeros((nb, nb))
+    for i in range(nb):
+        for j in range(nb):
+            yi, yj = int(orb.ylmidx[i]) - 1, int(orb.ylmidx[j]) - 1
+            if yi != yj:
+                continue
+            l = math.isqrt(yi)
+            ki, kj = int(orb.radidx[i]) - 1, int(orb.radidx[j]) - 1
+            g = 0.5 * math.gamma(l + 1.5)
+            acc = sum(b.D[ki, a, 0] * b.D[kj, c, 0] * (b.zeta[ki, a, 0] + b.zeta[kj, c, 0]) ** (-(l + 1.5))
+                      for a in range(b.K) for c in range(b.K))
+            San[i, j] = g * acc
+    assert np.max(np.abs(Snum - San)) < 1e-8
+    assert np.allclose(np.diag(San), 1.0, atol=1e-12)
