@@ -85,3 +85,37 @@ def test_analytic_single_atom_overlap_of_evaluated_orbitals():
             San[i, j] = g * acc
     assert np.max(np.abs(Snum - San)) < 1e-8
     assert np.allclose(np.diag(San), 1.0, atol=1e-12)
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-13), (torch.float32, 1e-5)])
+def test_sss_closed_form_3c(FT, tol):
+    """<s_a(A) s_b(B) s_c(C)> of unit-coefficient primitives =
+    (pi/q)^{3/2} exp(-(a b |A-B|^2 + a c |A-C|^2 + b c |B-C|^2)/q), q = a + b + c."""
+    a, b, c = 1.3, 0.7, 0.45
+    bc = _gb_basis([(0, [1.0], [a]), (0, [1.0], [b]), (0, [1.0], [c])])
+    rng = np.random.default_rng(43)
+    A, B, C = (0.5 * rng.standard_normal((3, 40)) for _ in range(3))
+    V = to_np(aok.batch_overlap_3c(bc, aok.Length(A, "bohr"), aok.Length(B, "bohr"), aok.Length(C, "bohr"), FT=FT))
+    d2 = lambda U, Y: np.sum((U - Y) ** 2, axis=0)
+
+    def closed(x, y, z):  # exponents x on A, y on B, z on C
+        q = x + y + z
+        return (math.pi / q) ** 1.5 * np.exp(-(x * y * d2(A, B) + x * z * d2(A, C) + y * z * d2(B, C)) / q)
+
+    for (i, j, k), ex in (((0, 1, 2), (a, b, c)), ((2, 0, 1), (c, a, b)), ((1, 1, 0), (b, b, a))):
+        expect = closed(*ex)
+        assert np.max(np.abs(V[i, j, k, :] - expect) / expect) < tol
+
+
+def test_3c_centre_swap_symmetry():
+    """V(A, B, C)[i, j, k] = V(B, A, C)[j, i, k] for contracted s and p shells.  Only for
+    l <= 1: from l = 2 on, the reference's block layout strides a shell's components by
+    2l + 1 rather than its Cartesian count (kernels_3c.jl:134-156), which is not a
+    transpose under a centre swap."""
+    bc = _gb_basis([(0, [0.6, 0.4], [2.1, 0.5]), (1, [1.0], [0.9]), (1, [0.8, 0.2], [1.4, 0.35])])
+    rng = np.random.default_rng(44)
+    A, B, C = (0.7 * rng.standard_normal((3, 32)) for _ in range(3))
+    L = lambda x: aok.Length(x, "bohr")
+    V1 = to_np(aok.batch_overlap_3c(bc, L(A), L(B), L(C)))
+    V2 = to_np(aok.batch_overlap_3c(bc, L(B), L(A), L(C)))
+    assert np.max(np.abs(V1 - V2.transpose(1, 0, 2, 3))) < 1e-13 * np.max(np.abs(V1))
