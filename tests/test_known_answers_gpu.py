@@ -119,3 +119,30 @@ def test_3c_centre_swap_symmetry():
     V1 = to_np(aok.batch_overlap_3c(bc, L(A), L(B), L(C)))
     V2 = to_np(aok.batch_overlap_3c(bc, L(B), L(A), L(C)))
     assert np.max(np.abs(V1 - V2.transpose(1, 0, 2, 3))) < 1e-13 * np.max(np.abs(V1))
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-13), (torch.float32, 2e-6)])
+def test_unit_self_overlap_of_normalised_s_p_shells(FT, tol):
+    """_compile_coef normalises every shell (cartesian_gto_basis.jl:74-120), so at
+    coincident centres with equal species each s and p component of the species-aware
+    2C overlap has <phi|phi> = 1 (4 species, ragged shells; absent shells skipped)."""
+    b = W.config2_basis()
+    cob = aok.compile_basis(aok.orbitals_from_species_basis(b), dtype=FT)
+    rng = np.random.default_rng(3)
+    B = 64
+    pos = rng.standard_normal((3, B))
+    lab = [int(b.zlist[i % b.NZ]) for i in range(B)]
+    S = to_np(aok.batch_overlap(cob, aok.PStates(pos, lab), aok.PStates(pos, lab), FT=FT))
+    ls = np.asarray(b.ls)
+    nbf = (ls + 1) * (ls + 2) // 2
+    off = np.concatenate([[0], np.cumsum(nbf)])
+    checked = 0
+    for e in range(B):
+        sg = e % b.NZ
+        for k, l in enumerate(ls):
+            if l > 1 or not np.any(b.D[k, :, sg] != 0):
+                continue
+            d = np.array([S[off[k] + c, off[k] + c, e] for c in range(nbf[k])])
+            assert np.max(np.abs(d - 1.0)) < tol
+            checked += nbf[k]
+    assert checked > 100
