@@ -112,3 +112,36 @@ def test_product_path_fails_loudly_without_gpu():
     orb = aok.orbitals_from_species_basis(b)
     with pytest.raises(aok.AOKError):
         aok.compile_basis(orb)
+
+
+def test_orbital_entry_points_reject_bad_arguments_without_gpu():
+    """Host-side argument checks of aok_orbitals_check and aok_evaluate_pullback_noalloc:
+    each case fails before any CUDA call, so no device memory is touched."""
+    L = _lib.load()
+    assert L.aok_orbitals_check(None, None) == _lib.AOK_ERR_INVALID
+    b = aok.workloads.config1_basis()
+    orb = aok.orbitals_from_species_basis(b)
+    nRad, K, NZ = b.zeta.shape
+    iR, iY = np.asarray(orb.radidx), np.asarray(orb.ylmidx)
+    fake = ctypes.c_void_p(256)  # never dereferenced: every call below is refused on the host
+
+    def call(nRad=nRad, iR=iR, iY=iY, Lh=orb.L, prec=_lib.AOK_PREC_F64, nX=1000, dzeta=fake, dD=fake):
+        return L.aok_evaluate_pullback_noalloc(
+            nRad, K, NZ, _lib.int64_array(np.zeros(nRad, np.int64)), len(iR), _lib.int64_array(iR),
+            _lib.int64_array(iY), Lh, orb.Rnl.kind, prec, fake, dzeta, dD, fake, fake, fake, fake, fake, nX, 1.0,
+            None)
+
+    assert call(nRad=65) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"64 radials" in L.aok_last_error()
+    bad = iR.copy()
+    bad[0] = 0
+    assert call(iR=bad) == _lib.AOK_ERR_INVALID
+    assert b"index map" in L.aok_last_error()
+    bad = iY.copy()
+    bad[-1] = (orb.L + 1) ** 2 + 1
+    assert call(iY=bad) == _lib.AOK_ERR_INVALID
+    assert call(Lh=5) == _lib.AOK_ERR_UNSUPPORTED
+    assert call(prec=7) == _lib.AOK_ERR_INVALID
+    assert call(dD=None) == _lib.AOK_ERR_INVALID
+    assert call(nX=1 << 21) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"scratch" in L.aok_last_error()
