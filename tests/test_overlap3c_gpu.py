@@ -126,3 +126,37 @@ def test_3c_rejects_g_shells_and_plain_positions():
     bc2 = aok.compile_basis([aok.CartesianShell(0, np.array([1.0]), np.array([1.0]))])
     with pytest.raises(aok.ArgumentError):
         aok.batch_overlap_3c(bc2, np.zeros((3, 1)), p, p)
+
+
+def _sized_basis(extra_s):
+    """f, 2 d, 2 p and 1 + extra_s s shells (contracted and not): N = 29 + extra_s."""
+    shells = [(3, [0.7, 0.3], [1.1, 0.35]), (2, [1.0], [0.8]), (2, [0.6, 0.4], [1.6, 0.5]), (1, [1.0], [0.9]),
+              (1, [0.5, 0.5], [2.0, 0.6]), (0, [1.0], [1.2])] + [(0, [1.0], [0.4 + 0.3 * i]) for i in range(extra_s)]
+    ls = np.array([s[0] for s in shells])
+    nprim = np.array([len(s[1]) for s in shells])
+    coef = np.concatenate([np.asarray(s[1], float) for s in shells])
+    z = np.concatenate([np.asarray(s[2], float) for s in shells])
+    bc = aok.compile_basis([aok.CartesianShell(l, np.asarray(c, float), np.asarray(e, float)) for l, c, e in shells])
+    return bc, ls, nprim, coef, z
+
+
+def test_largest_page_f64_and_the_limit():
+    """One FP64 output page of 32 batch elements (N^2 doubles each) must fit the 220 KB
+    slab: N = 29 is the largest basis and matches the oracle; N = 30 is refused with
+    AOK_ERR_UNSUPPORTED, while FP32C still takes it (its limit is N = 41)."""
+    tr = W.config4_triples(B=40, seed=1013)
+    pA, pB, pC = _L(tr.posA), _L(tr.posB), _L(tr.posC)
+    bc, ls, nprim, coef, z = _sized_basis(0)
+    assert bc.nbf_total == 29
+    V = aok.batch_overlap_3c(bc, pA, pB, pC)
+    ref = oracle.overlap3c_gb(ls, nprim, coef, z, aok.to_bohr(pA), aok.to_bohr(pB), aok.to_bohr(pC), nthreads=8)
+    assert rel_fro(V, ref) < 1e-12
+    bc, ls, nprim, coef, z = _sized_basis(1)
+    assert bc.nbf_total == 30
+    with pytest.raises(aok.AOKError, match="page"):
+        aok.batch_overlap_3c(bc, pA, pB, pC)
+    V = aok.batch_overlap_3c(bc, pA, pB, pC, FT=torch.float32)
+    ref = oracle.overlap3c_gb(ls, nprim, f32_round(coef), f32_round(z), f32_round(aok.to_bohr(pA, np.float32)),
+                              f32_round(aok.to_bohr(pB, np.float32)), f32_round(aok.to_bohr(pC, np.float32)),
+                              nthreads=8)
+    assert rel_fro(V, ref) < 2e-6
