@@ -45,6 +45,17 @@ def test_plan_create_rejects_bad_arguments_without_gpu():
     assert L.aok_plan_create(ctypes.byref(h), 0, ls, 2, 1, 0, 16) == _lib.AOK_ERR_INVALID
     assert L.aok_plan_create(ctypes.byref(h), 1, ls, 2, 1, 7, 16) == _lib.AOK_ERR_INVALID
     assert L.aok_overlap2c(None, None, None, None, None, None, None, None, 4, 1.0, None) == _lib.AOK_ERR_INVALID
+    # the plan's limits: 64 shells, 16 species, 128 primitive slots, batches below 2^31
+    many = _lib.int64_array([0] * 65)
+    assert L.aok_plan_create(ctypes.byref(h), 65, many, 2, 1, 0, 16) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"64 shells" in L.aok_last_error()
+    assert L.aok_plan_create(ctypes.byref(h), 1, ls, 2, 17, 0, 16) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"16 species" in L.aok_last_error()
+    assert L.aok_plan_create(ctypes.byref(h), 1, ls, 129, 1, 0, 16) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"128 primitives" in L.aok_last_error()
+    assert L.aok_plan_create(ctypes.byref(h), 1, ls, 2, 1, 0, 1 << 31) == _lib.AOK_ERR_UNSUPPORTED
+    assert L.aok_plan_create(ctypes.byref(h), 1, ls, 2, 1, 0, -1) == _lib.AOK_ERR_INVALID
+    assert not h.value  # no plan was handed out
 
 
 def test_to_bohr_requires_units_and_converts():
