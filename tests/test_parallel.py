@@ -89,3 +89,43 @@ def test_sharded_gradient_equals_full_batch(tmp_path):
     dz, dD = oracle.overlap_pullback_ps(dS, b.ls, b.zeta, b.D, pr.sidxA, pr.sidxB, pr.posA, pr.posB)
     for a, ref in ((got["dz"], dz), (got["dD"], dD)):
         assert np.linalg.norm(a - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def _eval_problem():
+    b = W.config1_basis()
+    orb = aok.orbitals_from_species_basis(b)
+    X, sidx = W.config1_points(nX=301, seed=9)
+    dP = np.random.default_rng(4).standard_normal((301, len(orb)))
+    return b, orb, X, sidx, dP
+
+
+def _eval_rank(rank, world, port, out_path):
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        b, orb, X, sidx, dP = _eval_problem()
+        lo, hi = parallel.shard_bounds(X.shape[1], rank, world)
+
+        def pb(dP_local, basis, X_local, ps, st):  # the oracle stands in for the device pullback
+            Xl, sl = X_local
+            dz, dD = oracle.evaluate_pb(dP_local, Xl, sl, b.zeta, b.D, basis.Rnl.powers(), basis.radidx,
+                                        basis.ylmidx, basis.L)
+            return {"Rnl": {"zeta": torch.as_tensor(dz), "D": torch.as_tensor(dD)}, "Ylm": {}}
+
+        g = parallel.evaluate_pullback_ps(dP[lo:hi], orb, (np.asfortranarray(X[:, lo:hi]), sidx[lo:hi]), None, None,
+                                          pullback=pb)
+        np.savez(f"{out_path}.{rank}.npz", dz=g["Rnl"]["zeta"].numpy(), dD=g["Rnl"]["D"].numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_evaluate_gradient_equals_full_batch(tmp_path):
+    """Three ranks, uneven shards of 301 points: every rank ends with the full-batch
+    (zeta, D) gradient of the orbital evaluation."""
+    out = str(tmp_path / "e")
+    mp.spawn(_eval_rank, args=(3, _free_port(), out), nprocs=3, join=True)
+    b, orb, X, sidx, dP = _eval_problem()
+    dz, dD = oracle.evaluate_pb(dP, X, sidx, b.zeta, b.D, orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L)
+    for r in range(3):
+        got = np.load(f"{out}.{r}.npz")
+        for a, ref in ((got["dz"], dz), (got["dD"], dD)):
+            assert np.linalg.norm(a - ref) <= 1e-12 * np.linalg.norm(ref)
