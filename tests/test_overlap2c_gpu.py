@@ -207,3 +207,44 @@ def test_species_index_on_device():
     with pytest.raises(aok.AOKError):
         _lib.check(L.aok_plan_check(plan.h, _dev.stream()))
     assert out2.cpu().tolist() == [1, 0, 2]
+
+
+def test_plan_check_reports_bad_device_species_in_overlap():
+    """Species indices handed to aok_overlap2c unchecked (4 species): pairs with an
+    index outside 1..NZ are dropped by the species binning and reported once by
+    aok_plan_check; every other pair's block is the same as in a clean call."""
+    import ctypes
+
+    from aok_b200 import _dev, _lib
+    FT = torch.float64
+    b = W.config2_basis()
+    pr = W.config2_pairs(B=500)
+    N, ns, K, NZ = b.nbf_total, b.nshells, b.K, b.NZ
+    L = _lib.load()
+    plan = _dev.Plan(b.ls, K, NZ, _dev.prec_of(FT), pr.B)
+    zeta, D = _dev.to_colmajor(b.zeta, FT), _dev.to_colmajor(b.D, FT)
+    coef = _dev.colmajor_empty((ns, K, NZ), FT)
+    _lib.check(L.aok_compile_coef(plan.h, _dev.ptr(coef), _dev.ptr(zeta), _dev.ptr(D), _dev.stream()))
+    pA, pB = _dev.to_colmajor(pr.posA, FT), _dev.to_colmajor(pr.posB, FT)
+
+    def run(sA, sB):
+        dA, dB = torch.as_tensor(np.ascontiguousarray(sA)).cuda(), torch.as_tensor(np.ascontiguousarray(sB)).cuda()
+        out = _dev.colmajor_zeros((N, N, pr.B), FT)
+        _lib.check(L.aok_overlap2c(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(pA), _dev.ptr(pB),
+                                   ctypes.c_void_p(dA.data_ptr()), ctypes.c_void_p(dB.data_ptr()), pr.B, 1.0,
+                                   _dev.stream()))
+        return out.cpu().numpy(), L.aok_plan_check(plan.h, _dev.stream())
+
+    S0, st = run(pr.sidxA, pr.sidxB)
+    assert st == 0
+    bad_at = [0, 77, 499]
+    sA = np.array(pr.sidxA, dtype=np.int64)
+    sB = np.array(pr.sidxB, dtype=np.int64)
+    sA[bad_at[0]], sB[bad_at[1]], sA[bad_at[2]] = 0, NZ + 1, -3
+    S1, st = run(sA, sB)
+    assert st == _lib.AOK_ERR_SPECIES
+    assert b"species" in L.aok_last_error()
+    assert L.aok_plan_check(plan.h, _dev.stream()) == 0  # cleared
+    keep = np.ones(pr.B, bool)
+    keep[bad_at] = False
+    assert np.array_equal(S1[:, :, keep], S0[:, :, keep])
