@@ -7,7 +7,7 @@ Mirrors (names, fields, argument meaning, errors):
   AtomicOrbitals                                src/orbitals/atomicorbitals.jl:31-75
   CartesianGTOBasis / compile_basis(orb)        src/integrals/orbital/cartesian_gto_basis.jl:48-150
   gaussian_orbitals / slater_orbitals examples  src/orbitals/utils.jl:11-64
-  PState (position + species)                   DecoratedParticles, used as in overlap_2c.jl:283-308
+  PState (position + species)                   DecoratedParticles, used as in overlap_2c.jl:133-158
 
 Numeric work (the Cartesian normalisation coef = D / sqrt(normsq)) runs on the
 GPU through the C ABI; the host keeps only structure (shell momenta, offsets,
@@ -269,7 +269,7 @@ def as_pstates(X):
 
 
 def species_indices(zlist, species):
-    """1-based species indices via zlist (overlap_2c.jl:298-308); unknown labels raise."""
+    """1-based species indices via zlist (overlap_2c.jl:148-158); unknown labels raise."""
     lut = {z: i + 1 for i, z in enumerate(zlist)}
     out = np.empty(len(species), dtype=np.int64)
     for b, s in enumerate(species):
@@ -310,13 +310,13 @@ def _example_radial(cls, N1, N2, K=1, T=np.float64, zlist=(1,)):
 
 
 def gaussian_orbitals(N1=4, N2=3, *, length_unit, K=1, T=np.float64, nspecies=1, zlist=None):
-    """Deterministic example Gaussian-type orbital basis (orbitals/utils.jl:375-379)."""
+    """Deterministic example Gaussian-type orbital basis (src/orbitals/utils.jl:40-51)."""
     zlist = tuple(range(1, nspecies + 1)) if zlist is None else tuple(zlist)
     return AtomicOrbitals(_example_radial(GaussianTypeRadials, N1, N2, K, T, zlist), N1 - 1, length_unit)
 
 
 def slater_orbitals(N1=4, N2=3, *, length_unit, K=1, T=np.float64, nspecies=1, zlist=None):
-    """Deterministic example Slater-type orbital basis (orbitals/utils.jl:388-392)."""
+    """Deterministic example Slater-type orbital basis (src/orbitals/utils.jl:53-64)."""
     zlist = tuple(range(1, nspecies + 1)) if zlist is None else tuple(zlist)
     return AtomicOrbitals(_example_radial(SlaterTypeRadials, N1, N2, K, T, zlist), N1 - 1, length_unit)
 

@@ -17,7 +17,7 @@ constexpr int kMaxPairs = 256;     // species pairs (NZ <= 16)
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
 // Cartesian component c of a shell of momentum l, in the reference's order
-// (kernels_2c.jl:201-217): for x = l..0, for z = 0..l-x: (x, y = l-x-z, z).
+// (kernels_2c.jl:102-119): for x = l..0, for z = 0..l-x: (x, y = l-x-z, z).
 // Closed form (no loops, so unrolled call sites fold instantly): with
 // n = l - x, the first component of that x is n(n+1)/2, so
 // n = #{t >= 1 : t(t+1)/2 <= c} and z = c - n(n+1)/2.

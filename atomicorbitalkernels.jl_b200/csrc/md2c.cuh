@@ -3,7 +3,7 @@
 // With p = a + b, ra = a/p, rb = b/p, q = 1/(2p) and X = A_x - B_x, the
 // McMurchie-Davidson t = 0 coefficient of the 1-D overlap (the quantity the
 // reference builds recursively, Reference/ecoeffs.jl and
-// src/integrals/kernels_2c.jl:160-190) has the closed form obtained by
+// src/integrals/kernels_2c.jl:57-97) has the closed form obtained by
 // expanding x_A = x_P + PA, x_B = x_P + PB about the Gaussian product centre,
 // with PA = -rb X, PB = ra X and int x_P^n exp(-p x_P^2) = (n-1)!! q^{n/2}
 // sqrt(pi/p) for even n:

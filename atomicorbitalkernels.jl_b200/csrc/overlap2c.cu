@@ -1,7 +1,7 @@
 // overlap2c.cu -- batched 2-center Cartesian-Gaussian overlap, sm_100a.
 //
-// Replaces batch_S_orbital_kernel! (src/integrals/orbital/overlap_2c.jl:165-281)
-// and batch_S_kernel! (src/integrals/kernels_2c.jl:110-224).
+// Replaces batch_S_orbital_kernel! (src/integrals/orbital/overlap_2c.jl:15-131)
+// and batch_S_kernel! (src/integrals/kernels_2c.jl:11-125).
 //
 // Pipeline per call (all stream-ordered, no host synchronisation):
 //   k_pack2c    per species pair: the execution order of the shell pairs and
@@ -26,7 +26,7 @@
 //               is contiguous in the reference layout).
 //
 // The reference's l >= 2 stride aliasing (block element lin = c1 + (2la+1)*c2,
-// read back as blk[i + nbf_a*j], kernels_2c.jl:209-223) is reproduced at
+// read back as blk[i + nbf_a*j], kernels_2c.jl:99-124) is reproduced at
 // compile time in the term tables.
 //
 // FP32C precision: FP32 arithmetic on FP64-computed records; the Gaussian

@@ -1,8 +1,8 @@
 """Batched 2- and 3-center overlaps and their (zeta, D) pullback: the reference's
 public API (names, argument meaning, errors) over the CUDA library.
 
-  batch_overlap_ / batch_overlap (GaussianBasis path)   kernels_2c.jl:247-283
-  batch_overlap_ / batch_overlap (species-aware path)   orbital/overlap_2c.jl:321-385
+  batch_overlap_ / batch_overlap (GaussianBasis path)   kernels_2c.jl:148-184
+  batch_overlap_ / batch_overlap (species-aware path)   orbital/overlap_2c.jl:171-235
   batch_overlap(orb, XA, XB, ps, st) (Lux form)         orbital/overlap_2c_grad.jl:41-57
   batch_overlap_3c_ / batch_overlap_3c                  kernels_3c.jl:183-222
   pullback_ps(dS, orb, XA, XB, ps, st), rrule           orbital/overlap_2c_grad.jl:296-318

@@ -29,7 +29,7 @@ def _dfac(n):
 
 def spherical_selfoverlap(D, z, l):
     """Self-overlap of R(r) Z_lm with R = sum_k D_k exp(-z_k r^2) and L2 harmonics:
-    sum_ij D_i D_j * Gamma(l+3/2)/2 * (z_i+z_j)^-(l+3/2)  (test_gaussianbasis.jl:226-246)."""
+    sum_ij D_i D_j * Gamma(l+3/2)/2 * (z_i+z_j)^-(l+3/2)  (test_gaussianbasis.jl:46-66)."""
     g = 0.5 * _dfac(2 * l + 1) / 2.0 ** (l + 1) * math.sqrt(math.pi)
     zz = z[:, None] + z[None, :]
     return g * float(np.sum(D[:, None] * D[None, :] * zz ** (-(l + 1.5))))

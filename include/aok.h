@@ -49,9 +49,10 @@ extern "C" {
 typedef struct aok_plan aok_plan;        /* overlap plan (2C and 3C)          */
 typedef struct aok_orbitals aok_orbitals;/* orbital-evaluation plan           */
 
-/* Thread-local message for the last failing call on this thread. */
+/* Thread-local message for the last failing call on this thread (no reference
+ * counterpart: the Julia extension raises error(aok_last_error()) with it). */
 const char* aok_last_error(void);
-/* Library version string. */
+/* Library version string (no reference counterpart). */
 const char* aok_version(void);
 
 /*
@@ -65,10 +66,13 @@ const char* aok_version(void);
 int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t K,
                     int64_t NZ, int precision, int64_t max_batch);
 int aok_plan_destroy(aok_plan* plan);
-/* nbf_total of the plan's shell structure (reference: basis.nbf_total). */
+/* nbf_total of the plan's shell structure (basis.nbf_total,
+ * src/integrals/orbital/cartesian_gto_basis.jl:42). */
 int aok_plan_nbf(const aok_plan* plan, int64_t* nbf_total);
 /* Synchronises `stream`, then reports (and clears) the plan's device error
- * word: AOK_ERR_SPECIES if a kernel met a species index outside 1..NZ. */
+ * word: AOK_ERR_SPECIES if a kernel met a species index outside 1..NZ.  The
+ * device half of the unknown-species error of _cgto_species_index
+ * (src/integrals/orbital/overlap_2c.jl:148-154). */
 int aok_plan_check(aok_plan* plan, void* stream);
 /* Measurement aid (no reference counterpart): when enabled, every call
  * records a CUDA event pair around its dominant kernel (up to `capacity`
@@ -129,12 +133,15 @@ int aok_plan_autotune(aok_plan* plan, void* out, const void* zeta, const void* c
 /*
  * Batched 2-center overlap, species-aware Cartesian basis.
  * Replaces batch_S_orbital_kernel! + batch_overlap!(out, ::CartesianGTOBasis, XA, XB)
- * (src/integrals/orbital/overlap_2c.jl:165-281, 321-347).
+ * (src/integrals/orbital/overlap_2c.jl:15-131, 171-197).
  * out (N,N,B); zeta, coef (ns,K,NZ); posA, posB (3,B) in the basis's input
- * unit (multiplied by lengthscale on the device, overlap_2c.jl:331-333);
+ * unit (multiplied by lengthscale on the device, overlap_2c.jl:184-185);
  * sidxA, sidxB (B) 1-based.  Zero-coefficient primitive pairs are skipped.
  * zeta = coef = NULL uses the parameters fixed by aok_plan_set_basis.
  */
+int aok_overlap2c(aok_plan* plan, void* out, const void* zeta, const void* coef,
+                  const void* posA, const void* posB, const int64_t* sidxA,
+                  const int64_t* sidxB, int64_t B, double lengthscale, void* stream);
 /*
  * Species labels -> 1-based species indices on the device.  Replaces the host
  * lookup _cgto_species_index / _cgto_sidx (src/integrals/orbital/overlap_2c.jl:148-158):
@@ -146,14 +153,10 @@ int aok_plan_autotune(aok_plan* plan, void* out, const void* zeta, const void* c
 int aok_species_index(aok_plan* plan, int64_t* sidx, const int64_t* label, int64_t n,
                       const int64_t* zlist, void* stream);
 
-int aok_overlap2c(aok_plan* plan, void* out, const void* zeta, const void* coef,
-                  const void* posA, const void* posB, const int64_t* sidxA,
-                  const int64_t* sidxB, int64_t B, double lengthscale, void* stream);
-
 /*
  * Batched 2-center overlap, GaussianBasis path (NZ = 1 plan, K = max nprim).
  * Replaces batch_S_kernel! + batch_overlap!(out, ::CompiledBasis, posA, posB)
- * (src/integrals/kernels_2c.jl:110-262).  nprim (ns), prim_offset (ns+1):
+ * (src/integrals/kernels_2c.jl:11-163).  nprim (ns), prim_offset (ns+1):
  * device int64; coef, alpha: flat per-primitive (prim_offset[ns]); posA,
  * posB (3,B) already in Bohr (the reference's to_bohr runs on the host,
  * src/integrals/units.jl:28-35).

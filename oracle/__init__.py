@@ -79,7 +79,7 @@ def _nbf(ls):
 
 
 def overlap2c_gb(ls, nprim, coef, alpha, posA, posB, nthreads=1):
-    """batch_S_kernel! (kernels_2c.jl:110-224); positions (3,B) in Bohr."""
+    """batch_S_kernel! (kernels_2c.jl:11-125); positions (3,B) in Bohr."""
     ls, nprim = _i(ls), _i(nprim)
     off = _i(np.concatenate([[0], np.cumsum(nprim)]))
     posA, posB = _f(posA), _f(posB)
@@ -92,7 +92,7 @@ def overlap2c_gb(ls, nprim, coef, alpha, posA, posB, nthreads=1):
 
 
 def overlap2c_orb(ls, coef, zeta, sidxA, sidxB, posA, posB, lengthscale=1.0, nthreads=1):
-    """batch_S_orbital_kernel! (overlap_2c.jl:165-281); coef/zeta (ns,K,NZ)."""
+    """batch_S_orbital_kernel! (overlap_2c.jl:15-131); coef/zeta (ns,K,NZ)."""
     ls = _i(ls)
     coef, zeta = _f(coef), _f(zeta)
     ns, K, NZ = coef.shape

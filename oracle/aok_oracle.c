@@ -45,7 +45,7 @@ static int set_threads(int nthreads) {
 
 /* ------------------------------------------------------------------------ */
 /* McMurchie-Davidson 2-center E table, one axis.                            */
-/* Follows kernels_2c.jl:164-195 (same recursion in overlap_2c.jl:222-253    */
+/* Follows kernels_2c.jl:57-97 (same recursion in overlap_2c.jl:64-104      */
 /* and overlap_2c_grad.jl:132-166).  1-based indices as in the reference:    */
 /* E[t, i, j] with t in 1..TM, i in 1..IM, j in 1..JM.                        */
 /* ------------------------------------------------------------------------ */
@@ -82,7 +82,7 @@ static void md_E2(double* E, int TM, int IM, int la1, int lb1,
 
 /* One primitive pair accumulated into the aliased shell-pair block.
  * Contraction order and the N1 = 2*l_a+1 linear stride follow
- * kernels_2c.jl:198-218 (= overlap_2c.jl:256-275).                           */
+ * kernels_2c.jl:99-119 (= overlap_2c.jl:106-126).                           */
 static void contract2(double* blk, const double* Ex, const double* Ey, const double* Ez,
                       int TM, int IM, int la, int lb, double prefac) {
     const double* E;
@@ -153,7 +153,7 @@ static void s2_block(double* out, int64_t N, int64_t b,
             out[(row_off + i) + N * ((col_off + j) + N * b)] = blk[i + nbf_a * j];
 }
 
-/* batch_S_kernel! + batch_overlap! (kernels_2c.jl:110-262): GaussianBasis path.
+/* batch_S_kernel! + batch_overlap! (kernels_2c.jl:11-163): GaussianBasis path.
  * Positions are in Bohr (the Unitful conversion happens above this layer).  */
 int aokor_overlap2c_gb(double* out, int64_t ns, const int64_t* ls, const int64_t* nprim,
                        const int64_t* prim_off, const double* coef, const double* alpha,
@@ -186,9 +186,9 @@ int aokor_overlap2c_gb(double* out, int64_t ns, const int64_t* ls, const int64_t
     return 0;
 }
 
-/* batch_S_orbital_kernel! + batch_overlap! (overlap_2c.jl:165-347):
+/* batch_S_orbital_kernel! + batch_overlap! (overlap_2c.jl:15-131,171-197):
  * species-indexed padded primitives, zero-coef skip, 1-based sidx.
- * lengthscale multiplies positions as in overlap_2c.jl:331-333.             */
+ * lengthscale multiplies positions as in overlap_2c.jl:184-185.             */
 int aokor_overlap2c_orb(double* out, int64_t ns, int64_t K, int64_t NZ, const int64_t* ls,
                         const double* coef, const double* zeta,
                         const int64_t* sidxA, const int64_t* sidxB,

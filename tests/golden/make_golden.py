@@ -6,7 +6,7 @@ independently of the oracle's recursions, to pin the oracle.
   polynomial degrees involved), then placed into the reference's aliased
   block layout: component pair (c1, c2[, c3]) accumulates into the flat block
   index lin = c1 + (2la+1) c2 [+ (2la+1)(2lb+1) c3], read back with the
-  shell's own nbf strides (src/integrals/kernels_2c.jl:201-223,
+  shell's own nbf strides (src/integrals/kernels_2c.jl:99-124,
   src/integrals/kernels_3c.jl:134-161).  Component order: for x = l..0,
   for z = 0..l-x: (x, l-x-z, z).
 * Real solid harmonics Z_lm (l <= 3, index l^2+l+m) from their explicit

@@ -1,0 +1,134 @@
+"""Reference citations stay inside the cited files.
+
+Every `name.jl:N-M` (or `.md` / `.toml`) citation in the committed sources,
+headers and documents must name lines that exist in the reference
+(ACEsuit/AtomicOrbitalKernels.jl v0.0.4).  The line counts of the reference's
+files are recorded below, so the check runs without the reference; where the
+reference tree is present (AOK_REFERENCE_DIR, default the read-only copy this
+build studied), the table itself is checked against it.
+"""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# path within the reference -> number of lines
+REF_LINES = {
+    "AGENTS.md": 159,
+    "CLAUDE.md": 109,
+    "Project.toml": 43,
+    "README.md": 224,
+    "benchmark/Project.toml": 16,
+    "benchmark/benchmarks.jl": 72,
+    "ext/CUDAExt.jl/CUDA_PLAN.md": 258,
+    "scaling/Project.toml": 10,
+    "scaling/scaling.jl": 111,
+    "src/AtomicOrbitalKernels.jl": 83,
+    "src/integrals/adapt.jl": 25,
+    "src/integrals/compiled_basis.jl": 99,
+    "src/integrals/kernels_2c.jl": 185,
+    "src/integrals/kernels_3c.jl": 222,
+    "src/integrals/orbital/cartesian_gto_basis.jl": 150,
+    "src/integrals/orbital/overlap_2c.jl": 235,
+    "src/integrals/orbital/overlap_2c_grad.jl": 318,
+    "src/integrals/reference/Reference.jl": 24,
+    "src/integrals/reference/ecoeffs.jl": 83,
+    "src/integrals/reference/shell_pair.jl": 96,
+    "src/integrals/reference/shell_triple.jl": 108,
+    "src/integrals/units.jl": 38,
+    "src/orbitals/atomicorbitals.jl": 328,
+    "src/orbitals/gaussianbasis.jl": 114,
+    "src/orbitals/gtostoradials.jl": 270,
+    "src/orbitals/utils.jl": 64,
+    "src/utils.jl": 23,
+    "test/fixtures.jl": 29,
+    "test/integrals/test_compile.jl": 51,
+    "test/integrals/test_compile_orbitals.jl": 194,
+    "test/integrals/test_gpu.jl": 48,
+    "test/integrals/test_overlap_2c.jl": 85,
+    "test/integrals/test_overlap_2c_diff.jl": 137,
+    "test/integrals/test_overlap_3c.jl": 73,
+    "test/integrals/test_reference.jl": 41,
+    "test/integrals/test_units.jl": 23,
+    "test/orbitals/test_gaussianbasis.jl": 181,
+    "test/orbitals/test_gpu.jl": 98,
+    "test/orbitals/test_length_unit.jl": 67,
+    "test/orbitals/test_orbitals.jl": 180,
+    "test/runtests.jl": 84,
+    "test/utils_gpu.jl": 71,
+}
+
+# documents of this build that cite the reference but are not reference files themselves
+_SKIP_DOCS = ("SURVEY.md", "VERDICT.md", "ADVICE.md", "BASELINE.md", "BASELINE.json")
+_CITE = re.compile(r"((?:[\w.]+/)*[\w]+\.(?:jl|md|toml))((?::\d+(?:-\d+)?)(?:,\s*:?\d+(?:-\d+)?)*)")
+
+
+def _candidates(cited):
+    """Reference files a citation can mean: exact path suffix match on the cited path."""
+    return [p for p in REF_LINES if p == cited or p.endswith("/" + cited)]
+
+
+def _citations():
+    files = subprocess.check_output(["git", "ls-files"], cwd=ROOT, text=True).split()
+    files.append("tests/test_citations.py")
+    for f in sorted(set(files)):
+        if os.path.basename(f) in _SKIP_DOCS or f == "tests/test_citations.py":
+            continue
+        if not f.endswith((".py", ".c", ".h", ".cu", ".cuh", ".md", "Makefile")):
+            continue
+        try:
+            text = open(os.path.join(ROOT, f), errors="ignore").read()
+        except OSError:
+            continue
+        for ln, line in enumerate(text.splitlines(), 1):
+            for m in _CITE.finditer(line):
+                cited = m.group(1)
+                if not _candidates(cited):
+                    continue
+                ranges = [tuple(int(x) for x in r.split("-")) for r in re.findall(r"\d+(?:-\d+)?", m.group(2))]
+                yield f, ln, cited, ranges
+
+
+def test_every_citation_is_within_the_cited_file():
+    bad, n = [], 0
+    for f, ln, cited, ranges in _citations():
+        n += 1
+        top = max(REF_LINES[p] for p in _candidates(cited))
+        for r in ranges:
+            if r[0] < 1 or r[-1] > top or r[0] > r[-1]:
+                bad.append(f"{f}:{ln}: {cited}:{r} (file has {top} lines)")
+    assert n > 50, f"only {n} citations found: the scanner is broken"
+    assert not bad, "citations past the end of the reference file:\n" + "\n".join(bad)
+
+
+def test_header_cites_the_reference_for_every_entry_point():
+    """Each exported aok_* function in include/aok.h is preceded by a comment that either
+    cites a reference file:line or states that it has no reference counterpart."""
+    text = open(os.path.join(ROOT, "include", "aok.h")).read()
+    missing, names, comment = [], [], ""
+    # walk the header: a declaration belongs to the closest comment block above it
+    for tok in re.finditer(r"/\*.*?\*/|^(?:int|const char\*)\s+(aok_\w+)\s*\(", text, re.S | re.M):
+        if tok.group(0).startswith("/*"):
+            comment = tok.group(0)
+            continue
+        name = tok.group(1)
+        names.append(name)
+        c = " ".join(comment.replace("*", " ").split()).lower()
+        if not (re.search(r"\.jl:\d+", comment) or "no reference counterpart" in c
+                or "no counterpart in the reference" in c):
+            missing.append(name)
+    assert len(names) >= 25, f"only {len(names)} declarations found: the scanner is broken"
+    assert not missing, f"entry points without a reference citation: {missing}"
+
+
+_REF_DIR = os.environ.get("AOK_REFERENCE_DIR", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(_REF_DIR), reason="reference tree not present")
+def test_line_table_matches_the_reference_tree():
+    for rel, n in REF_LINES.items():
+        with open(os.path.join(_REF_DIR, rel), errors="ignore") as fh:
+            assert sum(1 for _ in fh) == n, rel

@@ -10,7 +10,7 @@ device results are checked by
   centres, on the s and p functions (FP64, <= 1e-12), and invariance of every entry
   under a common translation of all centres (FP64, <= 1e-12).  The swap holds only for
   l <= 1: the reference writes a shell pair's components into a block of stride 2l+1
-  (src/integrals/kernels_2c.jl:201-223, src/integrals/kernels_3c.jl:134-161), so
+  (src/integrals/kernels_2c.jl:99-124, src/integrals/kernels_3c.jl:134-161), so
   d and f blocks alias component pairs and are not transposes of each other;
 - additivity of the pullbacks over the batch: the gradient of the whole batch equals
   the sum of the gradients of its two halves (FP64, <= 1e-12), and the per-point dX of

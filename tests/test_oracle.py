@@ -5,9 +5,9 @@ reference's own tests and against independent computations:
   polynomials, see make_golden.py),
 * s/s closed form (test/integrals/test_reference.jl:10-20),
 * p-shell transpose symmetry (test_reference.jl:24-41),
-* analytic single-atom orbital overlap (test/orbitals/test_gaussianbasis.jl:226-246),
+* analytic single-atom orbital overlap (test/orbitals/test_gaussianbasis.jl:46-66),
 * central finite differences for every pullback,
-* absent species -> zero gradient (test/integrals/test_overlap_2c_diff.jl:241-247).
+* absent species -> zero gradient (test/integrals/test_overlap_2c_diff.jl:115-121).
 """
 import math
 import os
@@ -97,7 +97,7 @@ def test_harmonics_gradient_and_orthonormality():
 
 def test_analytic_single_atom_overlap():
     """Numerical quadrature of <phi_i|phi_j> from the oracle's evaluate equals the
-    analytic single-atom overlap of test_gaussianbasis.jl:226-246."""
+    analytic single-atom overlap of test_gaussianbasis.jl:46-66."""
     b = W.config0_basis()
     sp = W.orbital_spec(b.ls)
     # radial Gauss-Legendre on [0, 12] x angular product rule

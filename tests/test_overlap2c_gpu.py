@@ -90,7 +90,7 @@ def test_self_overlap_diagonal_positive_s_shells():
     pr.posB = pr.posA.copy()
     S, ref, _, _ = _orb_case(b, pr, torch.float64)
     assert rel_fro(S, ref) < TOL64
-    # normalised s shells have unit self-overlap (test_overlap_2c.jl:83-86 analogue)
+    # normalised s shells have unit self-overlap (test_overlap_2c.jl:42-45 analogue)
     s_idx = [0, 1, 2]
     assert np.allclose(S.numpy()[s_idx, s_idx, :], 1.0, atol=1e-12)
 
