@@ -15,6 +15,9 @@ the dominant kernel's roofline, an end-to-end number through the C ABI with
 host buffers, and the CPU oracle on the host cores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl aok|reference]
+
+With --gpus N > 1 and no torchrun environment (WORLD_SIZE unset), bench.py starts
+N ranks itself under torch.distributed.run on 127.0.0.1.
 """
 import argparse
 import ctypes
@@ -170,6 +173,78 @@ def run_reference(args):
     return 0
 
 
+def _free_port():
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def launch_ranks(args):
+    """bench.py --gpus N started without torchrun: start N ranks (one per GPU) on this
+    node under torch.distributed.run with the same arguments, and return its status.
+    Only rank 0 prints the JSON line."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(__file__)] + sys.argv[1:]
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "1"))
+    return subprocess.call(cmd, env=env)
+
+
+def run_dry(args):
+    """The multi-rank structure of a step without a GPU: each rank takes its own batch
+    (weak scaling), waits at the barriers of the timed region, reduces its time with a
+    max over ranks, and sums a (zeta, D) gradient of the step's shape with the same
+    all-reduce the gradient step uses (aok_b200.parallel.allreduce_sum).  Rank r
+    contributes r + 1 in every entry, so the sum is known.  Prints one JSON line on
+    rank 0 with dry_run: true (no throughput is measured)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import aok_b200 as aok
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    basis, pairs = workload(rank, min(args.batch, 4096))
+    shape = (basis.nshells, basis.K, basis.NZ)
+    ok = True
+
+    def step():
+        nonlocal ok
+        dz = torch.full(shape, float(rank + 1), dtype=torch.float64)
+        dD = torch.full(shape, float(-(rank + 1)), dtype=torch.float64)
+        dz, dD = aok.parallel.allreduce_sum([dz, dD])
+        want = world * (world + 1) / 2
+        ok = ok and bool(torch.all(dz == want)) and bool(torch.all(dD == -want))
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    if world > 1:
+        dist.barrier()
+    ms = (time.perf_counter() - t0) * 1e3 / max(args.steps, 1)
+    t = torch.tensor([ms, 0.0 if ok else 1.0], dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": float(t[0]), "higher_is_better": True,
+                          "scaling": "weak", "dry_run": True, "allreduce_ok": bool(t[1] == 0.0),
+                          "config": {"workload": "rank plumbing only (gloo, CPU)", "batch_per_rank": pairs.B,
+                                     "global_batch": pairs.B * world, "gradient_shape": list(shape)}}),
+              flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -187,10 +262,17 @@ def main():
                     help="with --profile: which kernel family to run (ncu captures)")
     ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
     ap.add_argument("--fp64", action="store_true", help="with --profile: run the FP64 kernels (overlap2c, overlap3c)")
+    ap.add_argument("--cpu-dry", action="store_true",
+                    help="rank plumbing only, on CPU: gloo process group, barriers, max-over-ranks timing and the "
+                         "gradient all-reduce of the step, with no kernels (for tests without a GPU)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args)  # one process per GPU under torchrun; rank 0 prints the line
     if args.impl == "reference":
         return run_reference(args)
     args.warmup = max(args.warmup, 3)
+    if args.cpu_dry:
+        return run_dry(args)
 
     import torch
     import torch.distributed as dist
