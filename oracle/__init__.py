@@ -55,7 +55,11 @@ def lib():
         L.aokor_evaluate_ed.argtypes = [_d, _d, _d, _i64, _d, _d, _i64, _i64, _i64, i64, i64, i64, i64, i64, cint, cint, dbl, cint]
         L.aokor_evaluate_pb.argtypes = [_d, _d, _d, _d, _i64, _d, _d, _i64, _i64, _i64, i64, i64, i64, i64, i64, cint, cint, dbl]
         L.aokor_evaluate_pbx.argtypes = [_d, _d, _d, i64, i64]
-        for name in ("aokor_overlap2c_gb", "aokor_overlap2c_orb", "aokor_overlap3c_gb", "aokor_overlap2c_orb_pb"):
+        L.aokor_overlap2c_orb_dpos.argtypes = [_d, _d, _d, i64, i64, i64, _i64, _d, _d, _i64, _i64, _d, _d, i64,
+                                               dbl, cint]
+        L.aokor_radials_pb.argtypes = [_d, _d, _d, _d, _i64, _d, _d, _i64, i64, i64, i64, i64, cint]
+        for name in ("aokor_overlap2c_gb", "aokor_overlap2c_orb", "aokor_overlap3c_gb", "aokor_overlap2c_orb_pb",
+                     "aokor_overlap2c_orb_dpos"):
             getattr(L, name).restype = cint
         _lib = L
     return _lib
@@ -138,6 +142,24 @@ def overlap2c_orb_pb(dS, ls, coef, zeta, sidxA, sidxB, posA, posB, lengthscale=1
     return dcoef, dalpha
 
 
+def overlap2c_orb_dpos(dS, ls, coef, zeta, sidxA, sidxB, posA, posB, lengthscale=1.0, nthreads=1):
+    """Position pullback of the orbital-path 2C overlap (no reference counterpart):
+    dA, dB (3,B) = sum dS * dS/dA, sum dS * dS/dB, by differentiating each Gaussian."""
+    ls = _i(ls)
+    zeta, coef, dS = _f(zeta), _f(coef), _f(dS)
+    ns, K, NZ = zeta.shape
+    posA, posB = _f(posA), _f(posB)
+    B = posA.shape[1]
+    dA = np.zeros((3, B), order="F")
+    dB = np.zeros((3, B), order="F")
+    st = lib().aokor_overlap2c_orb_dpos(_p(dA), _p(dB), _p(dS), ns, K, NZ, _p(ls), _p(coef), _p(zeta),
+                                        _p(_i(sidxA)), _p(_i(sidxB)), _p(posA), _p(posB), B, float(lengthscale),
+                                        nthreads)
+    if st:
+        raise ValueError("species index outside 1..NZ")
+    return dA, dB
+
+
 def compile_coef(zeta, D, ls):
     """_compile_coef (cartesian_gto_basis.jl:110-120)."""
     zeta, D, ls = _f(zeta), _f(D), _i(ls)
@@ -175,6 +197,18 @@ def radials(r, sidx, zeta, D, poly, slater=False, with_grad=True):
     lib().aokor_radials(_p(R), _p(dR) if with_grad else None, _p(r), _p(_i(sidx)), _p(zeta), _p(D),
                         _p(_i(poly)), nX, nRad, K, NZ, int(bool(slater)))
     return (R, dR) if with_grad else R
+
+
+def radials_pb(dR, r, sidx, zeta, D, poly, slater=False):
+    """Radial-layer pullback_ps (gtostoradials.jl:232-267) -> (dzeta, dD) (nRad,K,NZ)."""
+    r, zeta, D, dR = _f(r), _f(zeta), _f(D), _f(dR)
+    nRad, K, NZ = zeta.shape
+    nX = r.shape[0]
+    dz = np.zeros((nRad, K, NZ), order="F")
+    dD = np.zeros((nRad, K, NZ), order="F")
+    lib().aokor_radials_pb(_p(dz), _p(dD), _p(dR), _p(r), _p(_i(sidx)), _p(zeta), _p(D), _p(_i(poly)), nX, nRad, K,
+                           NZ, int(bool(slater)))
+    return dz, dD
 
 
 def solid_harmonics(X, L):

@@ -233,6 +233,130 @@ int aokor_overlap2c_orb(double* out, int64_t ns, int64_t K, int64_t NZ, const in
 }
 
 /* ------------------------------------------------------------------------ */
+/* Position pullback of the orbital-path 2C overlap (no reference            */
+/* counterpart; the reference has no position gradient of the overlap).     */
+/* Independent of the product's moment formulation: each Cartesian Gaussian  */
+/* is differentiated itself,                                                 */
+/*   d/dA_x [x_A^i exp(-a x_A^2)] = 2a x_A^{i+1} exp(-a x_A^2) - i x_A^{i-1} exp(-a x_A^2), */
+/* (and with b, j for B), and the 1-D overlaps of the raised and lowered     */
+/* powers come from the same E-table recursion as the forward (tables to    */
+/* l+1 on each side).  The derivative blocks are placed with the forward's   */
+/* aliased lin = c1 + (2la+1) c2 layout and read back through the shell's    */
+/* nbf strides, so dA[c,b] = sum dS . dOut/dA_c exactly as the forward       */
+/* writes Out.  dA, dB (3,B); dS (N,N,B).                                    */
+/* ------------------------------------------------------------------------ */
+static double e0(const double* E, int TM, int IM, int i, int j) {
+    /* E^{ij}_0 with 0-based powers; 0 for a negative power */
+    if (i < 0 || j < 0) return 0.0;
+    return E2(1, i + 1, j + 1);
+}
+
+int aokor_overlap2c_orb_dpos(double* dA, double* dB, const double* dS, int64_t ns, int64_t K, int64_t NZ,
+                             const int64_t* ls, const double* coef, const double* zeta,
+                             const int64_t* sidxA, const int64_t* sidxB,
+                             const double* posA, const double* posB, int64_t B,
+                             double lengthscale, int nthreads) {
+    for (int64_t b = 0; b < B; ++b)
+        if (sidxA[b] < 1 || sidxA[b] > NZ || sidxB[b] < 1 || sidxB[b] > NZ) return 4;
+    int L = lmax_of(ls, ns);
+    int TM = 2 * L + 4, IM = L + 2;
+    int64_t* boff = (int64_t*)malloc(sizeof(int64_t) * (size_t)(ns + 1));
+    boff[0] = 0;
+    for (int64_t s = 0; s < ns; ++s) boff[s + 1] = boff[s] + (ls[s] + 1) * (ls[s] + 2) / 2;
+    int64_t N = boff[ns];
+    int nt = set_threads(nthreads);
+    (void)nt;
+    int nc = (L + 1) * (L + 2) / 2;
+#pragma omp parallel num_threads(nt)
+    {
+        double* Ebuf = (double*)malloc(sizeof(double) * (size_t)(3 * TM * IM * IM));
+        double* blkA = (double*)malloc(sizeof(double) * (size_t)(3 * nc * nc));
+        double* blkB = (double*)malloc(sizeof(double) * (size_t)(3 * nc * nc));
+#pragma omp for schedule(static)
+        for (int64_t b = 0; b < B; ++b) {
+            int64_t ga = sidxA[b] - 1, gb = sidxB[b] - 1;
+            double A[3], Bv[3], ga3[3] = {0, 0, 0}, gb3[3] = {0, 0, 0};
+            for (int c = 0; c < 3; ++c) {
+                A[c] = posA[3 * b + c];
+                Bv[c] = posB[3 * b + c];
+                if (lengthscale != 1.0) { A[c] *= lengthscale; Bv[c] *= lengthscale; }
+            }
+            for (int64_t sa = 0; sa < ns; ++sa)
+                for (int64_t sb = 0; sb < ns; ++sb) {
+                    int la = (int)ls[sa], lb = (int)ls[sb];
+                    int nbf_a = (la + 1) * (la + 2) / 2, nbf_b = (lb + 1) * (lb + 2) / 2;
+                    int N1 = 2 * la + 1;
+                    for (int k = 0; k < 3 * nc * nc; ++k) { blkA[k] = 0.0; blkB[k] = 0.0; }
+                    for (int64_t ip = 0; ip < K; ++ip)
+                        for (int64_t jp = 0; jp < K; ++jp) {
+                            double ca = coef[sa + ns * (ip + K * ga)], cb = coef[sb + ns * (jp + K * gb)];
+                            if (ca == 0.0 || cb == 0.0) continue;
+                            double aa = zeta[sa + ns * (ip + K * ga)], ab = zeta[sb + ns * (jp + K * gb)];
+                            double p = aa + ab;
+                            double mu = aa * ab / p, oo2p = 0.5 / p;
+                            double prefac = ca * cb * pow(M_PI / p, 1.5);
+                            for (int ax = 0; ax < 3; ++ax) {
+                                double Px = (aa * A[ax] + ab * Bv[ax]) / p;
+                                md_E2(Ebuf + ax * TM * IM * IM, TM, IM, la + 2, lb + 2, Px - A[ax], Px - Bv[ax],
+                                      A[ax] - Bv[ax], mu, oo2p);
+                            }
+                            /* component pairs in the forward's order (kernels_2c.jl:102-119) */
+                            int index1 = 1;
+                            for (int ll1 = la; ll1 >= 0; --ll1)
+                                for (int n1 = 0; n1 <= la - ll1; ++n1) {
+                                    int m1 = la - ll1 - n1;
+                                    int pa[3] = {ll1, m1, n1};
+                                    int index2 = 1;
+                                    for (int ll2 = lb; ll2 >= 0; --ll2)
+                                        for (int n2 = 0; n2 <= lb - ll2; ++n2) {
+                                            int m2 = lb - ll2 - n2;
+                                            int pb[3] = {ll2, m2, n2};
+                                            int lin = index1 + N1 * (index2 - 1);
+                                            double f[3], fa[3], fb[3];
+                                            for (int ax = 0; ax < 3; ++ax) {
+                                                const double* E = Ebuf + ax * TM * IM * IM;
+                                                int i = pa[ax], j = pb[ax];
+                                                f[ax] = e0(E, TM, IM, i, j);
+                                                fa[ax] = 2.0 * aa * e0(E, TM, IM, i + 1, j) - i * e0(E, TM, IM, i - 1, j);
+                                                fb[ax] = 2.0 * ab * e0(E, TM, IM, i, j + 1) - j * e0(E, TM, IM, i, j - 1);
+                                            }
+                                            for (int c = 0; c < 3; ++c) {
+                                                double oa = 1.0, ob = 1.0;
+                                                for (int ax = 0; ax < 3; ++ax) {
+                                                    oa *= (ax == c) ? fa[ax] : f[ax];
+                                                    ob *= (ax == c) ? fb[ax] : f[ax];
+                                                }
+                                                blkA[c * nc * nc + lin - 1] += oa * prefac;
+                                                blkB[c * nc * nc + lin - 1] += ob * prefac;
+                                            }
+                                            index2 += 1;
+                                        }
+                                    index1 += 1;
+                                }
+                        }
+                    for (int j = 0; j < nbf_b; ++j)
+                        for (int i = 0; i < nbf_a; ++i) {
+                            double g = dS[(boff[sa] + i) + N * ((boff[sb] + j) + N * b)];
+                            for (int c = 0; c < 3; ++c) {
+                                ga3[c] += g * blkA[c * nc * nc + i + nbf_a * j];
+                                gb3[c] += g * blkB[c * nc * nc + i + nbf_a * j];
+                            }
+                        }
+                }
+            for (int c = 0; c < 3; ++c) {
+                dA[3 * b + c] = lengthscale * ga3[c];
+                dB[3 * b + c] = lengthscale * gb3[c];
+            }
+        }
+        free(Ebuf);
+        free(blkA);
+        free(blkB);
+    }
+    free(boff);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* 3-center overlap: batch_V_kernel! (kernels_3c.jl:12-162).                 */
 /* E3[t, i, j, k], TM = 3Lmax+3.  The table is zeroed in full per primitive  */
 /* triple and axis; for l <= 3 this equals the reference's partial zeroing   */
@@ -619,7 +743,9 @@ void aokor_radials(double* R, double* dR, const double* r, const int64_t* sidx,
 /*   F_lm = sqrt((2l+1)/(4pi) (l-m)!/(l+m)!),  C_m + i S_m = (x + i y)^m,     */
 /*   Q_m^m = (2m-1)!!, Q_{m+1}^m = (2m+1) z Q_m^m,                            */
 /*   Q_l^m = ((2l-1) z Q_{l-1}^m - (l+m-1) r^2 Q_{l-2}^m) / (l-m)            */
-/* (no Condon-Shortley phase: Z_1,-1 : Z_1,0 : Z_1,1 = y : z : x).           */
+/* (no Condon-Shortley phase: Z_1,-1 : Z_1,0 : Z_1,1 = y : z : x).  This is  */
+/* SpheriCart's definition (Bigi et al., J. Chem. Phys. 159, 064802 (2023),  */
+/* Sec. II) with its two (-1)^m factors, in F_l^m and in Q_m^m, cancelled.   */
 /* Gradients by forward-mode dual numbers (value + 3 partials).              */
 /* ------------------------------------------------------------------------ */
 typedef struct { double v, x, y, z; } d4;
@@ -735,6 +861,35 @@ void aokor_evaluate_ed(double* P, double* dP, const double* X, const int64_t* si
     }
 }
 
+/* Radial-layer parameter pullback: the segmented reduction of              */
+/* _gtostoradials_pb_ka! and pullback_ps (gtostoradials.jl:232-267), one     */
+/* accumulator per (species, radial, primitive) slot over the points of that */
+/* species.  dzeta, dD (nRad,K,NZ); dRv (nX,nRad) is the cotangent of R.     */
+void aokor_radials_pb(double* dzeta, double* dD, const double* dRv, const double* r,
+                      const int64_t* sidx, const double* zeta, const double* D,
+                      const int64_t* poly, int64_t nX, int64_t nRad, int64_t K, int64_t NZ,
+                      int slater) {
+    for (int64_t q = 0; q < nRad * K * NZ; ++q) { dzeta[q] = 0.0; dD[q] = 0.0; }
+    for (int64_t sg = 0; sg < NZ; ++sg)
+        for (int64_t k = 0; k < nRad; ++k)
+            for (int64_t m = 0; m < K; ++m) {
+                int64_t slot = k + nRad * (m + K * sg);
+                double zkm = zeta[slot], Dkm = D[slot];
+                double pz = 0.0, pD = 0.0;
+                for (int64_t i = 0; i < nX; ++i) {
+                    if (sidx[i] - 1 != sg) continue;
+                    double ri = r[i];
+                    double fx = slater ? ri : ri * ri;
+                    double a = exp((-zkm) * fx);
+                    double gg = dRv[i + nX * k] * ipow(ri, poly[k]);
+                    pD += gg * a;
+                    pz += ((gg * Dkm) * a) * (-fx);
+                }
+                dD[slot] = pD;
+                dzeta[slot] = pz;
+            }
+}
+
 /* Parameter pullback of evaluate: pullback_ps (atomicorbitals.jl:254-267),  */
 /* _aorb_pbrad_ka! (:249-252) and the radial segmented pullback              */
 /* (gtostoradials.jl:232-267).  dzeta, dD (nRad,K,NZ); dP (nX,nOrb).         */
@@ -759,25 +914,7 @@ void aokor_evaluate_pb(double* dzeta, double* dD, const double* dPv, const doubl
     for (int64_t i = 0; i < nOrb; ++i)
         for (int64_t j = 0; j < nX; ++j)
             dR[j + nX * (iR[i] - 1)] += dPv[j + nX * i] * Y[j + nX * (iY[i] - 1)];
-    for (int64_t q = 0; q < nRad * K * NZ; ++q) { dzeta[q] = 0.0; dD[q] = 0.0; }
-    for (int64_t sg = 0; sg < NZ; ++sg)
-        for (int64_t k = 0; k < nRad; ++k)
-            for (int64_t m = 0; m < K; ++m) {
-                int64_t slot = k + nRad * (m + K * sg);
-                double zkm = zeta[slot], Dkm = D[slot];
-                double pz = 0.0, pD = 0.0;
-                for (int64_t i = 0; i < nX; ++i) {
-                    if (sidx[i] - 1 != sg) continue;
-                    double ri = r[i];
-                    double fx = slater ? ri : ri * ri;
-                    double a = exp((-zkm) * fx);
-                    double gg = dR[i + nX * k] * ipow(ri, poly[k]);
-                    pD += gg * a;
-                    pz += ((gg * Dkm) * a) * (-fx);
-                }
-                dD[slot] = pD;
-                dzeta[slot] = pz;
-            }
+    aokor_radials_pb(dzeta, dD, dR, r, sidx, zeta, D, poly, nX, nRad, K, NZ, slater);
     free(Xs); free(r); free(Y); free(dR);
 }
 

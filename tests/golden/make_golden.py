@@ -11,7 +11,10 @@ independently of the oracle's recursions, to pin the oracle.
   for z = 0..l-x: (x, l-x-z, z).
 * Real solid harmonics Z_lm (l <= 3, index l^2+l+m) from their explicit
   Cartesian polynomials (standard real-harmonic table, L2-normalised on the
-  unit sphere, no Condon-Shortley phase).
+  unit sphere, no Condon-Shortley phase): the convention of SpheriCart
+  (Bigi et al., J. Chem. Phys. 159, 064802 (2023)), whose F_l^m and Q_m^m each
+  carry a (-1)^m that cancel; tests/helpers.py restates that definition and
+  tests/test_oracle.py checks this table against it.
 
 Run from the repo root:  python tests/golden/make_golden.py
 """

@@ -211,3 +211,73 @@ def test_evaluate_gradients_fd(slater):
                                                         False)))
     fdx = (g(X + h * U) - g(X - h * U)) / (2 * h)
     assert abs(np.sum(dX * U) - fdx) < 1e-6 * max(1, abs(fdx))
+
+
+@pytest.mark.parametrize("slater", [False, True])
+def test_radials_derivative_and_pullback_fd(slater):
+    """The radial layer alone (gtostoradials.jl:117-185, 232-267): dR/dr and the (zeta, D)
+    pullback of R against central differences."""
+    b = W.config1_basis()
+    rng = np.random.default_rng(6)
+    r = np.abs(rng.normal(size=11)) * 2.0 + 0.05
+    sidx = rng.integers(1, 4, size=11)
+    poly = np.array([0, 1, 2, 0, 1, 0]) if slater else np.zeros(6, np.int64)
+    R, dR = oracle.radials(r, sidx, b.zeta, b.D, poly, slater)
+    h = 1e-6
+    fd = (oracle.radials(r + h, sidx, b.zeta, b.D, poly, slater, False) -
+          oracle.radials(r - h, sidx, b.zeta, b.D, poly, slater, False)) / (2 * h)
+    assert np.max(np.abs(fd - dR)) < 1e-6 * max(1.0, np.abs(dR).max())
+    dRv = rng.standard_normal(R.shape)
+    dz, dD = oracle.radials_pb(dRv, r, sidx, b.zeta, b.D, poly, slater)
+    V = rng.standard_normal(b.zeta.shape)
+    f = lambda z, D: float(np.sum(dRv * oracle.radials(r, sidx, z, D, poly, slater, False)))
+    fdz = (f(b.zeta + h * V, b.D) - f(b.zeta - h * V, b.D)) / (2 * h)
+    fdD = (f(b.zeta, b.D + h * V) - f(b.zeta, b.D - h * V)) / (2 * h)
+    assert abs(np.sum(dz * V) - fdz) < 1e-6 * max(1, abs(fdz))
+    assert abs(np.sum(dD * V) - fdD) < 1e-6 * max(1, abs(fdD))
+    # a species absent from the batch gets a zero gradient
+    dz1, dD1 = oracle.radials_pb(dRv, r, np.where(sidx == 3, 1, sidx), b.zeta, b.D, poly, slater)
+    assert np.all(dz1[:, :, 2] == 0) and np.all(dD1[:, :, 2] == 0)
+
+
+def test_solid_harmonics_follow_sphericart_definition():
+    """The m != 0 signs (and all factors) of the oracle's harmonics equal SpheriCart's
+    published definition, restated factor by factor in helpers.sphericart_solid_harmonics,
+    for l <= 4; and that definition reproduces the explicit l <= 3 polynomial table the
+    golden vectors were made from."""
+    from helpers import sphericart_solid_harmonics
+    pts = np.random.default_rng(12).normal(size=(3, 40)) * 1.3
+    Z, _ = oracle.solid_harmonics(pts, 4)
+    Zs = sphericart_solid_harmonics(pts, 4)
+    assert np.max(np.abs(Z - Zs)) < 1e-13 * max(1.0, np.abs(Zs).max())
+    Zg = sphericart_solid_harmonics(G["pts"], 3)
+    assert np.max(np.abs(Zg - G["Z"])) < 1e-13
+    # the l = 1 order and signs: (y, z, x) with the same positive factor sqrt(3 / 4 pi)
+    e = np.eye(3)
+    Z1 = sphericart_solid_harmonics(e, 1)[:, 1:4]
+    assert np.allclose(Z1, math.sqrt(3 / (4 * math.pi)) * np.array([[0, 0, 1], [1, 0, 0], [0, 1, 0]]))
+
+
+def test_overlap_position_pullback_fd_and_translation():
+    """The oracle's position pullback of the orbital-path 2C overlap (each Gaussian
+    differentiated, no moment formulation) against central differences of the oracle's
+    forward, h = 1e-6, for A and B separately, with a lengthscale; dA + dB = 0 as the
+    overlap depends on A - B only (both sides computed independently)."""
+    b = W.config2_basis()
+    pr = W.ragged_pairs(24, b.NZ, 11)
+    coef = oracle.compile_coef(b.zeta, b.D, b.ls)
+    N = b.nbf_total
+    dS = np.random.default_rng(12).standard_normal((N, N, pr.B))
+    dA, dB = oracle.overlap2c_orb_dpos(dS, b.ls, coef, b.zeta, pr.sidxA, pr.sidxB, pr.posA, pr.posB, 1.1)
+    h = 1e-6
+    for c in range(3):
+        for side, g in ((0, dA), (1, dB)):
+            P = [pr.posA, pr.posB]
+            Pp, Pm = [x.copy() for x in P], [x.copy() for x in P]
+            Pp[side][c] += h
+            Pm[side][c] -= h
+            Sp = oracle.overlap2c_orb(b.ls, coef, b.zeta, pr.sidxA, pr.sidxB, Pp[0], Pp[1], 1.1)
+            Sm = oracle.overlap2c_orb(b.ls, coef, b.zeta, pr.sidxA, pr.sidxB, Pm[0], Pm[1], 1.1)
+            fd = ((Sp - Sm) * dS).sum(axis=(0, 1)) / (2 * h)
+            assert np.max(np.abs(fd - g[c])) < 1e-8 * np.max(np.abs(fd))
+    assert np.max(np.abs(dA + dB)) < 1e-13 * np.max(np.abs(dA))
