@@ -12,7 +12,8 @@ from .basis import (AtomicOrbitals, CartesianGTOBasis, CartesianShell, CompiledB
                     slater_orbitals)
 from .units import Length, ang2bohr, to_bohr  # noqa: F401
 from .overlap import (NoTangent, batch_overlap, batch_overlap_, batch_overlap_3c, batch_overlap_3c_,  # noqa: F401
-                      compile_coef, compile_coef_pb, overlap_pb_coef_alpha, rrule_batch_overlap)
+                      compile_coef, compile_coef_pb, overlap_pb_coef_alpha, position_pullback,
+                      rrule_batch_overlap)
 from .overlap import pullback_ps as overlap_pullback_ps  # noqa: F401
 from ._dev import colmajor_empty, colmajor_zeros  # noqa: F401
 from .orbitals import evaluate, evaluate_ed, rrule_evaluate  # noqa: F401,E402

@@ -29,10 +29,13 @@ AOK_MAX_L = 3
 EXPORTS = [
     "aok_last_error", "aok_version", "aok_plan_create", "aok_plan_destroy", "aok_plan_nbf",
     "aok_plan_check", "aok_plan_set_basis", "aok_plan_set_graph", "aok_plan_autotune", "aok_plan_timing_enable", "aok_plan_timing_read", "aok_measure_fma_peak", "aok_compile_coef", "aok_species_index", "aok_overlap2c", "aok_overlap2c_gb", "aok_overlap3c_gb",
-    "aok_overlap2c_pullback", "aok_compile_coef_pullback", "aok_overlap_pullback_ps",
+    "aok_overlap2c_pullback", "aok_overlap2c_position_pullback", "aok_compile_coef_pullback",
+    "aok_overlap_pullback_ps",
     "aok_overlap2c_rrule", "aok_overlap_pullback_ps_rrule",
     "aok_orbitals_create", "aok_orbitals_destroy", "aok_orbitals_check", "aok_evaluate", "aok_evaluate_ed",
-    "aok_evaluate_pullback", "aok_evaluate_pullback_noalloc",
+    "aok_evaluate_pullback", "aok_radials_create", "aok_radials_destroy", "aok_radials_check",
+    "aok_radials_evaluate", "aok_radials_pullback",
+    "aok_evaluate_pullback_noalloc", "aok_evaluate_pullback_noalloc_check",
 ]
 
 
@@ -88,6 +91,7 @@ def load():
     L.aok_overlap2c_gb.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]
     L.aok_overlap3c_gb.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]
     L.aok_overlap2c_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
+    L.aok_overlap2c_position_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_compile_coef_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.aok_overlap_pullback_ps.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_overlap2c_rrule.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
@@ -100,6 +104,12 @@ def load():
     L.aok_evaluate_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_evaluate_pullback_noalloc.argtypes = [i64, i64, i64, pi64, i64, pi64, pi64, i64, cint, cint, vp, vp, vp,
                                                 vp, vp, vp, vp, vp, i64, dbl, vp]
+    L.aok_evaluate_pullback_noalloc_check.argtypes = [vp]
+    L.aok_radials_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, pi64, cint, cint]
+    L.aok_radials_destroy.argtypes = [vp]
+    L.aok_radials_check.argtypes = [vp, vp]
+    L.aok_radials_evaluate.argtypes = [vp, vp, vp, vp, vp, vp, vp, i64, vp]
+    L.aok_radials_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]
     for name in EXPORTS:
         if name not in ("aok_last_error", "aok_version"):
             getattr(L, name).restype = cint

@@ -57,6 +57,11 @@ struct aok_plan {
     void* d_partials = nullptr;      // per-CTA item sums
     int max_blocks = 0;
     void* d_coef_scratch = nullptr;  // ns*K*NZ
+    // position pullback (overlap2c_dpos.cu): records per (species pair, shell pair), their
+    // counts, and the shell-pair list heaviest class first
+    void* d_dpos_rec = nullptr;
+    int* d_dpos_counts = nullptr;
+    aok::Item* d_dpos_items = nullptr;
     // 3C schedule (overlap3c.cu)
     void* d_pp3 = nullptr;
     int* d_npp3 = nullptr;
@@ -145,6 +150,9 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
 // Counting sort of a batch by species key (stable), tiles of 32 elements of
 // one key, and the first tile of each key.  Buffers: perm (B), tiles
 // (B/32 + NZ^2 + 1), tbase (NZ^2 + 1), blockhist (kBinMaxBlocksHost * NZ^2).
+// An element with a species index outside 1..NZ sets *err and is left out of
+// the bins; when zero3 (zero3b) is set, its three values zero3[3b..3b+2]
+// (elements of zero3_bytes bytes, e.g. a position gradient) are written as zeros.
 struct BinBufs {
     int* perm;
     int4* tiles;
@@ -153,6 +161,9 @@ struct BinBufs {
     unsigned* counter;
     int* blockhist;
     int* err;
+    void* zero3 = nullptr;
+    void* zero3b = nullptr;
+    int zero3_bytes = 0;
 };
 constexpr int kBinMaxBlocksHost = 512;
 int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
@@ -161,6 +172,9 @@ int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t 
 int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* D,
                        const void* posA, const void* posB, double lengthscale, cudaStream_t s);
 int ensure_pb_buffers(aok_plan* p);
+int launch_overlap2c_dpos(aok_plan* p, void* dA, void* dB, const void* dS, const void* zeta, const void* coef,
+                          const int64_t* sidxA, const int64_t* sidxB, const void* posA, const void* posB, int64_t B,
+                          double lengthscale, cudaStream_t s);
 int launch_prep_pb(aok_plan* p, const void* zeta, const void* coef, int keep_absent, cudaStream_t s);
 int launch_overlap2c(aok_plan* p, void* out, const void* posA, const void* posB, int64_t B,
                      double lengthscale, cudaStream_t s);

@@ -147,7 +147,8 @@ int aok_plan_destroy(aok_plan* p) {
                     p->d_items,     p->d_blockhist, p->d_gb_zeta,    p->d_gb_coef,
                     p->d_pb_rec,    p->d_pb_counts, p->d_pb_items,  p->d_pb_itemidx, p->d_pb_rows,
                     p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3,    p->d_order3,
-                    p->d_pk,        p->d_segs,      p->d_nseg};
+                    p->d_pk,        p->d_segs,      p->d_nseg,      p->d_dpos_rec,   p->d_dpos_counts,
+                    p->d_dpos_items};
     for (void* b : bufs) dfree(b);
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     if (p->cap) cudaStreamDestroy(p->cap);
@@ -446,6 +447,20 @@ int aok_overlap2c_pullback(aok_plan* p, void* dcoef, void* dalpha, const void* d
     if (!dcoef || !dalpha || !zeta || !coef) return set_error(AOK_ERR_INVALID, "aok_overlap2c_pullback: null pointer");
     return overlap2c_pullback(p, dcoef, dalpha, dS, zeta, coef, nullptr, posA, posB, sidxA, sidxB, B, lengthscale, 1,
                               stream, "aok_overlap2c_pullback");
+}
+
+int aok_overlap2c_position_pullback(aok_plan* p, void* dA, void* dB, const void* dS, const void* zeta,
+                                    const void* coef, const void* posA, const void* posB, const int64_t* sidxA,
+                                    const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
+    static const char* who = "aok_overlap2c_position_pullback";
+    if (!p) return set_error(AOK_ERR_INVALID, std::string(who) + ": null plan");
+    if (!dA && !dB) return set_error(AOK_ERR_INVALID, std::string(who) + ": dA and dB are both null");
+    AOK_TRY(check_batch(p, B, who));
+    if (B == 0) return AOK_OK;
+    if (!dS || !zeta || !coef || !posA || !posB || !sidxA || !sidxB)
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    return launch_overlap2c_dpos(p, dA, dB, dS, zeta, coef, sidxA, sidxB, posA, posB, B, lengthscale,
+                                 (cudaStream_t)stream);
 }
 
 int aok_overlap2c_rrule(aok_plan* p, void* out, const void* zeta, const void* D, const void* posA, const void* posB,

@@ -75,6 +75,12 @@ __device__ __forceinline__ D4<FT> dlin(FT ca, const D4<FT>& a, FT cb, const D4<F
 }
 
 // Z_lm and gradients for l <= L at (x, y, z), written to Z[idx], G[3*idx + c].
+// The convention is SpheriCart's (Bigi, Fraux, Browning, Ceriotti, J. Chem. Phys.
+// 159, 064802 (2023), Sec. II), the harmonics the reference's SolidHarmonics
+// evaluates: Z_l^m = F_l^|m| Q_l^|m| {s_|m|, 1/sqrt2, c_m} with
+// F_l^m = (-1)^m sqrt((2l+1)/(2pi) (l-m)!/(l+m)!) and Q_m^m = (-1)^m (2m-1)!!.
+// The two (-1)^m cancel, so here both are dropped: Q_m^m = (2m-1)!! and the
+// m != 0 factor is sqrt(2) F_lm with F_lm = sqrt((2l+1)/(4pi) (l-m)!/(l+m)!).
 template <typename FT, int L>
 __device__ __forceinline__ void solid_harmonics(FT x, FT y, FT z, const double* F, FT* Zs, FT* Gs, int stride) {
     const D4<FT> X{x, FT(1), FT(0), FT(0)}, Y{y, FT(0), FT(1), FT(0)}, Zd{z, FT(0), FT(0), FT(1)};
@@ -342,7 +348,8 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
     const FT ux = x / r, uy = y / r, uz = z / r;
     // accumulate dRad into S.R after dX is done: first pass dX
     if (valid && P.dX) {
-        for (int i = 0; i < P.nOrb; ++i) {
+        // a point with a species index outside 1..NZ (sg = -1) gets dX = 0
+        for (int i = 0; i < (sg >= 0 ? P.nOrb : 0); ++i) {
             const int k = P.iR[i], yi = P.iY[i];
             const FT g = dPin[j + P.nX * i];
             const FT rn = S.R[k * kEvalThreads + t], yl = S.Z[yi * kEvalThreads + t];
@@ -440,7 +447,10 @@ __device__ __forceinline__ int epb_nch(const int* tbase, int sigma, int NZ) {
 // R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][32], f [32]
 __host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) { return (size_t)(3 * nRad + 4 * nY + 1) * 32; }
 
-template <typename FT, int L>
+// RAD: the radial layer's own pullback (gtostoradials.jl:232-267): X holds the
+// radii r (nX), dPin the cotangent of R (nX, nRad), so gg_k = dR[j,k] r^p_k and
+// there are no harmonics and no dX.
+template <typename FT, int L, bool RAD = false>
 __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ EpbParams Q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int nY = (L + 1) * (L + 1);
@@ -493,8 +503,25 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
             // phase A: lane = point
             {
                 const int e = c0 + lane;
-                const bool valid = e < e1;
-                const long long j = valid ? (long long)Q.perm[e] : 0;
+                const bool in_chunk = e < e1;
+                const long long j = in_chunk ? (long long)Q.perm[e] : 0;
+                // multi-species bins hold only points of species sigma; the single-species
+                // bin holds every point, so a point's own index is checked here: one
+                // outside 1..NZ gets dX = 0 and adds nothing to the (zeta, D) gradient
+                bool valid = in_chunk;
+                if (in_chunk && P.sidx[j] != (int64_t)(sigma + 1)) {
+                    atomicCAS(P.err, 0, AOK_ERR_SPECIES);
+                    valid = false;
+                    if (P.dX) {
+                        FT* dX = (FT*)P.dX;
+                        dX[3 * j] = dX[3 * j + 1] = dX[3 * j + 2] = FT(0);
+                    }
+                }
+                FT r;
+                if constexpr (RAD) {
+                    r = valid ? Xin[j] : FT(0);
+                    for (int k = 0; k < P.nRad; ++k) gg[k * 32 + lane] = valid ? dPin[j + P.nX * k] : FT(0);
+                } else {
                 FT x = FT(0), y = FT(0), z = FT(1);
                 if (valid) {
                     x = Xin[3 * j];
@@ -506,7 +533,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                         z = sc * z;
                     }
                 }
-                const FT r = sqrt(x * x + y * y + z * z);
+                r = sqrt(x * x + y * y + z * z);
                 for (int k = 0; k < P.nRad; ++k) {
                     FT Rk, dRk;
                     radial<FT>(sz, sD, sl, sn, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
@@ -534,6 +561,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                         dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
                     }
                 }
+                }  // RAD
                 for (int k = 0; k < P.nRad; ++k) {
                     FT rp = FT(1);
                     for (int i = 0; i < P.poly[k]; ++i) rp *= r;
@@ -608,6 +636,52 @@ __global__ void k_eval_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const
     for (int r = 0; r < nrows; ++r) s += rows[(size_t)r * 2 * ntab + t];
     if (t < ntab) dD[t] = (FT)s;
     else dzeta[t - ntab] = (FT)s;
+}
+
+// ---------------------------------------------------------------------------
+// The radial layer on its own (GaussianTypeRadials / SlaterTypeRadials
+// evaluate and evaluate_ed, gtostoradials.jl:117-185): R[j,k] (nX, nRad) and
+// dR/dr from the radii r (nX) and species indices.  One thread per point; the
+// blocks stay resident and stride over the points, staging the (zeta, D)
+// tables and the per-(radial, species) primitive counts once.  A point's
+// nRad values go to nRad columns, so the stores of a warp are coalesced per
+// column.  A species index outside 1..NZ sets the error word and the point is
+// evaluated as species 1 (as in evaluate).
+// ---------------------------------------------------------------------------
+template <typename FT, bool ED>
+__global__ void __launch_bounds__(kEvalThreads) k_radials(const __grid_constant__ EvalParams P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ntab = P.nRad * P.K * P.NZ;
+    FT* sz = reinterpret_cast<FT*>(smem_raw);
+    FT* sD = sz + ntab;
+    FT* sl = sD + ntab;
+    int* sn = reinterpret_cast<int*>(sl + ntab);
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
+        sz[i] = ((const FT*)P.zeta)[i];
+        sD[i] = ((const FT*)P.D)[i];
+        sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
+    }
+    for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
+        sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
+    __syncthreads();
+    const FT* rin = (const FT*)P.X;
+    FT* Rout = (FT*)P.P;
+    FT* dRout = (FT*)P.dP;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < P.nX;
+         j += (long long)gridDim.x * blockDim.x) {
+        const FT r = rin[j];
+        int sg = (int)P.sidx[j] - 1;
+        if (sg < 0 || sg >= P.NZ) {
+            atomicCAS(P.err, 0, AOK_ERR_SPECIES);
+            sg = 0;
+        }
+        for (int k = 0; k < P.nRad; ++k) {
+            FT R, dR;
+            radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, P.poly[k], P.slater, r, R, dR);
+            __stcs(Rout + j + P.nX * k, R);
+            if constexpr (ED) __stcs(dRout + j + P.nX * k, dR);
+        }
+    }
 }
 
 static size_t eval_smem_bytes(const aok_orbitals* o, bool pb) {
@@ -775,8 +849,11 @@ int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const v
     if (dzeta && dD && nslot <= 32 * kEpbMaxGroups && o->NZ * o->NZ <= kMaxPairs) {
         // slot-parallel: points binned by species, lanes = (radial, primitive) slots
         AOK_TRY_PB(ensure_epb_buffers(o, nX));
-        const BinBufs bb{o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
-                         o->d_epb_blockhist, o->d_err};
+        // points with a bad species index are left out of the bins; their dX is zeroed there
+        BinBufs bb{o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
+                   o->d_epb_blockhist, o->d_err};
+        bb.zero3 = dX;
+        bb.zero3_bytes = o->prec == AOK_PREC_F64 ? 8 : 4;
         AOK_TRY_PB(launch_bin_into(bb, sidx, nullptr, nX, (int)o->NZ, s));
         EpbParams Q;
         Q.E = P;
@@ -816,6 +893,76 @@ int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const v
     else
         k_eval_reduce<float><<<(2 * ntab + 127) / 128, 128, 0, s>>>((float*)dD, (float*)dzeta, P.rows, grid, ntab);
     return cuda_status(cudaGetLastError(), "k_eval_reduce");
+}
+
+// radial layer forward: R (and dR) at the radii r
+int launch_radials(aok_orbitals* o, void* R, void* dR, const void* r, const int64_t* sidx, const void* zeta,
+                   const void* D, int64_t nX, cudaStream_t s) {
+    EvalParams P;
+    fill_params(o, P, r, sidx, zeta, D, nX, 1.0);
+    P.P = R;
+    P.dP = dR;
+    const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
+    const size_t smem = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "radials: basis too large for shared memory");
+    void* k;
+    if (o->prec == AOK_PREC_F64) k = dR ? (void*)k_radials<double, true> : (void*)k_radials<double, false>;
+    else k = dR ? (void*)k_radials<float, true> : (void*)k_radials<float, false>;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return cuda_status(e, "cudaFuncSetAttribute(k_radials)");
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kEvalThreads, smem)) != cudaSuccess)
+        return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((nX + kEvalThreads - 1) / kEvalThreads, (int64_t)o->num_sms * std::max(occ, 1)));
+    void* args[] = {&P};
+    return cuda_status(cudaLaunchKernel(k, dim3(grid), dim3(kEvalThreads), args, smem, s), "k_radials");
+}
+
+// radial layer pullback: (dzeta, dD) from dR (nX, nRad), slot-parallel over species-binned points
+int launch_radials_pb(aok_orbitals* o, void* dzeta, void* dD, const void* dRin, const void* r, const int64_t* sidx,
+                      const void* zeta, const void* D, int64_t nX, cudaStream_t s) {
+    EvalParams P;
+    fill_params(o, P, r, sidx, zeta, D, nX, 1.0);
+    P.dPin = dRin;
+    const int nslot = (int)(o->nRad * o->K);
+    if (nslot > 32 * kEpbMaxGroups || o->NZ * o->NZ > kMaxPairs)
+        return set_error(AOK_ERR_UNSUPPORTED, "radials pullback: too many (radial, primitive) slots or species");
+    AOK_TRY_PB(ensure_epb_buffers(o, nX));
+    const BinBufs bb{o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
+                     o->d_epb_blockhist, o->d_err};
+    AOK_TRY_PB(launch_bin_into(bb, sidx, nullptr, nX, (int)o->NZ, s));
+    EpbParams Q;
+    Q.E = P;
+    Q.perm = o->d_epb_perm;
+    Q.tiles = o->d_epb_tiles;
+    Q.tbase = o->d_epb_tbase;
+    Q.counter = o->d_epb_counter;
+    Q.partial = (double*)o->d_epb_partial;
+    Q.ucap = (int)o->epb_ucap;
+    const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
+    const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    const size_t per_warp = epb_warp_words((int)o->nRad, 1) * fsz;
+    int nw = 8;
+    while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;
+    const size_t smem = tab + nw * per_warp;
+    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "radials pullback: basis too large");
+    void* k = o->prec == AOK_PREC_F64 ? (void*)k_evaluate_pbs<double, 0, true> : (void*)k_evaluate_pbs<float, 0, true>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs radial)");
+    const int per_sm = std::max(1, std::min(4, (int)((228 * 1024) / (smem + 1024))));
+    void* args[] = {&Q};
+    AOK_TRY_PB(cuda_status(cudaLaunchKernel(k, dim3(o->num_sms * per_sm), dim3(32 * nw), args, smem, s),
+                           "k_evaluate_pbs (radial)"));
+    const int nout = 2 * nslot * (int)o->NZ, rb = (nout * 32 + 255) / 256;
+    if (o->prec == AOK_PREC_F64)
+        k_epb_reduce<double><<<rb, 256, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, o->d_epb_tbase, nslot,
+                                               (int)o->NZ, Q.ucap);
+    else
+        k_epb_reduce<float><<<rb, 256, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, o->d_epb_tbase, nslot,
+                                              (int)o->NZ, Q.ucap);
+    return cuda_status(cudaGetLastError(), "k_epb_reduce");
 }
 
 }  // namespace aok
@@ -946,6 +1093,70 @@ int aok_evaluate_pullback(aok_orbitals* o, void* dX, void* dzeta, void* dD, cons
     return launch_evaluate_pb(o, dX, dzeta, dD, dP, X, sidx, zeta, D, nX, lengthscale, s);
 }
 
+// ---- the radial layer (GaussianTypeRadials / SlaterTypeRadials) ----
+
+struct aok_radials {
+    aok_orbitals* o = nullptr;  // radial tables, error word and the binned-pullback buffers
+};
+
+int aok_radials_create(aok_radials** out, int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly, int radial_kind,
+                       int precision) {
+    if (!out || !poly) return set_error(AOK_ERR_INVALID, "aok_radials_create: null pointer");
+    *out = nullptr;
+    const int64_t one = 1;
+    aok_orbitals* o = nullptr;
+    // one placeholder orbital (radial 1, Z_00): the radial layer uses only the radial half of the plan
+    int st = aok_orbitals_create(&o, nRad, K, NZ, poly, 1, &one, &one, 0, radial_kind, precision);
+    if (st != AOK_OK) {
+        std::string m = aok_last_error();
+        const std::string from = "aok_orbitals_create";
+        if (m.compare(0, from.size(), from) == 0) m = "aok_radials_create" + m.substr(from.size());
+        return set_error(st, m);
+    }
+    aok_radials* r = new aok_radials();
+    r->o = o;
+    *out = r;
+    return AOK_OK;
+}
+
+int aok_radials_destroy(aok_radials* r) {
+    if (!r) return AOK_OK;
+    aok_orbitals_destroy(r->o);
+    delete r;
+    return AOK_OK;
+}
+
+int aok_radials_check(aok_radials* r, void* stream) {
+    if (!r) return set_error(AOK_ERR_INVALID, "aok_radials_check: null plan");
+    return aok_orbitals_check(r->o, stream);
+}
+
+int aok_radials_evaluate(aok_radials* r, void* R, void* dR, const void* rad, const int64_t* sidx, const void* zeta,
+                         const void* D, int64_t nX, void* stream) {
+    if (!r) return set_error(AOK_ERR_INVALID, "aok_radials_evaluate: null plan");
+    if (nX < 0) return set_error(AOK_ERR_INVALID, "aok_radials_evaluate: negative nX");
+    if (nX == 0) return AOK_OK;
+    if (!R || !rad || !sidx || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_radials_evaluate: null pointer");
+    return launch_radials(r->o, R, dR, rad, sidx, zeta, D, nX, (cudaStream_t)stream);
+}
+
+int aok_radials_pullback(aok_radials* r, void* dzeta, void* dD, const void* dRin, const void* rad,
+                         const int64_t* sidx, const void* zeta, const void* D, int64_t nX, void* stream) {
+    if (!r) return set_error(AOK_ERR_INVALID, "aok_radials_pullback: null plan");
+    if (!dzeta || !dD) return set_error(AOK_ERR_INVALID, "aok_radials_pullback: null pointer");
+    if (nX < 0) return set_error(AOK_ERR_INVALID, "aok_radials_pullback: negative nX");
+    aok_orbitals* o = r->o;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (nX == 0) {
+        const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
+        int st = cuda_status(cudaMemsetAsync(dzeta, 0, fsz * o->nRad * o->K * o->NZ, s), "memset");
+        if (st) return st;
+        return cuda_status(cudaMemsetAsync(dD, 0, fsz * o->nRad * o->K * o->NZ, s), "memset");
+    }
+    if (!dRin || !rad || !sidx || !zeta || !D) return set_error(AOK_ERR_INVALID, "aok_radials_pullback: null pointer");
+    return launch_radials_pb(o, dzeta, dD, dRin, rad, sidx, zeta, D, nX, s);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -977,6 +1188,8 @@ namespace aok {
 constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
 constexpr int kNoAllocMaxRad = 64;
 constexpr int kNoAllocMaxOrb = 256;
+constexpr int kNoAllocMaxK = 64;
+constexpr int kNoAllocMaxNZ = 64;
 constexpr size_t kNoAllocMapsOffset = 256;        // after the error word
 constexpr size_t kNoAllocRowsOffset = 4096;       // after the index maps
 static_assert(kNoAllocMapsOffset + sizeof(int) * (kNoAllocMaxRad + 2 * kNoAllocMaxOrb) <= kNoAllocRowsOffset,
@@ -1024,6 +1237,31 @@ static int noalloc_scratch(unsigned char** out) {
 
 }  // namespace aok
 
+// Reads and clears the scratch's error word on the current device (after
+// synchronising `stream`): AOK_ERR_SPECIES if the last allocation-free
+// pullback met a species index outside 1..NZ.  Allocates nothing.
+extern "C" int aok_evaluate_pullback_noalloc_check(void* stream) {
+    using namespace aok;
+    int dev = 0;
+    int st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != AOK_OK) return st;
+    if (dev < 0 || dev >= 256) return set_error(AOK_ERR_UNSUPPORTED, "aok_evaluate_pullback_noalloc_check: device id");
+    unsigned char* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        scratch = (unsigned char*)g_noalloc_ptr[dev];
+    }
+    if (!scratch) return AOK_OK;  // no allocation-free call has run on this device
+    if ((st = cuda_status(cudaStreamSynchronize((cudaStream_t)stream), "cudaStreamSynchronize"))) return st;
+    int h = 0;
+    if ((st = cuda_status(cudaMemcpy(&h, scratch, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(err)")))
+        return st;
+    if ((st = cuda_status(cudaMemset(scratch, 0, sizeof(int)), "cudaMemset(err)"))) return st;
+    if (h == AOK_ERR_SPECIES) return set_error(h, "species index outside 1..NZ");
+    if (h != 0) return set_error(h, "device-side validation failed");
+    return AOK_OK;
+}
+
 extern "C" int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly, int64_t nOrb,
                                              const int64_t* iR, const int64_t* iY, int64_t L, int radial_kind,
                                              int precision, void* dX, void* dzeta, void* dD, const void* dP,
@@ -1043,6 +1281,11 @@ extern "C" int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ
         return set_error(AOK_ERR_INVALID, std::string(who) + ": dzeta and dD must both be given or both null");
     if (nRad > kNoAllocMaxRad || nOrb > kNoAllocMaxOrb)
         return set_error(AOK_ERR_UNSUPPORTED, std::string(who) + ": more than 64 radials or 256 orbitals");
+    // bounded before any product is formed, so nRad*K*NZ and the scratch size cannot wrap
+    if (K > kNoAllocMaxK || NZ > kNoAllocMaxNZ)
+        return set_error(AOK_ERR_UNSUPPORTED, std::string(who) + ": more than 64 primitive slots or 64 species");
+    if (nX > (int64_t)INT32_MAX)
+        return set_error(AOK_ERR_UNSUPPORTED, std::string(who) + ": nX above 2^31 - 1");
     const int64_t nY = (L + 1) * (L + 1);
     NoAllocMaps maps;
     memset(&maps, 0, sizeof(maps));
@@ -1058,9 +1301,11 @@ extern "C" int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ
         maps.iR[i] = (int)(iR[i] - 1);
         maps.iY[i] = (int)(iY[i] - 1);
     }
-    const int64_t ntab = nRad * K * NZ;
+    const int64_t ntab = nRad * K * NZ;  // <= 64^3
     const int64_t grid = (nX + kEvalThreads - 1) / kEvalThreads;
-    const size_t need = kNoAllocRowsOffset + sizeof(double) * 2 * (size_t)ntab * (size_t)grid;
+    // the partial rows are needed only for the (zeta, D) gradient; a dX-only call
+    // uses the index maps and the error word alone
+    const size_t need = kNoAllocRowsOffset + (dzeta ? sizeof(double) * 2 * (size_t)ntab * (size_t)grid : 0);
     if (need > kNoAllocScratchBytes)
         return set_error(AOK_ERR_UNSUPPORTED,
                          std::string(who) + ": nX = " + std::to_string(nX) + " needs " + std::to_string(need) +

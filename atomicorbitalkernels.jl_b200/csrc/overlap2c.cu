@@ -348,10 +348,22 @@ __device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sid
     return (int)((a - 1) * NZ + (c - 1));
 }
 
+// zeros for the three values of a left-out element (see BinBufs::zero3)
+__device__ __forceinline__ void zero_three(void* zero3, int bytes, int b) {
+    if (bytes == 8) {
+        double* d = (double*)zero3 + 3 * (size_t)b;
+        d[0] = d[1] = d[2] = 0.0;
+    } else {
+        float* f = (float*)zero3 + 3 * (size_t)b;
+        f[0] = f[1] = f[2] = 0.0f;
+    }
+}
+
 __global__ void __launch_bounds__(kBinThreads) k_bin_count(const int64_t* __restrict__ sidxA,
                                                             const int64_t* __restrict__ sidxB, int B, int NZ,
                                                             int chunk, int* __restrict__ blockhist,
-                                                            int* __restrict__ err) {
+                                                            int* __restrict__ err, void* zero3, void* zero3b,
+                                                            int zero3_bytes) {
     __shared__ int hist[kMaxPairs];
     const int np = NZ * NZ;
     for (int k = threadIdx.x; k < np; k += blockDim.x) hist[k] = 0;
@@ -359,7 +371,12 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const int64_t* __rest
     const int c0 = blockIdx.x * chunk, c1 = min(B, c0 + chunk);
     for (int b = c0 + threadIdx.x; b < c1; b += blockDim.x) {
         const int key = pair_key(sidxA, sidxB, b, c1, NZ, err);
-        if (key >= 0) atomicAdd(&hist[key], 1);
+        if (key >= 0) {
+            atomicAdd(&hist[key], 1);
+        } else {  // b < c1: a bad species index
+            if (zero3) zero_three(zero3, zero3_bytes, b);
+            if (zero3b) zero_three(zero3b, zero3_bytes, b);
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < np; k += blockDim.x) blockhist[(size_t)blockIdx.x * np + k] = hist[k];
@@ -465,10 +482,17 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
     }
 }
 
+// Single species (or no indices): every element in key 0, in batch order.  The
+// indices that are given are still range-checked (a bad one sets *err; the
+// element stays in the bin, and the kernels that read the index themselves
+// leave it out).
 __global__ void k_bin_identity(int B, int np, int* __restrict__ perm, int4* __restrict__ tiles,
-                               int* __restrict__ ntiles, int* __restrict__ tbase, unsigned* __restrict__ counter) {
+                               int* __restrict__ ntiles, int* __restrict__ tbase, unsigned* __restrict__ counter,
+                               const int64_t* __restrict__ sidxA, const int64_t* __restrict__ sidxB, int NZ,
+                               int* __restrict__ err) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     const int nt = (B + kTileB - 1) / kTileB;
+    if (b < B && (sidxA || sidxB)) (void)pair_key(sidxA, sidxB, b, B, NZ, err);
     if (b < B) perm[b] = b;
     if (b * kTileB < B) tiles[b] = make_int4(0, b * kTileB, min(kTileB, B - b * kTileB), 0);
     if (b <= np) tbase[b] = b == 0 ? 0 : nt;  // every element is in species pair 0
@@ -654,10 +678,11 @@ int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidx
     if (NZ == 1 || (!sidxA && !sidxB)) {
         const int np = NZ * NZ;
         k_bin_identity<<<(int)((std::max<int64_t>(B, np + 1) + 255) / 256), 256, 0, s>>>(
-            (int)B, np, bb.perm, bb.tiles, bb.ntiles, bb.tbase, bb.counter);
+            (int)B, np, bb.perm, bb.tiles, bb.ntiles, bb.tbase, bb.counter, sidxA, sidxB, NZ, bb.err);
         return cuda_status(cudaGetLastError(), "k_bin_identity");
     }
-    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.err);
+    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.err, bb.zero3,
+                                             bb.zero3b, bb.zero3_bytes);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_bin_count"));
     k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.perm, bb.tiles,
                                                bb.ntiles, bb.tbase, bb.counter, bb.err);

@@ -2,6 +2,7 @@
 reference's public API over the CUDA library.
 
   evaluate(basis, X[, ps, st])          src/orbitals/atomicorbitals.jl:148-190
+  evaluate(basis, Rs, sidx, ps, st)     atomicorbitals.jl:148-162 (indices already extracted)
   evaluate_ed(basis, X[, ps, st])       atomicorbitals.jl:192-231
   pullback_ps(dP, basis, X, ps, st)     atomicorbitals.jl:254-270
   rrule(evaluate, basis, X, ps, st)     atomicorbitals.jl:307-328
@@ -10,17 +11,23 @@ X is either a (3, nX) position array (species 1, as the reference's plain
 SVector input) or a PState batch (species from each point's label).  P is
 returned as a (nX, nOrb) column-major device tensor and dP as (nX, nOrb, 3)
 (the reference's Matrix{SVector{3}} memory layout).  Everything runs in one
-fused kernel per call; there is no CPU fallback.
+fused kernel per call; there is no CPU fallback.  Called with a radial basis
+(GaussianTypeRadials / SlaterTypeRadials), the three functions are the radial
+layer's own (radials.py).
 """
 import numpy as np
 import torch
 
-from . import _dev, _lib
-from .basis import PState, PStates, as_pstates, species_indices
+from . import _dev, _lib, radials
+from .basis import GSRadials, PState, PStates, as_pstates, species_indices
 from .overlap import NoTangent
 
 
-def _inputs(basis, X, FT):
+def _inputs(basis, X, FT, sidx=None):
+    if sidx is not None:
+        pos = _dev.to_colmajor(X, FT)
+        return pos, torch.as_tensor(np.ascontiguousarray(np.asarray(sidx, dtype=np.int64))).to("cuda"), \
+            int(pos.shape[1])
     if isinstance(X, PStates) or (isinstance(X, (list, tuple)) and len(X) and isinstance(X[0], PState)):
         Xs = as_pstates(X)
         pos = Xs.pos
@@ -61,10 +68,24 @@ def _plan(basis, st, FT):
                              _dev.prec_of(FT))
 
 
-def _run(basis, X, ps, st, grad):
+def _forms(args, kw):
+    """(sidx, ps, st) from the reference's call forms (X), (X, ps, st), (Rs, sidx, ps, st)."""
+    ps, st = kw.get("ps"), kw.get("st")
+    if len(args) == 3:
+        return args
+    if len(args) == 2:
+        return (None,) + tuple(args)
+    if len(args) == 1:
+        return None, args[0], st
+    if len(args) == 0:
+        return None, ps, st
+    raise _lib.ArgumentError("expected (basis, X[, ps, st]) or (basis, Rs, sidx, ps, st)")
+
+
+def _run(basis, X, ps, st, grad, sidx=None):
     _dev.require_cuda()
     FT = _ft(basis, ps, X)
-    pos, sidx, nX = _inputs(basis, X, FT)
+    pos, sidx, nX = _inputs(basis, X, FT, sidx)
     z, D = _params(basis, ps, FT)
     plan = _plan(basis, st, FT)
     nOrb = len(basis)
@@ -80,20 +101,29 @@ def _run(basis, X, ps, st, grad):
     return P
 
 
-def evaluate(basis, X, ps=None, st=None):
-    """P[j, i] = phi_i(X[j]) (device tensor, column-major (nX, nOrb))."""
-    return _run(basis, X, ps, st, False)
+def evaluate(basis, X, *args, **kw):
+    """P[j, i] = phi_i(X[j]) (device tensor, column-major (nX, nOrb)).  On a radial
+    basis (GaussianTypeRadials / SlaterTypeRadials) this is the radial layer's
+    evaluate, R (nX, nRad) at radii."""
+    if isinstance(basis, GSRadials):
+        return radials.evaluate(basis, X, *args, **kw)
+    sidx, ps, st = _forms(args, kw)
+    return _run(basis, X, ps, st, False, sidx)
 
 
-def evaluate_ed(basis, X, ps=None, st=None):
-    """(P, dP) with dP[j, i, :] the gradient w.r.t. the input coordinates."""
-    return _run(basis, X, ps, st, True)
+def evaluate_ed(basis, X, *args, **kw):
+    """(P, dP) with dP[j, i, :] the gradient w.r.t. the input coordinates; on a radial
+    basis, (R, dR/dr)."""
+    if isinstance(basis, GSRadials):
+        return radials.evaluate_ed(basis, X, *args, **kw)
+    sidx, ps, st = _forms(args, kw)
+    return _run(basis, X, ps, st, True, sidx)
 
 
-def _pullback(dP, basis, X, ps, st, want_x, want_ps):
+def _pullback(dP, basis, X, ps, st, want_x, want_ps, sidx=None):
     _dev.require_cuda()
     FT = _ft(basis, ps, X)
-    pos, sidx, nX = _inputs(basis, X, FT)
+    pos, sidx, nX = _inputs(basis, X, FT, sidx)
     z, D = _params(basis, ps, FT)
     plan = _plan(basis, st, FT)
     dPin = _dev.to_colmajor(dP, FT)
@@ -107,9 +137,13 @@ def _pullback(dP, basis, X, ps, st, want_x, want_ps):
     return dX, dz, dD
 
 
-def pullback_ps(dP, basis, X, ps, st):
-    """{'Rnl': {'zeta', 'D'}, 'Ylm': {}} (atomicorbitals.jl:254-270)."""
-    _, dz, dD = _pullback(dP, basis, X, ps, st, False, True)
+def pullback_ps(dP, basis, X, *args):
+    """{'Rnl': {'zeta', 'D'}, 'Ylm': {}} (atomicorbitals.jl:254-270); on a radial basis,
+    {'zeta', 'D'} of the radial layer (gtostoradials.jl:255-270)."""
+    if isinstance(basis, GSRadials):
+        return radials.pullback_ps(dP, basis, X, *args)
+    sidx, ps, st = _forms(args, {})
+    _, dz, dD = _pullback(dP, basis, X, ps, st, False, True, sidx)
     return {"Rnl": {"zeta": dz, "D": dD}, "Ylm": {}}
 
 

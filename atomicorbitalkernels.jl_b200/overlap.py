@@ -295,13 +295,48 @@ def pullback_ps(dS, orb, XA, XB, ps, st):
     return {"Rnl": {"zeta": dz, "D": dD}, "Ylm": {}}
 
 
-def rrule_batch_overlap(orb, XA, XB, ps, st):
+def position_pullback(dS, basis, XA, XB, ps=None, st=None):
+    """Position tangents of batch_overlap: (dXA, dXB), each (3, B) on the device, with
+    dXA[:, b] = sum dS[:, :, b] * dS_b/dA_b (the basis's lengthscale included).  No
+    reference counterpart (its rrule returns no position tangent).  `basis` is a
+    compiled CartesianGTOBasis, or the orbital basis with (ps, st) (coef compiled from
+    ps on the device).  dXB = -dXA: the overlap depends on A - B only."""
+    if ps is not None:
+        FT = _ps_dtype(ps, XA)
+        cob, _ = _compiled_from_ps(basis, ps, FT)
+    else:
+        cob = basis if isinstance(basis, CartesianGTOBasis) else compile_basis(basis)
+        FT = cob.zeta.dtype if torch.is_tensor(cob.zeta) else (
+            torch.float32 if np.asarray(cob.zeta).dtype == np.float32 else torch.float64)
+    XA, XB, sA, sB, B = _pstate_inputs(cob, XA, XB, FT)
+    dXA = _dev.colmajor_empty((3, B), FT)
+    dXB = _dev.colmajor_empty((3, B), FT)
+    if B == 0:
+        return dXA, dXB
+    _dev.require_cuda()
+    plan = _dev.plan_for(cob.ls, cob.K, cob.nspecies, _dev.prec_of(FT), B)
+    dSd = _dev.to_colmajor(dS, FT)
+    N = cob.nbf_total
+    if tuple(dSd.shape) != (N, N, B):
+        raise _lib.ArgumentError(f"dS must be (N, N, B) = {(N, N, B)}; got {tuple(dSd.shape)}")
+    pA, pB = _dev.to_colmajor(XA.pos, FT), _dev.to_colmajor(XB.pos, FT)
+    gA, gB = _dev_int64(sA), _dev_int64(sB)
+    _lib.check(_lib.load().aok_overlap2c_position_pullback(
+        plan.h, _dev.ptr(dXA), _dev.ptr(dXB), _dev.ptr(dSd), _dev.ptr(_dev.to_colmajor(cob.zeta, FT)),
+        _dev.ptr(_dev.to_colmajor(cob.coef, FT)), _dev.ptr(pA), _dev.ptr(pB), _dev.ptr(gA), _dev.ptr(gB), B,
+        float(cob.lengthscale), _dev.stream()))
+    return dXA, dXB
+
+
+def rrule_batch_overlap(orb, XA, XB, ps, st, positions=False):
     """rrule(batch_overlap, orb, XA, XB, ps, st) (overlap_2c_grad.jl:309-318).
 
     The forward (aok_overlap2c_rrule) also prepares the pullback's records and
     keeps the species bins, so that the pullback (aok_overlap_pullback_ps_rrule)
     runs only the pullback kernel and its reductions.  If another 2C call used
-    the plan in between, the pullback takes the full pullback_ps path."""
+    the plan in between, the pullback takes the full pullback_ps path.  With
+    positions=True the pullback also returns the position tangents (dXA, dXB)
+    (3, B) in the XA, XB slots (position_pullback) instead of NoTangent."""
     FT = _ps_dtype(ps, XA)
     XAp, XBp = as_pstates(XA), as_pstates(XB)
     stc = compile_struct(orb)
@@ -313,8 +348,11 @@ def rrule_batch_overlap(orb, XA, XB, ps, st):
     ns, K, NZ, N = stc["nshells"], stc["K"], stc["NZ"], stc["nbf_total"]
     S = _dev.colmajor_empty((N, N, B), FT)
     if B == 0:
-        return S, lambda dS: (NoTangent, NoTangent, NoTangent, NoTangent, pullback_ps(dS, orb, XA, XB, ps, st),
-                              NoTangent)
+        def _pb0(dS):
+            dX = (_dev.colmajor_empty((3, 0), FT), _dev.colmajor_empty((3, 0), FT)) if positions \
+                else (NoTangent, NoTangent)
+            return (NoTangent, NoTangent) + dX + (pullback_ps(dS, orb, XA, XB, ps, st), NoTangent)
+        return S, _pb0
     _dev.require_cuda()
     L = _lib.load()
     plan = _dev.plan_for(stc["ls"], K, NZ, _dev.prec_of(FT), B)
@@ -338,6 +376,9 @@ def rrule_batch_overlap(orb, XA, XB, ps, st):
         else:
             _lib.check(status)
             dps = {"Rnl": {"zeta": dz, "D": dD}, "Ylm": {}}
+        if positions:
+            dXA, dXB = position_pullback(dSd, orb, XA, XB, ps, st)
+            return (NoTangent, NoTangent, dXA, dXB, dps, NoTangent)
         return (NoTangent, NoTangent, NoTangent, NoTangent, dps, NoTangent)
 
     return S, _pb

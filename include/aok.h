@@ -48,6 +48,7 @@ extern "C" {
 
 typedef struct aok_plan aok_plan;        /* overlap plan (2C and 3C)          */
 typedef struct aok_orbitals aok_orbitals;/* orbital-evaluation plan           */
+typedef struct aok_radials aok_radials;  /* radial-layer plan                 */
 
 /* Thread-local message for the last failing call on this thread (no reference
  * counterpart: the Julia extension raises error(aok_last_error()) with it). */
@@ -191,6 +192,22 @@ int aok_overlap2c_pullback(aok_plan* plan, void* dcoef, void* dalpha, const void
                            int64_t B, double lengthscale, void* stream);
 
 /*
+ * Position pullback of the species-aware 2C overlap (no reference counterpart:
+ * the reference's rrule returns no position tangent and lists position
+ * gradients of the overlap as not implemented).  From the cotangent dS (N,N,B)
+ * of aok_overlap2c's output, dA, dB (3,B) = sum dS * dS/dA, sum dS * dS/dB with
+ * respect to the input positions (the lengthscale factor included); either may
+ * be NULL.  The overlap depends on A - B only, so dB = -dA.  zeta, coef,
+ * positions and species indices as aok_overlap2c.  Deterministic (fixed-order
+ * sums, no atomics on data).  A pair whose species index is outside 1..NZ gets
+ * dA = dB = 0 and sets the plan's error word (aok_plan_check).
+ */
+int aok_overlap2c_position_pullback(aok_plan* plan, void* dA, void* dB, const void* dS, const void* zeta,
+                                    const void* coef, const void* posA, const void* posB,
+                                    const int64_t* sidxA, const int64_t* sidxB, int64_t B,
+                                    double lengthscale, void* stream);
+
+/*
  * Closed-form VJP of the normalisation: (dD, dzeta_norm) from dcoef.
  * Replaces _compile_coef_pb (src/integrals/orbital/overlap_2c_grad.jl:251-286).
  */
@@ -240,12 +257,11 @@ int aok_orbitals_create(aok_orbitals** orb, int64_t nRad, int64_t K, int64_t NZ,
                         const int64_t* iY, int64_t L, int radial_kind, int precision);
 int aok_orbitals_destroy(aok_orbitals* orb);
 /* Synchronises `stream`, then reports (and clears) the orbitals' device error
- * word: AOK_ERR_SPECIES if aok_evaluate or aok_evaluate_ed met a species index
- * outside 1..NZ, or aok_evaluate_pullback did with NZ > 1.  No memory outside
- * the arguments is touched for such a point, but its outputs are not
- * meaningful: the forward evaluates it as species 1; the pullback leaves it
- * out of the (zeta, D) gradient (with NZ = 1 it counts as species 1, as every
- * point does) and may leave its dX unwritten.  The device half of the
+ * word: AOK_ERR_SPECIES if aok_evaluate, aok_evaluate_ed or
+ * aok_evaluate_pullback met a species index outside 1..NZ.  No memory outside
+ * the arguments is touched for such a point: the forward evaluates it as
+ * species 1 (its values are not meaningful); the pullback gives it dX = 0 and
+ * leaves it out of the (zeta, D) gradient.  The device half of the
  * reference's unknown-species error (_cgto_species_index,
  * src/integrals/orbital/overlap_2c.jl:148-158) for callers that pass device
  * species indices unchecked. */
@@ -284,6 +300,40 @@ int aok_evaluate_pullback(aok_orbitals* orb, void* dX, void* dzeta, void* dD,
                           void* stream);
 
 /*
+ * The radial layer on its own: GaussianTypeRadials / SlaterTypeRadials with
+ * nRad radials of K primitive slots for NZ species and radial powers poly[nRad]
+ * (host array; the layer's state st.poly, src/orbitals/gtostoradials.jl:14-46,
+ * 103-113).  Values are R[j,k] = r_j^poly[k] sum_m D[k,m,s_j] exp(-zeta[k,m,s_j] f(r_j))
+ * with f(r) = r^2 (Gaussian) or r (Slater).
+ */
+int aok_radials_create(aok_radials** rad, int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly,
+                       int radial_kind, int precision);
+int aok_radials_destroy(aok_radials* rad);
+/* Synchronises `stream`, then reports (and clears) the plan's device error word:
+ * AOK_ERR_SPECIES if a radial call met a species index outside 1..NZ (the device
+ * half of _z2i's unknown-species error, src/orbitals/gtostoradials.jl:58-62).  Such
+ * a point is evaluated as species 1 by the forward and left out of the pullback. */
+int aok_radials_check(aok_radials* rad, void* stream);
+/*
+ * R (nX,nRad) and, when dR is not NULL, dR/dr (nX,nRad) at the radii r (nX) for
+ * species indices sidx (nX, 1-based); zeta, D are ps.zeta, ps.D (nRad,K,NZ).
+ * Replaces evaluate / evaluate_ed(basis::GSRadials, r, sidx, ps, st)
+ * (src/orbitals/gtostoradials.jl:117-185: _rnl_val_ka!, _rnl_ed_ka!).
+ */
+int aok_radials_evaluate(aok_radials* rad, void* R, void* dR, const void* r, const int64_t* sidx,
+                         const void* zeta, const void* D, int64_t nX, void* stream);
+/*
+ * Parameter pullback of the radial layer: dzeta, dD (nRad,K,NZ) from the
+ * cotangent dRin (nX,nRad) of R.  Replaces pullback_ps(dR, basis::GSRadials, r,
+ * sidx, ps, st) (src/orbitals/gtostoradials.jl:232-267, _gtostoradials_pb_ka!):
+ * the points are binned by species and reduced per (radial, primitive) slot with
+ * per-unit FP64 partial rows summed in a fixed order (deterministic, no atomics
+ * on data).
+ */
+int aok_radials_pullback(aok_radials* rad, void* dzeta, void* dD, const void* dRin, const void* r,
+                         const int64_t* sidx, const void* zeta, const void* D, int64_t nX, void* stream);
+
+/*
  * Allocation-free variant of aok_evaluate_pullback.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory when
  * they need the pullback -- a host framework that owns the whole device
@@ -293,13 +343,17 @@ int aok_evaluate_pullback(aok_orbitals* orb, void* dX, void* dzeta, void* dD,
  * aok_orbitals_create) instead of a plan, and allocates nothing: its scratch
  * (index maps, error word, per-block FP64 partial rows) is one static device
  * array of AOK_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps
- * until the process exits.  Limits: nRad <= 64, nOrb <= 256, and
- * 4096 + 16 * nRad*K*NZ * ceil(nX / 128) bytes must fit the scratch; larger
- * requests return AOK_ERR_UNSUPPORTED with the sizes in the message.  The
- * first call on a device looks up the array's device address (make it before
- * any stream capture).  All calls share the array and overwrite it, so calls
- * that may overlap on the GPU race and must be serialised by the caller.
- * Arguments and results otherwise as aok_evaluate_pullback.
+ * until the process exits.  Limits: nRad <= 64, nOrb <= 256, K <= 64,
+ * NZ <= 64, nX < 2^31, and, when the (zeta, D) gradient is asked for,
+ * 4096 + 16 * nRad*K*NZ * ceil(nX / 128) bytes must fit the scratch (a
+ * dX-only call needs no partial rows); larger requests return
+ * AOK_ERR_UNSUPPORTED with the sizes in the message.  The first call on a
+ * device looks up the array's device address (make it before any stream
+ * capture).  All calls share the array and overwrite it, so calls that may
+ * overlap on the GPU race and must be serialised by the caller.  Arguments
+ * and results otherwise as aok_evaluate_pullback: a point whose species index
+ * is outside 1..NZ gets dX = 0, adds nothing to (dzeta, dD), and sets the
+ * scratch's error word, which aok_evaluate_pullback_noalloc_check reports.
  */
 #define AOK_NOALLOC_SCRATCH_BYTES (8u << 20)
 int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ, const int64_t* poly,
@@ -308,6 +362,14 @@ int aok_evaluate_pullback_noalloc(int64_t nRad, int64_t K, int64_t NZ, const int
                                   void* dD, const void* dP, const void* X, const int64_t* sidx,
                                   const void* zeta, const void* D, int64_t nX,
                                   double lengthscale, void* stream);
+/* The error report of aok_evaluate_pullback_noalloc (no reference counterpart;
+ * its role is that of aok_orbitals_check): synchronises `stream`, then reads
+ * and clears the static scratch's error word on the current device and returns
+ * AOK_ERR_SPECIES if the allocation-free pullback met a species index outside
+ * 1..NZ since the last check.  Each allocation-free call clears the word when
+ * it starts, so check after the call and before the next one.  Allocates
+ * nothing; AOK_OK if no allocation-free call has run on the device. */
+int aok_evaluate_pullback_noalloc_check(void* stream);
 
 #ifdef __cplusplus
 }

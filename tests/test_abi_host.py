@@ -136,7 +136,7 @@ def test_orbital_entry_points_reject_bad_arguments_without_gpu():
     iR, iY = np.asarray(orb.radidx), np.asarray(orb.ylmidx)
     fake = ctypes.c_void_p(256)  # never dereferenced: every call below is refused on the host
 
-    def call(nRad=nRad, iR=iR, iY=iY, Lh=orb.L, prec=_lib.AOK_PREC_F64, nX=1000, dzeta=fake, dD=fake):
+    def call(nRad=nRad, iR=iR, iY=iY, Lh=orb.L, prec=_lib.AOK_PREC_F64, nX=1000, dzeta=fake, dD=fake, K=K, NZ=NZ):
         return L.aok_evaluate_pullback_noalloc(
             nRad, K, NZ, _lib.int64_array(np.zeros(nRad, np.int64)), len(iR), _lib.int64_array(iR),
             _lib.int64_array(iY), Lh, orb.Rnl.kind, prec, fake, dzeta, dD, fake, fake, fake, fake, fake, nX, 1.0,
@@ -156,3 +156,11 @@ def test_orbital_entry_points_reject_bad_arguments_without_gpu():
     assert call(dD=None) == _lib.AOK_ERR_INVALID
     assert call(nX=1 << 21) == _lib.AOK_ERR_UNSUPPORTED
     assert b"scratch" in L.aok_last_error()
+    # sizes whose products would wrap a 64-bit scratch size are refused before any product is formed
+    assert call(K=1 << 40, NZ=1 << 40) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"64 primitive slots" in L.aok_last_error()
+    assert call(NZ=65) == _lib.AOK_ERR_UNSUPPORTED
+    assert call(nX=1 << 31) == _lib.AOK_ERR_UNSUPPORTED
+    assert b"2^31" in L.aok_last_error()
+    # the check call allocates nothing and has nothing to report before any allocation-free call
+    assert L.aok_evaluate_pullback_noalloc_check(None) in (_lib.AOK_OK, _lib.AOK_ERR_CUDA)

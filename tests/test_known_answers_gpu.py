@@ -146,3 +146,25 @@ def test_unit_self_overlap_of_normalised_s_p_shells(FT, tol):
             assert np.max(np.abs(d - 1.0)) < tol
             checked += nbf[k]
     assert checked > 100
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-13), (torch.float32, 2e-6)])
+def test_evaluate_harmonics_follow_sphericart_definition(FT, tol):
+    """With zeta = 0 and D = 1 every radial is 1, so evaluate returns the solid harmonics
+    themselves: the GPU kernel's Z_lm for l <= 4, m != 0 signs included, equal SpheriCart's
+    published definition (helpers.sphericart_solid_harmonics), with no oracle in the loop."""
+    from helpers import sphericart_solid_harmonics
+    ls = np.arange(5, dtype=np.int64)
+    sb = W.SpeciesBasis(ls=ls, zeta=np.zeros((5, 1, 1), order="F"), D=np.ones((5, 1, 1), order="F"),
+                        nprim=np.ones((5, 1), np.int64))
+    orb = aok.orbitals_from_species_basis(sb)
+    assert orb.L == 4
+    X = np.random.default_rng(41).normal(size=(3, 4096)) * 1.7
+    npft = np.float32 if FT == torch.float32 else np.float64
+    ps = {"Rnl": {"zeta": sb.zeta.astype(npft), "D": sb.D.astype(npft)}, "Ylm": {}}
+    P = aok.evaluate(orb, X.astype(npft), ps, aok.initialstates(orb)).cpu().numpy()
+    Zs = sphericart_solid_harmonics(X, 4)
+    ref = Zs[:, np.asarray(orb.ylmidx) - 1]
+    assert P.shape == ref.shape
+    scale = np.abs(ref).max(axis=0)
+    assert np.max(np.abs(P - ref) / scale) < tol

@@ -147,27 +147,80 @@ def test_orbitals_check_reports_bad_device_species():
         dP = _dev.colmajor_empty((3, n, len(orb)), FT)
         dz = _dev.colmajor_empty(b.zeta.shape, FT)
         dD = _dev.colmajor_empty(b.zeta.shape, FT)
+        dX = torch.full((n, 3), 7.0, dtype=FT, device="cuda")  # poisoned: every entry must be written
         dPd = _dev.to_colmajor(dPin[:n] if n == nX else np.delete(dPin, bad_at, axis=0), FT)
         sp = ctypes.c_void_p(sd.data_ptr())
         _lib.check(L.aok_evaluate_ed(plan.h, _dev.ptr(P), _dev.ptr(dP), _dev.ptr(Xd), sp, _dev.ptr(z), _dev.ptr(D),
                                      n, 1.0, _dev.stream()))
-        _lib.check(L.aok_evaluate_pullback(plan.h, None, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(dPd), _dev.ptr(Xd),
-                                           sp, _dev.ptr(z), _dev.ptr(D), n, 1.0, _dev.stream()))
-        return P.cpu().numpy(), dz.cpu().numpy(), dD.cpu().numpy(), L.aok_orbitals_check(plan.h, _dev.stream())
+        _lib.check(L.aok_evaluate_pullback(plan.h, ctypes.c_void_p(dX.data_ptr()), _dev.ptr(dz), _dev.ptr(dD),
+                                           _dev.ptr(dPd), _dev.ptr(Xd), sp, _dev.ptr(z), _dev.ptr(D), n, 1.0,
+                                           _dev.stream()))
+        return (P.cpu().numpy(), dz.cpu().numpy(), dD.cpu().numpy(), dX.cpu().numpy(),
+                L.aok_orbitals_check(plan.h, _dev.stream()))
 
     bad_at = [3, 10, 2999]
-    P0, _, _, st = run(X, sidx)
+    P0, _, _, _, st = run(X, sidx)
     assert st == 0
     bad = sidx.copy()
     bad[bad_at] = [0, b.NZ + 1, -5]
-    P1, dz1, dD1, st = run(X, bad)
+    P1, dz1, dD1, dX1, st = run(X, bad)
     assert st == _lib.AOK_ERR_SPECIES
     assert b"species" in L.aok_last_error()
     assert L.aok_orbitals_check(plan.h, _dev.stream()) == 0  # the error word was cleared
     keep = np.ones(nX, bool)
     keep[bad_at] = False
     assert np.array_equal(P1[keep], P0[keep])
-    # the gradient with the bad points equals the gradient without them
-    _, dz2, dD2, st = run(np.asfortranarray(X[:, keep]), sidx[keep])
+    # the gradient with the bad points equals the gradient without them; their dX is zero
+    _, dz2, dD2, dX2, st = run(np.asfortranarray(X[:, keep]), sidx[keep])
     assert st == 0
     assert rel_fro(dz1, dz2) < 1e-12 and rel_fro(dD1, dD2) < 1e-12
+    assert np.array_equal(dX1[bad_at], np.zeros((3, 3)))
+    assert rel_fro(dX1[keep], dX2) < 1e-12
+
+
+@pytest.mark.parametrize("with_params", [True, False])
+def test_orbitals_check_single_species_bad_index(with_params):
+    """With one species the points are not binned by species, yet a bad index is still
+    reported, and the pullback (slot-parallel with (zeta, D), per point without) gives
+    the point dX = 0 and leaves it out of the (zeta, D) gradient."""
+    import ctypes
+
+    from aok_b200 import _dev, _lib
+    FT = torch.float64
+    b1 = W.config0_basis()  # one species
+    orb = aok.orbitals_from_species_basis(b1)
+    nX = 2000
+    X, _ = W.config1_points(nX=nX, seed=17)
+    sidx = np.ones(nX, np.int64)
+    plan = _dev.OrbPlan(b1.zeta.shape[0], b1.K, 1, orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L,
+                        orb.Rnl.kind, _dev.prec_of(FT))
+    L = _lib.load()
+    z, D = _dev.to_colmajor(b1.zeta, FT), _dev.to_colmajor(b1.D, FT)
+    dPin = np.random.default_rng(18).standard_normal((nX, len(orb)))
+    bad_at = [0, 777, 1999]
+
+    def run(Xh, sh, dPh):
+        n = Xh.shape[1]
+        Xd, sd = _dev.to_colmajor(Xh, FT), torch.as_tensor(np.ascontiguousarray(sh)).cuda()
+        dz = _dev.colmajor_empty(b1.zeta.shape, FT)
+        dD = _dev.colmajor_empty(b1.zeta.shape, FT)
+        dX = torch.full((n, 3), 7.0, dtype=FT, device="cuda")
+        _lib.check(L.aok_evaluate_pullback(plan.h, ctypes.c_void_p(dX.data_ptr()),
+                                           _dev.ptr(dz) if with_params else None,
+                                           _dev.ptr(dD) if with_params else None, _dev.ptr(_dev.to_colmajor(dPh, FT)),
+                                           _dev.ptr(Xd), ctypes.c_void_p(sd.data_ptr()), _dev.ptr(z), _dev.ptr(D), n,
+                                           1.0, _dev.stream()))
+        return dz.cpu().numpy(), dD.cpu().numpy(), dX.cpu().numpy(), L.aok_orbitals_check(plan.h, _dev.stream())
+
+    bad = sidx.copy()
+    bad[bad_at] = [2, 0, -1]
+    dz1, dD1, dX1, st = run(X, bad, dPin)
+    assert st == _lib.AOK_ERR_SPECIES
+    keep = np.ones(nX, bool)
+    keep[bad_at] = False
+    dz2, dD2, dX2, st = run(np.asfortranarray(X[:, keep]), sidx[keep], dPin[keep])
+    assert st == 0
+    assert np.array_equal(dX1[bad_at], np.zeros((3, 3)))
+    assert rel_fro(dX1[keep], dX2) < 1e-12
+    if with_params:
+        assert rel_fro(dz1, dz2) < 1e-12 and rel_fro(dD1, dD2) < 1e-12
