@@ -31,7 +31,7 @@ EXPORTS = [
     "aok_plan_check", "aok_plan_set_basis", "aok_plan_set_graph", "aok_plan_autotune", "aok_plan_timing_enable", "aok_plan_timing_read", "aok_measure_fma_peak", "aok_compile_coef", "aok_species_index", "aok_overlap2c", "aok_overlap2c_gb", "aok_overlap3c_gb",
     "aok_overlap2c_pullback", "aok_overlap2c_position_pullback", "aok_compile_coef_pullback",
     "aok_overlap_pullback_ps",
-    "aok_overlap2c_rrule", "aok_overlap_pullback_ps_rrule",
+    "aok_overlap2c_rrule", "aok_overlap_pullback_ps_rrule", "aok_overlap_pullback_ps_rrule_residual",
     "aok_orbitals_create", "aok_orbitals_destroy", "aok_orbitals_check", "aok_evaluate", "aok_evaluate_ed",
     "aok_evaluate_pullback", "aok_radials_create", "aok_radials_destroy", "aok_radials_check",
     "aok_radials_evaluate", "aok_radials_pullback",
@@ -96,6 +96,8 @@ def load():
     L.aok_overlap_pullback_ps.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_overlap2c_rrule.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_overlap_pullback_ps_rrule.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
+    L.aok_overlap_pullback_ps_rrule_residual.argtypes = [vp, vp, vp, vp, vp, dbl, vp, vp, vp, vp, vp, vp, i64, dbl,
+                                                         vp]
     L.aok_orbitals_create.argtypes = [ctypes.POINTER(vp), i64, i64, i64, pi64, i64, pi64, pi64, i64, cint, cint]
     L.aok_orbitals_destroy.argtypes = [vp]
     L.aok_orbitals_check.argtypes = [vp, vp]

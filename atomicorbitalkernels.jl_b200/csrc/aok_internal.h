@@ -169,8 +169,9 @@ constexpr int kBinMaxBlocksHost = 512;
 int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
                     cudaStream_t s);
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s);
-int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* D,
-                       const void* posA, const void* posB, double lengthscale, cudaStream_t s);
+int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
+                       const void* zeta, const void* D, const void* posA, const void* posB, double lengthscale,
+                       cudaStream_t s);
 int ensure_pb_buffers(aok_plan* p);
 int launch_overlap2c_dpos(aok_plan* p, void* dA, void* dB, const void* dS, const void* zeta, const void* coef,
                           const int64_t* sidxA, const int64_t* sidxB, const void* posA, const void* posB, int64_t B,
@@ -191,10 +192,12 @@ int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef
                            const void* D, const void* dalpha_add, cudaStream_t s);
 
 // overlap2c_bwd*.cu
-int launch_pb_f32(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
-                  const void* D, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
-int launch_pb_f64(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
-                  const void* D, const void* posA, const void* posB, double lengthscale, cudaStream_t s);
+int launch_pb_f32(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
+                  const void* zeta, const void* coef, const void* D, const void* posA, const void* posB,
+                  double lengthscale, cudaStream_t s);
+int launch_pb_f64(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
+                  const void* zeta, const void* coef, const void* D, const void* posA, const void* posB,
+                  double lengthscale, cudaStream_t s);
 int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
                         const void* D, const int64_t* sidxA, const int64_t* sidxB, const void* posA,
                         const void* posB, int64_t B, double lengthscale, int keep_absent, cudaStream_t s);

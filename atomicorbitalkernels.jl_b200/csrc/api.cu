@@ -493,10 +493,11 @@ int aok_overlap2c_rrule(aok_plan* p, void* out, const void* zeta, const void* D,
     return AOK_OK;
 }
 
-int aok_overlap_pullback_ps_rrule(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta,
-                                  const void* D, const void* posA, const void* posB, const int64_t* sidxA,
-                                  const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
-    static const char* who = "aok_overlap_pullback_ps_rrule";
+// The rrule pullback with the cotangent dS, or alpha (dS - dS2) when dS2 is given.
+static int pullback_ps_rrule(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* dS2, double alpha,
+                             const void* zeta, const void* D, const void* posA, const void* posB,
+                             const int64_t* sidxA, const int64_t* sidxB, int64_t B, double lengthscale, void* stream,
+                             const char* who) {
     if (!p) return set_error(AOK_ERR_INVALID, std::string(who) + ": null plan");
     if (!dzeta || !dD || !zeta || !D) return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
     AOK_TRY(check_batch(p, B, who));
@@ -514,7 +515,24 @@ int aok_overlap_pullback_ps_rrule(aok_plan* p, void* dzeta, void* dD, const void
     if (!match)
         return set_error(AOK_ERR_INVALID, std::string(who) + ": no matching aok_overlap2c_rrule on this plan "
                                                              "(other arguments, or another 2C call in between)");
-    return launch_pb_prepared(p, dD, dzeta, dS, zeta, D, posA, posB, lengthscale, s);
+    return launch_pb_prepared(p, dD, dzeta, dS, dS2, alpha, zeta, D, posA, posB, lengthscale, s);
+}
+
+int aok_overlap_pullback_ps_rrule(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta,
+                                  const void* D, const void* posA, const void* posB, const int64_t* sidxA,
+                                  const int64_t* sidxB, int64_t B, double lengthscale, void* stream) {
+    return pullback_ps_rrule(p, dzeta, dD, dS, nullptr, 1.0, zeta, D, posA, posB, sidxA, sidxB, B, lengthscale,
+                             stream, "aok_overlap_pullback_ps_rrule");
+}
+
+int aok_overlap_pullback_ps_rrule_residual(aok_plan* p, void* dzeta, void* dD, const void* S, const void* T,
+                                           double alpha, const void* zeta, const void* D, const void* posA,
+                                           const void* posB, const int64_t* sidxA, const int64_t* sidxB, int64_t B,
+                                           double lengthscale, void* stream) {
+    static const char* who = "aok_overlap_pullback_ps_rrule_residual";
+    if (B > 0 && (!S || !T)) return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    return pullback_ps_rrule(p, dzeta, dD, S, T, alpha, zeta, D, posA, posB, sidxA, sidxB, B, lengthscale, stream,
+                             who);
 }
 
 int aok_overlap_pullback_ps(aok_plan* p, void* dzeta, void* dD, const void* dS, const void* zeta, const void* D,

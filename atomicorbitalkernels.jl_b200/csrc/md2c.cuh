@@ -176,4 +176,28 @@ __device__ __forceinline__ void md_cotangent(FT (&G)[(LA + 1) * (LB + 1)], const
     }
 }
 
+// The same with the cotangent given as the difference g = a - b of two arrays
+// (read at the same positions): the cotangent of a squared-residual loss without
+// materialising it (its scale is applied to the final gradient).
+template <int LA, int LB, typename FT>
+__device__ __forceinline__ void md_cotangent_diff(FT (&G)[(LA + 1) * (LB + 1)], const FT (&AB)[3], const FT* a,
+                                                  const FT* b, int N) {
+    using TB = MdTab<LA, LB>;
+    constexpr auto tb = TB::make();
+    FT xp[3][TB::W + 1];
+    md_powers<TB::W, FT>(xp, AB);
+#pragma unroll
+    for (int m = 0; m < TB::NM; ++m) G[m] = FT(0);
+    FT gv = FT(0);
+#pragma unroll
+    for (int i = 0; i < TB::T; ++i) {
+        const MdTerm e = tb.t[i];
+        if (i == 0 || tb.t[i - 1].lin != e.lin) {
+            const int o = (e.lin / TB::NA) * N + e.lin % TB::NA;
+            gv = a[o] - b[o];
+        }
+        if (e.cst != 0) G[e.m] = fma(gv * ((xp[0][e.px] * xp[1][e.py]) * xp[2][e.pz]), FT(e.cst), G[e.m]);
+    }
+}
+
 }  // namespace aok

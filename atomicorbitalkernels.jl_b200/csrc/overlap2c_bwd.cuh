@@ -249,6 +249,7 @@ template <> struct PBLoad<double> {
 template <typename FT>
 struct PbParams {
     const FT* dS;
+    const FT* dS2;         // non-null: the cotangent is dS - dS2 (scaled by alpha in the reductions)
     const FT* posA;
     const FT* posB;
     FT scale;
@@ -320,8 +321,11 @@ __device__ __noinline__ Sums4<FT> pb_unit(const PbParams<FT>& P, PbWarpSmem<FT>&
             if (e < e1) {
                 Geo<FT> geo;
                 load_geo(geo, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.scale, P.use_scale != 0);
-                const FT* gs = P.dS + (size_t)b * P.N * P.N + (size_t)P.boff[sb] * P.N + P.boff[sa];
-                md_cotangent<LA, LB, FT>(G, geo.AB, gs, P.N);
+                const size_t go = (size_t)b * P.N * P.N + (size_t)P.boff[sb] * P.N + P.boff[sa];
+                if (P.dS2)
+                    md_cotangent_diff<LA, LB, FT>(G, geo.AB, P.dS + go, P.dS2 + go, P.N);
+                else
+                    md_cotangent<LA, LB, FT>(G, geo.AB, P.dS + go, P.N);
                 R2 = geo.R2;
                 if constexpr (sizeof(FT) == 4) R2lo = geo.R2lo;
             } else {
@@ -587,14 +591,15 @@ __device__ __forceinline__ double pb_slot_sum(const double* __restrict__ rows, c
 template <typename FT>
 __global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, const double* __restrict__ rows,
                             const int* __restrict__ itemidx, const FT* __restrict__ zeta, const FT* __restrict__ coef,
-                            int ns, int K, int NZ, int nitems) {
+                            int ns, int K, int NZ, int nitems, double alpha) {
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int S = ns * K * NZ;
     if (wid >= 2 * S) return;
     const int kind = wid / S, slot = wid % S;
     const int s = slot % ns, kk = (slot / ns) % K, sigma = slot / (ns * K);
-    const double sum = pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, kind, s, kk, sigma, lane);
+    const double sum =
+        alpha * pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, kind, s, kk, sigma, lane);
     if (lane == 0) {
         if (kind == 0) dcoef[slot] = (FT)sum;
         else dalpha[slot] = (FT)sum;
@@ -608,7 +613,7 @@ template <typename FT>
 __global__ void k_pb_reduce_ps(FT* __restrict__ dD, FT* __restrict__ dz, const double* __restrict__ rows,
                                const int* __restrict__ itemidx, const FT* __restrict__ zeta,
                                const FT* __restrict__ coef, const FT* __restrict__ D, const int* __restrict__ ls,
-                               int ns, int K, int NZ, int nitems) {
+                               int ns, int K, int NZ, int nitems, double alpha) {
     extern __shared__ double red[];  // dcoef[K], dalpha[K], VJP terms [2][K*K]
     __shared__ double s_nsq;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -620,7 +625,7 @@ __global__ void k_pb_reduce_ps(FT* __restrict__ dD, FT* __restrict__ dz, const d
     }
     for (int w = warp - 1; w >= 0 && w < 2 * K; w += nw - 1) {
         const double v = pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, w / K, s, w % K, sigma, lane);
-        if (lane == 0) red[w] = v;
+        if (lane == 0) red[w] = alpha * v;  // the pullback is linear in the cotangent
     }
     __syncthreads();
     if (warp == 0)
@@ -635,14 +640,17 @@ template <typename FT> constexpr int pb_min_blocks() { return sizeof(FT) == 4 ? 
 
 // Launches the pullback kernel and its reductions.  D == nullptr: kernel-level
 // pullback, out0/out1 = (dcoef, dalpha).  Otherwise the parameter pullback,
-// out0/out1 = (dD, dzeta).
+// out0/out1 = (dD, dzeta).  The cotangent is dS, or alpha (dS - dS2) when dS2 is
+// given (alpha scales the reduced gradients).
 template <typename FT, int THREADS>
-inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
-                     const void* D, const void* posA, const void* posB, double lengthscale, cudaStream_t s) {
+inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
+                     const void* zeta, const void* coef, const void* D, const void* posA, const void* posB,
+                     double lengthscale, cudaStream_t s) {
     constexpr int MINB = pb_min_blocks<FT>();
     PbParams<FT> P;
     memset(&P, 0, sizeof(P));
     P.dS = (const FT*)dS;
+    P.dS2 = (const FT*)dS2;
     P.posA = (const FT*)posA;
     P.posB = (const FT*)posB;
     P.scale = (FT)lengthscale;
@@ -678,13 +686,13 @@ inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const 
         if (sm > 48 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "pullback: K too large");
         k_pb_reduce_ps<FT><<<(int)(p->ns * p->NZ), 256, sm, s>>>(
             (FT*)out0, (FT*)out1, (const double*)p->d_pb_rows, p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
-            (const FT*)D, p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems);
+            (const FT*)D, p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems, alpha);
         return cuda_status(cudaGetLastError(), "k_pb_reduce_ps");
     }
     const int S = (int)(p->ns * p->K * p->NZ);
     k_pb_reduce<FT><<<(2 * S * 32 + 255) / 256, 256, 0, s>>>((FT*)out0, (FT*)out1, (const double*)p->d_pb_rows,
                                                             p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
-                                                            (int)p->ns, (int)p->K, (int)p->NZ, p->nitems);
+                                                            (int)p->ns, (int)p->K, (int)p->NZ, p->nitems, alpha);
     return cuda_status(cudaGetLastError(), "k_pb_reduce");
 }
 

@@ -336,7 +336,9 @@ def rrule_batch_overlap(orb, XA, XB, ps, st, positions=False):
     runs only the pullback kernel and its reductions.  If another 2C call used
     the plan in between, the pullback takes the full pullback_ps path.  With
     positions=True the pullback also returns the position tangents (dXA, dXB)
-    (3, B) in the XA, XB slots (position_pullback) instead of NoTangent."""
+    (3, B) in the XA, XB slots (position_pullback) instead of NoTangent.  The
+    pullback's `residual(T, alpha)` gives the parameter gradient of
+    (alpha / 2) * sum (S - T)^2 without forming the cotangent in memory."""
     FT = _ps_dtype(ps, XA)
     XAp, XBp = as_pstates(XA), as_pstates(XB)
     stc = compile_struct(orb)
@@ -381,4 +383,22 @@ def rrule_batch_overlap(orb, XA, XB, ps, st, positions=False):
             return (NoTangent, NoTangent, dXA, dXB, dps, NoTangent)
         return (NoTangent, NoTangent, NoTangent, NoTangent, dps, NoTangent)
 
+    def _residual(T, alpha=2.0):
+        """{'Rnl': {'zeta', 'D'}, 'Ylm': {}}: the pullback of the cotangent alpha * (S - T),
+        i.e. the (zeta, D) gradient of (alpha / 2) * sum (S - T)^2, with the difference
+        taken inside the pullback kernel (aok_overlap_pullback_ps_rrule_residual)."""
+        Td = _dev.to_colmajor(T, FT)
+        if tuple(Td.shape) != tuple(S.shape):
+            raise _lib.ArgumentError(f"T must have the shape of S {tuple(S.shape)}; got {tuple(Td.shape)}")
+        dz = _dev.colmajor_empty((ns, K, NZ), FT)
+        dD = _dev.colmajor_empty((ns, K, NZ), FT)
+        status = L.aok_overlap_pullback_ps_rrule_residual(
+            plan.h, _dev.ptr(dz), _dev.ptr(dD), _dev.ptr(S), _dev.ptr(Td), float(alpha), _dev.ptr(zeta),
+            _dev.ptr(D), _dev.ptr(dA), _dev.ptr(dB), _dev.ptr(gA), _dev.ptr(gB), B, ls, _dev.stream())
+        if status == _lib.AOK_ERR_INVALID:  # the plan served another call since the forward
+            return pullback_ps(alpha * (S - Td), orb, XA, XB, ps, st)
+        _lib.check(status)
+        return {"Rnl": {"zeta": dz, "D": dD}, "Ylm": {}}
+
+    _pb.residual = _residual
     return S, _pb

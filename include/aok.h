@@ -244,6 +244,21 @@ int aok_overlap_pullback_ps_rrule(aok_plan* plan, void* dzeta, void* dD, const v
                                   const void* zeta, const void* D, const void* posA,
                                   const void* posB, const int64_t* sidxA, const int64_t* sidxB,
                                   int64_t B, double lengthscale, void* stream);
+/*
+ * The rrule pullback for a squared-residual loss, with the cotangent formed on
+ * the fly: dS = alpha * (S - T), S the forward's output and T a target of the
+ * same layout (N,N,B) -- the gradient of (alpha/2) * sum (S - T)^2, e.g.
+ * alpha = 2 for L = sum (S - T)^2.  Same conditions and results as
+ * aok_overlap_pullback_ps_rrule given that dS, without writing or reading dS
+ * (the difference is taken in the kernel that reads the cotangent, alpha is
+ * applied to the reduced gradient).  It fuses the loss's cotangent into the
+ * pullback of rrule(batch_overlap, ...) (src/integrals/orbital/overlap_2c_grad.jl:309-318).
+ */
+int aok_overlap_pullback_ps_rrule_residual(aok_plan* plan, void* dzeta, void* dD, const void* S,
+                                           const void* T, double alpha, const void* zeta,
+                                           const void* D, const void* posA, const void* posB,
+                                           const int64_t* sidxA, const int64_t* sidxB, int64_t B,
+                                           double lengthscale, void* stream);
 
 /*
  * Orbital-evaluation plan: radial spec (nRad radials, K slots, NZ species,

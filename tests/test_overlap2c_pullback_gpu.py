@@ -151,3 +151,29 @@ def test_pullback_deterministic():
     g1 = aok.overlap_pullback_ps(dS.astype(np.float32), orb, XA, XB, ps, aok.initialstates(orb))
     g2 = aok.overlap_pullback_ps(dS.astype(np.float32), orb, XA, XB, ps, aok.initialstates(orb))
     assert torch.equal(g1["Rnl"]["zeta"], g2["Rnl"]["zeta"]) and torch.equal(g1["Rnl"]["D"], g2["Rnl"]["D"])
+
+
+@pytest.mark.parametrize("FT", [torch.float64, torch.float32])
+def test_rrule_residual_pullback_equals_the_separate_cotangent(FT):
+    """The fused squared-residual pullback (cotangent alpha (S - T) formed inside the kernel)
+    equals the rrule pullback given dS = S - T and scaled by alpha, bit for bit for alpha = 2
+    (a power of two commutes with every rounding), and within round-off for alpha = 0.7."""
+    b, pr, _ = _inputs(2000, seed=29)
+    np_ft = np.float64 if FT == torch.float64 else np.float32
+    orb, cob, XA, XB = _cob_and_states(b, pr, FT)
+    ps = {"Rnl": {"zeta": b.zeta.astype(np_ft), "D": b.D.astype(np_ft)}, "Ylm": {}}
+    st = aok.initialstates(orb)
+    zt, Dt = aok.workloads.config3_target(b)
+    T = aok.batch_overlap(orb, XA, XB, {"Rnl": {"zeta": zt.astype(np_ft), "D": Dt.astype(np_ft)}, "Ylm": {}}, st)
+    T = T.to("cuda")
+    for alpha, exact in ((2.0, True), (0.7, False)):
+        S, pb = aok.rrule_batch_overlap(orb, XA, XB, ps, st)
+        g_res = pb.residual(T, alpha)
+        g_sep = pb((S - aok.colmajor_empty(tuple(S.shape), FT).copy_(T)))[4]
+        for k in ("zeta", "D"):
+            ref = alpha * g_sep["Rnl"][k]
+            if exact:
+                assert torch.equal(g_res["Rnl"][k], ref)
+            else:
+                tol = 1e-12 if FT == torch.float64 else 2e-6
+                assert rel_fro(g_res["Rnl"][k].cpu().numpy(), ref.cpu().numpy()) < tol
