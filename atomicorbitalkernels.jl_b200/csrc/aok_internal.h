@@ -68,9 +68,6 @@ struct aok_plan {
     void* d_items3 = nullptr;
     void* d_order3 = nullptr;        // per call: each panel's items, heaviest first (k_order3c)
     int nitems3 = 0;
-    alignas(8) unsigned char panels3_raw[528] = {};
-    size_t slab_stride3 = 0;
-    size_t smem3 = 0;
     // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated
     // launch chain, the arguments it was captured with, a private capture stream
     bool graph_on = false;

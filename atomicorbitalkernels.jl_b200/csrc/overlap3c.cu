@@ -1,5 +1,5 @@
 // overlap3c.cu -- 3-center overlap host side: primitive-triple records, the
-// page-panel schedule, and the aok_overlap3c_gb entry point.  The kernel is in
+// item list, and the aok_overlap3c_gb entry point.  The kernel is in
 // overlap3c_kernel.cuh (one instantiation per precision: overlap3c_f32.cu,
 // overlap3c_f64.cu).
 #include <algorithm>
@@ -69,25 +69,22 @@ __global__ void k_prep3c(typename PTT<FT>::type* __restrict__ pp, int* __restric
     if (lane == 0) npp[q] = n;
 }
 
-// Per call, one CTA per panel: the panel's items sorted by estimated cost,
-// heaviest first, so that the warps' dynamic queue ends with cheap items (the
-// panel's barrier then waits less for its slowest warp).  Cost = primitive
-// triples x (E tables + the chunk's products) + a fixed part per item; the f-shell
-// classes (run-time loops, FP64 tables) count four times.  Rank sort in shared
-// memory; panels of more than kOrder3Max items keep the static order.
+// Per call, one CTA: the items sorted by estimated cost, heaviest first, so
+// that the kernel's unit queue (item-major) ends with cheap items.  Cost =
+// primitive triples x (E tables + the chunk's products) + a fixed part per
+// item; the f-shell classes (run-time loops, FP64 tables) count four times.
+// Rank sort in shared memory; more than kOrder3Max items keep the static order.
 constexpr int kOrder3Max = 2048;
 
 __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, const Item3* __restrict__ items,
-                                                 const int* __restrict__ npp, Panels3 panels, int ns) {
+                                                 const int* __restrict__ npp, int n, int ns) {
     __shared__ unsigned long long key[kOrder3Max];
-    const int pn = blockIdx.x;
-    const int i0 = panels.item0[pn], n = panels.item0[pn + 1] - i0;
     if (n > kOrder3Max) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) order[i0 + i] = items[i0 + i];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = items[i];
         return;
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const Item3 it = items[i0 + i];
+        const Item3 it = items[i];
         const bool f = it.cls >= kClsF3;
         const int c = f ? it.cls - kClsF3 : it.cls;
         const int la = f ? c >> 4 : c / 9, lb = f ? (c >> 2) & 3 : (c / 3) % 3, lc = f ? c & 3 : c % 3;
@@ -103,7 +100,7 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         const unsigned long long ki = key[i];
         int r = 0;
         for (int j = 0; j < n; ++j) r += key[j] < ki;
-        order[i0 + r] = items[i0 + i];
+        order[r] = items[i];
     }
 }
 
@@ -111,74 +108,26 @@ int setup_overlap3c_schedule(aok_plan* p) {
     if (p->d_items3) return AOK_OK;
     if (p->NZ != 1) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: plan must have NZ = 1");
     if (p->Lmax > kMaxL3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: shells above l = 3");
-    const int ns = (int)p->ns, N = (int)p->N;
-    const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    const size_t N2 = (size_t)N * N;
-    const size_t budget = 220 * 1024;
-    auto stride_for = [&](int pages) {
-        size_t s = N2 * pages;
-        if (s % 2 == 0) s += 1;
-        return s;
-    };
-    int maxpages = 0;
-    while (maxpages < N && stride_for(maxpages + 1) * kTileB * fsz <= budget) ++maxpages;
-    if (maxpages == 0) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: one output page exceeds the slab");
-    // panels: whole shells where they fit, otherwise page ranges of one shell
-    std::vector<int> pg{0};
-    int cur = 0;
-    for (int s = 0; s < ns; ++s) {
-        const int np = ncart((int)p->ls[s]);
-        if (cur > 0 && cur + np > maxpages) {
-            pg.push_back(pg.back() + cur);
-            cur = 0;
-        }
-        int left = np;
-        while (left > maxpages) {
-            pg.push_back(pg.back() + cur + maxpages);
-            left -= maxpages;
-            cur = 0;
-        }
-        cur += left;
-    }
-    pg.push_back(pg.back() + cur);
-    const int npan = (int)pg.size() - 1;
-    if (npan > kMaxPanels3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: basis too large for the panels");
-    Panels3 pan{};
-    pan.n = npan;
-    std::vector<Item3> items;
-    for (int pn = 0; pn < npan; ++pn) {
-        pan.page0[pn] = pg[pn];
-        pan.item0[pn] = (int)items.size();
-        std::vector<std::pair<int, Item3>> v;
-        for (int sc = 0; sc < ns; ++sc) {
-            const int k0 = (int)p->boff[sc], k1 = (int)p->boff[sc + 1];
-            if (k1 <= pg[pn] || k0 >= pg[pn + 1]) continue;
-            for (int sa = 0; sa < ns; ++sa)
-                for (int sb = 0; sb < ns; ++sb) {
-                    const int la = (int)p->ls[sa], lb = (int)p->ls[sb], lc = (int)p->ls[sc];
-                    const int ppc = pages_per_chunk3(la, lb), nch = nchunks3(la, lb, lc);
-                    for (int c = 0; c < nch; ++c) {
-                        const int c0 = k0 + c * ppc, c1 = std::min(k0 + (c + 1) * ppc, k1);
-                        if (c1 <= pg[pn] || c0 >= pg[pn + 1]) continue;
-                        const int cost = (la + 1) * (lb + 1) * (lc + 1) * 12 + 2 * ncart(la) * ncart(lb) * (c1 - c0);
-                        const bool f = std::max(la, std::max(lb, lc)) > kMaxL3Spec;
-                        const int cls = f ? kClsF3 + la * 16 + lb * 4 + lc : la * 9 + lb * 3 + lc;
-                        v.push_back({f ? 4 * cost : cost, Item3{(int16_t)cls, (int16_t)c, (int16_t)sa, (int16_t)sb,
-                                                                (int16_t)sc, 0}});
-                    }
+    const int ns = (int)p->ns;
+    // every (shell triple, page chunk), statically ordered by class cost
+    std::vector<std::pair<int, Item3>> v;
+    for (int sc = 0; sc < ns; ++sc)
+        for (int sa = 0; sa < ns; ++sa)
+            for (int sb = 0; sb < ns; ++sb) {
+                const int la = (int)p->ls[sa], lb = (int)p->ls[sb], lc = (int)p->ls[sc];
+                const int ppc = pages_per_chunk3(la, lb), nch = nchunks3(la, lb, lc);
+                for (int c = 0; c < nch; ++c) {
+                    const int pages = std::min(ppc, ncart(lc) - c * ppc);
+                    const int cost = (la + 1) * (lb + 1) * (lc + 1) * 12 + 2 * ncart(la) * ncart(lb) * pages;
+                    const bool f = std::max(la, std::max(lb, lc)) > kMaxL3Spec;
+                    const int cls = f ? kClsF3 + la * 16 + lb * 4 + lc : la * 9 + lb * 3 + lc;
+                    v.push_back({f ? 4 * cost : cost,
+                                 Item3{(int16_t)cls, (int16_t)c, (int16_t)sa, (int16_t)sb, (int16_t)sc, 0}});
                 }
-        }
-        std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-        for (auto& x : v) items.push_back(x.second);
-    }
-    pan.page0[npan] = pg[npan];
-    pan.item0[npan] = (int)items.size();
-    static_assert(sizeof(Panels3) <= sizeof(p->panels3_raw), "panels3 storage");
-    memcpy(p->panels3_raw, &pan, sizeof(Panels3));
-    size_t maxw = 0;
-    for (int i = 0; i < npan; ++i) maxw = std::max(maxw, (size_t)(pg[i + 1] - pg[i]));
-    p->slab_stride3 = stride_for((int)maxw);
-    p->smem3 = p->slab_stride3 * kTileB * fsz;
+            }
+    std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<Item3> items;
+    for (auto& x : v) items.push_back(x.second);
     p->nitems3 = (int)items.size();
     const size_t nrec = (size_t)ns * ns * ns * p->K * p->K * p->K;
     const size_t rec = p->prec == AOK_PREC_F64 ? sizeof(PTd) : sizeof(PTf);
@@ -208,9 +157,7 @@ int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB,
                                           (const float*)p->d_gb_coef, (int)p->ns, (int)p->K);
     int st = cuda_status(cudaGetLastError(), "k_prep3c");
     if (st != AOK_OK) return st;
-    Panels3 pan;
-    memcpy(&pan, p->panels3_raw, sizeof(Panels3));
-    k_order3c<<<pan.n, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, pan, (int)p->ns);
+    k_order3c<<<1, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, p->nitems3, (int)p->ns);
     if ((st = cuda_status(cudaGetLastError(), "k_order3c")) != AOK_OK) return st;
     if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, s);
     return launch_ov3_f32(p, out, posA, posB, posC, s);

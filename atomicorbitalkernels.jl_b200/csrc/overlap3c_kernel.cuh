@@ -13,16 +13,14 @@
 // lin = c1 + (2la+1) c2 + (2la+1)(2lb+1) c3 (kernels_3c.jl:146-160) is
 // reproduced at compile time.
 //
-// Same execution model as the 2C kernel: tiles of 32 batch elements (lane =
-// element), a persistent CTA per SM, shell-triple classes (la, lb, lc <= 2)
-// compile-time specialised (classes with an f shell: run_item3_f, below), work items drained from a per-tile shared-memory
-// counter, results staged per output-page panel in shared memory and written
-// out coalesced (a batch element's (N,N,N) slab is contiguous).  Items are
-// whole shell-triple blocks or chunks of whole output pages; a chunk whose
-// pages straddle a panel boundary is computed in each panel it touches and
-// stores only the pages inside the current panel.
+// Execution: tiles of 32 batch elements (lane = element); shell-triple classes
+// (la, lb, lc <= 2) compile-time specialised (classes with an f shell:
+// run_item3_f, below).  Items are whole shell-triple blocks or chunks of whole
+// output pages; (item, tile) units are drained from one global queue, heaviest
+// items first (k_overlap3c below).
 #pragma once
 
+#include <algorithm>
 #include <cstring>
 
 #include "aok_internal.h"
@@ -32,8 +30,8 @@ namespace aok {
 constexpr int kMaxL3 = 3;        // shells up to f
 constexpr int kMaxL3Spec = 2;    // compile-time specialised classes up to d
 constexpr int kClsF3 = 100;      // Item3 class code of a triple with an f shell: kClsF3 + la*16 + lb*4 + lc
-constexpr int kThreads3 = 256;
-constexpr int kMaxPanels3 = 64;  // output-page panels (one page per panel for wide FP64 bases)
+constexpr int kThreads3 = 128;
+constexpr int kAllPages3 = 1 << 20;  // page window [0, kAllPages3): every page of an item's chunk
 
 __host__ __device__ constexpr int pages_per_chunk3(int la, int lb) {
     return (ncart(la) * ncart(lb)) >= 36 ? 1 : 36 / (ncart(la) * ncart(lb));
@@ -61,11 +59,6 @@ struct Item3 {
     int16_t sa, sb, sc, pad;
 };
 
-struct Panels3 {
-    int n;
-    int page0[kMaxPanels3 + 1];  // global output page (k index) range of each panel
-    int item0[kMaxPanels3 + 1];
-};
 
 template <typename FT> struct Geo3;
 template <> struct Geo3<float> {
@@ -158,7 +151,7 @@ struct Class3 {
 // Only pages inside [kp0, kp1) (block-local) are stored.
 template <int LA, int LB, int LC, int C>
 __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const Geo3<float> g, float* dst, int N,
-                                       int kp0, int kp1) {
+                                       int kp0, int kp1, bool valid) {
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
@@ -221,6 +214,7 @@ __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const 
                     }
                 }
     }
+    if (!valid) return;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int lin = L0 + m, pg = lin / CI::PS;
@@ -235,7 +229,7 @@ __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const 
 
 template <int LA, int LB, int LC, int C>
 __device__ __noinline__ void run_item3(const PTd* __restrict__ pp, int n, const Geo3<double> g, double* dst, int N,
-                                       int kp0, int kp1) {
+                                       int kp0, int kp1, bool valid) {
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
@@ -270,6 +264,7 @@ __device__ __noinline__ void run_item3(const PTd* __restrict__ pp, int n, const 
                     }
                 }
     }
+    if (!valid) return;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int lin = L0 + m, pg = lin / CI::PS;
@@ -328,7 +323,7 @@ __device__ __forceinline__ double pt_exponent(const PTd* r, const double (&R2)[3
 
 template <typename PT, typename FT>
 __device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const Geo3<FT> g, FT* dst, int N, int kp0,
-                                         int kp1, int cls, int chunk) {
+                                         int kp1, int cls, int chunk, bool valid) {
     const int c = cls - kClsF3, la = c >> 4, lb = (c >> 2) & 3, lc = c & 3;
     const int NA = ncart(la), NB = ncart(lb), NC = ncart(lc), PS = NA * NB, N1 = 2 * la + 1, N2 = 2 * lb + 1;
     const int ppc = pages_per_chunk3(la, lb);
@@ -373,6 +368,7 @@ __device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const
             }
         }
     }
+    if (!valid) return;
     for (int m = 0; m < M; ++m) {
         const int lin = L0 + m, pg = lin / PS;
         if (pg >= kp0 && pg < kp1) {
@@ -384,31 +380,31 @@ __device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const
 
 template <typename PT, typename FT, int LA, int LB, int LC>
 __device__ __forceinline__ void run_chunks3(int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N, int kp0,
-                                            int kp1) {
+                                            int kp1, bool valid) {
     constexpr int NCH = nchunks3(LA, LB, LC);
     switch (chunk) {
-        case 0: run_item3<LA, LB, LC, 0>(pp, n, g, dst, N, kp0, kp1); break;
-        case 1: if constexpr (NCH > 1) run_item3<LA, LB, LC, 1>(pp, n, g, dst, N, kp0, kp1); break;
-        case 2: if constexpr (NCH > 2) run_item3<LA, LB, LC, 2>(pp, n, g, dst, N, kp0, kp1); break;
-        case 3: if constexpr (NCH > 3) run_item3<LA, LB, LC, 3>(pp, n, g, dst, N, kp0, kp1); break;
-        case 4: if constexpr (NCH > 4) run_item3<LA, LB, LC, 4>(pp, n, g, dst, N, kp0, kp1); break;
-        case 5: if constexpr (NCH > 5) run_item3<LA, LB, LC, 5>(pp, n, g, dst, N, kp0, kp1); break;
+        case 0: run_item3<LA, LB, LC, 0>(pp, n, g, dst, N, kp0, kp1, valid); break;
+        case 1: if constexpr (NCH > 1) run_item3<LA, LB, LC, 1>(pp, n, g, dst, N, kp0, kp1, valid); break;
+        case 2: if constexpr (NCH > 2) run_item3<LA, LB, LC, 2>(pp, n, g, dst, N, kp0, kp1, valid); break;
+        case 3: if constexpr (NCH > 3) run_item3<LA, LB, LC, 3>(pp, n, g, dst, N, kp0, kp1, valid); break;
+        case 4: if constexpr (NCH > 4) run_item3<LA, LB, LC, 4>(pp, n, g, dst, N, kp0, kp1, valid); break;
+        case 5: if constexpr (NCH > 5) run_item3<LA, LB, LC, 5>(pp, n, g, dst, N, kp0, kp1, valid); break;
         default: break;
     }
 }
 
 template <typename PT, typename FT, bool F3>
 __device__ __forceinline__ void dispatch3(int cls, int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N,
-                                          int kp0, int kp1) {
+                                          int kp0, int kp1, bool valid) {
     if constexpr (F3) {
         if (cls >= kClsF3) {
-            run_item3_f<PT, FT>(pp, n, g, dst, N, kp0, kp1, cls, chunk);
+            run_item3_f<PT, FT>(pp, n, g, dst, N, kp0, kp1, cls, chunk, valid);
             return;
         }
     }
     switch (cls) {
 #define AOK_C3(LA, LB, LC) \
-    case (LA) * 9 + (LB) * 3 + (LC): run_chunks3<PT, FT, LA, LB, LC>(chunk, pp, n, g, dst, N, kp0, kp1); break;
+    case (LA) * 9 + (LB) * 3 + (LC): run_chunks3<PT, FT, LA, LB, LC>(chunk, pp, n, g, dst, N, kp0, kp1, valid); break;
         AOK_C3(0, 0, 0) AOK_C3(0, 0, 1) AOK_C3(0, 0, 2) AOK_C3(0, 1, 0) AOK_C3(0, 1, 1) AOK_C3(0, 1, 2)
         AOK_C3(0, 2, 0) AOK_C3(0, 2, 1) AOK_C3(0, 2, 2) AOK_C3(1, 0, 0) AOK_C3(1, 0, 1) AOK_C3(1, 0, 2)
         AOK_C3(1, 1, 0) AOK_C3(1, 1, 1) AOK_C3(1, 1, 2) AOK_C3(1, 2, 0) AOK_C3(1, 2, 1) AOK_C3(1, 2, 2)
@@ -431,67 +427,42 @@ struct Ov3Params {
     const int4* tiles;
     const int* ntiles;
     unsigned* counter;
-    const Item3* items;
-    Panels3 panels;
-    int ns, K, N, slab_stride;
+    const Item3* items;  // every (shell triple, page chunk), heaviest first (k_order3c)
+    int nitems, ns, K, N;
     int boff[kMaxShells + 1];
 };
 
-// F3: the instantiation for bases with f shells (it alone holds run_item3_f).
+// Work unit = (item, tile): one shell-triple block (or page chunk of it) for the
+// 32 batch elements of a tile, lane = element.  Units are drained from one
+// global counter item-major, so every tile's heaviest items run first and the
+// cheap ones fill the end; there are no panels and no barriers.  A lane writes
+// its element's block straight to the output: a batch element's (N,N,N) slab
+// is contiguous and the whole output is written exactly once, so the scattered
+// stores of a block meet in L2 before they reach DRAM.  Three CTAs of four
+// warps per SM (<= 168 registers).
 template <typename FT, bool F3>
-__global__ void __launch_bounds__(kThreads3, 1) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FT* slab = reinterpret_cast<FT*>(smem_raw);
-    __shared__ int s_tile;
-    __shared__ int s_next[kMaxPanels3];
-    constexpr int NW = kThreads3 / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
+    const int lane = threadIdx.x & 31;
     const int ntiles = *P.ntiles;
-    const size_t N2 = (size_t)P.N * P.N;
+    const unsigned total = (unsigned)ntiles * (unsigned)P.nitems;
+    const size_t N2 = (size_t)P.N * P.N, N3 = N2 * P.N;
     for (;;) {
-        if (threadIdx.x == 0) {
-            s_tile = (int)atomicAdd(P.counter, 1u);
-            for (int i = 0; i < P.panels.n; ++i) s_next[i] = 0;
-        }
-        __syncthreads();
-        const int tile = s_tile;
-        if (tile >= ntiles) break;
+        unsigned u = 0;
+        if (lane == 0) u = atomicAdd(P.counter, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= total) break;
+        const int it = (int)(u / (unsigned)ntiles), tile = (int)(u % (unsigned)ntiles);
         const int4 td = P.tiles[tile];
-        const int start = td.y, cnt = td.z;
+        const bool valid = lane < td.z;
+        const int b = P.perm[td.y + (valid ? lane : 0)];
         Geo3<FT> g;
-        {
-            const int b = lane < cnt ? P.perm[start + lane] : P.perm[start];
-            load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b);
-        }
-        FT* sl = slab + (size_t)lane * P.slab_stride;
-        for (int pn = 0; pn < P.panels.n; ++pn) {
-            const int pg0 = P.panels.page0[pn], pg1 = P.panels.page0[pn + 1];
-            const int i0 = P.panels.item0[pn], i1 = P.panels.item0[pn + 1];
-            for (;;) {
-                int it = 0;
-                if (lane == 0) it = atomicAdd(&s_next[pn], 1);
-                it = __shfl_sync(0xffffffffu, it, 0) + i0;
-                if (it >= i1) break;
-                const Item3 wi = P.items[it];
-                const int q = (wi.sa * P.ns + wi.sb) * P.ns + wi.sc;
-                const int n = __ldg(P.npp + q);
-                const int koff = P.boff[wi.sc];
-                // block-local page window of this panel, and the block's (0,0,first page) in the slab
-                const int kp0 = max(pg0 - koff, 0), kp1 = min(pg1 - koff, P.boff[wi.sc + 1] - koff);
-                FT* dst = sl + (size_t)(koff + kp0 - pg0) * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-                dispatch3<typename PTT<FT>::type, FT, F3>(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K * P.K, n,
-                                                          g, dst, P.N, kp0, kp1);
-            }
-            __syncthreads();
-            const size_t len = (size_t)(pg1 - pg0) * N2;
-            for (int bl = warp; bl < cnt; bl += NW) {
-                const int bg = P.perm[start + bl];
-                FT* o = P.out + (size_t)bg * N2 * P.N + (size_t)pg0 * N2;
-                const FT* s = slab + (size_t)bl * P.slab_stride;
-                for (size_t e = lane; e < len; e += 32) o[e] = s[e];
-            }
-            __syncthreads();
-        }
+        load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b);
+        const Item3 wi = P.items[it];
+        const int q = (wi.sa * P.ns + wi.sb) * P.ns + wi.sc;
+        const int n = __ldg(P.npp + q);
+        FT* dst = P.out + (size_t)b * N3 + (size_t)P.boff[wi.sc] * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
+        dispatch3<typename PTT<FT>::type, FT, F3>(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K * P.K, n, g, dst,
+                                                  P.N, 0, kAllPages3, valid);
     }
 }
 
@@ -510,17 +481,17 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.ntiles = p->d_ntiles;
     P.counter = p->d_counter;
     P.items = (const Item3*)p->d_order3;
-    memcpy(&P.panels, p->panels3_raw, sizeof(Panels3));
+    P.nitems = p->nitems3;
     P.ns = (int)p->ns;
     P.K = (int)p->K;
     P.N = (int)p->N;
-    P.slab_stride = (int)p->slab_stride3;
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
     auto kern = k_overlap3c<FT, F3>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem3);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap3c)");
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads3, 0);
+    if (e != cudaSuccess) return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     timing_begin(p, s);
-    kern<<<p->num_sms, kThreads3, p->smem3, s>>>(P);
+    kern<<<p->num_sms * std::max(occ, 1), kThreads3, 0, s>>>(P);
     timing_end(p, s);
     return cuda_status(cudaGetLastError(), "k_overlap3c");
 }

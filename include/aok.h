@@ -169,9 +169,8 @@ int aok_overlap2c_gb(aok_plan* plan, void* out, const int64_t* nprim,
 /*
  * Batched 3-center overlap, GaussianBasis path (NZ = 1 plan).
  * Replaces batch_V_kernel! + batch_overlap_3c! (src/integrals/kernels_3c.jl:12-200).
- * out (N,N,N,B); posA, posB, posC (3,B) in Bohr.  Shells up to l = 3.  One
- * output page (N x N) of 32 batch elements must fit 220 KB of shared memory
- * (N <= 29 in FP64, N <= 41 in FP32C); larger bases return AOK_ERR_UNSUPPORTED.
+ * out (N,N,N,B); posA, posB, posC (3,B) in Bohr.  Shells up to l = 3, at most
+ * 64 shells; no limit on N beyond the output's size.
  */
 int aok_overlap3c_gb(aok_plan* plan, void* out, const int64_t* nprim,
                      const int64_t* prim_offset, const void* coef, const void* alpha,

@@ -140,21 +140,18 @@ def _sized_basis(extra_s):
     return bc, ls, nprim, coef, z
 
 
-def test_largest_page_f64_and_the_limit():
-    """One FP64 output page of 32 batch elements (N^2 doubles each) must fit the 220 KB
-    slab: N = 29 is the largest basis and matches the oracle; N = 30 is refused with
-    AOK_ERR_UNSUPPORTED, while FP32C still takes it (its limit is N = 41)."""
+def test_wide_bases_f64_and_f32c():
+    """The kernel stages no output in shared memory, so the basis width has no page limit:
+    N = 29, 30 and 45 (f, d, p and up to 17 s shells) match the oracle in FP64, and
+    N = 45 in FP32C."""
     tr = W.config4_triples(B=40, seed=1013)
     pA, pB, pC = _L(tr.posA), _L(tr.posB), _L(tr.posC)
-    bc, ls, nprim, coef, z = _sized_basis(0)
-    assert bc.nbf_total == 29
-    V = aok.batch_overlap_3c(bc, pA, pB, pC)
-    ref = oracle.overlap3c_gb(ls, nprim, coef, z, aok.to_bohr(pA), aok.to_bohr(pB), aok.to_bohr(pC), nthreads=8)
-    assert rel_fro(V, ref) < 1e-12
-    bc, ls, nprim, coef, z = _sized_basis(1)
-    assert bc.nbf_total == 30
-    with pytest.raises(aok.AOKError, match="page"):
-        aok.batch_overlap_3c(bc, pA, pB, pC)
+    for extra, n in ((0, 29), (1, 30), (16, 45)):
+        bc, ls, nprim, coef, z = _sized_basis(extra)
+        assert bc.nbf_total == n
+        V = aok.batch_overlap_3c(bc, pA, pB, pC)
+        ref = oracle.overlap3c_gb(ls, nprim, coef, z, aok.to_bohr(pA), aok.to_bohr(pB), aok.to_bohr(pC), nthreads=8)
+        assert rel_fro(V, ref) < 1e-12
     V = aok.batch_overlap_3c(bc, pA, pB, pC, FT=torch.float32)
     ref = oracle.overlap3c_gb(ls, nprim, f32_round(coef), f32_round(z), f32_round(aok.to_bohr(pA, np.float32)),
                               f32_round(aok.to_bohr(pB, np.float32)), f32_round(aok.to_bohr(pC, np.float32)),
