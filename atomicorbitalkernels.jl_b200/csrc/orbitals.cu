@@ -289,6 +289,90 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
     }
 }
 
+// ---------------------------------------------------------------------------
+// Forward with the harmonics in registers (L <= 3, each (radial, harmonic) pair
+// used by at most one orbital).  The orbital maps are turned into a table
+// otab[k * nY + yi] -> orbital (or -1) held in the kernel's parameter space, so
+// that the loop over radials k (run time) nests an unrolled loop over the
+// harmonics yi (compile time): Z[yi], G[yi] stay in registers and R_k, dR_k
+// are used as soon as they are formed.  Compared with k_evaluate this drops
+// the per-thread shared-memory round trip of R, dR, Z, G and the per-orbital
+// map loads; the table entries are warp-uniform constant-bank reads.
+// ---------------------------------------------------------------------------
+constexpr int kRegMaxRad = 64;
+constexpr int kRegMaxL = 3;
+struct EvalRegParams {
+    EvalParams E;
+    int16_t otab[kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1)];
+    int8_t poly[kRegMaxRad];
+};
+
+template <typename FT, int L, bool GRAD>
+__global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_constant__ EvalRegParams Q) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const EvalParams& P = Q.E;
+    constexpr int nY = (L + 1) * (L + 1);
+    const int ntab = P.nRad * P.K * P.NZ;
+    FT* sz = reinterpret_cast<FT*>(smem_raw);
+    FT* sD = sz + ntab;
+    FT* sl = sD + ntab;
+    int* sn = reinterpret_cast<int*>(sl + ntab);
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
+        sz[i] = ((const FT*)P.zeta)[i];
+        sD[i] = ((const FT*)P.D)[i];
+        sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
+    }
+    for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
+        sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
+    __syncthreads();
+    FT* Pout = (FT*)P.P;
+    FT* dPout = (FT*)P.dP;
+    const FT sc = (FT)P.scale;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < P.nX;
+         j += (long long)gridDim.x * blockDim.x) {
+        const FT* X = (const FT*)P.X;
+        FT x = X[3 * j], y = X[3 * j + 1], z = X[3 * j + 2];
+        if (sc != FT(1)) {
+            x = sc * x;
+            y = sc * y;
+            z = sc * z;
+        }
+        const FT r = sqrt(x * x + y * y + z * z);
+        int sg = (int)P.sidx[j] - 1;
+        if (sg < 0 || sg >= P.NZ) {
+            atomicCAS(P.err, 0, AOK_ERR_SPECIES);
+            sg = 0;
+        }
+        FT Z[nY], G[3 * nY];
+        solid_harmonics<FT, L>(x, y, z, P.F, Z, G, 1);
+        const FT ux = x / r, uy = y / r, uz = z / r;  // X[j] / r[j] (NaN at r = 0, as the reference)
+        for (int k = 0; k < P.nRad; ++k) {
+            FT R, dR;
+            radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
+#pragma unroll
+            for (int yi = 0; yi < nY; ++yi) {
+                const int o = Q.otab[k * nY + yi];
+                if (o < 0) continue;
+                Pout[j + P.nX * o] = R * Z[yi];
+                if (GRAD) {
+                    FT gx = (dR * ux) * Z[yi] + R * G[3 * yi + 0];
+                    FT gy = (dR * uy) * Z[yi] + R * G[3 * yi + 1];
+                    FT gz = (dR * uz) * Z[yi] + R * G[3 * yi + 2];
+                    if (sc != FT(1)) {
+                        gx *= sc;
+                        gy *= sc;
+                        gz *= sc;
+                    }
+                    FT* op = dPout + 3 * (j + P.nX * o);
+                    op[0] = gx;
+                    op[1] = gy;
+                    op[2] = gz;
+                }
+            }
+        }
+    }
+}
+
 // Pullback: dX (optional) and per-block rows of (dD, dzeta) partials.
 template <typename FT, int L>
 __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_constant__ EvalParams P) {
@@ -768,12 +852,62 @@ static void fill_params(aok_orbitals* o, EvalParams& P, const void* X, const int
         }
 }
 
+// The register-path forward when the maps allow it (L <= 3, nRad <= 64, each
+// (radial, harmonic) pair at most once, radial powers < 128); returns -1 otherwise.
+template <typename FT, int L>
+static int launch_eval_reg_L(aok_orbitals* o, const EvalParams& P, bool grad, cudaStream_t s) {
+    constexpr int nY = (L + 1) * (L + 1);
+    EvalRegParams Q;
+    memset(&Q, 0, sizeof(Q));
+    Q.E = P;
+    for (int i = 0; i < kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1); ++i) Q.otab[i] = -1;
+    for (int64_t i = 0; i < o->nOrb; ++i) {
+        const int64_t k = o->iR[i] - 1, yi = o->iY[i] - 1;
+        int16_t& e = Q.otab[k * nY + yi];
+        if (e >= 0) return -1;  // a repeated (radial, harmonic) pair: the general kernel
+        e = (int16_t)i;
+    }
+    for (int64_t k = 0; k < o->nRad; ++k) {
+        if (o->poly[k] > 127) return -1;
+        Q.poly[k] = (int8_t)o->poly[k];
+    }
+    const size_t fsz = sizeof(FT);
+    const size_t smem = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    if (smem > 227 * 1024) return -1;
+    void* k = grad ? (void*)k_evaluate_reg<FT, L, true> : (void*)k_evaluate_reg<FT, L, false>;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_reg)");
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kEvalThreads, smem)) != cudaSuccess)
+        return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((P.nX + kEvalThreads - 1) / kEvalThreads, (int64_t)o->num_sms * std::max(occ, 1)));
+    void* args[] = {&Q};
+    return cuda_status(cudaLaunchKernel(k, dim3(grid), dim3(kEvalThreads), args, smem, s), "k_evaluate_reg");
+}
+
+template <typename FT>
+static int launch_eval_reg(aok_orbitals* o, const EvalParams& P, bool grad, cudaStream_t s) {
+    if (o->nRad > kRegMaxRad) return -1;
+    switch (o->L) {
+        case 0: return launch_eval_reg_L<FT, 0>(o, P, grad, s);
+        case 1: return launch_eval_reg_L<FT, 1>(o, P, grad, s);
+        case 2: return launch_eval_reg_L<FT, 2>(o, P, grad, s);
+        case 3: return launch_eval_reg_L<FT, 3>(o, P, grad, s);
+        default: return -1;
+    }
+}
+
 int launch_evaluate(aok_orbitals* o, void* Pv, void* dP, const void* X, const int64_t* sidx, const void* zeta,
                     const void* D, int64_t nX, double lengthscale, cudaStream_t s) {
     EvalParams P;
     fill_params(o, P, X, sidx, zeta, D, nX, lengthscale);
     P.P = Pv;
     P.dP = dP;
+    const int st = o->prec == AOK_PREC_F64 ? launch_eval_reg<double>(o, P, dP != nullptr, s)
+                                           : launch_eval_reg<float>(o, P, dP != nullptr, s);
+    if (st != -1) return st;
     if (o->prec == AOK_PREC_F64) return launch_eval_T<double>(o, P, dP != nullptr, false, s);
     return launch_eval_T<float>(o, P, dP != nullptr, false, s);
 }

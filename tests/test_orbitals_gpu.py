@@ -224,3 +224,32 @@ def test_orbitals_check_single_species_bad_index(with_params):
     assert rel_fro(dX1[keep], dX2) < 1e-12
     if with_params:
         assert rel_fro(dz1, dz2) < 1e-12 and rel_fro(dD1, dD2) < 1e-12
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-12), (torch.float32, 2e-6)])
+def test_evaluate_ed_general_maps(FT, tol):
+    """Orbital maps with a repeated (radial, harmonic) pair take the general kernel (the
+    harmonics staged per thread in shared memory) instead of the register-resident one:
+    both give the oracle's values; the repeated orbital equals its original."""
+    import ctypes
+
+    from aok_b200 import _dev, _lib
+    b, orb = _basis()
+    iR = np.concatenate([orb.radidx, orb.radidx[:2]])
+    iY = np.concatenate([orb.ylmidx, orb.ylmidx[:2]])
+    nX = 4000
+    X, sidx = W.config1_points(nX=nX, seed=19)
+    plan = _dev.OrbPlan(b.zeta.shape[0], b.K, b.NZ, orb.Rnl.powers(), iR, iY, orb.L, orb.Rnl.kind,
+                        _dev.prec_of(FT))
+    P = _dev.colmajor_empty((nX, len(iR)), FT)
+    dP = _dev.colmajor_empty((3, nX, len(iR)), FT)
+    Xd, sd = _dev.to_colmajor(X, FT), torch.as_tensor(sidx).cuda()
+    _lib.check(_lib.load().aok_evaluate_ed(plan.h, _dev.ptr(P), _dev.ptr(dP), _dev.ptr(Xd),
+                                           ctypes.c_void_p(sd.data_ptr()), _dev.ptr(_dev.to_colmajor(b.zeta, FT)),
+                                           _dev.ptr(_dev.to_colmajor(b.D, FT)), nX, 1.0, _dev.stream()))
+    rnd = f32_round if FT == torch.float32 else (lambda a: a)
+    Pr, dPr = oracle.evaluate_ed(rnd(X), sidx, rnd(b.zeta), rnd(b.D), orb.Rnl.powers(), iR, iY, orb.L, nthreads=8)
+    Pg, dPg = P.double().cpu().numpy(), dP.double().cpu().numpy()
+    assert rel_fro(Pg, Pr) < tol and rel_fro(dPg, dPr) < tol
+    n = len(orb)
+    assert np.array_equal(Pg[:, n:], Pg[:, :2])
