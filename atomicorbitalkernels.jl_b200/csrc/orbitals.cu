@@ -521,6 +521,9 @@ struct EpbParams {
     unsigned* counter;  // unit queue
     double* partial;    // [2][nRad*K][ucap]: dD, dzeta per slot, units contiguous
     int ucap;           // unit capacity (row length of partial)
+    // register path (REG): (radial, harmonic) -> orbital table and radial powers
+    int16_t otab[kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1)];
+    int8_t poly[kRegMaxRad];
 };
 
 __device__ __forceinline__ int epb_nch(const int* tbase, int sigma, int NZ) {
@@ -530,11 +533,16 @@ __device__ __forceinline__ int epb_nch(const int* tbase, int sigma, int NZ) {
 // per-warp shared memory of the slot-parallel pullback (floats of FT):
 // R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][32], f [32]
 __host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) { return (size_t)(3 * nRad + 4 * nY + 1) * 32; }
+// the register path keeps only gg [nRad][32] and f [32]
+__host__ __device__ constexpr size_t epb_warp_words_reg(int nRad) { return (size_t)(nRad + 1) * 32; }
 
 // RAD: the radial layer's own pullback (gtostoradials.jl:232-267): X holds the
 // radii r (nX), dPin the cotangent of R (nX, nRad), so gg_k = dR[j,k] r^p_k and
 // there are no harmonics and no dX.
-template <typename FT, int L, bool RAD = false>
+// REG (L <= 3, unique orbital maps): phase A keeps the harmonics and the current
+// radial in registers and walks the (radial, harmonic) -> orbital table (as
+// k_evaluate_reg), so a warp's shared memory holds only gg and f(r).
+template <typename FT, int L, bool RAD = false, bool REG = false>
 __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ EpbParams Q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int nY = (L + 1) * (L + 1);
@@ -546,9 +554,10 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
     FT* sD = sz + ntab;
     FT* sl = sD + ntab;  // zeta log2(e)
     int* sn = reinterpret_cast<int*>(sl + ntab);
-    FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) + (size_t)warp * epb_warp_words(P.nRad, nY);
-    FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY, *gg = G + 96 * nY,
-       *fv = gg + 32 * P.nRad;
+    FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) +
+                (size_t)warp * (REG ? epb_warp_words_reg(P.nRad) : epb_warp_words(P.nRad, nY));
+    FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
+       *gg = REG ? wbase : G + 96 * nY, *fv = gg + 32 * P.nRad;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         sz[i] = ((const FT*)P.zeta)[i];
         sD[i] = ((const FT*)P.D)[i];
@@ -605,6 +614,47 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                 if constexpr (RAD) {
                     r = valid ? Xin[j] : FT(0);
                     for (int k = 0; k < P.nRad; ++k) gg[k * 32 + lane] = valid ? dPin[j + P.nX * k] : FT(0);
+                } else if constexpr (REG) {
+                    FT x = FT(0), y = FT(0), z = FT(1);
+                    if (valid) {
+                        x = Xin[3 * j];
+                        y = Xin[3 * j + 1];
+                        z = Xin[3 * j + 2];
+                        if (sc != FT(1)) {
+                            x = sc * x;
+                            y = sc * y;
+                            z = sc * z;
+                        }
+                    }
+                    r = sqrt(x * x + y * y + z * z);
+                    FT Zr[nY], Gr[3 * nY];
+                    solid_harmonics<FT, L>(x, y, z, P.F, Zr, Gr, 1);
+                    const FT ux = x / r, uy = y / r, uz = z / r;
+                    FT ax = FT(0), ay = FT(0), az = FT(0);
+                    for (int k = 0; k < P.nRad; ++k) {
+                        FT Rk, dRk;
+                        radial<FT>(sz, sD, sl, sn, k, sigma, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
+                        FT gk = FT(0);
+                        if (valid) {
+#pragma unroll
+                            for (int yi = 0; yi < nY; ++yi) {
+                                const int o = Q.otab[k * nY + yi];
+                                if (o < 0) continue;
+                                const FT g = dPin[j + P.nX * o];
+                                ax += g * ((dRk * ux) * Zr[yi] + Rk * Gr[3 * yi + 0]);
+                                ay += g * ((dRk * uy) * Zr[yi] + Rk * Gr[3 * yi + 1]);
+                                az += g * ((dRk * uz) * Zr[yi] + Rk * Gr[3 * yi + 2]);
+                                gk += g * Zr[yi];
+                            }
+                        }
+                        gg[k * 32 + lane] = gk;
+                    }
+                    if (valid && P.dX) {
+                        FT* dX = (FT*)P.dX;
+                        dX[3 * j] = sc != FT(1) ? ax * sc : ax;
+                        dX[3 * j + 1] = sc != FT(1) ? ay * sc : ay;
+                        dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
+                    }
                 } else {
                 FT x = FT(0), y = FT(0), z = FT(1);
                 if (valid) {
@@ -947,6 +997,31 @@ static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
     constexpr int nY = (L + 1) * (L + 1);
     const size_t fsz = sizeof(FT);
     const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    if constexpr (L <= kRegMaxL) {
+        // the register path when every (radial, harmonic) pair is used at most once
+        bool ok = o->nRad <= kRegMaxRad;
+        for (int i = 0; ok && i < kRegMaxRad * nY; ++i) Q.otab[i] = -1;
+        for (int64_t i = 0; ok && i < o->nOrb; ++i) {
+            int16_t& e = Q.otab[(o->iR[i] - 1) * nY + (o->iY[i] - 1)];
+            if (e >= 0) ok = false;
+            else e = (int16_t)i;
+        }
+        for (int64_t k = 0; ok && k < o->nRad; ++k) {
+            if (o->poly[k] > 127) ok = false;
+            else Q.poly[k] = (int8_t)o->poly[k];
+        }
+        const size_t smem = tab + 8 * epb_warp_words_reg((int)o->nRad) * fsz;
+        if (ok && smem <= 227 * 1024) {
+            auto k = k_evaluate_pbs<FT, L, false, true>;
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs reg)");
+            int occ = 0;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem)) != cudaSuccess)
+                return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            k<<<o->num_sms * std::max(1, occ), 256, smem, s>>>(Q);
+            return cuda_status(cudaGetLastError(), "k_evaluate_pbs");
+        }
+    }
     const size_t per_warp = epb_warp_words((int)o->nRad, nY) * fsz;
     int nw = 8;
     while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;
