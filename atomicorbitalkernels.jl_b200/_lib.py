@@ -28,7 +28,7 @@ AOK_MAX_L = 3
 # every symbol include/aok.h declares
 EXPORTS = [
     "aok_last_error", "aok_version", "aok_plan_create", "aok_plan_destroy", "aok_plan_nbf",
-    "aok_plan_check", "aok_plan_set_basis", "aok_plan_set_graph", "aok_plan_autotune", "aok_plan_timing_enable", "aok_plan_timing_read", "aok_measure_fma_peak", "aok_compile_coef", "aok_species_index", "aok_overlap2c", "aok_overlap2c_gb", "aok_overlap3c_gb",
+    "aok_plan_check", "aok_plan_set_basis", "aok_plan_set_graph", "aok_plan_autotune", "aok_plan_timing_enable", "aok_plan_timing_read", "aok_measure_fma_peak", "aok_compile_coef", "aok_species_index", "aok_overlap2c", "aok_overlap2c_gb", "aok_overlap3c_gb", "aok_overlap3c",
     "aok_overlap2c_pullback", "aok_overlap2c_position_pullback", "aok_compile_coef_pullback",
     "aok_overlap_pullback_ps",
     "aok_overlap2c_rrule", "aok_overlap_pullback_ps_rrule", "aok_overlap_pullback_ps_rrule_residual",
@@ -90,6 +90,7 @@ def load():
     L.aok_species_index.argtypes = [vp, vp, vp, i64, pi64, vp]
     L.aok_overlap2c_gb.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]
     L.aok_overlap3c_gb.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]
+    L.aok_overlap3c.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_overlap2c_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_overlap2c_position_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, dbl, vp]
     L.aok_compile_coef_pullback.argtypes = [vp, vp, vp, vp, vp, vp, vp]

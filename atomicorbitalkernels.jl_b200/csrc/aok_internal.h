@@ -166,6 +166,12 @@ constexpr int kBinMaxBlocksHost = 512;
 int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
                     cudaStream_t s);
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s);
+// Binning by species triple (sidxC given): keys ((a-1) NZ + (b-1)) NZ + (c-1), NZ^3 <= 256.
+int launch_bin3_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, const int64_t* sidxC,
+                     int64_t B, int NZ, cudaStream_t s);
+// Keys a plan's bin buffers are sized for: species triples when NZ^3 fits the
+// binning's 256 keys (the species-aware 3C overlap), species pairs otherwise.
+inline int64_t bin_keys_max(int64_t NZ) { return NZ * NZ * NZ <= 256 ? NZ * NZ * NZ : NZ * NZ; }
 int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
                        const void* zeta, const void* D, const void* posA, const void* posB, double lengthscale,
                        cudaStream_t s);
@@ -201,10 +207,12 @@ int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, con
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);
-int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC,
-                     int64_t B, cudaStream_t s);
-int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s);
-int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s);
+int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
+                     const void* posC, double lengthscale, cudaStream_t s);
+int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                   cudaStream_t s);
+int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                   cudaStream_t s);
 
 // orbitals.cu
 int launch_evaluate(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx,

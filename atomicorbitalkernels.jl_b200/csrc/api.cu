@@ -109,7 +109,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
                           "cudaDeviceGetAttribute")) != AOK_OK)
         return fail(st);
     const size_t fsz = precision == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
-    p->max_tiles = (int)((max_batch + kTileB - 1) / kTileB + NZ * NZ + 1);
+    p->max_tiles = (int)((max_batch + kTileB - 1) / kTileB + bin_keys_max(NZ) + 1);
     std::vector<int> ls32(nshells), boff32(nshells + 1);
     for (int64_t s = 0; s < nshells; ++s) ls32[s] = (int)ls[s];
     for (int64_t s = 0; s <= nshells; ++s) boff32[s] = (int)p->boff[s];
@@ -118,7 +118,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
         (st = dmalloc(&p->d_perm, (size_t)max_batch, "cudaMalloc(perm)")) ||
         (st = dmalloc(&p->d_tiles, (size_t)p->max_tiles, "cudaMalloc(tiles)")) ||
         (st = dmalloc(&p->d_ntiles, 1, "cudaMalloc(ntiles)")) ||
-        (st = dmalloc(&p->d_tbase, (size_t)(NZ * NZ + 1), "cudaMalloc(tbase)")) ||
+        (st = dmalloc(&p->d_tbase, (size_t)(bin_keys_max(NZ) + 1), "cudaMalloc(tbase)")) ||
         (st = dmalloc(&p->d_counter, 1, "cudaMalloc(counter)")) ||
         (st = dmalloc(&p->d_err, 1, "cudaMalloc(err)")) ||
         (st = dmalloc_bytes(&p->d_gb_zeta, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_zeta)")) ||

@@ -338,14 +338,18 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
 constexpr int kBinThreads = 256;
 constexpr int kBinMaxBlocks = kBinMaxBlocksHost;
 
-__device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sidxB, int b, int B, int NZ, int* err) {
+// Key of element b: (a - 1) NZ + (c - 1) for a pair, ((a - 1) NZ + (c - 1)) NZ + (d - 1)
+// for a triple (sidxC given); -1 past the end or for a species index outside 1..NZ.
+__device__ __forceinline__ int pair_key(const int64_t* sidxA, const int64_t* sidxB, const int64_t* sidxC, int b,
+                                        int B, int NZ, int* err) {
     if (b >= B) return -1;
-    int64_t a = sidxA ? sidxA[b] : 1, c = sidxB ? sidxB[b] : 1;
-    if (a < 1 || a > NZ || c < 1 || c > NZ) {
+    int64_t a = sidxA ? sidxA[b] : 1, c = sidxB ? sidxB[b] : 1, d = sidxC ? sidxC[b] : 1;
+    if (a < 1 || a > NZ || c < 1 || c > NZ || d < 1 || d > NZ) {
         if (err) atomicCAS(err, 0, AOK_ERR_SPECIES);
         return -1;
     }
-    return (int)((a - 1) * NZ + (c - 1));
+    const int k = (int)((a - 1) * NZ + (c - 1));
+    return sidxC ? k * NZ + (int)(d - 1) : k;
 }
 
 // zeros for the three values of a left-out element (see BinBufs::zero3)
@@ -360,17 +364,17 @@ __device__ __forceinline__ void zero_three(void* zero3, int bytes, int b) {
 }
 
 __global__ void __launch_bounds__(kBinThreads) k_bin_count(const int64_t* __restrict__ sidxA,
-                                                            const int64_t* __restrict__ sidxB, int B, int NZ,
+                                                            const int64_t* __restrict__ sidxB,
+                                                            const int64_t* __restrict__ sidxC, int B, int NZ, int np,
                                                             int chunk, int* __restrict__ blockhist,
                                                             int* __restrict__ err, void* zero3, void* zero3b,
                                                             int zero3_bytes) {
     __shared__ int hist[kMaxPairs];
-    const int np = NZ * NZ;
     for (int k = threadIdx.x; k < np; k += blockDim.x) hist[k] = 0;
     __syncthreads();
     const int c0 = blockIdx.x * chunk, c1 = min(B, c0 + chunk);
     for (int b = c0 + threadIdx.x; b < c1; b += blockDim.x) {
-        const int key = pair_key(sidxA, sidxB, b, c1, NZ, err);
+        const int key = pair_key(sidxA, sidxB, sidxC, b, c1, NZ, err);
         if (key >= 0) {
             atomicAdd(&hist[key], 1);
         } else {  // b < c1: a bad species index
@@ -384,14 +388,15 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const int64_t* __rest
 
 constexpr int kBinWarps = kBinThreads / 32;
 __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __restrict__ sidxA,
-                                                              const int64_t* __restrict__ sidxB, int B, int NZ,
-                                                              int chunk, const int* __restrict__ blockhist,
+                                                              const int64_t* __restrict__ sidxB,
+                                                              const int64_t* __restrict__ sidxC, int B, int NZ,
+                                                              int np, int chunk, const int* __restrict__ blockhist,
                                                               int* __restrict__ perm, int4* __restrict__ tiles,
                                                               int* __restrict__ ntiles, int* __restrict__ tbase_out,
                                                               unsigned* __restrict__ counter, int* __restrict__ err) {
     __shared__ int wcount[kBinWarps][kMaxPairs];
     __shared__ int before[kMaxPairs], tot[kMaxPairs], base[kMaxPairs], tbase[kMaxPairs + 1];
-    const int np = NZ * NZ, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nblk = gridDim.x, me = blockIdx.x;
     // per key: elements in earlier blocks, and the total (integer sums, so the
     // order of the shared atomics does not matter)
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
     for (int k = lane; k < np; k += 32) wcount[warp][k] = 0;
     __syncwarp();
     for (int b0 = c0; b0 < c1; b0 += 32) {
-        const int key = pair_key(sidxA, sidxB, b0 + lane, c1, NZ, err);
+        const int key = pair_key(sidxA, sidxB, sidxC, b0 + lane, c1, NZ, err);
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         if (key >= 0 && lane == __ffs(peers) - 1) wcount[warp][key] += __popc(peers);
         __syncwarp();
@@ -473,7 +478,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
     __syncthreads();
     for (int b0 = c0; b0 < c1; b0 += 32) {
         const int b = b0 + lane;
-        const int key = pair_key(sidxA, sidxB, b, c1, NZ, err);
+        const int key = pair_key(sidxA, sidxB, sidxC, b, c1, NZ, err);
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         if (key >= 0) perm[wcount[warp][key] + __popc(peers & ((1u << lane) - 1u))] = b;
         __syncwarp();
@@ -488,11 +493,11 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const int64_t* __re
 // leave it out).
 __global__ void k_bin_identity(int B, int np, int* __restrict__ perm, int4* __restrict__ tiles,
                                int* __restrict__ ntiles, int* __restrict__ tbase, unsigned* __restrict__ counter,
-                               const int64_t* __restrict__ sidxA, const int64_t* __restrict__ sidxB, int NZ,
-                               int* __restrict__ err) {
+                               const int64_t* __restrict__ sidxA, const int64_t* __restrict__ sidxB,
+                               const int64_t* __restrict__ sidxC, int NZ, int* __restrict__ err) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     const int nt = (B + kTileB - 1) / kTileB;
-    if (b < B && (sidxA || sidxB)) (void)pair_key(sidxA, sidxB, b, B, NZ, err);
+    if (b < B && (sidxA || sidxB || sidxC)) (void)pair_key(sidxA, sidxB, sidxC, b, B, NZ, err);
     if (b < B) perm[b] = b;
     if (b * kTileB < B) tiles[b] = make_int4(0, b * kTileB, min(kTileB, B - b * kTileB), 0);
     if (b <= np) tbase[b] = b == 0 ? 0 : nt;  // every element is in species pair 0
@@ -629,7 +634,7 @@ int setup_overlap2c_schedule(aok_plan* p, int ctas, size_t stage_req) {
             return cuda_status(e, "cudaFuncSetAttribute(k_pack2c)");
     }
     p->max_bin_blocks = kBinMaxBlocks;
-    e = cudaMalloc(&p->d_blockhist, sizeof(int) * p->max_bin_blocks * p->NZ * p->NZ);
+    e = cudaMalloc(&p->d_blockhist, sizeof(int) * p->max_bin_blocks * bin_keys_max(p->NZ));
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(blockhist)");
     e = cudaMemcpy(p->d_items, items.data(), sizeof(Item) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(items)");
@@ -668,25 +673,30 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
     return cuda_status(cudaGetLastError(), "k_pack2c");
 }
 
-int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
-                    cudaStream_t s) {
+int launch_bin3_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, const int64_t* sidxC,
+                     int64_t B, int NZ, cudaStream_t s) {
+    const int np = sidxC ? NZ * NZ * NZ : NZ * NZ;
     // blocks of >= 512 elements; at most 512 blocks, and few enough that each
     // block's read of all block histograms stays <= 16K entries
-    const int maxb = std::min(kBinMaxBlocks, std::max(128, 16384 / (NZ * NZ)));
+    const int maxb = std::min(kBinMaxBlocks, std::max(128, 16384 / np));
     const int chunk = (int)std::max<int64_t>(512, (B + maxb - 1) / maxb);
     const int nblk = (int)((B + chunk - 1) / chunk);
-    if (NZ == 1 || (!sidxA && !sidxB)) {
-        const int np = NZ * NZ;
+    if (NZ == 1 || (!sidxA && !sidxB && !sidxC)) {
         k_bin_identity<<<(int)((std::max<int64_t>(B, np + 1) + 255) / 256), 256, 0, s>>>(
-            (int)B, np, bb.perm, bb.tiles, bb.ntiles, bb.tbase, bb.counter, sidxA, sidxB, NZ, bb.err);
+            (int)B, np, bb.perm, bb.tiles, bb.ntiles, bb.tbase, bb.counter, sidxA, sidxB, sidxC, NZ, bb.err);
         return cuda_status(cudaGetLastError(), "k_bin_identity");
     }
-    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.err, bb.zero3,
-                                             bb.zero3b, bb.zero3_bytes);
+    k_bin_count<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, sidxC, (int)B, NZ, np, chunk, bb.blockhist, bb.err,
+                                             bb.zero3, bb.zero3b, bb.zero3_bytes);
     AOK_TRY_ST(cuda_status(cudaGetLastError(), "k_bin_count"));
-    k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, (int)B, NZ, chunk, bb.blockhist, bb.perm, bb.tiles,
-                                               bb.ntiles, bb.tbase, bb.counter, bb.err);
+    k_bin_scatter<<<nblk, kBinThreads, 0, s>>>(sidxA, sidxB, sidxC, (int)B, NZ, np, chunk, bb.blockhist, bb.perm,
+                                               bb.tiles, bb.ntiles, bb.tbase, bb.counter, bb.err);
     return cuda_status(cudaGetLastError(), "k_bin_scatter");
+}
+
+int launch_bin_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, int64_t B, int NZ,
+                    cudaStream_t s) {
+    return launch_bin3_into(bb, sidxA, sidxB, nullptr, B, NZ, s);
 }
 
 int launch_bin(aok_plan* p, const int64_t* sidxA, const int64_t* sidxB, int64_t B, cudaStream_t s) {

@@ -1,5 +1,5 @@
-// overlap3c.cu -- 3-center overlap host side: primitive-triple records, the
-// item list, and the aok_overlap3c_gb entry point.  The kernel is in
+// overlap3c.cu -- 3-center overlap host side: the compact primitive lists, the
+// item list, and the aok_overlap3c_gb / aok_overlap3c entry points.  The kernel is in
 // overlap3c_kernel.cuh (one instantiation per precision: overlap3c_f32.cu,
 // overlap3c_f64.cu).
 #include <algorithm>
@@ -10,74 +10,38 @@
 
 namespace aok {
 
-__device__ __forceinline__ void fill_pt(PTf& r, double ca, double cb, double cc, double a, double b, double c, int grp) {
-    const double q = a + b + c, x = 3.14159265358979323846 / q, l2e = 1.4426950408889634074;
-    const double kab = a * b / q * l2e, kac = a * c / q * l2e, kbc = b * c / q * l2e;
-    r.w = (float)(ca * cb * cc * (x * sqrt(x)));
-    r.kab_hi = (float)kab;
-    r.kab_lo = (float)(kab - (double)r.kab_hi);
-    r.kac_hi = (float)kac;
-    r.kac_lo = (float)(kac - (double)r.kac_hi);
-    r.kbc_hi = (float)kbc;
-    r.kbc_lo = (float)(kbc - (double)r.kbc_hi);
-    r.ra = (float)(a / q);
-    r.rb = (float)(b / q);
-    r.rc = (float)(c / q);
-    r.oo2q = (float)(0.5 / q);
-    r.grp = (float)grp;
-}
-__device__ __forceinline__ void fill_pt(PTd& r, double ca, double cb, double cc, double a, double b, double c, int) {
-    const double q = a + b + c, x = 3.14159265358979323846 / q;
-    r.w = ca * cb * cc * (x * sqrt(x));
-    r.kab = a * b / q;
-    r.kac = a * c / q;
-    r.kbc = b * c / q;
-    r.ra = a / q;
-    r.rb = b / q;
-    r.rc = c / q;
-    r.oo2q = 0.5 / q;
-}
-
-// One warp per shell triple; lanes sweep the K^3 grid in (ip, jp, kp) order
-// and compact the non-zero-coefficient triples (ballot), preserving order.
+// The primitives of every (species g, shell s): the non-zero-coefficient slots of
+// the padded (ns,K,NZ) tables, compacted in slot order into pz/pc at (g ns + s) K,
+// and their number pn[g ns + s].  One thread per (shell, species).
 template <typename FT>
-__global__ void k_prep3c(typename PTT<FT>::type* __restrict__ pp, int* __restrict__ npp, const FT* __restrict__ zeta,
-                         const FT* __restrict__ coef, int ns, int K) {
-    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (q >= ns * ns * ns) return;
-    const int sc = q % ns, sb = (q / ns) % ns, sa = q / (ns * ns);
-    auto* out = pp + (size_t)q * K * K * K;
+__global__ void k_prim3c(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn, const FT* __restrict__ zeta,
+                         const FT* __restrict__ coef, int ns, int K, int NZ) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns * NZ) return;
+    const int sh = t % ns, g = t / ns;
     int n = 0;
-    const int K3 = K * K * K;
-    for (int e0 = 0; e0 < K3; e0 += 32) {
-        const int e = e0 + lane;
-        const int ip = e / (K * K), jp = (e / K) % K, kp = e % K;
-        double ca = 0, cb = 0, cc = 0, a = 1, b = 1, c = 1;
-        if (e < K3) {
-            ca = (double)coef[sa + ns * ip];
-            cb = (double)coef[sb + ns * jp];
-            cc = (double)coef[sc + ns * kp];
-            a = (double)zeta[sa + ns * ip];
-            b = (double)zeta[sb + ns * jp];
-            c = (double)zeta[sc + ns * kp];
+    for (int k = 0; k < K; ++k) {
+        const size_t o = (size_t)sh + (size_t)ns * (k + (size_t)K * g);
+        const FT c = coef[o];
+        if (c != FT(0)) {
+            pz[(size_t)t * K + n] = zeta[o];
+            pc[(size_t)t * K + n] = c;
+            ++n;
         }
-        const bool valid = e < K3 && ca != 0.0 && cb != 0.0 && cc != 0.0;
-        const unsigned m = __ballot_sync(0xffffffffu, valid);
-        if (valid) fill_pt(out[n + __popc(m & ((1u << lane) - 1u))], ca, cb, cc, a, b, c, ip * K + jp);
-        n += __popc(m);
     }
-    if (lane == 0) npp[q] = n;
+    pn[t] = n;
 }
 
 // Per call, one CTA: the items sorted by estimated cost, heaviest first, so
 // that the kernel's unit queue (item-major) ends with cheap items.  Cost =
-// primitive triples x (E tables + the chunk's products) + a fixed part per
-// item; the f-shell classes (run-time loops, FP64 tables) count four times.
+// primitive triples (the largest count over the species per shell) x (E tables
+// + the chunk's products) + a fixed part per item; the f-shell classes
+// (run-time loops, FP64 tables) count four times.
 // Rank sort in shared memory; more than kOrder3Max items keep the static order.
 constexpr int kOrder3Max = 2048;
 
 __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, const Item3* __restrict__ items,
-                                                 const int* __restrict__ npp, int n, int ns) {
+                                                 const int* __restrict__ pn, int n, int ns, int NZ) {
     __shared__ unsigned long long key[kOrder3Max];
     if (n > kOrder3Max) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = items[i];
@@ -91,7 +55,13 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         const int ppc = pages_per_chunk3(la, lb);
         const int pages = min(ppc, ncart(lc) - it.chunk * ppc);
         const long long per = 12LL * (la + 1) * (lb + 1) * (lc + 1) + 2LL * ncart(la) * ncart(lb) * pages;
-        long long cost = (long long)npp[(it.sa * ns + it.sb) * ns + it.sc] * per * (f ? 4 : 1) + 64;
+        int na = 0, nb = 0, nc = 0;  // primitive counts, the largest over the species
+        for (int g = 0; g < NZ; ++g) {
+            na = max(na, pn[g * ns + it.sa]);
+            nb = max(nb, pn[g * ns + it.sb]);
+            nc = max(nc, pn[g * ns + it.sc]);
+        }
+        long long cost = (long long)na * nb * nc * per * (f ? 4 : 1) + 64;
         cost = min(cost, (long long)0x7FFFFFFF);
         key[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | (unsigned)i;  // ascending key = descending cost
     }
@@ -106,8 +76,9 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
 
 int setup_overlap3c_schedule(aok_plan* p) {
     if (p->d_items3) return AOK_OK;
-    if (p->NZ != 1) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: plan must have NZ = 1");
-    if (p->Lmax > kMaxL3) return set_error(AOK_ERR_UNSUPPORTED, "aok_overlap3c_gb: shells above l = 3");
+    if (p->NZ * p->NZ * p->NZ > kMaxPairs)
+        return set_error(AOK_ERR_UNSUPPORTED, "3C overlap: more than 6 species (NZ^3 > 256 species triples)");
+    if (p->Lmax > kMaxL3) return set_error(AOK_ERR_UNSUPPORTED, "3C overlap: shells above l = 3");
     const int ns = (int)p->ns;
     // every (shell triple, page chunk), statically ordered by class cost
     std::vector<std::pair<int, Item3>> v;
@@ -129,8 +100,7 @@ int setup_overlap3c_schedule(aok_plan* p) {
     std::vector<Item3> items;
     for (auto& x : v) items.push_back(x.second);
     p->nitems3 = (int)items.size();
-    const size_t nrec = (size_t)ns * ns * ns * p->K * p->K * p->K;
-    const size_t rec = p->prec == AOK_PREC_F64 ? sizeof(PTd) : sizeof(PTf);
+    const size_t fsz = p->prec == AOK_PREC_F64 ? sizeof(double) : sizeof(float);
     cudaError_t e;
     if ((e = cudaMalloc(&p->d_items3, sizeof(Item3) * items.size())) != cudaSuccess)
         return cuda_status(e, "cudaMalloc(items3)");
@@ -139,28 +109,34 @@ int setup_overlap3c_schedule(aok_plan* p) {
     if ((e = cudaMemcpy(p->d_items3, items.data(), sizeof(Item3) * items.size(), cudaMemcpyHostToDevice)) !=
         cudaSuccess)
         return cuda_status(e, "cudaMemcpy(items3)");
-    if ((e = cudaMalloc(&p->d_pp3, nrec * rec)) != cudaSuccess) return cuda_status(e, "cudaMalloc(pp3)");
-    if ((e = cudaMalloc(&p->d_npp3, sizeof(int) * (size_t)ns * ns * ns)) != cudaSuccess)
-        return cuda_status(e, "cudaMalloc(npp3)");
+    // compact primitive lists: zeta then coef, each ns*K*NZ, and the ns*NZ lengths
+    if ((e = cudaMalloc(&p->d_pp3, 2 * fsz * (size_t)(ns * p->K * p->NZ))) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(prim3)");
+    if ((e = cudaMalloc(&p->d_npp3, sizeof(int) * (size_t)(ns * p->NZ))) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(nprim3)");
     return AOK_OK;
 }
 
-int launch_overlap3c(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
-                     cudaStream_t s) {
-    (void)B;
-    const int n = (int)(p->ns * p->ns * p->ns), th = 128, bl = (n * 32 + th - 1) / th;
+// The 3C overlap after the schedule is set up: compact primitive lists of the
+// padded (zeta, coef) tables, per-call item order, then the kernel over the
+// plan's bins (binned by the caller).
+int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
+                     const void* posC, double lengthscale, cudaStream_t s) {
+    const int nsz = (int)(p->ns * p->NZ), th = 128, bl = (nsz + th - 1) / th;
+    const size_t nt = (size_t)(p->ns * p->K * p->NZ);
     if (p->prec == AOK_PREC_F64)
-        k_prep3c<double><<<bl, th, 0, s>>>((PTd*)p->d_pp3, p->d_npp3, (const double*)p->d_gb_zeta,
-                                           (const double*)p->d_gb_coef, (int)p->ns, (int)p->K);
+        k_prim3c<double><<<bl, th, 0, s>>>((double*)p->d_pp3, (double*)p->d_pp3 + nt, p->d_npp3, (const double*)zeta,
+                                           (const double*)coef, (int)p->ns, (int)p->K, (int)p->NZ);
     else
-        k_prep3c<float><<<bl, th, 0, s>>>((PTf*)p->d_pp3, p->d_npp3, (const float*)p->d_gb_zeta,
-                                          (const float*)p->d_gb_coef, (int)p->ns, (int)p->K);
-    int st = cuda_status(cudaGetLastError(), "k_prep3c");
+        k_prim3c<float><<<bl, th, 0, s>>>((float*)p->d_pp3, (float*)p->d_pp3 + nt, p->d_npp3, (const float*)zeta,
+                                          (const float*)coef, (int)p->ns, (int)p->K, (int)p->NZ);
+    int st = cuda_status(cudaGetLastError(), "k_prim3c");
     if (st != AOK_OK) return st;
-    k_order3c<<<1, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, p->nitems3, (int)p->ns);
+    k_order3c<<<1, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, p->nitems3, (int)p->ns,
+                                (int)p->NZ);
     if ((st = cuda_status(cudaGetLastError(), "k_order3c")) != AOK_OK) return st;
-    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, s);
-    return launch_ov3_f32(p, out, posA, posB, posC, s);
+    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s);
+    return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s);
 }
 
 }  // namespace aok
@@ -171,6 +147,7 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
                                 const void* coef, const void* alpha, const void* posA, const void* posB,
                                 const void* posC, int64_t B, void* stream) {
     if (!p) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: null plan");
+    if (p->NZ != 1) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: plan must have NZ = 1");
     if (B < 0) return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: negative batch");
     if (B > p->max_batch) return set_error(AOK_ERR_LENGTH, "aok_overlap3c_gb: batch exceeds the plan's max_batch");
     int st = setup_overlap3c_schedule(p);
@@ -181,5 +158,24 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
     cudaStream_t s = (cudaStream_t)stream;
     if ((st = launch_gb_pad(p, nprim, prim_offset, coef, alpha, s)) != AOK_OK) return st;
     if ((st = launch_bin(p, nullptr, nullptr, B, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, posA, posB, posC, B, s);
+    return launch_overlap3c(p, out, p->d_gb_zeta, p->d_gb_coef, posA, posB, posC, 1.0, s);
+}
+
+extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
+                             const void* posB, const void* posC, const int64_t* sidxA, const int64_t* sidxB,
+                             const int64_t* sidxC, int64_t B, double lengthscale, void* stream) {
+    static const char* who = "aok_overlap3c";
+    if (!p) return set_error(AOK_ERR_INVALID, std::string(who) + ": null plan");
+    if (B < 0) return set_error(AOK_ERR_INVALID, std::string(who) + ": negative batch");
+    if (B > p->max_batch) return set_error(AOK_ERR_LENGTH, std::string(who) + ": batch exceeds the plan's max_batch");
+    int st = setup_overlap3c_schedule(p);
+    if (st != AOK_OK) return st;
+    if (B == 0) return AOK_OK;
+    if (!out || !zeta || !coef || !posA || !posB || !posC || !sidxA || !sidxB || !sidxC)
+        return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    ++p->gen;  // the plan's bins change
+    const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
+    if ((st = launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s)) != AOK_OK) return st;
+    return launch_overlap3c(p, out, zeta, coef, posA, posB, posC, lengthscale, s);
 }

@@ -70,12 +70,21 @@ template <> struct Geo3<double> {
     double R2[3];
 };
 
-__device__ __forceinline__ void load_geo3(Geo3<float>& g, const float* A, const float* B, const float* C) {
+// Positions multiplied by s when use_s (the orbital path's lengthscale), then
+// the pair differences; FP32: the differences of the FP32 values exact in FP64.
+__device__ __forceinline__ void load_geo3(Geo3<float>& g, const float* A, const float* B, const float* C, float s,
+                                          bool use_s) {
     double r[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double ab = (double)A[c] - (double)B[c], ac = (double)A[c] - (double)C[c],
-                     bc = (double)B[c] - (double)C[c];  // exact differences of FP32 values
+        float a = A[c], b = B[c], cc = C[c];
+        if (use_s) {
+            a *= s;
+            b *= s;
+            cc *= s;
+        }
+        const double ab = (double)a - (double)b, ac = (double)a - (double)cc,
+                     bc = (double)b - (double)cc;  // exact differences of FP32 values
         g.AB[c] = (float)ab;
         g.AC[c] = (float)ac;
         g.BC[c] = (float)bc;
@@ -89,14 +98,21 @@ __device__ __forceinline__ void load_geo3(Geo3<float>& g, const float* A, const 
         g.R2lo[i] = (float)(r[i] - (double)g.R2[i]);
     }
 }
-__device__ __forceinline__ void load_geo3(Geo3<double>& g, const double* A, const double* B, const double* C) {
+__device__ __forceinline__ void load_geo3(Geo3<double>& g, const double* A, const double* B, const double* C,
+                                          double s, bool use_s) {
 #pragma unroll
     for (int i = 0; i < 3; ++i) g.R2[i] = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        g.AB[c] = A[c] - B[c];
-        g.AC[c] = A[c] - C[c];
-        g.BC[c] = B[c] - C[c];
+        double a = A[c], b = B[c], cc = C[c];
+        if (use_s) {
+            a *= s;
+            b *= s;
+            cc *= s;
+        }
+        g.AB[c] = a - b;
+        g.AC[c] = a - cc;
+        g.BC[c] = b - cc;
         g.R2[0] += g.AB[c] * g.AB[c];
         g.R2[1] += g.AC[c] * g.AC[c];
         g.R2[2] += g.BC[c] * g.BC[c];
@@ -146,12 +162,65 @@ struct Class3 {
     static constexpr int PPC = pages_per_chunk3(LA, LB);
 };
 
+// Record of one primitive triple, FP64-computed (the product's weight, the
+// exponent coefficients, the exponent ratios and 1/2q); grp groups the triples
+// of one (ip, jp) for the FP32 path's compensated folding.
+__device__ __forceinline__ void fill_pt(PTf& r, double ca, double cb, double cc, double a, double b, double c, int grp) {
+    const double q = a + b + c, x = 3.14159265358979323846 / q, l2e = 1.4426950408889634074;
+    const double kab = a * b / q * l2e, kac = a * c / q * l2e, kbc = b * c / q * l2e;
+    r.w = (float)(ca * cb * cc * (x * sqrt(x)));
+    r.kab_hi = (float)kab;
+    r.kab_lo = (float)(kab - (double)r.kab_hi);
+    r.kac_hi = (float)kac;
+    r.kac_lo = (float)(kac - (double)r.kac_hi);
+    r.kbc_hi = (float)kbc;
+    r.kbc_lo = (float)(kbc - (double)r.kbc_hi);
+    r.ra = (float)(a / q);
+    r.rb = (float)(b / q);
+    r.rc = (float)(c / q);
+    r.oo2q = (float)(0.5 / q);
+    r.grp = (float)grp;
+}
+__device__ __forceinline__ void fill_pt(PTd& r, double ca, double cb, double cc, double a, double b, double c, int) {
+    const double q = a + b + c, x = 3.14159265358979323846 / q;
+    r.w = ca * cb * cc * (x * sqrt(x));
+    r.kab = a * b / q;
+    r.kac = a * c / q;
+    r.kbc = b * c / q;
+    r.ra = a / q;
+    r.rb = b / q;
+    r.rc = c / q;
+    r.oo2q = 0.5 / q;
+}
+
+// The three shells' primitives for one work unit (the tile's species): the
+// compact lists of non-zero (zeta, coef) slots (k_prim3c) and their lengths.
+template <typename FT>
+struct Prim3 {
+    const FT* z[3];
+    const FT* c[3];
+    int n[3];
+};
+
+// Records q0 .. q0 + 31 of the unit into the warp's buffer, one per lane (FP64
+// arithmetic), in (ip, jp, kp) order; the caller brackets it with __syncwarp.
+template <typename PT, typename FT>
+__device__ __forceinline__ void gen_records3(PT* buf, const Prim3<FT>& pr, int q0, int n, int lane) {
+    const int q = q0 + lane;
+    if (q >= n) return;
+    const int nb = pr.n[1], nc = pr.n[2];
+    const int ip = q / (nb * nc), jp = (q / nc) % nb, kp = q % nc;
+    fill_pt(buf[lane], (double)pr.c[0][ip], (double)pr.c[1][jp], (double)pr.c[2][kp], (double)pr.z[0][ip],
+            (double)pr.z[1][jp], (double)pr.z[2][kp], ip * nb + jp);
+}
+
 // lin (0-based, within the block) -> offset in the lane's panel slab;
 // block element (i, j, k) = (lin % NA, (lin / NA) % NB, lin / PS).
 // Only pages inside [kp0, kp1) (block-local) are stored.
 template <int LA, int LB, int LC, int C>
-__device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const Geo3<float> g, float* dst, int N,
+__device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Geo3<float> g, float* dst, int N,
                                        int kp0, int kp1, bool valid) {
+    const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
@@ -165,10 +234,17 @@ __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const 
 #pragma unroll
     for (int m = 0; m < M; ++m) lo[m] = 0.f;
     float prev = -1.f;
-    for (int q = 0; q < n; ++q) {
-        const float4 r0 = __ldg(reinterpret_cast<const float4*>(pp + q));
-        const float4 r1 = __ldg(reinterpret_cast<const float4*>(pp + q) + 1);
-        const float4 r2 = __ldg(reinterpret_cast<const float4*>(pp + q) + 2);
+#pragma unroll 1
+    for (int q0 = 0; q0 < n; q0 += 32) {
+      __syncwarp();
+      gen_records3(buf, pr, q0, n, lane);
+      __syncwarp();
+      const int m = min(32, n - q0);
+#pragma unroll 1
+      for (int q = 0; q < m; ++q) {
+        const float4 r0 = reinterpret_cast<const float4*>(buf + q)[0];
+        const float4 r1 = reinterpret_cast<const float4*>(buf + q)[1];
+        const float4 r2 = reinterpret_cast<const float4*>(buf + q)[2];
         const float w = r0.x;
         if (r2.w != prev) {
 #pragma unroll
@@ -190,7 +266,7 @@ __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const 
                          ((r0.z * g.R2[0] + r0.y * g.R2lo[0]) + (r1.x * g.R2[1] + r0.w * g.R2lo[1]) +
                           (r1.z * g.R2[2] + r1.y * g.R2lo[2])) +
                          (e1 + e2);
-        const float e000 = (exp2f(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
+        const float e000 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
         const float ra = r1.w, rb = r2.x, rc = r2.y, o2q = r2.z;
         float Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
         build_E3<LA, LB, LC, float>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
@@ -213,6 +289,7 @@ __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const 
                             fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
                     }
                 }
+      }
     }
     if (!valid) return;
 #pragma unroll
@@ -228,19 +305,27 @@ __device__ __noinline__ void run_item3(const PTf* __restrict__ pp, int n, const 
 }
 
 template <int LA, int LB, int LC, int C>
-__device__ __noinline__ void run_item3(const PTd* __restrict__ pp, int n, const Geo3<double> g, double* dst, int N,
+__device__ __noinline__ void run_item3(const Prim3<double> pr, PTd* buf, const Geo3<double> g, double* dst, int N,
                                        int kp0, int kp1, bool valid) {
+    const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
     double acc[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) acc[m] = 0.0;
-    for (int q = 0; q < n; ++q) {
-        const double2 r0 = __ldg(reinterpret_cast<const double2*>(pp + q));
-        const double2 r1 = __ldg(reinterpret_cast<const double2*>(pp + q) + 1);
-        const double2 r2 = __ldg(reinterpret_cast<const double2*>(pp + q) + 2);
-        const double2 r3 = __ldg(reinterpret_cast<const double2*>(pp + q) + 3);
+#pragma unroll 1
+    for (int q0 = 0; q0 < n; q0 += 32) {
+      __syncwarp();
+      gen_records3(buf, pr, q0, n, lane);
+      __syncwarp();
+      const int m = min(32, n - q0);
+#pragma unroll 1
+      for (int q = 0; q < m; ++q) {
+        const double2 r0 = reinterpret_cast<const double2*>(buf + q)[0];
+        const double2 r1 = reinterpret_cast<const double2*>(buf + q)[1];
+        const double2 r2 = reinterpret_cast<const double2*>(buf + q)[2];
+        const double2 r3 = reinterpret_cast<const double2*>(buf + q)[3];
         const double w = r0.x, kab = r0.y, kac = r1.x, kbc = r1.y, ra = r2.x, rb = r2.y, rc = r3.x, o2q = r3.y;
         const double e000 = exp(-(kab * g.R2[0] + kac * g.R2[1] + kbc * g.R2[2])) * w;
         double Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
@@ -263,6 +348,7 @@ __device__ __noinline__ void run_item3(const PTd* __restrict__ pp, int n, const 
                         acc[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, acc[lin - L0]);
                     }
                 }
+      }
     }
     if (!valid) return;
 #pragma unroll
@@ -322,8 +408,9 @@ __device__ __forceinline__ double pt_exponent(const PTd* r, const double (&R2)[3
 }
 
 template <typename PT, typename FT>
-__device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const Geo3<FT> g, FT* dst, int N, int kp0,
+__device__ __noinline__ void run_item3_f(const Prim3<FT> pr, PT* buf, const Geo3<FT> g, FT* dst, int N, int kp0,
                                          int kp1, int cls, int chunk, bool valid) {
+    const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     const int c = cls - kClsF3, la = c >> 4, lb = (c >> 2) & 3, lc = c & 3;
     const int NA = ncart(la), NB = ncart(lb), NC = ncart(lc), PS = NA * NB, N1 = 2 * la + 1, N2 = 2 * lb + 1;
     const int ppc = pages_per_chunk3(la, lb);
@@ -346,8 +433,15 @@ __device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const
         if constexpr (sizeof(FT) == 4) R2[a] += (double)g.R2lo[a];
     }
     double E[3][4][4][4];
-    for (int q = 0; q < n; ++q) {
-        const PT* r = pp + q;
+#pragma unroll 1
+    for (int q0 = 0; q0 < n; q0 += 32) {
+      __syncwarp();
+      gen_records3(buf, pr, q0, n, lane);
+      __syncwarp();
+      const int m = min(32, n - q0);
+#pragma unroll 1
+      for (int qq = 0; qq < m; ++qq) {
+        const PT* r = buf + qq;
         const double w = (double)r->w, ra = (double)r->ra, rb = (double)r->rb, rc = (double)r->rc,
                      o2q = (double)r->oo2q;
         const double e000 = exp(-pt_exponent(r, R2)) * w;
@@ -367,6 +461,7 @@ __device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const
                 }
             }
         }
+      }
     }
     if (!valid) return;
     for (int m = 0; m < M; ++m) {
@@ -379,8 +474,8 @@ __device__ __noinline__ void run_item3_f(const PT* __restrict__ pp, int n, const
 }
 
 template <typename PT, typename FT, int LA, int LB, int LC>
-__device__ __forceinline__ void run_chunks3(int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N, int kp0,
-                                            int kp1, bool valid) {
+__device__ __forceinline__ void run_chunks3(int chunk, const Prim3<FT>& pp, PT* n, const Geo3<FT>& g, FT* dst, int N,
+                                            int kp0, int kp1, bool valid) {
     constexpr int NCH = nchunks3(LA, LB, LC);
     switch (chunk) {
         case 0: run_item3<LA, LB, LC, 0>(pp, n, g, dst, N, kp0, kp1, valid); break;
@@ -393,9 +488,10 @@ __device__ __forceinline__ void run_chunks3(int chunk, const PT* pp, int n, cons
     }
 }
 
+// pp: the unit's primitive lists; n: the warp's record buffer
 template <typename PT, typename FT, bool F3>
-__device__ __forceinline__ void dispatch3(int cls, int chunk, const PT* pp, int n, const Geo3<FT>& g, FT* dst, int N,
-                                          int kp0, int kp1, bool valid) {
+__device__ __forceinline__ void dispatch3(int cls, int chunk, const Prim3<FT>& pp, PT* n, const Geo3<FT>& g, FT* dst,
+                                          int N, int kp0, int kp1, bool valid) {
     if constexpr (F3) {
         if (cls >= kClsF3) {
             run_item3_f<PT, FT>(pp, n, g, dst, N, kp0, kp1, cls, chunk, valid);
@@ -421,14 +517,17 @@ struct Ov3Params {
     const FT* posA;
     const FT* posB;
     const FT* posC;
-    const typename PTT<FT>::type* pp;
-    const int* npp;
+    const FT* pz;        // compact primitive lists: zeta, coef of (species g, shell s) at (g ns + s) K
+    const FT* pc;
+    const int* pn;       // their lengths, (g ns + s)
     const int* perm;
     const int4* tiles;
     const int* ntiles;
     unsigned* counter;
     const Item3* items;  // every (shell triple, page chunk), heaviest first (k_order3c)
-    int nitems, ns, K, N;
+    int nitems, ns, K, N, NZ;
+    FT scale;
+    int use_scale;
     int boff[kMaxShells + 1];
 };
 
@@ -442,7 +541,9 @@ struct Ov3Params {
 // warps per SM (<= 168 registers).
 template <typename FT, bool F3>
 __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
-    const int lane = threadIdx.x & 31;
+    using PT = typename PTT<FT>::type;
+    __shared__ PT recbuf[kThreads3 / 32][32];  // each warp's current 32 records
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ntiles = *P.ntiles;
     const unsigned total = (unsigned)ntiles * (unsigned)P.nitems;
     const size_t N2 = (size_t)P.N * P.N, N3 = N2 * P.N;
@@ -456,26 +557,39 @@ __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constan
         const bool valid = lane < td.z;
         const int b = P.perm[td.y + (valid ? lane : 0)];
         Geo3<FT> g;
-        load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b);
+        load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b, P.scale,
+                  P.use_scale != 0);
         const Item3 wi = P.items[it];
-        const int q = (wi.sa * P.ns + wi.sb) * P.ns + wi.sc;
-        const int n = __ldg(P.npp + q);
+        // the tile's species triple (key ((ga NZ) + gb) NZ + gc; 0 on the single-species path)
+        const int ga = td.x / (P.NZ * P.NZ), gb = (td.x / P.NZ) % P.NZ, gc = td.x % P.NZ;
+        Prim3<FT> pr;
+        const int la = ga * P.ns + wi.sa, lb = gb * P.ns + wi.sb, lc = gc * P.ns + wi.sc;
+        pr.z[0] = P.pz + (size_t)la * P.K;
+        pr.c[0] = P.pc + (size_t)la * P.K;
+        pr.n[0] = __ldg(P.pn + la);
+        pr.z[1] = P.pz + (size_t)lb * P.K;
+        pr.c[1] = P.pc + (size_t)lb * P.K;
+        pr.n[1] = __ldg(P.pn + lb);
+        pr.z[2] = P.pz + (size_t)lc * P.K;
+        pr.c[2] = P.pc + (size_t)lc * P.K;
+        pr.n[2] = __ldg(P.pn + lc);
         FT* dst = P.out + (size_t)b * N3 + (size_t)P.boff[wi.sc] * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-        dispatch3<typename PTT<FT>::type, FT, F3>(wi.cls, wi.chunk, P.pp + (size_t)q * P.K * P.K * P.K, n, g, dst,
-                                                  P.N, 0, kAllPages3, valid);
+        dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, recbuf[warp], g, dst, P.N, 0, kAllPages3, valid);
     }
 }
 
 template <typename FT, bool F3>
-inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, cudaStream_t s) {
+inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                      cudaStream_t s) {
     Ov3Params<FT> P;
     memset(&P, 0, sizeof(P));
     P.out = (FT*)out;
     P.posA = (const FT*)posA;
     P.posB = (const FT*)posB;
     P.posC = (const FT*)posC;
-    P.pp = (const typename PTT<FT>::type*)p->d_pp3;
-    P.npp = p->d_npp3;
+    P.pz = (const FT*)p->d_pp3;
+    P.pc = (const FT*)p->d_pp3 + p->ns * p->K * p->NZ;
+    P.pn = p->d_npp3;
     P.perm = p->d_perm;
     P.tiles = p->d_tiles;
     P.ntiles = p->d_ntiles;
@@ -485,6 +599,9 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.ns = (int)p->ns;
     P.K = (int)p->K;
     P.N = (int)p->N;
+    P.NZ = (int)p->NZ;
+    P.scale = (FT)lengthscale;
+    P.use_scale = (FT)lengthscale != FT(1);
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
     auto kern = k_overlap3c<FT, F3>;
     int occ = 0;

@@ -210,7 +210,41 @@ def batch_overlap(basis, *args, FT=None, device_out=False):
 # --------------------------------------------------------------------------
 
 
-def batch_overlap_3c_(out, bc, posA, posB, posC):
+def _orb_overlap_3c_(out, cob, XA, XB, XC):
+    """3C overlap on the species-aware path (no reference counterpart): PState batches
+    XA, XB, XC; out (N, N, N, B) on the device."""
+    FT = out.dtype
+    XA, XB, XC = as_pstates(XA), as_pstates(XB), as_pstates(XC)
+    B = len(XA)
+    if len(XB) != B or len(XC) != B:
+        raise RuntimeError(f"XA, XB and XC must have equal length; got {len(XA)}, {len(XB)} and {len(XC)}")
+    N = cob.nbf_total
+    _check_out(out, (N, N, N, B), "batch_overlap_3c!")
+    sA, sB, sC = (species_indices(cob.zlist, X.species) for X in (XA, XB, XC))
+    if B == 0:
+        return out
+    _dev.require_cuda()
+    plan = _dev.plan_for(cob.ls, cob.K, cob.nspecies, _dev.prec_of(FT), B)
+    zeta, coef = _dev.to_colmajor(cob.zeta, FT), _dev.to_colmajor(cob.coef, FT)
+    pA, pB, pC = (_dev.to_colmajor(X.pos, FT) for X in (XA, XB, XC))
+    gA, gB, gC = _dev_int64(sA), _dev_int64(sB), _dev_int64(sC)
+    _lib.check(_lib.load().aok_overlap3c(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(pA),
+                                         _dev.ptr(pB), _dev.ptr(pC), _dev.ptr(gA), _dev.ptr(gB), _dev.ptr(gC), B,
+                                         float(cob.lengthscale), _dev.stream()))
+    return out
+
+
+def batch_overlap_3c_(out, bc, posA, posB, posC, *args):
+    """batch_overlap_3c!(out, basis, ...): CompiledBasis with Length positions (the
+    reference's GaussianBasis path), or a CartesianGTOBasis / orbital basis with PState
+    batches (species-aware; an orbital basis is compiled on the call, or from (ps, st))."""
+    if isinstance(bc, (CartesianGTOBasis, AtomicOrbitals)):
+        if isinstance(bc, AtomicOrbitals):
+            if len(args) == 2:
+                bc, _ = _compiled_from_ps(bc, args[0], out.dtype)
+            else:
+                bc = compile_basis(bc, dtype=out.dtype)
+        return _orb_overlap_3c_(out, bc, posA, posB, posC)
     FT = out.dtype
     npft = np.float64 if FT == torch.float64 else np.float32
     pa, pb, pc = to_bohr(posA, npft), to_bohr(posB, npft), to_bohr(posC, npft)
@@ -236,11 +270,19 @@ def batch_overlap_3c_(out, bc, posA, posB, posC):
     return out
 
 
-def batch_overlap_3c(bc, posA, posB, posC, FT=torch.float64, device_out=False):
-    B = np.shape(posA.value if hasattr(posA, "value") else posA)[1]
-    N = bc.nbf_total
+def batch_overlap_3c(bc, posA, posB, posC, *args, FT=None, device_out=False):
+    """batch_overlap_3c(basis, ...) -> (N, N, N, B); see batch_overlap_3c_."""
+    if isinstance(bc, (CartesianGTOBasis, AtomicOrbitals)):
+        if FT is None:
+            FT = _ps_dtype(args[0], posA) if len(args) == 2 else torch.float64
+        B = len(as_pstates(posA))
+        N = bc.nbf_total if isinstance(bc, CartesianGTOBasis) else compile_struct(bc)["nbf_total"]
+    else:
+        FT = torch.float64 if FT is None else FT
+        B = np.shape(posA.value if hasattr(posA, "value") else posA)[1]
+        N = bc.nbf_total
     out = _dev.colmajor_empty((N, N, N, B), FT)
-    batch_overlap_3c_(out, bc, posA, posB, posC)
+    batch_overlap_3c_(out, bc, posA, posB, posC, *args)
     return out if device_out else out.cpu()
 
 

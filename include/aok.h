@@ -176,6 +176,20 @@ int aok_overlap3c_gb(aok_plan* plan, void* out, const int64_t* nprim,
                      const int64_t* prim_offset, const void* coef, const void* alpha,
                      const void* posA, const void* posB, const void* posC, int64_t B,
                      void* stream);
+/*
+ * Batched 3-center overlap on the species-aware (orbital) path: no reference
+ * counterpart (the reference computes the 3C overlap for a CompiledBasis only,
+ * src/integrals/kernels_3c.jl:183-222, and lists the orbital-path 3C overlap as
+ * not implemented).  Centre A of element b uses species sidxA[b] (1-based), and
+ * so on, with the padded (ns,K,NZ) zeta, coef of aok_overlap2c and its
+ * zero-coefficient skip; positions (3,B) times lengthscale.  out (N,N,N,B) in
+ * the reference's aliased 3C block layout.  NZ^3 <= 256 (at most 6 species);
+ * elements are binned by species triple.  A species index outside 1..NZ sets
+ * the plan's error word (aok_plan_check) and the element's slab is not written.
+ */
+int aok_overlap3c(aok_plan* plan, void* out, const void* zeta, const void* coef, const void* posA,
+                  const void* posB, const void* posC, const int64_t* sidxA, const int64_t* sidxB,
+                  const int64_t* sidxC, int64_t B, double lengthscale, void* stream);
 
 /*
  * Kernel pullback of the species-aware 2C overlap: dcoef and dalpha

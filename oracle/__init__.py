@@ -57,9 +57,11 @@ def lib():
         L.aokor_evaluate_pbx.argtypes = [_d, _d, _d, i64, i64]
         L.aokor_overlap2c_orb_dpos.argtypes = [_d, _d, _d, i64, i64, i64, _i64, _d, _d, _i64, _i64, _d, _d, i64,
                                                dbl, cint]
+        L.aokor_overlap3c_orb.argtypes = [_d, i64, i64, i64, _i64, _d, _d, _i64, _i64, _i64, _d, _d, _d, i64, dbl,
+                                          cint]
         L.aokor_radials_pb.argtypes = [_d, _d, _d, _d, _i64, _d, _d, _i64, i64, i64, i64, i64, cint]
         for name in ("aokor_overlap2c_gb", "aokor_overlap2c_orb", "aokor_overlap3c_gb", "aokor_overlap2c_orb_pb",
-                     "aokor_overlap2c_orb_dpos"):
+                     "aokor_overlap2c_orb_dpos", "aokor_overlap3c_orb"):
             getattr(L, name).restype = cint
         _lib = L
     return _lib
@@ -121,6 +123,23 @@ def overlap3c_gb(ls, nprim, coef, alpha, posA, posB, posC, nthreads=1):
     out = np.zeros((N, N, N, B), order="F")
     lib().aokor_overlap3c_gb(_p(out), len(ls), _p(ls), _p(nprim), _p(off), _p(_f(coef)),
                              _p(_f(alpha)), _p(posA), _p(posB), _p(posC), B, nthreads)
+    return out
+
+
+def overlap3c_orb(ls, coef, zeta, sidxA, sidxB, sidxC, posA, posB, posC, lengthscale=1.0, nthreads=1):
+    """3C overlap on the species-aware path (no reference counterpart): (N,N,N,B), centre
+    species from sidxA/B/C (1-based), padded (ns,K,NZ) coef/zeta, zero-coefficient skip."""
+    ls = _i(ls)
+    coef, zeta = _f(coef), _f(zeta)
+    ns, K, NZ = zeta.shape
+    posA, posB, posC = _f(posA), _f(posB), _f(posC)
+    B = posA.shape[1]
+    N = int(_nbf(ls).sum())
+    out = np.zeros((N, N, N, B), order="F")
+    st = lib().aokor_overlap3c_orb(_p(out), ns, K, NZ, _p(ls), _p(coef), _p(zeta), _p(_i(sidxA)), _p(_i(sidxB)),
+                                   _p(_i(sidxC)), _p(posA), _p(posB), _p(posC), B, float(lengthscale), nthreads)
+    if st:
+        raise ValueError("species index outside 1..NZ")
     return out
 
 

@@ -413,6 +413,82 @@ static void md_E3(double* E, int TM, int IM, int la1, int lb1, int lc1,
     }
 }
 
+/* One shell-triple block of one batch element: the primitive loop and the  */
+/* aliased contraction of batch_V_kernel! (kernels_3c.jl:12-162).  Each     */
+/* centre's primitives come as (coef, alpha) lists with a stride; with      */
+/* skip_zero a triple with a zero coefficient is skipped (the orbital path, */
+/* padded slots).  Ebuf: 3 * TM*IM^3, blk: NBF^3 doubles.                   */
+static void v3_block(double* out, int64_t N, int64_t b, const int64_t* ls, const int64_t* boff,
+                     int64_t s_a, int64_t s_b, int64_t s_c,
+                     const double* ca_v, const double* aa_v, int64_t na, int64_t sta,
+                     const double* cb_v, const double* ab_v, int64_t nb, int64_t stb,
+                     const double* cc_v, const double* ac_v, int64_t nc, int64_t stc,
+                     const double* A, const double* Bp, const double* C, int skip_zero,
+                     double* Ebuf, int TM, int IM, double* blk) {
+    size_t esz = (size_t)(TM * IM * IM * IM);
+    int la = (int)ls[s_a], lb = (int)ls[s_b], lc = (int)ls[s_c];
+    int nbf_a = (la + 1) * (la + 2) / 2, nbf_b = (lb + 1) * (lb + 2) / 2,
+        nbf_c = (lc + 1) * (lc + 2) / 2;
+    int N1 = 2 * la + 1, N2 = 2 * lb + 1;
+    for (int q = 0; q < nbf_a * nbf_b * nbf_c; ++q) blk[q] = 0.0;
+    for (int64_t ip = 0; ip < na; ++ip)
+        for (int64_t jp = 0; jp < nb; ++jp)
+            for (int64_t kp = 0; kp < nc; ++kp) {
+                double ca = ca_v[ip * sta], aa = aa_v[ip * sta];
+                double cb = cb_v[jp * stb], ab = ab_v[jp * stb];
+                double cc = cc_v[kp * stc], ac = ac_v[kp * stc];
+                if (skip_zero && (ca == 0.0 || cb == 0.0 || cc == 0.0)) continue;
+                double p = aa + ab;
+                double P[3], Q[3];
+                for (int c = 0; c < 3; ++c) P[c] = (aa * A[c] + ab * Bp[c]) / p;
+                double q = p + ac;
+                for (int c = 0; c < 3; ++c) Q[c] = (p * P[c] + ac * C[c]) / q;
+                double mu = aa * ab / p;
+                double nu = p * ac / q;
+                double oo2q = 0.5 / q;
+                double prefac = ca * cb * cc * pow(M_PI / q, 1.5);
+                for (int ax = 0; ax < 3; ++ax) {
+                    double AB = A[ax] - Bp[ax];
+                    double PC = P[ax] - C[ax];
+                    double QA = Q[ax] - A[ax];
+                    double QB = Q[ax] - Bp[ax];
+                    double QC = Q[ax] - C[ax];
+                    double e0 = exp((((-mu) * AB) * AB) - ((nu * PC) * PC));
+                    md_E3(Ebuf + ax * esz, TM, IM, la + 1, lb + 1, lc + 1, QA, QB, QC, e0, oo2q);
+                }
+                const double* E;
+                int index1 = 1;
+                for (int ll1 = la; ll1 >= 0; --ll1)
+                    for (int n1 = 0; n1 <= la - ll1; ++n1) {
+                        int m1 = la - ll1 - n1;
+                        int index2 = 1;
+                        for (int ll2 = lb; ll2 >= 0; --ll2)
+                            for (int n2 = 0; n2 <= lb - ll2; ++n2) {
+                                int m2 = lb - ll2 - n2;
+                                int index3 = 1;
+                                for (int ll3 = lc; ll3 >= 0; --ll3)
+                                    for (int n3 = 0; n3 <= lc - ll3; ++n3) {
+                                        int m3 = lc - ll3 - n3;
+                                        int lin = index1 + N1 * (index2 - 1) + N1 * N2 * (index3 - 1);
+                                        double ex, ey, ez;
+                                        E = Ebuf;           ex = E3I(1, ll1 + 1, ll2 + 1, ll3 + 1);
+                                        E = Ebuf + esz;     ey = E3I(1, m1 + 1, m2 + 1, m3 + 1);
+                                        E = Ebuf + 2 * esz; ez = E3I(1, n1 + 1, n2 + 1, n3 + 1);
+                                        blk[lin - 1] += ((ex * ey) * ez) * prefac;
+                                        index3 += 1;
+                                    }
+                                index2 += 1;
+                            }
+                        index1 += 1;
+                    }
+            }
+    for (int kk = 0; kk < nbf_c; ++kk)
+        for (int jj = 0; jj < nbf_b; ++jj)
+            for (int ii = 0; ii < nbf_a; ++ii)
+                out[(boff[s_a] + ii) + N * ((boff[s_b] + jj) + N * ((boff[s_c] + kk) + N * b))] =
+                    blk[ii + nbf_a * jj + nbf_a * nbf_b * kk];
+}
+
 int aokor_overlap3c_gb(double* out, int64_t ns, const int64_t* ls, const int64_t* nprim,
                        const int64_t* prim_off, const double* coef, const double* alpha,
                        const double* posA, const double* posB, const double* posC,
@@ -433,75 +509,68 @@ int aokor_overlap3c_gb(double* out, int64_t ns, const int64_t* ls, const int64_t
         double* Ebuf = (double*)malloc(sizeof(double) * 3 * esz);
         double* blk = (double*)malloc(sizeof(double) * (size_t)(NBF * NBF * NBF));
 #pragma omp for schedule(static)
-        for (int64_t b = 0; b < B; ++b) {
-            const double* A = posA + 3 * b;
-            const double* Bp = posB + 3 * b;
-            const double* C = posC + 3 * b;
+        for (int64_t b = 0; b < B; ++b)
             for (int64_t s_a = 0; s_a < ns; ++s_a)
                 for (int64_t s_b = 0; s_b < ns; ++s_b)
-                    for (int64_t s_c = 0; s_c < ns; ++s_c) {
-                        int la = (int)ls[s_a], lb = (int)ls[s_b], lc = (int)ls[s_c];
-                        int nbf_a = (la + 1) * (la + 2) / 2, nbf_b = (lb + 1) * (lb + 2) / 2,
-                            nbf_c = (lc + 1) * (lc + 2) / 2;
-                        int N1 = 2 * la + 1, N2 = 2 * lb + 1;
-                        for (int q = 0; q < nbf_a * nbf_b * nbf_c; ++q) blk[q] = 0.0;
-                        for (int64_t ip = 0; ip < nprim[s_a]; ++ip)
-                            for (int64_t jp = 0; jp < nprim[s_b]; ++jp)
-                                for (int64_t kp = 0; kp < nprim[s_c]; ++kp) {
-                                    double ca = coef[prim_off[s_a] + ip], aa = alpha[prim_off[s_a] + ip];
-                                    double cb = coef[prim_off[s_b] + jp], ab = alpha[prim_off[s_b] + jp];
-                                    double cc = coef[prim_off[s_c] + kp], ac = alpha[prim_off[s_c] + kp];
-                                    double p = aa + ab;
-                                    double P[3], Q[3];
-                                    for (int c = 0; c < 3; ++c) P[c] = (aa * A[c] + ab * Bp[c]) / p;
-                                    double q = p + ac;
-                                    for (int c = 0; c < 3; ++c) Q[c] = (p * P[c] + ac * C[c]) / q;
-                                    double mu = aa * ab / p;
-                                    double nu = p * ac / q;
-                                    double oo2q = 0.5 / q;
-                                    double prefac = ca * cb * cc * pow(M_PI / q, 1.5);
-                                    for (int ax = 0; ax < 3; ++ax) {
-                                        double AB = A[ax] - Bp[ax];
-                                        double PC = P[ax] - C[ax];
-                                        double QA = Q[ax] - A[ax];
-                                        double QB = Q[ax] - Bp[ax];
-                                        double QC = Q[ax] - C[ax];
-                                        double e0 = exp((((-mu) * AB) * AB) - ((nu * PC) * PC));
-                                        md_E3(Ebuf + ax * esz, TM, IM, la + 1, lb + 1, lc + 1,
-                                              QA, QB, QC, e0, oo2q);
-                                    }
-                                    const double* E;
-                                    int index1 = 1;
-                                    for (int ll1 = la; ll1 >= 0; --ll1)
-                                        for (int n1 = 0; n1 <= la - ll1; ++n1) {
-                                            int m1 = la - ll1 - n1;
-                                            int index2 = 1;
-                                            for (int ll2 = lb; ll2 >= 0; --ll2)
-                                                for (int n2 = 0; n2 <= lb - ll2; ++n2) {
-                                                    int m2 = lb - ll2 - n2;
-                                                    int index3 = 1;
-                                                    for (int ll3 = lc; ll3 >= 0; --ll3)
-                                                        for (int n3 = 0; n3 <= lc - ll3; ++n3) {
-                                                            int m3 = lc - ll3 - n3;
-                                                            int lin = index1 + N1 * (index2 - 1) + N1 * N2 * (index3 - 1);
-                                                            double ex, ey, ez;
-                                                            E = Ebuf;           ex = E3I(1, ll1 + 1, ll2 + 1, ll3 + 1);
-                                                            E = Ebuf + esz;     ey = E3I(1, m1 + 1, m2 + 1, m3 + 1);
-                                                            E = Ebuf + 2 * esz; ez = E3I(1, n1 + 1, n2 + 1, n3 + 1);
-                                                            blk[lin - 1] += ((ex * ey) * ez) * prefac;
-                                                            index3 += 1;
-                                                        }
-                                                    index2 += 1;
-                                                }
-                                            index1 += 1;
-                                        }
-                                }
-                        for (int kk = 0; kk < nbf_c; ++kk)
-                            for (int jj = 0; jj < nbf_b; ++jj)
-                                for (int ii = 0; ii < nbf_a; ++ii)
-                                    out[(boff[s_a] + ii) + N * ((boff[s_b] + jj) + N * ((boff[s_c] + kk) + N * b))] =
-                                        blk[ii + nbf_a * jj + nbf_a * nbf_b * kk];
-                    }
+                    for (int64_t s_c = 0; s_c < ns; ++s_c)
+                        v3_block(out, N, b, ls, boff, s_a, s_b, s_c,
+                                 coef + prim_off[s_a], alpha + prim_off[s_a], nprim[s_a], 1,
+                                 coef + prim_off[s_b], alpha + prim_off[s_b], nprim[s_b], 1,
+                                 coef + prim_off[s_c], alpha + prim_off[s_c], nprim[s_c], 1,
+                                 posA + 3 * b, posB + 3 * b, posC + 3 * b, 0, Ebuf, TM, IM, blk);
+        free(Ebuf);
+        free(blk);
+    }
+    free(boff);
+    return 0;
+}
+
+/* 3C overlap on the species-aware (orbital) path -- no reference counterpart */
+/* (the reference has the 3C kernel for CompiledBasis only): centre A of     */
+/* element b uses species sidxA[b] (1-based), and so on, with the padded     */
+/* (ns,K,NZ) tables of the 2C orbital path and its zero-coefficient skip;    */
+/* positions multiplied by lengthscale.  Returns 4 on a bad species index.   */
+int aokor_overlap3c_orb(double* out, int64_t ns, int64_t K, int64_t NZ, const int64_t* ls,
+                        const double* coef, const double* zeta, const int64_t* sidxA,
+                        const int64_t* sidxB, const int64_t* sidxC, const double* posA,
+                        const double* posB, const double* posC, int64_t B, double lengthscale,
+                        int nthreads) {
+    for (int64_t b = 0; b < B; ++b)
+        if (sidxA[b] < 1 || sidxA[b] > NZ || sidxB[b] < 1 || sidxB[b] > NZ || sidxC[b] < 1 || sidxC[b] > NZ)
+            return 4;
+    int L = lmax_of(ls, ns);
+    int TM = 3 * L + 3, IM = L + 1;
+    int NBF = (L + 1) * (L + 2) / 2;
+    int64_t* boff = (int64_t*)malloc(sizeof(int64_t) * (size_t)(ns + 1));
+    boff[0] = 0;
+    for (int64_t s = 0; s < ns; ++s) boff[s + 1] = boff[s] + (ls[s] + 1) * (ls[s] + 2) / 2;
+    int64_t N = boff[ns];
+    memset(out, 0, sizeof(double) * (size_t)(N * N * N * B));
+    int nt = set_threads(nthreads);
+    (void)nt;
+#pragma omp parallel num_threads(nt)
+    {
+        size_t esz = (size_t)(TM * IM * IM * IM);
+        double* Ebuf = (double*)malloc(sizeof(double) * 3 * esz);
+        double* blk = (double*)malloc(sizeof(double) * (size_t)(NBF * NBF * NBF));
+#pragma omp for schedule(static)
+        for (int64_t b = 0; b < B; ++b) {
+            int64_t ga = sidxA[b] - 1, gb = sidxB[b] - 1, gc = sidxC[b] - 1;
+            double A[3], Bv[3], C[3];
+            for (int c = 0; c < 3; ++c) {
+                A[c] = posA[3 * b + c];
+                Bv[c] = posB[3 * b + c];
+                C[c] = posC[3 * b + c];
+                if (lengthscale != 1.0) { A[c] *= lengthscale; Bv[c] *= lengthscale; C[c] *= lengthscale; }
+            }
+            for (int64_t s_a = 0; s_a < ns; ++s_a)
+                for (int64_t s_b = 0; s_b < ns; ++s_b)
+                    for (int64_t s_c = 0; s_c < ns; ++s_c)
+                        v3_block(out, N, b, ls, boff, s_a, s_b, s_c,
+                                 coef + s_a + ns * K * ga, zeta + s_a + ns * K * ga, K, ns,
+                                 coef + s_b + ns * K * gb, zeta + s_b + ns * K * gb, K, ns,
+                                 coef + s_c + ns * K * gc, zeta + s_c + ns * K * gc, K, ns,
+                                 A, Bv, C, 1, Ebuf, TM, IM, blk);
         }
         free(Ebuf);
         free(blk);

@@ -281,3 +281,46 @@ def test_overlap_position_pullback_fd_and_translation():
             fd = ((Sp - Sm) * dS).sum(axis=(0, 1)) / (2 * h)
             assert np.max(np.abs(fd - g[c])) < 1e-8 * np.max(np.abs(fd))
     assert np.max(np.abs(dA + dB)) < 1e-13 * np.max(np.abs(dA))
+
+
+def _golden_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(os.path.dirname(__file__), "golden",
+                                                                              "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_overlap3c_orbital_path():
+    """3C on the species-aware path (no reference counterpart): with one species it equals
+    the GaussianBasis-path routine on the same shells; with mixed species every block
+    equals Gauss-Hermite quadrature of the three centres' own (species) shells, placed in
+    the reference's aliased layout (make_golden.block3)."""
+    mg = _golden_module()
+    b = W.config0_basis(nspecies=2)
+    coef = oracle.compile_coef(b.zeta, b.D, b.ls)
+    tr = W.config4_triples(B=3, seed=77)
+    one = np.ones(3, np.int64)
+    V1 = oracle.overlap3c_orb(b.ls, coef, b.zeta, one, one, one, tr.posA, tr.posB, tr.posC)
+    ls, nprim, z, D = W.gb_tables(b)
+    c1 = np.concatenate([coef[s, :nprim[s], 0] for s in range(len(ls))])
+    Vg = oracle.overlap3c_gb(ls, nprim, c1, z, tr.posA, tr.posB, tr.posC)
+    assert np.max(np.abs(V1 - Vg)) < 1e-14 * np.abs(Vg).max()
+    sA, sB, sC = np.array([1, 2, 2]), np.array([2, 1, 2]), np.array([2, 2, 1])
+    V = oracle.overlap3c_orb(b.ls, coef, b.zeta, sA, sB, sC, tr.posA, tr.posB, tr.posC, lengthscale=1.1)
+    nbf = (b.ls + 1) * (b.ls + 2) // 2
+    off = np.concatenate([[0], np.cumsum(nbf)])
+
+    def shell(s, g):
+        keep = coef[s, :, g] != 0
+        return (int(b.ls[s]), list(coef[s, keep, g]), list(b.zeta[s, keep, g]))
+
+    for e in range(3):
+        A, Bp, C = (1.1 * tr.posA[:, e], 1.1 * tr.posB[:, e], 1.1 * tr.posC[:, e])
+        for sa in range(b.nshells):
+            for sb in range(b.nshells):
+                for sc in (0, 3, 5):  # an s, a p and the d shell as third centre
+                    ref = mg.block3(shell(sa, sA[e] - 1), shell(sb, sB[e] - 1), shell(sc, sC[e] - 1), A, Bp, C)
+                    got = V[off[sa]:off[sa + 1], off[sb]:off[sb + 1], off[sc]:off[sc + 1], e]
+                    assert np.max(np.abs(got - ref)) < 1e-12 * max(1.0, np.abs(ref).max())

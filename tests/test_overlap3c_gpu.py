@@ -157,3 +157,64 @@ def test_wide_bases_f64_and_f32c():
                               f32_round(aok.to_bohr(pB, np.float32)), f32_round(aok.to_bohr(pC, np.float32)),
                               nthreads=8)
     assert rel_fro(V, ref) < 2e-6
+
+
+def _orb3(nspecies, B, seed):
+    b = W.config0_basis(nspecies=nspecies)
+    orb = aok.orbitals_from_species_basis(b)
+    tr = W.config4_triples(B=B, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    sp = [rng.integers(1, nspecies + 1, size=B) for _ in range(3)]
+    coef = oracle.compile_coef(b.zeta, b.D, b.ls)
+    return b, orb, tr, sp, coef
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-12), (torch.float32, 2e-6)])
+def test_overlap3c_orbital_path_matches_oracle(FT, tol):
+    """3C on the species-aware path (no reference counterpart): mixed species per centre,
+    a lengthscale, against the oracle's restatement (itself pinned to quadrature)."""
+    b, orb, tr, (sA, sB, sC), coef = _orb3(3, 700, 91)
+    cob = aok.compile_basis(orb, dtype=FT)
+    st = lambda pos, s: aok.PStates(pos, list(s))
+    V = aok.batch_overlap_3c(cob, st(tr.posA, sA), st(tr.posB, sB), st(tr.posC, sC), FT=FT).numpy()
+    rnd = f32_round if FT == torch.float32 else (lambda a: a)
+    cref = rnd(np.asarray(cob.coef.cpu() if torch.is_tensor(cob.coef) else cob.coef, dtype=np.float64))
+    ref = oracle.overlap3c_orb(b.ls, cref, rnd(b.zeta), sA, sB, sC, rnd(tr.posA), rnd(tr.posB), rnd(tr.posC),
+                               nthreads=8)
+    assert rel_fro(V, ref) < tol
+
+
+def test_overlap3c_orbital_single_species_equals_gb_path():
+    """With one species the species-aware entry point computes the GaussianBasis-path
+    integral on the same shells (the oracle's GB routine, 1e-12)."""
+    b, orb, tr, _, coef = _orb3(1, 256, 93)
+    cob = aok.compile_basis(orb, dtype=torch.float64)
+    one = [1] * 256
+    V = aok.batch_overlap_3c(cob, aok.PStates(tr.posA, one), aok.PStates(tr.posB, one), aok.PStates(tr.posC, one))
+    ls, nprim, z, _ = W.gb_tables(b)
+    c1 = np.concatenate([coef[s, :nprim[s], 0] for s in range(len(ls))])
+    ref = oracle.overlap3c_gb(ls, nprim, c1, z, tr.posA, tr.posB, tr.posC, nthreads=8)
+    assert rel_fro(V.numpy(), ref) < 1e-12
+
+
+def test_overlap3c_orbital_bad_species_and_limits():
+    """A bad species index sets the plan's error word; more than 6 species is refused."""
+    import ctypes
+    from aok_b200 import _dev, _lib
+    b, orb, tr, (sA, sB, sC), coef = _orb3(2, 64, 95)
+    FT = torch.float64
+    plan = _dev.plan_for(b.ls, b.K, b.NZ, _lib.AOK_PREC_F64, 64)
+    out = _dev.colmajor_empty((b.nbf_total,) * 3 + (64,), FT)
+    bad = sC.copy()
+    bad[7] = 5
+    args = [torch.as_tensor(np.ascontiguousarray(x)).cuda() for x in (sA, sB, bad)]
+    L = _lib.load()
+    _lib.check(L.aok_overlap3c(plan.h, _dev.ptr(out), _dev.ptr(_dev.to_colmajor(b.zeta, FT)),
+                               _dev.ptr(_dev.to_colmajor(coef, FT)), _dev.ptr(_dev.to_colmajor(tr.posA, FT)),
+                               _dev.ptr(_dev.to_colmajor(tr.posB, FT)), _dev.ptr(_dev.to_colmajor(tr.posC, FT)),
+                               *[ctypes.c_void_p(a.data_ptr()) for a in args], 64, 1.0, _dev.stream()))
+    assert L.aok_plan_check(plan.h, _dev.stream()) == _lib.AOK_ERR_SPECIES
+    b7 = W.config0_basis(nspecies=7)
+    p7 = _dev.Plan(b7.ls, b7.K, 7, _lib.AOK_PREC_F64, 8)
+    assert L.aok_overlap3c(p7.h, None, None, None, None, None, None, None, None, None, 0, 1.0, None) == \
+        _lib.AOK_ERR_UNSUPPORTED
