@@ -61,17 +61,31 @@ struct EvalParams {
     double* rows;     // [block][2 * nRad*K*NZ] or null
 };
 
+// Rounding-pinned arithmetic for the values (R, Z, r): the compiler may not fuse
+// these into an FMA, so a value is computed by the same operations whether or
+// not the kernel also forms gradients (evaluate and evaluate_ed agree bitwise).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <typename FT>
+__device__ __forceinline__ FT norm3(FT x, FT y, FT z) {
+    return sqrt(fma_rn(x, x, fma_rn(y, y, mul_rn(z, z))));
+}
+
 // value + gradient
 template <typename FT> struct D4 {
     FT v, x, y, z;
 };
 template <typename FT>
 __device__ __forceinline__ D4<FT> dmul(const D4<FT>& a, const D4<FT>& b) {
-    return {a.v * b.v, a.x * b.v + a.v * b.x, a.y * b.v + a.v * b.y, a.z * b.v + a.v * b.z};
+    return {mul_rn(a.v, b.v), a.x * b.v + a.v * b.x, a.y * b.v + a.v * b.y, a.z * b.v + a.v * b.z};
 }
 template <typename FT>
 __device__ __forceinline__ D4<FT> dlin(FT ca, const D4<FT>& a, FT cb, const D4<FT>& b) {
-    return {ca * a.v + cb * b.v, ca * a.x + cb * b.x, ca * a.y + cb * b.y, ca * a.z + cb * b.z};
+    return {fma_rn(ca, a.v, mul_rn(cb, b.v)), ca * a.x + cb * b.x, ca * a.y + cb * b.y, ca * a.z + cb * b.z};
 }
 
 // Z_lm and gradients for l <= L at (x, y, z), written to Z[idx], G[3*idx + c].
@@ -84,7 +98,7 @@ __device__ __forceinline__ D4<FT> dlin(FT ca, const D4<FT>& a, FT cb, const D4<F
 template <typename FT, int L>
 __device__ __forceinline__ void solid_harmonics(FT x, FT y, FT z, const double* F, FT* Zs, FT* Gs, int stride) {
     const D4<FT> X{x, FT(1), FT(0), FT(0)}, Y{y, FT(0), FT(1), FT(0)}, Zd{z, FT(0), FT(0), FT(1)};
-    const D4<FT> r2{x * x + y * y + z * z, FT(2) * x, FT(2) * y, FT(2) * z};
+    const D4<FT> r2{fma_rn(x, x, fma_rn(y, y, mul_rn(z, z))), FT(2) * x, FT(2) * y, FT(2) * z};
     D4<FT> C[L + 1], S[L + 1];
     C[0] = {FT(1), FT(0), FT(0), FT(0)};
     S[0] = {FT(0), FT(0), FT(0), FT(0)};
@@ -102,10 +116,10 @@ __device__ __forceinline__ void solid_harmonics(FT x, FT y, FT z, const double* 
 #pragma unroll
         for (int l = m; l <= L; ++l) {
             if (l == m + 1) {
-                q = dmul(D4<FT>{FT(2 * m + 1) * z, FT(0), FT(0), FT(2 * m + 1)}, q1);
+                q = dmul(D4<FT>{mul_rn(FT(2 * m + 1), z), FT(0), FT(0), FT(2 * m + 1)}, q1);
             } else if (l >= m + 2) {
-                const D4<FT> a = dmul(D4<FT>{FT(2 * l - 1) * z, FT(0), FT(0), FT(2 * l - 1)}, q1);
-                const D4<FT> b = dmul(D4<FT>{FT(l + m - 1) * r2.v, FT(l + m - 1) * r2.x, FT(l + m - 1) * r2.y,
+                const D4<FT> a = dmul(D4<FT>{mul_rn(FT(2 * l - 1), z), FT(0), FT(0), FT(2 * l - 1)}, q1);
+                const D4<FT> b = dmul(D4<FT>{mul_rn(FT(l + m - 1), r2.v), FT(l + m - 1) * r2.x, FT(l + m - 1) * r2.y,
                                              FT(l + m - 1) * r2.z},
                                       q2);
                 const FT inv = FT(1) / FT(l - m);
@@ -114,18 +128,18 @@ __device__ __forceinline__ void solid_harmonics(FT x, FT y, FT z, const double* 
             const int i0 = l * l + l;
             if (m == 0) {
                 const FT f = (FT)F[i0];
-                Zs[i0 * stride] = f * q.v;
+                Zs[i0 * stride] = mul_rn(f, q.v);
                 Gs[(3 * i0 + 0) * stride] = f * q.x;
                 Gs[(3 * i0 + 1) * stride] = f * q.y;
                 Gs[(3 * i0 + 2) * stride] = f * q.z;
             } else {
                 const FT f = (FT)(1.4142135623730951 * F[i0 + m]);
                 const D4<FT> pc = dmul(q, C[m]), ps = dmul(q, S[m]);
-                Zs[(i0 + m) * stride] = f * pc.v;
+                Zs[(i0 + m) * stride] = mul_rn(f, pc.v);
                 Gs[(3 * (i0 + m) + 0) * stride] = f * pc.x;
                 Gs[(3 * (i0 + m) + 1) * stride] = f * pc.y;
                 Gs[(3 * (i0 + m) + 2) * stride] = f * pc.z;
-                Zs[(i0 - m) * stride] = f * ps.v;
+                Zs[(i0 - m) * stride] = mul_rn(f, ps.v);
                 Gs[(3 * (i0 - m) + 0) * stride] = f * ps.x;
                 Gs[(3 * (i0 - m) + 1) * stride] = f * ps.y;
                 Gs[(3 * (i0 - m) + 2) * stride] = f * ps.z;
@@ -171,13 +185,13 @@ __device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl,
     for (int m = 0; m < mk; ++m) {
         const int o = k + nRad * (m + K * sg);
         const FT z = sz[o];
-        const FT a = sD[o] * exp_neg(z, sl[o], f);
+        const FT a = mul_rn(sD[o], exp_neg(z, sl[o], f));
         if constexpr (sizeof(FT) == 4) {
             const float t = s + a, bb = t - s;
             se += (s - (t - bb)) + (a - bb);
             s = t;
         } else {
-            s += a;
+            s = add_rn(s, a);
         }
         ds += (-z * df) * a;
     }
@@ -189,7 +203,7 @@ __device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl,
         drp = FT(p);
         for (int i = 0; i < p - 1; ++i) drp *= r;
     }
-    R = rp * s;
+    R = mul_rn(rp, s);
     dR = drp * s + rp * ds;
 }
 
@@ -250,7 +264,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate(const __grid_constant
             y = sc * y;
             z = sc * z;
         }
-        const FT r = sqrt(x * x + y * y + z * z);
+        const FT r = norm3(x, y, z);
         int sg = (int)P.sidx[j] - 1;
         if (sg < 0 || sg >= P.NZ) {
             atomicCAS(P.err, 0, AOK_ERR_SPECIES);
@@ -337,7 +351,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_cons
             y = sc * y;
             z = sc * z;
         }
-        const FT r = sqrt(x * x + y * y + z * z);
+        const FT r = norm3(x, y, z);
         int sg = (int)P.sidx[j] - 1;
         if (sg < 0 || sg >= P.NZ) {
             atomicCAS(P.err, 0, AOK_ERR_SPECIES);
@@ -417,7 +431,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
             sg = -1;
         }
     }
-    const FT r = sqrt(x * x + y * y + z * z);
+    const FT r = norm3(x, y, z);
     const int sgc = sg < 0 ? 0 : sg;
     for (int k = 0; k < P.nRad; ++k) {
         FT R, dR;
@@ -626,7 +640,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                             z = sc * z;
                         }
                     }
-                    r = sqrt(x * x + y * y + z * z);
+                    r = norm3(x, y, z);
                     FT Zr[nY], Gr[3 * nY];
                     solid_harmonics<FT, L>(x, y, z, P.F, Zr, Gr, 1);
                     const FT ux = x / r, uy = y / r, uz = z / r;
@@ -667,7 +681,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                         z = sc * z;
                     }
                 }
-                r = sqrt(x * x + y * y + z * z);
+                r = norm3(x, y, z);
                 for (int k = 0; k < P.nRad; ++k) {
                     FT Rk, dRk;
                     radial<FT>(sz, sD, sl, sn, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);

@@ -303,9 +303,10 @@ def overlap_pb_coef_alpha(dS, cob, XA, XB):
     dalpha = _dev.colmajor_empty((ns, K, NZ), FT)
     dA, dB = _dev.to_colmajor(XA.pos, FT), _dev.to_colmajor(XB.pos, FT)
     gA, gB = _dev_int64(sA), _dev_int64(sB)
+    # held by name: a converted temporary's memory could be reused by the next conversion
+    zd, cd = _dev.to_colmajor(cob.zeta, FT), _dev.to_colmajor(cob.coef, FT)
     _lib.check(_lib.load().aok_overlap2c_pullback(plan.h, _dev.ptr(dcoef), _dev.ptr(dalpha), _dev.ptr(dS),
-                                                  _dev.ptr(_dev.to_colmajor(cob.zeta, FT)),
-                                                  _dev.ptr(_dev.to_colmajor(cob.coef, FT)), _dev.ptr(dA), _dev.ptr(dB),
+                                                  _dev.ptr(zd), _dev.ptr(cd), _dev.ptr(dA), _dev.ptr(dB),
                                                   _dev.ptr(gA), _dev.ptr(gB), B, float(cob.lengthscale),
                                                   _dev.stream()))
     return dcoef, dalpha
@@ -363,10 +364,10 @@ def position_pullback(dS, basis, XA, XB, ps=None, st=None):
         raise _lib.ArgumentError(f"dS must be (N, N, B) = {(N, N, B)}; got {tuple(dSd.shape)}")
     pA, pB = _dev.to_colmajor(XA.pos, FT), _dev.to_colmajor(XB.pos, FT)
     gA, gB = _dev_int64(sA), _dev_int64(sB)
+    zd, cd = _dev.to_colmajor(cob.zeta, FT), _dev.to_colmajor(cob.coef, FT)
     _lib.check(_lib.load().aok_overlap2c_position_pullback(
-        plan.h, _dev.ptr(dXA), _dev.ptr(dXB), _dev.ptr(dSd), _dev.ptr(_dev.to_colmajor(cob.zeta, FT)),
-        _dev.ptr(_dev.to_colmajor(cob.coef, FT)), _dev.ptr(pA), _dev.ptr(pB), _dev.ptr(gA), _dev.ptr(gB), B,
-        float(cob.lengthscale), _dev.stream()))
+        plan.h, _dev.ptr(dXA), _dev.ptr(dXB), _dev.ptr(dSd), _dev.ptr(zd), _dev.ptr(cd), _dev.ptr(pA), _dev.ptr(pB),
+        _dev.ptr(gA), _dev.ptr(gB), B, float(cob.lengthscale), _dev.stream()))
     return dXA, dXB
 
 

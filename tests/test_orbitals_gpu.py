@@ -205,9 +205,10 @@ def test_orbitals_check_single_species_bad_index(with_params):
         dz = _dev.colmajor_empty(b1.zeta.shape, FT)
         dD = _dev.colmajor_empty(b1.zeta.shape, FT)
         dX = torch.full((n, 3), 7.0, dtype=FT, device="cuda")
+        dPd = _dev.to_colmajor(dPh, FT)
         _lib.check(L.aok_evaluate_pullback(plan.h, ctypes.c_void_p(dX.data_ptr()),
                                            _dev.ptr(dz) if with_params else None,
-                                           _dev.ptr(dD) if with_params else None, _dev.ptr(_dev.to_colmajor(dPh, FT)),
+                                           _dev.ptr(dD) if with_params else None, _dev.ptr(dPd),
                                            _dev.ptr(Xd), ctypes.c_void_p(sd.data_ptr()), _dev.ptr(z), _dev.ptr(D), n,
                                            1.0, _dev.stream()))
         return dz.cpu().numpy(), dD.cpu().numpy(), dX.cpu().numpy(), L.aok_orbitals_check(plan.h, _dev.stream())
@@ -244,9 +245,12 @@ def test_evaluate_ed_general_maps(FT, tol):
     P = _dev.colmajor_empty((nX, len(iR)), FT)
     dP = _dev.colmajor_empty((3, nX, len(iR)), FT)
     Xd, sd = _dev.to_colmajor(X, FT), torch.as_tensor(sidx).cuda()
+    # the parameter tensors are held by name: a temporary's memory goes back to the
+    # caching allocator as soon as its pointer is taken, and the next one may reuse it
+    zd, Dd = _dev.to_colmajor(b.zeta, FT), _dev.to_colmajor(b.D, FT)
     _lib.check(_lib.load().aok_evaluate_ed(plan.h, _dev.ptr(P), _dev.ptr(dP), _dev.ptr(Xd),
-                                           ctypes.c_void_p(sd.data_ptr()), _dev.ptr(_dev.to_colmajor(b.zeta, FT)),
-                                           _dev.ptr(_dev.to_colmajor(b.D, FT)), nX, 1.0, _dev.stream()))
+                                           ctypes.c_void_p(sd.data_ptr()), _dev.ptr(zd), _dev.ptr(Dd), nX, 1.0,
+                                           _dev.stream()))
     rnd = f32_round if FT == torch.float32 else (lambda a: a)
     Pr, dPr = oracle.evaluate_ed(rnd(X), sidx, rnd(b.zeta), rnd(b.D), orb.Rnl.powers(), iR, iY, orb.L, nthreads=8)
     Pg, dPg = P.double().cpu().numpy(), dP.double().cpu().numpy()

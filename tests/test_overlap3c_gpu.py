@@ -209,9 +209,10 @@ def test_overlap3c_orbital_bad_species_and_limits():
     bad[7] = 5
     args = [torch.as_tensor(np.ascontiguousarray(x)).cuda() for x in (sA, sB, bad)]
     L = _lib.load()
-    _lib.check(L.aok_overlap3c(plan.h, _dev.ptr(out), _dev.ptr(_dev.to_colmajor(b.zeta, FT)),
-                               _dev.ptr(_dev.to_colmajor(coef, FT)), _dev.ptr(_dev.to_colmajor(tr.posA, FT)),
-                               _dev.ptr(_dev.to_colmajor(tr.posB, FT)), _dev.ptr(_dev.to_colmajor(tr.posC, FT)),
+    # every device input held by name until the call is enqueued (a temporary's memory
+    # could be handed to the next conversion)
+    dev = [_dev.to_colmajor(x, FT) for x in (b.zeta, coef, tr.posA, tr.posB, tr.posC)]
+    _lib.check(L.aok_overlap3c(plan.h, _dev.ptr(out), *[_dev.ptr(x) for x in dev],
                                *[ctypes.c_void_p(a.data_ptr()) for a in args], 64, 1.0, _dev.stream()))
     assert L.aok_plan_check(plan.h, _dev.stream()) == _lib.AOK_ERR_SPECIES
     b7 = W.config0_basis(nspecies=7)

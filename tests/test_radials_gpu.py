@@ -96,7 +96,7 @@ def test_radials_pstates_form_and_species_errors():
     b, rad = _radial_basis(False)
     X, sidx = W.config1_points(nX=500, seed=37)
     R = aok.evaluate(rad, aok.PStates(X, list(sidx)))
-    Rr = oracle.radials(np.sqrt((X ** 2).sum(axis=0)), sidx, b.zeta, b.D, rad.powers())
+    Rr = oracle.radials(np.sqrt((X ** 2).sum(axis=0)), sidx, b.zeta, b.D, rad.powers(), with_grad=False)
     assert rel_fro(R.cpu().numpy(), Rr) < 1e-12
     with pytest.raises(aok.AOKError):
         aok.evaluate(rad, aok.PStates(X[:, :2], [1, 99]))
