@@ -68,6 +68,8 @@ struct aok_plan {
     void* d_items3 = nullptr;
     void* d_order3 = nullptr;        // per call: each panel's items, heaviest first (k_order3c)
     int nitems3 = 0;
+    void* d_geo3 = nullptr;          // per call: the (tile, lane) geometry slots (k_geo3)
+    size_t geo3_bytes = 0;
     // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated
     // launch chain, the arguments it was captured with, a private capture stream
     bool graph_on = false;
@@ -208,11 +210,11 @@ int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, con
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);
 int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
-                     const void* posC, double lengthscale, cudaStream_t s);
-int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
-                   cudaStream_t s);
-int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
-                   cudaStream_t s);
+                     const void* posC, int64_t B, double lengthscale, cudaStream_t s);
+int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
+                   double lengthscale, cudaStream_t s);
+int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
+                   double lengthscale, cudaStream_t s);
 
 // orbitals.cu
 int launch_evaluate(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx,

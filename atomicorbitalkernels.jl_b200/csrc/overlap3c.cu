@@ -121,7 +121,7 @@ int setup_overlap3c_schedule(aok_plan* p) {
 // padded (zeta, coef) tables, per-call item order, then the kernel over the
 // plan's bins (binned by the caller).
 int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
-                     const void* posC, double lengthscale, cudaStream_t s) {
+                     const void* posC, int64_t B, double lengthscale, cudaStream_t s) {
     const int nsz = (int)(p->ns * p->NZ), th = 128, bl = (nsz + th - 1) / th;
     const size_t nt = (size_t)(p->ns * p->K * p->NZ);
     if (p->prec == AOK_PREC_F64)
@@ -135,8 +135,8 @@ int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef,
     k_order3c<<<1, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, p->nitems3, (int)p->ns,
                                 (int)p->NZ);
     if ((st = cuda_status(cudaGetLastError(), "k_order3c")) != AOK_OK) return st;
-    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s);
-    return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s);
+    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, B, lengthscale, s);
+    return launch_ov3_f32(p, out, posA, posB, posC, B, lengthscale, s);
 }
 
 }  // namespace aok
@@ -158,7 +158,7 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
     cudaStream_t s = (cudaStream_t)stream;
     if ((st = launch_gb_pad(p, nprim, prim_offset, coef, alpha, s)) != AOK_OK) return st;
     if ((st = launch_bin(p, nullptr, nullptr, B, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, p->d_gb_zeta, p->d_gb_coef, posA, posB, posC, 1.0, s);
+    return launch_overlap3c(p, out, p->d_gb_zeta, p->d_gb_coef, posA, posB, posC, B, 1.0, s);
 }
 
 extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
@@ -177,5 +177,5 @@ extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const voi
     ++p->gen;  // the plan's bins change
     const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
     if ((st = launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, zeta, coef, posA, posB, posC, lengthscale, s);
+    return launch_overlap3c(p, out, zeta, coef, posA, posB, posC, B, lengthscale, s);
 }
