@@ -118,13 +118,7 @@ struct aok_orbitals {
     int max_blocks = 0;
     int* d_err = nullptr;
     // slot-parallel pullback: points binned by species, unit partial rows
-    int64_t epb_cap = 0, epb_ucap = 0;
-    int* d_epb_perm = nullptr;
-    int4* d_epb_tiles = nullptr;
-    int* d_epb_ntiles = nullptr;
-    int* d_epb_tbase = nullptr;
-    unsigned* d_epb_counter = nullptr;
-    int* d_epb_blockhist = nullptr;
+    int64_t epb_ucap = 0;
     void* d_epb_partial = nullptr;
 };
 

@@ -512,43 +512,42 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
 // ---------------------------------------------------------------------------
 // Slot-parallel parameter pullback (used by aok_evaluate_pullback).
 //
-// The points are counting-sorted by species (the 2C batch binning, keys
-// sigma*NZ) into tiles of 32.  A work unit is (species sigma, 4 tiles = 128
-// points).  For each 32 points the warp first puts lane = point: radials,
-// harmonics, dX (written at the point's original index), and the radial
+// A work unit is kEpbUnit = 128 consecutive points in the caller's order,
+// dealt statically to the warps.  For each 32 points the warp first puts lane =
+// point: radials (of the point's own species), harmonics, dX, and the radial
 // cotangents gg_k = r^p_k sum_{i: iR[i] = k} dP[j,i] Z_{iY[i]} and f(r) into
-// shared memory.  Then lane = slot (k, m) of species sigma and the warp
-// loops over the 32 points:
+// shared memory (the dP rows and positions are read coalesced).  Then, per
+// species sigma present among the 32 points (a ballot), lane = slot (k, m) of
+// sigma and the warp loops over those points in order:
 //   dD[k,m,sigma]    += gg_k exp(-zeta f),
 //   dzeta[k,m,sigma] += -D gg_k exp(-zeta f) f        (gtostoradials.jl:232-253),
-// with no cross-lane reduction.  Each unit writes its own FP64 partial row;
-// k_epb_reduce adds a species' units in order, so the result is reproducible.
+// into the warp's per-unit accumulators (shared memory, one per (sigma, slot)),
+// with no cross-lane reduction.  Each unit writes its own FP64 partial rows;
+// k_epb_reduce adds the units in order, so the result is reproducible and does
+// not depend on how the points' species are mixed.  A point with a species
+// index outside 1..NZ gets dX = 0, is left out of every species, and sets the
+// error word.
 // ---------------------------------------------------------------------------
-constexpr int kEpbChunkTiles = 4;  // tiles of 32 points per unit
-constexpr int kEpbMaxGroups = 4;   // slots per species <= 128
+constexpr int kEpbUnit = 128;     // consecutive points per unit
+constexpr int kEpbMaxGroups = 4;  // slots per species <= 128
 
 struct EpbParams {
     EvalParams E;
-    const int* perm;
-    const int4* tiles;
-    const int* tbase;   // first tile of key sigma*NZ (species sigma)
-    unsigned* counter;  // unit queue
-    double* partial;    // [2][nRad*K][ucap]: dD, dzeta per slot, units contiguous
+    double* partial;    // [2][NZ][nRad*K][ucap]: dD, dzeta per (species, slot), units contiguous
     int ucap;           // unit capacity (row length of partial)
+    int wwords;         // per-warp shared-memory words (of FT): scratch + accumulators
     // register path (REG): (radial, harmonic) -> orbital table and radial powers
     int16_t otab[kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1)];
     int8_t poly[kRegMaxRad];
 };
 
-__device__ __forceinline__ int epb_nch(const int* tbase, int sigma, int NZ) {
-    return (tbase[sigma * NZ + 1] - tbase[sigma * NZ] + kEpbChunkTiles - 1) / kEpbChunkTiles;
-}
-
-// per-warp shared memory of the slot-parallel pullback (floats of FT):
+// per-warp shared-memory scratch of the slot-parallel pullback (floats of FT):
 // R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][32], f [32]
 __host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) { return (size_t)(3 * nRad + 4 * nY + 1) * 32; }
 // the register path keeps only gg [nRad][32] and f [32]
 __host__ __device__ constexpr size_t epb_warp_words_reg(int nRad) { return (size_t)(nRad + 1) * 32; }
+// then the unit's accumulators [2][NZ][nRad*K]
+__host__ __device__ constexpr size_t epb_acc_words(int nRad, int K, int NZ) { return (size_t)2 * NZ * nRad * K; }
 
 // RAD: the radial layer's own pullback (gtostoradials.jl:232-267): X holds the
 // radii r (nX), dPin the cotangent of R (nX, nRad), so gg_k = dR[j,k] r^p_k and
@@ -561,17 +560,15 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int nY = (L + 1) * (L + 1);
     const EvalParams& P = Q.E;
-    const int ntab = P.nRad * P.K * P.NZ, nslot = P.nRad * P.K;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __shared__ int chpre[kMaxPairs + 1];
+    const int ntab = P.nRad * P.K * P.NZ, nslot = P.nRad * P.K, NZ = P.NZ;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     FT* sz = reinterpret_cast<FT*>(smem_raw);
     FT* sD = sz + ntab;
     FT* sl = sD + ntab;  // zeta log2(e)
     int* sn = reinterpret_cast<int*>(sl + ntab);
-    FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) +
-                (size_t)warp * (REG ? epb_warp_words_reg(P.nRad) : epb_warp_words(P.nRad, nY));
+    FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) + (size_t)warp * Q.wwords;
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
-       *gg = REG ? wbase : G + 96 * nY, *fv = gg + 32 * P.nRad;
+       *gg = REG ? wbase : G + 96 * nY, *fv = gg + 32 * P.nRad, *acc = fv + 32;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         sz[i] = ((const FT*)P.zeta)[i];
         sD[i] = ((const FT*)P.D)[i];
@@ -579,51 +576,32 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
     }
     for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
         sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int g = 0; g < P.NZ; ++g) {
-            chpre[g] = acc;
-            acc += epb_nch(Q.tbase, g, P.NZ);
-        }
-        chpre[P.NZ] = acc;
-    }
     __syncthreads();
-    const int nunits = chpre[P.NZ];
+    const long long nunits = (P.nX + kEpbUnit - 1) / kEpbUnit;
     const FT* dPin = (const FT*)P.dPin;
     const FT* Xin = (const FT*)P.X;
     const FT sc = (FT)P.scale;
-    for (;;) {
-        int u = 0;
-        if (lane == 0) u = (int)atomicAdd(Q.counter, 1u);
-        u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= nunits) break;
-        int sigma = 0;
-        while (chpre[sigma + 1] <= u) ++sigma;
-        const int jch = u - chpre[sigma];
-        const int tb = Q.tbase[sigma * P.NZ];
-        const int t0 = tb + jch * kEpbChunkTiles, t1 = min(t0 + kEpbChunkTiles, Q.tbase[sigma * P.NZ + 1]);
-        const int e0 = Q.tiles[t0].y, e1 = Q.tiles[t1 - 1].y + Q.tiles[t1 - 1].z;
-        FT accD[kEpbMaxGroups], accZ[kEpbMaxGroups];
-#pragma unroll
-        for (int g = 0; g < kEpbMaxGroups; ++g) accD[g] = accZ[g] = FT(0);
-        for (int c0 = e0; c0 < e1; c0 += 32) {
+    for (long long u = (long long)blockIdx.x * nw + warp; u < nunits; u += (long long)gridDim.x * nw) {
+        for (int i = lane; i < 2 * NZ * nslot; i += 32) acc[i] = FT(0);
+        const long long j0 = u * kEpbUnit, j1 = min(P.nX, j0 + kEpbUnit);
+        for (long long c0 = j0; c0 < j1; c0 += 32) {
             // phase A: lane = point
-            {
-                const int e = c0 + lane;
-                const bool in_chunk = e < e1;
-                const long long j = in_chunk ? (long long)Q.perm[e] : 0;
-                // multi-species bins hold only points of species sigma; the single-species
-                // bin holds every point, so a point's own index is checked here: one
-                // outside 1..NZ gets dX = 0 and adds nothing to the (zeta, D) gradient
-                bool valid = in_chunk;
-                if (in_chunk && P.sidx[j] != (int64_t)(sigma + 1)) {
+            const long long j = c0 + lane;
+            int sg = -1;
+            if (j < j1) {
+                sg = (int)P.sidx[j] - 1;
+                if (sg < 0 || sg >= NZ) {
                     atomicCAS(P.err, 0, AOK_ERR_SPECIES);
-                    valid = false;
+                    sg = -1;
                     if (P.dX) {
                         FT* dX = (FT*)P.dX;
                         dX[3 * j] = dX[3 * j + 1] = dX[3 * j + 2] = FT(0);
                     }
                 }
+            }
+            const bool valid = sg >= 0;
+            const int sgr = valid ? sg : 0;  // a table row for the lanes that add nothing
+            {
                 FT r;
                 if constexpr (RAD) {
                     r = valid ? Xin[j] : FT(0);
@@ -647,7 +625,7 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                     FT ax = FT(0), ay = FT(0), az = FT(0);
                     for (int k = 0; k < P.nRad; ++k) {
                         FT Rk, dRk;
-                        radial<FT>(sz, sD, sl, sn, k, sigma, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
+                        radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
                         FT gk = FT(0);
                         if (valid) {
 #pragma unroll
@@ -670,109 +648,124 @@ __global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ Ep
                         dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
                     }
                 } else {
-                FT x = FT(0), y = FT(0), z = FT(1);
-                if (valid) {
-                    x = Xin[3 * j];
-                    y = Xin[3 * j + 1];
-                    z = Xin[3 * j + 2];
-                    if (sc != FT(1)) {
-                        x = sc * x;
-                        y = sc * y;
-                        z = sc * z;
+                    FT x = FT(0), y = FT(0), z = FT(1);
+                    if (valid) {
+                        x = Xin[3 * j];
+                        y = Xin[3 * j + 1];
+                        z = Xin[3 * j + 2];
+                        if (sc != FT(1)) {
+                            x = sc * x;
+                            y = sc * y;
+                            z = sc * z;
+                        }
+                    }
+                    r = norm3(x, y, z);
+                    for (int k = 0; k < P.nRad; ++k) {
+                        FT Rk, dRk;
+                        radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
+                        R[k * 32 + lane] = Rk;
+                        dR[k * 32 + lane] = dRk;
+                        gg[k * 32 + lane] = FT(0);
+                    }
+                    solid_harmonics<FT, L>(x, y, z, P.F, Z + lane, G + lane, 32);
+                    const FT ux = x / r, uy = y / r, uz = z / r;
+                    FT ax = FT(0), ay = FT(0), az = FT(0);
+                    if (valid) {
+                        for (int i = 0; i < P.nOrb; ++i) {
+                            const int k = P.iR[i], yi = P.iY[i];
+                            const FT g = dPin[j + P.nX * i];
+                            const FT rn = R[k * 32 + lane], yl = Z[yi * 32 + lane], dr = dR[k * 32 + lane];
+                            ax += g * ((dr * ux) * yl + rn * G[(3 * yi + 0) * 32 + lane]);
+                            ay += g * ((dr * uy) * yl + rn * G[(3 * yi + 1) * 32 + lane]);
+                            az += g * ((dr * uz) * yl + rn * G[(3 * yi + 2) * 32 + lane]);
+                            gg[k * 32 + lane] += g * yl;
+                        }
+                        if (P.dX) {
+                            FT* dX = (FT*)P.dX;
+                            dX[3 * j] = sc != FT(1) ? ax * sc : ax;
+                            dX[3 * j + 1] = sc != FT(1) ? ay * sc : ay;
+                            dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
+                        }
                     }
                 }
-                r = norm3(x, y, z);
-                for (int k = 0; k < P.nRad; ++k) {
-                    FT Rk, dRk;
-                    radial<FT>(sz, sD, sl, sn, k, sigma, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
-                    R[k * 32 + lane] = Rk;
-                    dR[k * 32 + lane] = dRk;
-                    gg[k * 32 + lane] = FT(0);
-                }
-                solid_harmonics<FT, L>(x, y, z, P.F, Z + lane, G + lane, 32);
-                const FT ux = x / r, uy = y / r, uz = z / r;
-                FT ax = FT(0), ay = FT(0), az = FT(0);
-                if (valid) {
-                    for (int i = 0; i < P.nOrb; ++i) {
-                        const int k = P.iR[i], yi = P.iY[i];
-                        const FT g = dPin[j + P.nX * i];
-                        const FT rn = R[k * 32 + lane], yl = Z[yi * 32 + lane], dr = dR[k * 32 + lane];
-                        ax += g * ((dr * ux) * yl + rn * G[(3 * yi + 0) * 32 + lane]);
-                        ay += g * ((dr * uy) * yl + rn * G[(3 * yi + 1) * 32 + lane]);
-                        az += g * ((dr * uz) * yl + rn * G[(3 * yi + 2) * 32 + lane]);
-                        gg[k * 32 + lane] += g * yl;
-                    }
-                    if (P.dX) {
-                        FT* dX = (FT*)P.dX;
-                        dX[3 * j] = sc != FT(1) ? ax * sc : ax;
-                        dX[3 * j + 1] = sc != FT(1) ? ay * sc : ay;
-                        dX[3 * j + 2] = sc != FT(1) ? az * sc : az;
-                    }
-                }
-                }  // RAD
                 for (int k = 0; k < P.nRad; ++k) {
                     FT rp = FT(1);
                     for (int i = 0; i < P.poly[k]; ++i) rp *= r;
-                    gg[k * 32 + lane] *= rp;  // zero for lanes past the chunk's end
+                    gg[k * 32 + lane] *= rp;  // zero for the lanes that add nothing
                 }
                 fv[lane] = P.slater ? r : r * r;
             }
             __syncwarp();
-            // phase B: lane = slot (k, m) of species sigma
-            const int np = min(32, e1 - c0);
+            // phase B: per species present, lane = slot (k, m) of sigma, the points in order
+            for (int sigma = 0; sigma < NZ; ++sigma) {
+                const unsigned msk = __ballot_sync(0xffffffffu, sg == sigma);
+                if (msk == 0u) continue;
 #pragma unroll
-            for (int g = 0; g < kEpbMaxGroups; ++g) {
-                const int s = g * 32 + lane;
-                if (g * 32 < nslot && s < nslot) {
-                    const int k = s % P.nRad;
-                    const FT zk = sz[s + nslot * sigma], zl = sl[s + nslot * sigma];
-                    FT aD = accD[g], aZ = accZ[g];
-                    for (int t = 0; t < np; ++t) {
-                        const FT f = fv[t], w = gg[k * 32 + t];
-                        const FT ex = exp_neg(zk, zl, f) * w;
-                        aD += ex;
-                        aZ = fma(ex, f, aZ);
+                for (int g = 0; g < kEpbMaxGroups; ++g) {
+                    const int s = g * 32 + lane;
+                    if (g * 32 < nslot && s < nslot) {
+                        const int k = s % P.nRad;
+                        const FT zk = sz[s + nslot * sigma], zl = sl[s + nslot * sigma];
+                        FT* aDp = acc + sigma * nslot + s;
+                        FT* aZp = aDp + NZ * nslot;
+                        FT aD = *aDp, aZ = *aZp;
+                        unsigned m = msk;
+                        while (m) {
+                            const int t = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const FT f = fv[t], w = gg[k * 32 + t];
+                            const FT ex = exp_neg(zk, zl, f) * w;
+                            aD += ex;
+                            aZ = fma(ex, f, aZ);
+                        }
+                        *aDp = aD;
+                        *aZp = aZ;
                     }
-                    accD[g] = aD;
-                    accZ[g] = aZ;
                 }
             }
             __syncwarp();
         }
-#pragma unroll
-        for (int g = 0; g < kEpbMaxGroups; ++g) {
-            const int s = g * 32 + lane;
-            if (s < nslot) {
-                Q.partial[(size_t)s * Q.ucap + u] = (double)accD[g];
-                Q.partial[(size_t)(nslot + s) * Q.ucap + u] = -(double)sD[s + nslot * sigma] * (double)accZ[g];
-            }
+        // the unit's partial rows: dD, then dzeta = -D * sum(ex f)
+        for (int i = lane; i < NZ * nslot; i += 32) {
+            const int sigma = i / nslot, s = i - sigma * nslot;
+            Q.partial[(size_t)i * Q.ucap + u] = (double)acc[i];
+            Q.partial[(size_t)(NZ * nslot + i) * Q.ucap + u] =
+                -(double)sD[s + nslot * sigma] * (double)acc[NZ * nslot + i];
         }
+        __syncwarp();
     }
 }
 
-// dD, dzeta of slot (k, m, sigma): one warp per output value; lanes take
-// species sigma's unit rows in a fixed strided order and a fixed butterfly
-// adds the lanes, so the result is reproducible.
+// dD, dzeta of slot (k, m, sigma): one warp per output value; lanes take the
+// unit rows in a fixed strided order and a fixed butterfly adds the lanes, so
+// the result is reproducible.
 template <typename FT>
 __global__ void k_epb_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const double* __restrict__ partial,
-                             const int* __restrict__ tbase, int nslot, int NZ, int ucap) {
+                             int nout, int nunits, int ucap) {
     const int lane = threadIdx.x & 31;
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= 2 * nslot * NZ) return;
-    const int kind = t / (nslot * NZ), o = t % (nslot * NZ);
-    const int sigma = o / nslot, s = o % nslot;
-    int u0 = 0;
-    for (int g = 0; g < sigma; ++g) u0 += epb_nch(tbase, g, NZ);
-    const int nu = epb_nch(tbase, sigma, NZ);
+    if (t >= 2 * nout) return;
     double sum = 0.0;
-    const double* row = partial + (size_t)(kind * nslot + s) * ucap + u0;
-    for (int v = lane; v < nu; v += 32) sum += row[v];
+    const double* row = partial + (size_t)t * ucap;
+    for (int v = lane; v < nunits; v += 32) sum += row[v];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
     if (lane == 0) {
-        if (kind == 0) dD[o] = (FT)sum;
-        else dzeta[o] = (FT)sum;
+        if (t < nout) dD[t] = (FT)sum;
+        else dzeta[t - nout] = (FT)sum;
     }
+}
+
+// the unit rows of one slot-parallel pullback call, summed (k_epb_reduce)
+static int launch_epb_reduce(aok_orbitals* o, void* dD, void* dzeta, const EpbParams& Q, int64_t nX,
+                             cudaStream_t s) {
+    const int nout = (int)(o->nRad * o->K * o->NZ), nunits = (int)((nX + kEpbUnit - 1) / kEpbUnit);
+    const int rb = (2 * nout * 32 + 255) / 256;
+    if (o->prec == AOK_PREC_F64)
+        k_epb_reduce<double><<<rb, 256, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, nout, nunits, Q.ucap);
+    else
+        k_epb_reduce<float><<<rb, 256, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, nout, nunits, Q.ucap);
+    return cuda_status(cudaGetLastError(), "k_epb_reduce");
 }
 
 template <typename FT>
@@ -976,34 +969,38 @@ int launch_evaluate(aok_orbitals* o, void* Pv, void* dP, const void* X, const in
     return launch_eval_T<float>(o, P, dP != nullptr, false, s);
 }
 
-// buffers of the slot-parallel pullback, grown to nX points
+// unit rows of the slot-parallel pullback, grown to nX points
 static int ensure_epb_buffers(aok_orbitals* o, int64_t nX) {
-    if (nX <= o->epb_cap) return AOK_OK;
-    void* bufs[] = {o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
-                    o->d_epb_blockhist, o->d_epb_partial};
-    for (void* b : bufs)
-        if (b) cudaFree(b);
-    o->d_epb_perm = nullptr;
-    o->d_epb_tiles = nullptr;
-    o->d_epb_ntiles = o->d_epb_tbase = o->d_epb_blockhist = nullptr;
-    o->d_epb_counter = nullptr;
+    const int64_t units = (nX + kEpbUnit - 1) / kEpbUnit;
+    if (units <= o->epb_ucap && o->d_epb_partial) return AOK_OK;
+    if (o->d_epb_partial) cudaFree(o->d_epb_partial);
     o->d_epb_partial = nullptr;
-    o->epb_cap = 0;
-    const int64_t np = o->NZ * o->NZ;
-    const int64_t tiles = (nX + 31) / 32 + np + 1;
-    const int64_t units = tiles / kEpbChunkTiles + o->NZ + 1;
-    cudaError_t e;
-    if ((e = cudaMalloc(&o->d_epb_perm, sizeof(int) * nX)) != cudaSuccess ||
-        (e = cudaMalloc(&o->d_epb_tiles, sizeof(int4) * tiles)) != cudaSuccess ||
-        (e = cudaMalloc(&o->d_epb_ntiles, sizeof(int))) != cudaSuccess ||
-        (e = cudaMalloc(&o->d_epb_tbase, sizeof(int) * (np + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&o->d_epb_counter, sizeof(unsigned))) != cudaSuccess ||
-        (e = cudaMalloc(&o->d_epb_blockhist, sizeof(int) * kBinMaxBlocksHost * np)) != cudaSuccess ||
-        (e = cudaMalloc(&o->d_epb_partial, sizeof(double) * units * 2 * o->nRad * o->K)) != cudaSuccess)
-        return cuda_status(e, "cudaMalloc(evaluate pullback buffers)");
-    o->epb_cap = nX;
+    o->epb_ucap = 0;
+    cudaError_t e = cudaMalloc(&o->d_epb_partial, sizeof(double) * (size_t)units * 2 * o->nRad * o->K * o->NZ);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(evaluate pullback rows)");
     o->epb_ucap = units;
     return AOK_OK;
+}
+
+// Blocks of the slot-parallel pullback: as many warps (up to 8) as the per-warp
+// shared memory allows, and the resident blocks per SM from the occupancy query.
+static int launch_epb_kernel(aok_orbitals* o, const void* k, EpbParams& Q, size_t tab, size_t wbytes,
+                             cudaStream_t s, const char* what) {
+    int nw = 8;
+    while (nw > 1 && tab + nw * wbytes > 227 * 1024) --nw;
+    const size_t smem = tab + nw * wbytes;
+    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, std::string(what) + ": basis too large");
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs)");
+    int occ = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * nw, smem)) != cudaSuccess)
+        return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    Q.wwords = (int)(wbytes / (o->prec == AOK_PREC_F64 ? 8 : 4));
+    const int64_t units = (Q.E.nX + kEpbUnit - 1) / kEpbUnit;
+    const int64_t want = (units + nw - 1) / nw;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)o->num_sms * std::max(occ, 1)));
+    void* args[] = {&Q};
+    return cuda_status(cudaLaunchKernel(k, dim3(grid), dim3(32 * nw), args, smem, s), what);
 }
 
 template <typename FT, int L>
@@ -1011,6 +1008,7 @@ static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
     constexpr int nY = (L + 1) * (L + 1);
     const size_t fsz = sizeof(FT);
     const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    const size_t accw = epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ);
     if constexpr (L <= kRegMaxL) {
         // the register path when every (radial, harmonic) pair is used at most once
         bool ok = o->nRad <= kRegMaxRad;
@@ -1024,29 +1022,13 @@ static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
             if (o->poly[k] > 127) ok = false;
             else Q.poly[k] = (int8_t)o->poly[k];
         }
-        const size_t smem = tab + 8 * epb_warp_words_reg((int)o->nRad) * fsz;
-        if (ok && smem <= 227 * 1024) {
-            auto k = k_evaluate_pbs<FT, L, false, true>;
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs reg)");
-            int occ = 0;
-            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem)) != cudaSuccess)
-                return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-            k<<<o->num_sms * std::max(1, occ), 256, smem, s>>>(Q);
-            return cuda_status(cudaGetLastError(), "k_evaluate_pbs");
-        }
+        const size_t wbytes = (epb_warp_words_reg((int)o->nRad) + accw) * fsz;
+        if (ok && tab + wbytes <= 227 * 1024)
+            return launch_epb_kernel(o, (const void*)k_evaluate_pbs<FT, L, false, true>, Q, tab, wbytes, s,
+                                     "k_evaluate_pbs");
     }
-    const size_t per_warp = epb_warp_words((int)o->nRad, nY) * fsz;
-    int nw = 8;
-    while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;
-    const size_t smem = tab + nw * per_warp;
-    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "evaluate pullback: basis too large");
-    auto k = k_evaluate_pbs<FT, L>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs)");
-    const int per_sm = std::max(1, std::min(2, (int)((228 * 1024) / (smem + 1024))));
-    k<<<o->num_sms * per_sm, 32 * nw, smem, s>>>(Q);
-    return cuda_status(cudaGetLastError(), "k_evaluate_pbs");
+    const size_t wbytes = (epb_warp_words((int)o->nRad, nY) + accw) * fsz;
+    return launch_epb_kernel(o, (const void*)k_evaluate_pbs<FT, L>, Q, tab, wbytes, s, "k_evaluate_pbs");
 }
 
 template <typename FT>
@@ -1069,32 +1051,20 @@ int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const v
     P.dPin = dPin;
     P.dX = dX;
     const int nslot = (int)(o->nRad * o->K);
-    if (dzeta && dD && nslot <= 32 * kEpbMaxGroups && o->NZ * o->NZ <= kMaxPairs) {
-        // slot-parallel: points binned by species, lanes = (radial, primitive) slots
+    if (dzeta && dD && nslot <= 32 * kEpbMaxGroups) {
+        // slot-parallel: units of consecutive points, lanes = (radial, primitive) slots per species
         AOK_TRY_PB(ensure_epb_buffers(o, nX));
-        // points with a bad species index are left out of the bins; their dX is zeroed there
-        BinBufs bb{o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
-                   o->d_epb_blockhist, o->d_err};
-        bb.zero3 = dX;
-        bb.zero3_bytes = o->prec == AOK_PREC_F64 ? 8 : 4;
-        AOK_TRY_PB(launch_bin_into(bb, sidx, nullptr, nX, (int)o->NZ, s));
         EpbParams Q;
+        memset(&Q, 0, sizeof(Q));
         Q.E = P;
-        Q.perm = o->d_epb_perm;
-        Q.tiles = o->d_epb_tiles;
-        Q.tbase = o->d_epb_tbase;
-        Q.counter = o->d_epb_counter;
         Q.partial = (double*)o->d_epb_partial;
         Q.ucap = (int)o->epb_ucap;
-        AOK_TRY_PB(o->prec == AOK_PREC_F64 ? launch_epb_T<double>(o, Q, s) : launch_epb_T<float>(o, Q, s));
-        const int nout = 2 * nslot * (int)o->NZ, rb = (nout * 32 + 255) / 256;
-        if (o->prec == AOK_PREC_F64)
-            k_epb_reduce<double><<<rb, 256, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, o->d_epb_tbase, nslot,
-                                                   (int)o->NZ, Q.ucap);
-        else
-            k_epb_reduce<float><<<rb, 256, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, o->d_epb_tbase, nslot,
-                                                  (int)o->NZ, Q.ucap);
-        return cuda_status(cudaGetLastError(), "k_epb_reduce");
+        const int st = o->prec == AOK_PREC_F64 ? launch_epb_T<double>(o, Q, s) : launch_epb_T<float>(o, Q, s);
+        if (st != AOK_ERR_UNSUPPORTED) {
+            AOK_TRY_PB(st);
+            return launch_epb_reduce(o, dD, dzeta, Q, nX, s);
+        }
+        // a basis whose per-warp scratch does not fit: the per-block-rows kernel below
     }
     const int grid = (int)((nX + kEvalThreads - 1) / kEvalThreads);
     const int ntab = (int)(o->nRad * o->K * o->NZ);
@@ -1150,42 +1120,21 @@ int launch_radials_pb(aok_orbitals* o, void* dzeta, void* dD, const void* dRin, 
     fill_params(o, P, r, sidx, zeta, D, nX, 1.0);
     P.dPin = dRin;
     const int nslot = (int)(o->nRad * o->K);
-    if (nslot > 32 * kEpbMaxGroups || o->NZ * o->NZ > kMaxPairs)
-        return set_error(AOK_ERR_UNSUPPORTED, "radials pullback: too many (radial, primitive) slots or species");
+    if (nslot > 32 * kEpbMaxGroups)
+        return set_error(AOK_ERR_UNSUPPORTED, "radials pullback: more than 128 (radial, primitive) slots");
     AOK_TRY_PB(ensure_epb_buffers(o, nX));
-    const BinBufs bb{o->d_epb_perm, o->d_epb_tiles, o->d_epb_ntiles, o->d_epb_tbase, o->d_epb_counter,
-                     o->d_epb_blockhist, o->d_err};
-    AOK_TRY_PB(launch_bin_into(bb, sidx, nullptr, nX, (int)o->NZ, s));
     EpbParams Q;
+    memset(&Q, 0, sizeof(Q));
     Q.E = P;
-    Q.perm = o->d_epb_perm;
-    Q.tiles = o->d_epb_tiles;
-    Q.tbase = o->d_epb_tbase;
-    Q.counter = o->d_epb_counter;
     Q.partial = (double*)o->d_epb_partial;
     Q.ucap = (int)o->epb_ucap;
     const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
     const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
-    const size_t per_warp = epb_warp_words((int)o->nRad, 1) * fsz;
-    int nw = 8;
-    while (nw > 1 && tab + nw * per_warp > 227 * 1024) --nw;
-    const size_t smem = tab + nw * per_warp;
-    if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "radials pullback: basis too large");
-    void* k = o->prec == AOK_PREC_F64 ? (void*)k_evaluate_pbs<double, 0, true> : (void*)k_evaluate_pbs<float, 0, true>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs radial)");
-    const int per_sm = std::max(1, std::min(4, (int)((228 * 1024) / (smem + 1024))));
-    void* args[] = {&Q};
-    AOK_TRY_PB(cuda_status(cudaLaunchKernel(k, dim3(o->num_sms * per_sm), dim3(32 * nw), args, smem, s),
-                           "k_evaluate_pbs (radial)"));
-    const int nout = 2 * nslot * (int)o->NZ, rb = (nout * 32 + 255) / 256;
-    if (o->prec == AOK_PREC_F64)
-        k_epb_reduce<double><<<rb, 256, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, o->d_epb_tbase, nslot,
-                                               (int)o->NZ, Q.ucap);
-    else
-        k_epb_reduce<float><<<rb, 256, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, o->d_epb_tbase, nslot,
-                                              (int)o->NZ, Q.ucap);
-    return cuda_status(cudaGetLastError(), "k_epb_reduce");
+    const size_t wbytes = (epb_warp_words((int)o->nRad, 1) + epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ)) * fsz;
+    const void* k =
+        o->prec == AOK_PREC_F64 ? (const void*)k_evaluate_pbs<double, 0, true> : (const void*)k_evaluate_pbs<float, 0, true>;
+    AOK_TRY_PB(launch_epb_kernel(o, k, Q, tab, wbytes, s, "k_evaluate_pbs (radial)"));
+    return launch_epb_reduce(o, dD, dzeta, Q, nX, s);
 }
 
 }  // namespace aok
@@ -1256,8 +1205,7 @@ int aok_orbitals_create(aok_orbitals** out, int64_t nRad, int64_t K, int64_t NZ,
 int aok_orbitals_destroy(aok_orbitals* o) {
     if (!o) return AOK_OK;
     void* bufs[] = {o->d_poly,        o->d_iR,          o->d_iY,          o->d_partials,      o->d_err,
-                    o->d_epb_perm,    o->d_epb_tiles,   o->d_epb_ntiles,  o->d_epb_tbase,     o->d_epb_counter,
-                    o->d_epb_blockhist, o->d_epb_partial};
+                    o->d_epb_partial};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete o;
