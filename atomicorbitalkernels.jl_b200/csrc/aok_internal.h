@@ -39,6 +39,7 @@ struct aok_plan {
     int pair16 = 0, seg_stride = 0;
     size_t stage_bytes = 0;          // shared-memory stage of the forward kernel
     int fwd_ctas = 2;                // forward kernel CTAs per SM
+    int fwd_deal = 0;                // forward items: 0 claimed from a shared counter, 1 dealt in snake order
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
     int max_bin_blocks = 0;
@@ -200,6 +201,12 @@ int launch_pb_f64(aok_plan* p, void* out0, void* out1, const void* dS, const voi
 int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
                         const void* D, const int64_t* sidxA, const int64_t* sidxB, const void* posA,
                         const void* posB, int64_t B, double lengthscale, int keep_absent, cudaStream_t s);
+
+// api.cu: a kernel's dynamic shared-memory limit (raised when a launch needs more
+// than the default) and its resident blocks per SM for (threads, smem bytes) on the
+// current device (occ may be null).  Both are kept per (device, kernel, threads,
+// smem), so a repeated launch shape costs one map lookup instead of driver calls.
+int kernel_prepare(const void* k, size_t smem, int threads, int* occ);
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);

@@ -840,34 +840,18 @@ static int launch_eval_L(aok_orbitals* o, EvalParams& P, bool grad, bool pb, cud
     const size_t smem = eval_smem_bytes(o, pb);
     if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "evaluate: basis too large for shared memory");
     int grid = (int)((P.nX + kEvalThreads - 1) / kEvalThreads);
-    cudaError_t e;
-    if (!pb) {  // resident blocks striding over the points (k_evaluate)
-        int occ = 0;
-        auto kq = grad ? k_evaluate<FT, L, true> : k_evaluate<FT, L, false>;
-        if ((e = cudaFuncSetAttribute(kq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate)");
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kq, kEvalThreads, smem)) != cudaSuccess)
-            return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        grid = std::max(1, std::min(grid, o->num_sms * std::max(occ, 1)));
-    }
     if (pb) {
         auto k = k_evaluate_pb<FT, L>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pb)");
+        AOK_TRY_PB(kernel_prepare((const void*)k, smem, kEvalThreads, nullptr));
         k<<<grid, kEvalThreads, smem, s>>>(P);
         return cuda_status(cudaGetLastError(), "k_evaluate_pb");
     }
-    if (grad) {
-        auto k = k_evaluate<FT, L, true>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate)");
-        k<<<grid, kEvalThreads, smem, s>>>(P);
-    } else {
-        auto k = k_evaluate<FT, L, false>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-            return cuda_status(e, "cudaFuncSetAttribute(k_evaluate)");
-        k<<<grid, kEvalThreads, smem, s>>>(P);
-    }
+    // resident blocks striding over the points (k_evaluate)
+    auto k = grad ? k_evaluate<FT, L, true> : k_evaluate<FT, L, false>;
+    int occ = 0;
+    AOK_TRY_PB(kernel_prepare((const void*)k, smem, kEvalThreads, &occ));
+    grid = std::max(1, std::min(grid, o->num_sms * std::max(occ, 1)));
+    k<<<grid, kEvalThreads, smem, s>>>(P);
     return cuda_status(cudaGetLastError(), "k_evaluate");
 }
 
@@ -932,12 +916,8 @@ static int launch_eval_reg_L(aok_orbitals* o, const EvalParams& P, bool grad, cu
     const size_t smem = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
     if (smem > 227 * 1024) return -1;
     void* k = grad ? (void*)k_evaluate_reg<FT, L, true> : (void*)k_evaluate_reg<FT, L, false>;
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-        return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_reg)");
     int occ = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kEvalThreads, smem)) != cudaSuccess)
-        return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    AOK_TRY_PB(kernel_prepare(k, smem, kEvalThreads, &occ));
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>((P.nX + kEvalThreads - 1) / kEvalThreads, (int64_t)o->num_sms * std::max(occ, 1)));
     void* args[] = {&Q};
@@ -990,11 +970,8 @@ static int launch_epb_kernel(aok_orbitals* o, const void* k, EpbParams& Q, size_
     while (nw > 1 && tab + nw * wbytes > 227 * 1024) --nw;
     const size_t smem = tab + nw * wbytes;
     if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, std::string(what) + ": basis too large");
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_evaluate_pbs)");
     int occ = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * nw, smem)) != cudaSuccess)
-        return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    AOK_TRY_PB(kernel_prepare(k, smem, 32 * nw, &occ));
     Q.wwords = (int)(wbytes / (o->prec == AOK_PREC_F64 ? 8 : 4));
     const int64_t units = (Q.E.nX + kEpbUnit - 1) / kEpbUnit;
     const int64_t want = (units + nw - 1) / nw;
@@ -1101,12 +1078,8 @@ int launch_radials(aok_orbitals* o, void* R, void* dR, const void* r, const int6
     void* k;
     if (o->prec == AOK_PREC_F64) k = dR ? (void*)k_radials<double, true> : (void*)k_radials<double, false>;
     else k = dR ? (void*)k_radials<float, true> : (void*)k_radials<float, false>;
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-        return cuda_status(e, "cudaFuncSetAttribute(k_radials)");
     int occ = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kEvalThreads, smem)) != cudaSuccess)
-        return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    AOK_TRY_PB(kernel_prepare(k, smem, kEvalThreads, &occ));
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>((nX + kEvalThreads - 1) / kEvalThreads, (int64_t)o->num_sms * std::max(occ, 1)));
     void* args[] = {&P};

@@ -334,8 +334,7 @@ static int launch_dpos_T(aok_plan* p, void* dA, void* dB, const void* dS, const 
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
     auto kern = k_overlap2c_dpos<FT>;
     int occ = 0;
-    AOK_TRY_PB(cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * kDposWarps, 0),
-                           "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
+    AOK_TRY_PB(kernel_prepare((const void*)kern, 0, 32 * kDposWarps, &occ));
     const int grid = std::max(1, std::min(p->max_tiles, p->num_sms * std::max(occ, 1)));
     timing_begin(p, s);
     kern<<<grid, 32 * kDposWarps, 0, s>>>(P);

@@ -75,7 +75,8 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         }
         long long cost = (long long)na * nb * nc * per * (f ? 4 : 1) + 64;
         cost = min(cost, (long long)0x7FFFFFFF);
-        ikey[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | (unsigned)i;  // ascending = heaviest first
+        // ascending = heaviest first; equal costs by routine, then by position
+        ikey[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | ((unsigned)code3(it) << 12) | (unsigned)i;
         atomicMax(&gmax[code3(it)], (int)cost);
     }
     __syncthreads();

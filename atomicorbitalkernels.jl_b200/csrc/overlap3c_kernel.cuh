@@ -32,8 +32,6 @@ constexpr int kMaxL3Spec = 2;    // compile-time specialised classes up to d
 constexpr int kClsF3 = 100;      // Item3 class code of a triple with an f shell: kClsF3 + la*16 + lb*4 + lc
 constexpr int kThreads3 = 128;
 constexpr int kAllPages3 = 1 << 20;  // page window [0, kAllPages3): every page of an item's chunk
-constexpr int kRes3 = 128;           // records a warp keeps resident (items of up to kRes3 primitive triples)
-constexpr int kChunk3 = 4;           // tiles per work unit
 
 __host__ __device__ constexpr int pages_per_chunk3(int la, int lb) {
     return (ncart(la) * ncart(lb)) >= 36 ? 1 : 36 / (ncart(la) * ncart(lb));
@@ -206,25 +204,16 @@ struct Prim3 {
 
 // Records q0 .. q0 + 31 of the unit into the warp's buffer, one per lane (FP64
 // arithmetic), in (ip, jp, kp) order; the caller brackets it with __syncwarp.
+// One out-of-line copy per precision: its FP64 divisions are long code, which
+// every class routine would otherwise carry through the instruction cache.
 template <typename PT, typename FT>
-__device__ __forceinline__ void gen_records3(PT* buf, const Prim3<FT>& pr, int q0, int n, int lane) {
+__device__ __noinline__ void gen_records3(PT* buf, const Prim3<FT> pr, int q0, int n, int lane) {
     const int q = q0 + lane;
     if (q >= n) return;
     const int nb = pr.n[1], nc = pr.n[2];
     const int ip = q / (nb * nc), jp = (q / nc) % nb, kp = q % nc;
     fill_pt(buf[lane], (double)pr.c[0][ip], (double)pr.c[1][jp], (double)pr.c[2][kp], (double)pr.z[0][ip],
             (double)pr.z[1][jp], (double)pr.z[2][kp], ip * nb + jp);
-}
-
-// Primitive triples in flight per loop step: U independent chains (record load,
-// exponential, E tables) before their products are accumulated in record order,
-// so a warp's latency per triple shrinks for the classes whose tables are small.
-// U is the largest of 4, 2, 1 whose U sets of tables plus the accumulators fit
-// about 100 registers (FP64 values count twice).
-template <int LA, int LB, int LC, int M, int FSZ>
-__host__ __device__ constexpr int unroll3() {
-    constexpr int T = 3 * (LA + 1) * (LB + 1) * (LC + 1), W = FSZ / 4, A = FSZ == 4 ? 3 * M : 2 * M;
-    return 4 * T * W + A <= 100 ? 4 : (2 * T * W + A <= 100 ? 2 : 1);
 }
 
 // lin (0-based, within the block) -> offset in the lane's output block;
@@ -237,7 +226,6 @@ __device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Ge
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
-    constexpr int U = unroll3<LA, LB, LC, M, 4>();
     float hi[M], part[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
@@ -248,74 +236,60 @@ __device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Ge
 #pragma unroll
     for (int m = 0; m < M; ++m) lo[m] = 0.f;
     float prev = -1.f;
-    const bool res = n <= kRes3;  // all records resident in buf (built by the caller)
 #pragma unroll 1
-    for (int q0 = 0; q0 < n; q0 += res ? kRes3 : 32) {
-      if (!res) {
-        __syncwarp();
-        gen_records3(buf, pr, q0, n, lane);
-        __syncwarp();
-      }
-      const int m = res ? n : min(32, n - q0);
+    for (int q0 = 0; q0 < n; q0 += 32) {
+      __syncwarp();
+      gen_records3(buf, pr, q0, n, lane);
+      __syncwarp();
+      const int m = min(32, n - q0);
 #pragma unroll 1
-      for (int q = 0; q < m; q += U) {
-        float Ex[U][LA + 1][LB + 1][LC + 1], Ey[U][LA + 1][LB + 1][LC + 1], Ez[U][LA + 1][LB + 1][LC + 1];
-        float grp[U];
+      for (int q = 0; q < m; ++q) {
+        const float4 r0 = reinterpret_cast<const float4*>(buf + q)[0];
+        const float4 r1 = reinterpret_cast<const float4*>(buf + q)[1];
+        const float4 r2 = reinterpret_cast<const float4*>(buf + q)[2];
+        const float w = r0.x;
+        if (r2.w != prev) {  // a new (ip, jp) group: fold the partial sums
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            // past the round's end: the last record again with weight 0 (finite, same group)
-            const int qq = min(q + u, m - 1);
-            const float4 r0 = reinterpret_cast<const float4*>(buf + qq)[0];
-            const float4 r1 = reinterpret_cast<const float4*>(buf + qq)[1];
-            const float4 r2 = reinterpret_cast<const float4*>(buf + qq)[2];
-            const float w = q + u < m ? r0.x : 0.f;
-            grp[u] = r2.w;
-            // exponent x = (k_ab |AB|^2 + k_ac |AC|^2 + k_bc |BC|^2) log2(e), double-float
-            const float xa = r0.y * g.R2[0], xb = r0.w * g.R2[1], xc = r1.y * g.R2[2];
-            float s1, e1, xh, e2;
-            two_sum(xa, xb, s1, e1);
-            two_sum(s1, xc, xh, e2);
-            const float xl = (fmaf(r0.y, g.R2[0], -xa) + fmaf(r0.w, g.R2[1], -xb) + fmaf(r1.y, g.R2[2], -xc)) +
-                             ((r0.z * g.R2[0] + r0.y * g.R2lo[0]) + (r1.x * g.R2[1] + r0.w * g.R2lo[1]) +
-                              (r1.z * g.R2[2] + r1.y * g.R2lo[2])) +
-                             (e1 + e2);
-            const float e000 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
-            const float ra = r1.w, rb = r2.x, rc = r2.y, o2q = r2.z;
-            build_E3<LA, LB, LC, float>(Ex[u], -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
-                                        ra * g.AC[0] + rb * g.BC[0], o2q, e000);
-            build_E3<LA, LB, LC, float>(Ey[u], -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
-                                        ra * g.AC[1] + rb * g.BC[1], o2q, 1.f);
-            build_E3<LA, LB, LC, float>(Ez[u], -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
-                                        ra * g.AC[2] + rb * g.BC[2], o2q, 1.f);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (grp[u] != prev) {  // a new (ip, jp) group: fold the partial sums
-#pragma unroll
-                for (int mm = 0; mm < M; ++mm) {
-                    float s, e;
-                    two_sum(hi[mm], part[mm], s, e);
-                    hi[mm] = s;
-                    part[mm] = 0.f;
-                    lo[mm] += e;
-                }
-                prev = grp[u];
+            for (int mm = 0; mm < M; ++mm) {
+                float s, e;
+                two_sum(hi[mm], part[mm], s, e);
+                hi[mm] = s;
+                part[mm] = 0.f;
+                lo[mm] += e;
             }
-#pragma unroll
-            for (int c3 = 0; c3 < CI::NC; ++c3)
-#pragma unroll
-                for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-                    for (int c1 = 0; c1 < CI::NA; ++c1) {
-                        const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
-                        if (lin >= L0 && lin < L0 + M) {
-                            const float yz = Ey[u][cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
-                                             Ez[u][cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
-                            part[lin - L0] =
-                                fmaf(Ex[u][cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
-                        }
-                    }
+            prev = r2.w;
         }
+        // exponent x = (k_ab |AB|^2 + k_ac |AC|^2 + k_bc |BC|^2) log2(e), double-float
+        const float xa = r0.y * g.R2[0], xb = r0.w * g.R2[1], xc = r1.y * g.R2[2];
+        float s1, e1, xh, e2;
+        two_sum(xa, xb, s1, e1);
+        two_sum(s1, xc, xh, e2);
+        const float xl = (fmaf(r0.y, g.R2[0], -xa) + fmaf(r0.w, g.R2[1], -xb) + fmaf(r1.y, g.R2[2], -xc)) +
+                         ((r0.z * g.R2[0] + r0.y * g.R2lo[0]) + (r1.x * g.R2[1] + r0.w * g.R2lo[1]) +
+                          (r1.z * g.R2[2] + r1.y * g.R2lo[2])) +
+                         (e1 + e2);
+        const float e000 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
+        const float ra = r1.w, rb = r2.x, rc = r2.y, o2q = r2.z;
+        float Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
+        build_E3<LA, LB, LC, float>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
+                                    ra * g.AC[0] + rb * g.BC[0], o2q, e000);
+        build_E3<LA, LB, LC, float>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
+                                    ra * g.AC[1] + rb * g.BC[1], o2q, 1.f);
+        build_E3<LA, LB, LC, float>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
+                                    ra * g.AC[2] + rb * g.BC[2], o2q, 1.f);
+#pragma unroll
+        for (int c3 = 0; c3 < CI::NC; ++c3)
+#pragma unroll
+            for (int c2 = 0; c2 < CI::NB; ++c2)
+#pragma unroll
+                for (int c1 = 0; c1 < CI::NA; ++c1) {
+                    const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
+                    if (lin >= L0 && lin < L0 + M) {
+                        const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
+                                         Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
+                        part[lin - L0] = fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
+                    }
+                }
       }
     }
     if (!valid) return;
@@ -338,55 +312,43 @@ __device__ __noinline__ void run_item3(const Prim3<double> pr, PTd* buf, const G
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
-    constexpr int U = unroll3<LA, LB, LC, M, 8>();
     double acc[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) acc[m] = 0.0;
-    const bool res = n <= kRes3;  // all records resident in buf (built by the caller)
 #pragma unroll 1
-    for (int q0 = 0; q0 < n; q0 += res ? kRes3 : 32) {
-      if (!res) {
-        __syncwarp();
-        gen_records3(buf, pr, q0, n, lane);
-        __syncwarp();
-      }
-      const int m = res ? n : min(32, n - q0);
+    for (int q0 = 0; q0 < n; q0 += 32) {
+      __syncwarp();
+      gen_records3(buf, pr, q0, n, lane);
+      __syncwarp();
+      const int m = min(32, n - q0);
 #pragma unroll 1
-      for (int q = 0; q < m; q += U) {
-        double Ex[U][LA + 1][LB + 1][LC + 1], Ey[U][LA + 1][LB + 1][LC + 1], Ez[U][LA + 1][LB + 1][LC + 1];
+      for (int q = 0; q < m; ++q) {
+        const double2 r0 = reinterpret_cast<const double2*>(buf + q)[0];
+        const double2 r1 = reinterpret_cast<const double2*>(buf + q)[1];
+        const double2 r2 = reinterpret_cast<const double2*>(buf + q)[2];
+        const double2 r3 = reinterpret_cast<const double2*>(buf + q)[3];
+        const double w = r0.x, kab = r0.y, kac = r1.x, kbc = r1.y, ra = r2.x, rb = r2.y, rc = r3.x, o2q = r3.y;
+        const double e000 = exp(-(kab * g.R2[0] + kac * g.R2[1] + kbc * g.R2[2])) * w;
+        double Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
+        build_E3<LA, LB, LC, double>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
+                                     ra * g.AC[0] + rb * g.BC[0], o2q, e000);
+        build_E3<LA, LB, LC, double>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
+                                     ra * g.AC[1] + rb * g.BC[1], o2q, 1.0);
+        build_E3<LA, LB, LC, double>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
+                                     ra * g.AC[2] + rb * g.BC[2], o2q, 1.0);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int qq = min(q + u, m - 1);
-            const double2 r0 = reinterpret_cast<const double2*>(buf + qq)[0];
-            const double2 r1 = reinterpret_cast<const double2*>(buf + qq)[1];
-            const double2 r2 = reinterpret_cast<const double2*>(buf + qq)[2];
-            const double2 r3 = reinterpret_cast<const double2*>(buf + qq)[3];
-            const double w = q + u < m ? r0.x : 0.0;
-            const double kab = r0.y, kac = r1.x, kbc = r1.y, ra = r2.x, rb = r2.y, rc = r3.x, o2q = r3.y;
-            const double e000 = exp(-(kab * g.R2[0] + kac * g.R2[1] + kbc * g.R2[2])) * w;
-            build_E3<LA, LB, LC, double>(Ex[u], -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
-                                         ra * g.AC[0] + rb * g.BC[0], o2q, e000);
-            build_E3<LA, LB, LC, double>(Ey[u], -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
-                                         ra * g.AC[1] + rb * g.BC[1], o2q, 1.0);
-            build_E3<LA, LB, LC, double>(Ez[u], -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
-                                         ra * g.AC[2] + rb * g.BC[2], o2q, 1.0);
-        }
+        for (int c3 = 0; c3 < CI::NC; ++c3)
 #pragma unroll
-        for (int u = 0; u < U; ++u)
+            for (int c2 = 0; c2 < CI::NB; ++c2)
 #pragma unroll
-            for (int c3 = 0; c3 < CI::NC; ++c3)
-#pragma unroll
-                for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-                    for (int c1 = 0; c1 < CI::NA; ++c1) {
-                        const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
-                        if (lin >= L0 && lin < L0 + M) {
-                            const double yz = Ey[u][cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
-                                              Ez[u][cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
-                            acc[lin - L0] =
-                                fma(Ex[u][cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, acc[lin - L0]);
-                        }
+                for (int c1 = 0; c1 < CI::NA; ++c1) {
+                    const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
+                    if (lin >= L0 && lin < L0 + M) {
+                        const double yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
+                                          Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
+                        acc[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, acc[lin - L0]);
                     }
+                }
       }
     }
     if (!valid) return;
@@ -472,15 +434,12 @@ __device__ __noinline__ void run_item3_f(const Prim3<FT> pr, PT* buf, const Geo3
         if constexpr (sizeof(FT) == 4) R2[a] += (double)g.R2lo[a];
     }
     double E[3][4][4][4];
-    const bool res = n <= kRes3;  // all records resident in buf (built by the caller)
 #pragma unroll 1
-    for (int q0 = 0; q0 < n; q0 += res ? kRes3 : 32) {
-      if (!res) {
-        __syncwarp();
-        gen_records3(buf, pr, q0, n, lane);
-        __syncwarp();
-      }
-      const int m = res ? n : min(32, n - q0);
+    for (int q0 = 0; q0 < n; q0 += 32) {
+      __syncwarp();
+      gen_records3(buf, pr, q0, n, lane);
+      __syncwarp();
+      const int m = min(32, n - q0);
 #pragma unroll 1
       for (int qq = 0; qq < m; ++qq) {
         const PT* r = buf + qq;
@@ -593,9 +552,8 @@ struct Ov3Params {
     const int4* tiles;
     const int* ntiles;
     unsigned* counter;
-    const Item3* items;    // every (shell triple, page chunk), heaviest first (k_order3c)
+    const Item3* items;    // every (shell triple, page chunk) in the per-call order (k_order3c)
     int nitems, ns, K, N, NZ;
-    int wave;                      // chunks per wave of the unit order
     int stage_lists, stage_items;  // copy the lists / the item list into shared memory first
     int boff[kMaxShells + 1];
 };
@@ -607,24 +565,22 @@ __host__ __device__ inline size_t ov3_stage_lists_bytes(int ns, int K, int NZ) {
     return ((2 * (size_t)ns * K * NZ * sizeof(FT) + (size_t)ns * NZ * sizeof(int)) + 15) / 16 * 16;
 }
 
-// Work unit = (item, chunk of kChunk3 consecutive tiles): one shell-triple block
-// (or page chunk of it) for the 32 batch elements of each tile, lane = element.
-// The warp builds the item's primitive-triple records once per species triple
-// (binning keeps a key's tiles consecutive) and keeps them in its shared-memory
-// buffer when there are at most kRes3 of them, so records, claim and decode are
-// paid once per chunk.  Units are drained from one global counter in waves of
-// `wave` chunks, and inside a wave item-major, heaviest item first: the blocks
-// being written at any time belong to one wave's elements (sized to stay well
-// inside L2, so the scattered stores of an element's slab meet there before they
-// reach DRAM), while every wave's heavy items start first.  The next unit is
+// Work unit = (item, tile): one shell-triple block (or page chunk of it) for the
+// 32 batch elements of a tile, lane = element.  Units are drained from one global
+// counter item-major in the per-call item order (k_order3c: the items of one
+// routine together, heaviest first), so the warps in flight run few distinct
+// routines and every routine's heavy items start first.  The next unit is
 // claimed when a unit starts, so the claim's latency hides behind the unit's
 // work; the geometry is one load per lane from the gathered slots, and the
-// primitive lists and items come from shared memory.  No panels and no barriers.
-// Three CTAs of four warps per SM (<= 168 registers).
+// primitive lists and the items come from shared memory.  A lane writes its
+// element's block straight to the output: a batch element's (N,N,N) slab is
+// contiguous and the whole output is written exactly once, so the scattered
+// stores of a block meet in L2.  No panels and no barriers.  Three CTAs of four
+// warps per SM (<= 168 registers).
 template <typename FT, bool F3>
 __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
     using PT = typename PTT<FT>::type;
-    __shared__ PT recbuf[kThreads3 / 32][kRes3];  // each warp's records
+    __shared__ PT recbuf[kThreads3 / 32][32];  // each warp's current 32 records
     extern __shared__ __align__(16) unsigned char sm3[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const FT* pz = P.pz;
@@ -651,11 +607,8 @@ __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constan
         }
         __syncthreads();
     }
-    PT* buf = recbuf[warp];
     const int ntiles = *P.ntiles;
-    const int nch = (ntiles + kChunk3 - 1) / kChunk3;
-    const unsigned per_wave = (unsigned)P.nitems * (unsigned)P.wave;
-    const unsigned total = (unsigned)P.nitems * (unsigned)nch;
+    const unsigned total = (unsigned)ntiles * (unsigned)P.nitems;
     const size_t N2 = (size_t)P.N * P.N, N3 = N2 * P.N;
     unsigned u = 0;
     if (lane == 0) u = atomicAdd(P.counter, 1u);
@@ -663,45 +616,27 @@ __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constan
     while (u < total) {
         unsigned un = 0;  // the next unit, used only at the end of this one
         if (lane == 0) un = atomicAdd(P.counter, 1u);
-        const unsigned w = u / per_wave, r = u - w * per_wave;
-        const unsigned ww = (unsigned)min(P.wave, nch - (int)w * P.wave);  // chunks in this wave
-        const int it = (int)(r / ww), ch = (int)(w * (unsigned)P.wave + r % ww);
+        const int it = (int)(u / (unsigned)ntiles), tile = (int)(u % (unsigned)ntiles);
+        const TGeo3<FT> tg = P.geo[(size_t)tile * 32 + lane];
+        const int key = __ldg(&P.tiles[tile].x);
         const Item3 wi = items[it];
-        const int t1 = min(ntiles, (ch + 1) * kChunk3);
-        int cur = -1;  // species triple whose records are in buf
+        const bool valid = tg.b >= 0;
+        // the tile's species triple (key ((ga NZ) + gb) NZ + gc; 0 on the single-species path)
+        const int ga = key / (P.NZ * P.NZ), gb = (key / P.NZ) % P.NZ, gc = key % P.NZ;
         Prim3<FT> pr;
-        int n = 0;
-#pragma unroll 1
-        for (int tile = ch * kChunk3; tile < t1; ++tile) {
-            const TGeo3<FT> tg = P.geo[(size_t)tile * 32 + lane];
-            const int key = __ldg(&P.tiles[tile].x);
-            if (key != cur) {
-                // the tile's species triple (key ((ga NZ) + gb) NZ + gc; 0 on the single-species path)
-                const int ga = key / (P.NZ * P.NZ), gb = (key / P.NZ) % P.NZ, gc = key % P.NZ;
-                const int la = ga * P.ns + wi.sa, lb = gb * P.ns + wi.sb, lc = gc * P.ns + wi.sc;
-                pr.z[0] = pz + (size_t)la * P.K;
-                pr.c[0] = pc + (size_t)la * P.K;
-                pr.n[0] = pn[la];
-                pr.z[1] = pz + (size_t)lb * P.K;
-                pr.c[1] = pc + (size_t)lb * P.K;
-                pr.n[1] = pn[lb];
-                pr.z[2] = pz + (size_t)lc * P.K;
-                pr.c[2] = pc + (size_t)lc * P.K;
-                pr.n[2] = pn[lc];
-                n = pr.n[0] * pr.n[1] * pr.n[2];
-                if (n <= kRes3) {  // build the resident records (larger items build theirs per round)
-                    __syncwarp();
-#pragma unroll 1
-                    for (int q0 = 0; q0 < n; q0 += 32) gen_records3(buf + q0, pr, q0, n, lane);
-                    __syncwarp();
-                }
-                cur = key;
-            }
-            const bool valid = tg.b >= 0;
-            FT* dst = P.out + (size_t)(valid ? tg.b : 0) * N3 + (size_t)P.boff[wi.sc] * N2 +
-                      (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-            dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, buf, tg.g, dst, P.N, 0, kAllPages3, valid);
-        }
+        const int la = ga * P.ns + wi.sa, lb = gb * P.ns + wi.sb, lc = gc * P.ns + wi.sc;
+        pr.z[0] = pz + (size_t)la * P.K;
+        pr.c[0] = pc + (size_t)la * P.K;
+        pr.n[0] = pn[la];
+        pr.z[1] = pz + (size_t)lb * P.K;
+        pr.c[1] = pc + (size_t)lb * P.K;
+        pr.n[1] = pn[lb];
+        pr.z[2] = pz + (size_t)lc * P.K;
+        pr.c[2] = pc + (size_t)lc * P.K;
+        pr.n[2] = pn[lc];
+        FT* dst = P.out + (size_t)(valid ? tg.b : 0) * N3 + (size_t)P.boff[wi.sc] * N2 +
+                  (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
+        dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, recbuf[warp], tg.g, dst, P.N, 0, kAllPages3, valid);
         u = __shfl_sync(0xffffffffu, un, 0);
     }
 }
@@ -712,7 +647,7 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     // the (tile, lane) geometry slots: at most B / 32 + one partial tile per key
     const int cap_tiles = (int)std::min<int64_t>(p->max_tiles, (B + 31) / 32 + bin_keys_max(p->NZ) + 1);
     // the unit counter (32 bits, each warp claims one past the end) must not wrap
-    if ((int64_t)p->nitems3 * ((cap_tiles + kChunk3 - 1) / kChunk3) >= ((int64_t)1 << 31))
+    if ((int64_t)p->nitems3 * cap_tiles >= ((int64_t)1 << 31))
         return set_error(AOK_ERR_LENGTH, "3C overlap: too many (shell triple, tile) units for one call; split the batch");
     const size_t slot = sizeof(TGeo3<FT>), need = (size_t)cap_tiles * 32 * slot;
     if (p->geo3_bytes < need) {
@@ -748,9 +683,6 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.N = (int)p->N;
     P.NZ = (int)p->NZ;
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
-    // waves of chunks whose output (kChunk3 x 32 elements x N^3 values each) stays near 40 MB
-    const double chunk_bytes = (double)kChunk3 * 32 * (double)p->N * p->N * p->N * sizeof(FT);
-    P.wave = (int)std::max(1.0, std::min(1e6, 40.0 * 1024 * 1024 / chunk_bytes));
     // shared-memory staging within 32 KB per CTA (three CTAs per SM keep fitting)
     const size_t lists = ov3_stage_lists_bytes<FT>(P.ns, P.K, P.NZ);
     const size_t with_items = lists + sizeof(Item3) * (size_t)P.nitems;
@@ -763,11 +695,8 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
         smem = lists;
     }
     auto kern = k_overlap3c<FT, F3>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 32 * 1024);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(k_overlap3c)");
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads3, smem);
-    if (e != cudaSuccess) return cuda_status(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if ((st = kernel_prepare((const void*)kern, smem, kThreads3, &occ)) != AOK_OK) return st;
     timing_begin(p, s);
     kern<<<p->num_sms * std::max(occ, 1), kThreads3, smem, s>>>(P);
     timing_end(p, s);

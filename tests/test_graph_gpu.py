@@ -121,3 +121,37 @@ def test_autotune_keeps_results_and_caches(FT):
     ctas, stage, cached = choices[0]
     assert ctas in ((1, 2) if FT == torch.float64 else (2, 3)) and stage > 0
     assert choices[1][:2] == choices[0][:2] and choices[1][2] == 1
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float32, 2e-6), (torch.float64, 1e-12)])
+def test_autotune_cheap_items_matches_oracle(FT, tol):
+    """A basis of one primitive per shell (s and p shells only: cheap items, where the
+    tuner may deal a segment's items to the warps in a fixed order instead of claiming
+    them): the tuned forward equals the untuned one bitwise and the oracle to the
+    precision's bar."""
+    import oracle
+    from helpers import f32_round, rel_fro
+    L = _lib.load()
+    b = W.outputbound_sp_basis()
+    pr = W.ragged_pairs(3000, b.NZ, 93)
+    N, B = b.nbf_total, pr.B
+    zeta = _dev.to_colmajor(b.zeta, FT)
+    D = _dev.to_colmajor(b.D, FT)
+    c = dict(pA=_dev.to_colmajor(pr.posA, FT), pB=_dev.to_colmajor(pr.posB, FT),
+             sA=torch.as_tensor(pr.sidxA).cuda(), sB=torch.as_tensor(pr.sidxB).cuda())
+    plan = _dev.Plan(b.ls, b.K, b.NZ, _dev.prec_of(FT), B)
+    coef = _dev.colmajor_empty(b.zeta.shape, FT)
+    _lib.check(L.aok_compile_coef(plan.h, _dev.ptr(coef), _dev.ptr(zeta), _dev.ptr(D), _dev.stream()))
+    ref = _dev.colmajor_empty((N, N, B), FT)
+    _lib.check(L.aok_overlap2c(plan.h, _dev.ptr(ref), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(c["pA"]),
+                               _dev.ptr(c["pB"]), ctypes.c_void_p(c["sA"].data_ptr()),
+                               ctypes.c_void_p(c["sB"].data_ptr()), B, 1.0, _dev.stream()))
+    out = _dev.colmajor_empty((N, N, B), FT)
+    _lib.check(L.aok_plan_autotune(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(coef), _dev.ptr(c["pA"]),
+                                   _dev.ptr(c["pB"]), ctypes.c_void_p(c["sA"].data_ptr()),
+                                   ctypes.c_void_p(c["sB"].data_ptr()), B, 1.0, _dev.stream(), None))
+    assert torch.equal(out, ref)
+    rnd = f32_round if FT == torch.float32 else (lambda a: a)
+    coef_h = coef.double().cpu().numpy()
+    o = oracle.overlap2c_orb(b.ls, coef_h, rnd(b.zeta), pr.sidxA, pr.sidxB, rnd(pr.posA), rnd(pr.posB), nthreads=8)
+    assert rel_fro(out.double().cpu().numpy(), o) < tol

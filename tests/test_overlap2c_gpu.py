@@ -248,3 +248,31 @@ def test_plan_check_reports_bad_device_species_in_overlap():
     keep = np.ones(pr.B, bool)
     keep[bad_at] = False
     assert np.array_equal(S1[:, :, keep], S0[:, :, keep])
+
+
+@pytest.mark.parametrize("which", ["config2", "outputbound", "config0"])
+def test_f32c_elementwise_bound(which):
+    """Element by element, FP32C against the oracle on the FP32-rounded inputs: every
+    element above 1e-6 of the batch's largest |S| satisfies
+        |S32 - S| <= 1e-6 max|S| + 4e-6 |S|
+    (an absolute floor at the matrix scale, from the FP32 rounding of the terms of the
+    geometry transform, plus a relative part).  Measured on a B200: largest absolute
+    error 2.7e-7 max|S|; relative error 1.6e-6 above 0.1 max|S|, 5.2e-3 at the 1e-6
+    max|S| threshold (config 2)."""
+    if which == "config2":
+        b, pr = W.config2_basis(), W.config2_pairs(B=3000)
+    elif which == "outputbound":
+        b = W.outputbound_basis()
+        pr = W.ragged_pairs(2500, b.NZ, 29)
+    else:
+        b, pr = W.config0_basis(), W.config0_pairs(B=1024)
+    S, ref, _, _ = _orb_case(b, pr, torch.float32)
+    S = S.numpy().astype(np.float64)
+    smax = np.abs(ref).max()
+    m = np.abs(ref) > 1e-6 * smax
+    assert m.sum() > 0
+    err = np.abs(S - ref)
+    bound = 1e-6 * smax + 4e-6 * np.abs(ref)
+    assert np.all(err[m] <= bound[m]), float(np.max(err[m] / bound[m]))
+    # below the threshold the absolute floor holds too
+    assert np.all(err <= 1e-6 * smax + 4e-6 * np.abs(ref))
