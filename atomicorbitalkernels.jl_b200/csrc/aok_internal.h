@@ -39,7 +39,6 @@ struct aok_plan {
     int pair16 = 0, seg_stride = 0;
     size_t stage_bytes = 0;          // shared-memory stage of the forward kernel
     int fwd_ctas = 2;                // forward kernel CTAs per SM
-    int fwd_deal = 0;                // forward items: 0 claimed from a shared counter, 1 dealt in snake order
     // multi-block binning scratch
     int* d_blockhist = nullptr;      // nblk * NZ*NZ
     int max_bin_blocks = 0;
@@ -69,8 +68,6 @@ struct aok_plan {
     void* d_items3 = nullptr;
     void* d_order3 = nullptr;        // per call: each panel's items, heaviest first (k_order3c)
     int nitems3 = 0;
-    void* d_geo3 = nullptr;          // per call: the (tile, lane) geometry slots (k_geo3)
-    size_t geo3_bytes = 0;
     // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated
     // launch chain, the arguments it was captured with, a private capture stream
     bool graph_on = false;
@@ -211,11 +208,11 @@ int kernel_prepare(const void* k, size_t smem, int threads, int* occ);
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);
 int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
-                     const void* posC, int64_t B, double lengthscale, cudaStream_t s);
-int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
-                   double lengthscale, cudaStream_t s);
-int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
-                   double lengthscale, cudaStream_t s);
+                     const void* posC, double lengthscale, cudaStream_t s);
+int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                   cudaStream_t s);
+int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                   cudaStream_t s);
 
 // orbitals.cu
 int launch_evaluate(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx,

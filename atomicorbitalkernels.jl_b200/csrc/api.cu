@@ -182,7 +182,7 @@ int aok_plan_destroy(aok_plan* p) {
                     p->d_pb_rec,    p->d_pb_counts, p->d_pb_items,  p->d_pb_itemidx, p->d_pb_rows,
                     p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3,    p->d_order3,
                     p->d_pk,        p->d_segs,      p->d_nseg,      p->d_dpos_rec,   p->d_dpos_counts,
-                    p->d_dpos_items,  p->d_geo3};
+                    p->d_dpos_items};
     for (void* b : bufs) dfree(b);
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     if (p->cap) cudaStreamDestroy(p->cap);
@@ -321,7 +321,6 @@ namespace {
 struct TuneChoice {
     int ctas;
     size_t stage;
-    int deal;
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneChoice> g_tune_cache;
@@ -349,9 +348,8 @@ int aok_plan_autotune(aok_plan* p, void* out, const void* zeta, const void* coef
         const double v = f64 ? ((const double*)c.data())[i] : (double)((const float*)c.data())[i];
         key += v != 0.0 ? '1' : '0';
     }
-    auto apply = [&](int ctas, size_t stage, int deal) -> int {
+    auto apply = [&](int ctas, size_t stage) -> int {
         AOK_TRY(setup_overlap2c_schedule(p, ctas, stage));
-        p->fwd_deal = deal;
         AOK_TRY(launch_prep2c(p, zeta, coef, s));
         p->basis_set = true;
         return AOK_OK;
@@ -364,7 +362,7 @@ int aok_plan_autotune(aok_plan* p, void* out, const void* zeta, const void* coef
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            AOK_TRY(apply(it->second.ctas, it->second.stage, it->second.deal));
+            AOK_TRY(apply(it->second.ctas, it->second.stage));
             AOK_TRY(forward());
             if (choice) {
                 choice[0] = p->fwd_ctas;
@@ -383,12 +381,11 @@ int aok_plan_autotune(aok_plan* p, void* out, const void* zeta, const void* coef
     int st = cuda_status(cudaEventCreate(&e0), "cudaEventCreate");
     if (st == AOK_OK) st = cuda_status(cudaEventCreate(&e1), "cudaEventCreate");
     float best = -1.f;
-    TuneChoice bestc{0, 0, 0};
+    TuneChoice bestc{0, 0};
     for (int ct : ctas)
-        for (size_t sb : stages)
-          for (int deal = 0; deal < 2; ++deal) {
+        for (size_t sb : stages) {
             if (st != AOK_OK) break;
-            if (apply(ct, sb, deal) != AOK_OK) continue;  // shape does not fit this basis
+            if (apply(ct, sb) != AOK_OK) continue;  // shape does not fit this basis
             if (forward() != AOK_OK || forward() != AOK_OK) continue;
             // the faster of two timed batches of kReps forwards
             constexpr int kReps = 6;
@@ -404,21 +401,20 @@ int aok_plan_autotune(aok_plan* p, void* out, const void* zeta, const void* coef
             }
             if (st == AOK_OK && (best < 0.f || ms < best)) {
                 best = ms;
-                bestc = TuneChoice{p->fwd_ctas, p->stage_bytes, p->fwd_deal};
+                bestc = TuneChoice{p->fwd_ctas, p->stage_bytes};
             }
-          }
+        }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     p->ev = ev0;
     if (st != AOK_OK || best < 0.f) {  // leave the plan with its default shape
         const int st2 = setup_overlap2c_schedule(p);
-        p->fwd_deal = 0;
         p->basis_set = false;
         if (st != AOK_OK) return st;
         if (st2 != AOK_OK) return st2;
         return set_error(AOK_ERR_UNSUPPORTED, "aok_plan_autotune: no launch shape fits this basis");
     }
-    AOK_TRY(apply(bestc.ctas, bestc.stage, bestc.deal));
+    AOK_TRY(apply(bestc.ctas, bestc.stage));
     AOK_TRY(forward());
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);

@@ -512,9 +512,9 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
 // ---------------------------------------------------------------------------
 // Slot-parallel parameter pullback (used by aok_evaluate_pullback).
 //
-// A work unit is kEpbUnit = 128 consecutive points in the caller's order,
-// dealt statically to the warps.  For each 32 points the warp first puts lane =
-// point: radials (of the point's own species), harmonics, dX, and the radial
+// A work unit is kEpbUnit = 64 consecutive points in the caller's order, dealt
+// statically to the warps; four blocks of 8 warps per SM (<= 64 registers).  For
+// each 32 points the warp first puts lane = point: radials (of the point's own species), harmonics, dX, and the radial
 // cotangents gg_k = r^p_k sum_{i: iR[i] = k} dP[j,i] Z_{iY[i]} and f(r) into
 // shared memory (the dP rows and positions are read coalesced).  Then, per
 // species sigma present among the 32 points (a ballot), lane = slot (k, m) of
@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
 // index outside 1..NZ gets dX = 0, is left out of every species, and sets the
 // error word.
 // ---------------------------------------------------------------------------
-constexpr int kEpbUnit = 128;     // consecutive points per unit
+constexpr int kEpbUnit = 64;      // consecutive points per unit
 constexpr int kEpbMaxGroups = 4;  // slots per species <= 128
 
 struct EpbParams {
@@ -556,7 +556,7 @@ __host__ __device__ constexpr size_t epb_acc_words(int nRad, int K, int NZ) { re
 // radial in registers and walks the (radial, harmonic) -> orbital table (as
 // k_evaluate_reg), so a warp's shared memory holds only gg and f(r).
 template <typename FT, int L, bool RAD = false, bool REG = false>
-__global__ void __launch_bounds__(256) k_evaluate_pbs(const __grid_constant__ EpbParams Q) {
+__global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__ EpbParams Q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int nY = (L + 1) * (L + 1);
     const EvalParams& P = Q.E;

@@ -324,7 +324,6 @@ struct Ov2Params {
     unsigned* counter;
     Panels panels;
     int N, slab_stride;
-    int deal;               // 1: a segment's items dealt to the warps in snake order, no claims
     unsigned stage_offset;  // byte offset of the stage in dynamic shared memory
 };
 
@@ -360,9 +359,7 @@ __device__ __forceinline__ void tile_geo(Geo<FT>& g, int& b, const Ov2Params<FT>
 
 // Persistent CTAs take tiles (<= 32 batch elements of one species pair, one per
 // lane) from a global queue.  Per tile the CTA walks the pair's segments: the
-// warps take the segment's items from a shared counter (or, with `deal`, in a
-// fixed snake order: no claim per item, which pays off for bases of cheap
-// items; the autotuner picks) and run them on the
+// warps take the segment's items from a shared counter and run them on the
 // staged chunk, writing their blocks into the lane's slab of the current panel;
 // at a panel's end the CTA streams the slab out.  A chunk is copied into the
 // stage only when it is not there already (consecutive tiles of one species
@@ -418,16 +415,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c(const __grid_consta
         Seg S = segs[0];
         for (int k = 0; k < nseg; ++k) {
             if (k == nseg - 1 && threadIdx.x == 0) s_tile = (int)atomicAdd(P.counter, 1u);
-#pragma unroll 1
-            for (int rd = 0;; ++rd) {
-                int it;
-                if (P.deal) {  // round rd: forward, then backward (the list is heaviest first)
-                    it = S.it0 + rd * NW + ((rd & 1) ? NW - 1 - warp : warp);
-                } else {
-                    it = 0;
-                    if (lane == 0) it = atomicAdd(&s_cnt, 1);
-                    it = __shfl_sync(0xffffffffu, it, 0) + S.it0;
-                }
+            for (;;) {
+                int it = 0;
+                if (lane == 0) it = atomicAdd(&s_cnt, 1);
+                it = __shfl_sync(0xffffffffu, it, 0) + S.it0;
                 if (it >= S.it1) break;
                 const ExecItem e = sitems[it - S.ibase];
                 dispatch(e.cls, stage_saddr + 16u * (uint32_t)e.rec, e.n, g, sl + e.dst, P.N);
@@ -510,7 +501,6 @@ inline int launch_ov2(aok_plan* p, void* out, const void* posA, const void* posB
     P.panels = p->panels;
     P.N = (int)p->N;
     P.slab_stride = (int)p->slab_stride;
-    P.deal = p->fwd_deal;
     const size_t slab = (p->smem_bytes + 15) / 16 * 16;
     P.stage_offset = (unsigned)slab;
     const size_t smem = slab + p->stage_bytes;

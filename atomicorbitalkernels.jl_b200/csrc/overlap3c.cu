@@ -32,33 +32,21 @@ __global__ void k_prim3c(FT* __restrict__ pz, FT* __restrict__ pc, int* __restri
     pn[t] = n;
 }
 
-// Per call, one CTA: the item order of the kernel's unit queue.  Items that run
-// the same code (one shell-triple class and page chunk; all f-shell classes share
-// one routine) are kept together, so that the warps in flight at any time run
-// few distinct routines and the instruction cache holds them; the groups are
-// ordered by their heaviest item, heaviest first, and the items inside a group
-// heaviest first, so the queue ends with cheap work.  Cost = primitive triples
-// (the largest count over the species per shell) x (E tables + the chunk's
-// products) + a fixed part per item; the f-shell classes (run-time loops, FP64
-// tables) count four times.  Rank sort in shared memory; more than kOrder3Max
-// items keep the static order.
+// Per call, one CTA: the items sorted by estimated cost, heaviest first, so
+// that the kernel's unit queue (item-major) ends with cheap items.  Cost =
+// primitive triples (the largest count over the species per shell) x (E tables
+// + the chunk's products) + a fixed part per item; the f-shell classes
+// (run-time loops, FP64 tables) count four times.
+// Rank sort in shared memory; more than kOrder3Max items keep the static order.
 constexpr int kOrder3Max = 2048;
-constexpr int kCodes3 = 27 * 8 + 1;  // (class, chunk) codes of the specialised classes, + one for the f shells
-
-__device__ __forceinline__ int code3(const Item3& it) {
-    return it.cls >= kClsF3 ? kCodes3 - 1 : it.cls * 8 + it.chunk;
-}
 
 __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, const Item3* __restrict__ items,
                                                  const int* __restrict__ pn, int n, int ns, int NZ) {
-    __shared__ unsigned long long ikey[kOrder3Max], gkey[kOrder3Max];
-    __shared__ int gmax[kCodes3];
+    __shared__ unsigned long long key[kOrder3Max];
     if (n > kOrder3Max) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = items[i];
         return;
     }
-    for (int c = threadIdx.x; c < kCodes3; c += blockDim.x) gmax[c] = 0;
-    __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const Item3 it = items[i];
         const bool f = it.cls >= kClsF3;
@@ -75,23 +63,13 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         }
         long long cost = (long long)na * nb * nc * per * (f ? 4 : 1) + 64;
         cost = min(cost, (long long)0x7FFFFFFF);
-        // ascending = heaviest first; equal costs by routine, then by position
-        ikey[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | ((unsigned)code3(it) << 12) | (unsigned)i;
-        atomicMax(&gmax[code3(it)], (int)cost);
+        key[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | (unsigned)i;  // ascending key = descending cost
     }
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int ci = code3(items[i]);
-        gkey[i] = ((unsigned long long)(0x7FFFFFFF - gmax[ci]) << 32) | (unsigned)ci;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const unsigned long long gi = gkey[i], ki = ikey[i];
+        const unsigned long long ki = key[i];
         int r = 0;
-        for (int j = 0; j < n; ++j) {
-            const unsigned long long gj = gkey[j];
-            r += gj < gi || (gj == gi && ikey[j] < ki);
-        }
+        for (int j = 0; j < n; ++j) r += key[j] < ki;
         order[r] = items[i];
     }
 }
@@ -139,11 +117,19 @@ int setup_overlap3c_schedule(aok_plan* p) {
     return AOK_OK;
 }
 
+// The kernel's unit counter (32 bits, each warp claims one past the end) must not
+// wrap: at most nitems x (B / 32 + one partial tile per key) units.
+static int check_units3(const aok_plan* p, int64_t B, const char* who) {
+    if ((int64_t)p->nitems3 * ((B + 31) / 32 + bin_keys_max(p->NZ) + 1) >= ((int64_t)1 << 31))
+        return set_error(AOK_ERR_LENGTH, std::string(who) + ": too many (shell triple, tile) units; split the batch");
+    return AOK_OK;
+}
+
 // The 3C overlap after the schedule is set up: compact primitive lists of the
 // padded (zeta, coef) tables, per-call item order, then the kernel over the
 // plan's bins (binned by the caller).
 int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
-                     const void* posC, int64_t B, double lengthscale, cudaStream_t s) {
+                     const void* posC, double lengthscale, cudaStream_t s) {
     const int nsz = (int)(p->ns * p->NZ), th = 128, bl = (nsz + th - 1) / th;
     const size_t nt = (size_t)(p->ns * p->K * p->NZ);
     if (p->prec == AOK_PREC_F64)
@@ -157,8 +143,8 @@ int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef,
     k_order3c<<<1, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, p->nitems3, (int)p->ns,
                                 (int)p->NZ);
     if ((st = cuda_status(cudaGetLastError(), "k_order3c")) != AOK_OK) return st;
-    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, B, lengthscale, s);
-    return launch_ov3_f32(p, out, posA, posB, posC, B, lengthscale, s);
+    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s);
+    return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s);
 }
 
 }  // namespace aok
@@ -177,10 +163,11 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
     if (B == 0) return AOK_OK;
     if (!out || !nprim || !prim_offset || !coef || !alpha || !posA || !posB || !posC)
         return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: null pointer");
+    if ((st = check_units3(p, B, "aok_overlap3c_gb")) != AOK_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     if ((st = launch_gb_pad(p, nprim, prim_offset, coef, alpha, s)) != AOK_OK) return st;
     if ((st = launch_bin(p, nullptr, nullptr, B, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, p->d_gb_zeta, p->d_gb_coef, posA, posB, posC, B, 1.0, s);
+    return launch_overlap3c(p, out, p->d_gb_zeta, p->d_gb_coef, posA, posB, posC, 1.0, s);
 }
 
 extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
@@ -195,9 +182,10 @@ extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const voi
     if (B == 0) return AOK_OK;
     if (!out || !zeta || !coef || !posA || !posB || !posC || !sidxA || !sidxB || !sidxC)
         return set_error(AOK_ERR_INVALID, std::string(who) + ": null pointer");
+    if ((st = check_units3(p, B, who)) != AOK_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     ++p->gen;  // the plan's bins change
     const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
     if ((st = launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, zeta, coef, posA, posB, posC, B, lengthscale, s);
+    return launch_overlap3c(p, out, zeta, coef, posA, posB, posC, lengthscale, s);
 }

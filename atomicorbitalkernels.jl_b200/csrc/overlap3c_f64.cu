@@ -3,10 +3,10 @@
 
 namespace aok {
 
-int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
-                   double lengthscale, cudaStream_t s) {
-    if (p->Lmax > kMaxL3Spec) return launch_ov3<double, true>(p, out, posA, posB, posC, B, lengthscale, s);
-    return launch_ov3<double, false>(p, out, posA, posB, posC, B, lengthscale, s);
+int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                   cudaStream_t s) {
+    if (p->Lmax > kMaxL3Spec) return launch_ov3<double, true>(p, out, posA, posB, posC, lengthscale, s);
+    return launch_ov3<double, false>(p, out, posA, posB, posC, lengthscale, s);
 }
 
 }  // namespace aok

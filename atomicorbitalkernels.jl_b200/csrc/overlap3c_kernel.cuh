@@ -204,10 +204,8 @@ struct Prim3 {
 
 // Records q0 .. q0 + 31 of the unit into the warp's buffer, one per lane (FP64
 // arithmetic), in (ip, jp, kp) order; the caller brackets it with __syncwarp.
-// One out-of-line copy per precision: its FP64 divisions are long code, which
-// every class routine would otherwise carry through the instruction cache.
 template <typename PT, typename FT>
-__device__ __noinline__ void gen_records3(PT* buf, const Prim3<FT> pr, int q0, int n, int lane) {
+__device__ __forceinline__ void gen_records3(PT* buf, const Prim3<FT>& pr, int q0, int n, int lane) {
     const int q = q0 + lane;
     if (q >= n) return;
     const int nb = pr.n[1], nc = pr.n[2];
@@ -216,7 +214,7 @@ __device__ __noinline__ void gen_records3(PT* buf, const Prim3<FT> pr, int q0, i
             (double)pr.z[1][jp], (double)pr.z[2][kp], ip * nb + jp);
 }
 
-// lin (0-based, within the block) -> offset in the lane's output block;
+// lin (0-based, within the block) -> offset in the lane's panel slab;
 // block element (i, j, k) = (lin % NA, (lin / NA) % NB, lin / PS).
 // Only pages inside [kp0, kp1) (block-local) are stored.
 template <int LA, int LB, int LC, int C>
@@ -248,14 +246,14 @@ __device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Ge
         const float4 r1 = reinterpret_cast<const float4*>(buf + q)[1];
         const float4 r2 = reinterpret_cast<const float4*>(buf + q)[2];
         const float w = r0.x;
-        if (r2.w != prev) {  // a new (ip, jp) group: fold the partial sums
+        if (r2.w != prev) {
 #pragma unroll
-            for (int mm = 0; mm < M; ++mm) {
+            for (int m = 0; m < M; ++m) {
                 float s, e;
-                two_sum(hi[mm], part[mm], s, e);
-                hi[mm] = s;
-                part[mm] = 0.f;
-                lo[mm] += e;
+                two_sum(hi[m], part[m], s, e);
+                hi[m] = s;
+                part[m] = 0.f;
+                lo[m] += e;
             }
             prev = r2.w;
         }
@@ -287,7 +285,8 @@ __device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Ge
                     if (lin >= L0 && lin < L0 + M) {
                         const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
                                          Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
-                        part[lin - L0] = fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
+                        part[lin - L0] =
+                            fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
                     }
                 }
       }
@@ -512,167 +511,86 @@ __device__ __forceinline__ void dispatch3(int cls, int chunk, const Prim3<FT>& p
     }
 }
 
-// Geometry of one (tile, lane) slot, gathered once per call (k_geo3): the pair
-// differences and squared distances of the lane's element, and the element (b < 0:
-// a lane past the tile's end).
-template <typename FT> struct __align__(16) TGeo3 {
-    Geo3<FT> g;
-    int b;
-};
-
-template <typename FT>
-__global__ void __launch_bounds__(128) k_geo3(TGeo3<FT>* __restrict__ out, const FT* __restrict__ posA,
-                                              const FT* __restrict__ posB, const FT* __restrict__ posC,
-                                              const int* __restrict__ perm, const int4* __restrict__ tiles,
-                                              const int* __restrict__ ntiles, int cap_tiles, FT s, int use_s) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = (int)(i >> 5), lane = (int)(i & 31);
-    if (t >= cap_tiles || t >= *ntiles) return;
-    const int4 td = tiles[t];
-    TGeo3<FT> r;
-    if (lane < td.z) {
-        const int b = perm[td.y + lane];
-        load_geo3(r.g, posA + 3 * (size_t)b, posB + 3 * (size_t)b, posC + 3 * (size_t)b, s, use_s != 0);
-        r.b = b;
-    } else {
-        const FT z[3] = {FT(0), FT(0), FT(0)};
-        load_geo3(r.g, z, z, z, s, false);
-        r.b = -1;
-    }
-    out[i] = r;
-}
-
 template <typename FT>
 struct Ov3Params {
     FT* out;
-    const TGeo3<FT>* geo;  // (tile, lane) slots (k_geo3)
-    const FT* pz;          // compact primitive lists: zeta, coef of (species g, shell s) at (g ns + s) K
+    const FT* posA;
+    const FT* posB;
+    const FT* posC;
+    const FT* pz;        // compact primitive lists: zeta, coef of (species g, shell s) at (g ns + s) K
     const FT* pc;
-    const int* pn;         // their lengths, (g ns + s)
+    const int* pn;       // their lengths, (g ns + s)
+    const int* perm;
     const int4* tiles;
     const int* ntiles;
     unsigned* counter;
-    const Item3* items;    // every (shell triple, page chunk) in the per-call order (k_order3c)
+    const Item3* items;  // every (shell triple, page chunk), heaviest first (k_order3c)
     int nitems, ns, K, N, NZ;
-    int stage_lists, stage_items;  // copy the lists / the item list into shared memory first
+    FT scale;
+    int use_scale;
     int boff[kMaxShells + 1];
 };
 
-// Dynamic shared memory of the staged tables: zeta, coef lists (ns K NZ each), the
-// lengths (ns NZ ints), then the items.
-template <typename FT>
-__host__ __device__ inline size_t ov3_stage_lists_bytes(int ns, int K, int NZ) {
-    return ((2 * (size_t)ns * K * NZ * sizeof(FT) + (size_t)ns * NZ * sizeof(int)) + 15) / 16 * 16;
-}
-
 // Work unit = (item, tile): one shell-triple block (or page chunk of it) for the
-// 32 batch elements of a tile, lane = element.  Units are drained from one global
-// counter item-major in the per-call item order (k_order3c: the items of one
-// routine together, heaviest first), so the warps in flight run few distinct
-// routines and every routine's heavy items start first.  The next unit is
-// claimed when a unit starts, so the claim's latency hides behind the unit's
-// work; the geometry is one load per lane from the gathered slots, and the
-// primitive lists and the items come from shared memory.  A lane writes its
-// element's block straight to the output: a batch element's (N,N,N) slab is
-// contiguous and the whole output is written exactly once, so the scattered
-// stores of a block meet in L2.  No panels and no barriers.  Three CTAs of four
+// 32 batch elements of a tile, lane = element.  Units are drained from one
+// global counter item-major, so every tile's heaviest items run first and the
+// cheap ones fill the end; there are no panels and no barriers.  A lane writes
+// its element's block straight to the output: a batch element's (N,N,N) slab
+// is contiguous and the whole output is written exactly once, so the scattered
+// stores of a block meet in L2 before they reach DRAM.  Three CTAs of four
 // warps per SM (<= 168 registers).
 template <typename FT, bool F3>
 __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
     using PT = typename PTT<FT>::type;
     __shared__ PT recbuf[kThreads3 / 32][32];  // each warp's current 32 records
-    extern __shared__ __align__(16) unsigned char sm3[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const FT* pz = P.pz;
-    const FT* pc = P.pc;
-    const int* pn = P.pn;
-    const Item3* items = P.items;
-    const int nl = P.ns * P.K * P.NZ, nn = P.ns * P.NZ;
-    if (P.stage_lists) {
-        FT* sz = reinterpret_cast<FT*>(sm3);
-        FT* sc = sz + nl;
-        int* sn = reinterpret_cast<int*>(sc + nl);
-        for (int i = threadIdx.x; i < nl; i += blockDim.x) {
-            sz[i] = pz[i];
-            sc[i] = pc[i];
-        }
-        for (int i = threadIdx.x; i < nn; i += blockDim.x) sn[i] = pn[i];
-        pz = sz;
-        pc = sc;
-        pn = sn;
-        if (P.stage_items) {
-            Item3* si = reinterpret_cast<Item3*>(sm3 + ov3_stage_lists_bytes<FT>(P.ns, P.K, P.NZ));
-            for (int i = threadIdx.x; i < P.nitems; i += blockDim.x) si[i] = items[i];
-            items = si;
-        }
-        __syncthreads();
-    }
     const int ntiles = *P.ntiles;
     const unsigned total = (unsigned)ntiles * (unsigned)P.nitems;
     const size_t N2 = (size_t)P.N * P.N, N3 = N2 * P.N;
-    unsigned u = 0;
-    if (lane == 0) u = atomicAdd(P.counter, 1u);
-    u = __shfl_sync(0xffffffffu, u, 0);
-    while (u < total) {
-        unsigned un = 0;  // the next unit, used only at the end of this one
-        if (lane == 0) un = atomicAdd(P.counter, 1u);
+    for (;;) {
+        unsigned u = 0;
+        if (lane == 0) u = atomicAdd(P.counter, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= total) break;
         const int it = (int)(u / (unsigned)ntiles), tile = (int)(u % (unsigned)ntiles);
-        const TGeo3<FT> tg = P.geo[(size_t)tile * 32 + lane];
-        const int key = __ldg(&P.tiles[tile].x);
-        const Item3 wi = items[it];
-        const bool valid = tg.b >= 0;
+        const int4 td = P.tiles[tile];
+        const bool valid = lane < td.z;
+        const int b = P.perm[td.y + (valid ? lane : 0)];
+        Geo3<FT> g;
+        load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b, P.scale,
+                  P.use_scale != 0);
+        const Item3 wi = P.items[it];
         // the tile's species triple (key ((ga NZ) + gb) NZ + gc; 0 on the single-species path)
-        const int ga = key / (P.NZ * P.NZ), gb = (key / P.NZ) % P.NZ, gc = key % P.NZ;
+        const int ga = td.x / (P.NZ * P.NZ), gb = (td.x / P.NZ) % P.NZ, gc = td.x % P.NZ;
         Prim3<FT> pr;
         const int la = ga * P.ns + wi.sa, lb = gb * P.ns + wi.sb, lc = gc * P.ns + wi.sc;
-        pr.z[0] = pz + (size_t)la * P.K;
-        pr.c[0] = pc + (size_t)la * P.K;
-        pr.n[0] = pn[la];
-        pr.z[1] = pz + (size_t)lb * P.K;
-        pr.c[1] = pc + (size_t)lb * P.K;
-        pr.n[1] = pn[lb];
-        pr.z[2] = pz + (size_t)lc * P.K;
-        pr.c[2] = pc + (size_t)lc * P.K;
-        pr.n[2] = pn[lc];
-        FT* dst = P.out + (size_t)(valid ? tg.b : 0) * N3 + (size_t)P.boff[wi.sc] * N2 +
-                  (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-        dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, recbuf[warp], tg.g, dst, P.N, 0, kAllPages3, valid);
-        u = __shfl_sync(0xffffffffu, un, 0);
+        pr.z[0] = P.pz + (size_t)la * P.K;
+        pr.c[0] = P.pc + (size_t)la * P.K;
+        pr.n[0] = __ldg(P.pn + la);
+        pr.z[1] = P.pz + (size_t)lb * P.K;
+        pr.c[1] = P.pc + (size_t)lb * P.K;
+        pr.n[1] = __ldg(P.pn + lb);
+        pr.z[2] = P.pz + (size_t)lc * P.K;
+        pr.c[2] = P.pc + (size_t)lc * P.K;
+        pr.n[2] = __ldg(P.pn + lc);
+        FT* dst = P.out + (size_t)b * N3 + (size_t)P.boff[wi.sc] * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
+        dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, recbuf[warp], g, dst, P.N, 0, kAllPages3, valid);
     }
 }
 
 template <typename FT, bool F3>
-inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, int64_t B,
-                      double lengthscale, cudaStream_t s) {
-    // the (tile, lane) geometry slots: at most B / 32 + one partial tile per key
-    const int cap_tiles = (int)std::min<int64_t>(p->max_tiles, (B + 31) / 32 + bin_keys_max(p->NZ) + 1);
-    // the unit counter (32 bits, each warp claims one past the end) must not wrap
-    if ((int64_t)p->nitems3 * cap_tiles >= ((int64_t)1 << 31))
-        return set_error(AOK_ERR_LENGTH, "3C overlap: too many (shell triple, tile) units for one call; split the batch");
-    const size_t slot = sizeof(TGeo3<FT>), need = (size_t)cap_tiles * 32 * slot;
-    if (p->geo3_bytes < need) {
-        if (p->d_geo3) cudaFree(p->d_geo3);
-        p->d_geo3 = nullptr;
-        p->geo3_bytes = 0;
-        cudaError_t e = cudaMalloc(&p->d_geo3, need);
-        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(geo3)");
-        p->geo3_bytes = need;
-    }
-    const FT sc = (FT)lengthscale;
-    const int use_s = sc != FT(1);
-    const long long slots = (long long)cap_tiles * 32;
-    k_geo3<FT><<<(unsigned)((slots + 127) / 128), 128, 0, s>>>((TGeo3<FT>*)p->d_geo3, (const FT*)posA,
-                                                              (const FT*)posB, (const FT*)posC, p->d_perm,
-                                                              p->d_tiles, p->d_ntiles, cap_tiles, sc, use_s);
-    int st = cuda_status(cudaGetLastError(), "k_geo3");
-    if (st != AOK_OK) return st;
+inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
+                      cudaStream_t s) {
     Ov3Params<FT> P;
     memset(&P, 0, sizeof(P));
     P.out = (FT*)out;
-    P.geo = (const TGeo3<FT>*)p->d_geo3;
+    P.posA = (const FT*)posA;
+    P.posB = (const FT*)posB;
+    P.posC = (const FT*)posC;
     P.pz = (const FT*)p->d_pp3;
     P.pc = (const FT*)p->d_pp3 + p->ns * p->K * p->NZ;
     P.pn = p->d_npp3;
+    P.perm = p->d_perm;
     P.tiles = p->d_tiles;
     P.ntiles = p->d_ntiles;
     P.counter = p->d_counter;
@@ -682,23 +600,15 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.K = (int)p->K;
     P.N = (int)p->N;
     P.NZ = (int)p->NZ;
+    P.scale = (FT)lengthscale;
+    P.use_scale = (FT)lengthscale != FT(1);
     for (int i = 0; i <= p->ns; ++i) P.boff[i] = (int)p->boff[i];
-    // shared-memory staging within 32 KB per CTA (three CTAs per SM keep fitting)
-    const size_t lists = ov3_stage_lists_bytes<FT>(P.ns, P.K, P.NZ);
-    const size_t with_items = lists + sizeof(Item3) * (size_t)P.nitems;
-    size_t smem = 0;
-    if (with_items <= 32 * 1024) {
-        P.stage_lists = P.stage_items = 1;
-        smem = with_items;
-    } else if (lists <= 32 * 1024) {
-        P.stage_lists = 1;
-        smem = lists;
-    }
     auto kern = k_overlap3c<FT, F3>;
     int occ = 0;
-    if ((st = kernel_prepare((const void*)kern, smem, kThreads3, &occ)) != AOK_OK) return st;
+    const int st = kernel_prepare((const void*)kern, 0, kThreads3, &occ);
+    if (st != AOK_OK) return st;
     timing_begin(p, s);
-    kern<<<p->num_sms * std::max(occ, 1), kThreads3, smem, s>>>(P);
+    kern<<<p->num_sms * std::max(occ, 1), kThreads3, 0, s>>>(P);
     timing_end(p, s);
     return cuda_status(cudaGetLastError(), "k_overlap3c");
 }
