@@ -319,9 +319,43 @@ struct EvalRegParams {
     EvalParams E;
     int16_t otab[kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1)];
     int8_t poly[kRegMaxRad];
+    // block maps (BLK): radial k feeds the 2l+1 orbitals ob[k] .. ob[k] + 2l, in
+    // harmonic order l^2 .. l^2 + 2l, with l = lk[k] (-1: a radial no orbital uses)
+    int8_t lk[kRegMaxRad];
+    int16_t ob[kRegMaxRad];
 };
 
-template <typename FT, int L, bool GRAD>
+// The orbitals of one radial under block maps: 2 LL + 1 outputs, harmonic and
+// orbital indices known at compile time relative to the block's start.
+template <typename FT, int LL, int L, bool GRAD>
+__device__ __forceinline__ void emit_block(FT R, FT dR, FT ux, FT uy, FT uz, FT sc, const FT (&Z)[(L + 1) * (L + 1)],
+                                           const FT (&G)[3 * (L + 1) * (L + 1)], FT* Pout, FT* dPout, long long j,
+                                           long long nX, int o0) {
+    if constexpr (LL <= L) {
+#pragma unroll
+        for (int m = 0; m <= 2 * LL; ++m) {
+            const int yi = LL * LL + m;
+            const long long at = j + nX * (o0 + m);
+            Pout[at] = R * Z[yi];
+            if (GRAD) {
+                FT gx = (dR * ux) * Z[yi] + R * G[3 * yi + 0];
+                FT gy = (dR * uy) * Z[yi] + R * G[3 * yi + 1];
+                FT gz = (dR * uz) * Z[yi] + R * G[3 * yi + 2];
+                if (sc != FT(1)) {
+                    gx *= sc;
+                    gy *= sc;
+                    gz *= sc;
+                }
+                FT* op = dPout + 3 * at;
+                op[0] = gx;
+                op[1] = gy;
+                op[2] = gz;
+            }
+        }
+    }
+}
+
+template <typename FT, int L, bool GRAD, bool BLK = false>
 __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_constant__ EvalRegParams Q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const EvalParams& P = Q.E;
@@ -360,27 +394,43 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_cons
         FT Z[nY], G[3 * nY];
         solid_harmonics<FT, L>(x, y, z, P.F, Z, G, 1);
         const FT ux = x / r, uy = y / r, uz = z / r;  // X[j] / r[j] (NaN at r = 0, as the reference)
-        for (int k = 0; k < P.nRad; ++k) {
-            FT R, dR;
-            radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
+        if constexpr (BLK) {
+            for (int k = 0; k < P.nRad; ++k) {
+                const int l = Q.lk[k];
+                if (l < 0) continue;
+                FT R, dR;
+                radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
+                const int o0 = Q.ob[k];
+                switch (l) {
+                    case 0: emit_block<FT, 0, L, GRAD>(R, dR, ux, uy, uz, sc, Z, G, Pout, dPout, j, P.nX, o0); break;
+                    case 1: emit_block<FT, 1, L, GRAD>(R, dR, ux, uy, uz, sc, Z, G, Pout, dPout, j, P.nX, o0); break;
+                    case 2: emit_block<FT, 2, L, GRAD>(R, dR, ux, uy, uz, sc, Z, G, Pout, dPout, j, P.nX, o0); break;
+                    default: emit_block<FT, 3, L, GRAD>(R, dR, ux, uy, uz, sc, Z, G, Pout, dPout, j, P.nX, o0); break;
+                }
+            }
+        } else {
+            for (int k = 0; k < P.nRad; ++k) {
+                FT R, dR;
+                radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
 #pragma unroll
-            for (int yi = 0; yi < nY; ++yi) {
-                const int o = Q.otab[k * nY + yi];
-                if (o < 0) continue;
-                Pout[j + P.nX * o] = R * Z[yi];
-                if (GRAD) {
-                    FT gx = (dR * ux) * Z[yi] + R * G[3 * yi + 0];
-                    FT gy = (dR * uy) * Z[yi] + R * G[3 * yi + 1];
-                    FT gz = (dR * uz) * Z[yi] + R * G[3 * yi + 2];
-                    if (sc != FT(1)) {
-                        gx *= sc;
-                        gy *= sc;
-                        gz *= sc;
+                for (int yi = 0; yi < nY; ++yi) {
+                    const int o = Q.otab[k * nY + yi];
+                    if (o < 0) continue;
+                    Pout[j + P.nX * o] = R * Z[yi];
+                    if (GRAD) {
+                        FT gx = (dR * ux) * Z[yi] + R * G[3 * yi + 0];
+                        FT gy = (dR * uy) * Z[yi] + R * G[3 * yi + 1];
+                        FT gz = (dR * uz) * Z[yi] + R * G[3 * yi + 2];
+                        if (sc != FT(1)) {
+                            gx *= sc;
+                            gy *= sc;
+                            gz *= sc;
+                        }
+                        FT* op = dPout + 3 * (j + P.nX * o);
+                        op[0] = gx;
+                        op[1] = gy;
+                        op[2] = gz;
                     }
-                    FT* op = dPout + 3 * (j + P.nX * o);
-                    op[0] = gx;
-                    op[1] = gy;
-                    op[2] = gz;
                 }
             }
         }
@@ -893,6 +943,35 @@ static void fill_params(aok_orbitals* o, EvalParams& P, const void* X, const int
         }
 }
 
+// Block maps: every radial k that any orbital uses feeds exactly the 2l+1
+// orbitals ob[k] .. ob[k] + 2l, in harmonic order l^2 .. l^2 + 2l (the layout
+// the reference's AtomicOrbitals builds, atomicorbitals.jl:56-75).  Fills lk, ob.
+static bool block_maps(const aok_orbitals* o, int8_t* lk, int16_t* ob) {
+    if (o->nRad > kRegMaxRad) return false;
+    for (int64_t k = 0; k < o->nRad; ++k) {
+        lk[k] = -1;
+        ob[k] = 0;
+    }
+    std::vector<int> cnt((size_t)o->nRad, 0);
+    for (int64_t i = 0; i < o->nOrb; ++i) {
+        const int64_t k = o->iR[i] - 1, yi = o->iY[i] - 1;
+        int& c = cnt[(size_t)k];
+        if (c == 0) {  // the radial's first orbital opens its block at m = 0
+            int l = 0;
+            while ((l + 1) * (l + 1) <= yi) ++l;
+            if (yi != l * l || l > kRegMaxL || i > 32767) return false;
+            lk[k] = (int8_t)l;
+            ob[k] = (int16_t)i;
+        } else if (i != ob[k] + c || yi != lk[k] * lk[k] + c || c > 2 * lk[k]) {
+            return false;
+        }
+        ++c;
+    }
+    for (int64_t k = 0; k < o->nRad; ++k)
+        if (cnt[(size_t)k] != 0 && cnt[(size_t)k] != 2 * lk[k] + 1) return false;
+    return true;
+}
+
 // The register-path forward when the maps allow it (L <= 3, nRad <= 64, each
 // (radial, harmonic) pair at most once, radial powers < 128); returns -1 otherwise.
 template <typename FT, int L>
@@ -912,10 +991,12 @@ static int launch_eval_reg_L(aok_orbitals* o, const EvalParams& P, bool grad, cu
         if (o->poly[k] > 127) return -1;
         Q.poly[k] = (int8_t)o->poly[k];
     }
+    const bool blk = block_maps(o, Q.lk, Q.ob);
     const size_t fsz = sizeof(FT);
     const size_t smem = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
     if (smem > 227 * 1024) return -1;
-    void* k = grad ? (void*)k_evaluate_reg<FT, L, true> : (void*)k_evaluate_reg<FT, L, false>;
+    void* k = blk ? (grad ? (void*)k_evaluate_reg<FT, L, true, true> : (void*)k_evaluate_reg<FT, L, false, true>)
+                  : (grad ? (void*)k_evaluate_reg<FT, L, true> : (void*)k_evaluate_reg<FT, L, false>);
     int occ = 0;
     AOK_TRY_PB(kernel_prepare(k, smem, kEvalThreads, &occ));
     const int grid = (int)std::max<int64_t>(

@@ -257,3 +257,31 @@ def test_evaluate_ed_general_maps(FT, tol):
     assert rel_fro(Pg, Pr) < tol and rel_fro(dPg, dPr) < tol
     n = len(orb)
     assert np.array_equal(Pg[:, n:], Pg[:, :2])
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-12), (torch.float32, 2e-6)])
+def test_evaluate_ed_permuted_maps(FT, tol):
+    """Orbitals listed in reverse order: each (radial, harmonic) pair is still used once,
+    but a radial's orbitals no longer form a block in harmonic order, so the forward
+    takes the table-driven register kernel instead of the block one; both give the
+    oracle's values."""
+    import ctypes
+
+    from aok_b200 import _dev, _lib
+    b, orb = _basis()
+    iR, iY = orb.radidx[::-1].copy(), orb.ylmidx[::-1].copy()
+    nX = 3000
+    X, sidx = W.config1_points(nX=nX, seed=23)
+    plan = _dev.OrbPlan(b.zeta.shape[0], b.K, b.NZ, orb.Rnl.powers(), iR, iY, orb.L, orb.Rnl.kind,
+                        _dev.prec_of(FT))
+    P = _dev.colmajor_empty((nX, len(iR)), FT)
+    dP = _dev.colmajor_empty((3, nX, len(iR)), FT)
+    Xd, sd = _dev.to_colmajor(X, FT), torch.as_tensor(sidx).cuda()
+    zd, Dd = _dev.to_colmajor(b.zeta, FT), _dev.to_colmajor(b.D, FT)
+    _lib.check(_lib.load().aok_evaluate_ed(plan.h, _dev.ptr(P), _dev.ptr(dP), _dev.ptr(Xd),
+                                           ctypes.c_void_p(sd.data_ptr()), _dev.ptr(zd), _dev.ptr(Dd), nX, 1.0,
+                                           _dev.stream()))
+    rnd = f32_round if FT == torch.float32 else (lambda a: a)
+    Pr, dPr = oracle.evaluate_ed(rnd(X), sidx, rnd(b.zeta), rnd(b.D), orb.Rnl.powers(), iR, iY, orb.L, nthreads=8)
+    Pg, dPg = P.double().cpu().numpy(), dP.double().cpu().numpy()
+    assert rel_fro(Pg, Pr) < tol and rel_fro(dPg, dPr) < tol
