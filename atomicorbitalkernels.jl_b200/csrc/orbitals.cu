@@ -175,17 +175,65 @@ __device__ __forceinline__ int radial_count(const FT* D, int k, int sg, int nRad
     return mk;
 }
 
+// (zeta, D, zeta log2 e) of primitive slot o: three separate shared-memory
+// tables, or one packed entry per slot (one 16-byte load in FP32).
 template <typename FT>
-__device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl, const int* sn, int k, int sg,
-                                       int nRad, int K, int p, int slater, FT r, FT& R, FT& dR) {
+struct SepTab {
+    const FT *z, *D, *l;
+    __device__ __forceinline__ void get(int o, FT& zo, FT& Do, FT& lo) const {
+        zo = z[o];
+        Do = D[o];
+        lo = l[o];
+    }
+};
+struct __align__(16) Pk64 {
+    double z, D, l, pad;
+};
+template <typename FT> struct PkEntry;
+template <> struct PkEntry<float> { using type = float4; };
+template <> struct PkEntry<double> { using type = Pk64; };
+template <typename FT>
+struct PkTab {
+    const typename PkEntry<FT>::type* p;
+    __device__ __forceinline__ void get(int o, FT& zo, FT& Do, FT& lo) const {
+        const auto t = p[o];
+        if constexpr (sizeof(FT) == 4) {
+            zo = t.x;
+            Do = t.y;
+            lo = t.z;
+        } else {
+            zo = t.z;
+            Do = t.D;
+            lo = t.l;
+        }
+    }
+};
+template <typename FT>
+__device__ __forceinline__ typename PkEntry<FT>::type pk_entry(FT z, FT D, FT l) {
+    typename PkEntry<FT>::type e;
+    if constexpr (sizeof(FT) == 4) {
+        e = make_float4(z, D, l, 0.f);
+    } else {
+        e.z = z;
+        e.D = D;
+        e.l = l;
+        e.pad = 0.0;
+    }
+    return e;
+}
+
+template <typename FT, typename Tab>
+__device__ __forceinline__ void radial_t(const Tab& tb, const int* sn, int k, int sg, int nRad, int K, int p,
+                                         int slater, FT r, FT& R, FT& dR) {
     const FT f = slater ? r : r * r;
     const FT df = slater ? FT(1) : FT(2) * r;
     FT s = FT(0), se = FT(0), ds = FT(0);
     const int mk = sn[k + nRad * sg];
     for (int m = 0; m < mk; ++m) {
         const int o = k + nRad * (m + K * sg);
-        const FT z = sz[o];
-        const FT a = mul_rn(sD[o], exp_neg(z, sl[o], f));
+        FT z, D, zl;
+        tb.get(o, z, D, zl);
+        const FT a = mul_rn(D, exp_neg(z, zl, f));
         if constexpr (sizeof(FT) == 4) {
             const float t = s + a, bb = t - s;
             se += (s - (t - bb)) + (a - bb);
@@ -205,6 +253,12 @@ __device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl,
     }
     R = mul_rn(rp, s);
     dR = drp * s + rp * ds;
+}
+
+template <typename FT>
+__device__ __forceinline__ void radial(const FT* sz, const FT* sD, const FT* sl, const int* sn, int k, int sg,
+                                       int nRad, int K, int p, int slater, FT r, FT& R, FT& dR) {
+    radial_t<FT>(SepTab<FT>{sz, sD, sl}, sn, k, sg, nRad, K, p, slater, r, R, dR);
 }
 
 // shared layout: zeta, D tables, then per-thread R, dR (nRad), Z (nY), G (3 nY)
@@ -361,14 +415,11 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_cons
     const EvalParams& P = Q.E;
     constexpr int nY = (L + 1) * (L + 1);
     const int ntab = P.nRad * P.K * P.NZ;
-    FT* sz = reinterpret_cast<FT*>(smem_raw);
-    FT* sD = sz + ntab;
-    FT* sl = sD + ntab;
-    int* sn = reinterpret_cast<int*>(sl + ntab);
+    auto* pk = reinterpret_cast<typename PkEntry<FT>::type*>(smem_raw);  // (zeta, D, zeta log2 e) per slot
+    int* sn = reinterpret_cast<int*>(pk + ntab);
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
-        sz[i] = ((const FT*)P.zeta)[i];
-        sD[i] = ((const FT*)P.D)[i];
-        sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
+        const FT z = ((const FT*)P.zeta)[i];
+        pk[i] = pk_entry<FT>(z, ((const FT*)P.D)[i], (FT)((double)z * 1.4426950408889634074));
     }
     for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
         sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
@@ -399,7 +450,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_cons
                 const int l = Q.lk[k];
                 if (l < 0) continue;
                 FT R, dR;
-                radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
+                radial_t<FT>(PkTab<FT>{pk}, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
                 const int o0 = Q.ob[k];
                 switch (l) {
                     case 0: emit_block<FT, 0, L, GRAD>(R, dR, ux, uy, uz, sc, Z, G, Pout, dPout, j, P.nX, o0); break;
@@ -411,7 +462,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_cons
         } else {
             for (int k = 0; k < P.nRad; ++k) {
                 FT R, dR;
-                radial<FT>(sz, sD, sl, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
+                radial_t<FT>(PkTab<FT>{pk}, sn, k, sg, P.nRad, P.K, Q.poly[k], P.slater, r, R, dR);
 #pragma unroll
                 for (int yi = 0; yi < nY; ++yi) {
                     const int o = Q.otab[k * nY + yi];
@@ -589,7 +640,33 @@ struct EpbParams {
     // register path (REG): (radial, harmonic) -> orbital table and radial powers
     int16_t otab[kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1)];
     int8_t poly[kRegMaxRad];
+    // and, for block maps (blk != 0), each radial's l and first orbital (block_maps)
+    int blk;
+    int8_t lk[kRegMaxRad];
+    int16_t ob[kRegMaxRad];
 };
+
+// Point phase of the register pullback under block maps: radial k's 2 LL + 1
+// orbitals o0 + m with harmonics LL^2 + m; adds their dX terms and returns the
+// radial cotangent sum_m dP[j, o0 + m] Z[LL^2 + m].
+template <typename FT, int LL, int L>
+__device__ __forceinline__ FT pb_block(FT Rk, FT dRk, FT ux, FT uy, FT uz, const FT (&Z)[(L + 1) * (L + 1)],
+                                       const FT (&G)[3 * (L + 1) * (L + 1)], const FT* dPin, long long j,
+                                       long long nX, int o0, FT& ax, FT& ay, FT& az) {
+    FT gk = FT(0);
+    if constexpr (LL <= L) {
+#pragma unroll
+        for (int m = 0; m <= 2 * LL; ++m) {
+            const int yi = LL * LL + m;
+            const FT g = dPin[j + nX * (o0 + m)];
+            ax += g * ((dRk * ux) * Z[yi] + Rk * G[3 * yi + 0]);
+            ay += g * ((dRk * uy) * Z[yi] + Rk * G[3 * yi + 1]);
+            az += g * ((dRk * uz) * Z[yi] + Rk * G[3 * yi + 2]);
+            gk += g * Z[yi];
+        }
+    }
+    return gk;
+}
 
 // per-warp shared-memory scratch of the slot-parallel pullback (floats of FT):
 // R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][32], f [32]
@@ -674,6 +751,35 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                     const FT ux = x / r, uy = y / r, uz = z / r;
                     FT ax = FT(0), ay = FT(0), az = FT(0);
                     for (int k = 0; k < P.nRad; ++k) {
+                        if (Q.blk) {  // block maps: one switch on the radial's l
+                            const int l = Q.lk[k];
+                            FT gk = FT(0);
+                            if (l >= 0 && valid) {
+                                FT Rk, dRk;
+                                radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
+                                const int o0 = Q.ob[k];
+                                switch (l) {
+                                    case 0:
+                                        gk = pb_block<FT, 0, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
+                                        break;
+                                    case 1:
+                                        gk = pb_block<FT, 1, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
+                                        break;
+                                    case 2:
+                                        gk = pb_block<FT, 2, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
+                                        break;
+                                    default:
+                                        gk = pb_block<FT, 3, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
+                                        break;
+                                }
+                            }
+                            gg[k * 32 + lane] = gk;
+                            continue;
+                        }
                         FT Rk, dRk;
                         radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
                         FT gk = FT(0);
@@ -993,7 +1099,7 @@ static int launch_eval_reg_L(aok_orbitals* o, const EvalParams& P, bool grad, cu
     }
     const bool blk = block_maps(o, Q.lk, Q.ob);
     const size_t fsz = sizeof(FT);
-    const size_t smem = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    const size_t smem = (4 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
     if (smem > 227 * 1024) return -1;
     void* k = blk ? (grad ? (void*)k_evaluate_reg<FT, L, true, true> : (void*)k_evaluate_reg<FT, L, false, true>)
                   : (grad ? (void*)k_evaluate_reg<FT, L, true> : (void*)k_evaluate_reg<FT, L, false>);
@@ -1080,6 +1186,7 @@ static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
             if (o->poly[k] > 127) ok = false;
             else Q.poly[k] = (int8_t)o->poly[k];
         }
+        Q.blk = ok && block_maps(o, Q.lk, Q.ob) ? 1 : 0;
         const size_t wbytes = (epb_warp_words_reg((int)o->nRad) + accw) * fsz;
         if (ok && tab + wbytes <= 227 * 1024)
             return launch_epb_kernel(o, (const void*)k_evaluate_pbs<FT, L, false, true>, Q, tab, wbytes, s,
