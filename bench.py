@@ -384,7 +384,9 @@ def main():
     if args.profile and args.workload == "grad":
         gd = _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch)
         for _ in range(args.warmup + args.steps):
-            gd["gstep"]()
+            torch.cuda.nvtx.range_push("gradstep")  # ncu --nvtx --nvtx-include "gradstep/" selects the step's launches
+            gd["gstep_res"]()
+            torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         return 0
     if args.profile:
