@@ -669,10 +669,15 @@ __device__ __forceinline__ FT pb_block(FT Rk, FT dRk, FT ux, FT uy, FT uz, const
 }
 
 // per-warp shared-memory scratch of the slot-parallel pullback (floats of FT):
-// R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][32], f [32]
-__host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) { return (size_t)(3 * nRad + 4 * nY + 1) * 32; }
-// the register path keeps only gg [nRad][32] and f [32]
-__host__ __device__ constexpr size_t epb_warp_words_reg(int nRad) { return (size_t)(nRad + 1) * 32; }
+// R, dR [nRad][32], Z [nY][32], G [3 nY][32], gg [nRad][kGgRow], f [32].  The
+// radial cotangents' rows are padded to 33 words: in the slot phase the lanes read
+// column t of different rows k, which a 32-word row would put in one bank.
+constexpr int kGgRow = 33;
+__host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) {
+    return (size_t)(2 * nRad + 4 * nY + 1) * 32 + (size_t)nRad * kGgRow;
+}
+// the register path keeps only gg [nRad][kGgRow] and f [32]
+__host__ __device__ constexpr size_t epb_warp_words_reg(int nRad) { return (size_t)nRad * kGgRow + 32; }
 // then the unit's accumulators [2][NZ][nRad*K]
 __host__ __device__ constexpr size_t epb_acc_words(int nRad, int K, int NZ) { return (size_t)2 * NZ * nRad * K; }
 
@@ -695,7 +700,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
     int* sn = reinterpret_cast<int*>(sl + ntab);
     FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) + (size_t)warp * Q.wwords;
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
-       *gg = REG ? wbase : G + 96 * nY, *fv = gg + 32 * P.nRad, *acc = fv + 32;
+       *gg = REG ? wbase : G + 96 * nY, *fv = gg + kGgRow * P.nRad, *acc = fv + 32;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         sz[i] = ((const FT*)P.zeta)[i];
         sD[i] = ((const FT*)P.D)[i];
@@ -732,7 +737,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                 FT r;
                 if constexpr (RAD) {
                     r = valid ? Xin[j] : FT(0);
-                    for (int k = 0; k < P.nRad; ++k) gg[k * 32 + lane] = valid ? dPin[j + P.nX * k] : FT(0);
+                    for (int k = 0; k < P.nRad; ++k) gg[k * kGgRow + lane] = valid ? dPin[j + P.nX * k] : FT(0);
                 } else if constexpr (REG) {
                     FT x = FT(0), y = FT(0), z = FT(1);
                     if (valid) {
@@ -777,7 +782,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                                         break;
                                 }
                             }
-                            gg[k * 32 + lane] = gk;
+                            gg[k * kGgRow + lane] = gk;
                             continue;
                         }
                         FT Rk, dRk;
@@ -795,7 +800,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                                 gk += g * Zr[yi];
                             }
                         }
-                        gg[k * 32 + lane] = gk;
+                        gg[k * kGgRow + lane] = gk;
                     }
                     if (valid && P.dX) {
                         FT* dX = (FT*)P.dX;
@@ -821,7 +826,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                         radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
                         R[k * 32 + lane] = Rk;
                         dR[k * 32 + lane] = dRk;
-                        gg[k * 32 + lane] = FT(0);
+                        gg[k * kGgRow + lane] = FT(0);
                     }
                     solid_harmonics<FT, L>(x, y, z, P.F, Z + lane, G + lane, 32);
                     const FT ux = x / r, uy = y / r, uz = z / r;
@@ -834,7 +839,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                             ax += g * ((dr * ux) * yl + rn * G[(3 * yi + 0) * 32 + lane]);
                             ay += g * ((dr * uy) * yl + rn * G[(3 * yi + 1) * 32 + lane]);
                             az += g * ((dr * uz) * yl + rn * G[(3 * yi + 2) * 32 + lane]);
-                            gg[k * 32 + lane] += g * yl;
+                            gg[k * kGgRow + lane] += g * yl;
                         }
                         if (P.dX) {
                             FT* dX = (FT*)P.dX;
@@ -847,7 +852,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                 for (int k = 0; k < P.nRad; ++k) {
                     FT rp = FT(1);
                     for (int i = 0; i < P.poly[k]; ++i) rp *= r;
-                    gg[k * 32 + lane] *= rp;  // zero for the lanes that add nothing
+                    gg[k * kGgRow + lane] *= rp;  // zero for the lanes that add nothing
                 }
                 fv[lane] = P.slater ? r : r * r;
             }
@@ -869,7 +874,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                         while (m) {
                             const int t = __ffs(m) - 1;
                             m &= m - 1u;
-                            const FT f = fv[t], w = gg[k * 32 + t];
+                            const FT f = fv[t], w = gg[k * kGgRow + t];
                             const FT ex = exp_neg(zk, zl, f) * w;
                             aD += ex;
                             aZ = fma(ex, f, aZ);
