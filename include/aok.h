@@ -354,9 +354,9 @@ int aok_radials_evaluate(aok_radials* rad, void* R, void* dR, const void* r, con
  * Parameter pullback of the radial layer: dzeta, dD (nRad,K,NZ) from the
  * cotangent dRin (nX,nRad) of R.  Replaces pullback_ps(dR, basis::GSRadials, r,
  * sidx, ps, st) (src/orbitals/gtostoradials.jl:232-267, _gtostoradials_pb_ka!):
- * the points are binned by species and reduced per (radial, primitive) slot with
- * per-unit FP64 partial rows summed in a fixed order (deterministic, no atomics
- * on data).
+ * units of consecutive points are reduced per species and (radial, primitive)
+ * slot into per-unit FP64 partial rows summed in a fixed order (deterministic,
+ * no atomics on data).
  */
 int aok_radials_pullback(aok_radials* rad, void* dzeta, void* dD, const void* dRin, const void* r,
                          const int64_t* sidx, const void* zeta, const void* D, int64_t nX, void* stream);
