@@ -180,7 +180,7 @@ __device__ __forceinline__ int radial_count(const FT* D, int k, int sg, int nRad
 template <typename FT>
 struct SepTab {
     const FT *z, *D, *l;
-    __device__ __forceinline__ void get(int o, FT& zo, FT& Do, FT& lo) const {
+    __device__ __forceinline__ void get(int o, int, FT& zo, FT& Do, FT& lo) const {
         zo = z[o];
         Do = D[o];
         lo = l[o];
@@ -192,11 +192,13 @@ struct __align__(16) Pk64 {
 template <typename FT> struct PkEntry;
 template <> struct PkEntry<float> { using type = float4; };
 template <> struct PkEntry<double> { using type = Pk64; };
+// Packed entries: species sg's block of nRad*K slots starts at sg (nRad*K + 1), one
+// spare entry per species, so lanes of different species read different banks.
 template <typename FT>
 struct PkTab {
     const typename PkEntry<FT>::type* p;
-    __device__ __forceinline__ void get(int o, FT& zo, FT& Do, FT& lo) const {
-        const auto t = p[o];
+    __device__ __forceinline__ void get(int o, int sg, FT& zo, FT& Do, FT& lo) const {
+        const auto t = p[o + sg];
         if constexpr (sizeof(FT) == 4) {
             zo = t.x;
             Do = t.y;
@@ -232,7 +234,7 @@ __device__ __forceinline__ void radial_t(const Tab& tb, const int* sn, int k, in
     for (int m = 0; m < mk; ++m) {
         const int o = k + nRad * (m + K * sg);
         FT z, D, zl;
-        tb.get(o, z, D, zl);
+        tb.get(o, sg, z, D, zl);
         const FT a = mul_rn(D, exp_neg(z, zl, f));
         if constexpr (sizeof(FT) == 4) {
             const float t = s + a, bb = t - s;
@@ -416,10 +418,11 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_reg(const __grid_cons
     constexpr int nY = (L + 1) * (L + 1);
     const int ntab = P.nRad * P.K * P.NZ;
     auto* pk = reinterpret_cast<typename PkEntry<FT>::type*>(smem_raw);  // (zeta, D, zeta log2 e) per slot
-    int* sn = reinterpret_cast<int*>(pk + ntab);
+    int* sn = reinterpret_cast<int*>(pk + ntab + P.NZ);
+    const int nsl = P.nRad * P.K;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         const FT z = ((const FT*)P.zeta)[i];
-        pk[i] = pk_entry<FT>(z, ((const FT*)P.D)[i], (FT)((double)z * 1.4426950408889634074));
+        pk[i + i / nsl] = pk_entry<FT>(z, ((const FT*)P.D)[i], (FT)((double)z * 1.4426950408889634074));
     }
     for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
         sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
@@ -897,23 +900,36 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
     }
 }
 
-// dD, dzeta of slot (k, m, sigma): one warp per output value; lanes take the
-// unit rows in a fixed strided order and a fixed butterfly adds the lanes, so
-// the result is reproducible.
+// dD, dzeta of slot (k, m, sigma): one block of kEpbRedThreads per output value.
+// Thread t adds the unit rows t, t + kEpbRedThreads, ... (four loads in flight);
+// the threads' sums are added by a fixed tree, so the result is reproducible.
+constexpr int kEpbRedThreads = 256;
 template <typename FT>
-__global__ void k_epb_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const double* __restrict__ partial,
-                             int nout, int nunits, int ucap) {
-    const int lane = threadIdx.x & 31;
-    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= 2 * nout) return;
-    double sum = 0.0;
+__global__ void __launch_bounds__(kEpbRedThreads) k_epb_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta,
+                                                               const double* __restrict__ partial, int nout,
+                                                               int nunits, int ucap) {
+    __shared__ double ws[kEpbRedThreads / 32];
+    const int t = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double* row = partial + (size_t)t * ucap;
-    for (int v = lane; v < nunits; v += 32) sum += row[v];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int v = threadIdx.x;
+    for (; v + 3 * kEpbRedThreads < nunits; v += 4 * kEpbRedThreads) {
+        s0 += row[v];
+        s1 += row[v + kEpbRedThreads];
+        s2 += row[v + 2 * kEpbRedThreads];
+        s3 += row[v + 3 * kEpbRedThreads];
+    }
+    for (; v < nunits; v += kEpbRedThreads) s0 += row[v];
+    double sum = (s0 + s1) + (s2 + s3);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-    if (lane == 0) {
-        if (t < nout) dD[t] = (FT)sum;
-        else dzeta[t - nout] = (FT)sum;
+    if (lane == 0) ws[warp] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < kEpbRedThreads / 32; ++w) tot += ws[w];
+        if (t < nout) dD[t] = (FT)tot;
+        else dzeta[t - nout] = (FT)tot;
     }
 }
 
@@ -921,11 +937,12 @@ __global__ void k_epb_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta, const 
 static int launch_epb_reduce(aok_orbitals* o, void* dD, void* dzeta, const EpbParams& Q, int64_t nX,
                              cudaStream_t s) {
     const int nout = (int)(o->nRad * o->K * o->NZ), nunits = (int)((nX + kEpbUnit - 1) / kEpbUnit);
-    const int rb = (2 * nout * 32 + 255) / 256;
     if (o->prec == AOK_PREC_F64)
-        k_epb_reduce<double><<<rb, 256, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, nout, nunits, Q.ucap);
+        k_epb_reduce<double><<<2 * nout, kEpbRedThreads, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, nout,
+                                                                  nunits, Q.ucap);
     else
-        k_epb_reduce<float><<<rb, 256, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, nout, nunits, Q.ucap);
+        k_epb_reduce<float><<<2 * nout, kEpbRedThreads, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, nout, nunits,
+                                                                 Q.ucap);
     return cuda_status(cudaGetLastError(), "k_epb_reduce");
 }
 
@@ -1104,7 +1121,8 @@ static int launch_eval_reg_L(aok_orbitals* o, const EvalParams& P, bool grad, cu
     }
     const bool blk = block_maps(o, Q.lk, Q.ob);
     const size_t fsz = sizeof(FT);
-    const size_t smem = (4 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    const size_t smem =
+        (4 * (size_t)(o->nRad * o->K * o->NZ + o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
     if (smem > 227 * 1024) return -1;
     void* k = blk ? (grad ? (void*)k_evaluate_reg<FT, L, true, true> : (void*)k_evaluate_reg<FT, L, false, true>)
                   : (grad ? (void*)k_evaluate_reg<FT, L, true> : (void*)k_evaluate_reg<FT, L, false>);
@@ -1296,9 +1314,10 @@ int launch_radials_pb(aok_orbitals* o, void* dzeta, void* dD, const void* dRin, 
     Q.ucap = (int)o->epb_ucap;
     const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
     const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
-    const size_t wbytes = (epb_warp_words((int)o->nRad, 1) + epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ)) * fsz;
-    const void* k =
-        o->prec == AOK_PREC_F64 ? (const void*)k_evaluate_pbs<double, 0, true> : (const void*)k_evaluate_pbs<float, 0, true>;
+    const size_t wbytes =
+        (epb_warp_words((int)o->nRad, 1) + epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ)) * fsz;
+    const void* k = o->prec == AOK_PREC_F64 ? (const void*)k_evaluate_pbs<double, 0, true>
+                                            : (const void*)k_evaluate_pbs<float, 0, true>;
     AOK_TRY_PB(launch_epb_kernel(o, k, Q, tab, wbytes, s, "k_evaluate_pbs (radial)"));
     return launch_epb_reduce(o, dD, dzeta, Q, nX, s);
 }
