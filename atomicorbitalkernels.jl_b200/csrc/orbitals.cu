@@ -681,6 +681,11 @@ __host__ __device__ constexpr size_t epb_warp_words(int nRad, int nY) {
 }
 // the register path keeps only gg [nRad][kGgRow] and f [32]
 __host__ __device__ constexpr size_t epb_warp_words_reg(int nRad) { return (size_t)nRad * kGgRow + 32; }
+// Integer words after the (zeta, D, zeta log2 e) tables, in FT words: the primitive
+// counts [nRad NZ], each species' representative slots [NZ][nRad K] and their counts [NZ].
+__host__ __device__ constexpr int epb_int_words(int nRad, int K, int NZ, int fsz) {
+    return (int)(((size_t)nRad * NZ + (size_t)NZ * nRad * K + NZ) * 4 + fsz - 1) / fsz;
+}
 // then the unit's accumulators [2][NZ][nRad*K]
 __host__ __device__ constexpr size_t epb_acc_words(int nRad, int K, int NZ) { return (size_t)2 * NZ * nRad * K; }
 
@@ -701,7 +706,9 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
     FT* sD = sz + ntab;
     FT* sl = sD + ntab;  // zeta log2(e)
     int* sn = reinterpret_cast<int*>(sl + ntab);
-    FT* wbase = sl + ntab + count_words(P.nRad, P.NZ, (int)sizeof(FT)) + (size_t)warp * Q.wwords;
+    int* srep = sn + P.nRad * P.NZ;  // [NZ][nslot]: each species' representative slots, in slot order
+    int* snrep = srep + NZ * nslot;  // [NZ]: their number
+    FT* wbase = sl + ntab + epb_int_words(P.nRad, P.K, P.NZ, (int)sizeof(FT)) + (size_t)warp * Q.wwords;
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
        *gg = REG ? wbase : G + 96 * nY, *fv = gg + kGgRow * P.nRad, *acc = fv + 32;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
@@ -711,6 +718,28 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
     }
     for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
         sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
+    __syncthreads();
+    // A slot whose exponent equals that of an earlier slot of the same radial and species
+    // (the padding of shorter contractions repeats one exponent) has the same sums
+    // sum gg e^{-zeta f} and sum gg e^{-zeta f} f: only the first such slot, its
+    // representative, is evaluated, and k_epb_reduce gives the others its sums.
+    for (int sg = warp; sg < NZ; sg += nw) {
+        int c = 0;
+        for (int s0 = 0; s0 < nslot; s0 += 32) {
+            const int s = s0 + lane;
+            bool rep = false;
+            if (s < nslot) {
+                const int k = s % P.nRad, m = s / P.nRad;
+                const FT z = sz[s + nslot * sg];
+                rep = true;
+                for (int m2 = 0; m2 < m && rep; ++m2) rep = sz[k + P.nRad * (m2 + P.K * sg)] != z;
+            }
+            const unsigned b = __ballot_sync(0xffffffffu, rep);
+            if (rep) srep[sg * nslot + c + __popc(b & ((1u << lane) - 1u))] = s;
+            c += __popc(b);
+        }
+        if (lane == 0) snrep[sg] = c;
+    }
     __syncthreads();
     const long long nunits = (P.nX + kEpbUnit - 1) / kEpbUnit;
     const FT* dPin = (const FT*)P.dPin;
@@ -860,14 +889,17 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                 fv[lane] = P.slater ? r : r * r;
             }
             __syncwarp();
-            // phase B: per species present, lane = slot (k, m) of sigma, the points in order
+            // phase B: per species present, lane = representative slot (k, m) of sigma,
+            // the points in order
             for (int sigma = 0; sigma < NZ; ++sigma) {
                 const unsigned msk = __ballot_sync(0xffffffffu, sg == sigma);
                 if (msk == 0u) continue;
+                const int nr = snrep[sigma];
 #pragma unroll
                 for (int g = 0; g < kEpbMaxGroups; ++g) {
-                    const int s = g * 32 + lane;
-                    if (g * 32 < nslot && s < nslot) {
+                    const int rr = g * 32 + lane;
+                    if (g * 32 < nr && rr < nr) {
+                        const int s = srep[sigma * nslot + rr];
                         const int k = s % P.nRad;
                         const FT zk = sz[s + nslot * sigma], zl = sl[s + nslot * sigma];
                         FT* aDp = acc + sigma * nslot + s;
@@ -889,12 +921,11 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
             }
             __syncwarp();
         }
-        // the unit's partial rows: dD, then dzeta = -D * sum(ex f)
+        // the unit's partial rows: sum gg e^{-zeta f} (dD), then sum gg e^{-zeta f} f
+        // (dzeta = -D times its total); zero for the slots that are not representatives
         for (int i = lane; i < NZ * nslot; i += 32) {
-            const int sigma = i / nslot, s = i - sigma * nslot;
             Q.partial[(size_t)i * Q.ucap + u] = (double)acc[i];
-            Q.partial[(size_t)(NZ * nslot + i) * Q.ucap + u] =
-                -(double)sD[s + nslot * sigma] * (double)acc[NZ * nslot + i];
+            Q.partial[(size_t)(NZ * nslot + i) * Q.ucap + u] = (double)acc[NZ * nslot + i];
         }
         __syncwarp();
     }
@@ -906,11 +937,21 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
 constexpr int kEpbRedThreads = 256;
 template <typename FT>
 __global__ void __launch_bounds__(kEpbRedThreads) k_epb_reduce(FT* __restrict__ dD, FT* __restrict__ dzeta,
-                                                               const double* __restrict__ partial, int nout,
-                                                               int nunits, int ucap) {
+                                                               const double* __restrict__ partial,
+                                                               const FT* __restrict__ zeta, const FT* __restrict__ D,
+                                                               int nRad, int K, int nout, int nunits, int ucap) {
     __shared__ double ws[kEpbRedThreads / 32];
     const int t = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const double* row = partial + (size_t)t * ucap;
+    const int kind = t / nout, o = t - kind * nout;  // o = slot + nRad K species
+    // the representative of slot o: the first slot of its radial and species with its exponent
+    const int k = o % nRad, m = (o / nRad) % K, base = o - k - nRad * m;
+    int orep = o;
+    for (int m2 = 0; m2 < m; ++m2)
+        if (zeta[base + k + nRad * m2] == zeta[o]) {
+            orep = base + k + nRad * m2;
+            break;
+        }
+    const double* row = partial + ((size_t)kind * nout + orep) * ucap;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     int v = threadIdx.x;
     for (; v + 3 * kEpbRedThreads < nunits; v += 4 * kEpbRedThreads) {
@@ -928,8 +969,8 @@ __global__ void __launch_bounds__(kEpbRedThreads) k_epb_reduce(FT* __restrict__ 
     if (threadIdx.x == 0) {
         double tot = 0.0;
         for (int w = 0; w < kEpbRedThreads / 32; ++w) tot += ws[w];
-        if (t < nout) dD[t] = (FT)tot;
-        else dzeta[t - nout] = (FT)tot;
+        if (kind == 0) dD[o] = (FT)tot;
+        else dzeta[o] = (FT)(-(double)D[o] * tot);
     }
 }
 
@@ -937,12 +978,15 @@ __global__ void __launch_bounds__(kEpbRedThreads) k_epb_reduce(FT* __restrict__ 
 static int launch_epb_reduce(aok_orbitals* o, void* dD, void* dzeta, const EpbParams& Q, int64_t nX,
                              cudaStream_t s) {
     const int nout = (int)(o->nRad * o->K * o->NZ), nunits = (int)((nX + kEpbUnit - 1) / kEpbUnit);
+    const int nRad = (int)o->nRad, K = (int)o->K;
     if (o->prec == AOK_PREC_F64)
-        k_epb_reduce<double><<<2 * nout, kEpbRedThreads, 0, s>>>((double*)dD, (double*)dzeta, Q.partial, nout,
-                                                                  nunits, Q.ucap);
+        k_epb_reduce<double><<<2 * nout, kEpbRedThreads, 0, s>>>((double*)dD, (double*)dzeta, Q.partial,
+                                                                  (const double*)Q.E.zeta, (const double*)Q.E.D,
+                                                                  nRad, K, nout, nunits, Q.ucap);
     else
-        k_epb_reduce<float><<<2 * nout, kEpbRedThreads, 0, s>>>((float*)dD, (float*)dzeta, Q.partial, nout, nunits,
-                                                                 Q.ucap);
+        k_epb_reduce<float><<<2 * nout, kEpbRedThreads, 0, s>>>((float*)dD, (float*)dzeta, Q.partial,
+                                                                 (const float*)Q.E.zeta, (const float*)Q.E.D, nRad,
+                                                                 K, nout, nunits, Q.ucap);
     return cuda_status(cudaGetLastError(), "k_epb_reduce");
 }
 
@@ -1194,7 +1238,8 @@ template <typename FT, int L>
 static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
     constexpr int nY = (L + 1) * (L + 1);
     const size_t fsz = sizeof(FT);
-    const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    const size_t tab =
+        (3 * (size_t)(o->nRad * o->K * o->NZ) + epb_int_words((int)o->nRad, (int)o->K, (int)o->NZ, (int)fsz)) * fsz;
     const size_t accw = epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ);
     if constexpr (L <= kRegMaxL) {
         // the register path when every (radial, harmonic) pair is used at most once
@@ -1313,7 +1358,8 @@ int launch_radials_pb(aok_orbitals* o, void* dzeta, void* dD, const void* dRin, 
     Q.partial = (double*)o->d_epb_partial;
     Q.ucap = (int)o->epb_ucap;
     const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
-    const size_t tab = (3 * (size_t)(o->nRad * o->K * o->NZ) + count_words((int)o->nRad, (int)o->NZ, (int)fsz)) * fsz;
+    const size_t tab =
+        (3 * (size_t)(o->nRad * o->K * o->NZ) + epb_int_words((int)o->nRad, (int)o->K, (int)o->NZ, (int)fsz)) * fsz;
     const size_t wbytes =
         (epb_warp_words((int)o->nRad, 1) + epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ)) * fsz;
     const void* k = o->prec == AOK_PREC_F64 ? (const void*)k_evaluate_pbs<double, 0, true>
