@@ -285,3 +285,32 @@ def test_evaluate_ed_permuted_maps(FT, tol):
     Pr, dPr = oracle.evaluate_ed(rnd(X), sidx, rnd(b.zeta), rnd(b.D), orb.Rnl.powers(), iR, iY, orb.L, nthreads=8)
     Pg, dPg = P.double().cpu().numpy(), dP.double().cpu().numpy()
     assert rel_fro(Pg, Pr) < tol and rel_fro(dPg, dPr) < tol
+
+
+@pytest.mark.parametrize("case", ["distinct_padding", "repeated_exponents"])
+def test_pullback_repeated_and_distinct_exponents(case):
+    """The pullback evaluates one representative per distinct exponent of a radial and
+    species and gives the other slots its sums.  Padding with distinct exponents (no
+    repeats), and two non-zero primitives of one radial sharing an exponent (repeats
+    with different D: dzeta = -D * the shared sum), both against the oracle."""
+    b, orb = _basis()
+    zeta, D = b.zeta.copy(), b.D.copy()
+    nRad, K, NZ = zeta.shape
+    if case == "distinct_padding":
+        for g in range(NZ):
+            for k in range(nRad):
+                for m in range(K):
+                    if D[k, m, g] == 0:
+                        zeta[k, m, g] = 0.3 + 0.07 * m + 0.011 * k + 0.005 * g
+    else:
+        zeta[0, 1, :] = zeta[0, 0, :]  # radial 0: primitives 0 and 1 share an exponent
+        zeta[3, 2, 1] = zeta[3, 0, 1]
+    X, sidx = W.config1_points(nX=2500, seed=47)
+    ps = {"Rnl": {"zeta": zeta, "D": D}, "Ylm": {}}
+    st = aok.initialstates(orb)
+    dPv = np.random.default_rng(48).standard_normal((2500, len(orb)))
+    g = aok.evaluate_pullback_ps(dPv, orb, aok.PStates(X, list(sidx)), ps, st)
+    rz, rD = oracle.evaluate_pb(dPv, X, sidx, zeta, D, orb.Rnl.powers(), orb.radidx, orb.ylmidx, orb.L,
+                                lengthscale=orb.lengthscale)
+    assert rel_fro(g["Rnl"]["zeta"].cpu().numpy(), rz) < 1e-12
+    assert rel_fro(g["Rnl"]["D"].cpu().numpy(), rD) < 1e-12
