@@ -702,19 +702,18 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
     const EvalParams& P = Q.E;
     const int ntab = P.nRad * P.K * P.NZ, nslot = P.nRad * P.K, NZ = P.NZ;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    FT* sz = reinterpret_cast<FT*>(smem_raw);
-    FT* sD = sz + ntab;
-    FT* sl = sD + ntab;  // zeta log2(e)
-    int* sn = reinterpret_cast<int*>(sl + ntab);
+    auto* pk = reinterpret_cast<typename PkEntry<FT>::type*>(smem_raw);  // (zeta, D, zeta log2 e), species-padded
+    const PkTab<FT> tb{pk};
+    int* sn = reinterpret_cast<int*>(pk + ntab + NZ);
     int* srep = sn + P.nRad * P.NZ;  // [NZ][nslot]: each species' representative slots, in slot order
     int* snrep = srep + NZ * nslot;  // [NZ]: their number
-    FT* wbase = sl + ntab + epb_int_words(P.nRad, P.K, P.NZ, (int)sizeof(FT)) + (size_t)warp * Q.wwords;
+    FT* wbase = reinterpret_cast<FT*>(pk + ntab + NZ) + epb_int_words(P.nRad, P.K, P.NZ, (int)sizeof(FT)) +
+                (size_t)warp * Q.wwords;
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
        *gg = REG ? wbase : G + 96 * nY, *fv = gg + kGgRow * P.nRad, *acc = fv + 32;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
-        sz[i] = ((const FT*)P.zeta)[i];
-        sD[i] = ((const FT*)P.D)[i];
-        sl[i] = (FT)((double)((const FT*)P.zeta)[i] * 1.4426950408889634074);
+        const FT z = ((const FT*)P.zeta)[i];
+        pk[i + i / nslot] = pk_entry<FT>(z, ((const FT*)P.D)[i], (FT)((double)z * 1.4426950408889634074));
     }
     for (int i = threadIdx.x; i < P.nRad * P.NZ; i += blockDim.x)
         sn[i] = radial_count((const FT*)P.D, i % P.nRad, i / P.nRad, P.nRad, P.K);
@@ -730,9 +729,14 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
             bool rep = false;
             if (s < nslot) {
                 const int k = s % P.nRad, m = s / P.nRad;
-                const FT z = sz[s + nslot * sg];
+                FT z, d, l;
+                tb.get(s + nslot * sg, sg, z, d, l);
                 rep = true;
-                for (int m2 = 0; m2 < m && rep; ++m2) rep = sz[k + P.nRad * (m2 + P.K * sg)] != z;
+                for (int m2 = 0; m2 < m && rep; ++m2) {
+                    FT z2;
+                    tb.get(k + P.nRad * (m2 + P.K * sg), sg, z2, d, l);
+                    rep = z2 != z;
+                }
             }
             const unsigned b = __ballot_sync(0xffffffffu, rep);
             if (rep) srep[sg * nslot + c + __popc(b & ((1u << lane) - 1u))] = s;
@@ -793,7 +797,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                             FT gk = FT(0);
                             if (l >= 0 && valid) {
                                 FT Rk, dRk;
-                                radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
+                                radial_t<FT>(tb, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
                                 const int o0 = Q.ob[k];
                                 switch (l) {
                                     case 0:
@@ -818,7 +822,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                             continue;
                         }
                         FT Rk, dRk;
-                        radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
+                        radial_t<FT>(tb, sn, k, sgr, P.nRad, P.K, Q.poly[k], P.slater, r, Rk, dRk);
                         FT gk = FT(0);
                         if (valid) {
 #pragma unroll
@@ -855,7 +859,7 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                     r = norm3(x, y, z);
                     for (int k = 0; k < P.nRad; ++k) {
                         FT Rk, dRk;
-                        radial<FT>(sz, sD, sl, sn, k, sgr, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
+                        radial_t<FT>(tb, sn, k, sgr, P.nRad, P.K, P.poly[k], P.slater, r, Rk, dRk);
                         R[k * 32 + lane] = Rk;
                         dR[k * 32 + lane] = dRk;
                         gg[k * kGgRow + lane] = FT(0);
@@ -901,7 +905,8 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                     if (g * 32 < nr && rr < nr) {
                         const int s = srep[sigma * nslot + rr];
                         const int k = s % P.nRad;
-                        const FT zk = sz[s + nslot * sigma], zl = sl[s + nslot * sigma];
+                        FT zk, dk, zl;
+                        tb.get(s + nslot * sigma, sigma, zk, dk, zl);
                         FT* aDp = acc + sigma * nslot + s;
                         FT* aZp = aDp + NZ * nslot;
                         FT aD = *aDp, aZ = *aZp;
@@ -1239,7 +1244,8 @@ static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
     constexpr int nY = (L + 1) * (L + 1);
     const size_t fsz = sizeof(FT);
     const size_t tab =
-        (3 * (size_t)(o->nRad * o->K * o->NZ) + epb_int_words((int)o->nRad, (int)o->K, (int)o->NZ, (int)fsz)) * fsz;
+        (4 * (size_t)(o->nRad * o->K * o->NZ + o->NZ) + epb_int_words((int)o->nRad, (int)o->K, (int)o->NZ, (int)fsz)) *
+        fsz;
     const size_t accw = epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ);
     if constexpr (L <= kRegMaxL) {
         // the register path when every (radial, harmonic) pair is used at most once
@@ -1359,7 +1365,8 @@ int launch_radials_pb(aok_orbitals* o, void* dzeta, void* dD, const void* dRin, 
     Q.ucap = (int)o->epb_ucap;
     const size_t fsz = o->prec == AOK_PREC_F64 ? 8 : 4;
     const size_t tab =
-        (3 * (size_t)(o->nRad * o->K * o->NZ) + epb_int_words((int)o->nRad, (int)o->K, (int)o->NZ, (int)fsz)) * fsz;
+        (4 * (size_t)(o->nRad * o->K * o->NZ + o->NZ) + epb_int_words((int)o->nRad, (int)o->K, (int)o->NZ, (int)fsz)) *
+        fsz;
     const size_t wbytes =
         (epb_warp_words((int)o->nRad, 1) + epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ)) * fsz;
     const void* k = o->prec == AOK_PREC_F64 ? (const void*)k_evaluate_pbs<double, 0, true>
