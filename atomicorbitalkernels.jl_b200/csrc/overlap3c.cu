@@ -32,21 +32,33 @@ __global__ void k_prim3c(FT* __restrict__ pz, FT* __restrict__ pc, int* __restri
     pn[t] = n;
 }
 
-// Per call, one CTA: the items sorted by estimated cost, heaviest first, so
-// that the kernel's unit queue (item-major) ends with cheap items.  Cost =
-// primitive triples (the largest count over the species per shell) x (E tables
-// + the chunk's products) + a fixed part per item; the f-shell classes
-// (run-time loops, FP64 tables) count four times.
-// Rank sort in shared memory; more than kOrder3Max items keep the static order.
+// Per call, one CTA: the item order of the kernel's unit queue.  Items that run
+// the same code (one shell-triple class and page chunk; all f-shell classes share
+// one routine) are kept together, so that the warps in flight at any time run
+// few distinct routines and the instruction cache holds them; the groups are
+// ordered by their heaviest item, heaviest first, and the items inside a group
+// heaviest first, so the queue ends with cheap work.  Cost = primitive triples
+// (the largest count over the species per shell) x (E tables + the chunk's
+// products) + a fixed part per item; the f-shell classes (run-time loops, FP64
+// tables) count four times.  Rank sort in shared memory; more than kOrder3Max
+// items keep the static order.
 constexpr int kOrder3Max = 2048;
+constexpr int kCodes3 = 27 * 8 + 1;  // (class, chunk) codes of the specialised classes, + one for the f shells
+
+__device__ __forceinline__ int code3(const Item3& it) {
+    return it.cls >= kClsF3 ? kCodes3 - 1 : it.cls * 8 + it.chunk;
+}
 
 __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, const Item3* __restrict__ items,
                                                  const int* __restrict__ pn, int n, int ns, int NZ) {
-    __shared__ unsigned long long key[kOrder3Max];
+    __shared__ unsigned long long ikey[kOrder3Max], gkey[kOrder3Max];
+    __shared__ int gmax[kCodes3];
     if (n > kOrder3Max) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = items[i];
         return;
     }
+    for (int c = threadIdx.x; c < kCodes3; c += blockDim.x) gmax[c] = 0;
+    __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const Item3 it = items[i];
         const bool f = it.cls >= kClsF3;
@@ -63,13 +75,23 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         }
         long long cost = (long long)na * nb * nc * per * (f ? 4 : 1) + 64;
         cost = min(cost, (long long)0x7FFFFFFF);
-        key[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | (unsigned)i;  // ascending key = descending cost
+        // ascending = heaviest first; equal costs by routine, then by position
+        ikey[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | ((unsigned)code3(it) << 12) | (unsigned)i;
+        atomicMax(&gmax[code3(it)], (int)cost);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const unsigned long long ki = key[i];
+        const int ci = code3(items[i]);
+        gkey[i] = ((unsigned long long)(0x7FFFFFFF - gmax[ci]) << 32) | (unsigned)ci;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned long long gi = gkey[i], ki = ikey[i];
         int r = 0;
-        for (int j = 0; j < n; ++j) r += key[j] < ki;
+        for (int j = 0; j < n; ++j) {
+            const unsigned long long gj = gkey[j];
+            r += gj < gi || (gj == gi && ikey[j] < ki);
+        }
         order[r] = items[i];
     }
 }
