@@ -626,9 +626,10 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
 //   dD[k,m,sigma]    += gg_k exp(-zeta f),
 //   dzeta[k,m,sigma] += -D gg_k exp(-zeta f) f        (gtostoradials.jl:232-253),
 // into the warp's per-unit accumulators (shared memory, one per (sigma, slot)),
-// with no cross-lane reduction.  Each unit writes its own FP64 partial rows;
-// k_epb_reduce adds the units in order, so the result is reproducible and does
-// not depend on how the points' species are mixed.  A point with a species
+// with no cross-lane reduction.  Each warp adds its units' sums into FP64
+// running sums, each block writes its warps' sums in warp order as one partial
+// row, and k_epb_reduce adds the rows in order, so the result is reproducible
+// and does not depend on how the points' species are mixed.  A point with a species
 // index outside 1..NZ gets dX = 0, is left out of every species, and sets the
 // error word.
 // ---------------------------------------------------------------------------
@@ -638,8 +639,9 @@ constexpr int kEpbMaxGroups = 4;  // slots per species <= 128
 struct EpbParams {
     EvalParams E;
     double* partial;    // [2][NZ][nRad*K][ucap]: dD, dzeta per (species, slot), units contiguous
-    int ucap;           // unit capacity (row length of partial)
+    int ucap;           // row length of partial (at least the grid)
     int wwords;         // per-warp shared-memory words (of FT): scratch + accumulators
+    int nrows;          // host side: the rows written (one per block of the launch)
     // register path (REG): (radial, harmonic) -> orbital table and radial powers
     int16_t otab[kRegMaxRad * (kRegMaxL + 1) * (kRegMaxL + 1)];
     int8_t poly[kRegMaxRad];
@@ -711,6 +713,12 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                 (size_t)warp * Q.wwords;
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
        *gg = REG ? wbase : G + 96 * nY, *fv = gg + kGgRow * P.nRad, *acc = fv + 32;
+    // each warp's FP64 running sums over its units, after all warps' scratch
+    const int nacc = 2 * NZ * nslot;
+    double* wacc_all = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(wbase - (size_t)warp * Q.wwords + (size_t)nw * Q.wwords) + 7) & ~(uintptr_t)7);
+    double* wacc = wacc_all + (size_t)warp * nacc;
+    for (int i = lane; i < nacc; i += 32) wacc[i] = 0.0;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) {
         const FT z = ((const FT*)P.zeta)[i];
         pk[i + i / nslot] = pk_entry<FT>(z, ((const FT*)P.D)[i], (FT)((double)z * 1.4426950408889634074));
@@ -926,13 +934,19 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
             }
             __syncwarp();
         }
-        // the unit's partial rows: sum gg e^{-zeta f} (dD), then sum gg e^{-zeta f} f
-        // (dzeta = -D times its total); zero for the slots that are not representatives
-        for (int i = lane; i < NZ * nslot; i += 32) {
-            Q.partial[(size_t)i * Q.ucap + u] = (double)acc[i];
-            Q.partial[(size_t)(NZ * nslot + i) * Q.ucap + u] = (double)acc[NZ * nslot + i];
-        }
+        // the unit's sums into the warp's FP64 running sums: sum gg e^{-zeta f} (dD), then
+        // sum gg e^{-zeta f} f (dzeta = -D times its total); zero for the slots that are
+        // not representatives
+        for (int i = lane; i < nacc; i += 32) wacc[i] += (double)acc[i];
         __syncwarp();
+    }
+    // the block's partial row: its warps' sums in warp order (the units of each warp
+    // are fixed by the launch shape, so the result is reproducible)
+    __syncthreads();
+    for (int i = threadIdx.x; i < nacc; i += blockDim.x) {
+        double sum = 0.0;
+        for (int w = 0; w < nw; ++w) sum += wacc_all[(size_t)w * nacc + i];
+        Q.partial[(size_t)i * Q.ucap + blockIdx.x] = sum;
     }
 }
 
@@ -979,10 +993,9 @@ __global__ void __launch_bounds__(kEpbRedThreads) k_epb_reduce(FT* __restrict__ 
     }
 }
 
-// the unit rows of one slot-parallel pullback call, summed (k_epb_reduce)
-static int launch_epb_reduce(aok_orbitals* o, void* dD, void* dzeta, const EpbParams& Q, int64_t nX,
-                             cudaStream_t s) {
-    const int nout = (int)(o->nRad * o->K * o->NZ), nunits = (int)((nX + kEpbUnit - 1) / kEpbUnit);
+// the partial rows of one slot-parallel pullback call, summed (k_epb_reduce)
+static int launch_epb_reduce(aok_orbitals* o, void* dD, void* dzeta, const EpbParams& Q, cudaStream_t s) {
+    const int nout = (int)(o->nRad * o->K * o->NZ), nunits = Q.nrows;
     const int nRad = (int)o->nRad, K = (int)o->K;
     if (o->prec == AOK_PREC_F64)
         k_epb_reduce<double><<<2 * nout, kEpbRedThreads, 0, s>>>((double*)dD, (double*)dzeta, Q.partial,
@@ -1225,9 +1238,11 @@ static int ensure_epb_buffers(aok_orbitals* o, int64_t nX) {
 // shared memory allows, and the resident blocks per SM from the occupancy query.
 static int launch_epb_kernel(aok_orbitals* o, const void* k, EpbParams& Q, size_t tab, size_t wbytes,
                              cudaStream_t s, const char* what) {
+    // per warp: the FT scratch and accumulators, then (after all warps' scratch) its FP64 sums
+    const size_t wd = sizeof(double) * epb_acc_words((int)o->nRad, (int)o->K, (int)o->NZ);
     int nw = 8;
-    while (nw > 1 && tab + nw * wbytes > 227 * 1024) --nw;
-    const size_t smem = tab + nw * wbytes;
+    while (nw > 1 && tab + nw * (wbytes + wd) + 8 > 227 * 1024) --nw;
+    const size_t smem = tab + nw * (wbytes + wd) + 8;
     if (smem > 227 * 1024) return set_error(AOK_ERR_UNSUPPORTED, std::string(what) + ": basis too large");
     int occ = 0;
     AOK_TRY_PB(kernel_prepare(k, smem, 32 * nw, &occ));
@@ -1235,6 +1250,7 @@ static int launch_epb_kernel(aok_orbitals* o, const void* k, EpbParams& Q, size_
     const int64_t units = (Q.E.nX + kEpbUnit - 1) / kEpbUnit;
     const int64_t want = (units + nw - 1) / nw;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)o->num_sms * std::max(occ, 1)));
+    Q.nrows = grid;
     void* args[] = {&Q};
     return cuda_status(cudaLaunchKernel(k, dim3(grid), dim3(32 * nw), args, smem, s), what);
 }
@@ -1301,7 +1317,7 @@ int launch_evaluate_pb(aok_orbitals* o, void* dX, void* dzeta, void* dD, const v
         const int st = o->prec == AOK_PREC_F64 ? launch_epb_T<double>(o, Q, s) : launch_epb_T<float>(o, Q, s);
         if (st != AOK_ERR_UNSUPPORTED) {
             AOK_TRY_PB(st);
-            return launch_epb_reduce(o, dD, dzeta, Q, nX, s);
+            return launch_epb_reduce(o, dD, dzeta, Q, s);
         }
         // a basis whose per-warp scratch does not fit: the per-block-rows kernel below
     }
@@ -1372,7 +1388,7 @@ int launch_radials_pb(aok_orbitals* o, void* dzeta, void* dD, const void* dRin, 
     const void* k = o->prec == AOK_PREC_F64 ? (const void*)k_evaluate_pbs<double, 0, true>
                                             : (const void*)k_evaluate_pbs<float, 0, true>;
     AOK_TRY_PB(launch_epb_kernel(o, k, Q, tab, wbytes, s, "k_evaluate_pbs (radial)"));
-    return launch_epb_reduce(o, dD, dzeta, Q, nX, s);
+    return launch_epb_reduce(o, dD, dzeta, Q, s);
 }
 
 }  // namespace aok
