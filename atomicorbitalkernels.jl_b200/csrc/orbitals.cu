@@ -651,30 +651,19 @@ struct EpbParams {
     int16_t ob[kRegMaxRad];
 };
 
-// Asynchronous 4- or 8-byte copies global -> shared (sm_80+ cp.async), used to
-// stage the next 32 points' dP rows while the current ones are processed.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gmem), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // Point phase of the register pullback under block maps: radial k's 2 LL + 1
 // orbitals o0 + m with harmonics LL^2 + m; adds their dX terms and returns the
-// radial cotangent sum_m dP[j, o0 + m] Z[LL^2 + m].  gsm: the lane's staged row
-// of dP (orbital o at gsm[32 o]).
+// radial cotangent sum_m dP[j, o0 + m] Z[LL^2 + m].
 template <typename FT, int LL, int L>
 __device__ __forceinline__ FT pb_block(FT Rk, FT dRk, FT ux, FT uy, FT uz, const FT (&Z)[(L + 1) * (L + 1)],
-                                       const FT (&G)[3 * (L + 1) * (L + 1)], const FT* gsm, int o0, FT& ax,
-                                       FT& ay, FT& az) {
+                                       const FT (&G)[3 * (L + 1) * (L + 1)], const FT* dPin, long long j,
+                                       long long nX, int o0, FT& ax, FT& ay, FT& az) {
     FT gk = FT(0);
     if constexpr (LL <= L) {
 #pragma unroll
         for (int m = 0; m <= 2 * LL; ++m) {
             const int yi = LL * LL + m;
-            const FT g = gsm[32 * (o0 + m)];
+            const FT g = dPin[j + nX * (o0 + m)];
             ax += g * ((dRk * ux) * Z[yi] + Rk * G[3 * yi + 0]);
             ay += g * ((dRk * uy) * Z[yi] + Rk * G[3 * yi + 1]);
             az += g * ((dRk * uz) * Z[yi] + Rk * G[3 * yi + 2]);
@@ -724,10 +713,6 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                 (size_t)warp * Q.wwords;
     FT *R = wbase, *dR = R + 32 * P.nRad, *Z = dR + 32 * P.nRad, *G = Z + 32 * nY,
        *gg = REG ? wbase : G + 96 * nY, *fv = gg + kGgRow * P.nRad, *acc = fv + 32;
-    // block-map register path: the next 32 points' dP rows are staged into
-    // pfb[2][nOrb][32] with cp.async while the current 32 points are processed
-    const bool pf = REG && Q.blk;
-    FT* pfb = acc + 2 * NZ * nslot;
     // each warp's FP64 running sums over its units, after all warps' scratch
     const int nacc = 2 * NZ * nslot;
     double* wacc_all = reinterpret_cast<double*>(
@@ -772,30 +757,10 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
     const FT* dPin = (const FT*)P.dPin;
     const FT* Xin = (const FT*)P.X;
     const FT sc = (FT)P.scale;
-    const long long ustride = (long long)gridDim.x * nw;
-    auto stage = [&](long long cs, int buf) {  // dP rows of points cs .. cs + 31 into buffer buf
-        const long long js = cs + lane;
-        if (js < P.nX) {
-            FT* d = pfb + (size_t)buf * P.nOrb * 32 + lane;
-            for (int o = 0; o < P.nOrb; ++o) cp_async<sizeof(FT)>(d + 32 * o, dPin + js + P.nX * o);
-        }
-        cp_async_commit();
-    };
-    int cur = 0;
-    if (pf && (long long)blockIdx.x * nw + warp < nunits) stage(((long long)blockIdx.x * nw + warp) * kEpbUnit, 0);
-    for (long long u = (long long)blockIdx.x * nw + warp; u < nunits; u += ustride) {
+    for (long long u = (long long)blockIdx.x * nw + warp; u < nunits; u += (long long)gridDim.x * nw) {
         for (int i = lane; i < 2 * NZ * nslot; i += 32) acc[i] = FT(0);
         const long long j0 = u * kEpbUnit, j1 = min(P.nX, j0 + kEpbUnit);
         for (long long c0 = j0; c0 < j1; c0 += 32) {
-            const FT* gsm = nullptr;  // this lane's staged dP row
-            if (pf) {
-                cp_async_wait_all();
-                // the warp's next 32 points: the rest of this unit, else its next unit's first
-                const long long nc = c0 + 32 < j1 ? c0 + 32 : (u + ustride < nunits ? (u + ustride) * kEpbUnit : -1);
-                if (nc >= 0) stage(nc, cur ^ 1);
-                gsm = pfb + (size_t)cur * P.nOrb * 32 + lane;
-                cur ^= 1;
-            }
             // phase A: lane = point
             const long long j = c0 + lane;
             int sg = -1;
@@ -844,16 +809,20 @@ __global__ void __launch_bounds__(256, 4) k_evaluate_pbs(const __grid_constant__
                                 const int o0 = Q.ob[k];
                                 switch (l) {
                                     case 0:
-                                        gk = pb_block<FT, 0, L>(Rk, dRk, ux, uy, uz, Zr, Gr, gsm, o0, ax, ay, az);
+                                        gk = pb_block<FT, 0, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
                                         break;
                                     case 1:
-                                        gk = pb_block<FT, 1, L>(Rk, dRk, ux, uy, uz, Zr, Gr, gsm, o0, ax, ay, az);
+                                        gk = pb_block<FT, 1, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
                                         break;
                                     case 2:
-                                        gk = pb_block<FT, 2, L>(Rk, dRk, ux, uy, uz, Zr, Gr, gsm, o0, ax, ay, az);
+                                        gk = pb_block<FT, 2, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
                                         break;
                                     default:
-                                        gk = pb_block<FT, 3, L>(Rk, dRk, ux, uy, uz, Zr, Gr, gsm, o0, ax, ay, az);
+                                        gk = pb_block<FT, 3, L>(Rk, dRk, ux, uy, uz, Zr, Gr, dPin, j, P.nX, o0, ax,
+                                                                  ay, az);
                                         break;
                                 }
                             }
@@ -1308,8 +1277,7 @@ static int launch_epb_L(aok_orbitals* o, EpbParams& Q, cudaStream_t s) {
             else Q.poly[k] = (int8_t)o->poly[k];
         }
         Q.blk = ok && block_maps(o, Q.lk, Q.ob) ? 1 : 0;
-        // block maps also stage two sets of 32 points' dP rows per warp
-        const size_t wbytes = (epb_warp_words_reg((int)o->nRad) + accw + (Q.blk ? 64 * (size_t)o->nOrb : 0)) * fsz;
+        const size_t wbytes = (epb_warp_words_reg((int)o->nRad) + accw) * fsz;
         if (ok && tab + wbytes <= 227 * 1024)
             return launch_epb_kernel(o, (const void*)k_evaluate_pbs<FT, L, false, true>, Q, tab, wbytes, s,
                                      "k_evaluate_pbs");
