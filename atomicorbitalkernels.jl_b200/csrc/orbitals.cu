@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
 // ---------------------------------------------------------------------------
 // Slot-parallel parameter pullback (used by aok_evaluate_pullback).
 //
-// A work unit is kEpbUnit = 64 consecutive points in the caller's order, dealt
+// A work unit is kEpbUnit = 32 consecutive points in the caller's order, dealt
 // statically to the warps; four blocks of 8 warps per SM (<= 64 registers).  For
 // each 32 points the warp first puts lane = point: radials (of the point's own species), harmonics, dX, and the radial
 // cotangents gg_k = r^p_k sum_{i: iR[i] = k} dP[j,i] Z_{iY[i]} and f(r) into
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(kEvalThreads) k_evaluate_pb(const __grid_const
 // index outside 1..NZ gets dX = 0, is left out of every species, and sets the
 // error word.
 // ---------------------------------------------------------------------------
-constexpr int kEpbUnit = 64;      // consecutive points per unit
+constexpr int kEpbUnit = 32;      // consecutive points per unit
 constexpr int kEpbMaxGroups = 4;  // slots per species <= 128
 
 struct EpbParams {
@@ -1221,9 +1221,10 @@ int launch_evaluate(aok_orbitals* o, void* Pv, void* dP, const void* X, const in
     return launch_eval_T<float>(o, P, dP != nullptr, false, s);
 }
 
-// unit rows of the slot-parallel pullback, grown to nX points
+// partial rows of the slot-parallel pullback: one per block of a launch, so at most
+// one per unit and at most 8 per SM (its blocks are at least 256 threads)
 static int ensure_epb_buffers(aok_orbitals* o, int64_t nX) {
-    const int64_t units = (nX + kEpbUnit - 1) / kEpbUnit;
+    const int64_t units = std::min<int64_t>((nX + kEpbUnit - 1) / kEpbUnit, (int64_t)o->num_sms * 8);
     if (units <= o->epb_ucap && o->d_epb_partial) return AOK_OK;
     if (o->d_epb_partial) cudaFree(o->d_epb_partial);
     o->d_epb_partial = nullptr;
@@ -1249,7 +1250,9 @@ static int launch_epb_kernel(aok_orbitals* o, const void* k, EpbParams& Q, size_
     Q.wwords = (int)(wbytes / (o->prec == AOK_PREC_F64 ? 8 : 4));
     const int64_t units = (Q.E.nX + kEpbUnit - 1) / kEpbUnit;
     const int64_t want = (units + nw - 1) / nw;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)o->num_sms * std::max(occ, 1)));
+    // one partial row per block: no more blocks than the rows allocated
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>(std::min<int64_t>(want, (int64_t)o->num_sms * std::max(occ, 1)), Q.ucap));
     Q.nrows = grid;
     void* args[] = {&Q};
     return cuda_status(cudaLaunchKernel(k, dim3(grid), dim3(32 * nw), args, smem, s), what);
