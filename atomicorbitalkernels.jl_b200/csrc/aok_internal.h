@@ -66,7 +66,8 @@ struct aok_plan {
     void* d_pp3 = nullptr;
     int* d_npp3 = nullptr;
     void* d_items3 = nullptr;
-    void* d_order3 = nullptr;        // per call: each panel's items, heaviest first (k_order3c)
+    void* d_order3 = nullptr;        // per call: the items in queue order (k_prep3c)
+    int* d_segs3 = nullptr;          // per call: segment starts in d_order3 (nitems3 + 1), then the count
     int nitems3 = 0;
     // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated
     // launch chain, the arguments it was captured with, a private capture stream
@@ -207,8 +208,9 @@ int kernel_prepare(const void* k, size_t smem, int threads, int* occ);
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);
-int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
-                     const void* posC, double lengthscale, cudaStream_t s);
+int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
+                     const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
+                     double lengthscale, cudaStream_t s);
 int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
                    cudaStream_t s);
 int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,

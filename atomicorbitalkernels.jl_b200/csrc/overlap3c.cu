@@ -14,47 +14,118 @@ namespace aok {
 // the padded (ns,K,NZ) tables, compacted in slot order into pz/pc at (g ns + s) K,
 // and their number pn[g ns + s].  One thread per (shell, species).
 template <typename FT>
-__global__ void k_prim3c(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn, const FT* __restrict__ zeta,
-                         const FT* __restrict__ coef, int ns, int K, int NZ) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ns * NZ) return;
-    const int sh = t % ns, g = t / ns;
-    int n = 0;
-    for (int k = 0; k < K; ++k) {
-        const size_t o = (size_t)sh + (size_t)ns * (k + (size_t)K * g);
-        const FT c = coef[o];
-        if (c != FT(0)) {
-            pz[(size_t)t * K + n] = zeta[o];
-            pc[(size_t)t * K + n] = c;
-            ++n;
+__device__ __forceinline__ void prim3c_padded(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn,
+                                              const FT* __restrict__ zeta, const FT* __restrict__ coef, int ns, int K,
+                                              int NZ) {
+    for (int t = threadIdx.x; t < ns * NZ; t += blockDim.x) {
+        const int sh = t % ns, g = t / ns;
+        int n = 0;
+        for (int k = 0; k < K; ++k) {
+            const size_t o = (size_t)sh + (size_t)ns * (k + (size_t)K * g);
+            const FT c = coef[o];
+            if (c != FT(0)) {
+                pz[(size_t)t * K + n] = zeta[o];
+                pc[(size_t)t * K + n] = c;
+                ++n;
+            }
         }
+        pn[t] = n;
     }
-    pn[t] = n;
 }
 
-// Per call, one CTA: the item order of the kernel's unit queue.  Items that run
-// the same code (one shell-triple class and page chunk; all f-shell classes share
-// one routine) are kept together, so that the warps in flight at any time run
-// few distinct routines and the instruction cache holds them; the groups are
-// ordered by their heaviest item, heaviest first, and the items inside a group
-// heaviest first, so the queue ends with cheap work.  Cost = primitive triples
-// (the largest count over the species per shell) x (E tables + the chunk's
-// products) + a fixed part per item; the f-shell classes (run-time loops, FP64
-// tables) count four times.  Rank sort in shared memory; more than kOrder3Max
-// items keep the static order.
+// The same lists from CompiledBasis-style flat tables (one species): shell s has
+// nprim[s] primitives at prim_offset[s] (0-based); counts outside 0..K are flagged
+// (AOK_ERR_INVALID in err) and read as 0.
+template <typename FT>
+__device__ __forceinline__ void prim3c_flat(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn,
+                                            const int64_t* __restrict__ nprim, const int64_t* __restrict__ off,
+                                            const FT* __restrict__ coef, const FT* __restrict__ alpha, int ns, int K,
+                                            int* __restrict__ err) {
+    for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+        int64_t m = nprim[t];
+        if (m < 0 || m > K) {
+            atomicCAS(err, 0, AOK_ERR_INVALID);
+            m = 0;
+        }
+        int n = 0;
+        for (int k = 0; k < (int)m; ++k) {
+            const FT c = coef[off[t] + k];
+            if (c != FT(0)) {
+                pz[(size_t)t * K + n] = alpha[off[t] + k];
+                pc[(size_t)t * K + n] = c;
+                ++n;
+            }
+        }
+        pn[t] = n;
+    }
+}
+
+// Per call, one CTA: the item order of the kernel's unit queue and its cut into
+// segments.  Items that run the same code (one shell-triple class and page
+// chunk; all f-shell classes share one routine) are kept together, so that the
+// warps in flight at any time run few distinct routines and the instruction
+// cache holds them; the groups are ordered by their heaviest item, heaviest
+// first, and the items inside a group heaviest first, so the queue ends with
+// cheap work.  Cost = primitive triples (the largest count over the species per
+// shell) x (the exponential + E tables + the chunk's products) + a fixed part per
+// item and per output; the f-shell classes (run-time loops, FP64 tables) count
+// four times.
+// Rank sort in shared memory.  The ordered list is then cut into segments of
+// about total / G cost, G = target_units / tiles (a warp takes a whole segment
+// of one tile per unit); an item that costs more than that is a segment alone.
+// More than kOrder3Max items keep the static order, one item per segment.
+// segs: the nseg + 1 segment bounds, then nseg at [n + 1] and H at [n + 2].
 constexpr int kOrder3Max = 2048;
+constexpr int kOrder3Threads = 256;
+constexpr int kOrder3Per = kOrder3Max / kOrder3Threads;
 constexpr int kCodes3 = 27 * 8 + 1;  // (class, chunk) codes of the specialised classes, + one for the f shells
 
 __device__ __forceinline__ int code3(const Item3& it) {
     return it.cls >= kClsF3 ? kCodes3 - 1 : it.cls * 8 + it.chunk;
 }
 
-__global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, const Item3* __restrict__ items,
-                                                 const int* __restrict__ pn, int n, int ns, int NZ) {
+// Inclusive scan of one value per thread over the kOrder3Threads threads.
+__device__ __forceinline__ long long block_scan3(long long v, long long* wtot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) wtot[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        long long t = lane < kOrder3Threads / 32 ? wtot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += u;
+        }
+        if (lane < kOrder3Threads / 32) wtot[lane] = t;
+    }
+    __syncthreads();
+    if (w > 0) v += wtot[w - 1];
+    __syncthreads();
+    return v;
+}
+
+__device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __restrict__ segs,
+                                             const Item3* __restrict__ items, const int* __restrict__ pn,
+                                             const int* __restrict__ ntiles, int n, int ns, int NZ, int target_units) {
     __shared__ unsigned long long ikey[kOrder3Max], gkey[kOrder3Max];
+    __shared__ int cst[kOrder3Max];
     __shared__ int gmax[kCodes3];
+    __shared__ long long wtot[kOrder3Threads / 32];
     if (n > kOrder3Max) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = items[i];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            order[i] = items[i];
+            segs[i] = i;
+        }
+        if (threadIdx.x == 0) {
+            segs[n] = n;
+            segs[n + 1] = n;
+            segs[n + 2] = 0;
+        }
         return;
     }
     for (int c = threadIdx.x; c < kCodes3; c += blockDim.x) gmax[c] = 0;
@@ -66,15 +137,16 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         const int la = f ? c >> 4 : c / 9, lb = f ? (c >> 2) & 3 : (c / 3) % 3, lc = f ? c & 3 : c % 3;
         const int ppc = pages_per_chunk3(la, lb);
         const int pages = min(ppc, ncart(lc) - it.chunk * ppc);
-        const long long per = 12LL * (la + 1) * (lb + 1) * (lc + 1) + 2LL * ncart(la) * ncart(lb) * pages;
+        const long long per = 40 + 12LL * (la + 1) * (lb + 1) * (lc + 1) + 2LL * ncart(la) * ncart(lb) * pages;
         int na = 0, nb = 0, nc = 0;  // primitive counts, the largest over the species
         for (int g = 0; g < NZ; ++g) {
             na = max(na, pn[g * ns + it.sa]);
             nb = max(nb, pn[g * ns + it.sb]);
             nc = max(nc, pn[g * ns + it.sc]);
         }
-        long long cost = (long long)na * nb * nc * per * (f ? 4 : 1) + 64;
+        long long cost = (long long)na * nb * nc * per * (f ? 4 : 1) + 100 + 8LL * ncart(la) * ncart(lb) * pages;
         cost = min(cost, (long long)0x7FFFFFFF);
+        cst[i] = (int)cost;
         // ascending = heaviest first; equal costs by routine, then by position
         ikey[i] = ((unsigned long long)(0x7FFFFFFF - cost) << 32) | ((unsigned)code3(it) << 12) | (unsigned)i;
         atomicMax(&gmax[code3(it)], (int)cost);
@@ -85,7 +157,12 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
         gkey[i] = ((unsigned long long)(0x7FFFFFFF - gmax[ci]) << 32) | (unsigned)ci;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int rank[kOrder3Per], rcost[kOrder3Per];
+#pragma unroll
+    for (int k = 0; k < kOrder3Per; ++k) {
+        const int i = threadIdx.x + k * kOrder3Threads;
+        rank[k] = -1;
+        if (i >= n) continue;
         const unsigned long long gi = gkey[i], ki = ikey[i];
         int r = 0;
         for (int j = 0; j < n; ++j) {
@@ -93,7 +170,89 @@ __global__ void __launch_bounds__(256) k_order3c(Item3* __restrict__ order, cons
             r += gj < gi || (gj == gi && ikey[j] < ki);
         }
         order[r] = items[i];
+        rank[k] = r;
+        rcost[k] = cst[i];
     }
+    __syncthreads();
+    // the costs in queue order (cst is free again)
+#pragma unroll
+    for (int k = 0; k < kOrder3Per; ++k)
+        if (rank[k] >= 0) cst[rank[k]] = rcost[k];
+    __syncthreads();
+    // exclusive cost prefix of this thread's kOrder3Per consecutive positions
+    const int r0 = threadIdx.x * kOrder3Per;
+    long long tsum = 0;
+#pragma unroll
+    for (int k = 0; k < kOrder3Per; ++k)
+        if (r0 + k < n) tsum += cst[r0 + k];
+    const long long incl = block_scan3(tsum, wtot);
+    __shared__ long long total_s;
+    if (threadIdx.x == kOrder3Threads - 1) total_s = incl;
+    __syncthreads();
+    const long long total = total_s;
+    const long long G = max(1LL, min((long long)n, (long long)target_units / max(*ntiles, 1)));
+    const long long C = max(1LL, (total + G - 1) / G);
+    // a segment starts at r when a multiple of C lies in (prefix(r - 1), prefix(r)], or next to an item of cost >= C
+    long long P = incl - tsum;
+    unsigned flags = 0u;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < kOrder3Per; ++k) {
+        const int r = r0 + k;
+        if (r >= n) break;
+        bool start = r == 0;
+        if (!start) {
+            const long long pc = cst[r - 1];
+            start = (P / C) != ((P - pc) / C) || pc >= C || cst[r] >= C;
+        }
+        if (start) {
+            flags |= 1u << k;
+            ++cnt;
+        }
+        P += cst[r];
+    }
+    const long long pos_incl = block_scan3(cnt, wtot);
+    int pos = (int)(pos_incl - cnt);
+#pragma unroll
+    for (int k = 0; k < kOrder3Per; ++k)
+        if (flags & (1u << k)) segs[pos++] = r0 + k;
+    if (threadIdx.x == kOrder3Threads - 1) {
+        segs[pos_incl] = n;
+        segs[n + 1] = (int)pos_incl;
+    }
+    // H: the leading items of cost >= 2C with blocks of <= kSplitM3 elements (each a
+    // segment alone), whose records the CTA's warps share for one tile per unit
+    if (threadIdx.x == 0) {
+        int h = 0;
+        while (h < n && cst[h] >= 2 * C) {
+            const Item3 it = order[h];
+            if (it.cls >= kClsF3) break;
+            const int la = it.cls / 9, lb = (it.cls / 3) % 3, lc = it.cls % 3;
+            if (ncart(la) * ncart(lb) * ncart(lc) > kSplitM3) break;
+            ++h;
+        }
+        segs[n + 2] = h;
+    }
+}
+
+// One CTA per call ahead of the kernel: the compact primitive lists (from the padded
+// tables, or from flat GaussianBasis-style tables when nprim is given), then the
+// queue order and its segments (order3c_body reads the lists back after a barrier).
+template <typename FT>
+__global__ void __launch_bounds__(kOrder3Threads) k_prep3c(FT* __restrict__ pz, FT* __restrict__ pc,
+                                                           int* __restrict__ pn, const FT* __restrict__ zeta,
+                                                           const FT* __restrict__ coef, const int64_t* __restrict__ nprim,
+                                                           const int64_t* __restrict__ off, int* __restrict__ err,
+                                                           Item3* __restrict__ order, int* __restrict__ segs,
+                                                           const Item3* __restrict__ items,
+                                                           const int* __restrict__ ntiles, int n, int ns, int K, int NZ,
+                                                           int target_units) {
+    if (nprim)
+        prim3c_flat<FT>(pz, pc, pn, nprim, off, coef, zeta, ns, K, err);
+    else
+        prim3c_padded<FT>(pz, pc, pn, zeta, coef, ns, K, NZ);
+    __syncthreads();
+    order3c_body(order, segs, items, pn, ntiles, n, ns, NZ, target_units);
 }
 
 int setup_overlap3c_schedule(aok_plan* p) {
@@ -128,6 +287,8 @@ int setup_overlap3c_schedule(aok_plan* p) {
         return cuda_status(e, "cudaMalloc(items3)");
     if ((e = cudaMalloc(&p->d_order3, sizeof(Item3) * items.size())) != cudaSuccess)
         return cuda_status(e, "cudaMalloc(order3)");
+    if ((e = cudaMalloc(&p->d_segs3, sizeof(int) * (items.size() + 3))) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(segs3)");
     if ((e = cudaMemcpy(p->d_items3, items.data(), sizeof(Item3) * items.size(), cudaMemcpyHostToDevice)) !=
         cudaSuccess)
         return cuda_status(e, "cudaMemcpy(items3)");
@@ -140,31 +301,37 @@ int setup_overlap3c_schedule(aok_plan* p) {
 }
 
 // The kernel's unit counter (32 bits, each warp claims one past the end) must not
-// wrap: at most nitems x (B / 32 + one partial tile per key) units.
+// wrap: at most nitems x (B / 32 + one partial tile per key) units (a segment holds
+// at least one item).
 static int check_units3(const aok_plan* p, int64_t B, const char* who) {
     if ((int64_t)p->nitems3 * ((B + 31) / 32 + bin_keys_max(p->NZ) + 1) >= ((int64_t)1 << 31))
         return set_error(AOK_ERR_LENGTH, std::string(who) + ": too many (shell triple, tile) units; split the batch");
     return AOK_OK;
 }
 
-// The 3C overlap after the schedule is set up: compact primitive lists of the
-// padded (zeta, coef) tables, per-call item order, then the kernel over the
-// plan's bins (binned by the caller).
-int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA, const void* posB,
-                     const void* posC, double lengthscale, cudaStream_t s) {
-    const int nsz = (int)(p->ns * p->NZ), th = 128, bl = (nsz + th - 1) / th;
+// The 3C overlap after the schedule is set up and the batch binned (by the caller):
+// one CTA builds the compact primitive lists (of the padded (zeta, coef) tables, or of
+// the flat tables when nprim is given, zeta = alpha) and the per-call item order and
+// segments, then the kernel runs over the plan's bins.
+int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
+                     const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
+                     double lengthscale, cudaStream_t s) {
     const size_t nt = (size_t)(p->ns * p->K * p->NZ);
+    // FP32: about eight (segment, tile) pairs per resident warp (three CTAs of four warps
+    // per SM); FP64: about one item per segment
+    const int target_units = p->prec == AOK_PREC_F64 ? (1 << 30) : p->num_sms * 3 * (kThreads3 / 32) * 8;
     if (p->prec == AOK_PREC_F64)
-        k_prim3c<double><<<bl, th, 0, s>>>((double*)p->d_pp3, (double*)p->d_pp3 + nt, p->d_npp3, (const double*)zeta,
-                                           (const double*)coef, (int)p->ns, (int)p->K, (int)p->NZ);
+        k_prep3c<double><<<1, kOrder3Threads, 0, s>>>(
+            (double*)p->d_pp3, (double*)p->d_pp3 + nt, p->d_npp3, (const double*)zeta, (const double*)coef, nprim,
+            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, p->d_ntiles,
+            p->nitems3, (int)p->ns, (int)p->K, (int)p->NZ, target_units);
     else
-        k_prim3c<float><<<bl, th, 0, s>>>((float*)p->d_pp3, (float*)p->d_pp3 + nt, p->d_npp3, (const float*)zeta,
-                                          (const float*)coef, (int)p->ns, (int)p->K, (int)p->NZ);
-    int st = cuda_status(cudaGetLastError(), "k_prim3c");
+        k_prep3c<float><<<1, kOrder3Threads, 0, s>>>(
+            (float*)p->d_pp3, (float*)p->d_pp3 + nt, p->d_npp3, (const float*)zeta, (const float*)coef, nprim,
+            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, p->d_ntiles,
+            p->nitems3, (int)p->ns, (int)p->K, (int)p->NZ, target_units);
+    const int st = cuda_status(cudaGetLastError(), "k_prep3c");
     if (st != AOK_OK) return st;
-    k_order3c<<<1, 256, 0, s>>>((Item3*)p->d_order3, (const Item3*)p->d_items3, p->d_npp3, p->nitems3, (int)p->ns,
-                                (int)p->NZ);
-    if ((st = cuda_status(cudaGetLastError(), "k_order3c")) != AOK_OK) return st;
     if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s);
     return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s);
 }
@@ -187,9 +354,8 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
         return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: null pointer");
     if ((st = check_units3(p, B, "aok_overlap3c_gb")) != AOK_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    if ((st = launch_gb_pad(p, nprim, prim_offset, coef, alpha, s)) != AOK_OK) return st;
     if ((st = launch_bin(p, nullptr, nullptr, B, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, p->d_gb_zeta, p->d_gb_coef, posA, posB, posC, 1.0, s);
+    return launch_overlap3c(p, out, alpha, coef, nprim, prim_offset, posA, posB, posC, 1.0, s);
 }
 
 extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
@@ -209,5 +375,5 @@ extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const voi
     ++p->gen;  // the plan's bins change
     const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
     if ((st = launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, zeta, coef, posA, posB, posC, lengthscale, s);
+    return launch_overlap3c(p, out, zeta, coef, nullptr, nullptr, posA, posB, posC, lengthscale, s);
 }

@@ -16,8 +16,9 @@
 // Execution: tiles of 32 batch elements (lane = element); shell-triple classes
 // (la, lb, lc <= 2) compile-time specialised (classes with an f shell:
 // run_item3_f, below).  Items are whole shell-triple blocks or chunks of whole
-// output pages; (item, tile) units are drained from one global queue, heaviest
-// items first (k_overlap3c below).
+// output pages; (segment, tile) units, a segment being a run of items of about
+// equal cost, are drained from one global queue, heaviest first (k_overlap3c
+// below).
 #pragma once
 
 #include <algorithm>
@@ -31,7 +32,12 @@ constexpr int kMaxL3 = 3;        // shells up to f
 constexpr int kMaxL3Spec = 2;    // compile-time specialised classes up to d
 constexpr int kClsF3 = 100;      // Item3 class code of a triple with an f shell: kClsF3 + la*16 + lb*4 + lc
 constexpr int kThreads3 = 128;
-constexpr int kAllPages3 = 1 << 20;  // page window [0, kAllPages3): every page of an item's chunk
+constexpr int kSplitM3 = 9;  // largest block that the CTA's warps may share (heavy items, l_a + l_b + l_c <= 2)
+// Claims per CTA (a segment for the CTA's W tiles, heavy items shared out over
+// its warps) in FP32; claims per warp of (item, tile) units in FP64, whose
+// longer and more variable exponentials balance better in small units (both
+// measured on config 4).
+template <typename FT> constexpr bool kCtaClaims3 = sizeof(FT) == 4;
 
 __host__ __device__ constexpr int pages_per_chunk3(int la, int lb) {
     return (ncart(la) * ncart(lb)) >= 36 ? 1 : 36 / (ncart(la) * ncart(lb));
@@ -40,13 +46,15 @@ __host__ __device__ constexpr int nchunks3(int la, int lb, int lc) {
     return (ncart(lc) + pages_per_chunk3(la, lb) - 1) / pages_per_chunk3(la, lb);
 }
 
-// Geometry-free primitive-triple record (FP64-computed).  FP32: exponent
-// coefficients k_xy = (x y / q) log2(e) as hi + lo; `grp` = ip*K + jp (the
-// partial sums are folded with TwoSum whenever it changes).
-struct PTf {
-    float w, kab_hi, kab_lo, kac_hi, kac_lo, kbc_hi, kbc_lo, ra, rb, rc, oo2q, grp, pad[4];
+// Geometry-free primitive-triple record (FP64-computed).  FP32: the exponent
+// coefficients k_xy = (x y / q) log2(e) stay FP64, so that the exponent
+// k_ab |AB|^2 + k_ac |AC|^2 + k_bc |BC|^2 is three FP64 FMAs split into hi + lo
+// floats for ex2; the rest is FP32.
+struct __align__(16) PTf {
+    double kab, kac, kbc;
+    float w, ra, rb, rc, oo2q, pad;
 };
-struct PTd {
+struct __align__(16) PTd {
     double w, kab, kac, kbc, ra, rb, rc, oo2q;
 };
 template <typename FT> struct PTT;
@@ -63,7 +71,7 @@ struct Item3 {
 template <typename FT> struct Geo3;
 template <> struct Geo3<float> {
     float AB[3], AC[3], BC[3];
-    float R2[3], R2lo[3];  // |AB|^2, |AC|^2, |BC|^2 as hi + lo
+    double R2[3];  // |AB|^2, |AC|^2, |BC|^2 of the FP32 positions, in FP64
 };
 template <> struct Geo3<double> {
     double AB[3], AC[3], BC[3];
@@ -93,10 +101,7 @@ __device__ __forceinline__ void load_geo3(Geo3<float>& g, const float* A, const 
         r[2] += bc * bc;
     }
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        g.R2[i] = (float)r[i];
-        g.R2lo[i] = (float)(r[i] - (double)g.R2[i]);
-    }
+    for (int i = 0; i < 3; ++i) g.R2[i] = r[i];
 }
 __device__ __forceinline__ void load_geo3(Geo3<double>& g, const double* A, const double* B, const double* C,
                                           double s, bool use_s) {
@@ -163,38 +168,33 @@ struct Class3 {
 };
 
 // Record of one primitive triple, FP64-computed (the product's weight, the
-// exponent coefficients, the exponent ratios and 1/2q); grp groups the triples
-// of one (ip, jp) for the FP32 path's compensated folding.
-__device__ __forceinline__ void fill_pt(PTf& r, double ca, double cb, double cc, double a, double b, double c, int grp) {
-    const double q = a + b + c, x = 3.14159265358979323846 / q, l2e = 1.4426950408889634074;
-    const double kab = a * b / q * l2e, kac = a * c / q * l2e, kbc = b * c / q * l2e;
+// exponent coefficients, the exponent ratios and 1/2q).
+__device__ __forceinline__ void fill_pt(PTf& r, double ca, double cb, double cc, double a, double b, double c) {
+    const double q = a + b + c, iq = 1.0 / q, x = 3.14159265358979323846 * iq, l2e = 1.4426950408889634074;
     r.w = (float)(ca * cb * cc * (x * sqrt(x)));
-    r.kab_hi = (float)kab;
-    r.kab_lo = (float)(kab - (double)r.kab_hi);
-    r.kac_hi = (float)kac;
-    r.kac_lo = (float)(kac - (double)r.kac_hi);
-    r.kbc_hi = (float)kbc;
-    r.kbc_lo = (float)(kbc - (double)r.kbc_hi);
-    r.ra = (float)(a / q);
-    r.rb = (float)(b / q);
-    r.rc = (float)(c / q);
-    r.oo2q = (float)(0.5 / q);
-    r.grp = (float)grp;
+    r.kab = a * b * iq * l2e;
+    r.kac = a * c * iq * l2e;
+    r.kbc = b * c * iq * l2e;
+    r.ra = (float)(a * iq);
+    r.rb = (float)(b * iq);
+    r.rc = (float)(c * iq);
+    r.oo2q = (float)(0.5 * iq);
+    r.pad = 0.f;
 }
-__device__ __forceinline__ void fill_pt(PTd& r, double ca, double cb, double cc, double a, double b, double c, int) {
-    const double q = a + b + c, x = 3.14159265358979323846 / q;
+__device__ __forceinline__ void fill_pt(PTd& r, double ca, double cb, double cc, double a, double b, double c) {
+    const double q = a + b + c, iq = 1.0 / q, x = 3.14159265358979323846 * iq;
     r.w = ca * cb * cc * (x * sqrt(x));
-    r.kab = a * b / q;
-    r.kac = a * c / q;
-    r.kbc = b * c / q;
-    r.ra = a / q;
-    r.rb = b / q;
-    r.rc = c / q;
-    r.oo2q = 0.5 / q;
+    r.kab = a * b * iq;
+    r.kac = a * c * iq;
+    r.kbc = b * c * iq;
+    r.ra = a * iq;
+    r.rb = b * iq;
+    r.rc = c * iq;
+    r.oo2q = 0.5 * iq;
 }
 
 // The three shells' primitives for one work unit (the tile's species): the
-// compact lists of non-zero (zeta, coef) slots (k_prim3c) and their lengths.
+// compact lists of non-zero (zeta, coef) slots (k_prep3c) and their lengths.
 template <typename FT>
 struct Prim3 {
     const FT* z[3];
@@ -211,102 +211,153 @@ __device__ __forceinline__ void gen_records3(PT* buf, const Prim3<FT>& pr, int q
     const int nb = pr.n[1], nc = pr.n[2];
     const int ip = q / (nb * nc), jp = (q / nc) % nb, kp = q % nc;
     fill_pt(buf[lane], (double)pr.c[0][ip], (double)pr.c[1][jp], (double)pr.c[2][kp], (double)pr.z[0][ip],
-            (double)pr.z[1][jp], (double)pr.z[2][kp], ip * nb + jp);
+            (double)pr.z[1][jp], (double)pr.z[2][kp]);
 }
 
-// lin (0-based, within the block) -> offset in the lane's panel slab;
+// One primitive triple's products E_x E_y E_z added into the sums of the
+// chunk's block elements [L0, L0 + M) (aliased lin order).
+template <int LA, int LB, int LC, int L0, int M, typename FT>
+__device__ __forceinline__ void add_products3(FT ra, FT rb, FT rc, FT o2q, FT e000, const Geo3<FT>& g,
+                                              FT (&part)[M]) {
+    using CI = Class3<LA, LB, LC>;
+    FT Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
+    build_E3<LA, LB, LC, FT>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
+                             ra * g.AC[0] + rb * g.BC[0], o2q, e000);
+    build_E3<LA, LB, LC, FT>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
+                             ra * g.AC[1] + rb * g.BC[1], o2q, FT(1));
+    build_E3<LA, LB, LC, FT>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
+                             ra * g.AC[2] + rb * g.BC[2], o2q, FT(1));
+#pragma unroll
+    for (int c3 = 0; c3 < CI::NC; ++c3)
+#pragma unroll
+        for (int c2 = 0; c2 < CI::NB; ++c2)
+#pragma unroll
+            for (int c1 = 0; c1 < CI::NA; ++c1) {
+                const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
+                if (lin >= L0 && lin < L0 + M) {
+                    const FT yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
+                                  Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
+                    part[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
+                }
+            }
+}
+
+// FP32: 2^-x with x = k_ab |AB|^2 + k_ac |AC|^2 + k_bc |BC|^2 (log2 units) in FP64,
+// split into hi + lo floats; FP64: exp(-x).
+template <int LA, int LB, int LC, int L0, int M>
+__device__ __forceinline__ void add_rec3(const PTf& r, const Geo3<float>& g, float (&part)[M]) {
+    const double x = fma(r.kbc, g.R2[2], fma(r.kac, g.R2[1], r.kab * g.R2[0]));
+    const float xh = __double2float_rn(x), xl = __double2float_rn(x - (double)xh);
+    const float e000 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * r.w;
+    add_products3<LA, LB, LC, L0, M, float>(r.ra, r.rb, r.rc, r.oo2q, e000, g, part);
+}
+template <int LA, int LB, int LC, int L0, int M>
+__device__ __forceinline__ void add_rec3(const PTd& r, const Geo3<double>& g, double (&part)[M]) {
+    const double e000 = exp(-(r.kab * g.R2[0] + r.kac * g.R2[1] + r.kbc * g.R2[2])) * r.w;
+    add_products3<LA, LB, LC, L0, M, double>(r.ra, r.rb, r.rc, r.oo2q, e000, g, part);
+}
+
+// Classes with l_a + l_b + l_c <= 2 take two triples per loop step (two
+// independent exponential chains in flight); larger classes one.
+template <int LA, int LB, int LC>
+__host__ __device__ constexpr bool pair_step3() {
+    return LA + LB + LC <= 2;
+}
+
+// lin (0-based, within the block) -> offset in the output;
 // block element (i, j, k) = (lin % NA, (lin / NA) % NB, lin / PS).
-// Only pages inside [kp0, kp1) (block-local) are stored.
+// With split, the CTA's warps share one tile: warp w takes the record chunks
+// w, w + W, ... and the partial sums meet in xbuf (blocks of <= kSplitM3).
 template <int LA, int LB, int LC, int C>
 __device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Geo3<float> g, float* dst, int N,
-                                       int kp0, int kp1, bool valid) {
+                                       bool split, void* xbuf, bool valid) {
     const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
-    float hi[M], part[M];
+    // Compensated contraction: runs of up to 8 triples are summed in part[], and
+    // each run is folded into hi + lo with TwoSum.
+    float hi[M], lo[M], part[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         hi[m] = 0.f;
+        lo[m] = 0.f;
         part[m] = 0.f;
     }
-    float lo[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) lo[m] = 0.f;
-    float prev = -1.f;
+    const int w = threadIdx.x >> 5, q00 = split ? 32 * w : 0, qs = split ? 32 * (kThreads3 / 32) : 32;
 #pragma unroll 1
-    for (int q0 = 0; q0 < n; q0 += 32) {
+    for (int q0 = q00; q0 < n; q0 += qs) {
       __syncwarp();
       gen_records3(buf, pr, q0, n, lane);
       __syncwarp();
       const int m = min(32, n - q0);
 #pragma unroll 1
-      for (int q = 0; q < m; ++q) {
-        const float4 r0 = reinterpret_cast<const float4*>(buf + q)[0];
-        const float4 r1 = reinterpret_cast<const float4*>(buf + q)[1];
-        const float4 r2 = reinterpret_cast<const float4*>(buf + q)[2];
-        const float w = r0.x;
-        if (r2.w != prev) {
+      for (int q8 = 0; q8 < m; q8 += 8) {
+        if (q0 + q8 > q00) {
 #pragma unroll
-            for (int m = 0; m < M; ++m) {
+            for (int k = 0; k < M; ++k) {
                 float s, e;
-                two_sum(hi[m], part[m], s, e);
-                hi[m] = s;
-                part[m] = 0.f;
-                lo[m] += e;
+                two_sum(hi[k], part[k], s, e);
+                hi[k] = s;
+                part[k] = 0.f;
+                lo[k] += e;
             }
-            prev = r2.w;
         }
-        // exponent x = (k_ab |AB|^2 + k_ac |AC|^2 + k_bc |BC|^2) log2(e), double-float
-        const float xa = r0.y * g.R2[0], xb = r0.w * g.R2[1], xc = r1.y * g.R2[2];
-        float s1, e1, xh, e2;
-        two_sum(xa, xb, s1, e1);
-        two_sum(s1, xc, xh, e2);
-        const float xl = (fmaf(r0.y, g.R2[0], -xa) + fmaf(r0.w, g.R2[1], -xb) + fmaf(r1.y, g.R2[2], -xc)) +
-                         ((r0.z * g.R2[0] + r0.y * g.R2lo[0]) + (r1.x * g.R2[1] + r0.w * g.R2lo[1]) +
-                          (r1.z * g.R2[2] + r1.y * g.R2lo[2])) +
-                         (e1 + e2);
-        const float e000 = (ex2_approx(-xh) * fmaf(-0.6931471805599453f, xl, 1.f)) * w;
-        const float ra = r1.w, rb = r2.x, rc = r2.y, o2q = r2.z;
-        float Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
-        build_E3<LA, LB, LC, float>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
-                                    ra * g.AC[0] + rb * g.BC[0], o2q, e000);
-        build_E3<LA, LB, LC, float>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
-                                    ra * g.AC[1] + rb * g.BC[1], o2q, 1.f);
-        build_E3<LA, LB, LC, float>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
-                                    ra * g.AC[2] + rb * g.BC[2], o2q, 1.f);
-#pragma unroll
-        for (int c3 = 0; c3 < CI::NC; ++c3)
-#pragma unroll
-            for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-                for (int c1 = 0; c1 < CI::NA; ++c1) {
-                    const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
-                    if (lin >= L0 && lin < L0 + M) {
-                        const float yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
-                                         Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
-                        part[lin - L0] =
-                            fmaf(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, part[lin - L0]);
-                    }
-                }
+        const int qe = min(q8 + 8, m);
+        int q = q8;
+        if constexpr (pair_step3<LA, LB, LC>()) {
+#pragma unroll 1
+            for (; q + 1 < qe; q += 2) {
+                const PTf r0 = buf[q], r1 = buf[q + 1];
+                add_rec3<LA, LB, LC, L0, M>(r0, g, part);
+                add_rec3<LA, LB, LC, L0, M>(r1, g, part);
+            }
+        }
+#pragma unroll 1
+        for (; q < qe; ++q) add_rec3<LA, LB, LC, L0, M>(buf[q], g, part);
       }
+    }
+    float sum[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float e;
+        two_sum(hi[m], part[m], sum[m], e);
+        lo[m] += e;
+    }
+    if constexpr (M <= kSplitM3) {
+        if (split) {
+            // the other warps' (sum, lo) pairs, added to warp 0's in warp order
+            float2* x = reinterpret_cast<float2*>(xbuf);
+            if (w > 0) {
+#pragma unroll
+                for (int m = 0; m < M; ++m) x[((w - 1) * kSplitM3 + m) * 32 + lane] = make_float2(sum[m], lo[m]);
+            }
+            __syncthreads();
+            if (w > 0) return;
+#pragma unroll 1
+            for (int v = 0; v < kThreads3 / 32 - 1; ++v)
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    const float2 o = x[(v * kSplitM3 + m) * 32 + lane];
+                    float s2, e;
+                    two_sum(sum[m], o.x, s2, e);
+                    sum[m] = s2;
+                    lo[m] += o.y + e;
+                }
+        }
     }
     if (!valid) return;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int lin = L0 + m, pg = lin / CI::PS;
-        if (pg >= kp0 && pg < kp1) {
-            float s, e;
-            two_sum(hi[m], part[m], s, e);
-            const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
-            dst[(size_t)(pg - kp0) * N * N + (size_t)j * N + i] = s + (lo[m] + e);
-        }
+        const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
+        dst[(size_t)pg * N * N + (size_t)j * N + i] = sum[m] + lo[m];
     }
 }
 
 template <int LA, int LB, int LC, int C>
 __device__ __noinline__ void run_item3(const Prim3<double> pr, PTd* buf, const Geo3<double> g, double* dst, int N,
-                                       int kp0, int kp1, bool valid) {
+                                       bool split, void* xbuf, bool valid) {
     const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
@@ -314,58 +365,54 @@ __device__ __noinline__ void run_item3(const Prim3<double> pr, PTd* buf, const G
     double acc[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) acc[m] = 0.0;
+    const int w = threadIdx.x >> 5, q00 = split ? 32 * w : 0, qs = split ? 32 * (kThreads3 / 32) : 32;
 #pragma unroll 1
-    for (int q0 = 0; q0 < n; q0 += 32) {
+    for (int q0 = q00; q0 < n; q0 += qs) {
       __syncwarp();
       gen_records3(buf, pr, q0, n, lane);
       __syncwarp();
       const int m = min(32, n - q0);
+      int q = 0;
+      if constexpr (pair_step3<LA, LB, LC>()) {
 #pragma unroll 1
-      for (int q = 0; q < m; ++q) {
-        const double2 r0 = reinterpret_cast<const double2*>(buf + q)[0];
-        const double2 r1 = reinterpret_cast<const double2*>(buf + q)[1];
-        const double2 r2 = reinterpret_cast<const double2*>(buf + q)[2];
-        const double2 r3 = reinterpret_cast<const double2*>(buf + q)[3];
-        const double w = r0.x, kab = r0.y, kac = r1.x, kbc = r1.y, ra = r2.x, rb = r2.y, rc = r3.x, o2q = r3.y;
-        const double e000 = exp(-(kab * g.R2[0] + kac * g.R2[1] + kbc * g.R2[2])) * w;
-        double Ex[LA + 1][LB + 1][LC + 1], Ey[LA + 1][LB + 1][LC + 1], Ez[LA + 1][LB + 1][LC + 1];
-        build_E3<LA, LB, LC, double>(Ex, -(rb * g.AB[0] + rc * g.AC[0]), ra * g.AB[0] - rc * g.BC[0],
-                                     ra * g.AC[0] + rb * g.BC[0], o2q, e000);
-        build_E3<LA, LB, LC, double>(Ey, -(rb * g.AB[1] + rc * g.AC[1]), ra * g.AB[1] - rc * g.BC[1],
-                                     ra * g.AC[1] + rb * g.BC[1], o2q, 1.0);
-        build_E3<LA, LB, LC, double>(Ez, -(rb * g.AB[2] + rc * g.AC[2]), ra * g.AB[2] - rc * g.BC[2],
-                                     ra * g.AC[2] + rb * g.BC[2], o2q, 1.0);
-#pragma unroll
-        for (int c3 = 0; c3 < CI::NC; ++c3)
-#pragma unroll
-            for (int c2 = 0; c2 < CI::NB; ++c2)
-#pragma unroll
-                for (int c1 = 0; c1 < CI::NA; ++c1) {
-                    const int lin = c1 + CI::N1 * c2 + CI::N1 * CI::N2 * c3;
-                    if (lin >= L0 && lin < L0 + M) {
-                        const double yz = Ey[cart_y(LA, c1)][cart_y(LB, c2)][cart_y(LC, c3)] *
-                                          Ez[cart_z(LA, c1)][cart_z(LB, c2)][cart_z(LC, c3)];
-                        acc[lin - L0] = fma(Ex[cart_x(LA, c1)][cart_x(LB, c2)][cart_x(LC, c3)], yz, acc[lin - L0]);
-                    }
-                }
+        for (; q + 1 < m; q += 2) {
+            const PTd r0 = buf[q], r1 = buf[q + 1];
+            add_rec3<LA, LB, LC, L0, M>(r0, g, acc);
+            add_rec3<LA, LB, LC, L0, M>(r1, g, acc);
+        }
       }
+#pragma unroll 1
+      for (; q < m; ++q) add_rec3<LA, LB, LC, L0, M>(buf[q], g, acc);
+    }
+    if constexpr (M <= kSplitM3) {
+        if (split) {
+            // the other warps' sums, added to warp 0's in warp order
+            double* x = reinterpret_cast<double*>(xbuf);
+            if (w > 0) {
+#pragma unroll
+                for (int m = 0; m < M; ++m) x[((w - 1) * kSplitM3 + m) * 32 + lane] = acc[m];
+            }
+            __syncthreads();
+            if (w > 0) return;
+#pragma unroll 1
+            for (int v = 0; v < kThreads3 / 32 - 1; ++v)
+#pragma unroll
+                for (int m = 0; m < M; ++m) acc[m] += x[(v * kSplitM3 + m) * 32 + lane];
+        }
     }
     if (!valid) return;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         const int lin = L0 + m, pg = lin / CI::PS;
-        if (pg >= kp0 && pg < kp1) {
-            const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
-            dst[(size_t)(pg - kp0) * N * N + (size_t)j * N + i] = acc[m];
-        }
+        const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
+        dst[(size_t)pg * N * N + (size_t)j * N + i] = acc[m];
     }
 }
 
 // Classes with an f shell (la, lb or lc = 3), one routine with run-time loops:
 // the E tables of the three axes (4 x 4 x 4 each) and the chunk's <= 100 block
 // elements live in local memory, and the recursion runs in FP64 for both
-// precisions (an FP32 record's exponent coefficient is rebuilt from its hi + lo
-// words).  The class and chunk follow the specialised path's conventions
+// precisions (an FP32 record's exponent coefficients are FP64 already).  The class and chunk follow the specialised path's conventions
 // (aliased lin, pages [P0, P1) of the block).  Only the kernel instantiated
 // for bases with f shells calls it, so its local memory is not reserved by
 // the others.
@@ -399,17 +446,15 @@ __device__ __forceinline__ void e3_axis(double (&E)[4][4][4], int la, int lb, in
 }
 
 __device__ __forceinline__ double pt_exponent(const PTf* r, const double (&R2)[3]) {
-    const double kab = (double)r->kab_hi + (double)r->kab_lo, kac = (double)r->kac_hi + (double)r->kac_lo,
-                 kbc = (double)r->kbc_hi + (double)r->kbc_lo;
-    return (kab * R2[0] + kac * R2[1] + kbc * R2[2]) * 0.69314718055994530942;  // records carry k log2(e)
+    return (r->kab * R2[0] + r->kac * R2[1] + r->kbc * R2[2]) * 0.69314718055994530942;  // records carry k log2(e)
 }
 __device__ __forceinline__ double pt_exponent(const PTd* r, const double (&R2)[3]) {
     return r->kab * R2[0] + r->kac * R2[1] + r->kbc * R2[2];
 }
 
 template <typename PT, typename FT>
-__device__ __noinline__ void run_item3_f(const Prim3<FT> pr, PT* buf, const Geo3<FT> g, FT* dst, int N, int kp0,
-                                         int kp1, int cls, int chunk, bool valid) {
+__device__ __noinline__ void run_item3_f(const Prim3<FT> pr, PT* buf, const Geo3<FT> g, FT* dst, int N, int cls,
+                                         int chunk, bool valid) {
     const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     const int c = cls - kClsF3, la = c >> 4, lb = (c >> 2) & 3, lc = c & 3;
     const int NA = ncart(la), NB = ncart(lb), NC = ncart(lc), PS = NA * NB, N1 = 2 * la + 1, N2 = 2 * lb + 1;
@@ -430,7 +475,6 @@ __device__ __noinline__ void run_item3_f(const Prim3<FT> pr, PT* buf, const Geo3
         AC[a] = (double)g.AC[a];
         BC[a] = (double)g.BC[a];
         R2[a] = (double)g.R2[a];
-        if constexpr (sizeof(FT) == 4) R2[a] += (double)g.R2lo[a];
     }
     double E[3][4][4][4];
 #pragma unroll 1
@@ -466,24 +510,22 @@ __device__ __noinline__ void run_item3_f(const Prim3<FT> pr, PT* buf, const Geo3
     if (!valid) return;
     for (int m = 0; m < M; ++m) {
         const int lin = L0 + m, pg = lin / PS;
-        if (pg >= kp0 && pg < kp1) {
-            const int i = lin % NA, j = (lin / NA) % NB;
-            dst[(size_t)(pg - kp0) * N * N + (size_t)j * N + i] = (FT)acc[m];
-        }
+        const int i = lin % NA, j = (lin / NA) % NB;
+        dst[(size_t)pg * N * N + (size_t)j * N + i] = (FT)acc[m];
     }
 }
 
 template <typename PT, typename FT, int LA, int LB, int LC>
 __device__ __forceinline__ void run_chunks3(int chunk, const Prim3<FT>& pp, PT* n, const Geo3<FT>& g, FT* dst, int N,
-                                            int kp0, int kp1, bool valid) {
+                                            bool split, void* xbuf, bool valid) {
     constexpr int NCH = nchunks3(LA, LB, LC);
     switch (chunk) {
-        case 0: run_item3<LA, LB, LC, 0>(pp, n, g, dst, N, kp0, kp1, valid); break;
-        case 1: if constexpr (NCH > 1) run_item3<LA, LB, LC, 1>(pp, n, g, dst, N, kp0, kp1, valid); break;
-        case 2: if constexpr (NCH > 2) run_item3<LA, LB, LC, 2>(pp, n, g, dst, N, kp0, kp1, valid); break;
-        case 3: if constexpr (NCH > 3) run_item3<LA, LB, LC, 3>(pp, n, g, dst, N, kp0, kp1, valid); break;
-        case 4: if constexpr (NCH > 4) run_item3<LA, LB, LC, 4>(pp, n, g, dst, N, kp0, kp1, valid); break;
-        case 5: if constexpr (NCH > 5) run_item3<LA, LB, LC, 5>(pp, n, g, dst, N, kp0, kp1, valid); break;
+        case 0: run_item3<LA, LB, LC, 0>(pp, n, g, dst, N, split, xbuf, valid); break;
+        case 1: if constexpr (NCH > 1) run_item3<LA, LB, LC, 1>(pp, n, g, dst, N, split, xbuf, valid); break;
+        case 2: if constexpr (NCH > 2) run_item3<LA, LB, LC, 2>(pp, n, g, dst, N, split, xbuf, valid); break;
+        case 3: if constexpr (NCH > 3) run_item3<LA, LB, LC, 3>(pp, n, g, dst, N, split, xbuf, valid); break;
+        case 4: if constexpr (NCH > 4) run_item3<LA, LB, LC, 4>(pp, n, g, dst, N, split, xbuf, valid); break;
+        case 5: if constexpr (NCH > 5) run_item3<LA, LB, LC, 5>(pp, n, g, dst, N, split, xbuf, valid); break;
         default: break;
     }
 }
@@ -491,16 +533,16 @@ __device__ __forceinline__ void run_chunks3(int chunk, const Prim3<FT>& pp, PT* 
 // pp: the unit's primitive lists; n: the warp's record buffer
 template <typename PT, typename FT, bool F3>
 __device__ __forceinline__ void dispatch3(int cls, int chunk, const Prim3<FT>& pp, PT* n, const Geo3<FT>& g, FT* dst,
-                                          int N, int kp0, int kp1, bool valid) {
+                                          int N, bool split, void* xbuf, bool valid) {
     if constexpr (F3) {
         if (cls >= kClsF3) {
-            run_item3_f<PT, FT>(pp, n, g, dst, N, kp0, kp1, cls, chunk, valid);
+            run_item3_f<PT, FT>(pp, n, g, dst, N, cls, chunk, valid);
             return;
         }
     }
     switch (cls) {
 #define AOK_C3(LA, LB, LC) \
-    case (LA) * 9 + (LB) * 3 + (LC): run_chunks3<PT, FT, LA, LB, LC>(chunk, pp, n, g, dst, N, kp0, kp1, valid); break;
+    case (LA) * 9 + (LB) * 3 + (LC): run_chunks3<PT, FT, LA, LB, LC>(chunk, pp, n, g, dst, N, split, xbuf, valid); break;
         AOK_C3(0, 0, 0) AOK_C3(0, 0, 1) AOK_C3(0, 0, 2) AOK_C3(0, 1, 0) AOK_C3(0, 1, 1) AOK_C3(0, 1, 2)
         AOK_C3(0, 2, 0) AOK_C3(0, 2, 1) AOK_C3(0, 2, 2) AOK_C3(1, 0, 0) AOK_C3(1, 0, 1) AOK_C3(1, 0, 2)
         AOK_C3(1, 1, 0) AOK_C3(1, 1, 1) AOK_C3(1, 1, 2) AOK_C3(1, 2, 0) AOK_C3(1, 2, 1) AOK_C3(1, 2, 2)
@@ -524,57 +566,101 @@ struct Ov3Params {
     const int4* tiles;
     const int* ntiles;
     unsigned* counter;
-    const Item3* items;  // every (shell triple, page chunk), heaviest first (k_order3c)
+    const Item3* items;  // every (shell triple, page chunk) in queue order (k_prep3c)
+    const int* segs;     // segment starts in items (nseg + 1 entries); nseg, H at segs[nitems + 1], [nitems + 2]
     int nitems, ns, K, N, NZ;
     FT scale;
     int use_scale;
     int boff[kMaxShells + 1];
 };
 
-// Work unit = (item, tile): one shell-triple block (or page chunk of it) for the
-// 32 batch elements of a tile, lane = element.  Units are drained from one
-// global counter item-major, so every tile's heaviest items run first and the
-// cheap ones fill the end; there are no panels and no barriers.  A lane writes
-// its element's block straight to the output: a batch element's (N,N,N) slab
-// is contiguous and the whole output is written exactly once, so the scattered
-// stores of a block meet in L2 before they reach DRAM.  Three CTAs of four
-// warps per SM (<= 168 registers).
+// Work unit = (segment, W tiles): a run of consecutive items of the queue order
+// (k_prep3c: items of one routine together, heaviest first, cut into segments
+// of about equal cost; an item heavier than that is a segment of its own) for
+// W consecutive tiles of 32 batch elements, one tile per warp, lane = element.
+// The first H segments (heavy single items of small blocks, H from k_prep3c)
+// take one tile per unit instead, their records shared out over the W warps,
+// so that the heaviest items do not set the kernel's length.  A CTA claims
+// one unit at a time from one global counter, segment-major, so the warps of a
+// CTA run the same routines and the warps in flight few distinct ones
+// (instruction-cache locality), and every tile's heaviest items start first; a
+// tile's geometry is loaded once per unit.  A lane writes its element's blocks
+// straight to the output: a batch element's (N,N,N) slab is contiguous and the
+// whole output is written exactly once.  Three CTAs of four warps per SM
+// (<= 168 registers).  FP64 claims per warp instead, with about one item per
+// segment (kCtaClaims3).
 template <typename FT, bool F3>
 __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constant__ Ov3Params<FT> P) {
     using PT = typename PTT<FT>::type;
-    __shared__ PT recbuf[kThreads3 / 32][32];  // each warp's current 32 records
+    constexpr int W = kThreads3 / 32;
+    __shared__ PT recbuf[W][32];                                    // each warp's current 32 records
+    __shared__ __align__(16) FT xbuf[(W - 1) * kSplitM3 * 32 * (sizeof(FT) == 4 ? 2 : 1)];  // split partial sums
+    __shared__ unsigned claim;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ntiles = *P.ntiles;
-    const unsigned total = (unsigned)ntiles * (unsigned)P.nitems;
+    const int ntiles = *P.ntiles, nseg = P.segs[P.nitems + 1], H = P.segs[P.nitems + 2];
+    const unsigned ngroups = (unsigned)(ntiles + W - 1) / W;
+    const unsigned nsplit = (unsigned)H * (unsigned)ntiles, total = nsplit + ngroups * (unsigned)(nseg - H);
     const size_t N2 = (size_t)P.N * P.N, N3 = N2 * P.N;
     for (;;) {
-        unsigned u = 0;
-        if (lane == 0) u = atomicAdd(P.counter, 1u);
-        u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= total) break;
-        const int it = (int)(u / (unsigned)ntiles), tile = (int)(u % (unsigned)ntiles);
+        bool split = false;
+        int sg, tile;
+        if constexpr (kCtaClaims3<FT>) {
+            // one claim per CTA: its warps take the same segment for W consecutive tiles (or share one)
+            if (threadIdx.x == 0) claim = atomicAdd(P.counter, 1u);
+            __syncthreads();
+            const unsigned u = claim;
+            __syncthreads();
+            if (u >= total) break;
+            split = u < nsplit;
+            if (split) {
+                sg = (int)(u / (unsigned)ntiles);
+                tile = (int)(u % (unsigned)ntiles);
+            } else {
+                sg = H + (int)((u - nsplit) / ngroups);
+                tile = (int)((u - nsplit) % ngroups) * W + warp;
+                if (tile >= ntiles) continue;
+            }
+        } else {
+            // one claim per warp: (segment, tile), segment-major
+            unsigned u = 0;
+            if (lane == 0) u = atomicAdd(P.counter, 1u);
+            u = __shfl_sync(0xffffffffu, u, 0);
+            if (u >= (unsigned)ntiles * (unsigned)nseg) break;
+            sg = (int)(u / (unsigned)ntiles);
+            tile = (int)(u % (unsigned)ntiles);
+        }
         const int4 td = P.tiles[tile];
         const bool valid = lane < td.z;
         const int b = P.perm[td.y + (valid ? lane : 0)];
         Geo3<FT> g;
         load_geo3(g, P.posA + 3 * (size_t)b, P.posB + 3 * (size_t)b, P.posC + 3 * (size_t)b, P.scale,
                   P.use_scale != 0);
-        const Item3 wi = P.items[it];
         // the tile's species triple (key ((ga NZ) + gb) NZ + gc; 0 on the single-species path)
         const int ga = td.x / (P.NZ * P.NZ), gb = (td.x / P.NZ) % P.NZ, gc = td.x % P.NZ;
-        Prim3<FT> pr;
-        const int la = ga * P.ns + wi.sa, lb = gb * P.ns + wi.sb, lc = gc * P.ns + wi.sc;
-        pr.z[0] = P.pz + (size_t)la * P.K;
-        pr.c[0] = P.pc + (size_t)la * P.K;
-        pr.n[0] = __ldg(P.pn + la);
-        pr.z[1] = P.pz + (size_t)lb * P.K;
-        pr.c[1] = P.pc + (size_t)lb * P.K;
-        pr.n[1] = __ldg(P.pn + lb);
-        pr.z[2] = P.pz + (size_t)lc * P.K;
-        pr.c[2] = P.pc + (size_t)lc * P.K;
-        pr.n[2] = __ldg(P.pn + lc);
-        FT* dst = P.out + (size_t)b * N3 + (size_t)P.boff[wi.sc] * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
-        dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, recbuf[warp], g, dst, P.N, 0, kAllPages3, valid);
+        const FT* zA = P.pz + (size_t)ga * P.ns * P.K;
+        const FT* cA = P.pc + (size_t)ga * P.ns * P.K;
+        const FT* zB = P.pz + (size_t)gb * P.ns * P.K;
+        const FT* cB = P.pc + (size_t)gb * P.ns * P.K;
+        const FT* zC = P.pz + (size_t)gc * P.ns * P.K;
+        const FT* cC = P.pc + (size_t)gc * P.ns * P.K;
+        FT* base = P.out + (size_t)b * N3;
+        const int i0 = P.segs[sg], i1 = P.segs[sg + 1];
+#pragma unroll 1
+        for (int it = i0; it < i1; ++it) {
+            const Item3 wi = P.items[it];
+            Prim3<FT> pr;
+            pr.z[0] = zA + (size_t)wi.sa * P.K;
+            pr.c[0] = cA + (size_t)wi.sa * P.K;
+            pr.n[0] = __ldg(P.pn + ga * P.ns + wi.sa);
+            pr.z[1] = zB + (size_t)wi.sb * P.K;
+            pr.c[1] = cB + (size_t)wi.sb * P.K;
+            pr.n[1] = __ldg(P.pn + gb * P.ns + wi.sb);
+            pr.z[2] = zC + (size_t)wi.sc * P.K;
+            pr.c[2] = cC + (size_t)wi.sc * P.K;
+            pr.n[2] = __ldg(P.pn + gc * P.ns + wi.sc);
+            FT* dst = base + (size_t)P.boff[wi.sc] * N2 + (size_t)P.boff[wi.sb] * P.N + P.boff[wi.sa];
+            dispatch3<PT, FT, F3>(wi.cls, wi.chunk, pr, recbuf[warp], g, dst, P.N, split, xbuf, valid);
+        }
     }
 }
 
@@ -595,6 +681,7 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     P.ntiles = p->d_ntiles;
     P.counter = p->d_counter;
     P.items = (const Item3*)p->d_order3;
+    P.segs = p->d_segs3;
     P.nitems = p->nitems3;
     P.ns = (int)p->ns;
     P.K = (int)p->K;
