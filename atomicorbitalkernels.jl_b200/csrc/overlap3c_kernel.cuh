@@ -269,7 +269,7 @@ __host__ __device__ constexpr bool pair_step3() {
 // With split, the CTA's warps share one tile: warp w takes the record chunks
 // w, w + W, ... and the partial sums meet in xbuf (blocks of <= kSplitM3).
 template <int LA, int LB, int LC, int C>
-__device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Geo3<float> g, float* dst, int N,
+__device__ __forceinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Geo3<float> g, float* dst, int N,
                                        bool split, void* xbuf, bool valid) {
     const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     using CI = Class3<LA, LB, LC>;
@@ -356,7 +356,7 @@ __device__ __noinline__ void run_item3(const Prim3<float> pr, PTf* buf, const Ge
 }
 
 template <int LA, int LB, int LC, int C>
-__device__ __noinline__ void run_item3(const Prim3<double> pr, PTd* buf, const Geo3<double> g, double* dst, int N,
+__device__ __forceinline__ void run_item3(const Prim3<double> pr, PTd* buf, const Geo3<double> g, double* dst, int N,
                                        bool split, void* xbuf, bool valid) {
     const int lane = threadIdx.x & 31, n = pr.n[0] * pr.n[1] * pr.n[2];
     using CI = Class3<LA, LB, LC>;
