@@ -38,6 +38,7 @@ constexpr int kSplitM3 = 9;  // largest block that the CTA's warps may share (he
 // longer and more variable exponentials balance better in small units (both
 // measured on config 4).
 template <typename FT> constexpr bool kCtaClaims3 = sizeof(FT) == 4;
+constexpr int kShortM3 = 18;  // FP32C blocks of >= this many elements take a plain path when n <= 8
 
 __host__ __device__ constexpr int pages_per_chunk3(int la, int lb) {
     return (ncart(la) * ncart(lb)) >= 36 ? 1 : 36 / (ncart(la) * ncart(lb));
@@ -275,6 +276,28 @@ __device__ __forceinline__ void run_item3(const Prim3<float> pr, PTf* buf, const
     using CI = Class3<LA, LB, LC>;
     constexpr int P0 = C * CI::PPC, P1 = (C + 1) * CI::PPC < CI::NC ? (C + 1) * CI::PPC : CI::NC;
     constexpr int L0 = P0 * CI::PS, M = (P1 - P0) * CI::PS;
+    if constexpr (M >= kShortM3) {
+        // Large blocks of at most 8 triples (one run): plain FP32 sums, so that the
+        // (hi, lo) registers of the compensated path are not live here.
+        if (n <= 8) {
+            float part[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) part[m] = 0.f;
+            __syncwarp();
+            gen_records3(buf, pr, 0, n, lane);
+            __syncwarp();
+#pragma unroll 1
+            for (int q = 0; q < n; ++q) add_rec3<LA, LB, LC, L0, M>(buf[q], g, part);
+            if (!valid) return;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const int lin = L0 + m, pg = lin / CI::PS;
+                const int i = lin % CI::NA, j = (lin / CI::NA) % CI::NB;
+                dst[(size_t)pg * N * N + (size_t)j * N + i] = part[m];
+            }
+            return;
+        }
+    }
     // Compensated contraction: runs of up to 8 triples are summed in part[], and
     // each run is folded into hi + lo with TwoSum.
     float hi[M], lo[M], part[M];
