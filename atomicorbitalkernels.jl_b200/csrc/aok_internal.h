@@ -208,9 +208,6 @@ int kernel_prepare(const void* k, size_t smem, int threads, int* occ);
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);
-int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
-                     const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
-                     double lengthscale, cudaStream_t s);
 int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
                    cudaStream_t s);
 int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,

@@ -12,24 +12,32 @@ namespace aok {
 
 // The primitives of every (species g, shell s): the non-zero-coefficient slots of
 // the padded (ns,K,NZ) tables, compacted in slot order into pz/pc at (g ns + s) K,
-// and their number pn[g ns + s].  One thread per (shell, species).
+// and their number pn[g ns + s] (also into spn, shared).  One warp per (shell,
+// species), lanes over the slots.
 template <typename FT>
 __device__ __forceinline__ void prim3c_padded(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn,
-                                              const FT* __restrict__ zeta, const FT* __restrict__ coef, int ns, int K,
-                                              int NZ) {
-    for (int t = threadIdx.x; t < ns * NZ; t += blockDim.x) {
+                                              int* spn, const FT* __restrict__ zeta, const FT* __restrict__ coef,
+                                              int ns, int K, int NZ) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int t = threadIdx.x >> 5; t < ns * NZ; t += nw) {
         const int sh = t % ns, g = t / ns;
         int n = 0;
-        for (int k = 0; k < K; ++k) {
+        for (int k0 = 0; k0 < K; k0 += 32) {
+            const int k = k0 + lane;
             const size_t o = (size_t)sh + (size_t)ns * (k + (size_t)K * g);
-            const FT c = coef[o];
+            const FT c = k < K ? coef[o] : FT(0);
+            const unsigned m = __ballot_sync(0xffffffffu, c != FT(0));
             if (c != FT(0)) {
-                pz[(size_t)t * K + n] = zeta[o];
-                pc[(size_t)t * K + n] = c;
-                ++n;
+                const int at = n + __popc(m & ((1u << lane) - 1u));
+                pz[(size_t)t * K + at] = zeta[o];
+                pc[(size_t)t * K + at] = c;
             }
+            n += __popc(m);
         }
-        pn[t] = n;
+        if (lane == 0) {
+            pn[t] = n;
+            spn[t] = n;
+        }
     }
 }
 
@@ -37,26 +45,34 @@ __device__ __forceinline__ void prim3c_padded(FT* __restrict__ pz, FT* __restric
 // nprim[s] primitives at prim_offset[s] (0-based); counts outside 0..K are flagged
 // (AOK_ERR_INVALID in err) and read as 0.
 template <typename FT>
-__device__ __forceinline__ void prim3c_flat(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn,
+__device__ __forceinline__ void prim3c_flat(FT* __restrict__ pz, FT* __restrict__ pc, int* __restrict__ pn, int* spn,
                                             const int64_t* __restrict__ nprim, const int64_t* __restrict__ off,
                                             const FT* __restrict__ coef, const FT* __restrict__ alpha, int ns, int K,
                                             int* __restrict__ err) {
-    for (int t = threadIdx.x; t < ns; t += blockDim.x) {
-        int64_t m = nprim[t];
-        if (m < 0 || m > K) {
-            atomicCAS(err, 0, AOK_ERR_INVALID);
-            m = 0;
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int t = threadIdx.x >> 5; t < ns; t += nw) {
+        int64_t mm = nprim[t];
+        if (mm < 0 || mm > K) {
+            if (lane == 0) atomicCAS(err, 0, AOK_ERR_INVALID);
+            mm = 0;
         }
+        const int64_t o0 = off[t];
         int n = 0;
-        for (int k = 0; k < (int)m; ++k) {
-            const FT c = coef[off[t] + k];
+        for (int k0 = 0; k0 < (int)mm; k0 += 32) {
+            const int k = k0 + lane;
+            const FT c = k < (int)mm ? coef[o0 + k] : FT(0);
+            const unsigned m = __ballot_sync(0xffffffffu, c != FT(0));
             if (c != FT(0)) {
-                pz[(size_t)t * K + n] = alpha[off[t] + k];
-                pc[(size_t)t * K + n] = c;
-                ++n;
+                const int at = n + __popc(m & ((1u << lane) - 1u));
+                pz[(size_t)t * K + at] = alpha[o0 + k];
+                pc[(size_t)t * K + at] = c;
             }
+            n += __popc(m);
         }
-        pn[t] = n;
+        if (lane == 0) {
+            pn[t] = n;
+            spn[t] = n;
+        }
     }
 }
 
@@ -110,8 +126,8 @@ __device__ __forceinline__ long long block_scan3(long long v, long long* wtot) {
 }
 
 __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __restrict__ segs,
-                                             const Item3* __restrict__ items, const int* __restrict__ pn,
-                                             const int* __restrict__ ntiles, int n, int ns, int NZ, int target_units) {
+                                             const Item3* __restrict__ items, const int* pn, int ntiles, int n,
+                                             int ns, int NZ, int target_units) {
     __shared__ unsigned long long ikey[kOrder3Max], gkey[kOrder3Max];
     __shared__ int cst[kOrder3Max];
     __shared__ int gmax[kCodes3];
@@ -157,7 +173,7 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
         gkey[i] = ((unsigned long long)(0x7FFFFFFF - gmax[ci]) << 32) | (unsigned)ci;
     }
     __syncthreads();
-    int rank[kOrder3Per], rcost[kOrder3Per];
+    int rank[kOrder3Per], rcost[kOrder3Per], rcls[kOrder3Per];
 #pragma unroll
     for (int k = 0; k < kOrder3Per; ++k) {
         const int i = threadIdx.x + k * kOrder3Threads;
@@ -169,15 +185,21 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
             const unsigned long long gj = gkey[j];
             r += gj < gi || (gj == gi && ikey[j] < ki);
         }
-        order[r] = items[i];
+        const Item3 it = items[i];
+        order[r] = it;
         rank[k] = r;
         rcost[k] = cst[i];
+        rcls[k] = it.cls;
     }
     __syncthreads();
-    // the costs in queue order (cst is free again)
+    // the costs and classes in queue order (cst and gkey are free again)
+    int* qcls = reinterpret_cast<int*>(gkey);
 #pragma unroll
     for (int k = 0; k < kOrder3Per; ++k)
-        if (rank[k] >= 0) cst[rank[k]] = rcost[k];
+        if (rank[k] >= 0) {
+            cst[rank[k]] = rcost[k];
+            qcls[rank[k]] = rcls[k];
+        }
     __syncthreads();
     // exclusive cost prefix of this thread's kOrder3Per consecutive positions
     const int r0 = threadIdx.x * kOrder3Per;
@@ -190,7 +212,7 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
     if (threadIdx.x == kOrder3Threads - 1) total_s = incl;
     __syncthreads();
     const long long total = total_s;
-    const long long G = max(1LL, min((long long)n, (long long)target_units / max(*ntiles, 1)));
+    const long long G = max(1LL, min((long long)n, (long long)target_units / max(ntiles, 1)));
     const long long C = max(1LL, (total + G - 1) / G);
     // a segment starts at r when a multiple of C lies in (prefix(r - 1), prefix(r)], or next to an item of cost >= C
     long long P = incl - tsum;
@@ -225,9 +247,9 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
     if (threadIdx.x == 0) {
         int h = 0;
         while (h < n && cst[h] >= 2 * C) {
-            const Item3 it = order[h];
-            if (it.cls >= kClsF3) break;
-            const int la = it.cls / 9, lb = (it.cls / 3) % 3, lc = it.cls % 3;
+            const int cls = qcls[h];
+            if (cls >= kClsF3) break;
+            const int la = cls / 9, lb = (cls / 3) % 3, lc = cls % 3;
             if (ncart(la) * ncart(lb) * ncart(lc) > kSplitM3) break;
             ++h;
         }
@@ -237,22 +259,24 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
 
 // One CTA per call ahead of the kernel: the compact primitive lists (from the padded
 // tables, or from flat GaussianBasis-style tables when nprim is given), then the
-// queue order and its segments (order3c_body reads the lists back after a barrier).
+// queue order and its segments.  It needs no binning result (the segment count uses
+// the tile count of the batch, ntiles = ceil(B / 32)), so it runs on the plan's side
+// stream while the batch is binned.
 template <typename FT>
 __global__ void __launch_bounds__(kOrder3Threads) k_prep3c(FT* __restrict__ pz, FT* __restrict__ pc,
                                                            int* __restrict__ pn, const FT* __restrict__ zeta,
                                                            const FT* __restrict__ coef, const int64_t* __restrict__ nprim,
                                                            const int64_t* __restrict__ off, int* __restrict__ err,
                                                            Item3* __restrict__ order, int* __restrict__ segs,
-                                                           const Item3* __restrict__ items,
-                                                           const int* __restrict__ ntiles, int n, int ns, int K, int NZ,
-                                                           int target_units) {
+                                                           const Item3* __restrict__ items, int ntiles, int n, int ns,
+                                                           int K, int NZ, int target_units) {
+    __shared__ int spn[kMaxShells * 6];
     if (nprim)
-        prim3c_flat<FT>(pz, pc, pn, nprim, off, coef, zeta, ns, K, err);
+        prim3c_flat<FT>(pz, pc, pn, spn, nprim, off, coef, zeta, ns, K, err);
     else
-        prim3c_padded<FT>(pz, pc, pn, zeta, coef, ns, K, NZ);
+        prim3c_padded<FT>(pz, pc, pn, spn, zeta, coef, ns, K, NZ);
     __syncthreads();
-    order3c_body(order, segs, items, pn, ntiles, n, ns, NZ, target_units);
+    order3c_body(order, segs, items, spn, ntiles, n, ns, NZ, target_units);
 }
 
 int setup_overlap3c_schedule(aok_plan* p) {
@@ -309,29 +333,42 @@ static int check_units3(const aok_plan* p, int64_t B, const char* who) {
     return AOK_OK;
 }
 
-// The 3C overlap after the schedule is set up and the batch binned (by the caller):
-// one CTA builds the compact primitive lists (of the padded (zeta, coef) tables, or of
-// the flat tables when nprim is given, zeta = alpha) and the per-call item order and
-// segments, then the kernel runs over the plan's bins.
-int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
-                     const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
-                     double lengthscale, cudaStream_t s) {
+// The 3C prep for B elements on stream `side` (see k_prep3c): the compact primitive
+// lists of the padded (zeta, coef) tables, or of the flat tables when nprim is given
+// (zeta = alpha), and the per-call item order and segments.
+static int launch_prep3c(aok_plan* p, const void* zeta, const void* coef, const int64_t* nprim,
+                         const int64_t* prim_offset, int64_t B, cudaStream_t side) {
     const size_t nt = (size_t)(p->ns * p->K * p->NZ);
     // FP32: about eight (segment, tile) pairs per resident warp (three CTAs of four warps
     // per SM); FP64: about one item per segment
     const int target_units = p->prec == AOK_PREC_F64 ? (1 << 30) : p->num_sms * 3 * (kThreads3 / 32) * 8;
+    const int ntiles = (int)std::min<int64_t>((B + 31) / 32, 1 << 30);
     if (p->prec == AOK_PREC_F64)
-        k_prep3c<double><<<1, kOrder3Threads, 0, s>>>(
+        k_prep3c<double><<<1, kOrder3Threads, 0, side>>>(
             (double*)p->d_pp3, (double*)p->d_pp3 + nt, p->d_npp3, (const double*)zeta, (const double*)coef, nprim,
-            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, p->d_ntiles,
-            p->nitems3, (int)p->ns, (int)p->K, (int)p->NZ, target_units);
+            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, ntiles, p->nitems3,
+            (int)p->ns, (int)p->K, (int)p->NZ, target_units);
     else
-        k_prep3c<float><<<1, kOrder3Threads, 0, s>>>(
+        k_prep3c<float><<<1, kOrder3Threads, 0, side>>>(
             (float*)p->d_pp3, (float*)p->d_pp3 + nt, p->d_npp3, (const float*)zeta, (const float*)coef, nprim,
-            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, p->d_ntiles,
-            p->nitems3, (int)p->ns, (int)p->K, (int)p->NZ, target_units);
-    const int st = cuda_status(cudaGetLastError(), "k_prep3c");
-    if (st != AOK_OK) return st;
+            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, ntiles, p->nitems3,
+            (int)p->ns, (int)p->K, (int)p->NZ, target_units);
+    return cuda_status(cudaGetLastError(), "k_prep3c");
+}
+
+// The 3C overlap: the prep on the plan's side stream while `bin` bins the batch on s,
+// then the kernel over the plan's bins once both are done.
+template <typename Bin>
+static int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
+                            const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
+                            int64_t B, double lengthscale, cudaStream_t s, Bin bin) {
+    int st;
+    if ((st = cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord")) != AOK_OK) return st;
+    if ((st = cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent")) != AOK_OK) return st;
+    if ((st = launch_prep3c(p, zeta, coef, nprim, prim_offset, B, p->side)) != AOK_OK) return st;
+    if ((st = cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord")) != AOK_OK) return st;
+    if ((st = bin()) != AOK_OK) return st;
+    if ((st = cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent")) != AOK_OK) return st;
     if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s);
     return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s);
 }
@@ -354,8 +391,8 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
         return set_error(AOK_ERR_INVALID, "aok_overlap3c_gb: null pointer");
     if ((st = check_units3(p, B, "aok_overlap3c_gb")) != AOK_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    if ((st = launch_bin(p, nullptr, nullptr, B, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, alpha, coef, nprim, prim_offset, posA, posB, posC, 1.0, s);
+    return launch_overlap3c(p, out, alpha, coef, nprim, prim_offset, posA, posB, posC, B, 1.0, s,
+                            [&] { return launch_bin(p, nullptr, nullptr, B, s); });
 }
 
 extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
@@ -374,6 +411,6 @@ extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const voi
     cudaStream_t s = (cudaStream_t)stream;
     ++p->gen;  // the plan's bins change
     const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
-    if ((st = launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s)) != AOK_OK) return st;
-    return launch_overlap3c(p, out, zeta, coef, nullptr, nullptr, posA, posB, posC, lengthscale, s);
+    return launch_overlap3c(p, out, zeta, coef, nullptr, nullptr, posA, posB, posC, B, lengthscale, s,
+                            [&] { return launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s); });
 }
