@@ -68,6 +68,7 @@ struct aok_plan {
     void* d_items3 = nullptr;
     void* d_order3 = nullptr;        // per call: the items in queue order (k_prep3c)
     int* d_segs3 = nullptr;          // per call: segment starts in d_order3 (nitems3 + 1), then the count
+    int* d_key3 = nullptr;           // what d_order3/d_segs3 were built from: (n, tiles, target, counts)
     int nitems3 = 0;
     // graph mode of the fixed-basis forward (aok_plan_set_graph): the instantiated
     // launch chain, the arguments it was captured with, a private capture stream

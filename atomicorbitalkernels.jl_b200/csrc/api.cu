@@ -180,7 +180,7 @@ int aok_plan_destroy(aok_plan* p) {
                     p->d_tiles,     p->d_ntiles,    p->d_tbase,     p->d_counter,    p->d_err,
                     p->d_items,     p->d_blockhist, p->d_gb_zeta,    p->d_gb_coef,
                     p->d_pb_rec,    p->d_pb_counts, p->d_pb_items,  p->d_pb_itemidx, p->d_pb_rows,
-                    p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3,    p->d_order3,    p->d_segs3,
+                    p->d_partials,  p->d_coef_scratch, p->d_pp3,    p->d_npp3,       p->d_items3,    p->d_order3,    p->d_segs3,     p->d_key3,
                     p->d_pk,        p->d_segs,      p->d_nseg,      p->d_dpos_rec,   p->d_dpos_counts,
                     p->d_dpos_items};
     for (void* b : bufs) dfree(b);

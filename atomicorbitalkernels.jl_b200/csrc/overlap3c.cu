@@ -262,21 +262,36 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
 // queue order and its segments.  It needs no binning result (the segment count uses
 // the tile count of the batch, ntiles = ceil(B / 32)), so it runs on the plan's side
 // stream while the batch is binned.
+// The order and the segments are a function of (n, ntiles, target_units) and the
+// primitive counts alone, and key[] holds those of the last build: when they match
+// (the usual case, a fixed basis over many batches) the sort and the cut are skipped
+// and the buffers from that build stand.  A miss rebuilds them and then the key.
 template <typename FT>
 __global__ void __launch_bounds__(kOrder3Threads) k_prep3c(FT* __restrict__ pz, FT* __restrict__ pc,
                                                            int* __restrict__ pn, const FT* __restrict__ zeta,
                                                            const FT* __restrict__ coef, const int64_t* __restrict__ nprim,
                                                            const int64_t* __restrict__ off, int* __restrict__ err,
                                                            Item3* __restrict__ order, int* __restrict__ segs,
-                                                           const Item3* __restrict__ items, int ntiles, int n, int ns,
-                                                           int K, int NZ, int target_units) {
+                                                           int* __restrict__ key, const Item3* __restrict__ items,
+                                                           int ntiles, int n, int ns, int K, int NZ, int target_units) {
     __shared__ int spn[kMaxShells * 6];
     if (nprim)
         prim3c_flat<FT>(pz, pc, pn, spn, nprim, off, coef, zeta, ns, K, err);
     else
         prim3c_padded<FT>(pz, pc, pn, spn, zeta, coef, ns, K, NZ);
     __syncthreads();
+    const int nc = nprim ? ns : ns * NZ;
+    int same = threadIdx.x != 0 || (key[0] == n && key[1] == ntiles && key[2] == target_units && key[3] == nc);
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) same &= key[4 + t] == spn[t];
+    if (__syncthreads_and(same)) return;
     order3c_body(order, segs, items, spn, ntiles, n, ns, NZ, target_units);
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) key[4 + t] = spn[t];
+    if (threadIdx.x == 0) {
+        key[0] = n;
+        key[1] = ntiles;
+        key[2] = target_units;
+        key[3] = nc;
+    }
 }
 
 int setup_overlap3c_schedule(aok_plan* p) {
@@ -321,6 +336,10 @@ int setup_overlap3c_schedule(aok_plan* p) {
         return cuda_status(e, "cudaMalloc(prim3)");
     if ((e = cudaMalloc(&p->d_npp3, sizeof(int) * (size_t)(ns * p->NZ))) != cudaSuccess)
         return cuda_status(e, "cudaMalloc(nprim3)");
+    // the schedule key of k_prep3c: all ones (n = -1) matches no call, so the first builds
+    const size_t kbytes = sizeof(int) * (size_t)(4 + ns * p->NZ);
+    if ((e = cudaMalloc(&p->d_key3, kbytes)) != cudaSuccess) return cuda_status(e, "cudaMalloc(key3)");
+    if ((e = cudaMemset(p->d_key3, 0xFF, kbytes)) != cudaSuccess) return cuda_status(e, "cudaMemset(key3)");
     return AOK_OK;
 }
 
@@ -346,12 +365,12 @@ static int launch_prep3c(aok_plan* p, const void* zeta, const void* coef, const 
     if (p->prec == AOK_PREC_F64)
         k_prep3c<double><<<1, kOrder3Threads, 0, side>>>(
             (double*)p->d_pp3, (double*)p->d_pp3 + nt, p->d_npp3, (const double*)zeta, (const double*)coef, nprim,
-            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, ntiles, p->nitems3,
+            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, p->d_key3, (const Item3*)p->d_items3, ntiles, p->nitems3,
             (int)p->ns, (int)p->K, (int)p->NZ, target_units);
     else
         k_prep3c<float><<<1, kOrder3Threads, 0, side>>>(
             (float*)p->d_pp3, (float*)p->d_pp3 + nt, p->d_npp3, (const float*)zeta, (const float*)coef, nprim,
-            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, (const Item3*)p->d_items3, ntiles, p->nitems3,
+            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, p->d_key3, (const Item3*)p->d_items3, ntiles, p->nitems3,
             (int)p->ns, (int)p->K, (int)p->NZ, target_units);
     return cuda_status(cudaGetLastError(), "k_prep3c");
 }

@@ -219,3 +219,40 @@ def test_overlap3c_orbital_bad_species_and_limits():
     p7 = _dev.Plan(b7.ls, b7.K, 7, _lib.AOK_PREC_F64, 8)
     assert L.aok_overlap3c(p7.h, None, None, None, None, None, None, None, None, None, 0, 1.0, None) == \
         _lib.AOK_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, 1e-12), (torch.float32, 2e-6)])
+def test_schedule_follows_primitive_counts_and_batch(FT, tol):
+    """One plan, calls whose primitive counts or batch size change between calls: the
+    per-plan item order and segments are rebuilt whenever the counts or the tile count
+    differ from the last build and reused otherwise; every call matches the oracle."""
+    import ctypes
+    from aok_b200 import _dev, _lib
+    L = _lib.load()
+    b = W.config0_basis()
+    ls, nprim0, z0, _ = W.gb_tables(b)
+    coef_full = oracle.compile_coef(b.zeta, b.D, b.ls)
+    K = int(nprim0.max())
+    plan = _dev.Plan(ls, K, 1, _dev.prec_of(FT), 600)
+    rnd = f32_round if FT == torch.float32 else (lambda a: a)
+    # (primitive counts per shell, batch): the full contraction, a truncated one, the full
+    # one again at another batch size, and again at the first size
+    for cut, B in ((None, 600), ([3, 1, 1, 2, 1, 1], 600), (None, 97), (None, 600), ([1] * 6, 97)):
+        npr = nprim0.copy() if cut is None else np.minimum(nprim0, cut)
+        coef = np.concatenate([coef_full[s, :npr[s], 0] for s in range(len(ls))])
+        off0 = np.concatenate([[0], np.cumsum(nprim0)])
+        z = np.concatenate([z0[off0[s]:off0[s] + npr[s]] for s in range(len(ls))])
+        off = np.concatenate([[0], np.cumsum(npr)])[:-1]
+        tr = W.config4_triples(B=B, seed=B)
+        out = _dev.colmajor_empty((15, 15, 15, B), FT)
+        npd, offd = torch.as_tensor(npr).cuda(), torch.as_tensor(off).cuda()
+        dev = [torch.as_tensor(coef).to("cuda", FT), torch.as_tensor(z).to("cuda", FT)]
+        pos = [_dev.to_colmajor(p, FT) for p in (tr.posA, tr.posB, tr.posC)]
+        _lib.check(L.aok_overlap3c_gb(plan.h, _dev.ptr(out), ctypes.c_void_p(npd.data_ptr()),
+                                      ctypes.c_void_p(offd.data_ptr()), ctypes.c_void_p(dev[0].data_ptr()),
+                                      ctypes.c_void_p(dev[1].data_ptr()), *[_dev.ptr(p) for p in pos], B,
+                                      _dev.stream()))
+        V = out.double().cpu().numpy()
+        ref = oracle.overlap3c_gb(ls, npr, rnd(coef), rnd(z), rnd(tr.posA), rnd(tr.posB), rnd(tr.posC),
+                                  nthreads=8)
+        assert rel_fro(V, ref) < tol, (cut, B)
