@@ -142,6 +142,15 @@ template <> __host__ __device__ constexpr int rec_words16<double>(int la, int lb
 // ballot compaction.  Dynamic shared memory: pack2c_smem(nitems) bytes.
 // --------------------------------------------------------------------------
 constexpr int kOrderMax = 2048;
+// Per species pair, after the NZ*NZ stage images in the same allocation: the key of
+// the last k_pack2c build (stage size, non-zero counts of the bra and ket species'
+// shells; all ones until the first build), then per item of the execution order the
+// item and the 16-byte word at which its records start.
+constexpr int kPackKeyStride = 4 + 2 * kMaxShells;
+static_assert(sizeof(Item) == sizeof(long long), "an item is loaded as one 8-byte word");
+size_t pack2c_cache_bytes(size_t npairs, int nitems) {
+    return npairs * (sizeof(int) * kPackKeyStride + (sizeof(Item) + sizeof(int)) * (size_t)nitems);
+}
 
 size_t pack2c_smem(int nitems) { return (size_t)28 * nitems + 16; }
 int pack2c_parts(int nitems) { return std::min(16, std::max(1, (nitems + 15) / 16)); }
@@ -151,7 +160,9 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
                                                 int* __restrict__ nseg, const Item* __restrict__ items,
                                                 const FT* __restrict__ zeta, const FT* __restrict__ coef,
                                                 Panels panels, const int* __restrict__ boff, int nitems, int ns,
-                                                int K, int NZ, int N, int stage16, int pair16, int seg_stride) {
+                                                int K, int NZ, int N, int stage16, int pair16, int seg_stride,
+                                                int* __restrict__ pkey, Item* __restrict__ citems,
+                                                int* __restrict__ cdst) {
     extern __shared__ unsigned long long psm64[];
     unsigned long long* key = psm64;                               // nitems
     Item* sorted = reinterpret_cast<Item*>(psm64 + nitems);        // nitems; chunk = primitive pairs
@@ -177,6 +188,48 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
         s_nnz[i / ns][sh] = c;
     }
     __syncthreads();
+    // the primitive-pair records of item `it` at `out` (compacted non-zero pairs, (ip, jp) order)
+    auto write_records = [&](const Item it, FT* out) {
+        const int la = it.cls >> 2, lb = it.cls & 3;
+        const int words = rec_words16<FT>(la, lb) * (16 / (int)sizeof(FT));
+        const int nb = s_nnz[1][it.sb];
+        int n = 0;
+        for (int e0 = 0; e0 < K * K; e0 += 32) {
+            const int e = e0 + lane;
+            const int ip = e / K, jp = e % K;
+            double ca = 0.0, cb = 0.0, aa = 0.0, ab = 0.0;
+            if (e < K * K) {
+                ca = (double)coef[it.sa + ns * (ip + K * ga)];
+                cb = (double)coef[it.sb + ns * (jp + K * gb)];
+                aa = (double)zeta[it.sa + ns * (ip + K * ga)];
+                ab = (double)zeta[it.sb + ns * (jp + K * gb)];
+            }
+            const bool valid = (e < K * K) && ca != 0.0 && cb != 0.0;
+            const unsigned m = __ballot_sync(0xffffffffu, valid);
+            if (valid) fill_pp(out + (size_t)(n + __popc(m & ((1u << lane) - 1u))) * words, la, lb, ca, cb, aa, ab, nb);
+            n += __popc(m);
+        }
+    };
+    // Everything but the record values (order, chunks, headers, segments) follows from
+    // the stage size and the non-zero counts of the two species' shells.  When they
+    // equal the key of the last build for this pair, the headers and segments in place
+    // stand and only the records are rewritten, at the offsets cached with the key.
+    int* bkey = pkey + (size_t)pair * kPackKeyStride;
+    {
+        int same = tid != 0 || __ldcg(bkey) == stage16;
+        for (int i = tid; i < 2 * ns; i += blockDim.x) same &= __ldcg(bkey + 1 + i) == s_nnz[i / ns][i % ns];
+        if (__syncthreads_and(same)) {
+            __threadfence();
+            for (int i = blockIdx.y * NW + warp; i < nitems; i += gridDim.y * NW) {
+                const long long w = __ldcg(reinterpret_cast<const long long*>(citems) + (size_t)pair * nitems + i);
+                Item it;
+                memcpy(&it, &w, sizeof(Item));
+                const int d16 = __ldcg(cdst + (size_t)pair * nitems + i);
+                write_records(it, reinterpret_cast<FT*>(pk + (size_t)pair * pair16 + d16));
+            }
+            return;
+        }
+    }
     auto panel_of = [&](int i) {
         int pn = 0;
         while (pn + 1 < npan && i >= s_item0[pn + 1]) ++pn;
@@ -281,6 +334,22 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
     }
     __syncthreads();
     const int nch = s_nch;
+    if (blockIdx.y == 0) {  // the cache for the next call: order and record offsets, then the key
+        for (int i = tid; i < nitems; i += blockDim.x) {
+            int lo = 0, hi = nch - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (cst[mid] <= i) lo = mid;
+                else hi = mid - 1;
+            }
+            citems[(size_t)pair * nitems + i] = sorted[i];
+            cdst[(size_t)pair * nitems + i] = chd[lo] + (cst[lo + 1] - cst[lo] + 1) / 2 + P[i];
+        }
+        __threadfence();
+        __syncthreads();
+        for (int i = tid; i < 2 * ns; i += blockDim.x) bkey[1 + i] = s_nnz[i / ns][i % ns];
+        if (tid == 0) bkey[0] = stage16;
+    }
     for (int i = blockIdx.y * NW + warp; i < nitems; i += gridDim.y * NW) {
         const Item it = sorted[i];
         int lo = 0, hi = nch - 1;  // chunk j with cst[j] <= i < cst[j + 1]
@@ -292,7 +361,6 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
         const int a0 = cst[lo], a1 = cst[lo + 1];
         float4* cbase = pk + (size_t)pair * pair16 + P[a0] + chd[lo];
         const int r0 = (a1 - a0 + 1) / 2 + P[i] - P[a0];
-        const int la = it.cls >> 2, lb = it.cls & 3;
         if (lane == 0) {
             const int pn = panel_of(i);
             ExecItem e;
@@ -302,25 +370,7 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
             e.dst = (int16_t)((s_boff[it.sb] - s_col0[pn]) * N + s_boff[it.sa]);
             reinterpret_cast<ExecItem*>(cbase)[i - a0] = e;
         }
-        FT* out = reinterpret_cast<FT*>(cbase + r0);
-        const int words = rec_words16<FT>(la, lb) * (16 / (int)sizeof(FT));
-        const int nb = s_nnz[1][it.sb];
-        int n = 0;
-        for (int e0 = 0; e0 < K * K; e0 += 32) {
-            const int e = e0 + lane;
-            const int ip = e / K, jp = e % K;
-            double ca = 0.0, cb = 0.0, aa = 0.0, ab = 0.0;
-            if (e < K * K) {
-                ca = (double)coef[it.sa + ns * (ip + K * ga)];
-                cb = (double)coef[it.sb + ns * (jp + K * gb)];
-                aa = (double)zeta[it.sa + ns * (ip + K * ga)];
-                ab = (double)zeta[it.sb + ns * (jp + K * gb)];
-            }
-            const bool valid = (e < K * K) && ca != 0.0 && cb != 0.0;
-            const unsigned m = __ballot_sync(0xffffffffu, valid);
-            if (valid) fill_pp(out + (size_t)(n + __popc(m & ((1u << lane) - 1u))) * words, la, lb, ca, cb, aa, ab, nb);
-            n += __popc(m);
-        }
+        write_records(it, reinterpret_cast<FT*>(cbase + r0));
     }
 }
 
@@ -617,8 +667,10 @@ int setup_overlap2c_schedule(aok_plan* p, int ctas, size_t stage_req) {
     p->pair16 = (int)pair16;
     p->seg_stride = p->nitems + npan;
     const size_t npairs = (size_t)(p->NZ * p->NZ);
-    cudaError_t e = cudaMalloc(&p->d_pk, 16 * pair16 * npairs);
+    cudaError_t e = cudaMalloc(&p->d_pk, 16 * pair16 * npairs + pack2c_cache_bytes(npairs, (int)items.size()));
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(pk)");
+    e = cudaMemset((char*)p->d_pk + 16 * pair16 * npairs, 0xFF, sizeof(int) * kPackKeyStride * npairs);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemset(pack keys)");
     e = cudaMalloc(&p->d_segs, sizeof(Seg) * p->seg_stride * npairs);
     if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(segs)");
     e = cudaMalloc(&p->d_nseg, sizeof(int) * npairs);
@@ -660,16 +712,20 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
     const dim3 grid((unsigned)(p->NZ * p->NZ), (unsigned)pack2c_parts(p->nitems));
     const size_t smem = pack2c_smem(p->nitems);
     const int stage16 = (int)(p->stage_bytes / 16);
+    const size_t npairs = npairs_of(p);
+    int* pkey = (int*)((char*)p->d_pk + 16 * (size_t)p->pair16 * npairs);
+    Item* citems = (Item*)(pkey + kPackKeyStride * npairs);
+    int* cdst = (int*)(citems + npairs * (size_t)p->nitems);
     if (p->prec == AOK_PREC_F64)
         k_pack2c<double><<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items,
                                                  (const double*)zeta, (const double*)coef, p->panels, p->d_boff,
                                                  p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16,
-                                                 p->pair16, p->seg_stride);
+                                                 p->pair16, p->seg_stride, pkey, citems, cdst);
     else
         k_pack2c<float><<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items,
                                                 (const float*)zeta, (const float*)coef, p->panels, p->d_boff,
                                                 p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16,
-                                                p->pair16, p->seg_stride);
+                                                p->pair16, p->seg_stride, pkey, citems, cdst);
     return cuda_status(cudaGetLastError(), "k_pack2c");
 }
 

@@ -276,3 +276,42 @@ def test_f32c_elementwise_bound(which):
     assert np.all(err[m] <= bound[m]), float(np.max(err[m] / bound[m]))
     # below the threshold the absolute floor holds too
     assert np.all(err <= 1e-6 * smax + 4e-6 * np.abs(ref))
+
+
+@pytest.mark.parametrize("FT,tol", [(torch.float64, TOL64), (torch.float32, TOL32)])
+def test_zero_pattern_changes_between_calls_on_one_plan(FT, tol):
+    """One plan, parameters passed with every call, the set of zero coefficients changing
+    between calls: the packed execution order is rebuilt whenever a species pair's
+    non-zero counts differ from the last build, and reused (records rewritten) when they
+    do not.  Every call matches the oracle, and a repeated call is bitwise the same."""
+    import ctypes
+
+    from aok_b200 import _dev, _lib
+    b = W.config2_basis()
+    pr = W.config2_pairs(B=700)
+    N, ns, K, NZ = b.nbf_total, b.nshells, b.K, b.NZ
+    L = _lib.load()
+    plan = _dev.Plan(b.ls, K, NZ, _dev.prec_of(FT), pr.B)
+    coef0 = oracle.compile_coef(b.zeta, b.D, b.ls)
+    dA = torch.as_tensor(np.ascontiguousarray(pr.sidxA)).cuda()
+    dB = torch.as_tensor(np.ascontiguousarray(pr.sidxB)).cuda()
+    rnd = f32_round if FT == torch.float32 else (lambda a: a)
+    pA, pB = _dev.to_colmajor(pr.posA, FT), _dev.to_colmajor(pr.posB, FT)
+    zeta = _dev.to_colmajor(b.zeta, FT)
+    rng = np.random.default_rng(17)
+    drop = coef0.copy()
+    drop[rng.random(drop.shape) < 0.3] = 0.0  # other non-zero counts in most species pairs
+    scaled = coef0 * 0.5                      # same zero pattern as coef0, other values
+    outs = []
+    for c in (coef0, drop, coef0, scaled, scaled):
+        cd = _dev.to_colmajor(c, FT)
+        out = _dev.colmajor_zeros((N, N, pr.B), FT)
+        _lib.check(L.aok_overlap2c(plan.h, _dev.ptr(out), _dev.ptr(zeta), _dev.ptr(cd), _dev.ptr(pA), _dev.ptr(pB),
+                                   ctypes.c_void_p(dA.data_ptr()), ctypes.c_void_p(dB.data_ptr()), pr.B, 1.0,
+                                   _dev.stream()))
+        S = out.double().cpu().numpy()
+        ref = oracle.overlap2c_orb(b.ls, rnd(c), rnd(b.zeta), pr.sidxA, pr.sidxB, rnd(pr.posA), rnd(pr.posB),
+                                   nthreads=8)
+        assert rel_fro(S, ref) < tol
+        outs.append(S)
+    assert np.array_equal(outs[3], outs[4])
