@@ -16,6 +16,14 @@ constexpr int kMaxPairs = 256;     // species pairs (NZ <= 16)
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while its predecessor in the stream still runs;
+// pdl_wait() blocks until that predecessor has completed and its writes are
+// visible (a no-op for a kernel launched without the attribute), and
+// pdl_trigger() lets the successor's launch begin before this kernel ends.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Cartesian component c of a shell of momentum l, in the reference's order
 // (kernels_2c.jl:102-119): for x = l..0, for z = 0..l-x: (x, y = l-x-z, z).
 // Closed form (no loops, so unrolled call sites fold instantly): with

@@ -25,7 +25,7 @@ struct aok_plan {
     int4* d_tiles = nullptr;
     int* d_ntiles = nullptr;
     int* d_tbase = nullptr;          // first tile of each species pair (NZ*NZ + 1)
-    unsigned* d_counter = nullptr;
+    unsigned* d_counter = nullptr;   // work counters: [0] binning-reset kernels, [1] the rrule pullback
     int max_tiles = 0;
     // device error word (AOK_ERR_* of the first fault a kernel met)
     int* d_err = nullptr;
@@ -139,7 +139,24 @@ void timing_begin(aok_plan* p, cudaStream_t s);
 void timing_end(aok_plan* p, cudaStream_t s);
 
 // launchers (overlap2c.cu)
-int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s);
+// pdl: launched with programmatic serialisation after k_compile_coef on the same stream
+int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s, bool pdl = false);
+
+// Launch of `k` with programmatic stream serialisation (see pdl_wait / pdl_trigger).
+template <typename... Exp, typename... Act>
+cudaError_t launch_pdl(void (*k)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Act&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<Act&&>(args)...);
+}
 // Counting sort of a batch by species key (stable), tiles of 32 elements of
 // one key, and the first tile of each key.  Buffers: perm (B), tiles
 // (B/32 + NZ^2 + 1), tbase (NZ^2 + 1), blockhist (kBinMaxBlocksHost * NZ^2).
@@ -193,10 +210,10 @@ int launch_compile_coef_pb(aok_plan* p, void* dD, void* dzeta, const void* dcoef
 // overlap2c_bwd*.cu
 int launch_pb_f32(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
                   const void* zeta, const void* coef, const void* D, const void* posA, const void* posB,
-                  double lengthscale, cudaStream_t s);
+                  double lengthscale, cudaStream_t s, unsigned* counter);
 int launch_pb_f64(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
                   const void* zeta, const void* coef, const void* D, const void* posA, const void* posB,
-                  double lengthscale, cudaStream_t s);
+                  double lengthscale, cudaStream_t s, unsigned* counter);
 int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* zeta, const void* coef,
                         const void* D, const int64_t* sidxA, const int64_t* sidxB, const void* posA,
                         const void* posB, int64_t B, double lengthscale, int keep_absent, cudaStream_t s);

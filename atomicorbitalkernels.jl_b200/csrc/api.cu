@@ -153,7 +153,7 @@ int aok_plan_create(aok_plan** plan, int64_t nshells, const int64_t* ls, int64_t
         (st = dmalloc(&p->d_tiles, (size_t)p->max_tiles, "cudaMalloc(tiles)")) ||
         (st = dmalloc(&p->d_ntiles, 1, "cudaMalloc(ntiles)")) ||
         (st = dmalloc(&p->d_tbase, (size_t)(bin_keys_max(NZ) + 1), "cudaMalloc(tbase)")) ||
-        (st = dmalloc(&p->d_counter, 1, "cudaMalloc(counter)")) ||
+        (st = dmalloc(&p->d_counter, 2, "cudaMalloc(counter)")) ||
         (st = dmalloc(&p->d_err, 1, "cudaMalloc(err)")) ||
         (st = dmalloc_bytes(&p->d_gb_zeta, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_zeta)")) ||
         (st = dmalloc_bytes(&p->d_gb_coef, (size_t)(nshells * K) * fsz, "cudaMalloc(gb_coef)")) ||
@@ -515,8 +515,10 @@ int aok_overlap2c_rrule(aok_plan* p, void* out, const void* zeta, const void* D,
     AOK_TRY(cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord"));
     AOK_TRY(cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent"));
     AOK_TRY(launch_compile_coef(p, coef, zeta, D, p->side));
-    AOK_TRY(launch_prep2c(p, zeta, coef, p->side));
+    AOK_TRY(launch_prep2c(p, zeta, coef, p->side, true));
     AOK_TRY(cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord"));
+    // the pullback kernel's work counter (the forward kernel uses the first one)
+    AOK_TRY(cuda_status(cudaMemsetAsync(p->d_counter + 1, 0, sizeof(unsigned), p->side), "cudaMemsetAsync"));
     AOK_TRY(launch_prep_pb(p, zeta, coef, 0, p->side));
     AOK_TRY(cuda_status(cudaEventRecord(p->ev_pb, p->side), "cudaEventRecord"));
     AOK_TRY(launch_bin(p, sidxA, sidxB, B, s));

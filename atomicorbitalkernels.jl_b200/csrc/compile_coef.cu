@@ -19,6 +19,7 @@ namespace aok {
 template <typename FT>
 __global__ void k_compile_coef(FT* __restrict__ coef, const FT* __restrict__ zeta, const FT* __restrict__ D,
                                const int* __restrict__ ls, int ns, int K, int NZ) {
+    pdl_trigger();  // the record packing may launch now (it waits for this grid's end)
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= ns * NZ) return;
     const int s = q % ns, g = q / ns;

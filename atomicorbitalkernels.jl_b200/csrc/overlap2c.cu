@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(256) k_pack2c(float4* __restrict__ pk, Seg* __
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = 8;
     const int npan = panels.n;
+    pdl_wait();  // coef may come from the k_compile_coef launched just before
     if (tid <= npan) {
         s_item0[tid] = panels.item0[tid];
         s_col0[tid] = panels.col0[tid];
@@ -708,7 +709,7 @@ int launch_gb_pad(aok_plan* p, const int64_t* nprim, const int64_t* prim_offset,
     return cuda_status(cudaGetLastError(), "k_gb_pad");
 }
 
-int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s) {
+int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t s, bool pdl) {
     const dim3 grid((unsigned)(p->NZ * p->NZ), (unsigned)pack2c_parts(p->nitems));
     const size_t smem = pack2c_smem(p->nitems);
     const int stage16 = (int)(p->stage_bytes / 16);
@@ -716,17 +717,20 @@ int launch_prep2c(aok_plan* p, const void* zeta, const void* coef, cudaStream_t 
     int* pkey = (int*)((char*)p->d_pk + 16 * (size_t)p->pair16 * npairs);
     Item* citems = (Item*)(pkey + kPackKeyStride * npairs);
     int* cdst = (int*)(citems + npairs * (size_t)p->nitems);
-    if (p->prec == AOK_PREC_F64)
-        k_pack2c<double><<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items,
-                                                 (const double*)zeta, (const double*)coef, p->panels, p->d_boff,
-                                                 p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16,
-                                                 p->pair16, p->seg_stride, pkey, citems, cdst);
-    else
-        k_pack2c<float><<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items,
-                                                (const float*)zeta, (const float*)coef, p->panels, p->d_boff,
-                                                p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16,
-                                                p->pair16, p->seg_stride, pkey, citems, cdst);
-    return cuda_status(cudaGetLastError(), "k_pack2c");
+    auto go = [&](auto kern, auto zt, auto cf) {
+        if (pdl)
+            return launch_pdl(kern, grid, dim3(256), smem, s, (float4*)p->d_pk, p->d_segs, p->d_nseg,
+                              (const Item*)p->d_items, zt, cf, p->panels, (const int*)p->d_boff, p->nitems, (int)p->ns,
+                              (int)p->K, (int)p->NZ, (int)p->N, stage16, p->pair16, p->seg_stride, pkey, citems, cdst);
+        kern<<<grid, 256, smem, s>>>((float4*)p->d_pk, p->d_segs, p->d_nseg, p->d_items, zt, cf, p->panels, p->d_boff,
+                                     p->nitems, (int)p->ns, (int)p->K, (int)p->NZ, (int)p->N, stage16, p->pair16,
+                                     p->seg_stride, pkey, citems, cdst);
+        return cudaGetLastError();
+    };
+    const cudaError_t e = p->prec == AOK_PREC_F64
+                              ? go(k_pack2c<double>, (const double*)zeta, (const double*)coef)
+                              : go(k_pack2c<float>, (const float*)zeta, (const float*)coef);
+    return cuda_status(e, "k_pack2c");
 }
 
 int launch_bin3_into(const BinBufs& bb, const int64_t* sidxA, const int64_t* sidxB, const int64_t* sidxC,

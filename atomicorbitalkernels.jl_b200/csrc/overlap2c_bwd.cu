@@ -89,23 +89,26 @@ int launch_overlap2c_pb(aok_plan* p, void* out0, void* out1, const void* dS, con
     AOK_TRY_PB(launch_bin(p, sidxA, sidxB, B, s));
     AOK_TRY_PB(cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent"));
     if (p->prec == AOK_PREC_F64)
-        return launch_pb_f64(p, out0, out1, dS, nullptr, 1.0, zeta, coef, D, posA, posB, lengthscale, s);
-    return launch_pb_f32(p, out0, out1, dS, nullptr, 1.0, zeta, coef, D, posA, posB, lengthscale, s);
+        return launch_pb_f64(p, out0, out1, dS, nullptr, 1.0, zeta, coef, D, posA, posB, lengthscale, s,
+                             p->d_counter);
+    return launch_pb_f32(p, out0, out1, dS, nullptr, 1.0, zeta, coef, D, posA, posB, lengthscale, s,
+                         p->d_counter);
 }
 
 // The pullback of an rrule forward (aok_overlap2c_rrule): its bins and its
-// pullback records (prepared on the side stream, ev_pb) are reused; the work
-// counter, consumed by the forward kernel, is reset.  The cotangent is dS, or
+// pullback records (prepared on the side stream, ev_pb) are reused; its kernel
+// claims units from the plan's second work counter, which the rrule forward reset
+// on the side stream (the first one is the forward kernel's).  The cotangent is dS, or
 // alpha (dS - dS2) when dS2 is given.
 int launch_pb_prepared(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
                        const void* zeta, const void* D, const void* posA, const void* posB, double lengthscale,
                        cudaStream_t s) {
     AOK_TRY_PB(cuda_status(cudaStreamWaitEvent(s, p->ev_pb, 0), "cudaStreamWaitEvent"));
-    AOK_TRY_PB(cuda_status(cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned), s), "cudaMemsetAsync"));
     if (p->prec == AOK_PREC_F64)
         return launch_pb_f64(p, out0, out1, dS, dS2, alpha, zeta, p->d_coef_scratch, D, posA, posB, lengthscale,
-                             s);
-    return launch_pb_f32(p, out0, out1, dS, dS2, alpha, zeta, p->d_coef_scratch, D, posA, posB, lengthscale, s);
+                             s, p->d_counter + 1);
+    return launch_pb_f32(p, out0, out1, dS, dS2, alpha, zeta, p->d_coef_scratch, D, posA, posB, lengthscale, s,
+                         p->d_counter + 1);
 }
 
 }  // namespace aok

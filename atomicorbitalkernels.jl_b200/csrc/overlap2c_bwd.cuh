@@ -470,6 +470,7 @@ __device__ __forceinline__ int pb_nch(const int* tbase, int k) {
 
 template <typename FT, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c_pb(const __grid_constant__ PbParams<FT> P) {
+    pdl_trigger();  // the unit sums may launch now (they wait for this grid's end)
     constexpr int NW = THREADS / 32;
     __shared__ int chpre[kMaxPairs + 1];
     __shared__ PbWarpSmem<FT> wsm[NW];
@@ -524,6 +525,8 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c_pb(const __grid_con
 static __global__ void k_pb_sum_units(double* __restrict__ rows, const double* __restrict__ partial,
                                       const int4* __restrict__ counts, const int* __restrict__ tbase,
                                       const Item* __restrict__ items, int ns, int K, int np, int nitems, int gmax) {
+    pdl_wait();
+    pdl_trigger();
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (wid >= np * nitems) return;
@@ -592,6 +595,7 @@ template <typename FT>
 __global__ void k_pb_reduce(FT* __restrict__ dcoef, FT* __restrict__ dalpha, const double* __restrict__ rows,
                             const int* __restrict__ itemidx, const FT* __restrict__ zeta, const FT* __restrict__ coef,
                             int ns, int K, int NZ, int nitems, double alpha) {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int S = ns * K * NZ;
@@ -623,6 +627,7 @@ __global__ void k_pb_reduce_ps(FT* __restrict__ dD, FT* __restrict__ dz, const d
         const double nsq = coef_vjp_prepare<FT>(zeta, D, red + 2 * K, base, ns, K, ls[s], lane);
         if (lane == 0) s_nsq = nsq;
     }
+    pdl_wait();  // the parameter-only half above overlaps the unit sums
     for (int w = warp - 1; w >= 0 && w < 2 * K; w += nw - 1) {
         const double v = pb_slot_sum<FT>(rows, itemidx, zeta, coef, ns, K, NZ, nitems, w / K, s, w % K, sigma, lane);
         if (lane == 0) red[w] = alpha * v;  // the pullback is linear in the cotangent
@@ -645,7 +650,7 @@ template <typename FT> constexpr int pb_min_blocks() { return sizeof(FT) == 4 ? 
 template <typename FT, int THREADS>
 inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const void* dS2, double alpha,
                      const void* zeta, const void* coef, const void* D, const void* posA, const void* posB,
-                     double lengthscale, cudaStream_t s) {
+                     double lengthscale, cudaStream_t s, unsigned* counter) {
     constexpr int MINB = pb_min_blocks<FT>();
     PbParams<FT> P;
     memset(&P, 0, sizeof(P));
@@ -660,7 +665,7 @@ inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const 
     P.perm = p->d_perm;
     P.tiles = p->d_tiles;
     P.tbase = p->d_tbase;
-    P.counter = p->d_counter;
+    P.counter = counter;
     P.items = p->d_pb_items;
     P.nitems = p->nitems;
     P.np = (int)(p->NZ * p->NZ);
@@ -677,23 +682,27 @@ inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const 
     timing_end(p, s);
     AOK_TRY_PB(cuda_status(cudaGetLastError(), "k_overlap2c_pb"));
     const int nw1 = P.np * p->nitems;
-    k_pb_sum_units<<<(nw1 * 32 + 255) / 256, 256, 0, s>>>((double*)p->d_pb_rows, (const double*)p->d_partials,
-                                                         p->d_pb_counts, p->d_tbase, p->d_pb_items, (int)p->ns,
-                                                         (int)p->K, P.np, p->nitems, P.gmax);
-    AOK_TRY_PB(cuda_status(cudaGetLastError(), "k_pb_sum_units"));
+    // the two reductions start with programmatic serialisation (pdl_wait before their first read)
+    AOK_TRY_PB(cuda_status(launch_pdl(k_pb_sum_units, dim3((nw1 * 32 + 255) / 256), dim3(256), 0, s,
+                                      (double*)p->d_pb_rows, (const double*)p->d_partials,
+                                      (const int4*)p->d_pb_counts, (const int*)p->d_tbase,
+                                      (const Item*)p->d_pb_items, (int)p->ns, (int)p->K, P.np, p->nitems, P.gmax),
+                           "k_pb_sum_units"));
     if (D) {
         const size_t sm = sizeof(double) * (2 * p->K + 2 * p->K * p->K);
         if (sm > 48 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "pullback: K too large");
-        k_pb_reduce_ps<FT><<<(int)(p->ns * p->NZ), 256, sm, s>>>(
-            (FT*)out0, (FT*)out1, (const double*)p->d_pb_rows, p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
-            (const FT*)D, p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems, alpha);
-        return cuda_status(cudaGetLastError(), "k_pb_reduce_ps");
+        return cuda_status(launch_pdl(k_pb_reduce_ps<FT>, dim3((unsigned)(p->ns * p->NZ)), dim3(256), sm, s,
+                                      (FT*)out0, (FT*)out1, (const double*)p->d_pb_rows,
+                                      (const int*)p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef, (const FT*)D,
+                                      (const int*)p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems, alpha),
+                           "k_pb_reduce_ps");
     }
     const int S = (int)(p->ns * p->K * p->NZ);
-    k_pb_reduce<FT><<<(2 * S * 32 + 255) / 256, 256, 0, s>>>((FT*)out0, (FT*)out1, (const double*)p->d_pb_rows,
-                                                            p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef,
-                                                            (int)p->ns, (int)p->K, (int)p->NZ, p->nitems, alpha);
-    return cuda_status(cudaGetLastError(), "k_pb_reduce");
+    return cuda_status(launch_pdl(k_pb_reduce<FT>, dim3((2 * S * 32 + 255) / 256), dim3(256), 0, s, (FT*)out0,
+                                  (FT*)out1, (const double*)p->d_pb_rows, (const int*)p->d_pb_itemidx,
+                                  (const FT*)zeta, (const FT*)coef, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems,
+                                  alpha),
+                       "k_pb_reduce");
 }
 
 }  // namespace aok
