@@ -264,6 +264,9 @@ def main():
                     help="with --profile: which kernel family to run (ncu captures)")
     ap.add_argument("--no-extra", action="store_true", help="skip the config-1/3/4 side measurements")
     ap.add_argument("--fp64", action="store_true", help="with --profile: run the FP64 kernels (overlap2c, overlap3c)")
+    ap.add_argument("--timeline", action="store_true",
+                    help="with --profile: warm launch list of the steps from CUPTI (torch.profiler): each launch's "
+                         "start, end and duration within the last step, and the mean duration per kernel")
     ap.add_argument("--cpu-dry", action="store_true",
                     help="rank plumbing only, on CPU: gloo process group, barriers, max-over-ranks timing and the "
                          "gradient all-reduce of the step, with no kernels (for tests without a GPU)")
@@ -374,6 +377,8 @@ def main():
 
     if args.profile and args.workload not in ("overlap2c", "grad"):
         fn = side_workload(args.workload, L, _dev, _lib, aok, torch, args.batch, torch.float64 if args.fp64 else None)
+        if args.timeline:
+            return _timeline(fn, args.steps, args.warmup, torch)
         for _ in range(args.warmup + args.steps):
             fn()
         torch.cuda.synchronize()
@@ -383,6 +388,8 @@ def main():
     c32 = setup(torch.float32)
     if args.profile and args.workload == "grad":
         gd = _grad_setup(basis, c32, B, L, _dev, _lib, aok, torch)
+        if args.timeline:
+            return _timeline(gd["gstep_res"], args.steps, args.warmup, torch)
         for _ in range(args.warmup + args.steps):
             torch.cuda.nvtx.range_push("gradstep")  # ncu --nvtx --nvtx-include "gradstep/" selects the step's launches
             gd["gstep_res"]()
@@ -391,6 +398,8 @@ def main():
         return 0
     if args.profile:
         cp = setup(torch.float64) if args.fp64 else c32
+        if args.timeline:
+            return _timeline(lambda: step(cp), args.steps, args.warmup, torch)
         for _ in range(args.warmup + args.steps):
             step(cp)
         torch.cuda.synchronize()
@@ -734,6 +743,37 @@ def side_workload(name, L, _dev, _lib, aok, torch, B=None, FT=None):
                                                  ctypes.c_void_p(d["coef"].data_ptr()),
                                                  ctypes.c_void_p(d["alpha"].data_ptr()), _dev.ptr(d["pA"]),
                                                  _dev.ptr(d["pB"]), _dev.ptr(d["pC"]), d["B"], _dev.stream()))
+
+
+def _timeline(fn, steps, warmup, torch):
+    """Warm launch list: `warmup` untimed steps, then `steps` steps under torch.profiler (CUPTI
+    activity records, device timestamps).  Prints the last step's launches (start and end in us
+    from its first launch, duration) and each kernel's mean duration over all profiled steps."""
+    from torch.profiler import ProfilerActivity, profile
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(steps):
+            fn()
+        torch.cuda.synchronize()
+    ev = sorted((e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA),
+                key=lambda e: e.time_range.start)
+    per = max(1, len(ev) // max(steps, 1))
+    last = ev[-per:]
+    t0 = last[0].time_range.start
+    print(f"last step: {per} launches, {last[-1].time_range.end - t0:.1f} us from the first start to the last end")
+    print(" start_us   end_us    dur_us  launch")
+    for e in last:
+        a, b = e.time_range.start - t0, e.time_range.end - t0
+        print(f"{a:8.1f} {b:8.1f} {b - a:9.1f}  {e.name[:100]}")
+    agg = {}
+    for e in ev:
+        agg.setdefault(e.name[:100], []).append(e.time_range.end - e.time_range.start)
+    print(" mean_us  count  kernel")
+    for k, v in sorted(agg.items(), key=lambda kv: -sum(kv[1])):
+        print(f"{sum(v) / len(v):8.2f} {len(v):6d}  {k}")
+    return 0
 
 
 def _time(fn, steps, warmup, torch, allmax):
