@@ -226,10 +226,11 @@ int kernel_prepare(const void* k, size_t smem, int threads, int* occ);
 
 // overlap3c.cu
 int setup_overlap3c_schedule(aok_plan* p);
+// pdl: launched with programmatic serialisation after the prep on the same stream
 int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
-                   cudaStream_t s);
+                   cudaStream_t s, bool pdl);
 int launch_ov3_f64(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
-                   cudaStream_t s);
+                   cudaStream_t s, bool pdl);
 
 // orbitals.cu
 int launch_evaluate(aok_orbitals* o, void* P, void* dP, const void* X, const int64_t* sidx,

@@ -546,6 +546,7 @@ __global__ void k_bin_identity(int B, int np, int* __restrict__ perm, int4* __re
                                int* __restrict__ ntiles, int* __restrict__ tbase, unsigned* __restrict__ counter,
                                const int64_t* __restrict__ sidxA, const int64_t* __restrict__ sidxB,
                                const int64_t* __restrict__ sidxC, int NZ, int* __restrict__ err) {
+    pdl_trigger();  // a programmatic successor may launch now (it waits for this grid's end)
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     const int nt = (B + kTileB - 1) / kTileB;
     if (b < B && (sidxA || sidxB || sidxC)) (void)pair_key(sidxA, sidxB, sidxC, b, B, NZ, err);

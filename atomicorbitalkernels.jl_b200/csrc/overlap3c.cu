@@ -275,6 +275,7 @@ __global__ void __launch_bounds__(kOrder3Threads) k_prep3c(FT* __restrict__ pz, 
                                                            int* __restrict__ key, const Item3* __restrict__ items,
                                                            int ntiles, int n, int ns, int K, int NZ, int target_units) {
     __shared__ int spn[kMaxShells * 6];
+    pdl_trigger();  // the kernel may launch now; it waits for this grid's end
     if (nprim)
         prim3c_flat<FT>(pz, pc, pn, spn, nprim, off, coef, zeta, ns, K, err);
     else
@@ -283,7 +284,10 @@ __global__ void __launch_bounds__(kOrder3Threads) k_prep3c(FT* __restrict__ pz, 
     const int nc = nprim ? ns : ns * NZ;
     int same = threadIdx.x != 0 || (key[0] == n && key[1] == ntiles && key[2] == target_units && key[3] == nc);
     for (int t = threadIdx.x; t < nc; t += blockDim.x) same &= key[4 + t] == spn[t];
-    if (__syncthreads_and(same)) return;
+    if (__syncthreads_and(same)) {
+        pdl_wait();  // launched after the bins: they are complete once this grid is
+        return;
+    }
     order3c_body(order, segs, items, spn, ntiles, n, ns, NZ, target_units);
     for (int t = threadIdx.x; t < nc; t += blockDim.x) key[4 + t] = spn[t];
     if (threadIdx.x == 0) {
@@ -292,6 +296,7 @@ __global__ void __launch_bounds__(kOrder3Threads) k_prep3c(FT* __restrict__ pz, 
         key[2] = target_units;
         key[3] = nc;
     }
+    pdl_wait();
 }
 
 int setup_overlap3c_schedule(aok_plan* p) {
@@ -354,25 +359,30 @@ static int check_units3(const aok_plan* p, int64_t B, const char* who) {
 
 // The 3C prep for B elements on stream `side` (see k_prep3c): the compact primitive
 // lists of the padded (zeta, coef) tables, or of the flat tables when nprim is given
-// (zeta = alpha), and the per-call item order and segments.
+// (zeta = alpha), and the per-call item order and segments.  pdl: launched with
+// programmatic serialisation right after the binning on the same stream.
 static int launch_prep3c(aok_plan* p, const void* zeta, const void* coef, const int64_t* nprim,
-                         const int64_t* prim_offset, int64_t B, cudaStream_t side) {
+                         const int64_t* prim_offset, int64_t B, cudaStream_t side, bool pdl) {
     const size_t nt = (size_t)(p->ns * p->K * p->NZ);
     // FP32: about eight (segment, tile) pairs per resident warp (three CTAs of four warps
     // per SM); FP64: about one item per segment
     const int target_units = p->prec == AOK_PREC_F64 ? (1 << 30) : p->num_sms * 3 * (kThreads3 / 32) * 8;
     const int ntiles = (int)std::min<int64_t>((B + 31) / 32, 1 << 30);
-    if (p->prec == AOK_PREC_F64)
-        k_prep3c<double><<<1, kOrder3Threads, 0, side>>>(
-            (double*)p->d_pp3, (double*)p->d_pp3 + nt, p->d_npp3, (const double*)zeta, (const double*)coef, nprim,
-            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, p->d_key3, (const Item3*)p->d_items3, ntiles, p->nitems3,
-            (int)p->ns, (int)p->K, (int)p->NZ, target_units);
-    else
-        k_prep3c<float><<<1, kOrder3Threads, 0, side>>>(
-            (float*)p->d_pp3, (float*)p->d_pp3 + nt, p->d_npp3, (const float*)zeta, (const float*)coef, nprim,
-            prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, p->d_key3, (const Item3*)p->d_items3, ntiles, p->nitems3,
-            (int)p->ns, (int)p->K, (int)p->NZ, target_units);
-    return cuda_status(cudaGetLastError(), "k_prep3c");
+    auto go = [&](auto kern, auto pz, auto zt, auto cf) {
+        if (pdl)
+            return launch_pdl(kern, dim3(1), dim3(kOrder3Threads), 0, side, pz, pz + nt, p->d_npp3, zt, cf, nprim,
+                              prim_offset, p->d_err, (Item3*)p->d_order3, p->d_segs3, p->d_key3,
+                              (const Item3*)p->d_items3, ntiles, p->nitems3, (int)p->ns, (int)p->K, (int)p->NZ,
+                              target_units);
+        kern<<<1, kOrder3Threads, 0, side>>>(pz, pz + nt, p->d_npp3, zt, cf, nprim, prim_offset, p->d_err,
+                                             (Item3*)p->d_order3, p->d_segs3, p->d_key3, (const Item3*)p->d_items3,
+                                             ntiles, p->nitems3, (int)p->ns, (int)p->K, (int)p->NZ, target_units);
+        return cudaGetLastError();
+    };
+    const cudaError_t e = p->prec == AOK_PREC_F64
+                              ? go(k_prep3c<double>, (double*)p->d_pp3, (const double*)zeta, (const double*)coef)
+                              : go(k_prep3c<float>, (float*)p->d_pp3, (const float*)zeta, (const float*)coef);
+    return cuda_status(e, "k_prep3c");
 }
 
 // The 3C overlap: the prep on the plan's side stream while `bin` bins the batch on s,
@@ -380,16 +390,24 @@ static int launch_prep3c(aok_plan* p, const void* zeta, const void* coef, const 
 template <typename Bin>
 static int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
                             const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
-                            int64_t B, double lengthscale, cudaStream_t s, Bin bin) {
+                            int64_t B, double lengthscale, cudaStream_t s, Bin bin, bool chain) {
     int st;
-    if ((st = cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord")) != AOK_OK) return st;
-    if ((st = cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent")) != AOK_OK) return st;
-    if ((st = launch_prep3c(p, zeta, coef, nprim, prim_offset, B, p->side)) != AOK_OK) return st;
-    if ((st = cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord")) != AOK_OK) return st;
-    if ((st = bin()) != AOK_OK) return st;
-    if ((st = cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent")) != AOK_OK) return st;
-    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s);
-    return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s);
+    if (chain) {
+        // one stream: the (one-launch) binning, then the prep and the kernel, each launched
+        // programmatically so that its launch overlaps its predecessor
+        if ((st = bin()) != AOK_OK) return st;
+        if ((st = launch_prep3c(p, zeta, coef, nprim, prim_offset, B, s, true)) != AOK_OK) return st;
+    } else {
+        if ((st = cuda_status(cudaEventRecord(p->ev_fork, s), "cudaEventRecord")) != AOK_OK) return st;
+        if ((st = cuda_status(cudaStreamWaitEvent(p->side, p->ev_fork, 0), "cudaStreamWaitEvent")) != AOK_OK)
+            return st;
+        if ((st = launch_prep3c(p, zeta, coef, nprim, prim_offset, B, p->side, false)) != AOK_OK) return st;
+        if ((st = cuda_status(cudaEventRecord(p->ev_join, p->side), "cudaEventRecord")) != AOK_OK) return st;
+        if ((st = bin()) != AOK_OK) return st;
+        if ((st = cuda_status(cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent")) != AOK_OK) return st;
+    }
+    if (p->prec == AOK_PREC_F64) return launch_ov3_f64(p, out, posA, posB, posC, lengthscale, s, chain);
+    return launch_ov3_f32(p, out, posA, posB, posC, lengthscale, s, chain);
 }
 
 }  // namespace aok
@@ -411,7 +429,7 @@ extern "C" int aok_overlap3c_gb(aok_plan* p, void* out, const int64_t* nprim, co
     if ((st = check_units3(p, B, "aok_overlap3c_gb")) != AOK_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     return launch_overlap3c(p, out, alpha, coef, nprim, prim_offset, posA, posB, posC, B, 1.0, s,
-                            [&] { return launch_bin(p, nullptr, nullptr, B, s); });
+                            [&] { return launch_bin(p, nullptr, nullptr, B, s); }, true);
 }
 
 extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const void* posA,
@@ -431,5 +449,5 @@ extern "C" int aok_overlap3c(aok_plan* p, void* out, const void* zeta, const voi
     ++p->gen;  // the plan's bins change
     const BinBufs bb{p->d_perm, p->d_tiles, p->d_ntiles, p->d_tbase, p->d_counter, p->d_blockhist, p->d_err};
     return launch_overlap3c(p, out, zeta, coef, nullptr, nullptr, posA, posB, posC, B, lengthscale, s,
-                            [&] { return launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s); });
+                            [&] { return launch_bin3_into(bb, sidxA, sidxB, sidxC, B, (int)p->NZ, s); }, false);
 }

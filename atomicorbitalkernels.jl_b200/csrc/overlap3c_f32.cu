@@ -4,9 +4,9 @@
 namespace aok {
 
 int launch_ov3_f32(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
-                   cudaStream_t s) {
-    if (p->Lmax > kMaxL3Spec) return launch_ov3<float, true>(p, out, posA, posB, posC, lengthscale, s);
-    return launch_ov3<float, false>(p, out, posA, posB, posC, lengthscale, s);
+                   cudaStream_t s, bool pdl) {
+    if (p->Lmax > kMaxL3Spec) return launch_ov3<float, true>(p, out, posA, posB, posC, lengthscale, s, pdl);
+    return launch_ov3<float, false>(p, out, posA, posB, posC, lengthscale, s, pdl);
 }
 
 }  // namespace aok

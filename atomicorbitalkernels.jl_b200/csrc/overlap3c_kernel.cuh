@@ -619,6 +619,7 @@ __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constan
     __shared__ PT recbuf[W][32];                                    // each warp's current 32 records
     __shared__ __align__(16) FT xbuf[(W - 1) * kSplitM3 * 32 * (sizeof(FT) == 4 ? 2 : 1)];  // split partial sums
     __shared__ unsigned claim;
+    pdl_wait();  // launched programmatically after the prep: its order and the bins are complete past here
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ntiles = *P.ntiles, nseg = P.segs[P.nitems + 1], H = P.segs[P.nitems + 2];
     const unsigned ngroups = (unsigned)(ntiles + W - 1) / W;
@@ -689,7 +690,7 @@ __global__ void __launch_bounds__(kThreads3, 3) k_overlap3c(const __grid_constan
 
 template <typename FT, bool F3>
 inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB, const void* posC, double lengthscale,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool pdl) {
     Ov3Params<FT> P;
     memset(&P, 0, sizeof(P));
     P.out = (FT*)out;
@@ -718,9 +719,17 @@ inline int launch_ov3(aok_plan* p, void* out, const void* posA, const void* posB
     const int st = kernel_prepare((const void*)kern, 0, kThreads3, &occ);
     if (st != AOK_OK) return st;
     timing_begin(p, s);
-    kern<<<p->num_sms * std::max(occ, 1), kThreads3, 0, s>>>(P);
+    cudaError_t e;
+    // timing events recorded around the kernel sit between it and the prep: launch it plainly then
+    const bool timed = !p->ev.empty() && 2 * p->ev_used + 1 < (int)p->ev.size();
+    if (pdl && !timed) {
+        e = launch_pdl(kern, dim3(p->num_sms * std::max(occ, 1)), dim3(kThreads3), 0, s, P);
+    } else {
+        kern<<<p->num_sms * std::max(occ, 1), kThreads3, 0, s>>>(P);
+        e = cudaGetLastError();
+    }
     timing_end(p, s);
-    return cuda_status(cudaGetLastError(), "k_overlap3c");
+    return cuda_status(e, "k_overlap3c");
 }
 
 }  // namespace aok
