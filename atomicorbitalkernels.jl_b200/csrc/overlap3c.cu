@@ -260,8 +260,10 @@ __device__ __forceinline__ void order3c_body(Item3* __restrict__ order, int* __r
 // One CTA per call ahead of the kernel: the compact primitive lists (from the padded
 // tables, or from flat GaussianBasis-style tables when nprim is given), then the
 // queue order and its segments.  It needs no binning result (the segment count uses
-// the tile count of the batch, ntiles = ceil(B / 32)), so it runs on the plan's side
-// stream while the batch is binned.
+// the tile count of the batch, ntiles = ceil(B / 32)), so on the species-aware path it
+// runs on the plan's side stream while the batch is binned; on the single-species path
+// it follows the one-launch identity binning programmatically on the caller's stream
+// and waits for the bins only before it ends.
 // The order and the segments are a function of (n, ntiles, target_units) and the
 // primitive counts alone, and key[] holds those of the last build: when they match
 // (the usual case, a fixed basis over many batches) the sort and the cut are skipped
@@ -386,7 +388,8 @@ static int launch_prep3c(aok_plan* p, const void* zeta, const void* coef, const 
 }
 
 // The 3C overlap: the prep on the plan's side stream while `bin` bins the batch on s,
-// then the kernel over the plan's bins once both are done.
+// then the kernel over the plan's bins once both are done; with `chain` (a one-launch
+// binning) all three on s, the prep and the kernel launched programmatically.
 template <typename Bin>
 static int launch_overlap3c(aok_plan* p, void* out, const void* zeta, const void* coef, const int64_t* nprim,
                             const int64_t* prim_offset, const void* posA, const void* posB, const void* posC,
