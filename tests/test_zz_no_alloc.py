@@ -179,3 +179,21 @@ def test_noalloc_rejects_oversized_batch_but_not_dx_only():
     _lib.check(st)
     torch.cuda.synchronize()
     assert bool(torch.isfinite(dX).all())
+
+
+def test_noalloc_takes_no_device_memory():
+    """After a first call on the device (module load, the static scratch's address), further
+    calls change the device's free memory by nothing: the entry point allocates nothing."""
+    FT, nX = torch.float32, 20000
+    b, orb, d = _setup(FT, nX, 23)
+    dX = _dev.colmajor_empty((3, nX), FT)
+    dz = _dev.colmajor_empty(b.zeta.shape, FT)
+    dD = _dev.colmajor_empty(b.zeta.shape, FT)
+    _lib.check(_call(orb, b, d, FT, nX, dX, dz, dD))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        _lib.check(_call(orb, b, d, FT, nX, dX, dz, dD))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert _lib.load().aok_evaluate_pullback_noalloc_check(_dev.stream()) == 0
