@@ -525,7 +525,6 @@ __global__ void __launch_bounds__(THREADS, MINB) k_overlap2c_pb(const __grid_con
 static __global__ void k_pb_sum_units(double* __restrict__ rows, const double* __restrict__ partial,
                                       const int4* __restrict__ counts, const int* __restrict__ tbase,
                                       const Item* __restrict__ items, int ns, int K, int np, int nitems, int gmax) {
-    pdl_wait();
     pdl_trigger();
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -540,6 +539,9 @@ static __global__ void k_pb_sum_units(double* __restrict__ rows, const double* _
     const int4 n = counts[((size_t)k * ns + wi.sa) * ns + wi.sb];
     const int ng = (n.x * n.y + n.z * n.y + n.w * n.x + 31) / 32;
     const int nu = nch * ng;
+    // the bins, counts and items above were complete before the pullback kernel started;
+    // only the partial rows below come from it
+    pdl_wait();
     double* out = rows + ((size_t)k * nitems + i) * 4 * K;
     for (int c = lane; c < 4 * K; c += 32) {
         double sum = 0.0;
@@ -691,7 +693,16 @@ inline int launch_pb(aok_plan* p, void* out0, void* out1, const void* dS, const 
     if (D) {
         const size_t sm = sizeof(double) * (2 * p->K + 2 * p->K * p->K);
         if (sm > 48 * 1024) return set_error(AOK_ERR_UNSUPPORTED, "pullback: K too large");
-        return cuda_status(launch_pdl(k_pb_reduce_ps<FT>, dim3((unsigned)(p->ns * p->NZ)), dim3(256), sm, s,
+        // one warp per slot sum (2K of them) plus the VJP warp, as far as the kernel's
+        // registers allow in one CTA (the kernel loops over the slots otherwise)
+        static int max_thr = 0;
+        if (max_thr == 0) {
+            cudaFuncAttributes fa;
+            max_thr = cudaFuncGetAttributes(&fa, k_pb_reduce_ps<FT>) == cudaSuccess ? fa.maxThreadsPerBlock : 256;
+        }
+        const int want = 32 * (int)(2 * p->K + 1), cap = max_thr / 32 * 32;
+        const unsigned thr = (unsigned)(want < cap ? want : cap < 64 ? 64 : cap);
+        return cuda_status(launch_pdl(k_pb_reduce_ps<FT>, dim3((unsigned)(p->ns * p->NZ)), dim3(thr), sm, s,
                                       (FT*)out0, (FT*)out1, (const double*)p->d_pb_rows,
                                       (const int*)p->d_pb_itemidx, (const FT*)zeta, (const FT*)coef, (const FT*)D,
                                       (const int*)p->d_ls, (int)p->ns, (int)p->K, (int)p->NZ, p->nitems, alpha),
