@@ -256,3 +256,40 @@ def test_schedule_follows_primitive_counts_and_batch(FT, tol):
         ref = oracle.overlap3c_gb(ls, npr, rnd(coef), rnd(z), rnd(tr.posA), rnd(tr.posB), rnd(tr.posC),
                                   nthreads=8)
         assert rel_fro(V, ref) < tol, (cut, B)
+
+
+def test_single_stream_chain_equals_plain_launches():
+    """The single-species call launches the prep and the kernel programmatically after their
+    predecessors; with the plan's kernel timing on, the kernel is launched plainly instead.
+    Both give the same output bit for bit, call after call."""
+    import ctypes
+    from aok_b200 import _dev, _lib
+    L = _lib.load()
+    FT, B = torch.float64, 777
+    b = W.config0_basis()
+    ls, nprim, z, _ = W.gb_tables(b)
+    coef_full = oracle.compile_coef(b.zeta, b.D, b.ls)
+    coef = np.concatenate([coef_full[s, :nprim[s], 0] for s in range(len(ls))])
+    off = np.concatenate([[0], np.cumsum(nprim)])[:-1]
+    plan = _dev.Plan(ls, int(nprim.max()), 1, _dev.prec_of(FT), B)
+    tr = W.config4_triples(B=B, seed=3)
+    npd, offd = torch.as_tensor(nprim).cuda(), torch.as_tensor(off).cuda()
+    cd, zd = torch.as_tensor(coef).to("cuda", FT), torch.as_tensor(z).to("cuda", FT)
+    pos = [_dev.to_colmajor(p, FT) for p in (tr.posA, tr.posB, tr.posC)]
+
+    def run():
+        out = _dev.colmajor_zeros((15, 15, 15, B), FT)
+        _lib.check(L.aok_overlap3c_gb(plan.h, _dev.ptr(out), ctypes.c_void_p(npd.data_ptr()),
+                                      ctypes.c_void_p(offd.data_ptr()), ctypes.c_void_p(cd.data_ptr()),
+                                      ctypes.c_void_p(zd.data_ptr()), *[_dev.ptr(p) for p in pos], B, _dev.stream()))
+        return out.cpu().numpy()
+
+    chained = [run(), run()]
+    _lib.check(L.aok_plan_timing_enable(plan.h, 4))
+    plain = [run(), run()]
+    _lib.check(L.aok_plan_timing_enable(plan.h, 0))
+    again = run()
+    for v in chained[1:] + plain + [again]:
+        assert np.array_equal(v, chained[0])
+    ref = oracle.overlap3c_gb(ls, nprim, coef, z, tr.posA, tr.posB, tr.posC, nthreads=8)
+    assert rel_fro(chained[0], ref) < 1e-12
